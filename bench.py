@@ -1,0 +1,387 @@
+"""Benchmark of the B200 pair_style tensormd path: MD atom-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config bcc128k|fcc4k|alloy432k]
+
+Workload (default): BCC a = 2.87 A, 40x40x40 cells = 128,000 atoms, Gaussian
+displacements sigma = 0.08 A, 600 K Maxwell velocities, one element, 16
+Gaussian radial functions, rc = 6.0 A cosine cutoff, moments of rank <= 3,
+MLP 64-64-64-1 tanh (random weights, seeded), NVE dt = 1 fs, neighbor skin
+1.0 A.  A step is one velocity-Verlet MD step: half kick + drift, rebuild
+check (rebuild when an atom moved more than skin/2), descriptor, MLP and its
+backward, pair forces, gather, half kick.
+
+value: atom-steps/s with all state resident in HBM (tmd_nve_run), timed with
+CUDA events on the library's stream, max over ranks.  e2e: the same metric
+through the reference-facing call pattern with host buffers (per step: H2D of
+positions from pinned memory, force evaluation, D2H of forces, velocity
+Verlet on the host, as LAMMPS drives PairTensorMD::compute).  N > 1 GPUs run
+independent replicas (weak scaling, no collective in the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "lammps-tensormd_b200"))
+
+METRIC = "atom-steps/s on 1 B200, BF16 vs plain FP32 at stated force err; p50/p99 latency"
+UNIT = "atom-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="bcc128k")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(cfg_name, seed):
+    from tmd_b200 import synth
+    c = synth.config(cfg_name)
+    tmp = Path(tempfile.mkdtemp(prefix="tmdbench"))
+    pot = tmp / f"{cfg_name}.npz"
+    syms = synth.gaussian_potential(pot, seed=1234, **c["pot"])
+    x, t, box, v = synth.build_system(c["kind"], c["a"], c["cells"], sigma=c["sigma"],
+                                      T=c["T"], nelt=c["nelt"], seed=seed)
+    cfg = {"workload": cfg_name, "natoms": int(len(x)), "lattice": c["kind"], "a": c["a"],
+           "cells": list(c["cells"]), "elements": c["nelt"],
+           "num_filters": c["pot"]["num_filters"], "rc": c["pot"]["rc"],
+           "max_moment": c["pot"]["max_moment"],
+           "mlp": [c["pot"]["nelt"] * c["pot"]["num_filters"] * (c["pot"]["max_moment"] + 1)]
+           + list(c["pot"]["hidden"]) + [1],
+           "actfn": {1: "softplus", 2: "tanh", 3: "squareplus"}[c["pot"]["actfn"]],
+           "dt_fs": 1.0, "skin": 1.0, "sigma": c["sigma"], "T": c["T"]}
+    return str(pot), syms, x, t, box, v, cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [q.strip() for q in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, p[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the force kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "force_traffic.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return d
+        except Exception:
+            return None
+    return None
+
+
+def algorithmic(cfg, npairs_rc, nlist, B, K, D, nin):
+    """Algorithmic FLOPs and HBM bytes per launch of the force kernel.
+
+    FLOPs: the U and V contractions, 2 x (2 K D) per pair inside rc
+    (tensor_ops.cpp kernel_U / kernel_V).  Bytes: each input read once and
+    each output written once: x (24 B/atom), neighbor row (4 B/entry), P
+    (4 B K D B), G and dE/dG (2 x 4 nin), pair forces (16 B/entry), virial
+    partials (48 B/atom)."""
+    n = cfg["natoms"]
+    flops = 4.0 * K * D * npairs_rc
+    bytes_ = n * (24 + 4 * B * K * D + 8 * nin + 48) + nlist * (4 + 16)
+    return flops, bytes_
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from tmd_b200 import TensorMDModel, TensorMDSystem
+    pot, syms, x, t, box, v, cfg = workload(args.config, seed=42 + rank)
+    n = len(x)
+    model = TensorMDModel(f"{pot} {' '.join(syms)}", device=local)
+    sys_ = TensorMDSystem(model, n, 1.0)
+    sys_.set_box(box)
+    sys_.set_atoms(x, t, v)
+    stream = torch.cuda.ExternalStream(sys_.stream(), device=dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=dev)
+    dt = 0.001
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # warm-up
+    sys_.nve_run(max(args.warmup, 3), dt)
+    torch.cuda.synchronize()
+    # timed region
+    l0 = sys_.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        sys_.nve_run(args.steps, dt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = sys_.launches() - l0
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = n * args.steps * world / (ms_max / 1000.0)
+
+    # per-kernel device times of the same step sequence (a second, profiled pass)
+    sys_.profile(True)
+    sys_.profile_read(reset=True)
+    nprof = max(10, min(args.steps, 50))
+    sys_.nve_run(nprof, dt)
+    prof = sys_.profile_read(reset=True)
+    sys_.profile(False)
+
+    # force-kernel roofline
+    off, ent = sys_.neighbor_list(model.cutmax)
+    npairs_rc = len(ent)
+    nlist = len(sys_.neighbor_list(model.cutmax + 1.0)[1])
+    B, K, D = model.nelt, model.num_filters, {1: 1, 2: 4, 3: 10, 4: 20}[model.mmax]
+    flops, abytes = algorithmic(cfg, npairs_rc, nlist, B, K, D, model.n_desc)
+    fcnt, fms = prof["force"]
+    force_ms = fms / max(fcnt, 1)
+    hbm_peak, peak_kind = measured_peaks()
+    clocks = clk.summary()
+    sm_mhz = clocks["sm_mhz"] or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
+    tr = ncu_traffic()
+    traffic = None
+    if tr and tr.get("workload") == args.config:
+        traffic = tr.get("bytes_per_launch")
+    ach_gbs = abytes / (force_ms / 1000.0) / 1e9
+    ach_tf = flops / (force_ms / 1000.0) / 1e12
+    roofline = {"kernel": "k_force", "bound": "hbm", "achieved": ach_gbs,
+                "peak": hbm_peak, "unit": "GB/s", "frac": ach_gbs / hbm_peak,
+                "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "algorithmic_bytes_per_launch": abytes, "launch_ms": force_ms}
+    roofline_fp32 = {"kernel": "k_force", "bound": "fp32", "achieved": ach_tf,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach_tf / fp32_peak,
+                     "peak_source": "148 SMs x 128 FP32 lanes x 2 x sampled SM clock "
+                                    "(no FP32 figure in MEASURED_PEAKS.json)",
+                     "algorithmic_flops_per_launch": flops}
+    kernel_ms = {k: (c, t / max(c, 1)) for k, (c, t) in prof.items()}
+
+    # e2e through the reference-facing call pattern (host buffers)
+    sys_.set_atoms(x, t, v)
+    xh = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    vh = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    fh = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    xh[:] = x
+    vh[:] = v
+    from tmd_b200.synth import MVV2E
+    from tmd_b200 import synth
+    masses = np.array([synth.MASSES.get(s, 50.0) for s in syms])[t - 1][:, None]
+    dtf = 0.5 * dt / MVV2E
+    import ctypes
+    from tmd_b200.lib import check
+    lib = sys_.lib
+    pd = ctypes.POINTER(ctypes.c_double)
+    xp, fp = xh.ctypes.data_as(pd), fh.ctypes.data_as(pd)
+    e = np.zeros(1)
+    vir = np.zeros(6)
+
+    def e2e_step():
+        # LAMMPS Verlet step with the pair on the device: initial integrate on
+        # the host, positions H2D, pair compute, forces D2H, final integrate
+        vh[:] += dtf / masses * fh
+        xh[:] += dt * vh
+        check(lib.tmd_system_set_positions(sys_.h, xp))
+        check(lib.tmd_compute(sys_.h, 1, 1, 1.0, e.ctypes.data_as(pd), vir.ctypes.data_as(pd),
+                              fp, None, None))
+        vh[:] += dtf / masses * fh
+
+    check(lib.tmd_compute(sys_.h, 1, 1, 1.0, e.ctypes.data_as(pd), vir.ctypes.data_as(pd),
+                          fp, None, None))
+    for _ in range(3):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    t1 = time.perf_counter()
+    e2e_s = torch.tensor([t1 - t0], device=dev, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    e2e_val = n * args.e2e_steps * world / float(e2e_s.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.config, samples=2)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32", "data": "synthetic (seeded lattice, random-init potential weights)",
+            "config": dict(cfg, parallelism=f"replicas x{world}", precision="plain fp32",
+                           l2="working set > 126 MB L2 (neighbor rows, pair forces, P)"),
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+                    "d2h_bytes_per_step": 24 * n + 7 * 8, "steps": args.e2e_steps,
+                    "timing": "host wall clock, includes host velocity Verlet"},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "roofline": roofline,
+            "roofline_fp32": roofline_fp32,
+            "kernel_ms": kernel_ms,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(cfg_name, samples=2):
+    """The FP64 oracle (port of the reference math, OpenMP) on a bounded
+    sample: `samples` full MD steps (neighbor build + force) of the workload."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from pack import Oracle, load_npz
+    pot, syms, x, t, box, v, cfg = workload(cfg_name, seed=42)
+    o = Oracle(load_npz(pot))
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    o.nve(x[:8], v[:8], (t - 1)[:8], box, [1, 1, 1], 0.001, 1)  # load / warm
+    t0 = time.perf_counter()
+    o.nve(x, v, t - 1, box, [1, 1, 1], 0.001, samples - 1, skin=1.0)
+    t1 = time.perf_counter()
+    val = len(x) * samples / (t1 - t0)
+    return {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{samples} full MD steps (neighbor rebuild + FP64 force) of the "
+                      f"{cfg['natoms']}-atom workload, oracle/tmd_oracle.c, OpenMP "
+                      f"{cores} threads"}
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference has no CPU pair path and its GPU path
+    cannot evaluate this potential (analytic radial basis, tanh MLP), so the
+    CPU restatement of its math (oracle, FP64, OpenMP) is timed instead."""
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from pack import Oracle, load_npz
+    pot, syms, x, t, box, v, cfg = workload(args.config, seed=42)
+    o = Oracle(load_npz(pot))
+    per = 1
+    for _ in range(max(1, min(args.warmup, 1))):
+        o.nve(x, v, t - 1, box, [1, 1, 1], 0.001, 0, skin=1.0)
+    steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    o.nve(x, v, t - 1, box, [1, 1, 1], 0.001, steps - 1, skin=1.0)
+    t1 = time.perf_counter()
+    val = len(x) * steps / (t1 - t0)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT,
+            "n_gpus": world, "steps": steps, "warmup": 1, "ms_per_step": (t1 - t0) * 1000 / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+            "data": "synthetic", "config": dict(cfg, parallelism="cpu"),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{steps} MD steps of the {cfg['natoms']}-atom workload "
+                                       "(FP64 oracle restatement, OpenMP)"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+/* tmd_b200.h -- C ABI of the B200 (sm_100a) force path of pair_style tensormd.
+ *
+ * A drop-in for the path PairTensorMD::compute -> TensorMD::calc_tensor_density
+ * -> TensorMD::run (src/ML-TENSORMD/pair_tensormd.cpp:141-184,
+ * tensormd.cpp:369-615): neighbor list -> tensor-moment descriptor ->
+ * per-element MLP and its backward -> forces/virial -> velocity Verlet.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: TMD_OK (0) or a negative code.
+ *     Nothing throws across the ABI; tmd_last_error() returns the message of
+ *     the last failure on the calling thread.
+ *   - The caller owns host arrays; the library owns device memory.  One CUDA
+ *     stream per system; a handle is used from one host thread at a time.
+ *   - Units are LAMMPS "metal": Angstrom, eV, ps, g/mol.
+ *   - box[9] = {xlo, ylo, zlo, xprd, yprd, zprd, xy, xz, yz} (LAMMPS
+ *     triclinic convention: a = (xprd,0,0), b = (xy,yprd,0), c = (xz,yz,zprd)).
+ *   - virial[6] and vatom rows are ordered xx, yy, zz, xy, xz, yz with
+ *     W = -sum_pairs r_ij (x) dE_i/dx_j, the value LAMMPS virial_fdotr_compute
+ *     (src/pair.cpp:1735-1776) returns for this pair style.
+ */
+#ifndef TMD_B200_H
+#define TMD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TMD_OK 0
+#define TMD_ERR_ARG (-1)       /* invalid argument */
+#define TMD_ERR_CUDA (-2)      /* CUDA runtime error (message has the call) */
+#define TMD_ERR_MODEL (-3)     /* potential file missing keys / unsupported */
+#define TMD_ERR_CAPACITY (-4)  /* atom or neighbor capacity exceeded */
+#define TMD_ERR_NONFINITE (-5) /* NaN/Inf in energies or forces */
+#define TMD_ERR_IO (-6)        /* cannot open or parse a file */
+#define TMD_ERR_STATE (-7)     /* call order (e.g. compute before set_atoms) */
+#define TMD_ERR_TIMEOUT (-8)   /* a bounded device wait gave up */
+
+/* MLP arithmetic of a loaded model.  FP32 is the plain form (FP32 arithmetic,
+ * FP64 cutoff test, energy/virial sums and position update). */
+#define TMD_PREC_FP32 0
+#define TMD_PREC_BF16 1
+#define TMD_PREC_FP8 2
+
+typedef struct tmd_model tmd_model;
+typedef struct tmd_system tmd_system;
+
+/* pair_coeff arguments after "* *":  "file.npz El1 El2 ... [interp dx]
+ * [cmax exact|default] [precision fp32|bf16|fp8]".
+ * Replaces PairTensorMD::coeff + read_potential_file + TensorMD::read_npz /
+ * setup_global / setup_interpolation (pair_tensormd.cpp:214-317,376-399;
+ * tensormd.cpp:109-280,438-446).  The element list maps LAMMPS atom types
+ * 1..n to potential elements exactly as PairTensorMD::setup_eltmap
+ * (pair_tensormd.cpp:349-370).  `device` is the CUDA ordinal. */
+int tmd_model_load(const char *coeff_args, int device, tmd_model **out);
+
+/* Free a model (systems created from it must be freed first). */
+void tmd_model_free(tmd_model *model);
+
+/* Model facts: cutmax (PairTensorMD::init_one, pair_tensormd.cpp:336-341),
+ * number of elements of the potential, number of LAMMPS types mapped,
+ * descriptor width (b*k*m), filters k, moments m.  Any pointer may be NULL. */
+int tmd_model_info(const tmd_model *model, double *cutmax, int *nelt,
+                   int *ntypes, int *n_desc, int *num_filters, int *mmax);
+
+/* map[t] (t = 1..ntypes) -> potential element index, -1 if unmapped
+ * (PairTensorMD::map); mass[t] -> mass the potential file gives that type
+ * (PairTensorMD::coeff sets atom->mass from it, pair_tensormd.cpp:303-312).
+ * Arrays have ntypes+1 entries; index 0 is unused. */
+int tmd_model_type_map(const tmd_model *model, int *map, double *mass);
+
+/* A device-resident periodic cell of up to natoms_cap atoms.  skin is the
+ * neighbor skin (LAMMPS `neighbor <skin> bin`); the list cutoff is
+ * cutmax + skin. */
+int tmd_system_create(const tmd_model *model, int natoms_cap, double skin,
+                      tmd_system **out);
+void tmd_system_free(tmd_system *sys);
+
+/* Box (see conventions) and periodic flags; forces a neighbor rebuild. */
+int tmd_system_set_box(tmd_system *sys, const double box[9], const int pbc[3]);
+
+/* Upload n atoms: x[n*3] positions, type[n] LAMMPS types (1-based, mapped
+ * through the pair_coeff element list), v[n*3] velocities (may be NULL).
+ * Types are fixed until the next call.  Positions outside the box are
+ * wrapped by the next neighbor rebuild as Domain::pbc() does. */
+int tmd_system_set_atoms(tmd_system *sys, int n, const double *x,
+                         const int *type, const double *v);
+
+/* Replace positions only (same n and types); the cheap per-step upload of
+ * the LAMMPS drop-in.  Triggers a rebuild check on the next compute. */
+int tmd_system_set_positions(tmd_system *sys, const double *x);
+
+/* Download state; NULL pointers are skipped.  image[n*3] are the periodic
+ * image counters accumulated by wrapping (Domain::pbc image flags). */
+int tmd_system_get(tmd_system *sys, double *x, double *v, double *f,
+                   int *image);
+
+/* One force evaluation: PairTensorMD::compute(eflag, vflag).  Outputs (any
+ * may be NULL, which leaves the value on the device): energy (eng_vdwl),
+ * virial[6], f[n*3], eatom[n], vatom[n*6].  scale is the pair_coeff scale
+ * factor of fix adapt (1.0 normally; PairTensorMD::extract("scale")). */
+int tmd_compute(tmd_system *sys, int eflag, int vflag, double scale,
+                double *energy, double *virial, double *f, double *eatom,
+                double *vatom);
+
+/* nsteps of velocity Verlet (FixNVE initial/final_integrate,
+ * fix_nve.cpp:64-141, metal units) driven as Verlet::run does
+ * (verlet.cpp:229-349), positions and velocities resident on the device,
+ * neighbor rebuild when an atom moved more than skin/2 (neigh_modify every 1
+ * delay 0 check yes).  If thermo is not NULL it receives (pe, ke) after
+ * every thermo_every-th step and the last one: rows = nsteps/thermo_every
+ * (+1 if nsteps % thermo_every != 0).  dt in ps. */
+int tmd_nve_run(tmd_system *sys, int nsteps, double dt, int thermo_every,
+                double *thermo);
+
+/* Export the current full neighbor list with cutoff `cut` (<= cutmax +
+ * skin) for parity checks: counts[n]; entries[total*4] = (j, sx, sy, sz)
+ * where the neighbor is atom j shifted by sx*a + sy*b + sz*c.  Pass
+ * entries = NULL to get the total in *total only.  cap = entries capacity. */
+int tmd_neighbor_list(tmd_system *sys, double cut, int *counts, int *entries,
+                      long cap, long *total);
+
+/* Per-atom descriptors G[n * n_desc] (compute tensormd/density,
+ * compute_tensormd_density.cpp:129-200) of the last compute, in atom order. */
+int tmd_get_descriptors(tmd_system *sys, double *G);
+
+/* CUDA stream of the system (cudaStream_t as void*), for event timing. */
+int tmd_system_stream(tmd_system *sys, void **stream);
+
+/* Number of kernels the library launched since the system was created. */
+long tmd_system_launches(const tmd_system *sys);
+
+/* Kernel timing (TensorMDTimer's phase report, tensormd_timer.h:25-46, with
+ * CUDA events instead of host clocks).  enable != 0 records an event pair
+ * around every kernel family on the system stream during tmd_compute and
+ * tmd_nve_run; tmd_profile_read returns, per family, the number of launches
+ * and the summed device milliseconds since the last reset.  Families:
+ * 0 neighbor build, 1 descriptor, 2 mlp, 3 force, 4 gather, 5 nve+check,
+ * 6 reductions.  Arrays hold TMD_NPROF entries. */
+#define TMD_NPROF 7
+int tmd_profile_enable(tmd_system *sys, int enable);
+int tmd_profile_read(tmd_system *sys, long *launches, double *ms, int reset);
+
+/* Copy the message of the last failed call on this thread into buf. */
+int tmd_last_error(char *buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TMD_B200_H */

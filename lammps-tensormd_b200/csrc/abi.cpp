@@ -1,0 +1,816 @@
+// abi.cpp -- the C ABI of include/tmd_b200.h.
+//
+// Host orchestration of one force evaluation (PairTensorMD::compute,
+// pair_tensormd.cpp:141-184, and TensorMD::calc_tensor_density/run,
+// tensormd.cpp:369-615) and of the NVE loop (Verlet::run + FixNVE,
+// verlet.cpp:229-349, fix_nve.cpp:64-141) on one stream, with every array
+// resident in device memory:
+//
+//   [nve initial] -> rebuild check -> (rebuild: bin, build, sort, partners)
+//   -> descriptor (P, G) -> MLP forward/backward (E, dE/dG) -> pair forces
+//   -> gather (f, FP64) -> [nve final] -> FP64 energy / virial sums
+//
+// The reference copies the neighbor list and positions to the device and the
+// forces back every step with ~15 device synchronisations
+// (kernel.cu:1500-1541,1760-1789); here the host synchronises only to return
+// requested results.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/tmd_b200.h"
+#include "model.h"
+#include "tmd_kernels.h"
+
+using namespace tmd;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define TMD_CUDA(call)                                                        \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return fail(TMD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T));
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+}  // namespace
+
+struct tmd_model {
+  int device = 0;
+  HostModel h;
+  KParams kp;
+  float *d_table = nullptr;
+  std::vector<float *> d_buf;   // weights and biases
+  MlpLayer *d_layers = nullptr;
+  double *d_mass = nullptr;     // per element
+  int mlp_tr = 64;
+  size_t mlp_smem = 0;
+  int nsys = 0;
+};
+
+struct tmd_system {
+  const tmd_model *m = nullptr;
+  cudaStream_t st = nullptr;
+  long launches = 0;
+  int natoms_cap = 0, n = 0;
+  double skin = 1.0;
+  bool have_box = false, have_atoms = false, have_v = false;
+  bool forces_valid = false;
+  BoxP box{};
+  BinP bin{};
+  int cap = 0, capp = 0;  // neighbor entries per atom, pow2 >= cap
+  int ncell_alloc = 0;
+  // device state
+  double *x = nullptr, *v = nullptr, *f = nullptr, *xbuild = nullptr;
+  int *image = nullptr, *elem = nullptr;
+  int *cell_of = nullptr, *cell_count = nullptr, *cell_start = nullptr,
+      *cell_cursor = nullptr, *cell_atoms = nullptr;
+  uint32_t *tmp = nullptr, *nbr = nullptr;
+  int *nraw = nullptr, *boff = nullptr, *rev = nullptr;
+  float *P = nullptr, *G = nullptr, *dEdG = nullptr, *E = nullptr;
+  float4 *pdf = nullptr;
+  double *wv = nullptr, *eatom = nullptr, *vatom = nullptr, *ke = nullptr;
+  double *partial = nullptr, *scal = nullptr;  // scal: [0] pe, [1..6] virial, [7] ke
+  int *flag = nullptr, *status = nullptr, *maxneed = nullptr;
+  int *perm = nullptr, *tiles = nullptr;
+  int ntiles = 0;
+  double *thermo_d = nullptr;
+  int thermo_rows_alloc = 0;
+  // host
+  std::vector<int> h_elem;
+  double *h_scal = nullptr;  // pinned [8]
+  int *h_status = nullptr;   // pinned [2]
+  // kernel timing
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+  long prof_n[TMD_NPROF] = {0};
+  double prof_ms[TMD_NPROF] = {0};
+  cudaEvent_t cur_start = nullptr;
+};
+
+namespace {
+
+cudaEvent_t prof_event(tmd_system *s) {
+  if (!s->ev_pool.empty()) {
+    cudaEvent_t e = s->ev_pool.back();
+    s->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void prof_begin(tmd_system *s) {
+  if (!s->prof) return;
+  s->cur_start = prof_event(s);
+  cudaEventRecord(s->cur_start, s->st);
+}
+
+void prof_end(tmd_system *s, int fam) {
+  if (!s->prof) return;
+  cudaEvent_t e = prof_event(s);
+  cudaEventRecord(e, s->st);
+  s->ev_pending.push_back({fam, {s->cur_start, e}});
+  if (s->ev_pending.size() > 4096) {  // resolve to bound the pool
+    cudaEventSynchronize(e);
+    for (auto &p : s->ev_pending) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+      s->prof_n[p.first]++;
+      s->prof_ms[p.first] += ms;
+      s->ev_pool.push_back(p.second.first);
+      s->ev_pool.push_back(p.second.second);
+    }
+    s->ev_pending.clear();
+  }
+}
+
+void box_setup(BoxP &b, const double bx[9], const int pbc[3]) {
+  b.lo[0] = bx[0]; b.lo[1] = bx[1]; b.lo[2] = bx[2];
+  b.xprd = bx[3]; b.yprd = bx[4]; b.zprd = bx[5];
+  b.xy = bx[6]; b.xz = bx[7]; b.yz = bx[8];
+  b.pbc[0] = pbc[0] ? 1 : 0; b.pbc[1] = pbc[1] ? 1 : 0; b.pbc[2] = pbc[2] ? 1 : 0;
+  b.triclinic = (b.xy != 0.0 || b.xz != 0.0 || b.yz != 0.0) ? 1 : 0;
+  // inverse of h = [[xprd, xy, xz], [0, yprd, yz], [0, 0, zprd]]
+  b.hinv[0] = 1.0 / b.xprd;
+  b.hinv[1] = 1.0 / b.yprd;
+  b.hinv[2] = 1.0 / b.zprd;
+  b.hinv[3] = -b.xy / (b.xprd * b.yprd);
+  b.hinv[4] = (b.xy * b.yz - b.yprd * b.xz) / (b.xprd * b.yprd * b.zprd);
+  b.hinv[5] = -b.yz / (b.yprd * b.zprd);
+}
+
+// Perpendicular widths of the cell (distance between opposite faces).
+void widths(const BoxP &b, double w[3]) {
+  double a[3] = {b.xprd, 0, 0}, bb[3] = {b.xy, b.yprd, 0}, c[3] = {b.xz, b.yz, b.zprd};
+  auto cross = [](const double *u, const double *v, double *o) {
+    o[0] = u[1] * v[2] - u[2] * v[1];
+    o[1] = u[2] * v[0] - u[0] * v[2];
+    o[2] = u[0] * v[1] - u[1] * v[0];
+  };
+  double V = b.xprd * b.yprd * b.zprd;
+  double t[3];
+  cross(bb, c, t); w[0] = V / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  cross(c, a, t); w[1] = V / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  cross(a, bb, t); w[2] = V / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+}
+
+int bin_setup(tmd_system *s) {
+  double cut = s->m->h.rmax + s->skin;
+  double w[3];
+  widths(s->box, w);
+  BinP b{};
+  long ncell = 1;
+  for (int a = 0; a < 3; a++) {
+    // bins slightly wider than cut/2 so a +-2 stencil covers the cutoff with
+    // a margin far above rounding of the fractional coordinates
+    int nb = (int)std::floor(w[a] / (0.5 * cut * (1.0 + 1e-6)));
+    if (nb < 1) nb = 1;
+    if (nb > 1024) nb = 1024;
+    b.nb[a] = nb;
+    int ns = (int)std::ceil(cut * (1.0 + 1e-9) / (w[a] / nb));
+    if (!s->box.pbc[a] && ns > nb) ns = nb;
+    if (ns < 1) ns = 1;
+    if (s->box.pbc[a] && (ns + nb - 1) / nb > kShiftR + 1)
+      return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff: more than "
+                               "3 images per axis would be needed");
+    b.ns[a] = ns;
+    ncell *= nb;
+  }
+  while (ncell > (1 << 22)) {  // keep the cell arrays modest
+    int a = (b.nb[0] >= b.nb[1] && b.nb[0] >= b.nb[2]) ? 0 : (b.nb[1] >= b.nb[2] ? 1 : 2);
+    b.nb[a] = (b.nb[a] + 1) / 2;
+    b.ns[a] = (int)std::ceil(cut * (1.0 + 1e-9) / (w[a] / b.nb[a]));
+    ncell = (long)b.nb[0] * b.nb[1] * b.nb[2];
+  }
+  b.ncell = (int)ncell;
+  s->bin = b;
+  if (b.ncell > s->ncell_alloc) {
+    dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_cursor);
+    TMD_CUDA(dalloc(&s->cell_count, b.ncell));
+    TMD_CUDA(dalloc(&s->cell_start, b.ncell + 1));
+    TMD_CUDA(dalloc(&s->cell_cursor, b.ncell));
+    s->ncell_alloc = b.ncell;
+  }
+  return TMD_OK;
+}
+
+int pow2_at_least(int v) {
+  int p = 32;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+int alloc_neighbors(tmd_system *s, int cap) {
+  cap = (cap + 31) / 32 * 32;
+  if (cap > 4096) return fail(TMD_ERR_CAPACITY, "more than 4096 neighbors per atom");
+  dfree(s->tmp); dfree(s->nbr); dfree(s->rev); dfree(s->pdf);
+  size_t tot = (size_t)s->natoms_cap * cap;
+  TMD_CUDA(dalloc(&s->tmp, tot));
+  TMD_CUDA(dalloc(&s->nbr, tot));
+  TMD_CUDA(dalloc(&s->rev, tot));
+  TMD_CUDA(dalloc(&s->pdf, tot));
+  s->cap = cap;
+  s->capp = pow2_at_least(cap);
+  return TMD_OK;
+}
+
+int initial_cap(tmd_system *s) {
+  double cut = s->m->h.rmax + s->skin;
+  double V = s->box.xprd * s->box.yprd * s->box.zprd;
+  double dens = s->n / V;
+  double est = dens * 4.0 / 3.0 * M_PI * cut * cut * cut;
+  int cap = (int)std::ceil(1.3 * est) + 32;
+  if (cap < 64) cap = 64;
+  return cap;
+}
+
+NbArgs nb_args(tmd_system *s) {
+  NbArgs a{};
+  a.n = s->n; a.B = s->m->h.nelt; a.cap = s->cap; a.capp = s->capp;
+  a.kp = s->m->kp; a.box = s->box; a.bin = s->bin;
+  double cut = s->m->h.rmax + s->skin;
+  a.cutsq = cut * cut;
+  a.x = s->x; a.image = s->image; a.elem = s->elem;
+  a.cell_of = s->cell_of; a.cell_count = s->cell_count; a.cell_start = s->cell_start;
+  a.cell_cursor = s->cell_cursor; a.cell_atoms = s->cell_atoms;
+  a.tmp = s->tmp; a.nraw = s->nraw; a.nbr = s->nbr; a.boff = s->boff; a.rev = s->rev;
+  a.xbuild = s->xbuild; a.flag = s->flag; a.status = s->status; a.maxneed = s->maxneed;
+  return a;
+}
+
+// Read the status words and clear them for the next kernels.
+int read_status(tmd_system *s) {
+  TMD_CUDA(cudaMemcpyAsync(s->h_status, s->status, 2 * sizeof(int),
+                           cudaMemcpyDeviceToHost, s->st));
+  TMD_CUDA(cudaMemsetAsync(s->status, 0, 2 * sizeof(int), s->st));
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  return TMD_OK;
+}
+
+int clear_status(tmd_system *s) {
+  TMD_CUDA(cudaMemsetAsync(s->status, 0, 2 * sizeof(int), s->st));
+  return TMD_OK;
+}
+
+// Rebuild the list now (flag forced), growing the capacity until it fits.
+int rebuild_now(tmd_system *s) {
+  for (int attempt = 0; attempt < 4; attempt++) {
+    int rc = clear_status(s);
+    if (rc) return rc;
+    launch_set_flag(s->flag, s->st, s->launches);
+    launch_neighbor_build(nb_args(s), s->st, s->launches);
+    TMD_CUDA(cudaGetLastError());
+    rc = read_status(s);
+    if (rc) return rc;
+    int st = s->h_status[0];
+    if (st & kStatusShift)
+      return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
+    if (st & kStatusOutside)
+      return fail(TMD_ERR_ARG, "atom outside a non-periodic boundary");
+    if (!(st & kStatusOverflow)) return TMD_OK;
+    int need = s->h_status[1];
+    rc = alloc_neighbors(s, need + need / 4 + 32);
+    if (rc) return rc;
+  }
+  return fail(TMD_ERR_CAPACITY, "neighbor list did not fit after resizing");
+}
+
+// Force evaluation on the current (valid) list.
+void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
+  const tmd_model *m = s->m;
+  DescArgs d{};
+  d.n = s->n; d.cap = s->cap; d.kp = m->kp; d.box = s->box; d.x = s->x;
+  d.elem = s->elem; d.nbr = s->nbr; d.boff = s->boff; d.P = s->P; d.G = s->G;
+  prof_begin(s);
+  launch_descriptor(d, s->st, s->launches);
+  prof_end(s, 1);
+  MlpArgs ma{};
+  ma.nl = m->h.nl; ma.actfn = m->h.actfn; ma.resnet = m->h.resnet; ma.nin = m->h.nin;
+  int maxh = 1;
+  for (int l = 1; l < m->h.nl; l++) maxh = std::max(maxh, m->h.sizes[l]);
+  ma.maxh = maxh; ma.tr = m->mlp_tr; ma.smem = m->mlp_smem;
+  ma.ntiles = s->ntiles; ma.tiles = s->tiles; ma.perm = s->perm; ma.G = s->G;
+  ma.dEdG = s->dEdG; ma.E = s->E; ma.layers = m->d_layers;
+  prof_begin(s);
+  launch_mlp_fp32(ma, s->st, s->launches);
+  prof_end(s, 2);
+  ForceArgs fa{};
+  fa.n = s->n; fa.cap = s->cap; fa.kp = m->kp; fa.box = s->box; fa.scale = scale;
+  fa.x = s->x; fa.elem = s->elem; fa.nbr = s->nbr; fa.boff = s->boff; fa.P = s->P;
+  fa.G = s->G; fa.dEdG = s->dEdG; fa.pdf = s->pdf; fa.wv = s->wv;
+  prof_begin(s);
+  launch_force(fa, s->st, s->launches);
+  prof_end(s, 3);
+  GatherArgs ga{};
+  ga.n = s->n; ga.cap = s->cap; ga.B = m->h.nelt; ga.boff = s->boff; ga.pdf = s->pdf;
+  ga.rev = s->rev; ga.nbr = s->nbr; ga.x = s->x; ga.box = s->box; ga.wv = s->wv;
+  ga.f = s->f; ga.vatom = want_vatom ? s->vatom : nullptr;
+  prof_begin(s);
+  launch_gather(ga, s->st, s->launches);
+  prof_end(s, 4);
+}
+
+}  // namespace
+
+extern "C" {
+
+int tmd_last_error(char *buf, int len) {
+  if (!buf || len <= 0) return TMD_ERR_ARG;
+  std::snprintf(buf, (size_t)len, "%s", g_err.c_str());
+  return TMD_OK;
+}
+
+int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
+  if (!coeff_args || !out) return fail(TMD_ERR_ARG, "null argument");
+  *out = nullptr;
+  tmd_model *m = new tmd_model();
+  try {
+    m->h = parse_model(coeff_args);
+  } catch (const ModelError &e) {
+    delete m;
+    return fail(TMD_ERR_MODEL, e.what());
+  } catch (const std::exception &e) {
+    delete m;
+    return fail(TMD_ERR_IO, e.what());
+  }
+  m->device = device;
+  cudaError_t ce = cudaSetDevice(device);
+  if (ce != cudaSuccess) {
+    delete m;
+    return fail(TMD_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
+  }
+  const HostModel &h = m->h;
+  fill_kparams(h, m->kp);
+  auto up = [&](const std::vector<float> &v, float **p) -> cudaError_t {
+    cudaError_t e = dalloc(p, v.size());
+    if (e != cudaSuccess) return e;
+    m->d_buf.push_back(*p);
+    return cudaMemcpy(*p, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice);
+  };
+  std::vector<MlpLayer> layers((size_t)h.nelt * h.nl);
+  cudaError_t e = cudaSuccess;
+  if (h.tab_n > 0) {
+    e = up(h.table, &m->d_table);
+    m->kp.table = m->d_table;
+  }
+  for (int el = 0; el < h.nelt && e == cudaSuccess; el++)
+    for (int l = 0; l < h.nl && e == cudaSuccess; l++) {
+      MlpLayer &L = layers[(size_t)el * h.nl + l];
+      L.K = h.sizes[l];
+      L.N = h.sizes[l + 1];
+      float *w = nullptr, *b = nullptr;
+      e = up(h.W[el][l], &w);
+      if (e == cudaSuccess && !h.Bs[el][l].empty()) e = up(h.Bs[el][l], &b);
+      L.W = w;
+      L.b = b;
+    }
+  if (e == cudaSuccess) e = dalloc(&m->d_layers, layers.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpy(m->d_layers, layers.data(), layers.size() * sizeof(MlpLayer),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = dalloc(&m->d_mass, h.nelt);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(m->d_mass, h.masses.data(), h.nelt * sizeof(double),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    tmd_model_free(m);
+    return fail(TMD_ERR_CUDA, std::string("model upload: ") + cudaGetErrorString(e));
+  }
+  // MLP tile: 64 atoms when the shared-memory footprint allows, else 32
+  size_t s64 = mlp_fp32_smem(h.nl, h.sizes.data(), 64);
+  size_t s32 = mlp_fp32_smem(h.nl, h.sizes.data(), 32);
+  if (s64 <= 110 * 1024) {
+    m->mlp_tr = 64; m->mlp_smem = s64;
+  } else if (s32 <= 220 * 1024) {
+    m->mlp_tr = 32; m->mlp_smem = s32;
+  } else {
+    tmd_model_free(m);
+    return fail(TMD_ERR_MODEL, "MLP too wide for the shared-memory tile");
+  }
+  mlp_fp32_prepare(m->mlp_tr, m->mlp_smem);
+  *out = m;
+  return TMD_OK;
+}
+
+void tmd_model_free(tmd_model *m) {
+  if (!m) return;
+  for (float *p : m->d_buf) cudaFree(p);
+  if (m->d_layers) cudaFree(m->d_layers);
+  if (m->d_mass) cudaFree(m->d_mass);
+  delete m;
+}
+
+int tmd_model_info(const tmd_model *m, double *cutmax, int *nelt, int *ntypes,
+                   int *n_desc, int *num_filters, int *mmax) {
+  if (!m) return fail(TMD_ERR_ARG, "null model");
+  if (cutmax) *cutmax = m->h.rmax;
+  if (nelt) *nelt = m->h.nelt;
+  if (ntypes) *ntypes = (int)m->h.type_elements.size();
+  if (n_desc) *n_desc = m->h.nin;
+  if (num_filters) *num_filters = m->h.K;
+  if (mmax) *mmax = m->h.M;
+  return TMD_OK;
+}
+
+int tmd_model_type_map(const tmd_model *m, int *map, double *mass) {
+  if (!m) return fail(TMD_ERR_ARG, "null model");
+  for (size_t t = 0; t < m->h.typemap.size(); t++) {
+    if (map) map[t] = m->h.typemap[t];
+    if (mass) mass[t] = m->h.typemass[t];
+  }
+  return TMD_OK;
+}
+
+int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
+                      tmd_system **out) {
+  if (!m || !out || natoms_cap < 1) return fail(TMD_ERR_ARG, "bad system arguments");
+  if (natoms_cap > kMaxAtoms) return fail(TMD_ERR_CAPACITY, "too many atoms for one system");
+  if (!(skin >= 0)) return fail(TMD_ERR_ARG, "skin must be >= 0");
+  *out = nullptr;
+  TMD_CUDA(cudaSetDevice(m->device));
+  tmd_system *s = new tmd_system();
+  s->m = m;
+  s->natoms_cap = natoms_cap;
+  s->skin = skin;
+  const HostModel &h = m->h;
+  size_t N = natoms_cap;
+  cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+#define A(p, cnt) if (e == cudaSuccess) e = dalloc(&s->p, (cnt))
+  A(x, 3 * N); A(v, 3 * N); A(f, 3 * N); A(xbuild, 3 * N);
+  A(image, 3 * N); A(elem, N);
+  A(cell_of, N); A(cell_atoms, N);
+  A(nraw, N); A(boff, N * (h.nelt + 1));
+  A(P, N * h.nelt * h.K * h.D); A(G, N * h.nin); A(dEdG, N * h.nin); A(E, N);
+  A(wv, 6 * N); A(eatom, N); A(vatom, 6 * N); A(ke, N);
+  A(partial, 1024 * 8); A(scal, 8);
+  A(flag, 1); A(status, 2); A(maxneed, 1);
+  A(perm, N); A(tiles, 3 * (N / 32 + h.nelt + 1));
+#undef A
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&s->h_scal), 8 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&s->h_status), 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(s->v, 0, 3 * N * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(s->image, 0, 3 * N * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(s->status, 0, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(s->maxneed, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(s->flag, 0, sizeof(int));
+  if (e != cudaSuccess) {
+    tmd_system_free(s);
+    return fail(TMD_ERR_CUDA, std::string("system allocation: ") + cudaGetErrorString(e));
+  }
+  const_cast<tmd_model *>(m)->nsys++;
+  *out = s;
+  return TMD_OK;
+}
+
+void tmd_system_free(tmd_system *s) {
+  if (!s) return;
+  if (s->st) cudaStreamSynchronize(s->st);
+  dfree(s->x); dfree(s->v); dfree(s->f); dfree(s->xbuild); dfree(s->image); dfree(s->elem);
+  dfree(s->cell_of); dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_cursor);
+  dfree(s->cell_atoms); dfree(s->tmp); dfree(s->nbr); dfree(s->nraw); dfree(s->boff);
+  dfree(s->rev); dfree(s->P); dfree(s->G); dfree(s->dEdG); dfree(s->E); dfree(s->pdf);
+  dfree(s->wv); dfree(s->eatom); dfree(s->vatom); dfree(s->ke); dfree(s->partial);
+  dfree(s->scal); dfree(s->flag); dfree(s->status); dfree(s->maxneed); dfree(s->perm);
+  dfree(s->tiles); dfree(s->thermo_d);
+  if (s->h_scal) cudaFreeHost(s->h_scal);
+  if (s->h_status) cudaFreeHost(s->h_status);
+  for (auto &p : s->ev_pending) {
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+  if (s->st) cudaStreamDestroy(s->st);
+  if (s->m) const_cast<tmd_model *>(s->m)->nsys--;
+  delete s;
+}
+
+int tmd_system_set_box(tmd_system *s, const double bx[9], const int pbc[3]) {
+  if (!s || !bx || !pbc) return fail(TMD_ERR_ARG, "null argument");
+  if (!(bx[3] > 0 && bx[4] > 0 && bx[5] > 0)) return fail(TMD_ERR_ARG, "box lengths must be > 0");
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  box_setup(s->box, bx, pbc);
+  s->have_box = true;
+  int rc = bin_setup(s);
+  if (rc) return rc;
+  s->forces_valid = false;
+  if (s->have_atoms) {
+    int cap = initial_cap(s);
+    if (cap > s->cap) {
+      rc = alloc_neighbors(s, cap);
+      if (rc) return rc;
+    }
+    return rebuild_now(s);
+  }
+  return TMD_OK;
+}
+
+int tmd_system_set_atoms(tmd_system *s, int n, const double *x, const int *type,
+                         const double *v) {
+  if (!s || !x || !type || n < 0) return fail(TMD_ERR_ARG, "null argument");
+  if (n > s->natoms_cap) return fail(TMD_ERR_CAPACITY, "n exceeds the system capacity");
+  if (!s->have_box) return fail(TMD_ERR_STATE, "set the box before the atoms");
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  const HostModel &h = s->m->h;
+  s->n = n;
+  s->h_elem.resize(n);
+  int ntypes = (int)h.type_elements.size();
+  std::vector<std::vector<int>> by_elt(h.nelt);
+  for (int i = 0; i < n; i++) {
+    int t = type[i];
+    if (t < 1 || t > ntypes || h.typemap[t] < 0)
+      return fail(TMD_ERR_ARG, "atom " + std::to_string(i) + " has type " +
+                                   std::to_string(t) + " that pair_coeff did not map");
+    s->h_elem[i] = h.typemap[t];
+    by_elt[h.typemap[t]].push_back(i);
+  }
+  // atoms grouped by element (TensorMD::calc_tensor_density i2row order)
+  std::vector<int> perm;
+  std::vector<int> tiles;
+  perm.reserve(n);
+  for (int e = 0; e < h.nelt; e++) {
+    int start = (int)perm.size();
+    perm.insert(perm.end(), by_elt[e].begin(), by_elt[e].end());
+    int cnt = (int)by_elt[e].size();
+    for (int o = 0; o < cnt; o += s->m->mlp_tr) {
+      tiles.push_back(e);
+      tiles.push_back(start + o);
+      tiles.push_back(std::min(s->m->mlp_tr, cnt - o));
+    }
+  }
+  s->ntiles = (int)tiles.size() / 3;
+  if (n > 0) {
+    TMD_CUDA(cudaMemcpyAsync(s->x, x, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    TMD_CUDA(cudaMemcpyAsync(s->elem, s->h_elem.data(), n * sizeof(int), cudaMemcpyHostToDevice, s->st));
+    TMD_CUDA(cudaMemcpyAsync(s->perm, perm.data(), n * sizeof(int), cudaMemcpyHostToDevice, s->st));
+    TMD_CUDA(cudaMemcpyAsync(s->tiles, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice, s->st));
+    if (v) {
+      TMD_CUDA(cudaMemcpyAsync(s->v, v, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    } else {
+      TMD_CUDA(cudaMemsetAsync(s->v, 0, 3 * n * sizeof(double), s->st));
+    }
+    TMD_CUDA(cudaMemsetAsync(s->image, 0, 3 * n * sizeof(int), s->st));
+  }
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  s->have_atoms = true;
+  s->forces_valid = false;
+  if (n == 0) return TMD_OK;
+  int cap = initial_cap(s);
+  if (cap > s->cap) {
+    int rc = alloc_neighbors(s, cap);
+    if (rc) return rc;
+  }
+  return rebuild_now(s);
+}
+
+int tmd_system_set_positions(tmd_system *s, const double *x) {
+  if (!s || !x) return fail(TMD_ERR_ARG, "null argument");
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms first");
+  if (s->n == 0) return TMD_OK;
+  TMD_CUDA(cudaMemcpyAsync(s->x, x, 3 * s->n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  s->forces_valid = false;
+  double half = 0.5 * s->skin;
+  launch_neighbor_check(s->n, s->x, s->xbuild, half * half, s->flag, s->st, s->launches);
+  launch_neighbor_build(nb_args(s), s->st, s->launches);
+  return TMD_OK;
+}
+
+int tmd_system_get(tmd_system *s, double *x, double *v, double *f, int *image) {
+  if (!s) return fail(TMD_ERR_ARG, "null system");
+  int n = s->n;
+  if (n == 0) return TMD_OK;
+  if (x) TMD_CUDA(cudaMemcpyAsync(x, s->x, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  if (v) TMD_CUDA(cudaMemcpyAsync(v, s->v, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  if (f) TMD_CUDA(cudaMemcpyAsync(f, s->f, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  if (image) TMD_CUDA(cudaMemcpyAsync(image, s->image, 3 * n * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  return TMD_OK;
+}
+
+int tmd_compute(tmd_system *s, int eflag, int vflag, double scale, double *energy,
+                double *virial, double *f, double *eatom, double *vatom) {
+  if (!s) return fail(TMD_ERR_ARG, "null system");
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before compute");
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  int n = s->n;
+  if (n == 0) {
+    if (energy) *energy = 0;
+    if (virial) for (int c = 0; c < 6; c++) virial[c] = 0;
+    return TMD_OK;
+  }
+  int rc;
+  bool want_vatom = vatom != nullptr;
+  launch_force_eval(s, (float)scale, want_vatom);
+  if (eflag || energy)
+    launch_reduce_f32(s->E, n, s->partial, s->scal, scale, s->st, s->launches);
+  if (vflag || virial)
+    launch_reduce_f64(s->wv, n, 6, s->partial, s->scal + 1, s->st, s->launches);
+  launch_check_finite(n, s->f, (eflag || energy) ? s->scal : nullptr, s->status, s->st,
+                      s->launches);
+  TMD_CUDA(cudaGetLastError());
+  if (eatom) launch_scale_copy_f32(s->E, n, scale, s->eatom, s->st, s->launches);
+  TMD_CUDA(cudaMemcpyAsync(s->h_scal, s->scal, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  if (f) TMD_CUDA(cudaMemcpyAsync(f, s->f, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  if (eatom) TMD_CUDA(cudaMemcpyAsync(eatom, s->eatom, n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  if (vatom) TMD_CUDA(cudaMemcpyAsync(vatom, s->vatom, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  rc = read_status(s);
+  if (rc) return rc;
+  int st = s->h_status[0];
+  if (st & kStatusOverflow) {
+    // positions moved enough to overflow the list: rebuild larger and redo
+    rc = rebuild_now(s);
+    if (rc) return rc;
+    return tmd_compute(s, eflag, vflag, scale, energy, virial, f, eatom, vatom);
+  }
+  if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
+  if (st & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside a non-periodic boundary");
+  if (energy) *energy = s->h_scal[0];
+  if (virial) for (int c = 0; c < 6; c++) virial[c] = s->h_scal[1 + c];
+  s->forces_valid = true;
+  if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite energy or force");
+  return TMD_OK;
+}
+
+int tmd_nve_run(tmd_system *s, int nsteps, double dt, int thermo_every, double *thermo) {
+  if (!s || nsteps < 0 || !(dt > 0)) return fail(TMD_ERR_ARG, "bad nve arguments");
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before nve_run");
+  if (thermo && thermo_every < 1) return fail(TMD_ERR_ARG, "thermo_every must be >= 1");
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  const int n = s->n;
+  if (n == 0) return TMD_OK;
+  const double ftm2v = 1.0 / 1.0364269e-4;  // metal units, update.cpp:187-206
+  const double dtf = 0.5 * dt * ftm2v;
+  const double half = 0.5 * s->skin;
+  const double trigsq = half * half;
+  int rows = thermo ? 1 + nsteps / thermo_every + ((nsteps % thermo_every) ? 1 : 0) : 0;
+  if (rows > s->thermo_rows_alloc) {
+    dfree(s->thermo_d);
+    TMD_CUDA(dalloc(&s->thermo_d, 2 * (size_t)rows));
+    s->thermo_rows_alloc = rows;
+  }
+  int rc = clear_status(s);
+  if (rc) return rc;
+  auto thermo_row = [&](int r) {
+    launch_reduce_f32(s->E, n, s->partial, s->thermo_d + 2 * r, 1.0, s->st, s->launches);
+    launch_kinetic(n, s->v, s->elem, s->m->d_mass, s->ke, s->st, s->launches);
+    launch_reduce_f64(s->ke, n, 1, s->partial, s->thermo_d + 2 * r + 1, s->st, s->launches);
+  };
+  // Verlet::setup: forces of the starting positions
+  launch_force_eval(s, 1.0f, false);
+  int row = 0;
+  if (thermo) thermo_row(row++);
+  for (int step = 1; step <= nsteps; step++) {
+    prof_begin(s);
+    launch_nve_initial(n, s->x, s->v, s->f, s->elem, s->m->d_mass, dtf, dt, s->st, s->launches);
+    launch_neighbor_check(n, s->x, s->xbuild, trigsq, s->flag, s->st, s->launches);
+    prof_end(s, 5);
+    prof_begin(s);
+    launch_neighbor_build(nb_args(s), s->st, s->launches);
+    prof_end(s, 0);
+    launch_force_eval(s, 1.0f, false);
+    prof_begin(s);
+    launch_nve_final(n, s->v, s->f, s->elem, s->m->d_mass, dtf, s->st, s->launches);
+    prof_end(s, 5);
+    if (thermo && (step % thermo_every == 0 || step == nsteps)) {
+      prof_begin(s);
+      thermo_row(row++);
+      prof_end(s, 6);
+    }
+  }
+  launch_check_finite(n, s->f, nullptr, s->status, s->st, s->launches);
+  TMD_CUDA(cudaGetLastError());
+  if (thermo && rows > 0)
+    TMD_CUDA(cudaMemcpyAsync(thermo, s->thermo_d, 2 * rows * sizeof(double),
+                             cudaMemcpyDeviceToHost, s->st));
+  rc = read_status(s);
+  if (rc) return rc;
+  int st = s->h_status[0];
+  if (st & kStatusOverflow)
+    return fail(TMD_ERR_CAPACITY, "neighbor list overflow during the run (raise the "
+                                  "capacity by calling set_atoms again)");
+  if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
+  if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite force during the run");
+  s->forces_valid = true;
+  return TMD_OK;
+}
+
+int tmd_neighbor_list(tmd_system *s, double cut, int *counts, int *entries, long cap,
+                      long *total) {
+  if (!s || !counts || !total) return fail(TMD_ERR_ARG, "null argument");
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "no atoms");
+  if (cut > s->m->h.rmax + s->skin) return fail(TMD_ERR_ARG, "cut exceeds cutmax + skin");
+  int n = s->n;
+  int B = s->m->h.nelt;
+  std::vector<uint32_t> nb((size_t)n * s->cap);
+  std::vector<int> bo((size_t)n * (B + 1));
+  std::vector<double> x(3 * (size_t)n);
+  if (n > 0) {
+    TMD_CUDA(cudaMemcpyAsync(nb.data(), s->nbr, nb.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->st));
+    TMD_CUDA(cudaMemcpyAsync(bo.data(), s->boff, bo.size() * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    TMD_CUDA(cudaMemcpyAsync(x.data(), s->x, x.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    TMD_CUDA(cudaStreamSynchronize(s->st));
+  }
+  double cutsq = cut * cut;
+  long tot = 0;
+  for (int i = 0; i < n; i++) {
+    int cnt = 0;
+    int m = bo[(size_t)i * (B + 1) + B];
+    for (int t = 0; t < m; t++) {
+      uint32_t e = nb[(size_t)i * s->cap + t];
+      int j = e & kAtomMask, sx, sy, sz;
+      shift_decode(int(e >> kAtomBits), sx, sy, sz);
+      double gx, gy, gz;
+      image_of(s->box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sx, sy, sz, gx, gy, gz);
+      double dx = x[3 * i] - gx, dy = x[3 * i + 1] - gy, dz = x[3 * i + 2] - gz;
+      double rsq = dx * dx + dy * dy + dz * dz;
+      if (rsq <= cutsq) {
+        if (entries && tot < cap) {
+          entries[4 * tot] = j;
+          entries[4 * tot + 1] = sx;
+          entries[4 * tot + 2] = sy;
+          entries[4 * tot + 3] = sz;
+        }
+        tot++;
+        cnt++;
+      }
+    }
+    counts[i] = cnt;
+  }
+  *total = tot;
+  if (entries && tot > cap) return fail(TMD_ERR_CAPACITY, "entries buffer too small");
+  return TMD_OK;
+}
+
+int tmd_get_descriptors(tmd_system *s, double *G) {
+  if (!s || !G) return fail(TMD_ERR_ARG, "null argument");
+  size_t cnt = (size_t)s->n * s->m->h.nin;
+  std::vector<float> tmp(cnt);
+  if (cnt) {
+    TMD_CUDA(cudaMemcpyAsync(tmp.data(), s->G, cnt * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+    TMD_CUDA(cudaStreamSynchronize(s->st));
+  }
+  for (size_t i = 0; i < cnt; i++) G[i] = tmp[i];
+  return TMD_OK;
+}
+
+int tmd_system_stream(tmd_system *s, void **stream) {
+  if (!s || !stream) return fail(TMD_ERR_ARG, "null argument");
+  *stream = (void *)s->st;
+  return TMD_OK;
+}
+
+long tmd_system_launches(const tmd_system *s) { return s ? s->launches : 0; }
+
+int tmd_profile_enable(tmd_system *s, int enable) {
+  if (!s) return fail(TMD_ERR_ARG, "null system");
+  s->prof = enable != 0;
+  return TMD_OK;
+}
+
+int tmd_profile_read(tmd_system *s, long *launches, double *ms, int reset) {
+  if (!s) return fail(TMD_ERR_ARG, "null system");
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  for (auto &p : s->ev_pending) {
+    float t = 0.f;
+    TMD_CUDA(cudaEventElapsedTime(&t, p.second.first, p.second.second));
+    s->prof_n[p.first]++;
+    s->prof_ms[p.first] += t;
+    s->ev_pool.push_back(p.second.first);
+    s->ev_pool.push_back(p.second.second);
+  }
+  s->ev_pending.clear();
+  for (int k = 0; k < TMD_NPROF; k++) {
+    if (launches) launches[k] = s->prof_n[k];
+    if (ms) ms[k] = s->prof_ms[k];
+    if (reset) { s->prof_n[k] = 0; s->prof_ms[k] = 0; }
+  }
+  return TMD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+// integrate.cu -- velocity Verlet, deterministic FP64 reductions, checks.
+//
+// FixNVE (src/fix_nve.cpp:64-141): dtfm = dtf / mass[type]; v += dtfm * f;
+// x += dtv * v; then after the force v += dtfm * f.  Products and sums are
+// rounded separately (no FMA) as the host arithmetic of LAMMPS does.
+// Reductions use a fixed grid and a fixed tree, so sums are bitwise
+// reproducible run to run.
+#include "tmd_kernels.h"
+
+namespace tmd {
+
+namespace {
+constexpr int kRedBlocks = 1024;
+constexpr int kRedThreads = 256;
+
+__device__ inline double block_sum(double v, double *sh) {
+  const int tid = threadIdx.x;
+  sh[tid] = v;
+  __syncthreads();
+  for (int s = kRedThreads / 2; s > 0; s >>= 1) {
+    if (tid < s) sh[tid] += sh[tid + s];
+    __syncthreads();
+  }
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}
+}  // namespace
+
+template <typename Tin>
+__global__ void k_reduce_partial(const Tin *__restrict__ in, int n, int ncomp,
+                                 double scale, double *__restrict__ partial) {
+  __shared__ double sh[kRedThreads];
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
+  for (int c = 0; c < ncomp; c++) {
+    double s = 0.0;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+      s += (double)in[(size_t)i * ncomp + c];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) partial[(size_t)blockIdx.x * ncomp + c] = s * scale;
+  }
+}
+
+__global__ void k_reduce_final(const double *__restrict__ partial, int nb, int ncomp,
+                               double *__restrict__ out) {
+  __shared__ double sh[kRedThreads];
+  for (int c = 0; c < ncomp; c++) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(size_t)b * ncomp + c];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) out[c] = s;
+  }
+}
+
+static int red_blocks(int n) {
+  int b = (n + kRedThreads - 1) / kRedThreads;
+  if (b > kRedBlocks) b = kRedBlocks;
+  if (b < 1) b = 1;
+  return b;
+}
+
+void launch_reduce_f64(const double *in, int n, int ncomp, double *partial,
+                       double *out, cudaStream_t st, long &launches) {
+  int nb = red_blocks(n);
+  k_reduce_partial<double><<<nb, kRedThreads, 0, st>>>(in, n, ncomp, 1.0, partial);
+  k_reduce_final<<<1, kRedThreads, 0, st>>>(partial, nb, ncomp, out);
+  launches += 2;
+}
+
+void launch_reduce_f32(const float *in, int n, double *partial, double *out,
+                       double scale, cudaStream_t st, long &launches) {
+  int nb = red_blocks(n);
+  k_reduce_partial<float><<<nb, kRedThreads, 0, st>>>(in, n, 1, scale, partial);
+  k_reduce_final<<<1, kRedThreads, 0, st>>>(partial, nb, 1, out);
+  launches += 2;
+}
+
+__global__ void k_scale_copy(const float *__restrict__ in, int n, double scale,
+                             double *__restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (double)in[i] * scale;
+}
+
+void launch_scale_copy_f32(const float *in, int n, double scale, double *out,
+                           cudaStream_t st, long &launches) {
+  k_scale_copy<<<(n + 255) / 256, 256, 0, st>>>(in, n, scale, out);
+  launches += 1;
+}
+
+__global__ void k_nve_initial(int n, double *__restrict__ x, double *__restrict__ v,
+                              const double *__restrict__ f, const int *__restrict__ elem,
+                              const double *__restrict__ mass_e, double dtf,
+                              double dtv) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double dtfm = dtf / mass_e[elem[i]];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    double vv = __dadd_rn(v[3 * i + c], __dmul_rn(dtfm, f[3 * i + c]));
+    v[3 * i + c] = vv;
+    x[3 * i + c] = __dadd_rn(x[3 * i + c], __dmul_rn(dtv, vv));
+  }
+}
+
+__global__ void k_nve_final(int n, double *__restrict__ v, const double *__restrict__ f,
+                            const int *__restrict__ elem,
+                            const double *__restrict__ mass_e, double dtf) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double dtfm = dtf / mass_e[elem[i]];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    v[3 * i + c] = __dadd_rn(v[3 * i + c], __dmul_rn(dtfm, f[3 * i + c]));
+}
+
+void launch_nve_initial(int n, double *x, double *v, const double *f,
+                        const int *elem, const double *mass_e, double dtf,
+                        double dtv, cudaStream_t st, long &launches) {
+  k_nve_initial<<<(n + 255) / 256, 256, 0, st>>>(n, x, v, f, elem, mass_e, dtf, dtv);
+  launches += 1;
+}
+
+void launch_nve_final(int n, double *v, const double *f, const int *elem,
+                      const double *mass_e, double dtf, cudaStream_t st,
+                      long &launches) {
+  k_nve_final<<<(n + 255) / 256, 256, 0, st>>>(n, v, f, elem, mass_e, dtf);
+  launches += 1;
+}
+
+// 0.5 * mvv2e * m * v^2 per atom (compute ke, metal mvv2e = 1.0364269e-4)
+__global__ void k_kinetic(int n, const double *__restrict__ v, const int *__restrict__ elem,
+                          const double *__restrict__ mass_e, double *__restrict__ ke) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double m = mass_e[elem[i]];
+  double s = v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2];
+  ke[i] = 0.5 * 1.0364269e-4 * m * s;
+}
+
+void launch_kinetic(int n, const double *v, const int *elem, const double *mass_e,
+                    double *ke_atom, cudaStream_t st, long &launches) {
+  k_kinetic<<<(n + 255) / 256, 256, 0, st>>>(n, v, elem, mass_e, ke_atom);
+  launches += 1;
+}
+
+__global__ void k_check_finite(int n, const double *__restrict__ f,
+                               const double *__restrict__ etot, int *status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool bad = false;
+  if (i == 0 && etot && !isfinite(*etot)) bad = true;
+  if (i < n)
+    bad |= !isfinite(f[3 * i]) || !isfinite(f[3 * i + 1]) || !isfinite(f[3 * i + 2]);
+  if (bad) atomicOr(status, kStatusNonfinite);
+}
+
+void launch_check_finite(int n, const double *f, const double *etot, int *status,
+                         cudaStream_t st, long &launches) {
+  int grid = (n + 255) / 256;
+  if (grid < 1) grid = 1;
+  k_check_finite<<<grid, 256, 0, st>>>(n, f, etot, status);
+  launches += 1;
+}
+
+}  // namespace tmd

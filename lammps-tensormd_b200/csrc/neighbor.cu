@@ -1,0 +1,414 @@
+// neighbor.cu -- on-device cell binning and full neighbor list.
+//
+// Semantics follow LAMMPS NBinStandard::bin_atoms + NPairFullBinAtomonly::build
+// (src/nbin_standard.cpp:221-261, src/npair_full_bin_atomonly.cpp:32-92): a
+// full list of every image (j, shift) with rsq <= (rc + skin)^2 except the atom
+// itself, rsq computed in FP64 without fused multiply-add from the image
+// coordinate x_j + shift built hop by hop as AtomVec::pack_border does.  The
+// ghost atoms of LAMMPS are represented as (j, shift) entries, so small and
+// triclinic periodic cells need no ghost arrays.
+//
+// Layout (n atoms, cap entries per atom):
+//   nbr[i*cap + t]  packed (shift_code << 23 | j), sorted by (element block,
+//                   packed key): block 0 = same element as i, then the others
+//                   in the order of tensormd.cpp:165-176
+//   boff[i*(B+1)+b] start of block b in the row, boff[i*(B+1)+B] = count
+//   rev[i*cap + t]  flat slot of the partner entry (j -> i, -shift), -1 if the
+//                   partner fell outside the list cutoff by rounding
+//
+// Every kernel takes `flag` and returns at once when no rebuild is pending, so
+// the sequence can sit inside a captured CUDA graph of the MD step.
+#include "tmd_kernels.h"
+
+namespace tmd {
+
+__global__ void k_nb_check(int n, const double *__restrict__ x,
+                           const double *__restrict__ xbuild, double trigsq,
+                           int *flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (*flag) return;
+  double dx = x[3 * i] - xbuild[3 * i];
+  double dy = x[3 * i + 1] - xbuild[3 * i + 1];
+  double dz = x[3 * i + 2] - xbuild[3 * i + 2];
+  double rsq = dx * dx + dy * dy + dz * dz;
+  if (rsq > trigsq) atomicOr(flag, 1);
+}
+
+__device__ inline void frac_of(const BoxP &b, double px, double py, double pz,
+                               double &fx, double &fy, double &fz) {
+  double dx = px - b.lo[0], dy = py - b.lo[1], dz = pz - b.lo[2];
+  fz = dz / b.zprd;
+  fy = (dy - fz * b.yz) / b.yprd;
+  fx = (dx - fy * b.xy - fz * b.xz) / b.xprd;
+}
+
+__global__ void k_nb_zero(int ncell, int *cell_count, const int *flag) {
+  if (!*flag) return;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+       c += gridDim.x * blockDim.x)
+    cell_count[c] = 0;
+}
+
+// Wrap atoms into the cell (Domain::pbc()), then bin them.
+__global__ void k_nb_bin(int n, double *__restrict__ x, int *__restrict__ image,
+                         BoxP box, BinP bin, int *__restrict__ cell_of,
+                         int *__restrict__ cell_count, int *status,
+                         const int *flag) {
+  if (!*flag) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
+  if (!box.triclinic) {
+    double lo[3] = {box.lo[0], box.lo[1], box.lo[2]};
+    double prd[3] = {box.xprd, box.yprd, box.zprd};
+    double p[3] = {px, py, pz};
+    for (int a = 0; a < 3; a++) {
+      if (!box.pbc[a]) continue;
+      if (p[a] < lo[a]) {
+        p[a] += prd[a];
+        image[3 * i + a] -= 1;
+      }
+      if (p[a] >= lo[a] + prd[a]) {
+        p[a] -= prd[a];
+        p[a] = p[a] < lo[a] ? lo[a] : p[a];
+        image[3 * i + a] += 1;
+      }
+    }
+    px = p[0]; py = p[1]; pz = p[2];
+  } else {
+    double f[3];
+    frac_of(box, px, py, pz, f[0], f[1], f[2]);
+    int s[3] = {0, 0, 0};
+    for (int a = 0; a < 3; a++)
+      if (box.pbc[a]) s[a] = (int)floor(f[a]);
+    if (s[0] || s[1] || s[2]) {
+      image_of(box, px, py, pz, -s[0], -s[1], -s[2], px, py, pz);
+      image[3 * i] += s[0];
+      image[3 * i + 1] += s[1];
+      image[3 * i + 2] += s[2];
+    }
+  }
+  x[3 * i] = px; x[3 * i + 1] = py; x[3 * i + 2] = pz;
+  double f[3];
+  frac_of(box, px, py, pz, f[0], f[1], f[2]);
+  int c3[3];
+  for (int a = 0; a < 3; a++) {
+    if (!box.pbc[a] && (f[a] < 0.0 || f[a] > 1.0)) atomicOr(status, kStatusOutside);
+    int q = (int)floor(f[a] * bin.nb[a]);
+    q = q < 0 ? 0 : (q >= bin.nb[a] ? bin.nb[a] - 1 : q);
+    c3[a] = q;
+  }
+  int c = (c3[2] * bin.nb[1] + c3[1]) * bin.nb[0] + c3[0];
+  cell_of[i] = c;
+  atomicAdd(&cell_count[c], 1);
+}
+
+// Exclusive scan of the cell counts with one block of 1024 threads.
+__global__ void k_nb_scan(int ncell, const int *__restrict__ cell_count,
+                          int *__restrict__ cell_start,
+                          int *__restrict__ cell_cursor, const int *flag) {
+  if (!*flag) return;
+  __shared__ int warp_sums[32];
+  int tid = threadIdx.x;
+  int per = (ncell + blockDim.x - 1) / blockDim.x;
+  int c0 = tid * per, c1 = min(c0 + per, ncell);
+  int local = 0;
+  for (int c = c0; c < c1; c++) local += cell_count[c];
+  int lane = tid & 31, w = tid >> 5;
+  int incl = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_sums[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int v = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
+    }
+    warp_sums[lane] = v;
+  }
+  __syncthreads();
+  int base = (w > 0 ? warp_sums[w - 1] : 0) + incl - local;
+  for (int c = c0; c < c1; c++) {
+    cell_start[c] = base;
+    cell_cursor[c] = base;
+    base += cell_count[c];
+  }
+  if (tid == blockDim.x - 1) cell_start[ncell] = base;
+}
+
+__global__ void k_nb_fill(int n, const int *__restrict__ cell_of,
+                          int *__restrict__ cell_cursor,
+                          int *__restrict__ cell_atoms, const int *flag) {
+  if (!*flag) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int pos = atomicAdd(&cell_cursor[cell_of[i]], 1);
+  cell_atoms[pos] = i;
+}
+
+// Order each cell's atoms by index so the build is deterministic.
+__global__ void k_nb_cellsort(int ncell, const int *__restrict__ cell_start,
+                              int *__restrict__ cell_atoms, const int *flag) {
+  if (!*flag) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int s0 = cell_start[c], s1 = cell_start[c + 1];
+  for (int a = s0 + 1; a < s1; a++) {
+    int v = cell_atoms[a];
+    int b = a - 1;
+    while (b >= s0 && cell_atoms[b] > v) {
+      cell_atoms[b + 1] = cell_atoms[b];
+      b--;
+    }
+    cell_atoms[b + 1] = v;
+  }
+}
+
+// FP64 squared distance, products and sums rounded separately (no FMA).
+__device__ inline double rsq_nofma(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                   __dmul_rn(dz, dz));
+}
+
+// One warp per atom; lanes walk stencil cells, two passes (count, write)
+// give a deterministic order.
+__global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
+                           BinP bin, const int *__restrict__ cell_of,
+                           const int *__restrict__ cell_start,
+                           const int *__restrict__ cell_atoms, double cutsq,
+                           int cap, uint32_t *__restrict__ tmp,
+                           int *__restrict__ nraw, int *status, int *maxneed,
+                           const int *flag) {
+  if (!*flag) return;
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
+  const int ci = cell_of[i];
+  const int cx = ci % bin.nb[0], cy = (ci / bin.nb[0]) % bin.nb[1],
+            cz = ci / (bin.nb[0] * bin.nb[1]);
+  const int wx = 2 * bin.ns[0] + 1, wy = 2 * bin.ns[1] + 1, wz = 2 * bin.ns[2] + 1;
+  const int S = wx * wy * wz;
+  int out = 0;
+  uint32_t *row = tmp + (size_t)i * cap;
+  for (int base = 0; base < S; base += 32) {
+    int s = base + lane;
+    int c = -1, sh[3] = {0, 0, 0};
+    if (s < S) {
+      int o[3] = {s % wx - bin.ns[0], (s / wx) % wy - bin.ns[1],
+                  s / (wx * wy) - bin.ns[2]};
+      int cc[3] = {cx + o[0], cy + o[1], cz + o[2]};
+      int w3[3];
+      bool ok = true;
+      for (int a = 0; a < 3; a++) {
+        int q = cc[a];
+        int sa = (q >= 0) ? q / bin.nb[a] : -((-q + bin.nb[a] - 1) / bin.nb[a]);
+        w3[a] = q - sa * bin.nb[a];
+        sh[a] = sa;
+        if (!box.pbc[a] && sa != 0) ok = false;
+        if (sa > kShiftR || sa < -kShiftR) {
+          ok = false;
+          atomicOr(status, kStatusShift);
+        }
+      }
+      if (ok) c = (w3[2] * bin.nb[1] + w3[1]) * bin.nb[0] + w3[0];
+    }
+    int cnt = 0;
+    int a0 = 0, a1 = 0;
+    if (c >= 0) {
+      a0 = cell_start[c];
+      a1 = cell_start[c + 1];
+    }
+    const bool self_cell = (sh[0] == 0 && sh[1] == 0 && sh[2] == 0);
+    for (int p = a0; p < a1; p++) {
+      int j = cell_atoms[p];
+      if (j == i && self_cell) continue;
+      double gx, gy, gz;
+      image_of(box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sh[0], sh[1], sh[2],
+               gx, gy, gz);
+      double r2 = rsq_nofma(xi - gx, yi - gy, zi - gz);
+      if (r2 <= cutsq) cnt++;
+    }
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    int total = __shfl_sync(0xffffffffu, incl, 31);
+    int pos = out + incl - cnt;
+    if (cnt > 0) {
+      int code = shift_code(sh[0], sh[1], sh[2]);
+      for (int p = a0; p < a1; p++) {
+        int j = cell_atoms[p];
+        if (j == i && self_cell) continue;
+        double gx, gy, gz;
+        image_of(box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sh[0], sh[1], sh[2],
+                 gx, gy, gz);
+        double r2 = rsq_nofma(xi - gx, yi - gy, zi - gz);
+        if (r2 <= cutsq) {
+          if (pos < cap) row[pos] = nb_pack(j, code);
+          pos++;
+        }
+      }
+    }
+    out += total;
+  }
+  if (lane == 0) {
+    nraw[i] = out;
+    if (out > cap) {
+      atomicOr(status, kStatusOverflow);
+      atomicMax(maxneed, out);
+    }
+  }
+}
+
+// One warp per atom: bitonic sort of the row by (block, packed key) in
+// shared memory, then block offsets.
+__global__ void k_nb_sort(int n, int B, KParams kp, const int *__restrict__ elem,
+                          int cap, int capp, const uint32_t *__restrict__ tmp,
+                          const int *__restrict__ nraw,
+                          uint32_t *__restrict__ nbr, int *__restrict__ boff,
+                          const int *flag) {
+  if (!*flag) return;
+  extern __shared__ unsigned long long sbuf[];
+  int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int i = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (i >= n) return;
+  unsigned long long *s = sbuf + (size_t)wib * capp;
+  int cnt = min(nraw[i], cap);
+  int ei = elem[i];
+  const uint32_t *row = tmp + (size_t)i * cap;
+  for (int t = lane; t < capp; t += 32) {
+    unsigned long long v = ~0ull;
+    if (t < cnt) {
+      uint32_t e = row[t];
+      int j = e & kAtomMask;
+      int b = kp.eltij[ei * kMaxElt + elem[j]];
+      v = ((unsigned long long)b << 32) | e;
+    }
+    s[t] = v;
+  }
+  __syncwarp();
+  for (int k = 2; k <= capp; k <<= 1) {
+    for (int jj = k >> 1; jj > 0; jj >>= 1) {
+      for (int t = lane; t < capp; t += 32) {
+        int p = t ^ jj;
+        if (p > t) {
+          unsigned long long a = s[t], c = s[p];
+          bool up = ((t & k) == 0);
+          if ((a > c) == up) {
+            s[t] = c;
+            s[p] = a;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  uint32_t *orow = nbr + (size_t)i * cap;
+  for (int t = lane; t < cnt; t += 32) orow[t] = (uint32_t)(s[t] & 0xffffffffu);
+  for (int b = 0; b <= B; b++) {
+    int c = 0;
+    for (int t = lane; t < cnt; t += 32) c += ((int)(s[t] >> 32) < b) ? 1 : 0;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) boff[(size_t)i * (B + 1) + b] = c;
+  }
+}
+
+// Partner slot of every entry: (j -> i, -shift) found by binary search in the
+// sorted block of atom j.
+__global__ void k_nb_rev(int n, int B, KParams kp, const int *__restrict__ elem,
+                         int cap, const uint32_t *__restrict__ nbr,
+                         const int *__restrict__ boff, int *__restrict__ rev,
+                         const int *flag) {
+  if (!*flag) return;
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  int i = warp;
+  int cnt = boff[(size_t)i * (B + 1) + B];
+  int ei = elem[i];
+  for (int t = lane; t < cnt; t += 32) {
+    uint32_t e = nbr[(size_t)i * cap + t];
+    int j = e & kAtomMask;
+    int code = e >> kAtomBits;
+    uint32_t key = nb_pack(i, neg_code(code));
+    int bj = kp.eltij[elem[j] * kMaxElt + ei];
+    int lo = boff[(size_t)j * (B + 1) + bj], hi = boff[(size_t)j * (B + 1) + bj + 1];
+    const uint32_t *rj = nbr + (size_t)j * cap;
+    int found = -1;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      uint32_t v = rj[mid];
+      if (v == key) { found = mid; break; }
+      if (v < key) lo = mid + 1; else hi = mid;
+    }
+    rev[(size_t)i * cap + t] = found >= 0 ? (int)((size_t)j * cap + found) : -1;
+  }
+}
+
+__global__ void k_nb_finish(int n, const double *__restrict__ x,
+                            double *__restrict__ xbuild, int *flag) {
+  if (!*flag) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    xbuild[3 * i] = x[3 * i];
+    xbuild[3 * i + 1] = x[3 * i + 1];
+    xbuild[3 * i + 2] = x[3 * i + 2];
+  }
+}
+
+__global__ void k_nb_clear(int *flag) { *flag = 0; }
+
+__global__ void k_set_flag(int *flag) { *flag = 1; }
+
+// Host driver: the whole rebuild sequence on `st`.  All launches are
+// conditional on *flag; `launches` counts them.
+void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
+  const int T = 256;
+  int gn = (a.n + T - 1) / T;
+  if (gn < 1) gn = 1;
+  k_nb_zero<<<(a.bin.ncell + T - 1) / T, T, 0, st>>>(a.bin.ncell, a.cell_count, a.flag);
+  k_nb_bin<<<gn, T, 0, st>>>(a.n, a.x, a.image, a.box, a.bin, a.cell_of,
+                             a.cell_count, a.status, a.flag);
+  k_nb_scan<<<1, 1024, 0, st>>>(a.bin.ncell, a.cell_count, a.cell_start,
+                                a.cell_cursor, a.flag);
+  k_nb_fill<<<gn, T, 0, st>>>(a.n, a.cell_of, a.cell_cursor, a.cell_atoms, a.flag);
+  k_nb_cellsort<<<(a.bin.ncell + T - 1) / T, T, 0, st>>>(a.bin.ncell, a.cell_start,
+                                                         a.cell_atoms, a.flag);
+  int gw = (a.n * 32 + T - 1) / T;
+  if (gw < 1) gw = 1;
+  k_nb_build<<<gw, T, 0, st>>>(a.n, a.x, a.box, a.bin, a.cell_of, a.cell_start,
+                               a.cell_atoms, a.cutsq, a.cap, a.tmp, a.nraw,
+                               a.status, a.maxneed, a.flag);
+  int wpb = a.capp >= 1024 ? 1 : (a.capp >= 512 ? 2 : 4);
+  size_t smem = (size_t)wpb * a.capp * sizeof(unsigned long long);
+  k_nb_sort<<<(a.n + wpb - 1) / wpb, 32 * wpb, smem, st>>>(
+      a.n, a.B, a.kp, a.elem, a.cap, a.capp, a.tmp, a.nraw, a.nbr, a.boff, a.flag);
+  k_nb_rev<<<gw, T, 0, st>>>(a.n, a.B, a.kp, a.elem, a.cap, a.nbr, a.boff, a.rev,
+                             a.flag);
+  k_nb_finish<<<gn, T, 0, st>>>(a.n, a.x, a.xbuild, a.flag);
+  k_nb_clear<<<1, 1, 0, st>>>(a.flag);
+  launches += 10;
+}
+
+void launch_neighbor_check(int n, const double *x, const double *xbuild,
+                           double trigsq, int *flag, cudaStream_t st,
+                           long &launches) {
+  const int T = 256;
+  k_nb_check<<<(n + T - 1) / T, T, 0, st>>>(n, x, xbuild, trigsq, flag);
+  launches += 1;
+}
+
+void launch_set_flag(int *flag, cudaStream_t st, long &launches) {
+  k_set_flag<<<1, 1, 0, st>>>(flag);
+  launches += 1;
+}
+
+}  // namespace tmd

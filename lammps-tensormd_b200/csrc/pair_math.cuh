@@ -1,0 +1,203 @@
+// pair_math.cuh -- per-pair geometry, radial basis and angular moments.
+//
+// Radial functions H_k(r) = f_c(r) g_k(r) follow descriptor.cpp:51-138 and
+// cutoff.cpp:20-37; the rational table follows ration.cu:27-69 (endpoint
+// intervals forced to zero, ration.hpp:29).  Monomials are ordered as
+// kernel.cu:1197-1232: 1, x, y, z, xx, xy, xz, yy, yz, zz, xxx, xxy, xxz,
+// xyy, xyz, xzz, yyy, yyz, yzz, zzz.
+#pragma once
+
+#include "tmd_internal.h"
+
+namespace tmd {
+
+// Pair geometry computed by one lane and broadcast to the atom's group.
+struct PairGeo {
+  float r, ux, uy, uz;  // distance and unit vector (x_j - x_i) / r
+  float fc, dfc;        // analytic cutoff and derivative
+  float tq;             // table: offset inside the interval
+  int ti;               // table interval, or -1 when the pair is inactive
+};
+
+__device__ inline double rsq_plain(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                   __dmul_rn(dz, dz));
+}
+
+// Geometry of neighbor entry e of atom i (FP64 difference and cutoff test
+// rij2 < rc^2 && rij2 > 1e-10 as kernel.cu:1163).  g.ti = -1 if inactive.
+__device__ inline void pair_geometry(const KParams &kp, const BoxP &box,
+                                     const double *__restrict__ x, double xi,
+                                     double yi, double zi, uint32_t e,
+                                     PairGeo &g) {
+  int j = e & kAtomMask;
+  int sx, sy, sz;
+  shift_decode(int(e >> kAtomBits), sx, sy, sz);
+  double gx, gy, gz;
+  image_of(box, __ldg(x + 3 * j), __ldg(x + 3 * j + 1), __ldg(x + 3 * j + 2), sx,
+           sy, sz, gx, gy, gz);
+  double dx = gx - xi, dy = gy - yi, dz = gz - zi;
+  double r2 = rsq_plain(dx, dy, dz);
+  g.ti = -1;
+  g.r = g.ux = g.uy = g.uz = g.fc = g.dfc = g.tq = 0.f;
+  if (!(r2 < kp.rcsq && r2 > 1e-10)) return;
+  double r = sqrt(r2);
+  float rf = float(r);
+  float rinv = 1.0f / rf;
+  g.r = rf;
+  g.ux = float(dx) * rinv;
+  g.uy = float(dy) * rinv;
+  g.uz = float(dz) * rinv;
+  if (kp.radial == 1) {
+    int ti = int(r * kp.tab_xdxd);
+    if (ti > kp.tab_n - 2) ti = kp.tab_n - 2;
+    g.ti = ti;
+    g.tq = float(r - ti * kp.tab_dxd);
+  } else {
+    g.ti = 0;
+    float z = rf * kp.inv_rc;
+    if (kp.fctype == 0) {
+      z = z > 1.f ? 1.f : z;
+      float s, c;
+      sincospif(z, &s, &c);
+      g.fc = 0.5f + 0.5f * c;
+      g.dfc = -0.5f * 3.14159265358979f * s * kp.inv_rc;
+    } else {
+      const float gm = 5.f;
+      z = z > 3.14159265358979f ? 3.14159265358979f : z;
+      float z4 = z * z * z * z, z5 = z4 * z;
+      g.fc = 1.f + gm * z5 * z - (gm + 1.f) * z5;
+      g.dfc = (gm + 1.f) * gm * kp.inv_rc * (z5 - z4);
+    }
+  }
+}
+
+__device__ inline PairGeo shfl_geo(unsigned mask, const PairGeo &g, int src,
+                                   int width) {
+  PairGeo o;
+  o.r = __shfl_sync(mask, g.r, src, width);
+  o.ux = __shfl_sync(mask, g.ux, src, width);
+  o.uy = __shfl_sync(mask, g.uy, src, width);
+  o.uz = __shfl_sync(mask, g.uz, src, width);
+  o.fc = __shfl_sync(mask, g.fc, src, width);
+  o.dfc = __shfl_sync(mask, g.dfc, src, width);
+  o.tq = __shfl_sync(mask, g.tq, src, width);
+  o.ti = __shfl_sync(mask, g.ti, src, width);
+  return o;
+}
+
+// H_k and (optionally) dH_k/dr for filters k0..k0+3.
+template <bool DERIV>
+__device__ inline void radial4(const KParams &kp, int k0, const PairGeo &g,
+                               float H[4], float dH[4]) {
+  if (kp.radial == 1) {
+    if (g.ti <= 0 || g.ti >= kp.tab_n - 2) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) { H[q] = 0.f; if (DERIV) dH[q] = 0.f; }
+      return;
+    }
+    const int K = kp.K;
+    const float4 *row = reinterpret_cast<const float4 *>(kp.table + (size_t)g.ti * 4 * K);
+    float4 y4 = __ldg(row + (k0 >> 2));
+    float4 s4 = __ldg(row + ((K + k0) >> 2));
+    float4 a4 = __ldg(row + ((2 * K + k0) >> 2));
+    float4 b4 = __ldg(row + ((3 * K + k0) >> 2));
+    const float ys[4] = {y4.x, y4.y, y4.z, y4.w};
+    const float ss[4] = {s4.x, s4.y, s4.z, s4.w};
+    const float c1s[4] = {a4.x, a4.y, a4.z, a4.w};
+    const float c2s[4] = {b4.x, b4.y, b4.z, b4.w};
+    const float q = g.tq, dx = kp.tab_dx, rr = dx - q;
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      float c1 = c1s[t], c2 = c2s[t], s = ss[t];
+      float c3 = fabsf(c2 * rr);
+      float c4 = c3 + fabsf(c1 * q);
+      if (c4 > 0.f) c3 /= c4;
+      c4 = c2 + c3 * (c1 - c2);
+      H[t] = ys[t] + q * (s - rr * c4);
+      if (DERIV) dH[t] = s + (q - rr) * c4 + dx * (c4 - c2) * (1.f - c3);
+    }
+    return;
+  }
+  const float r = g.r;
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    const int k = k0 + t;
+    const float a = kp.p0[k], b = kp.p1[k], c = kp.p2[k];
+    float f, df;
+    if (kp.method == 3) {
+      float d = r - b;
+      f = expf(-a * d * d * kp.inv_rc2);
+      df = -2.f * a * kp.inv_rc2 * d * f;
+    } else if (kp.method == 0) {
+      float xr = r / a;
+      float pw = powf(xr, b);
+      f = expf(-pw);
+      df = -f * b * powf(xr, b - 1.f) / a;
+    } else if (kp.method == 1) {
+      float gdr = b * (r - c);
+      float e1 = expf(-gdr), e2 = expf(-2.f * gdr);
+      f = a * (e2 - 2.f * e1);
+      df = -a * b * 2.f * (e2 - e1);
+    } else {
+      float z = -b * ((r - c) / c);
+      f = a * expf(z);
+      df = -f * b / c;
+    }
+    H[t] = g.fc * f;
+    if (DERIV) dH[t] = g.dfc * f + g.fc * df;
+  }
+}
+
+template <int D>
+__device__ inline void moments(float x, float y, float z, float M[D]) {
+  M[0] = 1.f;
+  if (D > 1) { M[1] = x; M[2] = y; M[3] = z; }
+  if (D > 4) {
+    float xx = x * x, xy = x * y, xz = x * z, yy = y * y, yz = z * y, zz = z * z;
+    M[4] = xx; M[5] = xy; M[6] = xz; M[7] = yy; M[8] = yz; M[9] = zz;
+    if (D > 10) {
+      M[10] = xx * x; M[11] = xx * y; M[12] = xx * z; M[13] = xy * y;
+      M[14] = xy * z; M[15] = xz * z; M[16] = yy * y; M[17] = yy * z;
+      M[18] = yz * z; M[19] = zz * z;
+    }
+  }
+}
+
+// Gradient of Q(u) = sum_d V_d M_d(u) with respect to u, and sum_d n_d V_d M_d
+// (n_d = rank of monomial d).  Then dQ/dx_j = (gradQ - u * nVM) / r, which
+// is sum_d V_d dM_d/dx_j (tensor_ops.cpp calculate_dM_{p,d,f}).
+template <int D>
+__device__ inline void poly_grad(const float V[D], float x, float y, float z,
+                                 float gq[3], float &nvm) {
+  float gx = 0.f, gy = 0.f, gz = 0.f, s = 0.f;
+  if (D > 1) {
+    gx += V[1]; gy += V[2]; gz += V[3];
+    s += V[1] * x + V[2] * y + V[3] * z;
+  }
+  if (D > 4) {
+    // xx, xy, xz, yy, yz, zz
+    gx += 2.f * V[4] * x + V[5] * y + V[6] * z;
+    gy += V[5] * x + 2.f * V[7] * y + V[8] * z;
+    gz += V[6] * x + V[8] * y + 2.f * V[9] * z;
+    s += 2.f * (V[4] * x * x + V[5] * x * y + V[6] * x * z + V[7] * y * y +
+                V[8] * y * z + V[9] * z * z);
+    if (D > 10) {
+      float xx = x * x, xy = x * y, xz = x * z, yy = y * y, yz = y * z, zz = z * z;
+      // xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
+      gx += 3.f * V[10] * xx + 2.f * V[11] * xy + 2.f * V[12] * xz + V[13] * yy +
+            V[14] * yz + V[15] * zz;
+      gy += V[11] * xx + 2.f * V[13] * xy + V[14] * xz + 3.f * V[16] * yy +
+            2.f * V[17] * yz + V[18] * zz;
+      gz += V[12] * xx + V[14] * xy + 2.f * V[15] * xz + V[17] * yy +
+            2.f * V[18] * yz + 3.f * V[19] * zz;
+      s += 3.f * (V[10] * xx * x + V[11] * xx * y + V[12] * xx * z + V[13] * xy * y +
+                  V[14] * xy * z + V[15] * xz * z + V[16] * yy * y + V[17] * yy * z +
+                  V[18] * yz * z + V[19] * zz * z);
+    }
+  }
+  gq[0] = gx; gq[1] = gy; gq[2] = gz;
+  nvm = s;
+}
+
+}  // namespace tmd

@@ -1,0 +1,128 @@
+// tmd_kernels.h -- launch interfaces of the device kernels.
+#pragma once
+
+#include "tmd_internal.h"
+
+namespace tmd {
+
+// status word bits set by kernels (read by the host after a step)
+constexpr int kStatusOverflow = 1;   // neighbor row longer than cap
+constexpr int kStatusShift = 2;      // image shift beyond +-3 cells
+constexpr int kStatusOutside = 4;    // atom outside a non-periodic boundary
+constexpr int kStatusNonfinite = 8;  // NaN/Inf energy or force
+
+struct NbArgs {
+  int n, B, cap, capp;
+  KParams kp;
+  BoxP box;
+  BinP bin;
+  double cutsq;
+  double *x;
+  int *image;
+  const int *elem;
+  int *cell_of, *cell_count, *cell_start, *cell_cursor, *cell_atoms;
+  uint32_t *tmp;
+  int *nraw;
+  uint32_t *nbr;
+  int *boff;
+  int *rev;
+  double *xbuild;
+  int *flag, *status, *maxneed;
+};
+
+void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches);
+void launch_neighbor_check(int n, const double *x, const double *xbuild,
+                           double trigsq, int *flag, cudaStream_t st,
+                           long &launches);
+void launch_set_flag(int *flag, cudaStream_t st, long &launches);
+
+// Descriptor: P[n][B][K][D], G[n][B*K*M].
+struct DescArgs {
+  int n, cap;
+  KParams kp;
+  BoxP box;
+  const double *x;
+  const int *elem;
+  const uint32_t *nbr;
+  const int *boff;
+  float *P, *G;
+};
+void launch_descriptor(const DescArgs &a, cudaStream_t st, long &launches);
+
+// MLP forward + backward over element-grouped tiles.
+struct MlpLayer {
+  int K, N;
+  const float *W;  // [K][N] row-major (npz weights_e_l)
+  const float *b;  // [N] or nullptr
+};
+struct MlpArgs {
+  int nl, actfn, resnet, nin, maxh;
+  int tr;             // atoms per CTA (32 or 64)
+  size_t smem;        // dynamic shared memory bytes
+  int ntiles;
+  const int *tiles;   // [ntiles][3] = (element, start, count) into perm
+  const int *perm;    // atom indices grouped by element
+  const float *G;     // [n][nin]
+  float *dEdG;        // [n][nin]
+  float *E;           // [n]
+  // per element, per layer (host table copied into a device param block)
+  const MlpLayer *layers;  // [nelt][nl] device array
+};
+void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches);
+size_t mlp_fp32_smem(int nl, const int *sizes, int tr);
+void mlp_fp32_prepare(int tr, size_t smem);
+
+// Force: per-pair dE_i/dx_j into pdf, per-atom virial partials.
+struct ForceArgs {
+  int n, cap;
+  KParams kp;
+  BoxP box;
+  float scale;
+  const double *x;
+  const int *elem;
+  const uint32_t *nbr;
+  const int *boff;
+  const float *P, *G, *dEdG;
+  float4 *pdf;
+  double *wv;  // [n][6] per-atom sum of -r_ij (x) df over own pairs
+};
+void launch_force(const ForceArgs &a, cudaStream_t st, long &launches);
+
+// Gather: f_i = sum_t pdf[t] - pdf[rev[t]] (FP64), optional per-atom virial.
+struct GatherArgs {
+  int n, cap, B;
+  const int *boff;
+  const float4 *pdf;
+  const int *rev;
+  const uint32_t *nbr;
+  const double *x;
+  BoxP box;
+  const double *wv;
+  double *f;
+  double *vatom;   // nullable
+};
+void launch_gather(const GatherArgs &a, cudaStream_t st, long &launches);
+
+// Deterministic FP64 reductions: out[c] = sum_i in[i*ncomp + c] (in FP64 or
+// FP32 input).  partial has >= 1024*ncomp doubles.
+void launch_reduce_f64(const double *in, int n, int ncomp, double *partial,
+                       double *out, cudaStream_t st, long &launches);
+void launch_reduce_f32(const float *in, int n, double *partial, double *out,
+                       double scale, cudaStream_t st, long &launches);
+void launch_scale_copy_f32(const float *in, int n, double scale, double *out,
+                           cudaStream_t st, long &launches);
+
+// Velocity Verlet halves (fix_nve.cpp:64-141).
+void launch_nve_initial(int n, double *x, double *v, const double *f,
+                        const int *elem, const double *mass_e, double dtf,
+                        double dtv, cudaStream_t st, long &launches);
+void launch_nve_final(int n, double *v, const double *f, const int *elem,
+                      const double *mass_e, double dtf, cudaStream_t st,
+                      long &launches);
+void launch_kinetic(int n, const double *v, const int *elem,
+                    const double *mass_e, double *ke_atom, cudaStream_t st,
+                    long &launches);
+void launch_check_finite(int n, const double *f, const double *etot,
+                         int *status, cudaStream_t st, long &launches);
+
+}  // namespace tmd

@@ -1,0 +1,229 @@
+"""PairTensorMD-shaped host interface over libtmd_b200.so.
+
+Mirrors the LAMMPS pair style of src/ML-TENSORMD/pair_tensormd.cpp:
+  settings()            no arguments allowed            (pair_tensormd.cpp:205-208)
+  coeff("* * f.npz El1 El2 [interp dx] [cmax ...]")      (:214-317)
+  init_one(i, j)        returns the cutoff rmax           (:336-341)
+  compute(eflag, vflag) energy -> eng_vdwl, forces -> f, virial via the
+                        fdotr convention, eatom / vatom   (:141-184)
+  extract("scale")      the fix-adapt scale factor        (:415-425)
+Atoms are handed over as LAMMPS would hold them for one rank with periodic
+images handled on the device: local positions x[n][3], 1-based types, box.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .lib import check, load_library
+
+_pd = ctypes.POINTER(ctypes.c_double)
+_pi = ctypes.POINTER(ctypes.c_int)
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(_pd)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(_pi)
+
+
+class TensorMDModel:
+    """A loaded potential (pair_coeff) on one CUDA device."""
+
+    def __init__(self, coeff_args: str, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        check(self.lib.tmd_model_load(coeff_args.encode(), device, ctypes.byref(h)))
+        self.h = h
+        cut = ctypes.c_double()
+        nelt, ntypes, nd, k, m = (ctypes.c_int() for _ in range(5))
+        check(self.lib.tmd_model_info(h, ctypes.byref(cut), ctypes.byref(nelt),
+                                      ctypes.byref(ntypes), ctypes.byref(nd),
+                                      ctypes.byref(k), ctypes.byref(m)))
+        self.cutmax = cut.value
+        self.nelt, self.ntypes, self.n_desc = nelt.value, ntypes.value, nd.value
+        self.num_filters, self.mmax = k.value, m.value
+        tmap = np.zeros(self.ntypes + 1, dtype=np.int32)
+        tmass = np.zeros(self.ntypes + 1, dtype=np.float64)
+        check(self.lib.tmd_model_type_map(h, _ip(tmap), _dp(tmass)))
+        self.type_map, self.type_mass = tmap, tmass
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tmd_model_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TensorMDSystem:
+    """Device-resident periodic cell (atoms, velocities, neighbor list)."""
+
+    def __init__(self, model: TensorMDModel, natoms_cap: int, skin: float = 1.0):
+        self.model = model
+        self.lib = model.lib
+        h = ctypes.c_void_p()
+        check(self.lib.tmd_system_create(model.h, int(natoms_cap), float(skin),
+                                         ctypes.byref(h)))
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tmd_system_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_box(self, box, pbc=(1, 1, 1)):
+        b = np.ascontiguousarray(box, dtype=np.float64)
+        p = np.ascontiguousarray(pbc, dtype=np.int32)
+        check(self.lib.tmd_system_set_box(self.h, _dp(b), _ip(p)))
+
+    def set_atoms(self, x, types, v=None):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        vv = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        self.n = x.shape[0]
+        check(self.lib.tmd_system_set_atoms(self.h, self.n, _dp(x), _ip(t), _dp(vv)))
+
+    def set_positions(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        check(self.lib.tmd_system_set_positions(self.h, _dp(x)))
+
+    def get(self):
+        n = self.n
+        x, v, f = (np.zeros((n, 3)) for _ in range(3))
+        img = np.zeros((n, 3), dtype=np.int32)
+        check(self.lib.tmd_system_get(self.h, _dp(x), _dp(v), _dp(f), _ip(img)))
+        return x, v, f, img
+
+    def compute(self, eflag=1, vflag=1, scale=1.0, peratom=False, forces=True):
+        n = self.n
+        e = np.zeros(1)
+        vir = np.zeros(6)
+        f = np.zeros((n, 3)) if forces else None
+        ea = np.zeros(n) if peratom else None
+        va = np.zeros((n, 6)) if peratom else None
+        check(self.lib.tmd_compute(self.h, int(eflag), int(vflag), float(scale), _dp(e),
+                                   _dp(vir), _dp(f), _dp(ea), _dp(va)))
+        out = dict(energy=float(e[0]), virial=vir, f=f)
+        if peratom:
+            out["eatom"], out["vatom"] = ea, va
+        return out
+
+    def nve_run(self, nsteps, dt, thermo_every=0):
+        rows = 0
+        th = None
+        if thermo_every:
+            rows = 1 + nsteps // thermo_every + (1 if nsteps % thermo_every else 0)
+            th = np.zeros((rows, 2))
+        check(self.lib.tmd_nve_run(self.h, int(nsteps), float(dt), int(thermo_every), _dp(th)))
+        return th
+
+    def neighbor_list(self, cut):
+        n = self.n
+        counts = np.zeros(max(n, 1), dtype=np.int32)
+        tot = ctypes.c_long()
+        check(self.lib.tmd_neighbor_list(self.h, float(cut), _ip(counts), None, 0,
+                                         ctypes.byref(tot)))
+        ent = np.zeros((max(tot.value, 1), 4), dtype=np.int32)
+        check(self.lib.tmd_neighbor_list(self.h, float(cut), _ip(counts), _ip(ent),
+                                         tot.value, ctypes.byref(tot)))
+        off = np.zeros(n + 1, dtype=np.int64)
+        off[1:] = np.cumsum(counts[:n])
+        return off, ent[: tot.value]
+
+    def descriptors(self):
+        G = np.zeros((self.n, self.model.n_desc))
+        check(self.lib.tmd_get_descriptors(self.h, _dp(G)))
+        return G
+
+    def stream(self) -> int:
+        p = ctypes.c_void_p()
+        check(self.lib.tmd_system_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def launches(self) -> int:
+        return int(self.lib.tmd_system_launches(self.h))
+
+    PROFILE_FAMILIES = ("neighbor", "descriptor", "mlp", "force", "gather", "nve", "reduce")
+
+    def profile(self, enable: bool):
+        check(self.lib.tmd_profile_enable(self.h, int(bool(enable))))
+
+    def profile_read(self, reset=True):
+        """{family: (launch-group count, summed device ms)} since the last reset."""
+        n = np.zeros(len(self.PROFILE_FAMILIES), dtype=np.int64)
+        ms = np.zeros(len(self.PROFILE_FAMILIES))
+        check(self.lib.tmd_profile_read(self.h, n.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
+                                        _dp(ms), int(bool(reset))))
+        return {f: (int(c), float(t)) for f, c, t in zip(self.PROFILE_FAMILIES, n, ms)}
+
+
+class PairTensorMD:
+    """The pair_style tensormd call surface, single rank, periodic on device."""
+
+    def __init__(self, device: int = 0, skin: float = 1.0):
+        self.device = device
+        self.skin = skin
+        self.model = None
+        self.system = None
+        self.scale = 1.0
+        self.eng_vdwl = 0.0
+        self.virial = np.zeros(6)
+        self.eatom = None
+        self.vatom = None
+
+    def settings(self, *args):
+        if args:
+            raise ValueError("Illegal pair_style command")
+
+    def coeff(self, args: str):
+        tok = args.split()
+        if len(tok) < 4 or tok[0] != "*" or tok[1] != "*":
+            raise ValueError("Incorrect args for pair coefficients")
+        self.model = TensorMDModel(" ".join(tok[2:]), self.device)
+        self.system = None
+
+    def init_one(self, i: int, j: int) -> float:
+        return self.model.cutmax
+
+    def extract(self, name: str):
+        if name == "scale":
+            return self.scale
+        return None
+
+    def compute(self, x, types, box, pbc=(1, 1, 1), eflag=1, vflag=1, eflag_atom=0,
+                vflag_atom=0):
+        """Forces f[n][3] for local atoms; sets eng_vdwl, virial, eatom, vatom."""
+        x = np.asarray(x, dtype=np.float64)
+        n = x.shape[0]
+        if self.system is None or n > self._cap:
+            self._cap = max(n, 1)
+            self.system = TensorMDSystem(self.model, self._cap, self.skin)
+            self._box = None
+        bx = tuple(np.asarray(box, dtype=np.float64).tolist()) + tuple(int(p) for p in pbc)
+        if self._box != bx:
+            self.system.set_box(box, pbc)
+            self._box = bx
+            self.system.set_atoms(x, types)
+        else:
+            self.system.set_atoms(x, types)
+        out = self.system.compute(eflag, vflag, self.scale, peratom=bool(eflag_atom or vflag_atom))
+        self.eng_vdwl = out["energy"] if eflag else 0.0
+        self.virial = out["virial"]
+        self.eatom = out.get("eatom")
+        self.vatom = out.get("vatom")
+        return out["f"]

@@ -1,0 +1,159 @@
+"""Seeded synthetic potentials and atom systems.
+
+Potential files use the key layout the reference reads (nnp.cpp:110-145,
+descriptor.h:45-85, tensormd.cpp:109-177, pair_tensormd.cpp:376-399), so the
+same .npz drives the reference and this package.  Weights are random (no
+trained checkpoint is available): N(0, 1/fan_in) with a fixed seed.
+
+Lattices, displacements and Maxwell-Boltzmann velocities follow LAMMPS metal
+units (update.cpp:187-206): boltz = 8.617343e-5 eV/K, mvv2e = 1.0364269e-4.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+BOLTZ = 8.617343e-5
+MVV2E = 1.0364269e-4
+NKTV2P = 1.6021765e6
+
+SYMBOLS = ["Cu", "Ni", "Al", "Fe", "Mo", "W", "Ti", "Co"]
+MASSES = {"Cu": 63.546, "Ni": 58.6934, "Al": 26.9815, "Fe": 55.845, "Mo": 95.95,
+          "W": 183.84, "Ti": 47.867, "Co": 58.9332}
+
+
+def gaussian_potential(path, *, nelt=1, num_filters=16, rc=6.0, max_moment=3,
+                       hidden=(64, 64), actfn=2, resnet=0, seed=1234, symbols=None,
+                       precision=64, fctype=0, output_bias=1):
+    """Write an analytic (descriptor::method = 3, Gaussian SF) potential.
+
+    Centers omega uniform on [0, rc]; eta so neighbouring Gaussians overlap at
+    one standard deviation (sigma = spacing):  exp(-eta (r-omega)^2 / rc^2)."""
+    rng = np.random.default_rng(seed)
+    symbols = list(symbols or SYMBOLS[:nelt])
+    K = num_filters
+    M = max_moment + 1
+    nin = nelt * K * M
+    ft = np.float32 if precision == 32 else np.float64
+    omega = np.linspace(0.0, rc, K)
+    spacing = rc / (K - 1)
+    eta = np.full(K, 0.5 * (rc / spacing) ** 2)
+    sizes = [nin] + list(hidden) + [1]
+    d = {
+        "precision": np.int32(precision),
+        "rmax": ft(rc),
+        "nelt": np.int32(nelt),
+        "max_moment": np.int32(max_moment),
+        "masses": np.array([MASSES.get(s, 50.0) for s in symbols], dtype=ft),
+        "numbers": np.array(sum(([ord(s[0]), ord(s[1]) if len(s) > 1 else 0]
+                                 for s in symbols), []), dtype=np.int32),
+        "tdnp": np.int32(0),
+        "use_fnn": np.int32(0),
+        "fctype": np.int32(fctype),
+        "is_T_symmetric": np.int32(0),
+        "descriptor::method": np.int32(3),
+        "descriptor::eta": eta.astype(ft),
+        "descriptor::omega": omega.astype(ft),
+        "nlayers": np.int32(len(sizes) - 1),
+        "actfn": np.int32(actfn),
+        "layer_sizes": np.array(sizes[1:], dtype=np.int32),
+        "use_resnet_dt": np.int32(resnet),
+        "apply_output_bias": np.int32(output_bias),
+    }
+    for e in range(nelt):
+        for l in range(len(sizes) - 1):
+            w = rng.normal(0.0, 1.0 / np.sqrt(sizes[l]), size=(sizes[l], sizes[l + 1]))
+            d[f"weights_{e}_{l}"] = (w if sizes[l + 1] > 1 else w[:, 0]).astype(ft)
+            if l < len(sizes) - 2 or output_bias:
+                b = rng.normal(0.0, 0.1, size=sizes[l + 1])
+                d[f"biases_{e}_{l}"] = (b if sizes[l + 1] > 1 else b.reshape(())).astype(ft)
+    np.savez(path, **d)
+    return symbols
+
+
+def _lattice_basis(kind):
+    if kind == "fcc":
+        return np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    if kind == "bcc":
+        return np.array([[0, 0, 0], [0.5, 0.5, 0.5]])
+    if kind == "sc":
+        return np.array([[0.0, 0.0, 0.0]])
+    raise ValueError(kind)
+
+
+def lattice(kind, a, nx, ny, nz):
+    """Positions of an orthogonal nx x ny x nz lattice and its box[9]."""
+    basis = _lattice_basis(kind)
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz),
+                             indexing="ij"), -1).reshape(-1, 3)
+    x = (g[:, None, :] + basis[None, :, :]).reshape(-1, 3) * a
+    box = np.array([0.0, 0.0, 0.0, nx * a, ny * a, nz * a, 0.0, 0.0, 0.0])
+    return x, box
+
+
+def wrap(x, box):
+    """Wrap positions into an orthogonal box (Domain::remap for orthogonal)."""
+    lo = box[:3]
+    prd = box[3:6]
+    return lo + np.mod(x - lo, prd)
+
+
+def maxwell(masses, T, rng):
+    """Velocities (A/ps) drawn from Maxwell-Boltzmann at T, zero momentum, then
+    scaled so the temperature with dof = 3N - 3 is exactly T (LAMMPS
+    velocity create ... dist gaussian, mom yes, rot no)."""
+    n = len(masses)
+    v = rng.normal(size=(n, 3)) / np.sqrt(masses)[:, None]
+    p = (masses[:, None] * v).sum(0) / masses.sum()
+    v -= p
+    ke = 0.5 * MVV2E * (masses[:, None] * v * v).sum()
+    dof = 3 * n - 3
+    t_now = 2.0 * ke / (dof * BOLTZ) if dof > 0 else 0.0
+    if t_now > 0:
+        v *= np.sqrt(T / t_now)
+    return v
+
+
+def temperature(masses, v):
+    n = len(masses)
+    ke = 0.5 * MVV2E * (masses[:, None] * v * v).sum()
+    return 2.0 * ke / ((3 * n - 3) * BOLTZ)
+
+
+def build_system(kind, a, cells, *, sigma=0.0, T=0.0, nelt=1, seed=7, masses=None):
+    """Lattice + Gaussian displacements + random equal-fraction occupancy.
+
+    Returns x, types (1-based), box, v."""
+    rng = np.random.default_rng(seed)
+    x, box = lattice(kind, a, *cells)
+    n = len(x)
+    if sigma > 0:
+        x = x + rng.normal(0.0, sigma, size=x.shape)
+        x = wrap(x, box)
+    if nelt > 1:
+        types = (np.arange(n) % nelt) + 1
+        rng.shuffle(types)
+    else:
+        types = np.ones(n, dtype=np.int32)
+    types = types.astype(np.int32)
+    v = np.zeros_like(x)
+    if T > 0:
+        m = np.ones(n) * 50.0 if masses is None else np.asarray(masses)[types - 1]
+        v = maxwell(m, T, rng)
+    return x, types, box, v
+
+
+def config(name):
+    """The workloads this path is measured on (shapes from the task spec)."""
+    if name == "fcc4k":  # plain CPU config: 4,000 atoms
+        return dict(kind="fcc", a=3.61, cells=(10, 10, 10), sigma=0.05, T=300.0, nelt=1,
+                    pot=dict(nelt=1, num_filters=16, rc=6.0, max_moment=3,
+                             hidden=(64, 64), actfn=2))
+    if name == "bcc128k":  # plain FP32 GPU config: 128,000 atoms
+        return dict(kind="bcc", a=2.87, cells=(40, 40, 40), sigma=0.08, T=600.0, nelt=1,
+                    pot=dict(nelt=1, num_filters=16, rc=6.0, max_moment=3,
+                             hidden=(64, 64), actfn=2))
+    if name == "alloy432k":  # precision config: 4 elements, 432,000 atoms
+        return dict(kind="fcc", a=3.6, cells=(60, 60, 30), sigma=0.05, T=300.0, nelt=4,
+                    pot=dict(nelt=4, num_filters=32, rc=6.5, max_moment=3,
+                             hidden=(128, 128, 128), actfn=1))
+    raise KeyError(name)

@@ -438,10 +438,10 @@ long tmdo_neighbors(int n, const double *x, const double *boxv, const int *pbc,
                  V / sqrt(axb[0] * axb[0] + axb[1] * axb[1] + axb[2] * axb[2])};
   int nb[3], ns[3];
   for (int a = 0; a < 3; a++) {
-    nb[a] = (int)floor(w[a] / cut);
+    nb[a] = (int)floor(w[a] / (cut * (1.0 + 1e-6)));
     if (nb[a] < 1) nb[a] = 1;
     if (nb[a] > 256) nb[a] = 256;
-    ns[a] = (int)ceil(cut / (w[a] / nb[a]) - 1e-12);
+    ns[a] = (int)ceil(cut * (1.0 + 1e-9) / (w[a] / nb[a]));
     if (!b.pbc[a]) { /* non-periodic: no images, cells only */
       if (ns[a] > nb[a]) ns[a] = nb[a];
     }

@@ -1,0 +1,102 @@
+"""Regenerate tests/golden/ from the reference tree (run where it is mounted).
+
+    python tests/golden/make_golden.py /path/to/lammps-tensormd
+
+Copies three shipped potentials and two data files, and extracts the
+published step-0 results of the reference (LAMMPS thermo lines and the
+force.yaml dump, read as text) into published.json:
+
+  examples/tensormd/binary/medium/output           96,000-atom MoNi_m3 run:
+        step-0 energy (15 digits), pressure components, max force component
+  examples/tensormd/binary/medium/force.yaml       per-atom step-0 forces
+  examples/tensormd/trinary/a100_log/log_release.lammps     AlMgSi energy
+  examples/tensormd/W/tensormd/speedup/a100_log/log_0114.lammps  W_k32 energy
+
+The test suite reads only the files written here.
+"""
+from __future__ import annotations
+
+import json
+import re
+import shutil
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+
+
+def main(ref: Path):
+    ex = ref / "examples" / "tensormd"
+    files = {
+        "MoNi_m3.npz": ex / "binary/medium/MoNi_m3.npz",
+        "W_k32_snapshot.npz": ex / "W/tensormd/W_k32_snapshot.npz",
+        "AlMgSi.24aug13.npz": ex / "trinary/AlMgSi.24aug13.npz",
+        "Mo8_Ni8_id3210.data": ex / "binary/Mo8_Ni8_id3210.data",
+        "AlMgSi.data": ex / "trinary/AlMgSi.data",
+    }
+    for dst, src in files.items():
+        shutil.copyfile(src, HERE / dst)
+
+    out = ex / "binary/medium/output"
+    txt = out.read_text()
+    m = re.search(r"Energy initial, next-to-last, final = \s*\n\s*(\S+)", txt)
+    e96k = float(m.group(1))
+    thermo0 = None
+    for line in txt.splitlines():
+        t = line.split()
+        if len(t) == 8 and t[0] == "0":
+            thermo0 = [float(v) for v in t]
+            break
+    fmax = float(re.search(r"Force max component initial, final = (\S+)", txt).group(1))
+    forces = []
+    for line in (ex / "binary/medium/force.yaml").read_text().splitlines():
+        mm = re.match(r"\s*- \[\s*(\d+)\s*,\s*(\d+)\s*,\s*(\S+)\s*,\s*(\S+)\s*,\s*(\S+?)\s*,", line)
+        if mm:
+            forces.append([int(mm.group(1)), int(mm.group(2)), float(mm.group(3)),
+                           float(mm.group(4)), float(mm.group(5))])
+
+    def thermo_pe(path):
+        """PotEng of the step-0 thermo line, located by the header column."""
+        header = None
+        for line in path.read_text().splitlines():
+            t = line.split()
+            if t and t[0] == "Step":
+                header = t
+            elif header and t and t[0] == "0" and len(t) == len(header):
+                return float(t[header.index("PotEng")])
+        raise RuntimeError(path)
+
+    almgsi = thermo_pe(ex / "trinary/a100_log/log_release.lammps")
+    w = thermo_pe(ex / "W/tensormd/speedup/a100_log/log_0114.lammps")
+    pub = {
+        "MoNi_m3": {
+            "source": "examples/tensormd/binary/medium/output (data file x 10x20x30, "
+                      "pair_coeff * * MoNi_m3.npz Mo Ni interp 0.0001, T = 0)",
+            "replicas": 6000, "energy_total": e96k,
+            "press": thermo0[4], "pxx": thermo0[5], "pyy": thermo0[6], "pzz": thermo0[7],
+            "fmax_component": fmax, "interp": 1e-4, "elements": ["Mo", "Ni"],
+        },
+        "MoNi_m3_forces": {
+            "source": "examples/tensormd/binary/medium/force.yaml (2x2x2 replica, "
+                      "columns id type fx fy fz)",
+            "rows": forces,
+        },
+        "AlMgSi": {
+            "source": "examples/tensormd/trinary/a100_log/log_release.lammps "
+                      "(AlMgSi.data x 10x10x3, interp 0.0001)",
+            "replicas": 300, "energy_total": almgsi, "elements": ["Al", "Mg", "Si"],
+            "interp": 1e-4,
+        },
+        "W_k32": {
+            "source": "examples/tensormd/W/tensormd/speedup/a100_log/log_0114.lammps "
+                      "(bcc 3.189, 24x24x20, interp 0.001)",
+            "natoms": 23040, "energy_total": w, "lattice": 3.189, "interp": 1e-3,
+            "elements": ["W"],
+        },
+    }
+    (HERE / "published.json").write_text(json.dumps(pub, indent=1))
+    print("wrote", HERE / "published.json")
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))

@@ -1,0 +1,58 @@
+"""Pin the FP64 oracle to the reference's own published outputs.
+
+The reference has no unit tests for pair_style tensormd; its only known
+answers are the example logs and the force.yaml dump (read as text into
+tests/golden/published.json by tests/golden/make_golden.py).  These tests run
+the oracle on the same potentials and cells and require agreement to the
+printed precision.
+"""
+import numpy as np
+import pytest
+
+from pack import Oracle
+from tmd_testutil import GOLDEN, NKTV2P, published, read_data, volume
+
+
+@pytest.fixture(scope="module")
+def pub():
+    return published()
+
+
+def test_moni_m3_energy_forces_pressure(pub):
+    p = pub["MoNi_m3"]
+    x, t, box = read_data(GOLDEN / "Mo8_Ni8_id3210.data")
+    o = Oracle(str(GOLDEN / "MoNi_m3.npz"), interp=p["interp"])
+    out = o.compute(x, t - 1, box, [1, 1, 1], skin=1.0)
+    # 96,000-atom energy printed with 15 significant digits
+    assert out["energy"] == pytest.approx(p["energy_total"] / p["replicas"], abs=1e-9)
+    vir = out["virial"] / volume(box) * NKTV2P
+    assert vir[0] == pytest.approx(p["pxx"], abs=1e-3)
+    assert vir[1] == pytest.approx(p["pyy"], abs=1e-3)
+    assert vir[2] == pytest.approx(p["pzz"], abs=1e-3)
+    assert vir[:3].mean() == pytest.approx(p["press"], abs=1e-3)
+    rows = np.array(pub["MoNi_m3_forces"]["rows"])
+    # force.yaml holds a 2x2x2 replica: 8 copies of the 16 distinct atoms
+    ref = rows[:16, 2:5]
+    for k in range(1, 8):
+        assert np.allclose(rows[16 * k:16 * (k + 1), 2:5], ref, atol=1e-8)
+    assert np.abs(out["f"] - ref).max() < 1e-8  # printed to 8 decimals
+    assert np.abs(out["f"]).max() == pytest.approx(p["fmax_component"], abs=1e-9)
+
+
+def test_almgsi_energy(pub):
+    p = pub["AlMgSi"]
+    x, t, box = read_data(GOLDEN / "AlMgSi.data")
+    o = Oracle(str(GOLDEN / "AlMgSi.24aug13.npz"), interp=p["interp"])
+    e = o.compute(x, t - 1, box, [1, 1, 1])["energy"]
+    # thermo prints 8 significant digits of the 32,400-atom total
+    assert e * p["replicas"] == pytest.approx(p["energy_total"], abs=0.5)
+
+
+def test_w_k32_energy(pub):
+    p = pub["W_k32"]
+    a = p["lattice"]
+    x = np.array([[0.0, 0.0, 0.0], [0.5 * a, 0.5 * a, 0.5 * a]])
+    box = np.array([0, 0, 0, a, a, a, 0, 0, 0], dtype=float)
+    o = Oracle(str(GOLDEN / "W_k32_snapshot.npz"), interp=p["interp"])
+    e = o.compute(x, [0, 0], box, [1, 1, 1])["energy"]
+    assert e / 2 * p["natoms"] == pytest.approx(p["energy_total"], abs=0.05)
