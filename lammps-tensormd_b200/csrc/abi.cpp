@@ -91,7 +91,8 @@ struct tmd_system {
       *cell_cursor = nullptr, *cell_atoms = nullptr;
   uint32_t *tmp = nullptr, *nbr = nullptr;
   int *nraw = nullptr, *boff = nullptr, *rev = nullptr;
-  float *P = nullptr, *G = nullptr, *dEdG = nullptr, *E = nullptr;
+  float *P = nullptr, *G = nullptr, *dEdG = nullptr;
+  double *E = nullptr;
   float4 *pdf = nullptr;
   double *wv = nullptr, *eatom = nullptr, *vatom = nullptr, *ke = nullptr;
   double *partial = nullptr, *scal = nullptr;  // scal: [0] pe, [1..6] virial, [7] ke
@@ -111,7 +112,18 @@ struct tmd_system {
   long prof_n[TMD_NPROF] = {0};
   double prof_ms[TMD_NPROF] = {0};
   cudaEvent_t cur_start = nullptr;
+  // captured MD step (velocity Verlet + rebuild check/rebuild + force)
+  cudaGraphExec_t step_exec = nullptr;
+  double step_dt = 0.0;
+  long step_launches = 0;
 };
+
+namespace {
+void drop_graph(tmd_system *s) {
+  if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
+  s->step_exec = nullptr;
+}
+}  // namespace
 
 namespace {
 
@@ -182,6 +194,7 @@ void widths(const BoxP &b, double w[3]) {
 }
 
 int bin_setup(tmd_system *s) {
+  drop_graph(s);
   double cut = s->m->h.rmax + s->skin;
   double w[3];
   widths(s->box, w);
@@ -228,6 +241,7 @@ int pow2_at_least(int v) {
 }
 
 int alloc_neighbors(tmd_system *s, int cap) {
+  drop_graph(s);
   cap = (cap + 31) / 32 * 32;
   if (cap > 4096) return fail(TMD_ERR_CAPACITY, "more than 4096 neighbors per atom");
   dfree(s->tmp); dfree(s->nbr); dfree(s->rev); dfree(s->pdf);
@@ -380,16 +394,29 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     e = up(h.table, &m->d_table);
     m->kp.table = m->d_table;
   }
+  auto upd = [&](const std::vector<double> &v, double **p) -> cudaError_t {
+    cudaError_t e2 = dalloc(p, v.size());
+    if (e2 != cudaSuccess) return e2;
+    m->d_buf.push_back(reinterpret_cast<float *>(*p));
+    return cudaMemcpy(*p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
+  };
   for (int el = 0; el < h.nelt && e == cudaSuccess; el++)
     for (int l = 0; l < h.nl && e == cudaSuccess; l++) {
       MlpLayer &L = layers[(size_t)el * h.nl + l];
       L.K = h.sizes[l];
       L.N = h.sizes[l + 1];
       float *w = nullptr, *b = nullptr;
+      double *wd = nullptr, *bd = nullptr;
       e = up(h.W[el][l], &w);
       if (e == cudaSuccess && !h.Bs[el][l].empty()) e = up(h.Bs[el][l], &b);
+      if (l == h.nl - 1) {
+        if (e == cudaSuccess) e = upd(h.Wout[el], &wd);
+        if (e == cudaSuccess && !h.Bout[el].empty()) e = upd(h.Bout[el], &bd);
+      }
       L.W = w;
       L.b = b;
+      L.Wd = wd;
+      L.bd = bd;
     }
   if (e == cudaSuccess) e = dalloc(&m->d_layers, layers.size());
   if (e == cudaSuccess)
@@ -492,6 +519,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
 void tmd_system_free(tmd_system *s) {
   if (!s) return;
   if (s->st) cudaStreamSynchronize(s->st);
+  drop_graph(s);
   dfree(s->x); dfree(s->v); dfree(s->f); dfree(s->xbuild); dfree(s->image); dfree(s->elem);
   dfree(s->cell_of); dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_cursor);
   dfree(s->cell_atoms); dfree(s->tmp); dfree(s->nbr); dfree(s->nraw); dfree(s->boff);
@@ -538,6 +566,7 @@ int tmd_system_set_atoms(tmd_system *s, int n, const double *x, const int *type,
   if (!s->have_box) return fail(TMD_ERR_STATE, "set the box before the atoms");
   TMD_CUDA(cudaSetDevice(s->m->device));
   const HostModel &h = s->m->h;
+  drop_graph(s);
   s->n = n;
   s->h_elem.resize(n);
   int ntypes = (int)h.type_elements.size();
@@ -628,13 +657,13 @@ int tmd_compute(tmd_system *s, int eflag, int vflag, double scale, double *energ
   bool want_vatom = vatom != nullptr;
   launch_force_eval(s, (float)scale, want_vatom);
   if (eflag || energy)
-    launch_reduce_f32(s->E, n, s->partial, s->scal, scale, s->st, s->launches);
+    launch_reduce_scaled(s->E, n, s->partial, s->scal, scale, s->st, s->launches);
   if (vflag || virial)
     launch_reduce_f64(s->wv, n, 6, s->partial, s->scal + 1, s->st, s->launches);
   launch_check_finite(n, s->f, (eflag || energy) ? s->scal : nullptr, s->status, s->st,
                       s->launches);
   TMD_CUDA(cudaGetLastError());
-  if (eatom) launch_scale_copy_f32(s->E, n, scale, s->eatom, s->st, s->launches);
+  if (eatom) launch_scale_copy(s->E, n, scale, s->eatom, s->st, s->launches);
   TMD_CUDA(cudaMemcpyAsync(s->h_scal, s->scal, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
   if (f) TMD_CUDA(cudaMemcpyAsync(f, s->f, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
   if (eatom) TMD_CUDA(cudaMemcpyAsync(eatom, s->eatom, n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
@@ -677,7 +706,7 @@ int tmd_nve_run(tmd_system *s, int nsteps, double dt, int thermo_every, double *
   int rc = clear_status(s);
   if (rc) return rc;
   auto thermo_row = [&](int r) {
-    launch_reduce_f32(s->E, n, s->partial, s->thermo_d + 2 * r, 1.0, s->st, s->launches);
+    launch_reduce_scaled(s->E, n, s->partial, s->thermo_d + 2 * r, 1.0, s->st, s->launches);
     launch_kinetic(n, s->v, s->elem, s->m->d_mass, s->ke, s->st, s->launches);
     launch_reduce_f64(s->ke, n, 1, s->partial, s->thermo_d + 2 * r + 1, s->st, s->launches);
   };
@@ -685,7 +714,7 @@ int tmd_nve_run(tmd_system *s, int nsteps, double dt, int thermo_every, double *
   launch_force_eval(s, 1.0f, false);
   int row = 0;
   if (thermo) thermo_row(row++);
-  for (int step = 1; step <= nsteps; step++) {
+  auto md_step = [&]() {
     prof_begin(s);
     launch_nve_initial(n, s->x, s->v, s->f, s->elem, s->m->d_mass, dtf, dt, s->st, s->launches);
     launch_neighbor_check(n, s->x, s->xbuild, trigsq, s->flag, s->st, s->launches);
@@ -697,6 +726,35 @@ int tmd_nve_run(tmd_system *s, int nsteps, double dt, int thermo_every, double *
     prof_begin(s);
     launch_nve_final(n, s->v, s->f, s->elem, s->m->d_mass, dtf, s->st, s->launches);
     prof_end(s, 5);
+  };
+  // Without kernel timing, the step runs as one captured CUDA graph: every
+  // launch (including the conditional rebuild kernels) is replayed with its
+  // arguments fixed at capture; buffers, box, atom count and dt key the graph.
+  const bool use_graph = !s->prof;
+  if (use_graph && (!s->step_exec || s->step_dt != dt)) {
+    drop_graph(s);
+    cudaGraph_t g;
+    long l0 = s->launches;
+    TMD_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+    md_step();
+    TMD_CUDA(cudaStreamEndCapture(s->st, &g));
+    cudaError_t ie = cudaGraphInstantiate(&s->step_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      s->step_exec = nullptr;
+      return fail(TMD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
+    }
+    s->step_launches = s->launches - l0;
+    s->launches = l0;
+    s->step_dt = dt;
+  }
+  for (int step = 1; step <= nsteps; step++) {
+    if (use_graph) {
+      TMD_CUDA(cudaGraphLaunch(s->step_exec, s->st));
+      s->launches += s->step_launches;
+    } else {
+      md_step();
+    }
     if (thermo && (step % thermo_every == 0 || step == nsteps)) {
       prof_begin(s);
       thermo_row(row++);

@@ -1,0 +1,190 @@
+// force_impl.cuh -- dE_i/dx_j for every neighbor pair, without atomics.
+//
+// Reverse mode through the descriptor (tensormd.cpp:563-602):
+//   dEdG'[b,k,0] = 0.5 dEdG[b,k,0] / G[b,k,0]   (0 if |G0| < 1e-8)
+//   S[b,k,d] = dE/dP = 2 P[b,k,d] sum_m T[m,d] dEdG'[b,k,m]
+//                                         (kernel.cu:775-817, tensor_ops.cpp:633-674)
+//   U_k = sum_d S[k,d] M_d, V_d = sum_k S[k,d] H_k
+//   df = (sum_k U_k dH_k) u + sum_d V_d dM_d/dx_j     (F1 + F2, kernel.cu:541-631,
+//                                                       tensor_ops.cpp:126-190,470-535)
+// The reference writes U, V, F1 and F2 per padded slot and scatters df with
+// FP64 atomics (kernel.cu:1639-1758).  Here S stays in registers (4 filters x D
+// per lane as FP32 pairs, TPA = K/4 lanes per atom), U and V are packed FP32x2
+// FMAs, sum_d V_d dM_d/dx_j is the gradient of the polynomial
+// Q(u) = sum_d V_d M_d(u), and df (times the pair_coeff scale) goes to its
+// slot pdf[i*cap + t].  Pair geometry is shared through shared memory as in
+// the descriptor kernel.  The reaction -df on j is summed later by k_gather
+// through the partner slot, in a fixed order.
+//
+// wv[i] = sum over i's pairs of -r_ij (x) df (xx, yy, zz, xy, xz, yz): the
+// per-pair virial of sum_forces_device (kernel.cu:1714-1758), accumulated in
+// FP64 by the lane that computed the pair's FP64 geometry; its sum over atoms
+// is the global virial.
+#pragma once
+
+#include "descriptor_impl.cuh"
+
+namespace tmd {
+
+template <int TPA, int D, int RK>
+__global__ void __launch_bounds__(kPairThreads, 3)
+k_force(KParams kp, BoxP box, int n, int cap, float scale,
+        const double *__restrict__ x, const int *__restrict__ elem,
+        const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
+        const float *__restrict__ P, const float *__restrict__ G,
+        const float *__restrict__ dEdG, float4 *__restrict__ pdf,
+        double *__restrict__ wv) {
+  constexpr int D2 = (D + 1) / 2;
+  __shared__ GeoSlot geo[kPairThreads];
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = gt / TPA;
+  const int sub = gt % TPA;
+  if (a >= n) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask =
+      TPA == 32 ? 0xffffffffu : (((1u << TPA) - 1u) << (lane & ~(TPA - 1)));
+  GeoSlot *gslot = geo + (threadIdx.x - sub);
+  const int B = kp.B, K = kp.K, M = kp.M;
+  const int k0 = 4 * sub;
+  const Radial4<RK> R = load_radial4<RK>(kp, k0);
+  const double xi = x[3 * a], yi = x[3 * a + 1], zi = x[3 * a + 2];
+  const uint32_t *row = nbr + (size_t)a * cap;
+  const int *bo = boff + (size_t)a * (B + 1);
+  double w6[6] = {0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < B; b++) {
+    const int s0 = bo[b], s1 = bo[b + 1];
+    if (s0 == s1) continue;
+    // S = dE/dP for this lane's 4 filters, as FP32 pairs over d
+    float2 S2[4][D2];
+    {
+      const float *Pp = P + (((size_t)a * B + b) * K + k0) * D;
+      const float *Gp = G + (size_t)a * kp.nin + ((size_t)b * K + k0) * M;
+      const float *dGp = dEdG + (size_t)a * kp.nin + ((size_t)b * K + k0) * M;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        float gp[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int m = 0; m < M; m++) gp[m] = dGp[q * M + m];
+        float g0 = Gp[q * M];
+        gp[0] = fabsf(g0) < 1e-8f ? 0.f : gp[0] / g0 * 0.5f;
+        float Sq[2 * D2];
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          float t = 0.f;
+          for (int m = 0; m < M; m++) t = fmaf(gp[m], kp.T[m * D + d], t);
+          Sq[d] = 2.f * t * Pp[q * D + d];
+        }
+        if (D & 1) Sq[D] = 0.f;
+#pragma unroll
+        for (int p = 0; p < D2; p++) S2[q][p] = make_float2(Sq[2 * p], Sq[2 * p + 1]);
+      }
+    }
+    NbPos pnext = load_nb(x, s0 + sub < s1 ? row[s0 + sub] : 0u, s0 + sub < s1);
+    uint32_t enext = (s0 + TPA + sub < s1) ? row[s0 + TPA + sub] : 0u;
+    for (int t0 = s0; t0 < s1; t0 += TPA) {
+      const NbPos pc = pnext;
+      pnext = load_nb(x, enext, t0 + TPA + sub < s1);
+      enext = (t0 + 2 * TPA + sub < s1) ? row[t0 + 2 * TPA + sub] : 0u;
+      PairGeo mine;
+      pair_geometry(kp, box, xi, yi, zi, pc, mine);
+      __syncwarp(gmask);
+      geo_store(gslot + sub, mine);
+      __syncwarp(gmask);
+      const int cnt = min(TPA, s1 - t0);
+      float3 mydf = make_float3(0.f, 0.f, 0.f);
+      for (int c = 0; c < cnt; c++) {
+        const PairGeo g = geo_load(gslot + c);
+        if (g.ti < 0) continue;
+        float H[4], dH[4];
+        radial4<RK, true>(kp, R, g, H, dH);
+        float2 M2[D2];
+        moments2<D, D2>(g.ux, g.uy, g.uz, M2);
+        float f1 = 0.f;
+        float2 V2[D2];
+#pragma unroll
+        for (int p = 0; p < D2; p++) V2[p] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          float2 U2 = make_float2(0.f, 0.f);
+          const float2 h2 = make_float2(H[q], H[q]);
+#pragma unroll
+          for (int p = 0; p < D2; p++) {
+            U2 = __ffma2_rn(S2[q][p], M2[p], U2);
+            V2[p] = __ffma2_rn(S2[q][p], h2, V2[p]);
+          }
+          f1 = fmaf(U2.x + U2.y, dH[q], f1);
+        }
+        float V[2 * D2];
+#pragma unroll
+        for (int p = 0; p < D2; p++) { V[2 * p] = V2[p].x; V[2 * p + 1] = V2[p].y; }
+        float gq[3], nvm;
+        poly_grad<D>(V, g.ux, g.uy, g.uz, gq, nvm);
+        const float rinv = 1.f / g.r;
+        float fx = f1 * g.ux + (gq[0] - g.ux * nvm) * rinv;
+        float fy = f1 * g.uy + (gq[1] - g.uy * nvm) * rinv;
+        float fz = f1 * g.uz + (gq[2] - g.uz * nvm) * rinv;
+#pragma unroll
+        for (int o = TPA >> 1; o > 0; o >>= 1) {
+          fx += __shfl_xor_sync(gmask, fx, o, TPA);
+          fy += __shfl_xor_sync(gmask, fy, o, TPA);
+          fz += __shfl_xor_sync(gmask, fz, o, TPA);
+        }
+        if (c == sub) mydf = make_float3(fx * scale, fy * scale, fz * scale);
+      }
+      // every lane owns one pair of the chunk: store it and add its virial
+      // with the FP64 separation this lane computed
+      if (t0 + sub < s1) {
+        pdf[(size_t)a * cap + t0 + sub] = make_float4(mydf.x, mydf.y, mydf.z, 0.f);
+        if (mine.ti >= 0) {
+          double rr = (double)mine.r + (double)mine.rlo;
+          double rx = (double)mine.ux * rr, ry = (double)mine.uy * rr,
+                 rz = (double)mine.uz * rr;
+          w6[0] -= rx * mydf.x;
+          w6[1] -= ry * mydf.y;
+          w6[2] -= rz * mydf.z;
+          w6[3] -= rx * mydf.y;
+          w6[4] -= rx * mydf.z;
+          w6[5] -= ry * mydf.z;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 6; c++) {
+#pragma unroll
+    for (int o = TPA >> 1; o > 0; o >>= 1) w6[c] += __shfl_xor_sync(gmask, w6[c], o, TPA);
+  }
+  if (sub == 0) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) wv[(size_t)a * 6 + c] = w6[c];
+  }
+}
+
+template <int TPA, int RK>
+void launch_force_tpa(const ForceArgs &a, cudaStream_t st) {
+  const int T = kPairThreads;
+  long threads = (long)a.n * TPA;
+  int grid = (int)((threads + T - 1) / T);
+  if (grid < 1) grid = 1;
+#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.dEdG, a.pdf, a.wv
+  switch (a.kp.D) {
+    case 1: k_force<TPA, 1, RK><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
+    case 4: k_force<TPA, 4, RK><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
+    case 10: k_force<TPA, 10, RK><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
+    default: k_force<TPA, 20, RK><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
+  }
+#undef TMD_FORCE_ARGS
+}
+
+template <int RK>
+void launch_force_rk(const ForceArgs &a, cudaStream_t st) {
+  switch (a.kp.K / 4) {
+    case 1: launch_force_tpa<1, RK>(a, st); break;
+    case 2: launch_force_tpa<2, RK>(a, st); break;
+    case 4: launch_force_tpa<4, RK>(a, st); break;
+    case 8: launch_force_tpa<8, RK>(a, st); break;
+    case 16: launch_force_tpa<16, RK>(a, st); break;
+    default: launch_force_tpa<32, RK>(a, st); break;
+  }
+}
+
+}  // namespace tmd

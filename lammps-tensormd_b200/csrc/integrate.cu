@@ -68,22 +68,22 @@ void launch_reduce_f64(const double *in, int n, int ncomp, double *partial,
   launches += 2;
 }
 
-void launch_reduce_f32(const float *in, int n, double *partial, double *out,
-                       double scale, cudaStream_t st, long &launches) {
+void launch_reduce_scaled(const double *in, int n, double *partial, double *out,
+                          double scale, cudaStream_t st, long &launches) {
   int nb = red_blocks(n);
-  k_reduce_partial<float><<<nb, kRedThreads, 0, st>>>(in, n, 1, scale, partial);
+  k_reduce_partial<double><<<nb, kRedThreads, 0, st>>>(in, n, 1, scale, partial);
   k_reduce_final<<<1, kRedThreads, 0, st>>>(partial, nb, 1, out);
   launches += 2;
 }
 
-__global__ void k_scale_copy(const float *__restrict__ in, int n, double scale,
+__global__ void k_scale_copy(const double *__restrict__ in, int n, double scale,
                              double *__restrict__ out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = (double)in[i] * scale;
+  if (i < n) out[i] = in[i] * scale;
 }
 
-void launch_scale_copy_f32(const float *in, int n, double scale, double *out,
-                           cudaStream_t st, long &launches) {
+void launch_scale_copy(const double *in, int n, double scale, double *out,
+                       cudaStream_t st, long &launches) {
   k_scale_copy<<<(n + 255) / 256, 256, 0, st>>>(in, n, scale, out);
   launches += 1;
 }

@@ -43,8 +43,11 @@ __device__ inline float act_fwd(int actfn, float z, float &d) {
       return y;
     }
     default: {
+      // squareplus 0.5 (z + sqrt(z^2 + 4)); for z < 0 the same value is
+      // 2 / (sqrt(z^2 + 4) - z), which avoids the cancellation that costs
+      // FP32 most of its digits when z << 0
       float q = sqrtf(z * z + 4.f);
-      float y = 0.5f * (z + q);
+      float y = z >= 0.f ? 0.5f * (z + q) : 2.f / (q - z);
       d = y / q;
       return y;
     }
@@ -166,22 +169,22 @@ k_mlp_fp32(MlpArgs a) {
                   });
     float *t = in; in = out; out = t;
   }
-  // output layer (one output per atom; the reference sums outputs)
+  // output layer in FP64 (one output per atom; the reference sums outputs)
   {
     const MlpLayer ly = Ls[L - 1];
     const int per = kThreads / TR;  // threads per row
     const int r = tid / per, part = tid % per;
-    float s = 0.f;
+    double s = 0.0;
     for (int k = part; k < ly.K; k += per) {
-      float wsum = 0.f;
-      for (int o2 = 0; o2 < ly.N; o2++) wsum += __ldg(ly.W + (size_t)k * ly.N + o2);
-      s = fmaf(in[(size_t)k * LDT + r], wsum, s);
+      double wsum = 0.0;
+      for (int o2 = 0; o2 < ly.N; o2++) wsum += __ldg(ly.Wd + (size_t)k * ly.N + o2);
+      s = fma((double)in[(size_t)k * LDT + r], wsum, s);
     }
     for (int o2 = per >> 1; o2 > 0; o2 >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o2);
     if (part == 0 && rows[r] >= 0) {
-      float e = s;
-      if (ly.b)
-        for (int o2 = 0; o2 < ly.N; o2++) e += __ldg(ly.b + o2);
+      double e = s;
+      if (ly.bd)
+        for (int o2 = 0; o2 < ly.N; o2++) e += __ldg(ly.bd + o2);
       a.E[rows[r]] = e;
     }
   }

@@ -325,16 +325,20 @@ HostModel parse_model(const std::string &coeff_args) {
   h.resnet = (res_raw && n_res > 0) ? 1 : 0;
   h.W.assign(h.nelt, std::vector<std::vector<float>>(h.nl));
   h.Bs.assign(h.nelt, std::vector<std::vector<float>>(h.nl));
+  h.Wout.assign(h.nelt, {});
+  h.Bout.assign(h.nelt, {});
   for (int e = 0; e < h.nelt; e++)
     for (int l = 0; l < h.nl; l++) {
       const auto &w = need(z, "weights_" + std::to_string(e) + "_" + std::to_string(l));
       if ((int)w.size() != h.sizes[l] * h.sizes[l + 1])
         bad("weights_" + std::to_string(e) + "_" + std::to_string(l) + " has a wrong shape");
       h.W[e][l].assign(w.d.begin(), w.d.end());
+      if (l == h.nl - 1) h.Wout[e] = w.d;
       if (l < h.nl - 1 || h.outbias) {
         const auto &b = need(z, "biases_" + std::to_string(e) + "_" + std::to_string(l));
         if ((int)b.size() != h.sizes[l + 1]) bad("bias shape mismatch");
         h.Bs[e][l].assign(b.d.begin(), b.d.end());
+        if (l == h.nl - 1) h.Bout[e] = b.d;
       }
     }
   if (h.interp_dx > 0) {
@@ -384,8 +388,12 @@ void fill_kparams(const HostModel &h, KParams &kp) {
   }
   for (int k = 0; k < h.K; k++) {
     if (!h.p0.empty()) kp.p0[k] = float(h.p0[k]);
-    if (!h.p1.empty()) kp.p1[k] = float(h.p1[k]);
+    if (!h.p1.empty()) {
+      kp.p1[k] = float(h.p1[k]);
+      kp.p1lo[k] = float(h.p1[k] - double(kp.p1[k]));
+    }
     if (!h.p2.empty()) kp.p2[k] = float(h.p2[k]);
+    if (!h.p0.empty()) kp.gc[k] = float(h.p0[k] / (h.rmax * h.rmax));
   }
   // element blocks: tensormd.cpp:165-176
   for (int i = 0; i < h.nelt; i++) {

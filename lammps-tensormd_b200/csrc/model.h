@@ -38,6 +38,7 @@ struct HostModel {
   int nl = 0, actfn = 0, outbias = 0, resnet = 0;
   std::vector<int> sizes;                              // [nl+1]
   std::vector<std::vector<std::vector<float>>> W, Bs;  // [e][l]
+  std::vector<std::vector<double>> Wout, Bout;         // [e] output layer, FP64
 };
 
 // Parse "file.npz El1 El2 ... [interp dx] [cmax ...] [precision ...]" and the

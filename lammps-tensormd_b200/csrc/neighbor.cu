@@ -56,8 +56,8 @@ __global__ void k_nb_bin(int n, double *__restrict__ x, int *__restrict__ image,
                          int *__restrict__ cell_count, int *status,
                          const int *flag) {
   if (!*flag) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
   double px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
   if (!box.triclinic) {
     double lo[3] = {box.lo[0], box.lo[1], box.lo[2]};
@@ -102,6 +102,7 @@ __global__ void k_nb_bin(int n, double *__restrict__ x, int *__restrict__ image,
   int c = (c3[2] * bin.nb[1] + c3[1]) * bin.nb[0] + c3[0];
   cell_of[i] = c;
   atomicAdd(&cell_count[c], 1);
+  }
 }
 
 // Exclusive scan of the cell counts with one block of 1024 threads.
@@ -145,27 +146,29 @@ __global__ void k_nb_fill(int n, const int *__restrict__ cell_of,
                           int *__restrict__ cell_cursor,
                           int *__restrict__ cell_atoms, const int *flag) {
   if (!*flag) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int pos = atomicAdd(&cell_cursor[cell_of[i]], 1);
-  cell_atoms[pos] = i;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    int pos = atomicAdd(&cell_cursor[cell_of[i]], 1);
+    cell_atoms[pos] = i;
+  }
 }
 
 // Order each cell's atoms by index so the build is deterministic.
 __global__ void k_nb_cellsort(int ncell, const int *__restrict__ cell_start,
                               int *__restrict__ cell_atoms, const int *flag) {
   if (!*flag) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncell) return;
-  int s0 = cell_start[c], s1 = cell_start[c + 1];
-  for (int a = s0 + 1; a < s1; a++) {
-    int v = cell_atoms[a];
-    int b = a - 1;
-    while (b >= s0 && cell_atoms[b] > v) {
-      cell_atoms[b + 1] = cell_atoms[b];
-      b--;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+       c += gridDim.x * blockDim.x) {
+    int s0 = cell_start[c], s1 = cell_start[c + 1];
+    for (int a = s0 + 1; a < s1; a++) {
+      int v = cell_atoms[a];
+      int b = a - 1;
+      while (b >= s0 && cell_atoms[b] > v) {
+        cell_atoms[b + 1] = cell_atoms[b];
+        b--;
+      }
+      cell_atoms[b + 1] = v;
     }
-    cell_atoms[b + 1] = v;
   }
 }
 
@@ -185,10 +188,9 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
                            int *__restrict__ nraw, int *status, int *maxneed,
                            const int *flag) {
   if (!*flag) return;
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const int i = warp;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
   const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
   const int ci = cell_of[i];
   const int cx = ci % bin.nb[0], cy = (ci / bin.nb[0]) % bin.nb[1],
@@ -266,6 +268,7 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
       atomicMax(maxneed, out);
     }
   }
+  }
 }
 
 // One warp per atom: bitonic sort of the row by (block, packed key) in
@@ -277,10 +280,11 @@ __global__ void k_nb_sort(int n, int B, KParams kp, const int *__restrict__ elem
                           const int *flag) {
   if (!*flag) return;
   extern __shared__ unsigned long long sbuf[];
-  int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int i = blockIdx.x * (blockDim.x >> 5) + wib;
-  if (i >= n) return;
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int i = blockIdx.x * wpb + wib; i < n; i += gridDim.x * wpb) {
   unsigned long long *s = sbuf + (size_t)wib * capp;
+  __syncwarp();
   int cnt = min(nraw[i], cap);
   int ei = elem[i];
   const uint32_t *row = tmp + (size_t)i * cap;
@@ -319,6 +323,7 @@ __global__ void k_nb_sort(int n, int B, KParams kp, const int *__restrict__ elem
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     if (lane == 0) boff[(size_t)i * (B + 1) + b] = c;
   }
+  }
 }
 
 // Partner slot of every entry: (j -> i, -shift) found by binary search in the
@@ -328,10 +333,9 @@ __global__ void k_nb_rev(int n, int B, KParams kp, const int *__restrict__ elem,
                          const int *__restrict__ boff, int *__restrict__ rev,
                          const int *flag) {
   if (!*flag) return;
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  int i = warp;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
   int cnt = boff[(size_t)i * (B + 1) + B];
   int ei = elem[i];
   for (int t = lane; t < cnt; t += 32) {
@@ -351,13 +355,14 @@ __global__ void k_nb_rev(int n, int B, KParams kp, const int *__restrict__ elem,
     }
     rev[(size_t)i * cap + t] = found >= 0 ? (int)((size_t)j * cap + found) : -1;
   }
+  }
 }
 
 __global__ void k_nb_finish(int n, const double *__restrict__ x,
                             double *__restrict__ xbuild, int *flag) {
   if (!*flag) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
     xbuild[3 * i] = x[3 * i];
     xbuild[3 * i + 1] = x[3 * i + 1];
     xbuild[3 * i + 2] = x[3 * i + 2];
@@ -371,25 +376,27 @@ __global__ void k_set_flag(int *flag) { *flag = 1; }
 // Host driver: the whole rebuild sequence on `st`.  All launches are
 // conditional on *flag; `launches` counts them.
 void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
+  // Grids are capped at a few waves of the 148 SMs and the kernels stride
+  // over atoms, so a launch with no rebuild pending costs a few microseconds.
   const int T = 256;
-  int gn = (a.n + T - 1) / T;
-  if (gn < 1) gn = 1;
-  k_nb_zero<<<(a.bin.ncell + T - 1) / T, T, 0, st>>>(a.bin.ncell, a.cell_count, a.flag);
+  const int kMaxGrid = 148 * 8;
+  auto cap_grid = [&](long g) { return (int)(g < 1 ? 1 : (g > kMaxGrid ? kMaxGrid : g)); };
+  int gn = cap_grid((a.n + T - 1) / T);
+  int gc = cap_grid((a.bin.ncell + T - 1) / T);
+  k_nb_zero<<<gc, T, 0, st>>>(a.bin.ncell, a.cell_count, a.flag);
   k_nb_bin<<<gn, T, 0, st>>>(a.n, a.x, a.image, a.box, a.bin, a.cell_of,
                              a.cell_count, a.status, a.flag);
   k_nb_scan<<<1, 1024, 0, st>>>(a.bin.ncell, a.cell_count, a.cell_start,
                                 a.cell_cursor, a.flag);
   k_nb_fill<<<gn, T, 0, st>>>(a.n, a.cell_of, a.cell_cursor, a.cell_atoms, a.flag);
-  k_nb_cellsort<<<(a.bin.ncell + T - 1) / T, T, 0, st>>>(a.bin.ncell, a.cell_start,
-                                                         a.cell_atoms, a.flag);
-  int gw = (a.n * 32 + T - 1) / T;
-  if (gw < 1) gw = 1;
+  k_nb_cellsort<<<gc, T, 0, st>>>(a.bin.ncell, a.cell_start, a.cell_atoms, a.flag);
+  int gw = cap_grid(((long)a.n * 32 + T - 1) / T);
   k_nb_build<<<gw, T, 0, st>>>(a.n, a.x, a.box, a.bin, a.cell_of, a.cell_start,
                                a.cell_atoms, a.cutsq, a.cap, a.tmp, a.nraw,
                                a.status, a.maxneed, a.flag);
   int wpb = a.capp >= 1024 ? 1 : (a.capp >= 512 ? 2 : 4);
   size_t smem = (size_t)wpb * a.capp * sizeof(unsigned long long);
-  k_nb_sort<<<(a.n + wpb - 1) / wpb, 32 * wpb, smem, st>>>(
+  k_nb_sort<<<cap_grid((a.n + wpb - 1) / wpb), 32 * wpb, smem, st>>>(
       a.n, a.B, a.kp, a.elem, a.cap, a.capp, a.tmp, a.nraw, a.nbr, a.boff, a.flag);
   k_nb_rev<<<gw, T, 0, st>>>(a.n, a.B, a.kp, a.elem, a.cap, a.nbr, a.boff, a.rev,
                              a.flag);

@@ -13,10 +13,11 @@ namespace tmd {
 
 // Pair geometry computed by one lane and broadcast to the atom's group.
 struct PairGeo {
-  float r, ux, uy, uz;  // distance and unit vector (x_j - x_i) / r
+  float r, rlo;         // distance as an FP32 hi/lo pair (r = hi + lo)
+  float ux, uy, uz;     // unit vector (x_j - x_i) / r
   float fc, dfc;        // analytic cutoff and derivative
   float tq;             // table: offset inside the interval
-  int ti;               // table interval, or -1 when the pair is inactive
+  int ti;               // table interval (0 for analytic), -1 when inactive
 };
 
 __device__ inline double rsq_plain(double dx, double dy, double dz) {
@@ -24,27 +25,48 @@ __device__ inline double rsq_plain(double dx, double dy, double dz) {
                    __dmul_rn(dz, dz));
 }
 
-// Geometry of neighbor entry e of atom i (FP64 difference and cutoff test
-// rij2 < rc^2 && rij2 > 1e-10 as kernel.cu:1163).  g.ti = -1 if inactive.
-__device__ inline void pair_geometry(const KParams &kp, const BoxP &box,
-                                     const double *__restrict__ x, double xi,
-                                     double yi, double zi, uint32_t e,
+// Position of neighbor entry e, loaded early so the gather latency overlaps
+// the previous chunk's arithmetic.
+struct NbPos {
+  double x, y, z;
+  int code;  // shift code, -1 when the slot is empty
+};
+
+__device__ inline NbPos load_nb(const double *__restrict__ x, uint32_t e, bool valid) {
+  NbPos p;
+  if (valid) {
+    int j = e & kAtomMask;
+    p.x = __ldg(x + 3 * j);
+    p.y = __ldg(x + 3 * j + 1);
+    p.z = __ldg(x + 3 * j + 2);
+    p.code = int(e >> kAtomBits);
+  } else {
+    p.x = p.y = p.z = 0.0;
+    p.code = -1;
+  }
+  return p;
+}
+
+// Geometry of one pair (FP64 difference and cutoff test rij2 < rc^2 &&
+// rij2 > 1e-10 as kernel.cu:1163).  g.ti = -1 if inactive.
+__device__ inline void pair_geometry(const KParams &kp, const BoxP &box, double xi,
+                                     double yi, double zi, const NbPos &p,
                                      PairGeo &g) {
-  int j = e & kAtomMask;
+  g.ti = -1;
+  g.r = g.rlo = g.ux = g.uy = g.uz = g.fc = g.dfc = g.tq = 0.f;
+  if (p.code < 0) return;
   int sx, sy, sz;
-  shift_decode(int(e >> kAtomBits), sx, sy, sz);
+  shift_decode(p.code, sx, sy, sz);
   double gx, gy, gz;
-  image_of(box, __ldg(x + 3 * j), __ldg(x + 3 * j + 1), __ldg(x + 3 * j + 2), sx,
-           sy, sz, gx, gy, gz);
+  image_of(box, p.x, p.y, p.z, sx, sy, sz, gx, gy, gz);
   double dx = gx - xi, dy = gy - yi, dz = gz - zi;
   double r2 = rsq_plain(dx, dy, dz);
-  g.ti = -1;
-  g.r = g.ux = g.uy = g.uz = g.fc = g.dfc = g.tq = 0.f;
   if (!(r2 < kp.rcsq && r2 > 1e-10)) return;
   double r = sqrt(r2);
   float rf = float(r);
   float rinv = 1.0f / rf;
   g.r = rf;
+  g.rlo = float(r - double(rf));
   g.ux = float(dx) * rinv;
   g.uy = float(dy) * rinv;
   g.uz = float(dz) * rinv;
@@ -76,6 +98,7 @@ __device__ inline PairGeo shfl_geo(unsigned mask, const PairGeo &g, int src,
                                    int width) {
   PairGeo o;
   o.r = __shfl_sync(mask, g.r, src, width);
+  o.rlo = __shfl_sync(mask, g.rlo, src, width);
   o.ux = __shfl_sync(mask, g.ux, src, width);
   o.uy = __shfl_sync(mask, g.uy, src, width);
   o.uz = __shfl_sync(mask, g.uz, src, width);
@@ -86,17 +109,55 @@ __device__ inline PairGeo shfl_geo(unsigned mask, const PairGeo &g, int src,
   return o;
 }
 
-// H_k and (optionally) dH_k/dr for filters k0..k0+3.
-template <bool DERIV>
-__device__ inline void radial4(const KParams &kp, int k0, const PairGeo &g,
+// Radial kinds the kernels are specialised on.
+constexpr int kRadTable = 0;    // rational-interpolation table (FNN or tabulated)
+constexpr int kRadGauss = 1;    // analytic Gaussian SF (descriptor::method 3)
+constexpr int kRadGeneric = 2;  // analytic power-exponential / Morse / density
+
+inline int radial_kind(const KParams &kp) {
+  if (kp.radial == 1) return kRadTable;
+  return kp.method == 3 ? kRadGauss : kRadGeneric;
+}
+
+// Radial parameters of a lane's 4 filters, loaded once per kernel.
+template <int RK>
+struct Radial4 {
+  float a[RK == kRadGeneric ? 4 : 1], b[RK == kRadTable ? 1 : 4],
+      c[RK == kRadGeneric ? 4 : 1], blo[RK == kRadGauss ? 4 : 1],
+      gc[RK == kRadGauss ? 4 : 1];
+  int k0;
+};
+
+template <int RK>
+__device__ inline Radial4<RK> load_radial4(const KParams &kp, int k0) {
+  Radial4<RK> R;
+  R.k0 = k0;
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    if (RK == kRadGeneric) {
+      R.a[t] = kp.p0[k0 + t];
+      R.c[t] = kp.p2[k0 + t];
+    }
+    if (RK != kRadTable) R.b[t] = kp.p1[k0 + t];
+    if (RK == kRadGauss) {
+      R.blo[t] = kp.p1lo[k0 + t];
+      R.gc[t] = kp.gc[k0 + t];
+    }
+  }
+  return R;
+}
+
+// H_k and (optionally) dH_k/dr for the lane's filters k0..k0+3.
+template <int RK, bool DERIV>
+__device__ inline void radial4(const KParams &kp, const Radial4<RK> &R, const PairGeo &g,
                                float H[4], float dH[4]) {
-  if (kp.radial == 1) {
+  if (RK == kRadTable) {
     if (g.ti <= 0 || g.ti >= kp.tab_n - 2) {
 #pragma unroll
       for (int q = 0; q < 4; q++) { H[q] = 0.f; if (DERIV) dH[q] = 0.f; }
       return;
     }
-    const int K = kp.K;
+    const int K = kp.K, k0 = R.k0;
     const float4 *row = reinterpret_cast<const float4 *>(kp.table + (size_t)g.ti * 4 * K);
     float4 y4 = __ldg(row + (k0 >> 2));
     float4 s4 = __ldg(row + ((K + k0) >> 2));
@@ -122,27 +183,30 @@ __device__ inline void radial4(const KParams &kp, int k0, const PairGeo &g,
   const float r = g.r;
 #pragma unroll
   for (int t = 0; t < 4; t++) {
-    const int k = k0 + t;
-    const float a = kp.p0[k], b = kp.p1[k], c = kp.p2[k];
     float f, df;
-    if (kp.method == 3) {
-      float d = r - b;
-      f = expf(-a * d * d * kp.inv_rc2);
-      df = -2.f * a * kp.inv_rc2 * d * f;
-    } else if (kp.method == 0) {
-      float xr = r / a;
-      float pw = powf(xr, b);
-      f = expf(-pw);
-      df = -f * b * powf(xr, b - 1.f) / a;
-    } else if (kp.method == 1) {
-      float gdr = b * (r - c);
-      float e1 = expf(-gdr), e2 = expf(-2.f * gdr);
-      f = a * (e2 - 2.f * e1);
-      df = -a * b * 2.f * (e2 - e1);
+    if (RK == kRadGauss) {
+      // (r - omega) from the hi/lo pairs of both: no systematic rounding of
+      // the Gaussian centre
+      float d = (r - R.b[t]) + (g.rlo - R.blo[t]);
+      f = expf(-R.gc[t] * d * d);
+      df = -2.f * R.gc[t] * d * f;
     } else {
-      float z = -b * ((r - c) / c);
-      f = a * expf(z);
-      df = -f * b / c;
+      const float a = R.a[t], b = R.b[t], c = R.c[t];
+      if (kp.method == 0) {
+        float xr = r / a;
+        float pw = powf(xr, b);
+        f = expf(-pw);
+        df = -f * b * powf(xr, b - 1.f) / a;
+      } else if (kp.method == 1) {
+        float gdr = b * (r - c);
+        float e1 = expf(-gdr), e2 = expf(-2.f * gdr);
+        f = a * (e2 - 2.f * e1);
+        df = -a * b * 2.f * (e2 - e1);
+      } else {
+        float z = -b * ((r - c) / c);
+        f = a * expf(z);
+        df = -f * b / c;
+      }
     }
     H[t] = g.fc * f;
     if (DERIV) dH[t] = g.dfc * f + g.fc * df;

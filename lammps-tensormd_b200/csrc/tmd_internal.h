@@ -26,6 +26,9 @@ struct KParams {
   double rcsq;          // FP64 force cutoff test rij2 < rcsq
   float T[4 * kMaxD];   // multiplicity tensor T[m][d]
   float p0[kMaxK], p1[kMaxK], p2[kMaxK];
+  // Gaussian SF: exp(-gc (r - omega)^2) with gc = eta / rc^2 rounded once
+  // from FP64, omega = p1 + p1lo (FP32 hi/lo pair)
+  float gc[kMaxK], p1lo[kMaxK];
   int eltij[kMaxElt * kMaxElt];  // element block of (elt_i, elt_j)
   const float *table;   // [tab_n][4][K] : y, s, c1, c2
   int tab_n;

@@ -54,6 +54,9 @@ struct MlpLayer {
   int K, N;
   const float *W;  // [K][N] row-major (npz weights_e_l)
   const float *b;  // [N] or nullptr
+  // output layer only: FP64 copies, the atomic energy is formed in FP64
+  const double *Wd;
+  const double *bd;
 };
 struct MlpArgs {
   int nl, actfn, resnet, nin, maxh;
@@ -64,7 +67,7 @@ struct MlpArgs {
   const int *perm;    // atom indices grouped by element
   const float *G;     // [n][nin]
   float *dEdG;        // [n][nin]
-  float *E;           // [n]
+  double *E;          // [n] atomic energies (FP64 output layer)
   // per element, per layer (host table copied into a device param block)
   const MlpLayer *layers;  // [nelt][nl] device array
 };
@@ -107,10 +110,10 @@ void launch_gather(const GatherArgs &a, cudaStream_t st, long &launches);
 // FP32 input).  partial has >= 1024*ncomp doubles.
 void launch_reduce_f64(const double *in, int n, int ncomp, double *partial,
                        double *out, cudaStream_t st, long &launches);
-void launch_reduce_f32(const float *in, int n, double *partial, double *out,
-                       double scale, cudaStream_t st, long &launches);
-void launch_scale_copy_f32(const float *in, int n, double scale, double *out,
-                           cudaStream_t st, long &launches);
+void launch_reduce_scaled(const double *in, int n, double *partial, double *out,
+                          double scale, cudaStream_t st, long &launches);
+void launch_scale_copy(const double *in, int n, double scale, double *out,
+                       cudaStream_t st, long &launches);
 
 // Velocity Verlet halves (fix_nve.cpp:64-141).
 void launch_nve_initial(int n, double *x, double *v, const double *f,
