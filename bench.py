@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--config", default="bcc128k")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-bf16", action="store_true")
     return ap.parse_args()
 
 
@@ -295,6 +296,53 @@ def run_ours(args, rank, world, local):
         dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
     e2e_val = n * args.e2e_steps * world / float(e2e_s.item())
 
+    # tensor-core MLP forms of the same workload (same steps, same timing)
+    forms = {"fp32": {"value": value, "ms_per_step": ms_max / args.steps,
+                      "mlp_ms": prof["mlp"][1] / max(prof["mlp"][0], 1)}}
+    for prec in ([] if args.no_bf16 else ["bf16x3", "bf16"]):
+        try:
+            mb = TensorMDModel(f"{pot} {' '.join(syms)} precision {prec}", device=local)
+            sb = TensorMDSystem(mb, n, 1.0)
+            sb.set_box(box)
+            sb.set_atoms(x, t, v)
+            fp = TensorMDSystem(model, n, 1.0)
+            fp.set_box(box)
+            fp.set_atoms(x, t, v)
+            f32 = fp.compute(1, 1)
+            fb = sb.compute(1, 1)
+            ferr = float(np.sqrt(np.mean((fb["f"] - f32["f"]) ** 2)))
+            eerr = abs(fb["energy"] - f32["energy"]) / n
+            fp.close()
+            sb.nve_run(max(args.warmup, 3), dt)
+            torch.cuda.synchronize()
+            sb_stream = torch.cuda.ExternalStream(sb.stream(), device=dev)
+            b0 = torch.cuda.Event(enable_timing=True)
+            b1 = torch.cuda.Event(enable_timing=True)
+            barrier()
+            torch.cuda.synchronize()
+            b0.record(sb_stream)
+            sb.nve_run(args.steps, dt)
+            b1.record(sb_stream)
+            torch.cuda.synchronize()
+            bms = torch.tensor([b0.elapsed_time(b1)], device=dev, dtype=torch.float64)
+            if world > 1:
+                import torch.distributed as dist
+                dist.all_reduce(bms, op=dist.ReduceOp.MAX)
+            bms = float(bms.item())
+            sb.profile(True)
+            sb.profile_read(reset=True)
+            sb.nve_run(nprof, dt)
+            bprof = sb.profile_read(reset=True)
+            forms[prec] = {"value": n * args.steps * world / (bms / 1000.0),
+                           "ms_per_step": bms / args.steps,
+                           "force_rms_err_vs_fp32_eV_per_A": ferr,
+                           "energy_err_vs_fp32_eV_per_atom": eerr,
+                           "mlp_ms": bprof["mlp"][1] / max(bprof["mlp"][0], 1)}
+            sb.close()
+            mb.close()
+        except Exception as exc:  # report, do not hide
+            forms[prec] = {"error": str(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.config, samples=2)
@@ -315,6 +363,7 @@ def run_ours(args, rank, world, local):
             "roofline": roofline,
             "roofline_fp32": roofline_fp32,
             "kernel_ms": kernel_ms,
+            "forms": forms,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

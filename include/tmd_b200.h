@@ -40,12 +40,13 @@ extern "C" {
 #define TMD_PREC_FP32 0
 #define TMD_PREC_BF16 1
 #define TMD_PREC_FP8 2
+#define TMD_PREC_BF16X3 3 /* split BF16 products: FP32-class accuracy */
 
 typedef struct tmd_model tmd_model;
 typedef struct tmd_system tmd_system;
 
 /* pair_coeff arguments after "* *":  "file.npz El1 El2 ... [interp dx]
- * [cmax exact|default] [precision fp32|bf16|fp8]".
+ * [cmax exact|default] [precision fp32|bf16|bf16x3|fp8]".
  * Replaces PairTensorMD::coeff + read_potential_file + TensorMD::read_npz /
  * setup_global / setup_interpolation (pair_tensormd.cpp:214-317,376-399;
  * tensormd.cpp:109-280,438-446).  The element list maps LAMMPS atom types

@@ -14,6 +14,7 @@
 // forces back every step with ~15 device synchronisations
 // (kernel.cu:1500-1541,1760-1789); here the host synchronises only to return
 // requested results.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -66,6 +67,11 @@ struct tmd_model {
   float *d_table = nullptr;
   std::vector<float *> d_buf;   // weights and biases
   MlpLayer *d_layers = nullptr;
+  MlpTcLayer *d_tc_layers = nullptr;  // tensor-core MLP (precision bf16)
+  size_t tc_smem = 0;
+  bool tc_dz_bf16 = false;
+  int tc_np = 1;
+  int maxh = 1;
   double *d_mass = nullptr;     // per element
   int mlp_tr = 64;
   size_t mlp_smem = 0;
@@ -333,7 +339,17 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   ma.ntiles = s->ntiles; ma.tiles = s->tiles; ma.perm = s->perm; ma.G = s->G;
   ma.dEdG = s->dEdG; ma.E = s->E; ma.layers = m->d_layers;
   prof_begin(s);
-  launch_mlp_fp32(ma, s->st, s->launches);
+  if (m->d_tc_layers) {
+    MlpTcArgs ta{};
+    ta.nl = m->h.nl; ta.actfn = m->h.actfn; ta.resnet = m->h.resnet; ta.nin = m->h.nin;
+    ta.maxh = m->maxh; ta.ntiles = s->ntiles; ta.tiles = s->tiles; ta.perm = s->perm;
+    ta.G = s->G; ta.dEdG = s->dEdG; ta.E = s->E; ta.layers = m->d_tc_layers;
+    ta.status = s->status; ta.smem = m->tc_smem; ta.dz_bf16 = m->tc_dz_bf16 ? 1 : 0;
+    ta.np = m->tc_np;
+    launch_mlp_tc(ta, s->st, s->launches);
+  } else {
+    launch_mlp_fp32(ma, s->st, s->launches);
+  }
   prof_end(s, 2);
   ForceArgs fa{};
   fa.n = s->n; fa.cap = s->cap; fa.kp = m->kp; fa.box = s->box; fa.scale = scale;
@@ -442,6 +458,81 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     return fail(TMD_ERR_MODEL, "MLP too wide for the shared-memory tile");
   }
   mlp_fp32_prepare(m->mlp_tr, m->mlp_smem);
+  for (int l = 1; l < h.nl; l++) m->maxh = std::max(m->maxh, h.sizes[l]);
+  if (h.precision == TMD_PREC_BF16 || h.precision == TMD_PREC_BF16X3) {
+    const int np = h.precision == TMD_PREC_BF16X3 ? 3 : 1;
+    m->tc_np = np;
+    // tcgen05 MLP: 128-atom tiles, widths in multiples of the 64-column chunk
+    bool shape_ok = h.nin % 64 == 0 && h.nin <= 1024;
+    for (int l = 1; l < h.nl; l++) shape_ok = shape_ok && h.sizes[l] % 64 == 0 && h.sizes[l] <= 128;
+    if (!shape_ok) {
+      tmd_model_free(m);
+      return fail(TMD_ERR_MODEL, "precision bf16 needs nelt*k*m and hidden widths that are "
+                                 "multiples of 64, hidden widths <= 128");
+    }
+    size_t sm32 = mlp_tc_smem(h.nl, m->maxh, h.resnet, false, np);
+    size_t sm16 = mlp_tc_smem(h.nl, m->maxh, h.resnet, true, np);
+    const size_t kSmemMax = 227 * 1024;
+    if (sm32 <= kSmemMax / 2 || (sm32 <= kSmemMax && sm16 > kSmemMax / 2)) {
+      m->tc_smem = sm32; m->tc_dz_bf16 = false;
+    } else if (sm16 <= kSmemMax) {
+      m->tc_smem = sm16; m->tc_dz_bf16 = true;
+    } else {
+      tmd_model_free(m);
+      return fail(TMD_ERR_MODEL, "MLP too large for the tensor-core tile");
+    }
+    std::vector<MlpTcLayer> tl((size_t)h.nelt * h.nl);
+    for (int el = 0; el < h.nelt && e == cudaSuccess; el++)
+      for (int l = 0; l < h.nl && e == cudaSuccess; l++) {
+        MlpTcLayer &T = tl[(size_t)el * h.nl + l];
+        const MlpLayer &F = layers[(size_t)el * h.nl + l];
+        T.K = h.sizes[l];
+        T.N = h.sizes[l + 1];
+        T.b = F.b;
+        T.wd = F.Wd;
+        T.bd = F.bd;
+        if (l < h.nl - 1) {
+          const int K = T.K, N = T.N;
+          const size_t nf = (size_t)N * K, nbk = (size_t)K * N;
+          std::vector<uint16_t> pf(nf * np), pb(nbk * np);
+          // hi part, then (split form) lo = W - bf16(W)
+          const std::vector<float> &Wh = h.W[el][l];
+          std::vector<float> Wlo(Wh.size());
+          for (size_t q = 0; q < Wh.size(); q++) {
+            __nv_bfloat16 hb = __float2bfloat16_rn(Wh[q]);
+            Wlo[q] = Wh[q] - __bfloat162float(hb);
+          }
+          pack_core_chunks(Wh.data(), N, K, 1, N, pf.data());   // W^T
+          pack_core_chunks(Wh.data(), K, N, N, 1, pb.data());   // W
+          if (np == 3) {
+            pack_core_chunks(Wlo.data(), N, K, 1, N, pf.data() + nf);
+            pack_core_chunks(Wlo.data(), K, N, N, 1, pb.data() + nbk);
+          }
+          for (auto *vec : {&pf, &pb}) {
+            uint16_t *d = nullptr;
+            if (e == cudaSuccess) e = dalloc(&d, vec->size());
+            if (e == cudaSuccess) {
+              m->d_buf.push_back(reinterpret_cast<float *>(d));
+              e = cudaMemcpy(d, vec->data(), vec->size() * 2, cudaMemcpyHostToDevice);
+            }
+            if (vec == &pf) T.Wf = d; else T.Wb = d;
+          }
+        }
+      }
+    if (e == cudaSuccess) e = dalloc(&m->d_tc_layers, tl.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(m->d_tc_layers, tl.data(), tl.size() * sizeof(MlpTcLayer),
+                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      tmd_model_free(m);
+      return fail(TMD_ERR_CUDA, std::string("bf16 weight upload: ") + cudaGetErrorString(e));
+    }
+    mlp_tc_prepare(m->tc_smem, m->tc_dz_bf16, np);
+    m->mlp_tr = 128;
+  } else if (h.precision != TMD_PREC_FP32) {
+    tmd_model_free(m);
+    return fail(TMD_ERR_MODEL, "precision fp8 is not available in this build");
+  }
   *out = m;
   return TMD_OK;
 }
@@ -450,6 +541,7 @@ void tmd_model_free(tmd_model *m) {
   if (!m) return;
   for (float *p : m->d_buf) cudaFree(p);
   if (m->d_layers) cudaFree(m->d_layers);
+  if (m->d_tc_layers) cudaFree(m->d_tc_layers);
   if (m->d_mass) cudaFree(m->d_mass);
   delete m;
 }
@@ -677,6 +769,7 @@ int tmd_compute(tmd_system *s, int eflag, int vflag, double scale, double *energ
     if (rc) return rc;
     return tmd_compute(s, eflag, vflag, scale, energy, virial, f, eatom, vatom);
   }
+  if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
   if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
   if (st & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside a non-periodic boundary");
   if (energy) *energy = s->h_scal[0];
@@ -772,6 +865,7 @@ int tmd_nve_run(tmd_system *s, int nsteps, double dt, int thermo_every, double *
   if (st & kStatusOverflow)
     return fail(TMD_ERR_CAPACITY, "neighbor list overflow during the run (raise the "
                                   "capacity by calling set_atoms again)");
+  if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
   if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
   if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite force during the run");
   s->forces_valid = true;

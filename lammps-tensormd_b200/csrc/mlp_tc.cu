@@ -1,0 +1,403 @@
+// mlp_tc.cu -- per-element MLP forward + backward on the 5th-generation tensor
+// cores (tcgen05, sm_100a): BF16 operands, FP32 accumulation in tensor memory.
+//
+// Same semantics as the FP32 kernel (nnp.cu:9-57,149-281, nnp.cpp:246-365);
+// only the GEMM operand precision changes.  One CTA of 128 threads owns 128
+// atoms of one element (the MMA M dimension); thread t owns atom row t, which
+// is TMEM lane t, so each thread reads its row of every accumulator with
+// tcgen05.ld and runs the epilogue (bias, activation, act', residual, the
+// FP64 output layer and the gradient seed) on its own row.
+//
+//   forward  layer l:  D[128 x N_l] = X_l[128 x K_l] . W_l           (TMEM)
+//   backward layer l:  D[128 x K_l] = (g_l * act'_l)[128 x N_l] . W_l^T
+//
+// Operands live in shared memory in the canonical K-major no-swizzle layout
+// of tcgen05 (8-row x 16-byte core matrices): A = activations / gradients
+// written by the epilogue, or the G tile staged from global memory; B =
+// weights pre-packed on the host in 64-column chunks that are copied to
+// shared memory as contiguous blocks.  One thread issues the MMAs and a
+// tcgen05.commit arrives on an mbarrier; every wait is bounded, and a timeout
+// sets an error bit, releases the tensor memory and leaves the kernel.
+#include <cuda_bf16.h>
+
+#include <cstring>
+
+#include "tmd_kernels.h"
+
+namespace tmd {
+
+namespace {
+
+constexpr int TM = 128;      // atoms per tile (MMA M)
+constexpr int KCH = 64;      // reduction chunk (columns) staged at a time
+constexpr int EPC = 8;       // BF16 elements per 16-byte core-matrix row
+constexpr int KSTEP = 16;    // MMA K of kind::f16
+constexpr int TMEM_COLS = 128;
+constexpr long long kWaitCycles = 4000000000LL;  // about 2 s
+
+__device__ inline uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// K-major, no-swizzle shared-memory matrix descriptor (sm_100 format:
+// start >> 4 [0,14), LBO >> 4 [16,30), SBO >> 4 [32,46), version 1 [46,48),
+// layout SWIZZLE_NONE [61,64) = 0).  LBO = distance between the two 16-byte
+// core columns of one MMA K step, SBO = distance between 8-row groups.
+__device__ inline uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// Instruction descriptor of kind::f16: D = FP32, A = B = BF16, K-major both,
+// N >> 3 at [17,23), M >> 4 at [24,29).
+__device__ inline uint32_t idesc_bf16(int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(TM >> 4) << 24);
+}
+
+__device__ inline void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t id,
+                                uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(id), "r"(acc));
+}
+
+__device__ inline void commit(uint64_t *mbar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(mbar)));
+}
+
+// Bounded wait for the mbarrier phase; false on timeout.
+__device__ inline bool mbar_wait(uint64_t *mbar, uint32_t phase) {
+  const uint32_t a = smem_u32(mbar);
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+}
+
+__device__ inline void tmem_ld32(uint32_t taddr, float v[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ inline float act_fwd(int actfn, float z, float &d) {
+  switch (actfn) {
+    case 0:
+      d = z > 0.f ? 1.f : 0.f;
+      return z > 0.f ? z : 0.f;
+    case 1: {
+      float ex = expf(z);
+      d = 1.f / (1.f + 1.f / ex);
+      return z < 13.942385152878742f ? log1pf(ex) : z;
+    }
+    case 2: {
+      float y = tanhf(z);
+      d = 1.f - y * y;
+      return y;
+    }
+    default: {
+      float q = sqrtf(z * z + 4.f);
+      float y = z >= 0.f ? 0.5f * (z + q) : 2.f / (q - z);
+      d = y / q;
+      return y;
+    }
+  }
+}
+
+// element offset of (r, k) in a K-major core-matrix operand with kfull columns
+__device__ inline int core_off(int r, int k, int kfull) {
+  return ((r >> 3) * (kfull / EPC) + k / EPC) * (8 * EPC) + (r & 7) * EPC + (k % EPC);
+}
+
+template <typename DZ>
+__device__ inline DZ dz_store(float v);
+template <>
+__device__ inline float dz_store<float>(float v) { return v; }
+template <>
+__device__ inline __nv_bfloat16 dz_store<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+}  // namespace
+
+// Store v as a BF16 operand: with NP = 3 also the residual v - hi in the
+// second buffer (lo), so a product of two split operands is
+// hi*hi' + hi*lo' + lo*hi' (FP32-class accuracy on BF16 tensor cores).
+template <int NP>
+__device__ inline void put_op(__nv_bfloat16 *buf, size_t lo_stride, int off, float v) {
+  __nv_bfloat16 h = __float2bfloat16_rn(v);
+  buf[off] = h;
+  if (NP == 3) buf[lo_stride + off] = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+// DZ: storage type of act'(z) per hidden layer (FP32 when it fits in shared
+// memory, BF16 otherwise).  NP: 1 = BF16 products, 3 = split BF16 (hi/lo).
+template <typename DZ, int NP>
+__global__ void __launch_bounds__(TM)
+k_mlp_tc(MlpTcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base_s;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tile = blockIdx.x;
+  const int elt = a.tiles[3 * tile], start = a.tiles[3 * tile + 1], count = a.tiles[3 * tile + 2];
+  const int row_atom = tid < count ? a.perm[start + tid] : -1;
+  const MlpTcLayer *Ls = a.layers + (size_t)elt * a.nl;
+  const int L = a.nl;
+  const int maxh = a.maxh;  // multiple of 64
+  const int nin = a.nin;    // multiple of 64
+  typedef __nv_bfloat16 T;
+  // operand buffers; with NP = 3 each holds hi, then lo at +lo stride
+  constexpr int NB = NP == 3 ? 2 : 1;
+  T *opA = reinterpret_cast<T *>(smraw);                 // [NB][TM][KCH] staged G chunk
+  T *opB = opA + NB * TM * KCH;                          // [NB][128][KCH] weight chunk
+  T *actb = opB + NB * 128 * KCH;                        // [NB][TM][maxh] activations / gz
+  const size_t act_lo = (size_t)TM * maxh;
+  DZ *dzb = reinterpret_cast<DZ *>(actb + NB * TM * maxh);  // act' per hidden layer
+  float *gres = reinterpret_cast<float *>(dzb + (size_t)(L - 1) * TM * maxh);  // resnet only
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+  uint32_t phase = 0;
+  bool ok = true;
+
+  // D[TM x nout] (TMEM columns 0..nout-1) = A[TM x kred] . B^T with B rows
+  // n0..n0+nout-1 of a packed weight block of brows rows.
+  // a_src: 0 = stage the G tile from global memory, 1 = actb (whole buffer).
+  // bsize: elements of one packed weight block (the lo block follows it)
+  auto gemm = [&](int a_src, int kred, const T *Bpk, int brows, int n0, int nout) {
+    const size_t bsize = (size_t)brows * kred;
+    const int nch = kred / KCH;
+    for (int c = 0; c < nch && ok; c++) {
+      if (a_src == 0) {
+        for (int idx = tid; idx < TM * KCH; idx += TM) {
+          int r = idx / KCH, k = idx % KCH;
+          int at = r < count ? a.perm[start + r] : -1;
+          float v = at >= 0 ? __ldg(a.G + (size_t)at * nin + c * KCH + k) : 0.f;
+          put_op<NP>(opA, (size_t)TM * KCH, core_off(r, k, KCH), v);
+        }
+      }
+      for (int h = 0; h < NB; h++) {
+        // packed weights: hi block, then (NP = 3) lo block of the same shape
+        const T *blk = Bpk + (size_t)h * bsize;
+        const uint4 *src = reinterpret_cast<const uint4 *>(blk + ((size_t)c * brows + n0) * KCH);
+        uint4 *dst = reinterpret_cast<uint4 *>(opB + (size_t)h * 128 * KCH);
+        const int nvec = nout * KCH * (int)sizeof(T) / 16;
+        for (int i = tid; i < nvec; i += TM) dst[i] = __ldg(src + i);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t id = idesc_bf16(nout);
+#pragma unroll
+        for (int s = 0; s < KCH / KSTEP; s++) {
+          uint64_t da;
+          if (a_src == 0)
+            da = sdesc(smem_u32(opA) + (uint32_t)(s * KSTEP / EPC) * 128u, 128u,
+                       (uint32_t)(KCH / EPC) * 128u);
+          else
+            da = sdesc(smem_u32(actb) + (uint32_t)((c * KCH + s * KSTEP) / EPC) * 128u, 128u,
+                       (uint32_t)(maxh / EPC) * 128u);
+          uint64_t db = sdesc(smem_u32(opB) + (uint32_t)(s * KSTEP / EPC) * 128u, 128u,
+                              (uint32_t)(KCH / EPC) * 128u);
+          mma_bf16(tmem, da, db, id, (c > 0 || s > 0) ? 1u : 0u);
+          if (NP == 3) {
+            // start-address offsets of the lo halves (descriptor units of 16 B)
+            const uint64_t a_lo = (uint64_t)(((a_src == 0 ? (size_t)TM * KCH : act_lo) * 2) >> 4);
+            const uint64_t b_lo = (uint64_t)(((size_t)128 * KCH * 2) >> 4);
+            mma_bf16(tmem, da, db + b_lo, id, 1u);  // hi * lo'
+            mma_bf16(tmem, da + a_lo, db, id, 1u);  // lo * hi'
+          }
+        }
+        commit(&mbar);
+      }
+      // every thread waits (bounded); the outcome is made block-uniform so all
+      // threads take the same path through the remaining barriers
+      const bool done = mbar_wait(&mbar, phase);
+      ok = __syncthreads_and(done ? 1 : 0) != 0;
+      phase ^= 1u;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+    }
+  };
+
+  // ---------------- forward ----------------
+  double E = 0.0;
+  for (int l = 0; l < L - 1 && ok; l++) {
+    const MlpTcLayer ly = Ls[l];
+    gemm(l == 0 ? 0 : 1, ly.K, reinterpret_cast<const T *>(ly.Wf), ly.N, 0, ly.N);
+    if (!ok) break;
+    const bool res = a.resnet && l > 0 && ly.K == ly.N;
+    const bool last = (l == L - 2);
+    const double *wout = Ls[L - 1].wd;
+    DZ *dz = dzb + (size_t)l * TM * maxh;
+    for (int c0 = 0; c0 < ly.N; c0 += 32) {
+      float v[32];
+      tmem_ld32(trow + c0, v);
+#pragma unroll 4
+      for (int j = 0; j < 32; j++) {
+        const int c = c0 + j;
+        float z = v[j] + __ldg(ly.b + c);
+        float d;
+        float y = act_fwd(a.actfn, z, d);
+        if (res) y += gres[(size_t)tid * maxh + c];  // layer input, FP32
+        if (!last) {
+          dz[(size_t)tid * maxh + c] = dz_store<DZ>(d);
+          put_op<NP>(actb, act_lo, core_off(tid, c, maxh), y);
+          if (a.resnet) gres[(size_t)tid * maxh + c] = y;
+        } else {
+          // output layer in FP64; gradient seed g = w_out, gz = g * act'
+          const double w = __ldg(wout + c);
+          E = fma((double)y, w, E);
+          put_op<NP>(actb, act_lo, core_off(tid, c, maxh), (float)w * d);
+          if (a.resnet) gres[(size_t)tid * maxh + c] = (float)w;
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+  }
+  if (ok && row_atom >= 0) a.E[row_atom] = E + (Ls[L - 1].bd ? *Ls[L - 1].bd : 0.0);
+
+  // ---------------- backward ----------------
+  for (int l = L - 2; l >= 0 && ok; l--) {
+    const MlpTcLayer ly = Ls[l];
+    if (l == 0) {
+      for (int n0 = 0; n0 < ly.K && ok; n0 += 128) {
+        const int nout = min(128, ly.K - n0);
+        gemm(1, ly.N, reinterpret_cast<const T *>(ly.Wb), ly.K, n0, nout);
+        if (!ok) break;
+        for (int c0 = 0; c0 < nout; c0 += 32) {
+          float v[32];
+          tmem_ld32(trow + c0, v);
+          if (row_atom >= 0) {
+            float4 *dst = reinterpret_cast<float4 *>(a.dEdG + (size_t)row_atom * nin + n0 + c0);
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+              dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+      }
+    } else {
+      gemm(1, ly.N, reinterpret_cast<const T *>(ly.Wb), ly.K, 0, ly.K);
+      if (!ok) break;
+      const bool res = a.resnet && ly.K == ly.N;
+      const DZ *dzn = dzb + (size_t)(l - 1) * TM * maxh;
+      for (int c0 = 0; c0 < ly.K; c0 += 32) {
+        float v[32];
+        tmem_ld32(trow + c0, v);
+#pragma unroll 4
+        for (int j = 0; j < 32; j++) {
+          const int c = c0 + j;
+          float g = v[j] + (res ? gres[(size_t)tid * maxh + c] : 0.f);
+          if (a.resnet) gres[(size_t)tid * maxh + c] = g;
+          put_op<NP>(actb, act_lo, core_off(tid, c, maxh),
+                     g * (float)dzn[(size_t)tid * maxh + c]);
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncthreads();
+    }
+  }
+  if (!ok && tid == 0) atomicOr(a.status, kStatusTimeout);
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS));
+}
+
+void pack_core_chunks(const float *src, int rows, int cols, long ld_r, long ld_k,
+                      uint16_t *dst) {
+  // chunk c holds columns [64c, 64c + 64) of every row; inside a chunk the
+  // element (r, k) sits at ((r/8) * 8 + k/8) * 64 + (r%8) * 8 + k%8
+  const int nch = (cols + KCH - 1) / KCH;
+  for (int c = 0; c < nch; c++)
+    for (int r = 0; r < rows; r++)
+      for (int kk = 0; kk < KCH; kk++) {
+        int k = c * KCH + kk;
+        float v = k < cols ? src[(long)r * ld_r + (long)k * ld_k] : 0.f;
+        __nv_bfloat16 h = __float2bfloat16_rn(v);
+        uint16_t bits;
+        memcpy(&bits, &h, 2);
+        size_t off = (size_t)c * rows * KCH +
+                     (size_t)(((r >> 3) * (KCH / EPC) + kk / EPC) * (8 * EPC) + (r & 7) * EPC + kk % EPC);
+        dst[off] = bits;
+      }
+}
+
+size_t mlp_tc_smem(int nl, int maxh, int resnet, bool dz_bf16, int np) {
+  const size_t nb = np == 3 ? 2 : 1;
+  size_t b = nb * ((size_t)TM * KCH * 2 + (size_t)128 * KCH * 2);  // opA + opB
+  b += nb * (size_t)TM * maxh * 2;                                 // actb
+  b += (size_t)(nl - 1) * TM * maxh * (dz_bf16 ? 2 : 4);           // act'
+  if (resnet) b += (size_t)TM * maxh * 4;                          // residual rows
+  return b;
+}
+
+void mlp_tc_prepare(size_t smem, bool dz_bf16, int np) {
+  const int s = (int)smem;
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (np == 3) {
+    if (dz_bf16) cudaFuncSetAttribute(k_mlp_tc<__nv_bfloat16, 3>, at, s);
+    else cudaFuncSetAttribute(k_mlp_tc<float, 3>, at, s);
+  } else {
+    if (dz_bf16) cudaFuncSetAttribute(k_mlp_tc<__nv_bfloat16, 1>, at, s);
+    else cudaFuncSetAttribute(k_mlp_tc<float, 1>, at, s);
+  }
+}
+
+void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches) {
+  if (a.ntiles <= 0) return;
+  if (a.np == 3) {
+    if (a.dz_bf16) k_mlp_tc<__nv_bfloat16, 3><<<a.ntiles, TM, a.smem, st>>>(a);
+    else k_mlp_tc<float, 3><<<a.ntiles, TM, a.smem, st>>>(a);
+  } else {
+    if (a.dz_bf16) k_mlp_tc<__nv_bfloat16, 1><<<a.ntiles, TM, a.smem, st>>>(a);
+    else k_mlp_tc<float, 1><<<a.ntiles, TM, a.smem, st>>>(a);
+  }
+  launches += 1;
+}
+
+}  // namespace tmd

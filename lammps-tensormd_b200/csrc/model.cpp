@@ -224,7 +224,8 @@ HostModel parse_model(const std::string &coeff_args) {
       if (c == "fp32") h.precision = 0;
       else if (c == "bf16") h.precision = 1;
       else if (c == "fp8") h.precision = 2;
-      else bad("precision must be fp32, bf16 or fp8");
+      else if (c == "bf16x3") h.precision = 3;
+      else bad("precision must be fp32, bf16, bf16x3 or fp8");
       read_elt = false;
       i += 2;
     } else if (read_elt) {

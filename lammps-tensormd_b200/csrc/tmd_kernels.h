@@ -10,6 +10,7 @@ constexpr int kStatusOverflow = 1;   // neighbor row longer than cap
 constexpr int kStatusShift = 2;      // image shift beyond +-3 cells
 constexpr int kStatusOutside = 4;    // atom outside a non-periodic boundary
 constexpr int kStatusNonfinite = 8;  // NaN/Inf energy or force
+constexpr int kStatusTimeout = 16;   // a bounded device wait gave up
 
 struct NbArgs {
   int n, B, cap, capp;
@@ -74,6 +75,38 @@ struct MlpArgs {
 void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches);
 size_t mlp_fp32_smem(int nl, const int *sizes, int tr);
 void mlp_fp32_prepare(int tr, size_t smem);
+
+// Tensor-core (tcgen05) MLP, BF16 operands.  Weights are packed on the host
+// in 64-column chunks of the K-major core-matrix layout (pack_core_chunks).
+struct MlpTcLayer {
+  int K, N;
+  const void *Wf;    // forward B = W^T: N rows x K cols (bf16, packed; the lo
+                     // block of the split form follows the hi block)
+  const void *Wb;    // backward B = W: K rows x N cols (bf16, packed, same)
+  const float *b;    // [N] bias (hidden layers)
+  const double *wd;  // output layer weights (FP64), last layer only
+  const double *bd;  // output bias (FP64) or nullptr, last layer only
+};
+struct MlpTcArgs {
+  int nl, actfn, resnet, nin, maxh, ntiles;
+  const int *tiles, *perm;
+  const float *G;
+  float *dEdG;
+  double *E;
+  const MlpTcLayer *layers;  // [nelt][nl] device array
+  int *status;
+  size_t smem;
+  int dz_bf16;
+  int np;  // 1: BF16 products; 3: split BF16 (hi*hi + hi*lo + lo*hi)
+};
+void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches);
+size_t mlp_tc_smem(int nl, int maxh, int resnet, bool dz_bf16, int np);
+void mlp_tc_prepare(size_t smem, bool dz_bf16, int np);
+
+// Host: pack a rows x cols matrix (element (r, k) = src[r * ld_r + k * ld_k])
+// into 64-column chunks of 8x8 BF16 core matrices, K-major.
+void pack_core_chunks(const float *src, int rows, int cols, long ld_r, long ld_k,
+                      uint16_t *dst);
 
 // Force: per-pair dE_i/dx_j into pdf, per-atom virial partials.
 struct ForceArgs {
