@@ -143,15 +143,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the force kernel from the committed ncu summary."""
-    p = ROOT / "profiles" / "force_traffic.json"
-    if p.exists():
-        try:
-            d = json.loads(p.read_text())
-            return d
-        except Exception:
-            return None
+def ncu_traffic(config):
+    """Per-launch DRAM bytes (read + write) of the force kernel, from the
+    committed ncu summary of the same workload (profiles/), or None."""
+    p = ROOT / "profiles" / f"force_descriptor_{config}.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if "traffic_bytes_per_launch:" in line:
+            try:
+                return int(line.split("traffic_bytes_per_launch:")[1].split()[0])
+            except ValueError:
+                return None
     return None
 
 
@@ -235,10 +238,7 @@ def run_ours(args, rank, world, local):
     clocks = clk.summary()
     sm_mhz = clocks["sm_mhz"] or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
-    tr = ncu_traffic()
-    traffic = None
-    if tr and tr.get("workload") == args.config:
-        traffic = tr.get("bytes_per_launch")
+    traffic = ncu_traffic(args.config)
     ach_gbs = abytes / (force_ms / 1000.0) / 1e9
     ach_tf = flops / (force_ms / 1000.0) / 1e12
     roofline = {"kernel": "k_force", "bound": "hbm", "achieved": ach_gbs,

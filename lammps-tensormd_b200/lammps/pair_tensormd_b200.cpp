@@ -1,0 +1,204 @@
+/* pair_tensormd_b200.cpp -- LAMMPS pair style "tensormd/b200" over the C ABI
+ * of libtmd_b200.so.
+ *
+ * Mirrors PairTensorMD (src/ML-TENSORMD/pair_tensormd.cpp): settings() takes
+ * no arguments (:205-208); coeff() takes "* * file.npz El1 ... [keywords]"
+ * (:214-317) and sets the per-type masses from the potential file (:303-312);
+ * init_style() requires newton_pair on (:323-330); init_one() returns the
+ * cutoff (:336-341); extract("scale") exposes the fix-adapt scale (:415-425).
+ * compute() hands local positions and the box to the device, which builds its
+ * own periodic neighbor list, and adds forces, energy and the virial (no
+ * fdotr: the virial comes from the pair separations on the device).
+ */
+#include "pair_tensormd_b200.h"
+
+#include "atom.h"
+#include "comm.h"
+#include "domain.h"
+#include "error.h"
+#include "force.h"
+#include "memory.h"
+#include "neighbor.h"
+
+#include "tmd_b200.h"
+
+#include <cstring>
+#include <string>
+
+using namespace LAMMPS_NS;
+
+PairTensorMDB200::PairTensorMDB200(LAMMPS *lmp) : Pair(lmp)
+{
+  single_enable = 0;
+  restartinfo = 0;
+  one_coeff = 1;
+  manybody_flag = 1;
+  no_virial_fdotr_compute = 1;
+  centroidstressflag = CENTROID_NOTAVAIL;
+  model = nullptr;
+  sys = nullptr;
+  cutmax = 0.0;
+  skin = 1.0;
+  scale = nullptr;
+  natoms_cap = 0;
+  last_nlocal = -1;
+  last_box_stamp = -1;
+}
+
+PairTensorMDB200::~PairTensorMDB200()
+{
+  if (sys) tmd_system_free(sys);
+  if (model) tmd_model_free(model);
+  if (allocated) {
+    memory->destroy(setflag);
+    memory->destroy(cutsq);
+    memory->destroy(scale);
+  }
+}
+
+void PairTensorMDB200::check(int rc, const char *what)
+{
+  if (rc == TMD_OK) return;
+  char buf[512];
+  tmd_last_error(buf, sizeof(buf));
+  error->one(FLERR, std::string("pair tensormd/b200: ") + what + ": " + buf);
+}
+
+void PairTensorMDB200::allocate()
+{
+  allocated = 1;
+  int n = atom->ntypes;
+  memory->create(setflag, n + 1, n + 1, "pair:setflag");
+  memory->create(cutsq, n + 1, n + 1, "pair:cutsq");
+  memory->create(scale, n + 1, n + 1, "pair:scale");
+  map = new int[n + 1];
+  for (int i = 0; i <= n; i++) map[i] = -1;
+}
+
+void PairTensorMDB200::settings(int narg, char ** /*arg*/)
+{
+  if (narg != 0) error->all(FLERR, "Illegal pair_style command");
+}
+
+void PairTensorMDB200::coeff(int narg, char **arg)
+{
+  if (!allocated) allocate();
+  if (narg < 4) error->all(FLERR, "Incorrect args for pair coefficients");
+  if (strcmp(arg[0], "*") != 0 || strcmp(arg[1], "*") != 0)
+    error->all(FLERR, "Incorrect args for pair coefficients");
+  std::string args;
+  for (int i = 2; i < narg; i++) {
+    if (i > 2) args += " ";
+    args += arg[i];
+  }
+  if (sys) { tmd_system_free(sys); sys = nullptr; }
+  if (model) { tmd_model_free(model); model = nullptr; }
+  check(tmd_model_load(args.c_str(), 0, &model), "pair_coeff");
+  int ntypes_mapped = 0;
+  check(tmd_model_info(model, &cutmax, nullptr, &ntypes_mapped, nullptr, nullptr, nullptr),
+        "model info");
+  int n = atom->ntypes;
+  if (ntypes_mapped != n)
+    error->all(FLERR, "Number of elements in pair_coeff must equal the number of atom types");
+  std::vector<int> tmap(n + 1);
+  std::vector<double> tmass(n + 1);
+  check(tmd_model_type_map(model, tmap.data(), tmass.data()), "type map");
+  int count = 0;
+  for (int i = 1; i <= n; i++) {
+    map[i] = tmap[i];
+    for (int j = i; j <= n; j++) {
+      setflag[i][j] = (tmap[i] >= 0 && tmap[j] >= 0) ? 1 : 0;
+      scale[i][j] = 1.0;
+      if (setflag[i][j]) count++;
+    }
+    if (tmap[i] >= 0) atom->set_mass(FLERR, i, tmass[i]);
+  }
+  if (count == 0) error->all(FLERR, "Incorrect args for pair coefficients");
+  last_nlocal = -1;
+  last_box_stamp = -1;
+}
+
+void PairTensorMDB200::init_style()
+{
+  if (force->newton_pair == 0) error->all(FLERR, "Pair style tensormd/b200 requires newton pair on");
+  if (comm->nprocs > 1)
+    error->all(FLERR, "Pair style tensormd/b200 runs on one MPI rank (periodic images on the GPU)");
+  skin = neighbor->skin;
+}
+
+double PairTensorMDB200::init_one(int i, int j)
+{
+  if (setflag[i][j] == 0) scale[i][j] = 1.0;
+  scale[j][i] = scale[i][j];
+  return cutmax;
+}
+
+void PairTensorMDB200::compute(int eflag, int vflag)
+{
+  ev_init(eflag, vflag);
+  const int n = atom->nlocal;
+  if (!sys || n > natoms_cap) {
+    if (sys) tmd_system_free(sys);
+    natoms_cap = n + n / 5 + 64;
+    check(tmd_system_create(model, natoms_cap, skin, &sys), "system");
+    last_nlocal = -1;
+    last_box_stamp = -1;
+  }
+  double box[9] = {domain->boxlo[0], domain->boxlo[1], domain->boxlo[2],
+                   domain->xprd,     domain->yprd,     domain->zprd,
+                   domain->xy,       domain->xz,       domain->yz};
+  int pbc[3] = {domain->xperiodic, domain->yperiodic, domain->zperiodic};
+  bool box_changed = last_box_stamp < 0;
+  for (int c = 0; c < 9 && !box_changed; c++) box_changed = box[c] != last_box[c];
+  if (box_changed) {
+    check(tmd_system_set_box(sys, box, pbc), "box");
+    memcpy(last_box, box, sizeof(box));
+    last_box_stamp = 1;
+    last_nlocal = -1;
+  }
+  xbuf.assign(atom->x[0], atom->x[0] + 3 * (size_t)n);
+  // atoms migrate and LAMMPS re-sorts them on reneighboring steps: re-upload
+  // types and order then, positions only otherwise
+  if (n != last_nlocal || neighbor->ago == 0) {
+    tbuf.assign(atom->type, atom->type + n);
+    check(tmd_system_set_atoms(sys, n, xbuf.data(), tbuf.data(), nullptr), "atoms");
+    last_nlocal = n;
+  } else {
+    check(tmd_system_set_positions(sys, xbuf.data()), "positions");
+  }
+  fbuf.resize(3 * (size_t)n);
+  double e = 0.0, v6[6] = {0, 0, 0, 0, 0, 0};
+  double *ea = nullptr, *va = nullptr;
+  if (eflag_atom) { ebuf.resize(n); ea = ebuf.data(); }
+  if (vflag_atom) { vbuf.resize(6 * (size_t)n); va = vbuf.data(); }
+  check(tmd_compute(sys, eflag, vflag, scale[1][1], &e, v6, fbuf.data(), ea, va), "compute");
+  double **f = atom->f;
+  for (int i = 0; i < n; i++) {
+    f[i][0] += fbuf[3 * i];
+    f[i][1] += fbuf[3 * i + 1];
+    f[i][2] += fbuf[3 * i + 2];
+  }
+  if (eflag_global) eng_vdwl += e;
+  if (vflag_global)
+    for (int c = 0; c < 6; c++) virial[c] += v6[c];
+  if (eflag_atom)
+    for (int i = 0; i < n; i++) eatom[i] += ebuf[i];
+  if (vflag_atom)
+    for (int i = 0; i < n; i++)
+      for (int c = 0; c < 6; c++) vatom[i][c] += vbuf[6 * i + c];
+}
+
+void *PairTensorMDB200::extract(const char *str, int &dim)
+{
+  if (strcmp(str, "scale") == 0) {
+    dim = 2;
+    return (void *) scale;
+  }
+  return nullptr;
+}
+
+double PairTensorMDB200::memory_usage()
+{
+  return (double) (xbuf.capacity() + fbuf.capacity() + ebuf.capacity() + vbuf.capacity()) *
+      sizeof(double);
+}
