@@ -144,6 +144,36 @@ int tmd_profile_read(tmd_system *sys, long *launches, double *ms, int reset);
 /* Copy the message of the last failed call on this thread into buf. */
 int tmd_last_error(char *buf, int len);
 
+/* Full neighbor list without allocating any memory.  This entry point has no
+ * counterpart in the reference.  It is meant for callers that must not call
+ * cudaMalloc: code that records into a CUDA graph (allocation is not allowed
+ * while a stream is being captured), and hosts that give a library no device
+ * memory of its own because they manage every byte through their own pool.
+ *
+ * x_dev[n*3]: device positions, already inside the periodic cell (no
+ * wrapping is done; atoms outside a periodic cell give TMD_ERR_ARG).
+ * box/pbc as tmd_system_set_box; cut: list cutoff (<= any cell width * 3).
+ * Outputs, device memory owned by the caller: counts_dev[n] and
+ * rows_dev[n*cap]; row i holds counts_dev[i] entries (shift_code << 23 | j)
+ * with shift_code = (sx+3) + 7*(sy+3) + 49*(sz+3), in no particular order.
+ * A row longer than cap gives TMD_ERR_CAPACITY (rows are then incomplete).
+ * stream: cudaStream_t or NULL for the default stream; the call returns after
+ * the stream has finished the work.
+ *
+ * Cell binning uses one scratch array of 4 MiB in the library's static device
+ * memory, which every GPU that loads the library keeps until the process
+ * exits.  Limits: n <= TMD_NOALLOC_MAX_ATOMS and at most TMD_NOALLOC_MAX_CELLS
+ * cells (larger requests give TMD_ERR_CAPACITY).  All calls share that one
+ * array: calls whose work overlaps on the GPU race and corrupt each other, so
+ * serialise them.  The first call on each device looks the array up
+ * (cudaGetSymbolAddress); make that first call before any stream capture. */
+#define TMD_NOALLOC_MAX_ATOMS 262144
+#define TMD_NOALLOC_MAX_CELLS 131072
+int tmd_neighbor_list_noalloc(const double *x_dev, int n, const double box[9],
+                              const int pbc[3], double cut, int cap,
+                              int *counts_dev, unsigned int *rows_dev,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif

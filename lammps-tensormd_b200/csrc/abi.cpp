@@ -124,6 +124,11 @@ struct tmd_system {
   long step_launches = 0;
 };
 
+namespace tmd {
+// error message of calls implemented in other translation units
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace tmd
+
 namespace {
 void drop_graph(tmd_system *s) {
   if (s->step_exec) cudaGraphExecDestroy(s->step_exec);

@@ -39,6 +39,8 @@ SIGNATURES = [
     ("tmd_profile_enable", _c_int, [_vp, _c_int]),
     ("tmd_profile_read", _c_int, [_vp, _pl, _pd, _c_int]),
     ("tmd_last_error", _c_int, [ctypes.c_char_p, _c_int]),
+    ("tmd_neighbor_list_noalloc", _c_int, [_vp, _c_int, _pd, _pi, _c_double, _c_int, _vp,
+                                           _vp, _vp]),
 ]
 
 
