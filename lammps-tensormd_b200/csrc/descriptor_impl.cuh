@@ -8,11 +8,12 @@
 // The reference materialises R, M and H per (atom, block, padded slot) and
 // runs a batched GEMM; here a group of TPA = K/4 lanes owns one atom and each
 // lane accumulates 4 filters x D monomials in registers with packed FP32x2
-// FMAs (sm_100 FFMA2).  Each lane computes the FP64 geometry of one pair of a
-// chunk of TPA neighbors and publishes it in shared memory; the group then
-// reads each pair with vector loads (broadcast).  Neighbor entries are fetched
-// two chunks ahead and neighbor positions one chunk ahead, so the gather
-// latency overlaps the arithmetic.  Nothing per pair goes to global memory.
+// FMAs (sm_100 FFMA2).  Each lane computes the FP64 geometry of one entry of
+// a chunk of TPA neighbors; the active pairs (r < rc) are queued in shared
+// memory (PairRing) and the group reads each pair with vector loads
+// (broadcast).  Neighbor entries are fetched two chunks ahead and neighbor
+// positions one chunk ahead, so the gather latency overlaps the arithmetic.
+// Nothing per pair goes to global memory.
 //
 // Output layout: P[n][B][K][D] (kept for the force kernel), G[n][B*K*M] (the
 // MLP input rows, m fastest, as TensorMD::get_G).
@@ -29,13 +30,13 @@ constexpr int kPairThreads = 128;  // block size of the pair kernels
 struct GeoSlot {
   float4 a;  // r, rlo, ux, uy
   float4 b;  // uz, fc, dfc, tq
-  float4 c;  // ti (bits), unused
+  float4 c;  // ti (bits), neighbor slot t (bits), unused
 };
 
-__device__ inline void geo_store(GeoSlot *s, const PairGeo &g) {
+__device__ inline void geo_store(GeoSlot *s, const PairGeo &g, int t) {
   s->a = make_float4(g.r, g.rlo, g.ux, g.uy);
   s->b = make_float4(g.uz, g.fc, g.dfc, g.tq);
-  s->c = make_float4(__int_as_float(g.ti), 0.f, 0.f, 0.f);
+  s->c = make_float4(__int_as_float(g.ti), __int_as_float(t), 0.f, 0.f);
 }
 
 __device__ inline PairGeo geo_load(const GeoSlot *s) {
@@ -57,6 +58,66 @@ __device__ inline void moments2(float x, float y, float z, float2 M2[D2]) {
   for (int p = 0; p < D2; p++) M2[p] = make_float2(M[2 * p], M[2 * p + 1]);
 }
 
+// The active pairs of one atom's row, TPA at a time.  About 40% of a row
+// lies in the skin shell (rc < r < rc + skin) and rows are sorted by image
+// and index, not by distance, so active pairs are scattered along the row.
+// Each group therefore keeps a ring of 2*TPA geometry slots in shared memory:
+// feed() computes the geometry of the next TPA entries (one per lane) and
+// appends the active ones in row order (ballot + prefix count) until the ring
+// holds TPA pairs or the row ends.  The group then runs its per-pair work on
+// exactly TPA pairs, and a warp's groups stay converged on full chunks
+// instead of idling on other groups' inactive entries.
+template <int TPA>
+struct PairRing {
+  static constexpr int kSlots = 2 * TPA;
+  static constexpr unsigned kBits = TPA == 32 ? 0xffffffffu : ((1u << TPA) - 1u);
+  GeoSlot *ring;        // this group's 2*TPA slots
+  unsigned gmask;       // this group's lanes in the warp
+  int gshift, sub;      // first lane of the group, lane within the group
+  int head, qn;         // ring head and number of queued pairs
+  int t, s1;            // next row entry to fetch, end of the block's entries
+  NbPos pnext;          // positions of entries t..t+TPA-1 (one per lane)
+  uint32_t enext;       // packed entries t+TPA..t+2TPA-1
+
+  __device__ inline void begin(const double *__restrict__ x,
+                               const uint32_t *__restrict__ row, int s0, int s1_) {
+    head = 0; qn = 0; t = s0; s1 = s1_;
+    pnext = load_nb(x, s0 + sub < s1 ? row[s0 + sub] : 0u, s0 + sub < s1);
+    enext = (s0 + TPA + sub < s1) ? row[s0 + TPA + sub] : 0u;
+  }
+  __device__ inline GeoSlot *slot(int c) const { return ring + ((head + c) & (kSlots - 1)); }
+
+  // Fill the ring to >= TPA pairs (or the end of the row); returns the number
+  // of pairs in the next chunk.  When pdf_row is given, each inactive entry's
+  // pdf slot is written as zero here.
+  __device__ inline int feed(const KParams &kp, const BoxP &box, double xi, double yi,
+                             double zi, const double *__restrict__ x,
+                             const uint32_t *__restrict__ row, float4 *__restrict__ pdf_row) {
+    while (qn < TPA && t < s1) {
+      const NbPos pc = pnext;
+      pnext = load_nb(x, enext, t + TPA + sub < s1);
+      enext = (t + 2 * TPA + sub < s1) ? row[t + 2 * TPA + sub] : 0u;
+      PairGeo g;
+      pair_geometry(kp, box, xi, yi, zi, pc, g);
+      const bool act = g.ti >= 0;
+      const unsigned bal = (__ballot_sync(gmask, act) >> gshift) & kBits;
+      if (act) geo_store(slot(qn + __popc(bal & ((1u << sub) - 1u))), g, t + sub);
+      else if (pdf_row != nullptr && t + sub < s1)
+        pdf_row[t + sub] = make_float4(0.f, 0.f, 0.f, 0.f);
+      qn += __popc(bal);
+      t += TPA;
+    }
+    __syncwarp(gmask);
+    return min(qn, TPA);
+  }
+  // Drop the chunk just processed (after every lane has read its slots).
+  __device__ inline void pop(int cnt) {
+    __syncwarp(gmask);
+    head = (head + cnt) & (kSlots - 1);
+    qn -= cnt;
+  }
+};
+
 template <int TPA, int D, int RK>
 __global__ void __launch_bounds__(kPairThreads, 4)
 k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
@@ -64,15 +125,17 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
              const int *__restrict__ boff, float *__restrict__ P,
              float *__restrict__ G) {
   constexpr int D2 = (D + 1) / 2;
-  __shared__ GeoSlot geo[kPairThreads];
+  __shared__ GeoSlot geo[2 * kPairThreads];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gt / TPA;
   const int sub = gt % TPA;
   if (a >= n) return;
   const int lane = threadIdx.x & 31;
-  const unsigned gmask =
-      TPA == 32 ? 0xffffffffu : (((1u << TPA) - 1u) << (lane & ~(TPA - 1)));
-  GeoSlot *gslot = geo + (threadIdx.x - sub);  // slots of this atom's group
+  PairRing<TPA> pr;
+  pr.sub = sub;
+  pr.gshift = lane & ~(TPA - 1);
+  pr.gmask = PairRing<TPA>::kBits << pr.gshift;
+  pr.ring = geo + 2 * (threadIdx.x - sub);  // the ring of this atom's group
   const int B = kp.B, K = kp.K, M = kp.M;
   const int k0 = 4 * sub;
   const Radial4<RK> R = load_radial4<RK>(kp, k0);
@@ -85,22 +148,12 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
     for (int q = 0; q < 4; q++)
 #pragma unroll
       for (int p = 0; p < D2; p++) acc[q][p] = make_float2(0.f, 0.f);
-    const int s0 = bo[b], s1 = bo[b + 1];
-    NbPos pnext = load_nb(x, s0 + sub < s1 ? row[s0 + sub] : 0u, s0 + sub < s1);
-    uint32_t enext = (s0 + TPA + sub < s1) ? row[s0 + TPA + sub] : 0u;
-    for (int t0 = s0; t0 < s1; t0 += TPA) {
-      const NbPos pc = pnext;
-      pnext = load_nb(x, enext, t0 + TPA + sub < s1);
-      enext = (t0 + 2 * TPA + sub < s1) ? row[t0 + 2 * TPA + sub] : 0u;
-      PairGeo mine;
-      pair_geometry(kp, box, xi, yi, zi, pc, mine);
-      __syncwarp(gmask);
-      geo_store(gslot + sub, mine);
-      __syncwarp(gmask);
-      const int cnt = min(TPA, s1 - t0);
+    pr.begin(x, row, bo[b], bo[b + 1]);
+    for (;;) {
+      const int cnt = pr.feed(kp, box, xi, yi, zi, x, row, nullptr);
+      if (cnt == 0) break;
       for (int c = 0; c < cnt; c++) {
-        const PairGeo g = geo_load(gslot + c);
-        if (g.ti < 0) continue;
+        const PairGeo g = geo_load(pr.slot(c));
         float H[4], dH[4];
         radial4<RK, false>(kp, R, g, H, dH);
         float2 M2[D2];
@@ -112,6 +165,7 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
           for (int p = 0; p < D2; p++) acc[q][p] = __ffma2_rn(h2, M2[p], acc[q][p]);
         }
       }
+      pr.pop(cnt);
     }
     // P rows of this lane: 4 filters x D values, contiguous
     float *Pp = P + (((size_t)a * B + b) * K + k0) * D;

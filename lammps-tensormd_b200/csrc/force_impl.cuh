@@ -12,14 +12,14 @@
 // per lane as FP32 pairs, TPA = K/4 lanes per atom), U and V are packed FP32x2
 // FMAs, sum_d V_d dM_d/dx_j is the gradient of the polynomial
 // Q(u) = sum_d V_d M_d(u), and df (times the pair_coeff scale) goes to its
-// slot pdf[i*cap + t].  Pair geometry is shared through shared memory as in
-// the descriptor kernel.  The reaction -df on j is summed later by k_gather
-// through the partner slot, in a fixed order.
+// slot pdf[i*cap + t] (zero for entries beyond rc).  Active pairs are queued
+// in shared memory as in the descriptor kernel (PairRing).  The reaction -df
+// on j is summed later by k_gather through the partner slot, in a fixed order.
 //
 // wv[i] = sum over i's pairs of -r_ij (x) df (xx, yy, zz, xy, xz, yz): the
 // per-pair virial of sum_forces_device (kernel.cu:1714-1758), accumulated in
-// FP64 by the lane that computed the pair's FP64 geometry; its sum over atoms
-// is the global virial.
+// FP64 by the lane that owns the pair in its chunk; its sum over atoms is the
+// global virial.
 #pragma once
 
 #include "descriptor_impl.cuh"
@@ -35,15 +35,18 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
         const float *__restrict__ dEdG, float4 *__restrict__ pdf,
         double *__restrict__ wv) {
   constexpr int D2 = (D + 1) / 2;
-  __shared__ GeoSlot geo[kPairThreads];
+  __shared__ GeoSlot geo[2 * kPairThreads];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gt / TPA;
   const int sub = gt % TPA;
   if (a >= n) return;
   const int lane = threadIdx.x & 31;
-  const unsigned gmask =
-      TPA == 32 ? 0xffffffffu : (((1u << TPA) - 1u) << (lane & ~(TPA - 1)));
-  GeoSlot *gslot = geo + (threadIdx.x - sub);
+  PairRing<TPA> pr;
+  pr.sub = sub;
+  pr.gshift = lane & ~(TPA - 1);
+  pr.gmask = PairRing<TPA>::kBits << pr.gshift;
+  pr.ring = geo + 2 * (threadIdx.x - sub);
+  const unsigned gmask = pr.gmask;
   const int B = kp.B, K = kp.K, M = kp.M;
   const int k0 = 4 * sub;
   const Radial4<RK> R = load_radial4<RK>(kp, k0);
@@ -78,41 +81,45 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
         for (int p = 0; p < D2; p++) S2[q][p] = make_float2(Sq[2 * p], Sq[2 * p + 1]);
       }
     }
-    NbPos pnext = load_nb(x, s0 + sub < s1 ? row[s0 + sub] : 0u, s0 + sub < s1);
-    uint32_t enext = (s0 + TPA + sub < s1) ? row[s0 + TPA + sub] : 0u;
-    for (int t0 = s0; t0 < s1; t0 += TPA) {
-      const NbPos pc = pnext;
-      pnext = load_nb(x, enext, t0 + TPA + sub < s1);
-      enext = (t0 + 2 * TPA + sub < s1) ? row[t0 + 2 * TPA + sub] : 0u;
-      PairGeo mine;
-      pair_geometry(kp, box, xi, yi, zi, pc, mine);
-      __syncwarp(gmask);
-      geo_store(gslot + sub, mine);
-      __syncwarp(gmask);
-      const int cnt = min(TPA, s1 - t0);
+    float4 *pdf_row = pdf + (size_t)a * cap;
+    pr.begin(x, row, s0, s1);
+    for (;;) {
+      // inactive entries get their zero pdf inside feed()
+      const int cnt = pr.feed(kp, box, xi, yi, zi, x, row, pdf_row);
+      if (cnt == 0) break;
       float3 mydf = make_float3(0.f, 0.f, 0.f);
       for (int c = 0; c < cnt; c++) {
-        const PairGeo g = geo_load(gslot + c);
-        if (g.ti < 0) continue;
+        const PairGeo g = geo_load(pr.slot(c));
         float H[4], dH[4];
         radial4<RK, true>(kp, R, g, H, dH);
         float2 M2[D2];
         moments2<D, D2>(g.ux, g.uy, g.uz, M2);
-        float f1 = 0.f;
-        float2 V2[D2];
+        // V_d = sum_k S[k,d] H_k and W_d = sum_k S[k,d] dH_k: 2 x D2
+        // independent FFMA2 chains of length 4; then the F1 scalar
+        // sum_k U_k dH_k = sum_d M_d W_d as two interleaved partial dots
+        float2 V2[D2], W2[D2];
 #pragma unroll
-        for (int p = 0; p < D2; p++) V2[p] = make_float2(0.f, 0.f);
+        for (int p = 0; p < D2; p++) {
+          V2[p] = make_float2(0.f, 0.f);
+          W2[p] = make_float2(0.f, 0.f);
+        }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          float2 U2 = make_float2(0.f, 0.f);
           const float2 h2 = make_float2(H[q], H[q]);
+          const float2 d2 = make_float2(dH[q], dH[q]);
 #pragma unroll
           for (int p = 0; p < D2; p++) {
-            U2 = __ffma2_rn(S2[q][p], M2[p], U2);
             V2[p] = __ffma2_rn(S2[q][p], h2, V2[p]);
+            W2[p] = __ffma2_rn(S2[q][p], d2, W2[p]);
           }
-          f1 = fmaf(U2.x + U2.y, dH[q], f1);
         }
+        float2 fa = make_float2(0.f, 0.f), fb = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int p = 0; p < D2; p += 2) {
+          fa = __ffma2_rn(M2[p], W2[p], fa);
+          if (p + 1 < D2) fb = __ffma2_rn(M2[p + 1], W2[p + 1], fb);
+        }
+        const float f1 = (fa.x + fb.x) + (fa.y + fb.y);
         float V[2 * D2];
 #pragma unroll
         for (int p = 0; p < D2; p++) { V[2 * p] = V2[p].x; V[2 * p + 1] = V2[p].y; }
@@ -130,22 +137,24 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
         }
         if (c == sub) mydf = make_float3(fx * scale, fy * scale, fz * scale);
       }
-      // every lane owns one pair of the chunk: store it and add its virial
-      // with the FP64 separation this lane computed
-      if (t0 + sub < s1) {
-        pdf[(size_t)a * cap + t0 + sub] = make_float4(mydf.x, mydf.y, mydf.z, 0.f);
-        if (mine.ti >= 0) {
-          double rr = (double)mine.r + (double)mine.rlo;
-          double rx = (double)mine.ux * rr, ry = (double)mine.uy * rr,
-                 rz = (double)mine.uz * rr;
-          w6[0] -= rx * mydf.x;
-          w6[1] -= ry * mydf.y;
-          w6[2] -= rz * mydf.z;
-          w6[3] -= rx * mydf.y;
-          w6[4] -= rx * mydf.z;
-          w6[5] -= ry * mydf.z;
-        }
+      // lane c owns pair c of the chunk: store its pdf slot and add its
+      // virial, with the separation as r (hi + lo) times u
+      if (sub < cnt) {
+        const GeoSlot *s = pr.slot(sub);
+        const float4 ga = s->a;
+        const float uz = s->b.x;
+        const int t = __float_as_int(s->c.y);
+        pdf_row[t] = make_float4(mydf.x, mydf.y, mydf.z, 0.f);
+        double rr = (double)ga.x + (double)ga.y;
+        double rx = (double)ga.z * rr, ry = (double)ga.w * rr, rz = (double)uz * rr;
+        w6[0] -= rx * mydf.x;
+        w6[1] -= ry * mydf.y;
+        w6[2] -= rz * mydf.z;
+        w6[3] -= rx * mydf.y;
+        w6[4] -= rx * mydf.z;
+        w6[5] -= ry * mydf.z;
       }
+      pr.pop(cnt);
     }
   }
 #pragma unroll
