@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-bf16", action="store_true")
+    ap.add_argument("--cells-steps", type=int, default=500,
+                    help="NVE steps of the 4,096-cell batch line (0 skips it)")
     return ap.parse_args()
 
 
@@ -343,6 +345,10 @@ def run_ours(args, rank, world, local):
         except Exception as exc:  # report, do not hide
             forms[prec] = {"error": str(exc)}
 
+    cells = None
+    if args.cells_steps > 0:
+        cells = run_cells(args, rank, world, local, dev, barrier)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.config, samples=2)
@@ -364,12 +370,69 @@ def run_ours(args, rank, world, local):
             "roofline_fp32": roofline_fp32,
             "kernel_ms": kernel_ms,
             "forms": forms,
+            "cells4096": cells,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_cells(args, rank, world, local, dev, barrier):
+    """Multi-cell batch: 4,096 cells x 256 atoms (half FCC, half BCC), two
+    elements, per-cell temperatures 300-1200 K, NVE through tmd_batch_nve_run
+    (every step one CUDA graph launch), timed with CUDA events on the batch
+    stream, max over ranks."""
+    import torch
+    from tmd_b200 import TensorMDBatch, TensorMDModel, synth
+    c = synth.config("cells4096")
+    pot = f"/tmp/tmd_bench_cells_{rank}.npz"
+    syms = synth.gaussian_potential(pot, seed=2024, **c["pot"])
+    data = synth.batch_cells(c["ncells"], c["natoms"], nelt=c["nelt"], sigma=c["sigma"],
+                             t_range=c["t_range"], seed=99 + rank)
+    model = TensorMDModel(f"{pot} {' '.join(syms)}", device=local)
+    b = TensorMDBatch(model, data["natoms"], 1.0)
+    b.set_cells(data["boxes"])
+    b.set_atoms(data["x"], data["types"], data["v"])
+    n = b.n
+    dt = 0.001
+    stream = torch.cuda.ExternalStream(b.system().stream(), device=dev)
+    b.nve_run(max(args.warmup, 3), dt)
+    torch.cuda.synchronize()
+    sv = b.system()
+    l0 = sv.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    th = b.nve_run(args.cells_steps, dt, thermo_every=args.cells_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms = float(ms.item())
+    launches = sv.launches() - l0
+    sv.profile(True)
+    sv.profile_read(reset=True)
+    b.nve_run(20, dt)
+    prof = sv.profile_read(reset=True)
+    sv.profile(False)
+    etot = th.sum(-1)  # rows x cells
+    drift = float(np.abs(etot[-1] - etot[0]).max() / c["natoms"])
+    out = {"value": n * args.cells_steps * world / (ms / 1000.0), "unit": UNIT,
+           "ms_per_step": ms / args.cells_steps, "steps": args.cells_steps,
+           "natoms": n, "ncells": c["ncells"], "gpu_launches": launches,
+           "max_cell_energy_drift_eV_per_atom": drift,
+           "kernel_ms": {k: (cnt, t / max(cnt, 1)) for k, (cnt, t) in prof.items()},
+           "config": {k: v for k, v in c.items() if k != "pot"} | {"potential": c["pot"]}}
+    b.close()
+    model.close()
+    return out
 
 
 def cpu_baseline(cfg_name, samples=2):

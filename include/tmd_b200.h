@@ -54,7 +54,8 @@ typedef struct tmd_system tmd_system;
  * (pair_tensormd.cpp:349-370).  `device` is the CUDA ordinal. */
 int tmd_model_load(const char *coeff_args, int device, tmd_model **out);
 
-/* Free a model (systems created from it must be freed first). */
+/* Free a model.  If systems created from it are still alive, the model is
+ * released when the last of them is freed (any free order is safe). */
 void tmd_model_free(tmd_model *model);
 
 /* Model facts: cutmax (PairTensorMD::init_one, pair_tensormd.cpp:336-341),
@@ -143,6 +144,37 @@ int tmd_profile_read(tmd_system *sys, long *launches, double *ms, int reset);
 
 /* Copy the message of the last failed call on this thread into buf. */
 int tmd_last_error(char *buf, int len);
+
+/* ---- Multi-cell batches ---------------------------------------------------
+ * Many independent small periodic systems ("cells", e.g. 4096 cells of 256
+ * atoms) evaluated together: one launch per kernel over all cells.  The
+ * reference runs one LAMMPS system per process (pair_tensormd.cpp:141-184);
+ * a batch of C cells gives, cell by cell, the results of C separate systems
+ * (tmd_system_*), with per-cell energies, virials and thermo.
+ *
+ * Atom arrays are concatenated cell by cell: cell c holds natoms[c] atoms
+ * starting at sum(natoms[0..c-1]).  Each cell has its own box[9] and pbc[3]
+ * (conventions above); a cell may be smaller than the cutoff (up to 3 images
+ * per axis).  tmd_batch_system() returns the underlying system handle for
+ * tmd_system_stream / launches / profile / get / neighbor_list /
+ * get_descriptors; its tmd_compute gives the sum over cells. */
+typedef struct tmd_batch tmd_batch;
+int tmd_batch_create(const tmd_model *model, int ncells, const int *natoms,
+                     double skin, tmd_batch **out);
+void tmd_batch_free(tmd_batch *batch);
+int tmd_batch_system(tmd_batch *batch, tmd_system **sys);
+/* boxes[ncells*9], pbc[ncells*3]. */
+int tmd_batch_set_cells(tmd_batch *batch, const double *boxes, const int *pbc);
+/* x[N*3], type[N], v[N*3] or NULL, N = total atoms of the batch. */
+int tmd_batch_set_atoms(tmd_batch *batch, const double *x, const int *type,
+                        const double *v);
+int tmd_batch_get(tmd_batch *batch, double *x, double *v, double *f, int *image);
+/* energy[ncells], virial[ncells*6], f[N*3]; any may be NULL. */
+int tmd_batch_compute(tmd_batch *batch, double *energy, double *virial, double *f);
+/* As tmd_nve_run for every cell at once; thermo[rows*ncells*2] holds
+ * (pe, ke) per cell, row-major by thermo row then cell. */
+int tmd_batch_nve_run(tmd_batch *batch, int nsteps, double dt, int thermo_every,
+                      double *thermo);
 
 /* Full neighbor list without allocating any memory.  This entry point has no
  * counterpart in the reference.  It is meant for callers that must not call

@@ -23,118 +23,27 @@
 #include <string>
 #include <vector>
 
-#include "../../include/tmd_b200.h"
-#include "model.h"
-#include "tmd_kernels.h"
+#include "system.h"
 
 using namespace tmd;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
+
+namespace tmd {
+// error message of calls implemented in other translation units
+void set_last_error(const std::string &msg) { g_err = msg; }
 
 int fail(int code, const std::string &msg) {
   g_err = msg;
   return code;
 }
 
-#define TMD_CUDA(call)                                                        \
-  do {                                                                        \
-    cudaError_t e_ = (call);                                                  \
-    if (e_ != cudaSuccess)                                                    \
-      return fail(TMD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-template <typename T>
-cudaError_t dalloc(T **p, size_t count) {
-  *p = nullptr;
-  if (count == 0) count = 1;
-  return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T));
-}
-
-template <typename T>
-void dfree(T *&p) {
-  if (p) cudaFree(p);
-  p = nullptr;
-}
-
-}  // namespace
-
-struct tmd_model {
-  int device = 0;
-  HostModel h;
-  KParams kp;
-  float *d_table = nullptr;
-  std::vector<float *> d_buf;   // weights and biases
-  MlpLayer *d_layers = nullptr;
-  MlpTcLayer *d_tc_layers = nullptr;  // tensor-core MLP (precision bf16)
-  size_t tc_smem = 0;
-  bool tc_dz_bf16 = false;
-  int tc_np = 1;
-  int maxh = 1;
-  double *d_mass = nullptr;     // per element
-  int mlp_tr = 64;
-  size_t mlp_smem = 0;
-  int nsys = 0;
-};
-
-struct tmd_system {
-  const tmd_model *m = nullptr;
-  cudaStream_t st = nullptr;
-  long launches = 0;
-  int natoms_cap = 0, n = 0;
-  double skin = 1.0;
-  bool have_box = false, have_atoms = false, have_v = false;
-  bool forces_valid = false;
-  BoxP box{};
-  BinP bin{};
-  int cap = 0, capp = 0;  // neighbor entries per atom, pow2 >= cap
-  int ncell_alloc = 0;
-  // device state
-  double *x = nullptr, *v = nullptr, *f = nullptr, *xbuild = nullptr;
-  int *image = nullptr, *elem = nullptr;
-  int *cell_of = nullptr, *cell_count = nullptr, *cell_start = nullptr,
-      *cell_cursor = nullptr, *cell_atoms = nullptr;
-  uint32_t *tmp = nullptr, *nbr = nullptr;
-  int *nraw = nullptr, *boff = nullptr, *rev = nullptr;
-  float *P = nullptr, *G = nullptr, *dEdG = nullptr;
-  double *E = nullptr;
-  float4 *pdf = nullptr;
-  double *wv = nullptr, *eatom = nullptr, *vatom = nullptr, *ke = nullptr;
-  double *partial = nullptr, *scal = nullptr;  // scal: [0] pe, [1..6] virial, [7] ke
-  int *flag = nullptr, *status = nullptr, *maxneed = nullptr;
-  int *perm = nullptr, *tiles = nullptr;
-  int ntiles = 0;
-  double *thermo_d = nullptr;
-  int thermo_rows_alloc = 0;
-  // host
-  std::vector<int> h_elem;
-  double *h_scal = nullptr;  // pinned [8]
-  int *h_status = nullptr;   // pinned [2]
-  // kernel timing
-  bool prof = false;
-  std::vector<cudaEvent_t> ev_pool;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
-  long prof_n[TMD_NPROF] = {0};
-  double prof_ms[TMD_NPROF] = {0};
-  cudaEvent_t cur_start = nullptr;
-  // captured MD step (velocity Verlet + rebuild check/rebuild + force)
-  cudaGraphExec_t step_exec = nullptr;
-  double step_dt = 0.0;
-  long step_launches = 0;
-};
-
-namespace tmd {
-// error message of calls implemented in other translation units
-void set_last_error(const std::string &msg) { g_err = msg; }
-}  // namespace tmd
-
-namespace {
 void drop_graph(tmd_system *s) {
   if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
   s->step_exec = nullptr;
 }
-}  // namespace
 
 namespace {
 
@@ -174,6 +83,8 @@ void prof_end(tmd_system *s, int fam) {
   }
 }
 
+}  // namespace
+
 void box_setup(BoxP &b, const double bx[9], const int pbc[3]) {
   b.lo[0] = bx[0]; b.lo[1] = bx[1]; b.lo[2] = bx[2];
   b.xprd = bx[3]; b.yprd = bx[4]; b.zprd = bx[5];
@@ -204,6 +115,7 @@ void widths(const BoxP &b, double w[3]) {
   cross(a, bb, t); w[2] = V / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
 }
 
+namespace {
 int bin_setup(tmd_system *s) {
   drop_graph(s);
   double cut = s->m->h.rmax + s->skin;
@@ -250,6 +162,7 @@ int pow2_at_least(int v) {
   while (p < v) p <<= 1;
   return p;
 }
+}  // namespace
 
 int alloc_neighbors(tmd_system *s, int cap) {
   drop_graph(s);
@@ -268,14 +181,23 @@ int alloc_neighbors(tmd_system *s, int cap) {
 
 int initial_cap(tmd_system *s) {
   double cut = s->m->h.rmax + s->skin;
-  double V = s->box.xprd * s->box.yprd * s->box.zprd;
-  double dens = s->n / V;
+  double dens = 0.0;
+  if (s->ncells > 0) {
+    for (int c = 0; c < s->ncells; c++) {
+      const BoxP &b = s->h_cbox[c];
+      double nc = s->h_coff[c + 1] - s->h_coff[c];
+      dens = std::max(dens, nc / (b.xprd * b.yprd * b.zprd));
+    }
+  } else {
+    dens = s->n / (s->box.xprd * s->box.yprd * s->box.zprd);
+  }
   double est = dens * 4.0 / 3.0 * M_PI * cut * cut * cut;
   int cap = (int)std::ceil(1.3 * est) + 32;
   if (cap < 64) cap = 64;
   return cap;
 }
 
+namespace {
 NbArgs nb_args(tmd_system *s) {
   NbArgs a{};
   a.n = s->n; a.B = s->m->h.nelt; a.cap = s->cap; a.capp = s->capp;
@@ -287,8 +209,11 @@ NbArgs nb_args(tmd_system *s) {
   a.cell_cursor = s->cell_cursor; a.cell_atoms = s->cell_atoms;
   a.tmp = s->tmp; a.nraw = s->nraw; a.nbr = s->nbr; a.boff = s->boff; a.rev = s->rev;
   a.xbuild = s->xbuild; a.flag = s->flag; a.status = s->status; a.maxneed = s->maxneed;
+  a.ncells = s->ncells; a.cbox = s->cbox; a.cgeom = s->cgeom; a.acell = s->acell;
+  a.coff = s->coff;
   return a;
 }
+}  // namespace
 
 // Read the status words and clear them for the next kernels.
 int read_status(tmd_system *s) {
@@ -333,6 +258,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   DescArgs d{};
   d.n = s->n; d.cap = s->cap; d.kp = m->kp; d.box = s->box; d.x = s->x;
   d.elem = s->elem; d.nbr = s->nbr; d.boff = s->boff; d.P = s->P; d.G = s->G;
+  d.cbox = s->ncells ? s->cbox : nullptr; d.acell = s->acell;
   prof_begin(s);
   launch_descriptor(d, s->st, s->launches);
   prof_end(s, 1);
@@ -360,6 +286,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   fa.n = s->n; fa.cap = s->cap; fa.kp = m->kp; fa.box = s->box; fa.scale = scale;
   fa.x = s->x; fa.elem = s->elem; fa.nbr = s->nbr; fa.boff = s->boff; fa.P = s->P;
   fa.G = s->G; fa.dEdG = s->dEdG; fa.pdf = s->pdf; fa.wv = s->wv;
+  fa.cbox = d.cbox; fa.acell = s->acell;
   prof_begin(s);
   launch_force(fa, s->st, s->launches);
   prof_end(s, 3);
@@ -367,12 +294,107 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   ga.n = s->n; ga.cap = s->cap; ga.B = m->h.nelt; ga.boff = s->boff; ga.pdf = s->pdf;
   ga.rev = s->rev; ga.nbr = s->nbr; ga.x = s->x; ga.box = s->box; ga.wv = s->wv;
   ga.f = s->f; ga.vatom = want_vatom ? s->vatom : nullptr;
+  ga.cbox = d.cbox; ga.acell = s->acell;
   prof_begin(s);
   launch_gather(ga, s->st, s->launches);
   prof_end(s, 4);
 }
 
-}  // namespace
+int thermo_reserve(tmd_system *s, long count) {
+  if (count > s->thermo_alloc) {
+    dfree(s->thermo_d);
+    TMD_CUDA(dalloc(&s->thermo_d, (size_t)count));
+    s->thermo_alloc = count;
+  }
+  return TMD_OK;
+}
+
+int run_nve(tmd_system *s, int nsteps, double dt, int thermo_every,
+            void (*thermo_row)(tmd_system *, int), double *thermo, long thermo_count) {
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  const int n = s->n;
+  if (n == 0) return TMD_OK;
+  const double ftm2v = 1.0 / 1.0364269e-4;  // metal units, update.cpp:187-206
+  const double dtf = 0.5 * dt * ftm2v;
+  const double half = 0.5 * s->skin;
+  const double trigsq = half * half;
+  const bool want_thermo = thermo && thermo_every > 0;
+  if (want_thermo) {
+    int rc = thermo_reserve(s, thermo_count);
+    if (rc) return rc;
+  }
+  int rc = clear_status(s);
+  if (rc) return rc;
+  // Verlet::setup: forces of the starting positions
+  launch_force_eval(s, 1.0f, false);
+  int row = 0;
+  if (want_thermo) thermo_row(s, row++);
+  auto md_step = [&]() {
+    prof_begin(s);
+    launch_nve_initial(n, s->x, s->v, s->f, s->elem, s->m->d_mass, dtf, dt, s->st, s->launches);
+    launch_neighbor_check(n, s->x, s->xbuild, trigsq, s->flag, s->st, s->launches);
+    prof_end(s, 5);
+    prof_begin(s);
+    launch_neighbor_build(nb_args(s), s->st, s->launches);
+    prof_end(s, 0);
+    launch_force_eval(s, 1.0f, false);
+    prof_begin(s);
+    launch_nve_final(n, s->v, s->f, s->elem, s->m->d_mass, dtf, s->st, s->launches);
+    prof_end(s, 5);
+  };
+  // Without kernel timing, the step runs as one captured CUDA graph: every
+  // launch (including the conditional rebuild kernels) is replayed with its
+  // arguments fixed at capture; buffers, box, atom count and dt key the graph.
+  const bool use_graph = !s->prof;
+  if (use_graph && (!s->step_exec || s->step_dt != dt)) {
+    drop_graph(s);
+    cudaGraph_t g;
+    long l0 = s->launches;
+    TMD_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+    md_step();
+    TMD_CUDA(cudaStreamEndCapture(s->st, &g));
+    cudaError_t ie = cudaGraphInstantiate(&s->step_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      s->step_exec = nullptr;
+      return fail(TMD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
+    }
+    s->step_launches = s->launches - l0;
+    s->launches = l0;
+    s->step_dt = dt;
+  }
+  for (int step = 1; step <= nsteps; step++) {
+    if (use_graph) {
+      TMD_CUDA(cudaGraphLaunch(s->step_exec, s->st));
+      s->launches += s->step_launches;
+    } else {
+      md_step();
+    }
+    if (want_thermo && (step % thermo_every == 0 || step == nsteps)) {
+      prof_begin(s);
+      thermo_row(s, row++);
+      prof_end(s, 6);
+    }
+  }
+  launch_check_finite(n, s->f, nullptr, s->status, s->st, s->launches);
+  TMD_CUDA(cudaGetLastError());
+  if (want_thermo && thermo_count > 0)
+    TMD_CUDA(cudaMemcpyAsync(thermo, s->thermo_d, thermo_count * sizeof(double),
+                             cudaMemcpyDeviceToHost, s->st));
+  rc = read_status(s);
+  if (rc) return rc;
+  int st = s->h_status[0];
+  if (st & kStatusOverflow)
+    return fail(TMD_ERR_CAPACITY, "neighbor list overflow during the run (raise the "
+                                  "capacity by calling set_atoms again)");
+  if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
+  if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
+  if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite force during the run");
+  s->forces_valid = true;
+  return TMD_OK;
+}
+
+}  // namespace tmd
 
 extern "C" {
 
@@ -544,6 +566,10 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
 
 void tmd_model_free(tmd_model *m) {
   if (!m) return;
+  if (m->nsys > 0) {  // systems still use it: the last tmd_system_free releases it
+    m->released = true;
+    return;
+  }
   for (float *p : m->d_buf) cudaFree(p);
   if (m->d_layers) cudaFree(m->d_layers);
   if (m->d_tc_layers) cudaFree(m->d_tc_layers);
@@ -624,6 +650,7 @@ void tmd_system_free(tmd_system *s) {
   dfree(s->wv); dfree(s->eatom); dfree(s->vatom); dfree(s->ke); dfree(s->partial);
   dfree(s->scal); dfree(s->flag); dfree(s->status); dfree(s->maxneed); dfree(s->perm);
   dfree(s->tiles); dfree(s->thermo_d);
+  dfree(s->cbox); dfree(s->cgeom); dfree(s->acell); dfree(s->coff); dfree(s->cell_out);
   if (s->h_scal) cudaFreeHost(s->h_scal);
   if (s->h_status) cudaFreeHost(s->h_status);
   for (auto &p : s->ev_pending) {
@@ -632,13 +659,18 @@ void tmd_system_free(tmd_system *s) {
   }
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   if (s->st) cudaStreamDestroy(s->st);
-  if (s->m) const_cast<tmd_model *>(s->m)->nsys--;
+  if (s->m) {
+    tmd_model *m = const_cast<tmd_model *>(s->m);
+    if (--m->nsys == 0 && m->released) tmd_model_free(m);
+  }
   delete s;
 }
 
 int tmd_system_set_box(tmd_system *s, const double bx[9], const int pbc[3]) {
   if (!s || !bx || !pbc) return fail(TMD_ERR_ARG, "null argument");
   if (!(bx[3] > 0 && bx[4] > 0 && bx[5] > 0)) return fail(TMD_ERR_ARG, "box lengths must be > 0");
+  if (s->ncells > 0)
+    return fail(TMD_ERR_STATE, "a batch takes one box per cell (tmd_batch_set_cells)");
   TMD_CUDA(cudaSetDevice(s->m->device));
   box_setup(s->box, bx, pbc);
   s->have_box = true;
@@ -661,6 +693,8 @@ int tmd_system_set_atoms(tmd_system *s, int n, const double *x, const int *type,
   if (!s || !x || !type || n < 0) return fail(TMD_ERR_ARG, "null argument");
   if (n > s->natoms_cap) return fail(TMD_ERR_CAPACITY, "n exceeds the system capacity");
   if (!s->have_box) return fail(TMD_ERR_STATE, "set the box before the atoms");
+  if (s->ncells > 0 && n != s->h_coff[s->ncells])
+    return fail(TMD_ERR_ARG, "a batch takes exactly the atoms of its cells");
   TMD_CUDA(cudaSetDevice(s->m->device));
   const HostModel &h = s->m->h;
   drop_graph(s);
@@ -788,93 +822,14 @@ int tmd_nve_run(tmd_system *s, int nsteps, double dt, int thermo_every, double *
   if (!s || nsteps < 0 || !(dt > 0)) return fail(TMD_ERR_ARG, "bad nve arguments");
   if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before nve_run");
   if (thermo && thermo_every < 1) return fail(TMD_ERR_ARG, "thermo_every must be >= 1");
-  TMD_CUDA(cudaSetDevice(s->m->device));
-  const int n = s->n;
-  if (n == 0) return TMD_OK;
-  const double ftm2v = 1.0 / 1.0364269e-4;  // metal units, update.cpp:187-206
-  const double dtf = 0.5 * dt * ftm2v;
-  const double half = 0.5 * s->skin;
-  const double trigsq = half * half;
   int rows = thermo ? 1 + nsteps / thermo_every + ((nsteps % thermo_every) ? 1 : 0) : 0;
-  if (rows > s->thermo_rows_alloc) {
-    dfree(s->thermo_d);
-    TMD_CUDA(dalloc(&s->thermo_d, 2 * (size_t)rows));
-    s->thermo_rows_alloc = rows;
-  }
-  int rc = clear_status(s);
-  if (rc) return rc;
-  auto thermo_row = [&](int r) {
-    launch_reduce_scaled(s->E, n, s->partial, s->thermo_d + 2 * r, 1.0, s->st, s->launches);
-    launch_kinetic(n, s->v, s->elem, s->m->d_mass, s->ke, s->st, s->launches);
-    launch_reduce_f64(s->ke, n, 1, s->partial, s->thermo_d + 2 * r + 1, s->st, s->launches);
+  // row r: potential energy, kinetic energy of the whole system
+  auto row_fn = [](tmd_system *q, int r) {
+    launch_reduce_scaled(q->E, q->n, q->partial, q->thermo_d + 2 * r, 1.0, q->st, q->launches);
+    launch_kinetic(q->n, q->v, q->elem, q->m->d_mass, q->ke, q->st, q->launches);
+    launch_reduce_f64(q->ke, q->n, 1, q->partial, q->thermo_d + 2 * r + 1, q->st, q->launches);
   };
-  // Verlet::setup: forces of the starting positions
-  launch_force_eval(s, 1.0f, false);
-  int row = 0;
-  if (thermo) thermo_row(row++);
-  auto md_step = [&]() {
-    prof_begin(s);
-    launch_nve_initial(n, s->x, s->v, s->f, s->elem, s->m->d_mass, dtf, dt, s->st, s->launches);
-    launch_neighbor_check(n, s->x, s->xbuild, trigsq, s->flag, s->st, s->launches);
-    prof_end(s, 5);
-    prof_begin(s);
-    launch_neighbor_build(nb_args(s), s->st, s->launches);
-    prof_end(s, 0);
-    launch_force_eval(s, 1.0f, false);
-    prof_begin(s);
-    launch_nve_final(n, s->v, s->f, s->elem, s->m->d_mass, dtf, s->st, s->launches);
-    prof_end(s, 5);
-  };
-  // Without kernel timing, the step runs as one captured CUDA graph: every
-  // launch (including the conditional rebuild kernels) is replayed with its
-  // arguments fixed at capture; buffers, box, atom count and dt key the graph.
-  const bool use_graph = !s->prof;
-  if (use_graph && (!s->step_exec || s->step_dt != dt)) {
-    drop_graph(s);
-    cudaGraph_t g;
-    long l0 = s->launches;
-    TMD_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-    md_step();
-    TMD_CUDA(cudaStreamEndCapture(s->st, &g));
-    cudaError_t ie = cudaGraphInstantiate(&s->step_exec, g, 0);
-    cudaGraphDestroy(g);
-    if (ie != cudaSuccess) {
-      s->step_exec = nullptr;
-      return fail(TMD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
-    }
-    s->step_launches = s->launches - l0;
-    s->launches = l0;
-    s->step_dt = dt;
-  }
-  for (int step = 1; step <= nsteps; step++) {
-    if (use_graph) {
-      TMD_CUDA(cudaGraphLaunch(s->step_exec, s->st));
-      s->launches += s->step_launches;
-    } else {
-      md_step();
-    }
-    if (thermo && (step % thermo_every == 0 || step == nsteps)) {
-      prof_begin(s);
-      thermo_row(row++);
-      prof_end(s, 6);
-    }
-  }
-  launch_check_finite(n, s->f, nullptr, s->status, s->st, s->launches);
-  TMD_CUDA(cudaGetLastError());
-  if (thermo && rows > 0)
-    TMD_CUDA(cudaMemcpyAsync(thermo, s->thermo_d, 2 * rows * sizeof(double),
-                             cudaMemcpyDeviceToHost, s->st));
-  rc = read_status(s);
-  if (rc) return rc;
-  int st = s->h_status[0];
-  if (st & kStatusOverflow)
-    return fail(TMD_ERR_CAPACITY, "neighbor list overflow during the run (raise the "
-                                  "capacity by calling set_atoms again)");
-  if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
-  if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
-  if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite force during the run");
-  s->forces_valid = true;
-  return TMD_OK;
+  return run_nve(s, nsteps, dt, thermo ? thermo_every : 0, row_fn, thermo, 2L * rows);
 }
 
 int tmd_neighbor_list(tmd_system *s, double cut, int *counts, int *entries, long cap,
@@ -903,7 +858,8 @@ int tmd_neighbor_list(tmd_system *s, double cut, int *counts, int *entries, long
       int j = e & kAtomMask, sx, sy, sz;
       shift_decode(int(e >> kAtomBits), sx, sy, sz);
       double gx, gy, gz;
-      image_of(s->box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sx, sy, sz, gx, gy, gz);
+      const BoxP &bx = s->ncells ? s->h_cbox[s->h_acell[i]] : s->box;
+      image_of(bx, x[3 * j], x[3 * j + 1], x[3 * j + 2], sx, sy, sz, gx, gy, gz);
       double dx = x[3 * i] - gx, dy = x[3 * i + 1] - gy, dz = x[3 * i + 2] - gz;
       double rsq = dx * dx + dy * dy + dz * dz;
       if (rsq <= cutsq) {

@@ -1,0 +1,203 @@
+// batch.cpp -- multi-cell batches: many small periodic systems (cells) in one
+// set of device arrays, each cell with its own box, evaluated by the same
+// kernels in one launch per kernel.
+//
+// Cells are concatenated: atoms of cell c are coff[c]..coff[c+1]-1, every
+// atom records its cell, and a pair never leaves its cell (images are taken
+// in the cell's own box).  The neighbor build tests each atom against the
+// atoms of its cell under the image shifts that can reach the cutoff; the
+// descriptor, MLP, force and gather kernels are the single-system kernels
+// with the box read per atom.  Energies and virials are summed per cell in a
+// fixed order.  The reference evaluates one LAMMPS system per process
+// (pair_tensormd.cpp:141-184); a batch of C cells gives the same per-cell
+// results as C separate systems.
+#include <cmath>
+#include <vector>
+
+#include "system.h"
+
+using namespace tmd;
+
+struct tmd_batch {
+  tmd_system *s = nullptr;
+};
+
+namespace {
+
+int batch_ok(const tmd_batch *b) {
+  if (!b || !b->s) return fail(TMD_ERR_ARG, "null batch");
+  return TMD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tmd_batch_create(const tmd_model *m, int ncells, const int *natoms, double skin,
+                     tmd_batch **out) {
+  if (!m || !natoms || !out || ncells < 1) return fail(TMD_ERR_ARG, "bad batch arguments");
+  *out = nullptr;
+  long total = 0;
+  for (int c = 0; c < ncells; c++) {
+    if (natoms[c] < 0) return fail(TMD_ERR_ARG, "negative atom count");
+    total += natoms[c];
+  }
+  if (total < 1) return fail(TMD_ERR_ARG, "a batch needs at least one atom");
+  if (total > kMaxAtoms) return fail(TMD_ERR_CAPACITY, "too many atoms for one batch");
+  tmd_system *s = nullptr;
+  int rc = tmd_system_create(m, (int)total, skin, &s);
+  if (rc) return rc;
+  s->ncells = ncells;
+  s->h_coff.assign(ncells + 1, 0);
+  s->h_acell.resize(total);
+  for (int c = 0; c < ncells; c++) {
+    s->h_coff[c + 1] = s->h_coff[c] + natoms[c];
+    for (int a = s->h_coff[c]; a < s->h_coff[c + 1]; a++) s->h_acell[a] = c;
+  }
+  cudaError_t e = dalloc(&s->cbox, ncells);
+  if (e == cudaSuccess) e = dalloc(&s->cgeom, ncells);
+  if (e == cudaSuccess) e = dalloc(&s->acell, total);
+  if (e == cudaSuccess) e = dalloc(&s->coff, ncells + 1);
+  if (e == cudaSuccess) e = dalloc(&s->cell_out, 8 * (size_t)ncells);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(s->acell, s->h_acell.data(), total * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(s->coff, s->h_coff.data(), (ncells + 1) * sizeof(int),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    tmd_system_free(s);
+    return fail(TMD_ERR_CUDA, std::string("batch allocation: ") + cudaGetErrorString(e));
+  }
+  tmd_batch *b = new tmd_batch();
+  b->s = s;
+  *out = b;
+  return TMD_OK;
+}
+
+void tmd_batch_free(tmd_batch *b) {
+  if (!b) return;
+  tmd_system_free(b->s);
+  delete b;
+}
+
+int tmd_batch_system(tmd_batch *b, tmd_system **sys) {
+  if (int rc = batch_ok(b)) return rc;
+  if (!sys) return fail(TMD_ERR_ARG, "null argument");
+  *sys = b->s;
+  return TMD_OK;
+}
+
+int tmd_batch_set_cells(tmd_batch *b, const double *boxes, const int *pbc) {
+  if (int rc = batch_ok(b)) return rc;
+  if (!boxes || !pbc) return fail(TMD_ERR_ARG, "null argument");
+  tmd_system *s = b->s;
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  const int C = s->ncells;
+  const double cut = s->m->h.rmax + s->skin;
+  std::vector<BoxP> hb(C);
+  std::vector<CellGeom> hg(C);
+  for (int c = 0; c < C; c++) {
+    const double *bx = boxes + 9 * (size_t)c;
+    if (!(bx[3] > 0 && bx[4] > 0 && bx[5] > 0))
+      return fail(TMD_ERR_ARG, "cell " + std::to_string(c) + ": box lengths must be > 0");
+    box_setup(hb[c], bx, pbc + 3 * (size_t)c);
+    CellGeom g{};
+    widths(hb[c], g.w);
+    for (int a = 0; a < 3; a++) {
+      g.m[a] = 0;
+      if (!hb[c].pbc[a]) continue;
+      // the largest shift whose slab can come within cut of an atom
+      g.m[a] = (int)std::ceil(cut * (1.0 + 1e-9) / g.w[a] + 1e-6);
+      if (g.m[a] > kShiftR)
+        return fail(TMD_ERR_ARG, "cell " + std::to_string(c) +
+                                     " is too small for the cutoff: more than 3 images "
+                                     "per axis would be needed");
+    }
+    hg[c] = g;
+  }
+  drop_graph(s);
+  TMD_CUDA(cudaMemcpyAsync(s->cbox, hb.data(), C * sizeof(BoxP), cudaMemcpyHostToDevice, s->st));
+  TMD_CUDA(cudaMemcpyAsync(s->cgeom, hg.data(), C * sizeof(CellGeom), cudaMemcpyHostToDevice,
+                           s->st));
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  s->h_cbox = hb;
+  s->have_box = true;
+  s->forces_valid = false;
+  if (s->have_atoms) {
+    int cap = initial_cap(s);
+    if (cap > s->cap) {
+      int rc = alloc_neighbors(s, cap);
+      if (rc) return rc;
+    }
+    return rebuild_now(s);
+  }
+  return TMD_OK;
+}
+
+int tmd_batch_set_atoms(tmd_batch *b, const double *x, const int *type, const double *v) {
+  if (int rc = batch_ok(b)) return rc;
+  return tmd_system_set_atoms(b->s, b->s->h_coff[b->s->ncells], x, type, v);
+}
+
+int tmd_batch_get(tmd_batch *b, double *x, double *v, double *f, int *image) {
+  if (int rc = batch_ok(b)) return rc;
+  return tmd_system_get(b->s, x, v, f, image);
+}
+
+int tmd_batch_compute(tmd_batch *b, double *energy, double *virial, double *f) {
+  if (int rc = batch_ok(b)) return rc;
+  tmd_system *s = b->s;
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before compute");
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  const int C = s->ncells, n = s->n;
+  launch_force_eval(s, 1.0f, false);
+  launch_cell_sum(C, s->coff, s->E, 1, 1.0, s->cell_out, 8, s->st, s->launches);
+  launch_cell_sum(C, s->coff, s->wv, 6, 1.0, s->cell_out + 1, 8, s->st, s->launches);
+  launch_check_finite(n, s->f, nullptr, s->status, s->st, s->launches);
+  TMD_CUDA(cudaGetLastError());
+  std::vector<double> out(8 * (size_t)C);
+  TMD_CUDA(cudaMemcpyAsync(out.data(), s->cell_out, out.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, s->st));
+  if (f) TMD_CUDA(cudaMemcpyAsync(f, s->f, 3 * (size_t)n * sizeof(double),
+                                  cudaMemcpyDeviceToHost, s->st));
+  int rc = read_status(s);
+  if (rc) return rc;
+  const int st = s->h_status[0];
+  if (st & kStatusOverflow) {
+    rc = rebuild_now(s);
+    if (rc) return rc;
+    return tmd_batch_compute(b, energy, virial, f);
+  }
+  if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
+  if (st & kStatusShift) return fail(TMD_ERR_ARG, "a cell is too small for the cutoff");
+  if (st & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside a non-periodic boundary");
+  for (int c = 0; c < C; c++) {
+    if (energy) energy[c] = out[8 * (size_t)c];
+    if (virial)
+      for (int k = 0; k < 6; k++) virial[6 * (size_t)c + k] = out[8 * (size_t)c + 1 + k];
+  }
+  s->forces_valid = true;
+  if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite energy or force");
+  return TMD_OK;
+}
+
+int tmd_batch_nve_run(tmd_batch *b, int nsteps, double dt, int thermo_every,
+                      double *thermo) {
+  if (int rc = batch_ok(b)) return rc;
+  tmd_system *s = b->s;
+  if (nsteps < 0 || !(dt > 0)) return fail(TMD_ERR_ARG, "bad nve arguments");
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before nve_run");
+  if (thermo && thermo_every < 1) return fail(TMD_ERR_ARG, "thermo_every must be >= 1");
+  const long rows = thermo ? 1 + nsteps / thermo_every + ((nsteps % thermo_every) ? 1 : 0) : 0;
+  // row r: (potential, kinetic) energy of every cell
+  auto row_fn = [](tmd_system *q, int r) {
+    double *o = q->thermo_d + 2 * (size_t)r * q->ncells;
+    launch_cell_sum(q->ncells, q->coff, q->E, 1, 1.0, o, 2, q->st, q->launches);
+    launch_kinetic(q->n, q->v, q->elem, q->m->d_mass, q->ke, q->st, q->launches);
+    launch_cell_sum(q->ncells, q->coff, q->ke, 1, 1.0, o + 1, 2, q->st, q->launches);
+  };
+  return run_nve(s, nsteps, dt, thermo ? thermo_every : 0, row_fn, thermo,
+                 2 * rows * s->ncells);
+}
+
+}  // extern "C"

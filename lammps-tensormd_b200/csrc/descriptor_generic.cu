@@ -4,6 +4,6 @@
 
 namespace tmd {
 void launch_descriptor_generic(const DescArgs &a, cudaStream_t st) {
-  launch_descriptor_rk<kRadGeneric>(a, st);
+  launch_descriptor_rk<kRadGeneric, false>(a, st);
 }
 }  // namespace tmd

@@ -48,6 +48,21 @@ __device__ inline PairGeo geo_load(const GeoSlot *s) {
   return g;
 }
 
+// Lanes of thread gt's warp whose global thread index is below nthreads
+// (threads past the last atom return at kernel entry).
+__device__ inline unsigned live_lanes(int gt, long nthreads) {
+  const long rem = nthreads - (long)(gt & ~31);
+  return rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+}
+
+// Box of atom a: the system's box, or in multi-cell mode the box of a's cell.
+template <bool MULTI>
+__device__ inline const BoxP &box_of(const BoxP &box, const BoxP *__restrict__ cbox,
+                                     const int *__restrict__ acell, int a) {
+  if constexpr (MULTI) return cbox[acell[a]];
+  else return box;
+}
+
 // Monomials as FP32 pairs (D2 = ceil(D/2), the last pair padded with 0).
 template <int D, int D2>
 __device__ inline void moments2(float x, float y, float z, float2 M2[D2]) {
@@ -118,12 +133,13 @@ struct PairRing {
   }
 };
 
-template <int TPA, int D, int RK>
+template <int TPA, int D, int RK, bool MULTI>
 __global__ void __launch_bounds__(kPairThreads, 4)
 k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
              const int *__restrict__ elem, const uint32_t *__restrict__ nbr,
              const int *__restrict__ boff, float *__restrict__ P,
-             float *__restrict__ G) {
+             float *__restrict__ G, const BoxP *__restrict__ cbox,
+             const int *__restrict__ acell) {
   constexpr int D2 = (D + 1) / 2;
   __shared__ GeoSlot geo[2 * kPairThreads];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -139,10 +155,14 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
   const int B = kp.B, K = kp.K, M = kp.M;
   const int k0 = 4 * sub;
   const Radial4<RK> R = load_radial4<RK>(kp, k0);
+  const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
   const double xi = x[3 * a], yi = x[3 * a + 1], zi = x[3 * a + 2];
   const uint32_t *row = nbr + (size_t)a * cap;
   const int *bo = boff + (size_t)a * (B + 1);
+  const unsigned live = live_lanes(gt, (long)n * TPA);
   for (int b = 0; b < B; b++) {
+    // keep the warp's groups on the same element block (see k_force)
+    if (b > 0) __syncwarp(live);
     float2 acc[4][D2];
 #pragma unroll
     for (int q = 0; q < 4; q++)
@@ -150,7 +170,7 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
       for (int p = 0; p < D2; p++) acc[q][p] = make_float2(0.f, 0.f);
     pr.begin(x, row, bo[b], bo[b + 1]);
     for (;;) {
-      const int cnt = pr.feed(kp, box, xi, yi, zi, x, row, nullptr);
+      const int cnt = pr.feed(kp, bx, xi, yi, zi, x, row, nullptr);
       if (cnt == 0) break;
       for (int c = 0; c < cnt; c++) {
         const PairGeo g = geo_load(pr.slot(c));
@@ -191,31 +211,33 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
   }
 }
 
-template <int TPA, int RK>
+template <int TPA, int RK, bool MULTI>
 void launch_descriptor_tpa(const DescArgs &a, cudaStream_t st) {
   const int T = kPairThreads;
   long threads = (long)a.n * TPA;
   int grid = (int)((threads + T - 1) / T);
   if (grid < 1) grid = 1;
-#define TMD_DESC_ARGS a.kp, a.box, a.n, a.cap, a.x, a.elem, a.nbr, a.boff, a.P, a.G
+#define TMD_DESC_ARGS a.kp, a.box, a.n, a.cap, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.cbox, a.acell
   switch (a.kp.D) {
-    case 1: k_descriptor<TPA, 1, RK><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;
-    case 4: k_descriptor<TPA, 4, RK><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;
-    case 10: k_descriptor<TPA, 10, RK><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;
-    default: k_descriptor<TPA, 20, RK><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;
+    case 1: k_descriptor<TPA, 1, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;
+    case 4: k_descriptor<TPA, 4, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;
+    case 10: k_descriptor<TPA, 10, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;
+    default: k_descriptor<TPA, 20, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;
   }
 #undef TMD_DESC_ARGS
 }
 
-template <int RK>
+// One radial kind and box mode; each (kind, mode) pair is instantiated in its
+// own translation unit so the variants compile in parallel.
+template <int RK, bool MULTI>
 void launch_descriptor_rk(const DescArgs &a, cudaStream_t st) {
   switch (a.kp.K / 4) {
-    case 1: launch_descriptor_tpa<1, RK>(a, st); break;
-    case 2: launch_descriptor_tpa<2, RK>(a, st); break;
-    case 4: launch_descriptor_tpa<4, RK>(a, st); break;
-    case 8: launch_descriptor_tpa<8, RK>(a, st); break;
-    case 16: launch_descriptor_tpa<16, RK>(a, st); break;
-    default: launch_descriptor_tpa<32, RK>(a, st); break;
+    case 1: launch_descriptor_tpa<1, RK, MULTI>(a, st); break;
+    case 2: launch_descriptor_tpa<2, RK, MULTI>(a, st); break;
+    case 4: launch_descriptor_tpa<4, RK, MULTI>(a, st); break;
+    case 8: launch_descriptor_tpa<8, RK, MULTI>(a, st); break;
+    case 16: launch_descriptor_tpa<16, RK, MULTI>(a, st); break;
+    default: launch_descriptor_tpa<32, RK, MULTI>(a, st); break;
   }
 }
 

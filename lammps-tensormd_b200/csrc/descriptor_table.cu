@@ -3,6 +3,6 @@
 
 namespace tmd {
 void launch_descriptor_table(const DescArgs &a, cudaStream_t st) {
-  launch_descriptor_rk<kRadTable>(a, st);
+  launch_descriptor_rk<kRadTable, false>(a, st);
 }
 }  // namespace tmd

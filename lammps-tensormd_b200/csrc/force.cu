@@ -1,18 +1,29 @@
-// force.cu -- dispatch of the pair-force kernel on the radial kind (Gaussian
-// instantiated here; table and generic kinds in force_table.cu and
-// force_generic.cu) and the atomics-free force gather.
+// force.cu -- dispatch of the pair-force kernel on the radial kind and the
+// box mode (single-box Gaussian instantiated here; the other variants in
+// force_table.cu, force_generic.cu, force_cells.cu and force_cells_other.cu)
+// and the atomics-free force gather.
 #include "force_impl.cuh"
 
 namespace tmd {
 
 void launch_force_table(const ForceArgs &a, cudaStream_t st);
 void launch_force_generic(const ForceArgs &a, cudaStream_t st);
+void launch_force_gauss_cells(const ForceArgs &a, cudaStream_t st);
+void launch_force_table_cells(const ForceArgs &a, cudaStream_t st);
+void launch_force_generic_cells(const ForceArgs &a, cudaStream_t st);
 
 void launch_force(const ForceArgs &a, cudaStream_t st, long &launches) {
+  const bool cells = a.cbox != nullptr;
   switch (radial_kind(a.kp)) {
-    case kRadTable: launch_force_table(a, st); break;
-    case kRadGauss: launch_force_rk<kRadGauss>(a, st); break;
-    default: launch_force_generic(a, st); break;
+    case kRadTable:
+      if (cells) launch_force_table_cells(a, st); else launch_force_table(a, st);
+      break;
+    case kRadGauss:
+      if (cells) launch_force_gauss_cells(a, st); else launch_force_rk<kRadGauss, false>(a, st);
+      break;
+    default:
+      if (cells) launch_force_generic_cells(a, st); else launch_force_generic(a, st);
+      break;
   }
   launches += 1;
 }
@@ -27,7 +38,8 @@ __global__ void k_gather(int n, int cap, int B, const int *__restrict__ boff,
                          const float4 *__restrict__ pdf, const int *__restrict__ rev,
                          const uint32_t *__restrict__ nbr, const double *__restrict__ x,
                          BoxP box, const double *__restrict__ wv,
-                         double *__restrict__ f, double *__restrict__ vatom) {
+                         double *__restrict__ f, double *__restrict__ vatom,
+                         const BoxP *__restrict__ cbox, const int *__restrict__ acell) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gt >> 3, sub = gt & 7;
   if (a >= n) return;
@@ -50,7 +62,8 @@ __global__ void k_gather(int n, int cap, int B, const int *__restrict__ boff,
       int sx, sy, sz;
       shift_decode(int(e >> kAtomBits), sx, sy, sz);
       double gx, gy, gz;
-      image_of(box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sx, sy, sz, gx, gy, gz);
+      image_of(cbox ? cbox[acell[a]] : box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sx, sy,
+               sz, gx, gy, gz);
       double rx = gx - x[3 * a], ry = gy - x[3 * a + 1], rz = gz - x[3 * a + 2];
       v6[0] += rx * q.x;
       v6[1] += ry * q.y;
@@ -89,7 +102,7 @@ void launch_gather(const GatherArgs &a, cudaStream_t st, long &launches) {
   int grid = (int)((threads + T - 1) / T);
   if (grid < 1) grid = 1;
   k_gather<<<grid, T, 0, st>>>(a.n, a.cap, a.B, a.boff, a.pdf, a.rev, a.nbr, a.x,
-                               a.box, a.wv, a.f, a.vatom);
+                               a.box, a.wv, a.f, a.vatom, a.cbox, a.acell);
   launches += 1;
 }
 

@@ -4,6 +4,6 @@
 
 namespace tmd {
 void launch_force_generic(const ForceArgs &a, cudaStream_t st) {
-  launch_force_rk<kRadGeneric>(a, st);
+  launch_force_rk<kRadGeneric, false>(a, st);
 }
 }  // namespace tmd

@@ -26,20 +26,22 @@
 
 namespace tmd {
 
-template <int TPA, int D, int RK>
+template <int TPA, int D, int RK, bool MULTI>
 __global__ void __launch_bounds__(kPairThreads, 3)
 k_force(KParams kp, BoxP box, int n, int cap, float scale,
         const double *__restrict__ x, const int *__restrict__ elem,
         const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
         const float *__restrict__ P, const float *__restrict__ G,
         const float *__restrict__ dEdG, float4 *__restrict__ pdf,
-        double *__restrict__ wv) {
+        double *__restrict__ wv, const BoxP *__restrict__ cbox,
+        const int *__restrict__ acell) {
   constexpr int D2 = (D + 1) / 2;
   __shared__ GeoSlot geo[2 * kPairThreads];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gt / TPA;
   const int sub = gt % TPA;
   if (a >= n) return;
+  const unsigned live = live_lanes(gt, (long)n * TPA);
   const int lane = threadIdx.x & 31;
   PairRing<TPA> pr;
   pr.sub = sub;
@@ -50,11 +52,17 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
   const int B = kp.B, K = kp.K, M = kp.M;
   const int k0 = 4 * sub;
   const Radial4<RK> R = load_radial4<RK>(kp, k0);
+  const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
   const double xi = x[3 * a], yi = x[3 * a + 1], zi = x[3 * a + 2];
   const uint32_t *row = nbr + (size_t)a * cap;
   const int *bo = boff + (size_t)a * (B + 1);
   double w6[6] = {0, 0, 0, 0, 0, 0};
   for (int b = 0; b < B; b++) {
+    // the warp's groups wait for each other at the end of every element
+    // block, so no group runs ahead into the next block while others still
+    // work on this one (that would split the warp across two copies of the
+    // pair loop)
+    if (b > 0) __syncwarp(live);
     const int s0 = bo[b], s1 = bo[b + 1];
     if (s0 == s1) continue;
     // S = dE/dP for this lane's 4 filters, as FP32 pairs over d
@@ -85,7 +93,7 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
     pr.begin(x, row, s0, s1);
     for (;;) {
       // inactive entries get their zero pdf inside feed()
-      const int cnt = pr.feed(kp, box, xi, yi, zi, x, row, pdf_row);
+      const int cnt = pr.feed(kp, bx, xi, yi, zi, x, row, pdf_row);
       if (cnt == 0) break;
       float3 mydf = make_float3(0.f, 0.f, 0.f);
       for (int c = 0; c < cnt; c++) {
@@ -168,31 +176,32 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
   }
 }
 
-template <int TPA, int RK>
+template <int TPA, int RK, bool MULTI>
 void launch_force_tpa(const ForceArgs &a, cudaStream_t st) {
   const int T = kPairThreads;
   long threads = (long)a.n * TPA;
   int grid = (int)((threads + T - 1) / T);
   if (grid < 1) grid = 1;
-#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.dEdG, a.pdf, a.wv
+#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.dEdG, a.pdf, a.wv, a.cbox, a.acell
   switch (a.kp.D) {
-    case 1: k_force<TPA, 1, RK><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
-    case 4: k_force<TPA, 4, RK><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
-    case 10: k_force<TPA, 10, RK><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
-    default: k_force<TPA, 20, RK><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
+    case 1: k_force<TPA, 1, RK, MULTI><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
+    case 4: k_force<TPA, 4, RK, MULTI><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
+    case 10: k_force<TPA, 10, RK, MULTI><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
+    default: k_force<TPA, 20, RK, MULTI><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
   }
 #undef TMD_FORCE_ARGS
 }
 
-template <int RK>
+// One radial kind and box mode per translation unit (parallel compilation).
+template <int RK, bool MULTI>
 void launch_force_rk(const ForceArgs &a, cudaStream_t st) {
   switch (a.kp.K / 4) {
-    case 1: launch_force_tpa<1, RK>(a, st); break;
-    case 2: launch_force_tpa<2, RK>(a, st); break;
-    case 4: launch_force_tpa<4, RK>(a, st); break;
-    case 8: launch_force_tpa<8, RK>(a, st); break;
-    case 16: launch_force_tpa<16, RK>(a, st); break;
-    default: launch_force_tpa<32, RK>(a, st); break;
+    case 1: launch_force_tpa<1, RK, MULTI>(a, st); break;
+    case 2: launch_force_tpa<2, RK, MULTI>(a, st); break;
+    case 4: launch_force_tpa<4, RK, MULTI>(a, st); break;
+    case 8: launch_force_tpa<8, RK, MULTI>(a, st); break;
+    case 16: launch_force_tpa<16, RK, MULTI>(a, st); break;
+    default: launch_force_tpa<32, RK, MULTI>(a, st); break;
   }
 }
 

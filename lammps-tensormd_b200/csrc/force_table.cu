@@ -3,6 +3,6 @@
 
 namespace tmd {
 void launch_force_table(const ForceArgs &a, cudaStream_t st) {
-  launch_force_rk<kRadTable>(a, st);
+  launch_force_rk<kRadTable, false>(a, st);
 }
 }  // namespace tmd

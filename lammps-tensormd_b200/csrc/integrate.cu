@@ -76,6 +76,31 @@ void launch_reduce_scaled(const double *in, int n, double *partial, double *out,
   launches += 2;
 }
 
+// One block per cell (grid-stride over cells), a fixed tree per block.
+__global__ void k_cell_sum(int ncells, const int *__restrict__ coff,
+                           const double *__restrict__ in, int ncomp, double scale,
+                           double *__restrict__ out, int ostride) {
+  __shared__ double sh[kRedThreads];
+  for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
+    const int a0 = coff[c], a1 = coff[c + 1];
+    for (int k = 0; k < ncomp; k++) {
+      double s = 0.0;
+      for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) s += in[(size_t)a * ncomp + k];
+      s = block_sum(s, sh);
+      if (threadIdx.x == 0) out[(size_t)c * ostride + k] = s * scale;
+    }
+  }
+}
+
+void launch_cell_sum(int ncells, const int *coff, const double *in, int ncomp,
+                     double scale, double *out, int ostride, cudaStream_t st,
+                     long &launches) {
+  int g = ncells < 148 * 16 ? ncells : 148 * 16;
+  if (g < 1) g = 1;
+  k_cell_sum<<<g, kRedThreads, 0, st>>>(ncells, coff, in, ncomp, scale, out, ostride);
+  launches += 1;
+}
+
 __global__ void k_scale_copy(const double *__restrict__ in, int n, double scale,
                              double *__restrict__ out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;

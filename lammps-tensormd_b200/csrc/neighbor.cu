@@ -18,6 +18,8 @@
 //
 // Every kernel takes `flag` and returns at once when no rebuild is pending, so
 // the sequence can sit inside a captured CUDA graph of the MD step.
+#include <cmath>
+
 #include "tmd_kernels.h"
 
 namespace tmd {
@@ -50,15 +52,12 @@ __global__ void k_nb_zero(int ncell, int *cell_count, const int *flag) {
     cell_count[c] = 0;
 }
 
-// Wrap atoms into the cell (Domain::pbc()), then bin them.
-__global__ void k_nb_bin(int n, double *__restrict__ x, int *__restrict__ image,
-                         BoxP box, BinP bin, int *__restrict__ cell_of,
-                         int *__restrict__ cell_count, int *status,
-                         const int *flag) {
-  if (!*flag) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += gridDim.x * blockDim.x) {
-  double px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
+// Wrap atom i back into the periodic cell (Domain::pbc()), counting the
+// crossings in image[]; returns the wrapped position.
+__device__ inline void wrap_atom(const BoxP &box, int i, double *__restrict__ x,
+                                 int *__restrict__ image, double &px, double &py,
+                                 double &pz) {
+  px = x[3 * i]; py = x[3 * i + 1]; pz = x[3 * i + 2];
   if (!box.triclinic) {
     double lo[3] = {box.lo[0], box.lo[1], box.lo[2]};
     double prd[3] = {box.xprd, box.yprd, box.zprd};
@@ -90,6 +89,18 @@ __global__ void k_nb_bin(int n, double *__restrict__ x, int *__restrict__ image,
     }
   }
   x[3 * i] = px; x[3 * i + 1] = py; x[3 * i + 2] = pz;
+}
+
+// Wrap atoms into the cell, then bin them.
+__global__ void k_nb_bin(int n, double *__restrict__ x, int *__restrict__ image,
+                         BoxP box, BinP bin, int *__restrict__ cell_of,
+                         int *__restrict__ cell_count, int *status,
+                         const int *flag) {
+  if (!*flag) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+  double px, py, pz;
+  wrap_atom(box, i, x, image, px, py, pz);
   double f[3];
   frac_of(box, px, py, pz, f[0], f[1], f[2]);
   int c3[3];
@@ -271,6 +282,93 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
   }
 }
 
+// ---------------------------------------------------------------------
+// Multi-cell batches: many small periodic cells, each in its own box.  Atoms
+// of cell c are coff[c]..coff[c+1]-1 and see only atoms of their own cell
+// and its images.  Cells hold a few hundred atoms, so instead of bins each
+// atom tests every atom of its cell under every image shift that can reach
+// the cutoff.  A shift s on axis a is skipped when the slab of fractional
+// coordinates [s, s + 1) lies farther than cut from atom i along a: the
+// distance between planes of constant fractional coordinate is |df_a| w_a
+// (w_a = perpendicular width), a lower bound of the true distance.  The
+// kept set is the same (j, shift) set as the binned build, with the same
+// FP64 image construction and no-FMA rsq.
+// ---------------------------------------------------------------------
+__global__ void k_nbc_wrap(int n, double *__restrict__ x, int *__restrict__ image,
+                           const BoxP *__restrict__ cbox, const int *__restrict__ acell,
+                           int *status, const int *flag) {
+  if (!*flag) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const BoxP &box = cbox[acell[i]];
+    double px, py, pz, f[3];
+    wrap_atom(box, i, x, image, px, py, pz);
+    frac_of(box, px, py, pz, f[0], f[1], f[2]);
+    for (int a = 0; a < 3; a++)
+      if (!box.pbc[a] && (f[a] < 0.0 || f[a] > 1.0)) atomicOr(status, kStatusOutside);
+  }
+}
+
+// One warp per atom; entries in (shift, j) order, compacted with a ballot.
+__global__ void k_nbc_build(int n, const double *__restrict__ x,
+                            const BoxP *__restrict__ cbox,
+                            const CellGeom *__restrict__ cgeom,
+                            const int *__restrict__ acell, const int *__restrict__ coff,
+                            double cut, double cutsq, int cap, uint32_t *__restrict__ tmp,
+                            int *__restrict__ nraw, int *status, int *maxneed,
+                            const int *flag) {
+  if (!*flag) return;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+    const int c = acell[i];
+    const BoxP &box = cbox[c];
+    const CellGeom &cg = cgeom[c];
+    const int j0 = coff[c], j1 = coff[c + 1];
+    const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
+    double fi[3];
+    frac_of(box, xi, yi, zi, fi[0], fi[1], fi[2]);
+    // shift range per axis: keep s unless the slab [s, s+1) is beyond cut
+    int lo[3], hi[3];
+    const double reach = cut * (1.0 + 1e-9), eps = 1e-6;
+    for (int a = 0; a < 3; a++) {
+      lo[a] = 0; hi[a] = 0;
+      if (!box.pbc[a]) continue;
+      lo[a] = -cg.m[a]; hi[a] = cg.m[a];
+      while (lo[a] < 0 && (fi[a] - (lo[a] + 1) - eps) * cg.w[a] > reach) lo[a]++;
+      while (hi[a] > 0 && (hi[a] - fi[a] - eps) * cg.w[a] > reach) hi[a]--;
+    }
+    uint32_t *row = tmp + (size_t)i * cap;
+    int out = 0;
+    for (int sz = lo[2]; sz <= hi[2]; sz++)
+      for (int sy = lo[1]; sy <= hi[1]; sy++)
+        for (int sx = lo[0]; sx <= hi[0]; sx++) {
+          const bool self_img = (sx == 0 && sy == 0 && sz == 0);
+          const int code = shift_code(sx, sy, sz);
+          for (int jb = j0; jb < j1; jb += 32) {
+            const int j = jb + lane;
+            bool hit = false;
+            if (j < j1 && !(self_img && j == i)) {
+              double gx, gy, gz;
+              image_of(box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sx, sy, sz, gx, gy, gz);
+              hit = rsq_nofma(xi - gx, yi - gy, zi - gz) <= cutsq;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, hit);
+            const int pos = out + __popc(bal & ((1u << lane) - 1u));
+            if (hit && pos < cap) row[pos] = nb_pack(j, code);
+            out += __popc(bal);
+          }
+        }
+    if (lane == 0) {
+      nraw[i] = out;
+      if (out > cap) {
+        atomicOr(status, kStatusOverflow);
+        atomicMax(maxneed, out);
+      }
+    }
+  }
+}
+
 // One warp per atom: bitonic sort of the row by (block, packed key) in
 // shared memory, then block offsets.
 __global__ void k_nb_sort(int n, int B, KParams kp, const int *__restrict__ elem,
@@ -382,18 +480,27 @@ void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
   const int kMaxGrid = 148 * 8;
   auto cap_grid = [&](long g) { return (int)(g < 1 ? 1 : (g > kMaxGrid ? kMaxGrid : g)); };
   int gn = cap_grid((a.n + T - 1) / T);
-  int gc = cap_grid((a.bin.ncell + T - 1) / T);
-  k_nb_zero<<<gc, T, 0, st>>>(a.bin.ncell, a.cell_count, a.flag);
-  k_nb_bin<<<gn, T, 0, st>>>(a.n, a.x, a.image, a.box, a.bin, a.cell_of,
-                             a.cell_count, a.status, a.flag);
-  k_nb_scan<<<1, 1024, 0, st>>>(a.bin.ncell, a.cell_count, a.cell_start,
-                                a.cell_cursor, a.flag);
-  k_nb_fill<<<gn, T, 0, st>>>(a.n, a.cell_of, a.cell_cursor, a.cell_atoms, a.flag);
-  k_nb_cellsort<<<gc, T, 0, st>>>(a.bin.ncell, a.cell_start, a.cell_atoms, a.flag);
   int gw = cap_grid(((long)a.n * 32 + T - 1) / T);
-  k_nb_build<<<gw, T, 0, st>>>(a.n, a.x, a.box, a.bin, a.cell_of, a.cell_start,
-                               a.cell_atoms, a.cutsq, a.cap, a.tmp, a.nraw,
-                               a.status, a.maxneed, a.flag);
+  if (a.ncells > 0) {
+    k_nbc_wrap<<<gn, T, 0, st>>>(a.n, a.x, a.image, a.cbox, a.acell, a.status, a.flag);
+    k_nbc_build<<<gw, T, 0, st>>>(a.n, a.x, a.cbox, a.cgeom, a.acell, a.coff,
+                                  std::sqrt(a.cutsq), a.cutsq, a.cap, a.tmp, a.nraw,
+                                  a.status, a.maxneed, a.flag);
+    launches += 2;
+  } else {
+    int gc = cap_grid((a.bin.ncell + T - 1) / T);
+    k_nb_zero<<<gc, T, 0, st>>>(a.bin.ncell, a.cell_count, a.flag);
+    k_nb_bin<<<gn, T, 0, st>>>(a.n, a.x, a.image, a.box, a.bin, a.cell_of,
+                               a.cell_count, a.status, a.flag);
+    k_nb_scan<<<1, 1024, 0, st>>>(a.bin.ncell, a.cell_count, a.cell_start,
+                                  a.cell_cursor, a.flag);
+    k_nb_fill<<<gn, T, 0, st>>>(a.n, a.cell_of, a.cell_cursor, a.cell_atoms, a.flag);
+    k_nb_cellsort<<<gc, T, 0, st>>>(a.bin.ncell, a.cell_start, a.cell_atoms, a.flag);
+    k_nb_build<<<gw, T, 0, st>>>(a.n, a.x, a.box, a.bin, a.cell_of, a.cell_start,
+                                 a.cell_atoms, a.cutsq, a.cap, a.tmp, a.nraw,
+                                 a.status, a.maxneed, a.flag);
+    launches += 6;
+  }
   int wpb = a.capp >= 1024 ? 1 : (a.capp >= 512 ? 2 : 4);
   size_t smem = (size_t)wpb * a.capp * sizeof(unsigned long long);
   k_nb_sort<<<cap_grid((a.n + wpb - 1) / wpb), 32 * wpb, smem, st>>>(
@@ -402,7 +509,7 @@ void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
                              a.flag);
   k_nb_finish<<<gn, T, 0, st>>>(a.n, a.x, a.xbuild, a.flag);
   k_nb_clear<<<1, 1, 0, st>>>(a.flag);
-  launches += 10;
+  launches += 4;
 }
 
 void launch_neighbor_check(int n, const double *x, const double *xbuild,

@@ -1,0 +1,133 @@
+// system.h -- host-side state behind the opaque handles of tmd_b200.h, shared
+// by the translation units of the C ABI (abi.cpp: model, system, NVE;
+// batch.cpp: multi-cell batches).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/tmd_b200.h"
+#include "model.h"
+#include "tmd_kernels.h"
+
+struct tmd_model {
+  int device = 0;
+  tmd::HostModel h;
+  tmd::KParams kp;
+  float *d_table = nullptr;
+  std::vector<float *> d_buf;   // weights and biases
+  tmd::MlpLayer *d_layers = nullptr;
+  tmd::MlpTcLayer *d_tc_layers = nullptr;  // tensor-core MLP (precision bf16)
+  size_t tc_smem = 0;
+  bool tc_dz_bf16 = false;
+  int tc_np = 1;
+  int maxh = 1;
+  double *d_mass = nullptr;     // per element
+  int mlp_tr = 64;
+  size_t mlp_smem = 0;
+  int nsys = 0;            // systems created from this model and not yet freed
+  bool released = false;   // tmd_model_free called while nsys > 0
+};
+
+struct tmd_system {
+  const tmd_model *m = nullptr;
+  cudaStream_t st = nullptr;
+  long launches = 0;
+  int natoms_cap = 0, n = 0;
+  double skin = 1.0;
+  bool have_box = false, have_atoms = false, have_v = false;
+  bool forces_valid = false;
+  tmd::BoxP box{};
+  tmd::BinP bin{};
+  int cap = 0, capp = 0;  // neighbor entries per atom, pow2 >= cap
+  int ncell_alloc = 0;
+  // multi-cell batch (ncells > 0): cell c holds atoms coff[c]..coff[c+1]-1
+  // in its own periodic box; box/bin above are unused
+  int ncells = 0;
+  std::vector<int> h_coff, h_acell;
+  std::vector<tmd::BoxP> h_cbox;
+  tmd::BoxP *cbox = nullptr;
+  tmd::CellGeom *cgeom = nullptr;
+  int *acell = nullptr, *coff = nullptr;
+  double *cell_out = nullptr;  // [ncells][8]: energy, virial[6], spare
+  // device state
+  double *x = nullptr, *v = nullptr, *f = nullptr, *xbuild = nullptr;
+  int *image = nullptr, *elem = nullptr;
+  int *cell_of = nullptr, *cell_count = nullptr, *cell_start = nullptr,
+      *cell_cursor = nullptr, *cell_atoms = nullptr;
+  uint32_t *tmp = nullptr, *nbr = nullptr;
+  int *nraw = nullptr, *boff = nullptr, *rev = nullptr;
+  float *P = nullptr, *G = nullptr, *dEdG = nullptr;
+  double *E = nullptr;
+  float4 *pdf = nullptr;
+  double *wv = nullptr, *eatom = nullptr, *vatom = nullptr, *ke = nullptr;
+  double *partial = nullptr, *scal = nullptr;  // scal: [0] pe, [1..6] virial, [7] ke
+  int *flag = nullptr, *status = nullptr, *maxneed = nullptr;
+  int *perm = nullptr, *tiles = nullptr;
+  int ntiles = 0;
+  double *thermo_d = nullptr;
+  long thermo_alloc = 0;
+  // host
+  std::vector<int> h_elem;
+  double *h_scal = nullptr;  // pinned [8]
+  int *h_status = nullptr;   // pinned [2]
+  // kernel timing
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+  long prof_n[TMD_NPROF] = {0};
+  double prof_ms[TMD_NPROF] = {0};
+  cudaEvent_t cur_start = nullptr;
+  // captured MD step (velocity Verlet + rebuild check/rebuild + force)
+  cudaGraphExec_t step_exec = nullptr;
+  double step_dt = 0.0;
+  long step_launches = 0;
+};
+
+namespace tmd {
+
+// Record msg as the thread's last error and return code.
+int fail(int code, const std::string &msg);
+
+#define TMD_CUDA(call)                                                        \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return ::tmd::fail(TMD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T));
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+void drop_graph(tmd_system *s);
+void box_setup(BoxP &b, const double bx[9], const int pbc[3]);
+void widths(const BoxP &b, double w[3]);
+int alloc_neighbors(tmd_system *s, int cap);
+int initial_cap(tmd_system *s);
+int read_status(tmd_system *s);
+int clear_status(tmd_system *s);
+int rebuild_now(tmd_system *s);
+void launch_force_eval(tmd_system *s, float scale, bool want_vatom);
+// Make sure s->thermo_d holds count doubles.
+int thermo_reserve(tmd_system *s, long count);
+// Velocity Verlet for nsteps on the device (graph-captured step).  thermo_row(r)
+// enqueues thermo row r; it is called for the starting state (r = 0) and
+// every thermo_every steps and at the last step when thermo_every > 0.  On
+// success the first thermo_count doubles of s->thermo_d are copied to thermo.
+int run_nve(tmd_system *s, int nsteps, double dt, int thermo_every,
+            void (*thermo_row)(tmd_system *, int), double *thermo, long thermo_count);
+
+}  // namespace tmd

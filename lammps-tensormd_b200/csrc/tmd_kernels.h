@@ -12,6 +12,14 @@ constexpr int kStatusOutside = 4;    // atom outside a non-periodic boundary
 constexpr int kStatusNonfinite = 8;  // NaN/Inf energy or force
 constexpr int kStatusTimeout = 16;   // a bounded device wait gave up
 
+// Per-cell constants of the multi-cell neighbor build: perpendicular widths
+// and the largest image shift per axis (0 on non-periodic axes).
+struct CellGeom {
+  double w[3];
+  int m[3];
+  int pad;
+};
+
 struct NbArgs {
   int n, B, cap, capp;
   KParams kp;
@@ -25,6 +33,12 @@ struct NbArgs {
   uint32_t *tmp;
   int *nraw;
   uint32_t *nbr;
+  // multi-cell mode (ncells > 0): atoms of cell c are coff[c]..coff[c+1]-1,
+  // each cell periodic in its own box; bins are not used
+  int ncells;
+  const BoxP *cbox;
+  const CellGeom *cgeom;
+  const int *acell, *coff;
   int *boff;
   int *rev;
   double *xbuild;
@@ -47,6 +61,8 @@ struct DescArgs {
   const uint32_t *nbr;
   const int *boff;
   float *P, *G;
+  const BoxP *cbox;   // multi-cell mode: box of each cell, else nullptr
+  const int *acell;   // multi-cell mode: cell of each atom
 };
 void launch_descriptor(const DescArgs &a, cudaStream_t st, long &launches);
 
@@ -121,6 +137,8 @@ struct ForceArgs {
   const float *P, *G, *dEdG;
   float4 *pdf;
   double *wv;  // [n][6] per-atom sum of -r_ij (x) df over own pairs
+  const BoxP *cbox;   // multi-cell mode (as DescArgs)
+  const int *acell;
 };
 void launch_force(const ForceArgs &a, cudaStream_t st, long &launches);
 
@@ -136,6 +154,8 @@ struct GatherArgs {
   const double *wv;
   double *f;
   double *vatom;   // nullable
+  const BoxP *cbox;   // multi-cell mode (as DescArgs)
+  const int *acell;
 };
 void launch_gather(const GatherArgs &a, cudaStream_t st, long &launches);
 
@@ -145,6 +165,11 @@ void launch_reduce_f64(const double *in, int n, int ncomp, double *partial,
                        double *out, cudaStream_t st, long &launches);
 void launch_reduce_scaled(const double *in, int n, double *partial, double *out,
                           double scale, cudaStream_t st, long &launches);
+// Per-cell sums in a fixed order: out[c*ostride + k] = scale * sum over the
+// atoms a of cell c of in[a*ncomp + k].
+void launch_cell_sum(int ncells, const int *coff, const double *in, int ncomp,
+                     double scale, double *out, int ostride, cudaStream_t st,
+                     long &launches);
 void launch_scale_copy(const double *in, int n, double scale, double *out,
                        cudaStream_t st, long &launches);
 

@@ -39,6 +39,14 @@ SIGNATURES = [
     ("tmd_profile_enable", _c_int, [_vp, _c_int]),
     ("tmd_profile_read", _c_int, [_vp, _pl, _pd, _c_int]),
     ("tmd_last_error", _c_int, [ctypes.c_char_p, _c_int]),
+    ("tmd_batch_create", _c_int, [_vp, _c_int, _pi, _c_double, ctypes.POINTER(_vp)]),
+    ("tmd_batch_free", None, [_vp]),
+    ("tmd_batch_system", _c_int, [_vp, ctypes.POINTER(_vp)]),
+    ("tmd_batch_set_cells", _c_int, [_vp, _pd, _pi]),
+    ("tmd_batch_set_atoms", _c_int, [_vp, _pd, _pi, _pd]),
+    ("tmd_batch_get", _c_int, [_vp, _pd, _pd, _pd, _pi]),
+    ("tmd_batch_compute", _c_int, [_vp, _pd, _pd, _pd]),
+    ("tmd_batch_nve_run", _c_int, [_vp, _c_int, _c_double, _c_int, _pd]),
     ("tmd_neighbor_list_noalloc", _c_int, [_vp, _c_int, _pd, _pi, _c_double, _c_int, _vp,
                                            _vp, _vp]),
 ]

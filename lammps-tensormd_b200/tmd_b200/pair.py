@@ -76,9 +76,9 @@ class TensorMDSystem:
         self.n = 0
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self, "_owned", True):
             self.lib.tmd_system_free(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -170,6 +170,80 @@ class TensorMDSystem:
         check(self.lib.tmd_profile_read(self.h, n.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
                                         _dp(ms), int(bool(reset))))
         return {f: (int(c), float(t)) for f, c, t in zip(self.PROFILE_FAMILIES, n, ms)}
+
+
+class TensorMDBatch:
+    """Many small periodic cells evaluated together (tmd_batch_*).
+
+    natoms[c] atoms per cell; atom arrays are concatenated cell by cell."""
+
+    def __init__(self, model: TensorMDModel, natoms, skin: float = 1.0):
+        self.model = model
+        self.lib = model.lib
+        na = np.ascontiguousarray(natoms, dtype=np.int32)
+        self.natoms = na
+        self.ncells = len(na)
+        self.n = int(na.sum())
+        self.offsets = np.concatenate([[0], np.cumsum(na)]).astype(np.int64)
+        h = ctypes.c_void_p()
+        check(self.lib.tmd_batch_create(model.h, self.ncells, _ip(na), float(skin),
+                                        ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tmd_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_cells(self, boxes, pbc=None):
+        b = np.ascontiguousarray(boxes, dtype=np.float64).reshape(self.ncells, 9)
+        p = (np.ones((self.ncells, 3), dtype=np.int32) if pbc is None
+             else np.ascontiguousarray(pbc, dtype=np.int32).reshape(self.ncells, 3))
+        check(self.lib.tmd_batch_set_cells(self.h, _dp(b), _ip(p)))
+
+    def set_atoms(self, x, types, v=None):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n, 3)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        vv = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        check(self.lib.tmd_batch_set_atoms(self.h, _dp(x), _ip(t), _dp(vv)))
+
+    def get(self):
+        x, v, f = (np.zeros((self.n, 3)) for _ in range(3))
+        img = np.zeros((self.n, 3), dtype=np.int32)
+        check(self.lib.tmd_batch_get(self.h, _dp(x), _dp(v), _dp(f), _ip(img)))
+        return x, v, f, img
+
+    def compute(self, forces=True):
+        e = np.zeros(self.ncells)
+        vir = np.zeros((self.ncells, 6))
+        f = np.zeros((self.n, 3)) if forces else None
+        check(self.lib.tmd_batch_compute(self.h, _dp(e), _dp(vir), _dp(f)))
+        return dict(energy=e, virial=vir, f=f)
+
+    def nve_run(self, nsteps, dt, thermo_every=0):
+        th = None
+        if thermo_every:
+            rows = 1 + nsteps // thermo_every + (1 if nsteps % thermo_every else 0)
+            th = np.zeros((rows, self.ncells, 2))
+        check(self.lib.tmd_batch_nve_run(self.h, int(nsteps), float(dt), int(thermo_every),
+                                         _dp(th)))
+        return th
+
+    def system(self) -> "TensorMDSystem":
+        """The underlying system handle (stream, launches, profile, lists)."""
+        h = ctypes.c_void_p()
+        check(self.lib.tmd_batch_system(self.h, ctypes.byref(h)))
+        s = TensorMDSystem.__new__(TensorMDSystem)
+        s.model, s.lib, s.h, s.n = self.model, self.lib, h, self.n
+        s._owned = False  # the batch frees it
+        s._batch = self
+        return s
 
 
 class PairTensorMD:

@@ -142,6 +142,36 @@ def build_system(kind, a, cells, *, sigma=0.0, T=0.0, nelt=1, seed=7, masses=Non
     return x, types, box, v
 
 
+def batch_cells(ncells=4096, natoms=256, *, nelt=2, sigma=0.1, t_range=(300.0, 1200.0),
+                seed=11, masses=None):
+    """Multi-cell workload: half FCC (a = 3.6 A, 4x4x4 cells), half BCC
+    (a = 2.87 A, 4x4x8 cells), natoms = 256 atoms each, random equal-fraction
+    occupancy of nelt elements, Gaussian displacements sigma, per-cell
+    temperature uniform in t_range.  Returns per-cell lists
+    (x, types, box, v) and the concatenated arrays."""
+    if natoms != 256:
+        raise ValueError("the FCC/BCC cells of this workload hold 256 atoms")
+    rng = np.random.default_rng(seed)
+    xs, ts, boxes, vs = [], [], [], []
+    m_el = np.asarray(masses if masses is not None
+                      else [MASSES[s] for s in SYMBOLS[:nelt]], dtype=np.float64)
+    for c in range(ncells):
+        if c % 2 == 0:
+            x, box = lattice("fcc", 3.6, 4, 4, 4)
+        else:
+            x, box = lattice("bcc", 2.87, 4, 4, 8)
+        n = len(x)
+        x = wrap(x + rng.normal(0.0, sigma, size=x.shape), box)
+        t = (np.arange(n) % nelt) + 1
+        rng.shuffle(t)
+        T = rng.uniform(*t_range)
+        v = maxwell(m_el[t - 1], T, rng)
+        xs.append(x); ts.append(t.astype(np.int32)); boxes.append(box); vs.append(v)
+    return dict(x=np.concatenate(xs), types=np.concatenate(ts), boxes=np.stack(boxes),
+                v=np.concatenate(vs), natoms=np.full(ncells, 256, dtype=np.int32),
+                cells=list(zip(xs, ts, boxes, vs)))
+
+
 def config(name):
     """The workloads this path is measured on (shapes from the task spec)."""
     if name == "fcc4k":  # plain CPU config: 4,000 atoms
@@ -152,6 +182,10 @@ def config(name):
         return dict(kind="bcc", a=2.87, cells=(40, 40, 40), sigma=0.08, T=600.0, nelt=1,
                     pot=dict(nelt=1, num_filters=16, rc=6.0, max_moment=3,
                              hidden=(64, 64), actfn=2))
+    if name == "cells4096":  # batched config: 4,096 cells x 256 atoms, 2 elements
+        return dict(kind="cells", ncells=4096, natoms=256, sigma=0.1, t_range=(300.0, 1200.0),
+                    nelt=2, pot=dict(nelt=2, num_filters=16, rc=6.0, max_moment=3,
+                                     hidden=(64, 64), actfn=2))
     if name == "alloy432k":  # precision config: 4 elements, 432,000 atoms
         return dict(kind="fcc", a=3.6, cells=(60, 60, 30), sigma=0.05, T=300.0, nelt=4,
                     pot=dict(nelt=4, num_filters=32, rc=6.5, max_moment=3,
