@@ -282,10 +282,13 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
     launch_mlp_fp32(ma, s->st, s->launches);
   }
   prof_end(s, 2);
+  prof_begin(s);
+  launch_dedp(s->n, m->kp, s->P, s->G, s->dEdG, s->st, s->launches);  // P becomes S
+  prof_end(s, 7);
   ForceArgs fa{};
   fa.n = s->n; fa.cap = s->cap; fa.kp = m->kp; fa.box = s->box; fa.scale = scale;
-  fa.x = s->x; fa.elem = s->elem; fa.nbr = s->nbr; fa.boff = s->boff; fa.P = s->P;
-  fa.G = s->G; fa.dEdG = s->dEdG; fa.pdf = s->pdf; fa.wv = s->wv;
+  fa.x = s->x; fa.elem = s->elem; fa.nbr = s->nbr; fa.boff = s->boff; fa.S = s->P;
+  fa.pdf = s->pdf; fa.wv = s->wv;
   fa.cbox = d.cbox; fa.acell = s->acell;
   prof_begin(s);
   launch_force(fa, s->st, s->launches);

@@ -25,7 +25,8 @@ void launch_descriptor(const DescArgs &a, cudaStream_t st, long &launches) {
       if (cells) launch_descriptor_generic_cells(a, st); else launch_descriptor_generic(a, st);
       break;
   }
-  launches += 1;
+  launch_invariants(a, st);
+  launches += 2;
 }
 
 }  // namespace tmd

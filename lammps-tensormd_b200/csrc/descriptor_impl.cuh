@@ -15,8 +15,9 @@
 // positions one chunk ahead, so the gather latency overlaps the arithmetic.
 // Nothing per pair goes to global memory.
 //
-// Output layout: P[n][B][K][D] (kept for the force kernel), G[n][B*K*M] (the
-// MLP input rows, m fastest, as TensorMD::get_G).
+// Output layout: P[n][B][K][D] (kept for the force kernel), then
+// k_invariants forms G[n][B*K*M] (the MLP input rows, m fastest, as
+// TensorMD::get_G) from P.
 #pragma once
 
 #include "pair_math.cuh"
@@ -152,7 +153,7 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
   pr.gshift = lane & ~(TPA - 1);
   pr.gmask = PairRing<TPA>::kBits << pr.gshift;
   pr.ring = geo + 2 * (threadIdx.x - sub);  // the ring of this atom's group
-  const int B = kp.B, K = kp.K, M = kp.M;
+  const int B = kp.B, K = kp.K;
   const int k0 = 4 * sub;
   const Radial4<RK> R = load_radial4<RK>(kp, k0);
   const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
@@ -187,27 +188,58 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
       }
       pr.pop(cnt);
     }
-    // P rows of this lane: 4 filters x D values, contiguous
+    // P rows of this lane: 4 filters x D values, contiguous (G = T P^2 is
+    // formed by k_invariants)
     float *Pp = P + (((size_t)a * B + b) * K + k0) * D;
+    if constexpr (D % 2 == 0) {
+      float2 *P2 = reinterpret_cast<float2 *>(Pp);
 #pragma unroll
-    for (int q = 0; q < 4; q++)
+      for (int q = 0; q < 4; q++)
 #pragma unroll
-      for (int d = 0; d < D; d++) Pp[q * D + d] = (d & 1) ? acc[q][d >> 1].y : acc[q][d >> 1].x;
-    // G = T P^2 for the 4 filters
-    float *Gp = G + (size_t)a * kp.nin + ((size_t)b * K + k0) * M;
+        for (int p = 0; p < D2; p++) P2[q * D2 + p] = acc[q][p];
+    } else {
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      for (int m = 0; m < M; m++) {
-        float s = 0.f;
+      for (int q = 0; q < 4; q++)
 #pragma unroll
-        for (int d = 0; d < D; d++) {
-          float pv = (d & 1) ? acc[q][d >> 1].y : acc[q][d >> 1].x;
-          s = fmaf(kp.T[m * D + d], pv * pv, s);
-        }
-        if (m == 0) s = copysignf(1.f, acc[q][0].x) * sqrtf(s);
-        Gp[q * M + m] = s;
-      }
+        for (int d = 0; d < D; d++) Pp[q * D + d] = (d & 1) ? acc[q][d >> 1].y : acc[q][d >> 1].x;
     }
+  }
+}
+
+// G[b,k,m] = sum_d T[m,d] P[b,k,d]^2, G[b,k,0] = sign(P0) sqrt(.)
+// (kernel_1_fused_device, kernel.cu:1028-1061): one thread per output, the D
+// values of the row from L1, coalesced writes in the MLP row layout.
+template <int D, int M>
+__global__ void k_invariants(long nout, KParams kp, const float *__restrict__ P,
+                             float *__restrict__ G) {
+  __shared__ float sT[M * D];  // lanes read different m: no per-lane param index
+  for (int i = threadIdx.x; i < M * D; i += blockDim.x) sT[i] = kp.T[i];
+  __syncthreads();
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nout) return;
+  const long row = e / M;
+  const int m = (int)(e - row * M);
+  const float *p = P + row * D;
+  float s = 0.f;
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    const float pv = __ldg(p + d);
+    s = fmaf(sT[m * D + d], pv * pv, s);
+  }
+  if (m == 0) s = copysignf(1.f, __ldg(p)) * sqrtf(s);
+  G[e] = s;
+}
+
+inline void launch_invariants(const DescArgs &a, cudaStream_t st) {
+  const long nout = (long)a.n * a.kp.B * a.kp.K * a.kp.M;
+  if (nout == 0) return;
+  const int T = 256;
+  const unsigned grid = (unsigned)((nout + T - 1) / T);
+  switch (a.kp.D) {
+    case 1: k_invariants<1, 1><<<grid, T, 0, st>>>(nout, a.kp, a.P, a.G); break;
+    case 4: k_invariants<4, 2><<<grid, T, 0, st>>>(nout, a.kp, a.P, a.G); break;
+    case 10: k_invariants<10, 3><<<grid, T, 0, st>>>(nout, a.kp, a.P, a.G); break;
+    default: k_invariants<20, 4><<<grid, T, 0, st>>>(nout, a.kp, a.P, a.G); break;
   }
 }
 

@@ -7,6 +7,7 @@
 //   U_k = sum_d S[k,d] M_d, V_d = sum_k S[k,d] H_k
 //   df = (sum_k U_k dH_k) u + sum_d V_d dM_d/dx_j     (F1 + F2, kernel.cu:541-631,
 //                                                       tensor_ops.cpp:126-190,470-535)
+// S is formed by k_dedp (force.cu) over P in place; this kernel loads it.
 // The reference writes U, V, F1 and F2 per padded slot and scatters df with
 // FP64 atomics (kernel.cu:1639-1758).  Here S stays in registers (4 filters x D
 // per lane as FP32 pairs, TPA = K/4 lanes per atom), U and V are packed FP32x2
@@ -31,8 +32,7 @@ __global__ void __launch_bounds__(kPairThreads, 3)
 k_force(KParams kp, BoxP box, int n, int cap, float scale,
         const double *__restrict__ x, const int *__restrict__ elem,
         const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
-        const float *__restrict__ P, const float *__restrict__ G,
-        const float *__restrict__ dEdG, float4 *__restrict__ pdf,
+        const float *__restrict__ S, float4 *__restrict__ pdf,
         double *__restrict__ wv, const BoxP *__restrict__ cbox,
         const int *__restrict__ acell) {
   constexpr int D2 = (D + 1) / 2;
@@ -49,7 +49,7 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
   pr.gmask = PairRing<TPA>::kBits << pr.gshift;
   pr.ring = geo + 2 * (threadIdx.x - sub);
   const unsigned gmask = pr.gmask;
-  const int B = kp.B, K = kp.K, M = kp.M;
+  const int B = kp.B, K = kp.K;
   const int k0 = 4 * sub;
   const Radial4<RK> R = load_radial4<RK>(kp, k0);
   const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
@@ -65,28 +65,24 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
     if (b > 0) __syncwarp(live);
     const int s0 = bo[b], s1 = bo[b + 1];
     if (s0 == s1) continue;
-    // S = dE/dP for this lane's 4 filters, as FP32 pairs over d
+    // S = dE/dP of this lane's 4 filters (4 x D contiguous floats), as FP32
+    // pairs over d
     float2 S2[4][D2];
     {
-      const float *Pp = P + (((size_t)a * B + b) * K + k0) * D;
-      const float *Gp = G + (size_t)a * kp.nin + ((size_t)b * K + k0) * M;
-      const float *dGp = dEdG + (size_t)a * kp.nin + ((size_t)b * K + k0) * M;
+      const float *Sp = S + (((size_t)a * B + b) * K + k0) * D;
+      if constexpr (D % 2 == 0) {
+        const float2 *S2p = reinterpret_cast<const float2 *>(Sp);
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        float gp[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int m = 0; m < M; m++) gp[m] = dGp[q * M + m];
-        float g0 = Gp[q * M];
-        gp[0] = fabsf(g0) < 1e-8f ? 0.f : gp[0] / g0 * 0.5f;
-        float Sq[2 * D2];
+        for (int q = 0; q < 4; q++)
 #pragma unroll
-        for (int d = 0; d < D; d++) {
-          float t = 0.f;
-          for (int m = 0; m < M; m++) t = fmaf(gp[m], kp.T[m * D + d], t);
-          Sq[d] = 2.f * t * Pp[q * D + d];
-        }
-        if (D & 1) Sq[D] = 0.f;
+          for (int p = 0; p < D2; p++) S2[q][p] = __ldg(S2p + q * D2 + p);
+      } else {
 #pragma unroll
-        for (int p = 0; p < D2; p++) S2[q][p] = make_float2(Sq[2 * p], Sq[2 * p + 1]);
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+          for (int p = 0; p < D2; p++)
+            S2[q][p] = make_float2(__ldg(Sp + q * D + 2 * p),
+                                   2 * p + 1 < D ? __ldg(Sp + q * D + 2 * p + 1) : 0.f);
       }
     }
     float4 *pdf_row = pdf + (size_t)a * cap;
@@ -182,7 +178,7 @@ void launch_force_tpa(const ForceArgs &a, cudaStream_t st) {
   long threads = (long)a.n * TPA;
   int grid = (int)((threads + T - 1) / T);
   if (grid < 1) grid = 1;
-#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.dEdG, a.pdf, a.wv, a.cbox, a.acell
+#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.S, a.pdf, a.wv, a.cbox, a.acell
   switch (a.kp.D) {
     case 1: k_force<TPA, 1, RK, MULTI><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
     case 4: k_force<TPA, 4, RK, MULTI><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;

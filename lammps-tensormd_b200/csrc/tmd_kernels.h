@@ -124,6 +124,11 @@ void mlp_tc_prepare(size_t smem, bool dz_bf16, int np);
 void pack_core_chunks(const float *src, int rows, int cols, long ld_r, long ld_k,
                       uint16_t *dst);
 
+// dE/dP: S[n][B][K][D] = 2 P sum_m T[m][d] dEdG'[b][k][m] (dEdG'0 =
+// 0.5 dEdG0 / G0), written over P in place.
+void launch_dedp(int n, const KParams &kp, float *P, const float *G, const float *dEdG,
+                 cudaStream_t st, long &launches);
+
 // Force: per-pair dE_i/dx_j into pdf, per-atom virial partials.
 struct ForceArgs {
   int n, cap;
@@ -134,7 +139,7 @@ struct ForceArgs {
   const int *elem;
   const uint32_t *nbr;
   const int *boff;
-  const float *P, *G, *dEdG;
+  const float *S;     // dE/dP [n][B][K][D] (launch_dedp)
   float4 *pdf;
   double *wv;  // [n][6] per-atom sum of -r_ij (x) df over own pairs
   const BoxP *cbox;   // multi-cell mode (as DescArgs)

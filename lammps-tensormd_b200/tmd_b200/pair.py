@@ -158,7 +158,8 @@ class TensorMDSystem:
     def launches(self) -> int:
         return int(self.lib.tmd_system_launches(self.h))
 
-    PROFILE_FAMILIES = ("neighbor", "descriptor", "mlp", "force", "gather", "nve", "reduce")
+    PROFILE_FAMILIES = ("neighbor", "descriptor", "mlp", "force", "gather", "nve", "reduce",
+                        "dedp")
 
     def profile(self, enable: bool):
         check(self.lib.tmd_profile_enable(self.h, int(bool(enable))))
