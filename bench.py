@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--no-bf16", action="store_true")
     ap.add_argument("--cells-steps", type=int, default=500,
                     help="NVE steps of the 4,096-cell batch line (0 skips it)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0,
+                    help="serving line: Poisson arrival rate (jobs/s)")
+    ap.add_argument("--serve-window", type=float, default=2.0,
+                    help="serving line: seconds of arrivals (0 skips it)")
     return ap.parse_args()
 
 
@@ -348,6 +352,9 @@ def run_ours(args, rank, world, local):
     cells = None
     if args.cells_steps > 0:
         cells = run_cells(args, rank, world, local, dev, barrier)
+    serving = None
+    if args.serve_window > 0:
+        serving = run_serving(args, rank, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -371,6 +378,7 @@ def run_ours(args, rank, world, local):
             "kernel_ms": kernel_ms,
             "forms": forms,
             "cells4096": cells,
+            "serving": serving,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -432,6 +440,80 @@ def run_cells(args, rank, world, local, dev, barrier):
            "config": {k: v for k, v in c.items() if k != "pot"} | {"potential": c["pot"]}}
     b.close()
     model.close()
+    return out
+
+
+def run_serving(args, rank, local):
+    """Serving: Poisson arrivals (rate args.serve_rate per s over
+    args.serve_window s) of jobs with N log-uniform in [32, 4096] atoms, FCC /
+    BCC lattices or random packings (0.085 A^-3, dmin 2 A), 1-4 elements; 60%
+    single-point, 25% 200-step NVE, 15% FIRE to fmax 0.01 eV/A (at most 1000
+    iterations).  Jobs go through tmd_server_submit / tmd_server_wait; latency
+    is submit -> completion on the host clock."""
+    import threading
+    from tmd_b200 import TensorMDModel, TensorMDServer, synth
+    rng = np.random.default_rng(77 + rank)
+    pot = f"/tmp/tmd_bench_serve_{rank}.npz"
+    syms = synth.gaussian_potential(pot, seed=4242, nelt=4, num_filters=16, rc=6.0,
+                                    max_moment=3, hidden=(64, 64), actfn=2)
+    model = TensorMDModel(f"{pot} {' '.join(syms)}", device=local)
+    sizes = np.unique(np.round(np.geomspace(32, 4096, 12)).astype(int))
+    packings = {int(n): synth.random_packing(int(n), rng) for n in sizes}
+    t_arr = np.cumsum(rng.exponential(1.0 / args.serve_rate,
+                                      size=int(args.serve_rate * args.serve_window * 1.5)))
+    t_arr = t_arr[t_arr < args.serve_window]
+    kinds = rng.choice(3, size=len(t_arr), p=[0.60, 0.25, 0.15])
+    jobs = [synth.serving_job(rng, kind=int(k), packings=packings) for k in kinds]
+    srv = TensorMDServer(model, max_atoms=2_000_000, max_cells=8192, steps_per_tick=8)
+    # warm-up: one job of each kind
+    for k in range(3):
+        x, t, box, v = jobs[k]
+        srv.wait(srv.submit(k, x, t, box, v=v, nsteps=20, dt=0.001, fmax=0.01))
+    st0 = srv.stats()
+    tickets = [None] * len(jobs)
+    done = [None] * len(jobs)
+
+    def submitter():
+        t0 = time.perf_counter()
+        for i, (ta, k, (x, t, box, v)) in enumerate(zip(t_arr, kinds, jobs)):
+            dly = ta - (time.perf_counter() - t0)
+            if dly > 0:
+                time.sleep(dly)
+            tickets[i] = srv.submit(int(k), x, t, box, v=v,
+                                    nsteps=(200 if k == 1 else 1000), dt=0.001, fmax=0.01)
+
+    th = threading.Thread(target=submitter)
+    t_start = time.perf_counter()
+    th.start()
+    for i in range(len(jobs)):
+        while tickets[i] is None:
+            time.sleep(0.0005)
+        done[i] = srv.wait(tickets[i])
+    t_end = time.perf_counter()
+    th.join()
+    st1 = srv.stats()
+    phases = srv.timing()
+    srv.close()
+    model.close()
+    lat = np.array([d["latency"] for d in done]) * 1000.0
+    natoms = np.array([len(j[0]) for j in jobs])
+    out = {"jobs": len(jobs), "arrival_rate_per_s": args.serve_rate,
+           "window_s": args.serve_window, "makespan_s": t_end - t_start,
+           "solves_per_s": len(jobs) / (t_end - t_start),
+           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "atom_steps_per_s": (st1["atom_steps"] - st0["atom_steps"])
+           / max(st1["busy_s"] - st0["busy_s"], 1e-9),
+           "mean_atoms": float(natoms.mean()),
+           "worker_seconds_by_phase": phases,
+           "fire_converged_frac": float(np.mean([d["steps"] < 1000 for d, k in
+                                                 zip(done, kinds) if k == 2] or [1.0])),
+           "by_kind": {}}
+    for k, name in enumerate(("single_point", "nve200", "fire")):
+        sel = kinds == k
+        if sel.any():
+            out["by_kind"][name] = {"jobs": int(sel.sum()),
+                                    "p50_ms": float(np.percentile(lat[sel], 50)),
+                                    "p99_ms": float(np.percentile(lat[sel], 99))}
     return out
 
 

@@ -176,6 +176,47 @@ int tmd_batch_compute(tmd_batch *batch, double *energy, double *virial, double *
 int tmd_batch_nve_run(tmd_batch *batch, int nsteps, double dt, int thermo_every,
                       double *thermo);
 
+/* ---- Serving ---------------------------------------------------------------
+ * A job server on one GPU: callers submit independent small systems from any
+ * thread; one library thread keeps every job in flight as a cell of one
+ * multi-cell batch and advances all of them together (continuous batching:
+ * finished jobs leave and queued jobs join between ticks, FIFO, within
+ * max_atoms / max_cells; each tick runs steps_per_tick steps).  There is no
+ * counterpart in the reference, which runs one LAMMPS system per process.
+ * Job kinds:
+ *   TMD_JOB_ENERGY  one force evaluation (energy, virial, forces)
+ *   TMD_JOB_NVE     nsteps of velocity Verlet with step dt (as tmd_nve_run)
+ *   TMD_JOB_FIRE    FIRE relaxation (Bitzek et al. 2006, semi-implicit Euler,
+ *                   initial step dt, dt_max = 10 dt) until every force
+ *                   component norm |F_i| <= fmax or nsteps iterations ran
+ * tmd_server_wait blocks up to timeout_s seconds (< 0: no limit) and returns
+ * TMD_ERR_TIMEOUT if the job is not done (the ticket stays valid); on
+ * completion it fills the non-NULL outputs: energy, virial[6], final x / v /
+ * f [n*3] (positions wrapped into the box), steps run, latency from submit to
+ * completion, and releases the ticket. */
+#define TMD_JOB_ENERGY 0
+#define TMD_JOB_NVE 1
+#define TMD_JOB_FIRE 2
+typedef struct tmd_server tmd_server;
+int tmd_server_create(const tmd_model *model, int max_atoms, int max_cells,
+                      double skin, int steps_per_tick, tmd_server **out);
+void tmd_server_free(tmd_server *server);
+int tmd_server_submit(tmd_server *server, int kind, int n, const double *x,
+                      const int *type, const double *v, const double box[9],
+                      const int pbc[3], int nsteps, double dt, double fmax,
+                      long *ticket);
+int tmd_server_wait(tmd_server *server, long ticket, double timeout_s,
+                    double *energy, double *virial, double *x, double *v,
+                    double *f, int *steps, double *latency_s);
+/* Counters since creation: jobs submitted / completed, atoms in flight,
+ * atom-steps evaluated (force evaluations x atoms), worker busy seconds. */
+int tmd_server_stats(tmd_server *server, long *submitted, long *completed,
+                     long *active_atoms, double *atom_steps, double *busy_s);
+/* Worker seconds by phase since creation: seconds[0] relayout (admission and
+ * retirement, with the neighbor rebuild), [1] force evaluations of newly
+ * admitted jobs, [2] integrator steps, [3] copying results out. */
+int tmd_server_timing(tmd_server *server, double *seconds);
+
 /* Full neighbor list without allocating any memory.  This entry point has no
  * counterpart in the reference.  It is meant for callers that must not call
  * cudaMalloc: code that records into a CUDA graph (allocation is not allowed

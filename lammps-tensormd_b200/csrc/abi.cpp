@@ -197,7 +197,6 @@ int initial_cap(tmd_system *s) {
   return cap;
 }
 
-namespace {
 NbArgs nb_args(tmd_system *s) {
   NbArgs a{};
   a.n = s->n; a.B = s->m->h.nelt; a.cap = s->cap; a.capp = s->capp;
@@ -213,7 +212,6 @@ NbArgs nb_args(tmd_system *s) {
   a.coff = s->coff;
   return a;
 }
-}  // namespace
 
 // Read the status words and clear them for the next kernels.
 int read_status(tmd_system *s) {
@@ -301,6 +299,51 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   prof_begin(s);
   launch_gather(ga, s->st, s->launches);
   prof_end(s, 4);
+}
+
+int map_types(const tmd_model *m, int n, const int *type, std::vector<int> &elem) {
+  const HostModel &h = m->h;
+  const int ntypes = (int)h.type_elements.size();
+  elem.resize(n);
+  for (int i = 0; i < n; i++) {
+    const int t = type[i];
+    if (t < 1 || t > ntypes || h.typemap[t] < 0)
+      return fail(TMD_ERR_ARG, "atom " + std::to_string(i) + " has type " +
+                                   std::to_string(t) + " that pair_coeff did not map");
+    elem[i] = h.typemap[t];
+  }
+  return TMD_OK;
+}
+
+int set_elements(tmd_system *s, int n, const int *elem) {
+  const HostModel &h = s->m->h;
+  s->n = n;
+  s->h_elem.assign(elem, elem + n);
+  // atoms grouped by element (TensorMD::calc_tensor_density i2row order),
+  // MLP tiles of up to mlp_tr atoms of one element
+  std::vector<int> cnt(h.nelt, 0), start(h.nelt + 1, 0);
+  for (int i = 0; i < n; i++) cnt[elem[i]]++;
+  for (int e = 0; e < h.nelt; e++) start[e + 1] = start[e] + cnt[e];
+  std::vector<int> perm(n > 0 ? n : 1), fill(start.begin(), start.end() - 1);
+  for (int i = 0; i < n; i++) perm[fill[elem[i]]++] = i;
+  std::vector<int> tiles;
+  for (int e = 0; e < h.nelt; e++)
+    for (int o = 0; o < cnt[e]; o += s->m->mlp_tr) {
+      tiles.push_back(e);
+      tiles.push_back(start[e] + o);
+      tiles.push_back(std::min(s->m->mlp_tr, cnt[e] - o));
+    }
+  s->ntiles = (int)tiles.size() / 3;
+  if (n > 0) {
+    TMD_CUDA(cudaMemcpyAsync(s->elem, s->h_elem.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                             s->st));
+    TMD_CUDA(cudaMemcpyAsync(s->perm, perm.data(), n * sizeof(int), cudaMemcpyHostToDevice, s->st));
+    TMD_CUDA(cudaMemcpyAsync(s->tiles, tiles.data(), tiles.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, s->st));
+    // the copies read host vectors that go out of scope: wait for them
+    TMD_CUDA(cudaStreamSynchronize(s->st));
+  }
+  return TMD_OK;
 }
 
 int thermo_reserve(tmd_system *s, long count) {
@@ -699,40 +742,14 @@ int tmd_system_set_atoms(tmd_system *s, int n, const double *x, const int *type,
   if (s->ncells > 0 && n != s->h_coff[s->ncells])
     return fail(TMD_ERR_ARG, "a batch takes exactly the atoms of its cells");
   TMD_CUDA(cudaSetDevice(s->m->device));
-  const HostModel &h = s->m->h;
   drop_graph(s);
-  s->n = n;
-  s->h_elem.resize(n);
-  int ntypes = (int)h.type_elements.size();
-  std::vector<std::vector<int>> by_elt(h.nelt);
-  for (int i = 0; i < n; i++) {
-    int t = type[i];
-    if (t < 1 || t > ntypes || h.typemap[t] < 0)
-      return fail(TMD_ERR_ARG, "atom " + std::to_string(i) + " has type " +
-                                   std::to_string(t) + " that pair_coeff did not map");
-    s->h_elem[i] = h.typemap[t];
-    by_elt[h.typemap[t]].push_back(i);
-  }
-  // atoms grouped by element (TensorMD::calc_tensor_density i2row order)
-  std::vector<int> perm;
-  std::vector<int> tiles;
-  perm.reserve(n);
-  for (int e = 0; e < h.nelt; e++) {
-    int start = (int)perm.size();
-    perm.insert(perm.end(), by_elt[e].begin(), by_elt[e].end());
-    int cnt = (int)by_elt[e].size();
-    for (int o = 0; o < cnt; o += s->m->mlp_tr) {
-      tiles.push_back(e);
-      tiles.push_back(start + o);
-      tiles.push_back(std::min(s->m->mlp_tr, cnt - o));
-    }
-  }
-  s->ntiles = (int)tiles.size() / 3;
+  std::vector<int> elem;
+  int rc = map_types(s->m, n, type, elem);
+  if (rc) return rc;
+  rc = set_elements(s, n, elem.data());
+  if (rc) return rc;
   if (n > 0) {
     TMD_CUDA(cudaMemcpyAsync(s->x, x, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s->st));
-    TMD_CUDA(cudaMemcpyAsync(s->elem, s->h_elem.data(), n * sizeof(int), cudaMemcpyHostToDevice, s->st));
-    TMD_CUDA(cudaMemcpyAsync(s->perm, perm.data(), n * sizeof(int), cudaMemcpyHostToDevice, s->st));
-    TMD_CUDA(cudaMemcpyAsync(s->tiles, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice, s->st));
     if (v) {
       TMD_CUDA(cudaMemcpyAsync(s->v, v, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s->st));
     } else {
@@ -746,7 +763,7 @@ int tmd_system_set_atoms(tmd_system *s, int n, const double *x, const int *type,
   if (n == 0) return TMD_OK;
   int cap = initial_cap(s);
   if (cap > s->cap) {
-    int rc = alloc_neighbors(s, cap);
+    rc = alloc_neighbors(s, cap);
     if (rc) return rc;
   }
   return rebuild_now(s);

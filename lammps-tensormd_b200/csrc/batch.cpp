@@ -22,31 +22,30 @@ struct tmd_batch {
   tmd_system *s = nullptr;
 };
 
-namespace {
+namespace tmd {
 
-int batch_ok(const tmd_batch *b) {
-  if (!b || !b->s) return fail(TMD_ERR_ARG, "null batch");
+int cells_alloc(tmd_system *s, int max_cells) {
+  cudaError_t e = dalloc(&s->cbox, max_cells);
+  if (e == cudaSuccess) e = dalloc(&s->cgeom, max_cells);
+  if (e == cudaSuccess) e = dalloc(&s->acell, s->natoms_cap);
+  if (e == cudaSuccess) e = dalloc(&s->coff, max_cells + 1);
+  if (e == cudaSuccess) e = dalloc(&s->cell_out, 8 * (size_t)max_cells);
+  if (e != cudaSuccess)
+    return fail(TMD_ERR_CUDA, std::string("batch allocation: ") + cudaGetErrorString(e));
+  s->max_cells = max_cells;
   return TMD_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int tmd_batch_create(const tmd_model *m, int ncells, const int *natoms, double skin,
-                     tmd_batch **out) {
-  if (!m || !natoms || !out || ncells < 1) return fail(TMD_ERR_ARG, "bad batch arguments");
-  *out = nullptr;
+int cells_layout(tmd_system *s, int ncells, const int *natoms) {
+  if (ncells < 1 || ncells > s->max_cells)
+    return fail(TMD_ERR_CAPACITY, "cell count outside the batch capacity");
   long total = 0;
   for (int c = 0; c < ncells; c++) {
     if (natoms[c] < 0) return fail(TMD_ERR_ARG, "negative atom count");
     total += natoms[c];
   }
-  if (total < 1) return fail(TMD_ERR_ARG, "a batch needs at least one atom");
-  if (total > kMaxAtoms) return fail(TMD_ERR_CAPACITY, "too many atoms for one batch");
-  tmd_system *s = nullptr;
-  int rc = tmd_system_create(m, (int)total, skin, &s);
-  if (rc) return rc;
+  if (total > s->natoms_cap) return fail(TMD_ERR_CAPACITY, "atoms exceed the batch capacity");
+  drop_graph(s);
   s->ncells = ncells;
   s->h_coff.assign(ncells + 1, 0);
   s->h_acell.resize(total);
@@ -54,44 +53,16 @@ int tmd_batch_create(const tmd_model *m, int ncells, const int *natoms, double s
     s->h_coff[c + 1] = s->h_coff[c] + natoms[c];
     for (int a = s->h_coff[c]; a < s->h_coff[c + 1]; a++) s->h_acell[a] = c;
   }
-  cudaError_t e = dalloc(&s->cbox, ncells);
-  if (e == cudaSuccess) e = dalloc(&s->cgeom, ncells);
-  if (e == cudaSuccess) e = dalloc(&s->acell, total);
-  if (e == cudaSuccess) e = dalloc(&s->coff, ncells + 1);
-  if (e == cudaSuccess) e = dalloc(&s->cell_out, 8 * (size_t)ncells);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(s->acell, s->h_acell.data(), total * sizeof(int), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(s->coff, s->h_coff.data(), (ncells + 1) * sizeof(int),
-                   cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) {
-    tmd_system_free(s);
-    return fail(TMD_ERR_CUDA, std::string("batch allocation: ") + cudaGetErrorString(e));
-  }
-  tmd_batch *b = new tmd_batch();
-  b->s = s;
-  *out = b;
+  if (total > 0)
+    TMD_CUDA(cudaMemcpyAsync(s->acell, s->h_acell.data(), total * sizeof(int),
+                             cudaMemcpyHostToDevice, s->st));
+  TMD_CUDA(cudaMemcpyAsync(s->coff, s->h_coff.data(), (ncells + 1) * sizeof(int),
+                           cudaMemcpyHostToDevice, s->st));
+  TMD_CUDA(cudaStreamSynchronize(s->st));
   return TMD_OK;
 }
 
-void tmd_batch_free(tmd_batch *b) {
-  if (!b) return;
-  tmd_system_free(b->s);
-  delete b;
-}
-
-int tmd_batch_system(tmd_batch *b, tmd_system **sys) {
-  if (int rc = batch_ok(b)) return rc;
-  if (!sys) return fail(TMD_ERR_ARG, "null argument");
-  *sys = b->s;
-  return TMD_OK;
-}
-
-int tmd_batch_set_cells(tmd_batch *b, const double *boxes, const int *pbc) {
-  if (int rc = batch_ok(b)) return rc;
-  if (!boxes || !pbc) return fail(TMD_ERR_ARG, "null argument");
-  tmd_system *s = b->s;
-  TMD_CUDA(cudaSetDevice(s->m->device));
+int cells_geometry(tmd_system *s, const double *boxes, const int *pbc) {
   const int C = s->ncells;
   const double cut = s->m->h.rmax + s->skin;
   std::vector<BoxP> hb(C);
@@ -123,10 +94,72 @@ int tmd_batch_set_cells(tmd_batch *b, const double *boxes, const int *pbc) {
   s->h_cbox = hb;
   s->have_box = true;
   s->forces_valid = false;
+  return TMD_OK;
+}
+
+}  // namespace tmd
+
+namespace {
+
+int batch_ok(const tmd_batch *b) {
+  if (!b || !b->s) return fail(TMD_ERR_ARG, "null batch");
+  return TMD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tmd_batch_create(const tmd_model *m, int ncells, const int *natoms, double skin,
+                     tmd_batch **out) {
+  if (!m || !natoms || !out || ncells < 1) return fail(TMD_ERR_ARG, "bad batch arguments");
+  *out = nullptr;
+  long total = 0;
+  for (int c = 0; c < ncells; c++) {
+    if (natoms[c] < 0) return fail(TMD_ERR_ARG, "negative atom count");
+    total += natoms[c];
+  }
+  if (total < 1) return fail(TMD_ERR_ARG, "a batch needs at least one atom");
+  if (total > kMaxAtoms) return fail(TMD_ERR_CAPACITY, "too many atoms for one batch");
+  tmd_system *s = nullptr;
+  int rc = tmd_system_create(m, (int)total, skin, &s);
+  if (rc) return rc;
+  rc = cells_alloc(s, ncells);
+  if (!rc) rc = cells_layout(s, ncells, natoms);
+  if (rc) {
+    tmd_system_free(s);
+    return rc;
+  }
+  tmd_batch *b = new tmd_batch();
+  b->s = s;
+  *out = b;
+  return TMD_OK;
+}
+
+void tmd_batch_free(tmd_batch *b) {
+  if (!b) return;
+  tmd_system_free(b->s);
+  delete b;
+}
+
+int tmd_batch_system(tmd_batch *b, tmd_system **sys) {
+  if (int rc = batch_ok(b)) return rc;
+  if (!sys) return fail(TMD_ERR_ARG, "null argument");
+  *sys = b->s;
+  return TMD_OK;
+}
+
+int tmd_batch_set_cells(tmd_batch *b, const double *boxes, const int *pbc) {
+  if (int rc = batch_ok(b)) return rc;
+  if (!boxes || !pbc) return fail(TMD_ERR_ARG, "null argument");
+  tmd_system *s = b->s;
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  int rc = cells_geometry(s, boxes, pbc);
+  if (rc) return rc;
   if (s->have_atoms) {
     int cap = initial_cap(s);
     if (cap > s->cap) {
-      int rc = alloc_neighbors(s, cap);
+      rc = alloc_neighbors(s, cap);
       if (rc) return rc;
     }
     return rebuild_now(s);

@@ -46,7 +46,7 @@ struct tmd_system {
   int ncell_alloc = 0;
   // multi-cell batch (ncells > 0): cell c holds atoms coff[c]..coff[c+1]-1
   // in its own periodic box; box/bin above are unused
-  int ncells = 0;
+  int ncells = 0, max_cells = 0;
   std::vector<int> h_coff, h_acell;
   std::vector<tmd::BoxP> h_cbox;
   tmd::BoxP *cbox = nullptr;
@@ -121,6 +121,17 @@ int read_status(tmd_system *s);
 int clear_status(tmd_system *s);
 int rebuild_now(tmd_system *s);
 void launch_force_eval(tmd_system *s, float scale, bool want_vatom);
+NbArgs nb_args(tmd_system *s);
+// LAMMPS types (1-based) -> potential elements; TMD_ERR_ARG for unmapped types.
+int map_types(const tmd_model *m, int n, const int *type, std::vector<int> &elem);
+// Set n atoms' elements: host mirror, device elem[], MLP element grouping
+// (perm, tiles).  Synchronises the stream.
+int set_elements(tmd_system *s, int n, const int *elem);
+// Multi-cell mode (batch.cpp): device arrays for up to max_cells cells, the
+// cell layout (atoms per cell, concatenated), per-cell boxes.
+int cells_alloc(tmd_system *s, int max_cells);
+int cells_layout(tmd_system *s, int ncells, const int *natoms);
+int cells_geometry(tmd_system *s, const double *boxes, const int *pbc);
 // Make sure s->thermo_d holds count doubles.
 int thermo_reserve(tmd_system *s, long count);
 // Velocity Verlet for nsteps on the device (graph-captured step).  thermo_row(r)

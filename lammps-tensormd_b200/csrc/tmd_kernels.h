@@ -178,6 +178,47 @@ void launch_cell_sum(int ncells, const int *coff, const double *in, int ncomp,
 void launch_scale_copy(const double *in, int n, double scale, double *out,
                        cudaStream_t st, long &launches);
 
+// ---- serving: per-cell control of mixed jobs in one multi-cell system ----
+constexpr int kJobEnergy = 0;  // one force evaluation, atoms fixed
+constexpr int kJobNve = 1;     // velocity Verlet, `left` steps
+constexpr int kJobFire = 2;    // FIRE relaxation until max |F| <= fmax or `left` runs out
+
+struct CellCtl {
+  int mode;      // kJob*
+  int left;      // NVE steps / FIRE iterations still to run
+  int npos;      // FIRE: consecutive steps with P = F.v > 0
+  int conv;      // FIRE: converged (max |F|^2 <= fmax2)
+  int it;        // FIRE: iterations run
+  int pad;
+  double dt;     // NVE step; FIRE current step (ps)
+  double dtmax;  // FIRE
+  double alpha;  // FIRE mixing parameter
+  double fmax2;  // FIRE convergence threshold, (eV/A)^2
+  double mix1, mix2;  // FIRE velocity mixing of the current step
+};
+
+// New layout of a server batch: atom a of new cell c comes from old atom
+// src[c] + (a - coff[c]) when src[c] >= 0, else from staging slot
+// -src[c] - 1 + (a - coff[c]) (new requests; image counters start at 0).
+void launch_srv_gather(int n, const int *acell, const int *coff, const int *src,
+                       const double *x_old, const double *v_old, const double *f_old,
+                       const int *img_old, const double *x_stage, const double *v_stage,
+                       double *x, double *v, double *f, int *img, cudaStream_t st,
+                       long &launches);
+// One serving step, before the force evaluation: FIRE power (F.v, v.v, F.F)
+// summed per cell, FIRE state update, then the position update of NVE (half
+// kick + drift) and FIRE (mix + semi-implicit Euler) cells.
+void launch_srv_pre(int n, int ncells, const int *acell, const int *coff, CellCtl *ctl,
+                    double *x, double *v, const double *f, const int *elem,
+                    const double *mass_e, double *pw, double *csum, cudaStream_t st,
+                    long &launches);
+// After the force evaluation: NVE second half kick (kick != 0), per-cell
+// max |F|^2, step bookkeeping (count != 0) and FIRE convergence.
+void launch_srv_post(int n, int ncells, const int *acell, const int *coff, CellCtl *ctl,
+                     double *v, const double *f, const int *elem, const double *mass_e,
+                     double *fsq, double *cfmax, int kick, int count, cudaStream_t st,
+                     long &launches);
+
 // Velocity Verlet halves (fix_nve.cpp:64-141).
 void launch_nve_initial(int n, double *x, double *v, const double *f,
                         const int *elem, const double *mass_e, double dtf,

@@ -7,7 +7,8 @@ There is no CPU fallback: importing a class that needs the library raises if
 libtmd_b200.so is missing or cannot find a CUDA device.
 """
 from .lib import TmdError, library_path, load_library
-from .pair import PairTensorMD, TensorMDBatch, TensorMDModel, TensorMDSystem
+from .pair import (PairTensorMD, TensorMDBatch, TensorMDModel, TensorMDServer,
+                   TensorMDSystem)
 
 __all__ = ["TmdError", "library_path", "load_library", "PairTensorMD",
-           "TensorMDBatch", "TensorMDModel", "TensorMDSystem"]
+           "TensorMDBatch", "TensorMDModel", "TensorMDServer", "TensorMDSystem"]

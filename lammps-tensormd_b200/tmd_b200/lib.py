@@ -47,6 +47,14 @@ SIGNATURES = [
     ("tmd_batch_get", _c_int, [_vp, _pd, _pd, _pd, _pi]),
     ("tmd_batch_compute", _c_int, [_vp, _pd, _pd, _pd]),
     ("tmd_batch_nve_run", _c_int, [_vp, _c_int, _c_double, _c_int, _pd]),
+    ("tmd_server_create", _c_int, [_vp, _c_int, _c_int, _c_double, _c_int,
+                                   ctypes.POINTER(_vp)]),
+    ("tmd_server_free", None, [_vp]),
+    ("tmd_server_submit", _c_int, [_vp, _c_int, _c_int, _pd, _pi, _pd, _pd, _pi, _c_int,
+                                   _c_double, _c_double, _pl]),
+    ("tmd_server_wait", _c_int, [_vp, _c_long, _c_double, _pd, _pd, _pd, _pd, _pd, _pi, _pd]),
+    ("tmd_server_stats", _c_int, [_vp, _pl, _pl, _pl, _pd, _pd]),
+    ("tmd_server_timing", _c_int, [_vp, _pd]),
     ("tmd_neighbor_list_noalloc", _c_int, [_vp, _c_int, _pd, _pi, _c_double, _c_int, _vp,
                                            _vp, _vp]),
 ]

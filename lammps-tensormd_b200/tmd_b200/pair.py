@@ -247,6 +247,78 @@ class TensorMDBatch:
         return s
 
 
+class TensorMDServer:
+    """Job server (tmd_server_*): continuous batching of small systems.
+
+    submit() may be called from any thread; wait() returns the job's results."""
+
+    ENERGY, NVE, FIRE = 0, 1, 2
+
+    def __init__(self, model: TensorMDModel, max_atoms: int, max_cells: int = 8192,
+                 skin: float = 1.0, steps_per_tick: int = 8):
+        self.model = model
+        self.lib = model.lib
+        h = ctypes.c_void_p()
+        check(self.lib.tmd_server_create(model.h, int(max_atoms), int(max_cells), float(skin),
+                                         int(steps_per_tick), ctypes.byref(h)))
+        self.h = h
+        self._n = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tmd_server_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, kind, x, types, box, pbc=(1, 1, 1), v=None, nsteps=0, dt=0.001,
+               fmax=0.01) -> int:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        vv = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        b = np.ascontiguousarray(box, dtype=np.float64)
+        p = np.ascontiguousarray(pbc, dtype=np.int32)
+        tk = ctypes.c_long()
+        check(self.lib.tmd_server_submit(self.h, int(kind), len(x), _dp(x), _ip(t), _dp(vv),
+                                         _dp(b), _ip(p), int(nsteps), float(dt), float(fmax),
+                                         ctypes.byref(tk)))
+        self._n[tk.value] = len(x)
+        return tk.value
+
+    def wait(self, ticket: int, timeout: float = -1.0):
+        """dict(energy, virial, x, v, f, steps, latency); raises TmdError (code -8
+        when the job is not done within timeout seconds)."""
+        n = self._n[ticket]
+        e = np.zeros(1)
+        vir = np.zeros(6)
+        x, v, f = (np.zeros((n, 3)) for _ in range(3))
+        steps = ctypes.c_int()
+        lat = np.zeros(1)
+        check(self.lib.tmd_server_wait(self.h, int(ticket), float(timeout), _dp(e), _dp(vir),
+                                       _dp(x), _dp(v), _dp(f), ctypes.byref(steps), _dp(lat)))
+        del self._n[ticket]
+        return dict(energy=float(e[0]), virial=vir, x=x, v=v, f=f, steps=steps.value,
+                    latency=float(lat[0]))
+
+    def stats(self):
+        sub, comp, act = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
+        ast, busy = np.zeros(1), np.zeros(1)
+        check(self.lib.tmd_server_stats(self.h, ctypes.byref(sub), ctypes.byref(comp),
+                                        ctypes.byref(act), _dp(ast), _dp(busy)))
+        return dict(submitted=sub.value, completed=comp.value, active_atoms=act.value,
+                    atom_steps=float(ast[0]), busy_s=float(busy[0]))
+
+    def timing(self):
+        """Worker seconds by phase: relayout, admission evaluation, steps, results."""
+        t = np.zeros(4)
+        check(self.lib.tmd_server_timing(self.h, _dp(t)))
+        return dict(zip(("relayout", "admission_eval", "steps", "results"), t.tolist()))
+
+
 class PairTensorMD:
     """The pair_style tensormd call surface, single rank, periodic on device."""
 

@@ -172,6 +172,98 @@ def batch_cells(ncells=4096, natoms=256, *, nelt=2, sigma=0.1, t_range=(300.0, 1
                 cells=list(zip(xs, ts, boxes, vs)))
 
 
+def random_packing(n, rng, density=0.085, dmin=2.0, h=0.25, attempts=5):
+    """n atoms in a periodic cube at `density` (1/A^3), no pair closer than
+    dmin: random sequential addition (rejection sampling).  0.085 A^-3 with
+    dmin = 2 A is a volume fraction of 0.356, close to the jamming limit of
+    sequential addition (about 0.38), where uniform candidates are almost all
+    rejected; candidates are therefore drawn uniformly inside voxels (side ~h)
+    that no accepted atom fully excludes yet, then tested exactly against the
+    accepted atoms and the round's earlier candidates.  Returns x[n, 3], box[9]."""
+    from scipy.spatial import cKDTree
+    L = (n / density) ** (1.0 / 3.0)
+    g = max(1, int(np.ceil(L / h)))
+    h = L / g
+    # voxel offsets entirely within dmin of any point of the centre voxel
+    r = int(np.ceil(dmin / h))
+    o = np.stack(np.meshgrid(*(np.arange(-r, r + 1),) * 3, indexing="ij"), -1).reshape(-1, 3)
+    o = o[np.linalg.norm(o, axis=1) * h + h * np.sqrt(3.0) < dmin]
+    for _ in range(attempts):
+        free = np.ones(g ** 3, dtype=bool)
+        pts = np.zeros((0, 3))
+        while len(pts) < n:
+            fi = np.flatnonzero(free)
+            if len(fi) == 0:
+                break
+            m = min(len(fi), max(2048, 4 * (n - len(pts))))
+            pick = np.unique(fi[rng.integers(len(fi), size=m)])
+            m = len(pick)
+            vox = np.stack(np.unravel_index(pick, (g, g, g)), -1)
+            cand = (vox + rng.uniform(size=(m, 3))) * h
+            if len(pts):
+                d, _ = cKDTree(pts, boxsize=L).query(cand, k=1)
+                ok = d >= dmin
+                free[pick[~ok & (d < dmin - h * np.sqrt(3.0))]] = False
+                cand, vox = cand[ok], vox[ok]
+            taken = np.ones(len(cand), dtype=bool)
+            if len(cand) > 1:
+                close = cKDTree(cand, boxsize=L).query_pairs(dmin, output_type="ndarray")
+                if len(close):
+                    taken[np.max(close, axis=1)] = False  # the later one of a close pair
+            keep = np.nonzero(taken)[0][: n - len(pts)]
+            pts = np.concatenate([pts, cand[keep]])
+            blk = (vox[keep][:, None, :] + o[None, :, :]) % g
+            free[np.ravel_multi_index((blk[..., 0], blk[..., 1], blk[..., 2]), (g, g, g))] = False
+        if len(pts) >= n:
+            return pts, np.array([0.0, 0.0, 0.0, L, L, L, 0.0, 0.0, 0.0])
+    raise RuntimeError("random packing did not reach the requested density")
+
+
+def _near_cubic(cells):
+    """nx, ny, nz with nx*ny*nz close to `cells`, as cubic as possible."""
+    c = max(1, int(round(cells)))
+    best = (1, 1, c)
+    for nx in range(1, int(round(c ** (1 / 3))) + 2):
+        for ny in range(nx, int(round((c / nx) ** 0.5)) + 2):
+            nz = max(ny, int(round(c / (nx * ny))))
+            if abs(nx * ny * nz - c) < abs(best[0] * best[1] * best[2] - c) or (
+                    nx * ny * nz == best[0] * best[1] * best[2] and nz - nx < best[2] - best[0]):
+                best = (nx, ny, nz)
+    return best
+
+
+def serving_job(rng, *, kind, nmin=32, nmax=4096, max_elements=4, packings=None):
+    """One job of the serving workload: N log-uniform in [nmin, nmax], an FCC
+    (a = 3.6 A) or BCC (a = 2.87 A) lattice or a random packing (0.085 A^-3,
+    dmin 2 A; `packings` may hold prepared ones by size), 1..max_elements
+    elements.  NVE jobs get Maxwell-Boltzmann velocities at T in [300, 1200] K
+    and FIRE jobs displaced positions (sigma 0.1 A).  Returns x, types, box, v."""
+    n = int(round(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
+    shape = rng.integers(3)
+    if shape == 0:
+        x, box = lattice("fcc", 3.6, *_near_cubic(n / 4))
+    elif shape == 1:
+        x, box = lattice("bcc", 2.87, *_near_cubic(n / 2))
+    else:
+        if packings:
+            sizes = np.array(sorted(packings))
+            x, box = packings[int(sizes[np.argmin(np.abs(sizes - n))])]
+        else:
+            x, box = random_packing(n, rng)
+    n = len(x)
+    ne = int(rng.integers(1, max_elements + 1))
+    types = rng.integers(1, ne + 1, size=n).astype(np.int32)
+    v = np.zeros_like(x)
+    if kind == 2:
+        x = wrap(x + rng.normal(0.0, 0.1, size=x.shape), box)
+    else:
+        x = wrap(x + rng.normal(0.0, 0.05, size=x.shape), box)
+    if kind == 1:
+        m = np.array([MASSES[s] for s in SYMBOLS[:max_elements]])[types - 1]
+        v = maxwell(m, rng.uniform(300.0, 1200.0), rng)
+    return x, types, box, v
+
+
 def config(name):
     """The workloads this path is measured on (shapes from the task spec)."""
     if name == "fcc4k":  # plain CPU config: 4,000 atoms

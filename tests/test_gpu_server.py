@@ -1,0 +1,145 @@
+"""Serving loop (tmd_server_*) through the C ABI.
+
+  single-point jobs  forces bit-identical to a separate system of the same
+                     atoms (the server runs them as cells of one batch, whose
+                     per-cell results equal separate systems), energy and
+                     virial to 1e-12 relative (sums in another order)
+  NVE jobs           nsteps run; thermo end state close to tmd_nve_run of the
+                     same system (1e-6 relative in energy: the batch rebuilds
+                     and wraps at other steps, see test_gpu_batch)
+  FIRE jobs          end with every |F_i| <= fmax and a lower energy
+  concurrency        mixed jobs from several threads all complete; results
+                     do not depend on what else was in flight
+  errors             unknown kind, job beyond the atom budget, wait timeout"""
+import threading
+
+import numpy as np
+import pytest
+
+from tmd_b200 import TensorMDModel, TensorMDServer, TensorMDSystem, TmdError, synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def model4(tmp_path_factory):
+    p = tmp_path_factory.mktemp("pot") / "serve.npz"
+    syms = synth.gaussian_potential(p, seed=31, nelt=4, num_filters=16, rc=6.0,
+                                    max_moment=3, hidden=(64, 64), actfn=2)
+    return TensorMDModel(f"{p} {' '.join(syms)}")
+
+
+def _separate(model, x, t, box, v=None):
+    s = TensorMDSystem(model, len(x), 1.0)
+    s.set_box(box)
+    s.set_atoms(x, t, v)
+    return s
+
+
+def test_single_point_jobs_equal_separate_systems(model4):
+    rng = np.random.default_rng(1)
+    srv = TensorMDServer(model4, max_atoms=200000, max_cells=256)
+    jobs = [synth.serving_job(rng, kind=0, nmax=1200) for _ in range(12)]
+    tickets = [srv.submit(0, x, t, box) for x, t, box, _ in jobs]
+    for tk, (x, t, box, _) in zip(tickets, jobs):
+        out = srv.wait(tk, timeout=120)
+        ref = _separate(model4, x, t, box).compute(1, 1)
+        assert np.array_equal(out["f"], ref["f"])
+        assert out["energy"] == pytest.approx(ref["energy"], rel=1e-12, abs=1e-10)
+        np.testing.assert_allclose(out["virial"], ref["virial"], rtol=1e-12, atol=1e-10)
+        assert out["steps"] == 0 and out["latency"] > 0
+    srv.close()
+
+
+def test_nve_job_matches_system_run(model4):
+    rng = np.random.default_rng(2)
+    x, t, box, v = synth.serving_job(rng, kind=1, nmin=500, nmax=600)
+    srv = TensorMDServer(model4, max_atoms=100000, max_cells=64, steps_per_tick=8)
+    tk = srv.submit(1, x, t, box, v=v, nsteps=100, dt=0.001)
+    # a second job in flight at the same time
+    x2, t2, box2, v2 = synth.serving_job(rng, kind=1, nmin=200, nmax=300)
+    tk2 = srv.submit(1, x2, t2, box2, v=v2, nsteps=37, dt=0.001)
+    out = srv.wait(tk, timeout=120)
+    out2 = srv.wait(tk2, timeout=120)
+    assert out["steps"] == 100 and out2["steps"] == 37
+    s = _separate(model4, x, t, box, v)
+    th = s.nve_run(100, 0.001, thermo_every=100)
+    ref = s.compute(1, 1)
+    assert out["energy"] == pytest.approx(ref["energy"], rel=1e-6)
+    m = model4.type_mass[t]
+    ke = 0.5 * synth.MVV2E * np.sum(m[:, None] * out["v"] ** 2)
+    assert ke == pytest.approx(th[-1, 1], rel=1e-6)
+    srv.close()
+
+
+def test_fire_job_relaxes(model4):
+    rng = np.random.default_rng(3)
+    x, t, box, _ = synth.serving_job(rng, kind=2, nmin=100, nmax=200)
+    e0 = _separate(model4, x, t, box).compute(1, 1)["energy"]
+    srv = TensorMDServer(model4, max_atoms=100000, max_cells=64, steps_per_tick=16)
+    fmax = 0.05
+    tk = srv.submit(2, x, t, box, nsteps=3000, dt=0.001, fmax=fmax)
+    out = srv.wait(tk, timeout=300)
+    fnorm = np.linalg.norm(out["f"], axis=1).max()
+    assert out["steps"] < 3000, "FIRE did not converge"
+    assert fnorm <= fmax
+    assert out["energy"] < e0
+    # the returned state is consistent: forces of the returned positions
+    ref = _separate(model4, out["x"], t, box).compute(1, 1)
+    np.testing.assert_allclose(ref["f"], out["f"], atol=1e-9)
+    srv.close()
+
+
+def test_concurrent_mixed_jobs(model4):
+    rng = np.random.default_rng(4)
+    srv = TensorMDServer(model4, max_atoms=60000, max_cells=64, steps_per_tick=4)
+    jobs = []
+    for k in range(30):
+        kind = (0, 0, 1, 2)[k % 4]
+        jobs.append((kind, synth.serving_job(rng, kind=kind, nmax=800)))
+    results = {}
+    errors = []
+
+    def client(part):
+        try:
+            for i in part:
+                kind, (x, t, box, v) = jobs[i]
+                tk = srv.submit(kind, x, t, box, v=v, nsteps=40 if kind == 1 else 400,
+                                dt=0.001, fmax=0.2)
+                results[i] = srv.wait(tk, timeout=300)
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=client, args=(range(r, 30, 3),)) for r in range(3)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    assert not errors, errors
+    assert len(results) == 30
+    for i, (kind, (x, t, box, v)) in enumerate(jobs):
+        if kind == 0:  # independent of what else was in flight
+            ref = _separate(model4, x, t, box).compute(1, 1)
+            assert np.array_equal(results[i]["f"], ref["f"])
+        if kind == 1:
+            assert results[i]["steps"] == 40
+    st = srv.stats()
+    assert st["submitted"] == 30 and st["completed"] == 30 and st["atom_steps"] > 0
+    srv.close()
+
+
+def test_server_errors(model4):
+    srv = TensorMDServer(model4, max_atoms=1000, max_cells=8)
+    x, t, box, _ = synth.serving_job(np.random.default_rng(5), kind=0, nmin=64, nmax=64)
+    with pytest.raises(TmdError) as e:
+        srv.submit(7, x, t, box)
+    assert e.value.code == -1
+    big, tb, boxb, _ = synth.build_system("fcc", 3.6, (8, 8, 8))
+    with pytest.raises(TmdError) as e:
+        srv.submit(0, big, tb, boxb)
+    assert e.value.code == -4
+    tk = srv.submit(1, x, t, box, nsteps=200000, dt=0.001)
+    with pytest.raises(TmdError) as e:
+        srv.wait(tk, timeout=0.0)
+    assert e.value.code == -8
+    srv.close()  # stops with the job unfinished
