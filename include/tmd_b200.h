@@ -114,6 +114,21 @@ int tmd_compute(tmd_system *sys, int eflag, int vflag, double scale,
 int tmd_nve_run(tmd_system *sys, int nsteps, double dt, int thermo_every,
                 double *thermo);
 
+/* nsteps of `fix nvt temp t_start t_stop t_damp` (FixNH, fix_nh.cpp:741-930,
+ * 1758-1822): velocity Verlet with a Nose-Hoover chain thermostat of 3
+ * (tchain 3, tloop 1, drag 0: the fix's defaults), target temperature ramped
+ * linearly from t_start to t_stop over the run, temperature with 3N - 3
+ * degrees of freedom (compute temp).  The chain state is kept between runs on
+ * the same atoms, as the fix keeps it between LAMMPS runs; set_atoms starts a
+ * fresh one.  Temperatures in K, t_damp and dt in ps; thermo as tmd_nve_run. */
+int tmd_nvt_run(tmd_system *sys, int nsteps, double dt, double t_start,
+                double t_stop, double t_damp, int thermo_every, double *thermo);
+/* Energy of the thermostat chain after the last nvt run (what `thermo` prints
+ * as f_ID of fix nvt, FixNH::compute_scalar, fix_nh.cpp:1447-1473): one value
+ * for a system, one per cell for the system of a batch.  pe + ke + this is
+ * the conserved quantity of the thermostatted dynamics. */
+int tmd_nvt_energy(tmd_system *sys, double *energy);
+
 /* Export the current full neighbor list with cutoff `cut` (<= cutmax +
  * skin) for parity checks: counts[n]; entries[total*4] = (j, sx, sy, sz)
  * where the neighbor is atom j shifted by sx*a + sy*b + sz*c.  Pass
@@ -174,6 +189,10 @@ int tmd_batch_compute(tmd_batch *batch, double *energy, double *virial, double *
 /* As tmd_nve_run for every cell at once; thermo[rows*ncells*2] holds
  * (pe, ke) per cell, row-major by thermo row then cell. */
 int tmd_batch_nve_run(tmd_batch *batch, int nsteps, double dt, int thermo_every,
+                      double *thermo);
+/* As tmd_nvt_run with one thermostat per cell: t_start[ncells], t_stop[ncells]. */
+int tmd_batch_nvt_run(tmd_batch *batch, int nsteps, double dt, const double *t_start,
+                      const double *t_stop, double t_damp, int thermo_every,
                       double *thermo);
 
 /* ---- Serving ---------------------------------------------------------------

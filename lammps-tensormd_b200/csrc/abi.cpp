@@ -319,6 +319,7 @@ int set_elements(tmd_system *s, int n, const int *elem) {
   const HostModel &h = s->m->h;
   s->n = n;
   s->h_elem.assign(elem, elem + n);
+  s->nhc_valid = false;  // new atoms: a fresh thermostat
   // atoms grouped by element (TensorMD::calc_tensor_density i2row order),
   // MLP tiles of up to mlp_tr atoms of one element
   std::vector<int> cnt(h.nelt, 0), start(h.nelt + 1, 0);
@@ -355,8 +356,51 @@ int thermo_reserve(tmd_system *s, long count) {
   return TMD_OK;
 }
 
-int run_nve(tmd_system *s, int nsteps, double dt, int thermo_every,
-            void (*thermo_row)(tmd_system *, int), double *thermo, long thermo_count) {
+// Kinetic energy of every thermostat group into s->nhc_ke.
+void group_ke(tmd_system *s) {
+  launch_kinetic(s->n, s->v, s->elem, s->m->d_mass, s->ke, s->st, s->launches);
+  if (s->ncells > 0)
+    launch_cell_sum(s->ncells, s->coff, s->ke, 1, 1.0, s->nhc_ke, 1, s->st, s->launches);
+  else
+    launch_reduce_f64(s->ke, s->n, 1, s->partial, s->nhc_ke, s->st, s->launches);
+}
+
+// Thermostat state for this run: one group per cell (or one for the
+// system), eta / eta_dot kept from the previous run of the same layout.
+int nhc_prepare(tmd_system *s, const NvtSpec &nvt, int nsteps, double dt) {
+  const int G = s->ncells > 0 ? s->ncells : 1;
+  if (G > s->nhc_alloc) {
+    dfree(s->nhc);
+    dfree(s->nhc_ke);
+    TMD_CUDA(dalloc(&s->nhc, G));
+    TMD_CUDA(dalloc(&s->nhc_ke, G));
+    s->nhc_alloc = G;
+    s->nhc_valid = false;
+  }
+  std::vector<NhcState> h(G);
+  if (s->nhc_valid && s->nhc_groups == G)
+    TMD_CUDA(cudaMemcpy(h.data(), s->nhc, G * sizeof(NhcState), cudaMemcpyDeviceToHost));
+  else
+    for (auto &c : h) c = NhcState{};
+  for (int g = 0; g < G; g++) {
+    const int na = s->ncells > 0 ? s->h_coff[g + 1] - s->h_coff[g] : s->n;
+    h[g].tdof = 3.0 * na - 3.0;  // compute temp: dof = 3N - dimension
+    h[g].t_freq = 1.0 / nvt.t_damp;
+    h[g].t_start = nvt.t_start[g];
+    h[g].t_stop = nvt.t_stop[g];
+    h[g].dt = dt;
+    h[g].nsteps = nsteps;
+  }
+  TMD_CUDA(cudaMemcpyAsync(s->nhc, h.data(), G * sizeof(NhcState), cudaMemcpyHostToDevice,
+                           s->st));
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  s->nhc_groups = G;
+  s->nhc_valid = true;
+  return TMD_OK;
+}
+
+int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_every,
+           void (*thermo_row)(tmd_system *, int), double *thermo, long thermo_count) {
   TMD_CUDA(cudaSetDevice(s->m->device));
   const int n = s->n;
   if (n == 0) return TMD_OK;
@@ -371,12 +415,23 @@ int run_nve(tmd_system *s, int nsteps, double dt, int thermo_every,
   }
   int rc = clear_status(s);
   if (rc) return rc;
-  // Verlet::setup: forces of the starting positions
+  if (nvt) {
+    rc = nhc_prepare(s, *nvt, nsteps, dt);
+    if (rc) return rc;
+  }
+  const int G = s->nhc_groups;
+  const int *acell = s->ncells > 0 ? s->acell : nullptr;
+  // Verlet::setup: forces of the starting positions (and FixNH::setup)
   launch_force_eval(s, 1.0f, false);
+  if (nvt) {
+    group_ke(s);
+    launch_nhc_setup(G, s->nhc, s->nhc_ke, s->st, s->launches);
+  }
   int row = 0;
   if (want_thermo) thermo_row(s, row++);
   auto md_step = [&]() {
     prof_begin(s);
+    if (nvt) launch_nhc_half(G, s->nhc, nullptr, n, acell, s->v, s->st, s->launches);
     launch_nve_initial(n, s->x, s->v, s->f, s->elem, s->m->d_mass, dtf, dt, s->st, s->launches);
     launch_neighbor_check(n, s->x, s->xbuild, trigsq, s->flag, s->st, s->launches);
     prof_end(s, 5);
@@ -386,13 +441,17 @@ int run_nve(tmd_system *s, int nsteps, double dt, int thermo_every,
     launch_force_eval(s, 1.0f, false);
     prof_begin(s);
     launch_nve_final(n, s->v, s->f, s->elem, s->m->d_mass, dtf, s->st, s->launches);
+    if (nvt) {
+      group_ke(s);
+      launch_nhc_half(G, s->nhc, s->nhc_ke, n, acell, s->v, s->st, s->launches);
+    }
     prof_end(s, 5);
   };
   // Without kernel timing, the step runs as one captured CUDA graph: every
   // launch (including the conditional rebuild kernels) is replayed with its
   // arguments fixed at capture; buffers, box, atom count and dt key the graph.
   const bool use_graph = !s->prof;
-  if (use_graph && (!s->step_exec || s->step_dt != dt)) {
+  if (use_graph && (!s->step_exec || s->step_dt != dt || s->step_nvt != (nvt != nullptr))) {
     drop_graph(s);
     cudaGraph_t g;
     long l0 = s->launches;
@@ -408,6 +467,7 @@ int run_nve(tmd_system *s, int nsteps, double dt, int thermo_every,
     s->step_launches = s->launches - l0;
     s->launches = l0;
     s->step_dt = dt;
+    s->step_nvt = nvt != nullptr;
   }
   for (int step = 1; step <= nsteps; step++) {
     if (use_graph) {
@@ -697,6 +757,7 @@ void tmd_system_free(tmd_system *s) {
   dfree(s->scal); dfree(s->flag); dfree(s->status); dfree(s->maxneed); dfree(s->perm);
   dfree(s->tiles); dfree(s->thermo_d);
   dfree(s->cbox); dfree(s->cgeom); dfree(s->acell); dfree(s->coff); dfree(s->cell_out);
+  dfree(s->nhc); dfree(s->nhc_ke);
   if (s->h_scal) cudaFreeHost(s->h_scal);
   if (s->h_status) cudaFreeHost(s->h_status);
   for (auto &p : s->ev_pending) {
@@ -849,7 +910,43 @@ int tmd_nve_run(tmd_system *s, int nsteps, double dt, int thermo_every, double *
     launch_kinetic(q->n, q->v, q->elem, q->m->d_mass, q->ke, q->st, q->launches);
     launch_reduce_f64(q->ke, q->n, 1, q->partial, q->thermo_d + 2 * r + 1, q->st, q->launches);
   };
-  return run_nve(s, nsteps, dt, thermo ? thermo_every : 0, row_fn, thermo, 2L * rows);
+  return run_md(s, nsteps, dt, nullptr, thermo ? thermo_every : 0, row_fn, thermo, 2L * rows);
+}
+
+int tmd_nvt_run(tmd_system *s, int nsteps, double dt, double t_start, double t_stop,
+                double t_damp, int thermo_every, double *thermo) {
+  if (!s || nsteps < 0 || !(dt > 0)) return fail(TMD_ERR_ARG, "bad nvt arguments");
+  if (!(t_start > 0) || !(t_stop > 0) || !(t_damp > 0))
+    return fail(TMD_ERR_ARG, "fix nvt needs t_start, t_stop and t_damp > 0");
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before nvt_run");
+  if (s->ncells > 0) return fail(TMD_ERR_STATE, "a batch runs nvt through tmd_batch_nvt_run");
+  if (thermo && thermo_every < 1) return fail(TMD_ERR_ARG, "thermo_every must be >= 1");
+  int rows = thermo ? 1 + nsteps / thermo_every + ((nsteps % thermo_every) ? 1 : 0) : 0;
+  auto row_fn = [](tmd_system *q, int r) {
+    launch_reduce_scaled(q->E, q->n, q->partial, q->thermo_d + 2 * r, 1.0, q->st, q->launches);
+    launch_kinetic(q->n, q->v, q->elem, q->m->d_mass, q->ke, q->st, q->launches);
+    launch_reduce_f64(q->ke, q->n, 1, q->partial, q->thermo_d + 2 * r + 1, q->st, q->launches);
+  };
+  const NvtSpec nvt{&t_start, &t_stop, t_damp};
+  return run_md(s, nsteps, dt, &nvt, thermo ? thermo_every : 0, row_fn, thermo, 2L * rows);
+}
+
+int tmd_nvt_energy(tmd_system *s, double *energy) {
+  if (!s || !energy) return fail(TMD_ERR_ARG, "null argument");
+  if (!s->nhc_valid) return fail(TMD_ERR_STATE, "no nvt run on these atoms");
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  std::vector<NhcState> h(s->nhc_groups);
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  TMD_CUDA(cudaMemcpy(h.data(), s->nhc, h.size() * sizeof(NhcState), cudaMemcpyDeviceToHost));
+  const double boltz = 8.617343e-5;
+  for (size_t g = 0; g < h.size(); g++) {  // FixNH::compute_scalar (fix_nh.cpp:1447-1473)
+    const NhcState &c = h[g];
+    double e = c.ke_target * c.eta[0] + 0.5 * c.eta_mass[0] * c.eta_dot[0] * c.eta_dot[0];
+    for (int k = 1; k < kNhcChain; k++)
+      e += boltz * c.t_target * c.eta[k] + 0.5 * c.eta_mass[k] * c.eta_dot[k] * c.eta_dot[k];
+    energy[g] = e;
+  }
+  return TMD_OK;
 }
 
 int tmd_neighbor_list(tmd_system *s, double cut, int *counts, int *entries, long cap,

@@ -229,8 +229,32 @@ int tmd_batch_nve_run(tmd_batch *b, int nsteps, double dt, int thermo_every,
     launch_kinetic(q->n, q->v, q->elem, q->m->d_mass, q->ke, q->st, q->launches);
     launch_cell_sum(q->ncells, q->coff, q->ke, 1, 1.0, o + 1, 2, q->st, q->launches);
   };
-  return run_nve(s, nsteps, dt, thermo ? thermo_every : 0, row_fn, thermo,
-                 2 * rows * s->ncells);
+  return run_md(s, nsteps, dt, nullptr, thermo ? thermo_every : 0, row_fn, thermo,
+                2 * rows * s->ncells);
+}
+
+int tmd_batch_nvt_run(tmd_batch *b, int nsteps, double dt, const double *t_start,
+                      const double *t_stop, double t_damp, int thermo_every, double *thermo) {
+  if (int rc = batch_ok(b)) return rc;
+  tmd_system *s = b->s;
+  if (nsteps < 0 || !(dt > 0) || !t_start || !t_stop)
+    return fail(TMD_ERR_ARG, "bad nvt arguments");
+  for (int c = 0; c < s->ncells; c++)
+    if (!(t_start[c] > 0) || !(t_stop[c] > 0))
+      return fail(TMD_ERR_ARG, "fix nvt needs t_start and t_stop > 0 in every cell");
+  if (!(t_damp > 0)) return fail(TMD_ERR_ARG, "fix nvt needs t_damp > 0");
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before nvt_run");
+  if (thermo && thermo_every < 1) return fail(TMD_ERR_ARG, "thermo_every must be >= 1");
+  const long rows = thermo ? 1 + nsteps / thermo_every + ((nsteps % thermo_every) ? 1 : 0) : 0;
+  auto row_fn = [](tmd_system *q, int r) {
+    double *o = q->thermo_d + 2 * (size_t)r * q->ncells;
+    launch_cell_sum(q->ncells, q->coff, q->E, 1, 1.0, o, 2, q->st, q->launches);
+    launch_kinetic(q->n, q->v, q->elem, q->m->d_mass, q->ke, q->st, q->launches);
+    launch_cell_sum(q->ncells, q->coff, q->ke, 1, 1.0, o + 1, 2, q->st, q->launches);
+  };
+  const NvtSpec nvt{t_start, t_stop, t_damp};
+  return run_md(s, nsteps, dt, &nvt, thermo ? thermo_every : 0, row_fn, thermo,
+                2 * rows * s->ncells);
 }
 
 }  // extern "C"

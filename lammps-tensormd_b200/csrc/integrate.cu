@@ -153,6 +153,118 @@ void launch_nve_final(int n, double *v, const double *f, const int *elem,
   launches += 1;
 }
 
+// ---------------------------------------------------------------------
+// fix nvt (FixNH, fix_nh.cpp).  One thread per group runs the chain update;
+// the velocity factor is applied by a per-atom kernel.  With the default one
+// loop per half step (nc_tchain = 1) this is the same arithmetic as
+// nh_v_temp scaling every velocity by factor_eta.
+// ---------------------------------------------------------------------
+namespace {
+constexpr double kBoltz = 8.617343e-5;  // metal units, update.cpp:187-206
+
+// FixNH::nhc_temp_integrate (fix_nh.cpp:1758-1822), nc_tchain = 1, drag = 0
+// (the defaults, fix_nh.cpp:78-86), masses kept at the current target.
+__device__ void nhc_integrate(NhcState &c) {
+  const double dthalf = 0.5 * c.dt, dt4 = 0.25 * c.dt, dt8 = 0.125 * c.dt;
+  const double w2 = c.t_freq * c.t_freq;
+  double kecurrent = c.tdof * kBoltz * c.t_current;
+  c.eta_mass[0] = c.tdof * kBoltz * c.t_target / w2;
+  for (int k = 1; k < kNhcChain; k++) c.eta_mass[k] = kBoltz * c.t_target / w2;
+  c.eta_dotdot[0] = c.eta_mass[0] > 0.0 ? (kecurrent - c.ke_target) / c.eta_mass[0] : 0.0;
+  double expfac;
+  for (int k = kNhcChain - 1; k > 0; k--) {
+    expfac = exp(-dt8 * c.eta_dot[k + 1]);
+    c.eta_dot[k] *= expfac;
+    c.eta_dot[k] += c.eta_dotdot[k] * dt4;
+    c.eta_dot[k] *= expfac;
+  }
+  expfac = exp(-dt8 * c.eta_dot[1]);
+  c.eta_dot[0] *= expfac;
+  c.eta_dot[0] += c.eta_dotdot[0] * dt4;
+  c.eta_dot[0] *= expfac;
+  const double factor = exp(-dthalf * c.eta_dot[0]);
+  c.t_current *= factor * factor;
+  kecurrent = c.tdof * kBoltz * c.t_current;
+  c.eta_dotdot[0] = c.eta_mass[0] > 0.0 ? (kecurrent - c.ke_target) / c.eta_mass[0] : 0.0;
+  for (int k = 0; k < kNhcChain; k++) c.eta[k] += dthalf * c.eta_dot[k];
+  c.eta_dot[0] *= expfac;
+  c.eta_dot[0] += c.eta_dotdot[0] * dt4;
+  c.eta_dot[0] *= expfac;
+  for (int k = 1; k < kNhcChain; k++) {
+    expfac = exp(-dt8 * c.eta_dot[k + 1]);
+    c.eta_dot[k] *= expfac;
+    c.eta_dotdot[k] =
+        (c.eta_mass[k - 1] * c.eta_dot[k - 1] * c.eta_dot[k - 1] - kBoltz * c.t_target) /
+        c.eta_mass[k];
+    c.eta_dot[k] += c.eta_dotdot[k] * dt4;
+    c.eta_dot[k] *= expfac;
+  }
+  c.factor = factor;
+}
+}  // namespace
+
+// FixNH::setup (fix_nh.cpp:741-800) for a thermostat-only fix.
+__global__ void k_nhc_setup(int G, NhcState *__restrict__ st, const double *__restrict__ keg) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G) return;
+  NhcState c = st[g];
+  c.t_current = c.tdof > 0.0 ? 2.0 * keg[g] / (c.tdof * kBoltz) : 0.0;
+  c.t_target = c.t_start;
+  c.ke_target = c.tdof * kBoltz * c.t_target;
+  const double w2 = c.t_freq * c.t_freq;
+  c.eta_mass[0] = c.tdof * kBoltz * c.t_target / w2;
+  for (int k = 1; k < kNhcChain; k++) c.eta_mass[k] = kBoltz * c.t_target / w2;
+  for (int k = 1; k < kNhcChain; k++)
+    c.eta_dotdot[k] =
+        (c.eta_mass[k - 1] * c.eta_dot[k - 1] * c.eta_dot[k - 1] - kBoltz * c.t_target) /
+        c.eta_mass[k];
+  c.step = 0;
+  c.factor = 1.0;
+  st[g] = c;
+}
+
+__global__ void k_nhc_update(int G, NhcState *__restrict__ st, const double *__restrict__ keg) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G) return;
+  NhcState c = st[g];
+  if (keg == nullptr) {  // initial_integrate: FixNH::compute_temp_target
+    c.step++;
+    double delta = c.nsteps > 0 ? (double)c.step / (double)c.nsteps : 0.0;
+    c.t_target = c.t_start + delta * (c.t_stop - c.t_start);
+    c.ke_target = c.tdof * kBoltz * c.t_target;
+  } else {  // final_integrate: temperature after the second half kick
+    c.t_current = c.tdof > 0.0 ? 2.0 * keg[g] / (c.tdof * kBoltz) : 0.0;
+  }
+  if (c.tdof > 0.0 && c.t_freq > 0.0 && c.t_target > 0.0)
+    nhc_integrate(c);
+  else
+    c.factor = 1.0;
+  st[g] = c;
+}
+
+__global__ void k_nhc_scale(int n, const int *__restrict__ acell,
+                            const NhcState *__restrict__ st, double *__restrict__ v) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const double f = st[acell ? acell[a] : 0].factor;
+  v[3 * a] *= f;
+  v[3 * a + 1] *= f;
+  v[3 * a + 2] *= f;
+}
+
+void launch_nhc_setup(int ngroups, NhcState *st, const double *ke_group, cudaStream_t s,
+                      long &launches) {
+  k_nhc_setup<<<(ngroups + 127) / 128, 128, 0, s>>>(ngroups, st, ke_group);
+  launches += 1;
+}
+
+void launch_nhc_half(int ngroups, NhcState *st, const double *ke_group, int n,
+                     const int *acell, double *v, cudaStream_t s, long &launches) {
+  k_nhc_update<<<(ngroups + 127) / 128, 128, 0, s>>>(ngroups, st, ke_group);
+  if (n > 0) k_nhc_scale<<<(n + 255) / 256, 256, 0, s>>>(n, acell, st, v);
+  launches += 2;
+}
+
 // 0.5 * mvv2e * m * v^2 per atom (compute ke, metal mvv2e = 1.0364269e-4)
 __global__ void k_kinetic(int n, const double *__restrict__ v, const int *__restrict__ elem,
                           const double *__restrict__ mass_e, double *__restrict__ ke) {

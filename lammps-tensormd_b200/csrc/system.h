@@ -84,7 +84,14 @@ struct tmd_system {
   // captured MD step (velocity Verlet + rebuild check/rebuild + force)
   cudaGraphExec_t step_exec = nullptr;
   double step_dt = 0.0;
+  bool step_nvt = false;
   long step_launches = 0;
+  // fix nvt: one Nose-Hoover chain per group (cell, or the whole system);
+  // kept between runs of the same atoms like the fix's state in LAMMPS
+  tmd::NhcState *nhc = nullptr;
+  double *nhc_ke = nullptr;
+  int nhc_alloc = 0, nhc_groups = 0;
+  bool nhc_valid = false;
 };
 
 namespace tmd {
@@ -134,11 +141,17 @@ int cells_layout(tmd_system *s, int ncells, const int *natoms);
 int cells_geometry(tmd_system *s, const double *boxes, const int *pbc);
 // Make sure s->thermo_d holds count doubles.
 int thermo_reserve(tmd_system *s, long count);
-// Velocity Verlet for nsteps on the device (graph-captured step).  thermo_row(r)
-// enqueues thermo row r; it is called for the starting state (r = 0) and
-// every thermo_every steps and at the last step when thermo_every > 0.  On
-// success the first thermo_count doubles of s->thermo_d are copied to thermo.
-int run_nve(tmd_system *s, int nsteps, double dt, int thermo_every,
-            void (*thermo_row)(tmd_system *, int), double *thermo, long thermo_count);
+// fix nvt parameters, one target ramp per thermostat group (cell or system).
+struct NvtSpec {
+  const double *t_start, *t_stop;
+  double t_damp;
+};
+// Velocity Verlet for nsteps on the device (graph-captured step), with the
+// Nose-Hoover chain of fix nvt when nvt is given.  thermo_row(r) enqueues
+// thermo row r; it is called for the starting state (r = 0) and every
+// thermo_every steps and at the last step when thermo_every > 0.  On success
+// the first thermo_count doubles of s->thermo_d are copied to thermo.
+int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_every,
+           void (*thermo_row)(tmd_system *, int), double *thermo, long thermo_count);
 
 }  // namespace tmd

@@ -219,6 +219,27 @@ void launch_srv_post(int n, int ncells, const int *acell, const int *coff, CellC
                      double *fsq, double *cfmax, int kick, int count, cudaStream_t st,
                      long &launches);
 
+// ---- fix nvt: Nose-Hoover chain thermostat per group of atoms ----
+// (FixNH, fix_nh.cpp: chain of 3, one loop, no drag).  A group is a whole
+// system or one cell of a batch; goff[g]..goff[g+1]-1 are its atoms.
+constexpr int kNhcChain = 3;
+struct NhcState {
+  double eta[kNhcChain], eta_dot[kNhcChain + 1], eta_dotdot[kNhcChain], eta_mass[kNhcChain];
+  double t_current, t_target, ke_target, tdof, t_freq;
+  double t_start, t_stop;  // linear ramp of the target over the run
+  double dt, factor;       // step; velocity factor of the last chain update
+  int step, nsteps;        // steps run in this run / its length
+};
+// FixNH::setup: temperature from the group's kinetic energy, target, masses.
+void launch_nhc_setup(int ngroups, NhcState *st, const double *ke_group, cudaStream_t s,
+                      long &launches);
+// initial_integrate (step += 1, target of this step) or final_integrate
+// (temperature from ke_group): one chain update per group, then v of every
+// atom scaled by its group's factor (acell = group of each atom, or nullptr
+// for a single group).
+void launch_nhc_half(int ngroups, NhcState *st, const double *ke_group, int n,
+                     const int *acell, double *v, cudaStream_t s, long &launches);
+
 // Velocity Verlet halves (fix_nve.cpp:64-141).
 void launch_nve_initial(int n, double *x, double *v, const double *f,
                         const int *elem, const double *mass_e, double dtf,

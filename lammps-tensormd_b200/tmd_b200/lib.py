@@ -32,6 +32,9 @@ SIGNATURES = [
     ("tmd_system_get", _c_int, [_vp, _pd, _pd, _pd, _pi]),
     ("tmd_compute", _c_int, [_vp, _c_int, _c_int, _c_double, _pd, _pd, _pd, _pd, _pd]),
     ("tmd_nve_run", _c_int, [_vp, _c_int, _c_double, _c_int, _pd]),
+    ("tmd_nvt_run", _c_int, [_vp, _c_int, _c_double, _c_double, _c_double, _c_double, _c_int,
+                             _pd]),
+    ("tmd_nvt_energy", _c_int, [_vp, _pd]),
     ("tmd_neighbor_list", _c_int, [_vp, _c_double, _pi, _pi, _c_long, _pl]),
     ("tmd_get_descriptors", _c_int, [_vp, _pd]),
     ("tmd_system_stream", _c_int, [_vp, ctypes.POINTER(_vp)]),
@@ -47,6 +50,7 @@ SIGNATURES = [
     ("tmd_batch_get", _c_int, [_vp, _pd, _pd, _pd, _pi]),
     ("tmd_batch_compute", _c_int, [_vp, _pd, _pd, _pd]),
     ("tmd_batch_nve_run", _c_int, [_vp, _c_int, _c_double, _c_int, _pd]),
+    ("tmd_batch_nvt_run", _c_int, [_vp, _c_int, _c_double, _pd, _pd, _c_double, _c_int, _pd]),
     ("tmd_server_create", _c_int, [_vp, _c_int, _c_int, _c_double, _c_int,
                                    ctypes.POINTER(_vp)]),
     ("tmd_server_free", None, [_vp]),

@@ -132,6 +132,22 @@ class TensorMDSystem:
         check(self.lib.tmd_nve_run(self.h, int(nsteps), float(dt), int(thermo_every), _dp(th)))
         return th
 
+    def nvt_run(self, nsteps, dt, t_start, t_stop, t_damp, thermo_every=0):
+        """fix nvt temp t_start t_stop t_damp for nsteps (Nose-Hoover chain)."""
+        th = None
+        if thermo_every:
+            rows = 1 + nsteps // thermo_every + (1 if nsteps % thermo_every else 0)
+            th = np.zeros((rows, 2))
+        check(self.lib.tmd_nvt_run(self.h, int(nsteps), float(dt), float(t_start), float(t_stop),
+                                   float(t_damp), int(thermo_every), _dp(th)))
+        return th
+
+    def nvt_energy(self, ngroups=1):
+        """Thermostat chain energy per group after the last nvt run."""
+        e = np.zeros(ngroups)
+        check(self.lib.tmd_nvt_energy(self.h, _dp(e)))
+        return e
+
     def neighbor_list(self, cut):
         n = self.n
         counts = np.zeros(max(n, 1), dtype=np.int32)
@@ -234,6 +250,20 @@ class TensorMDBatch:
             th = np.zeros((rows, self.ncells, 2))
         check(self.lib.tmd_batch_nve_run(self.h, int(nsteps), float(dt), int(thermo_every),
                                          _dp(th)))
+        return th
+
+    def nvt_run(self, nsteps, dt, t_start, t_stop, t_damp, thermo_every=0):
+        """fix nvt per cell: t_start / t_stop scalars or one value per cell."""
+        ts = np.ascontiguousarray(np.broadcast_to(np.asarray(t_start, dtype=np.float64),
+                                                  (self.ncells,)))
+        te = np.ascontiguousarray(np.broadcast_to(np.asarray(t_stop, dtype=np.float64),
+                                                  (self.ncells,)))
+        th = None
+        if thermo_every:
+            rows = 1 + nsteps // thermo_every + (1 if nsteps % thermo_every else 0)
+            th = np.zeros((rows, self.ncells, 2))
+        check(self.lib.tmd_batch_nvt_run(self.h, int(nsteps), float(dt), _dp(ts), _dp(te),
+                                         float(t_damp), int(thermo_every), _dp(th)))
         return th
 
     def system(self) -> "TensorMDSystem":

@@ -267,6 +267,17 @@ class Oracle:
                                    ctypes.POINTER(ctypes.c_int), ctypes.c_double,
                                    ctypes.c_int, ctypes.c_double,
                                    ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+            L.tmdo_nvt.restype = ctypes.c_int
+            L.tmdo_nvt.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_int), ctypes.c_double,
+                                   ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double,
+                                   ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
             cls._lib = L
         return cls._lib
 
@@ -370,6 +381,27 @@ class Oracle:
                         _p(f, ctypes.c_double), th.ctypes.data)
         if rc != 0:
             raise RuntimeError("oracle nve failed")
+        return x, v, f, th
+
+    def nvt(self, x, v, elem, box, pbc, dt, nsteps, t_start, t_stop, t_damp, skin=1.0):
+        """fix nvt (Nose-Hoover chain of 3, fresh thermostat); returns
+        (x, v, f, thermo[n+1, 3] = pe, ke, chain energy)."""
+        L = self.lib()
+        x = np.array(x, dtype=np.float64, order="C")
+        v = np.array(v, dtype=np.float64, order="C")
+        n = x.shape[0]
+        el = np.ascontiguousarray(elem, dtype=np.int32)
+        bx = np.ascontiguousarray(box, dtype=np.float64)
+        pb = np.ascontiguousarray(pbc, dtype=np.int32)
+        ms = np.ascontiguousarray(self.masses, dtype=np.float64)
+        f = np.zeros((n, 3))
+        th = np.zeros((nsteps + 1, 3))
+        rc = L.tmdo_nvt(self.h, n, _p(x, ctypes.c_double), _p(v, ctypes.c_double),
+                        _p(el, ctypes.c_int), _p(ms, ctypes.c_double),
+                        _p(bx, ctypes.c_double), _p(pb, ctypes.c_int), dt, nsteps, skin,
+                        t_start, t_stop, t_damp, _p(f, ctypes.c_double), th.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("oracle nvt failed")
         return x, v, f, th
 
 

@@ -785,3 +785,163 @@ int tmdo_nve(void *h, int n, double *x, double *v, const int *elem,
   free(ent);
   return rc;
 }
+
+/* ------------------------------------------------------------------ */
+/* fix nvt: Nose-Hoover chain thermostat (FixNH, fix_nh.cpp)            */
+/* ------------------------------------------------------------------ */
+
+#define OM_BOLTZ 8.617343e-5
+#define OM_NHC 3 /* mtchain default (fix_nh.cpp:81) */
+
+typedef struct {
+  double eta[OM_NHC], eta_dot[OM_NHC + 1], eta_dotdot[OM_NHC], eta_mass[OM_NHC];
+  double t_current, t_target, ke_target, tdof, t_freq;
+} om_nhc;
+
+/* temperature of compute temp: mvv2e sum m v^2 / (dof boltz), dof = 3N - 3 */
+static double om_temp(int n, const double *v, const int *elem, const double *mass_e,
+                      double tdof)
+{
+  double s = 0.0;
+  for (int i = 0; i < n; i++)
+    s += mass_e[elem[i]] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] +
+                            v[3 * i + 2] * v[3 * i + 2]);
+  return s * OM_MVV2E / (tdof * OM_BOLTZ);
+}
+
+/* FixNH::nhc_temp_integrate (fix_nh.cpp:1758-1822) with nc_tchain = 1 and
+ * drag = 0 (the defaults, fix_nh.cpp:78-86); returns factor_eta. */
+static double om_nhc_integrate(om_nhc *c, double dt)
+{
+  const double dthalf = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
+  double kecurrent = c->tdof * OM_BOLTZ * c->t_current;
+  c->eta_mass[0] = c->tdof * OM_BOLTZ * c->t_target / (c->t_freq * c->t_freq);
+  for (int k = 1; k < OM_NHC; k++)
+    c->eta_mass[k] = OM_BOLTZ * c->t_target / (c->t_freq * c->t_freq);
+  c->eta_dotdot[0] = c->eta_mass[0] > 0.0 ? (kecurrent - c->ke_target) / c->eta_mass[0] : 0.0;
+  double expfac;
+  for (int k = OM_NHC - 1; k > 0; k--) {
+    expfac = exp(-dt8 * c->eta_dot[k + 1]);
+    c->eta_dot[k] *= expfac;
+    c->eta_dot[k] += c->eta_dotdot[k] * dt4;
+    c->eta_dot[k] *= expfac;
+  }
+  expfac = exp(-dt8 * c->eta_dot[1]);
+  c->eta_dot[0] *= expfac;
+  c->eta_dot[0] += c->eta_dotdot[0] * dt4;
+  c->eta_dot[0] *= expfac;
+  const double factor = exp(-dthalf * c->eta_dot[0]);
+  c->t_current *= factor * factor;
+  kecurrent = c->tdof * OM_BOLTZ * c->t_current;
+  c->eta_dotdot[0] = c->eta_mass[0] > 0.0 ? (kecurrent - c->ke_target) / c->eta_mass[0] : 0.0;
+  for (int k = 0; k < OM_NHC; k++) c->eta[k] += dthalf * c->eta_dot[k];
+  c->eta_dot[0] *= expfac;
+  c->eta_dot[0] += c->eta_dotdot[0] * dt4;
+  c->eta_dot[0] *= expfac;
+  for (int k = 1; k < OM_NHC; k++) {
+    expfac = exp(-dt8 * c->eta_dot[k + 1]);
+    c->eta_dot[k] *= expfac;
+    c->eta_dotdot[k] = (c->eta_mass[k - 1] * c->eta_dot[k - 1] * c->eta_dot[k - 1] -
+                        OM_BOLTZ * c->t_target) / c->eta_mass[k];
+    c->eta_dot[k] += c->eta_dotdot[k] * dt4;
+    c->eta_dot[k] *= expfac;
+  }
+  return factor;
+}
+
+/* Energy of the chain, FixNH::compute_scalar (fix_nh.cpp:1447-1473). */
+static double om_nhc_energy(const om_nhc *c)
+{
+  double kt = OM_BOLTZ * c->t_target;
+  double e = c->ke_target * c->eta[0] + 0.5 * c->eta_mass[0] * c->eta_dot[0] * c->eta_dot[0];
+  for (int k = 1; k < OM_NHC; k++)
+    e += kt * c->eta[k] + 0.5 * c->eta_mass[k] * c->eta_dot[k] * c->eta_dot[k];
+  return e;
+}
+
+/* nsteps of fix nvt temp t_start t_stop t_damp (Verlet + FixNH::setup /
+ * initial_integrate / final_integrate, fix_nh.cpp:741-930) from a fresh
+ * thermostat; thermo[(nsteps+1)*3] = (pe, ke, chain energy) after every
+ * step. */
+int tmdo_nvt(void *h, int n, double *x, double *v, const int *elem,
+             const double *mass_e, const double *boxv, const int *pbc, double dt,
+             int nsteps, double skin, double t_start, double t_stop, double t_damp,
+             double *f, double *thermo)
+{
+  om_model *m = (om_model *)h;
+  om_box b;
+  om_box_from(boxv, pbc, &b);
+  double cut = m->rmax + skin;
+  double dtf = 0.5 * dt * OM_FTM2V;
+  long *off = (long *)malloc(sizeof(long) * (n + 1));
+  int *cnt = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+  int *ent = NULL;
+  long cap = 0;
+  om_nhc c;
+  memset(&c, 0, sizeof c);
+  c.tdof = 3.0 * n - 3.0;
+  c.t_freq = 1.0 / t_damp;
+  for (int step = 0; step <= nsteps; step++) {
+    if (step == 0) {
+      /* FixNH::setup */
+      c.t_current = om_temp(n, v, elem, mass_e, c.tdof);
+      c.t_target = t_start;
+      c.ke_target = c.tdof * OM_BOLTZ * c.t_target;
+      c.eta_mass[0] = c.tdof * OM_BOLTZ * c.t_target / (c.t_freq * c.t_freq);
+      for (int k = 1; k < OM_NHC; k++)
+        c.eta_mass[k] = OM_BOLTZ * c.t_target / (c.t_freq * c.t_freq);
+      for (int k = 1; k < OM_NHC; k++)
+        c.eta_dotdot[k] = (c.eta_mass[k - 1] * c.eta_dot[k - 1] * c.eta_dot[k - 1] -
+                           OM_BOLTZ * c.t_target) / c.eta_mass[k];
+    } else {
+      /* initial_integrate: compute_temp_target, nhc, nve_v, nve_x */
+      double delta = (double)step / (double)nsteps;
+      c.t_target = t_start + delta * (t_stop - t_start);
+      c.ke_target = c.tdof * OM_BOLTZ * c.t_target;
+      double fe = om_nhc_integrate(&c, dt);
+      for (int i = 0; i < 3 * n; i++) v[i] *= fe;
+      for (int i = 0; i < n; i++) {
+        double dtfm = dtf / mass_e[elem[i]];
+        for (int a = 0; a < 3; a++) {
+          v[3 * i + a] += dtfm * f[3 * i + a];
+          x[3 * i + a] += dt * v[3 * i + a];
+        }
+      }
+      om_remap(&b, n, x);
+    }
+    long tot = tmdo_neighbors(n, x, boxv, pbc, cut, cnt, NULL, 0);
+    if (tot > cap) {
+      free(ent);
+      cap = tot + tot / 4 + 16;
+      ent = (int *)malloc(sizeof(int) * 4 * cap);
+    }
+    tmdo_neighbors(n, x, boxv, pbc, cut, cnt, ent, cap);
+    off[0] = 0;
+    for (int i = 0; i < n; i++) off[i + 1] = off[i] + cnt[i];
+    double pe = tmdo_compute(h, n, x, elem, boxv, pbc, off, ent, 1.0, NULL, f,
+                             NULL, NULL, NULL, NULL);
+    if (step > 0) {
+      /* final_integrate: nve_v, t_current, nhc */
+      for (int i = 0; i < n; i++) {
+        double dtfm = dtf / mass_e[elem[i]];
+        for (int a = 0; a < 3; a++) v[3 * i + a] += dtfm * f[3 * i + a];
+      }
+      c.t_current = om_temp(n, v, elem, mass_e, c.tdof);
+      double fe = om_nhc_integrate(&c, dt);
+      for (int i = 0; i < 3 * n; i++) v[i] *= fe;
+    }
+    if (thermo) {
+      double ke = 0.0;
+      for (int i = 0; i < n; i++)
+        ke += mass_e[elem[i]] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] +
+                                 v[3 * i + 2] * v[3 * i + 2]);
+      thermo[3 * step] = pe;
+      thermo[3 * step + 1] = 0.5 * OM_MVV2E * ke;
+      thermo[3 * step + 2] = om_nhc_energy(&c);
+    }
+  }
+  free(off);
+  free(cnt);
+  free(ent);
+  return 0;
+}
