@@ -355,6 +355,7 @@ def run_ours(args, rank, world, local):
     serving = None
     if args.serve_window > 0:
         serving = run_serving(args, rank, local)
+    w23k = run_w23k(args, rank, world, local, dev, barrier)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -379,6 +380,7 @@ def run_ours(args, rank, world, local):
             "forms": forms,
             "cells4096": cells,
             "serving": serving,
+            "reference_workload_w23k": w23k,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -441,6 +443,52 @@ def run_cells(args, rank, world, local, dev, barrier):
     b.close()
     model.close()
     return out
+
+
+def run_w23k(args, rank, world, local, dev, barrier):
+    """The reference's own speed benchmark, run the same way: W_k32_snapshot.npz
+    (shipped trained potential, FNN radial net + rational table, interp
+    0.001), BCC a = 3.189 A, 24x24x20 cells = 23,040 atoms, velocities 300 K,
+    fix nvt temp 300 300 0.1, 100 steps, skin 1 A
+    (examples/tensormd/W/tensormd/speedup/in.lammps).  Published on an A100:
+    3.221 M atom-steps/s (log_0114.lammps, the reference's optimized build)."""
+    import torch
+    from tmd_b200 import TensorMDModel, TensorMDSystem, synth
+    model = TensorMDModel(f"{ROOT}/tests/golden/W_k32_snapshot.npz W interp 0.001", device=local)
+    x, box = synth.lattice("bcc", 3.189, 24, 24, 20)
+    n = len(x)
+    t = np.ones(n, dtype=np.int32)
+    v = synth.maxwell(np.full(n, model.type_mass[1]), 300.0, np.random.default_rng(984523 + rank))
+    s = TensorMDSystem(model, n, 1.0)
+    s.set_box(box)
+    s.set_atoms(x, t, v)
+    stream = torch.cuda.ExternalStream(s.stream(), device=dev)
+    s.nvt_run(max(args.warmup, 3), 0.001, 300.0, 300.0, 0.1)
+    s.set_atoms(x, t, v)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    s.nvt_run(100, 0.001, 300.0, 300.0, 0.1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier()
+    ms = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms = float(ms.item())
+    value = n * 100 * world / (ms / 1000.0)
+    s.close()
+    model.close()
+    return {"value": value, "unit": UNIT, "ms_per_step": ms / 100, "natoms": n, "steps": 100,
+            "host_wall_s": wall, "published_a100": 3.221e6, "ratio_vs_published_a100": value / 3.221e6,
+            "config": "W_k32_snapshot.npz interp 0.001, bcc 3.189 24x24x20, 300 K, "
+                      "fix nvt temp 300 300 0.1, skin 1.0, dt 1 fs"}
 
 
 def run_serving(args, rank, local):

@@ -207,7 +207,9 @@ NbArgs nb_args(tmd_system *s) {
   a.cell_of = s->cell_of; a.cell_count = s->cell_count; a.cell_start = s->cell_start;
   a.cell_cursor = s->cell_cursor; a.cell_atoms = s->cell_atoms;
   a.tmp = s->tmp; a.nraw = s->nraw; a.nbr = s->nbr; a.boff = s->boff; a.rev = s->rev;
-  a.xbuild = s->xbuild; a.flag = s->flag; a.status = s->status; a.maxneed = s->maxneed;
+  // status[0]: status bits; status[1]: the longest row a build needed (read
+  // back and cleared together by read_status)
+  a.xbuild = s->xbuild; a.flag = s->flag; a.status = s->status; a.maxneed = s->status + 1;
   a.ncells = s->ncells; a.cbox = s->cbox; a.cgeom = s->cgeom; a.acell = s->acell;
   a.coff = s->coff;
   return a;
@@ -356,6 +358,37 @@ int thermo_reserve(tmd_system *s, long count) {
   return TMD_OK;
 }
 
+// Device checkpoint of the dynamic state for rolling back a chunk of steps.
+int checkpoint_reserve(tmd_system *s) {
+  if (!s->ck_x) {
+    const size_t N = s->natoms_cap;
+    TMD_CUDA(dalloc(&s->ck_x, 3 * N));
+    TMD_CUDA(dalloc(&s->ck_v, 3 * N));
+    TMD_CUDA(dalloc(&s->ck_f, 3 * N));
+    TMD_CUDA(dalloc(&s->ck_img, 3 * N));
+  }
+  if (s->nhc_alloc > s->ck_nhc_alloc) {
+    dfree(s->ck_nhc);
+    TMD_CUDA(dalloc(&s->ck_nhc, s->nhc_alloc));
+    s->ck_nhc_alloc = s->nhc_alloc;
+  }
+  return TMD_OK;
+}
+
+// save: state -> checkpoint; else checkpoint -> state (stream-ordered).
+void checkpoint_copy(tmd_system *s, bool save) {
+  const size_t b3 = 3 * (size_t)s->n * sizeof(double), i3 = 3 * (size_t)s->n * sizeof(int);
+  auto cp = [&](void *live, void *ck, size_t bytes) {
+    if (bytes == 0) return;
+    cudaMemcpyAsync(save ? ck : live, save ? live : ck, bytes, cudaMemcpyDeviceToDevice, s->st);
+  };
+  cp(s->x, s->ck_x, b3);
+  cp(s->v, s->ck_v, b3);
+  cp(s->f, s->ck_f, b3);
+  cp(s->image, s->ck_img, i3);
+  if (s->nhc_valid && s->ck_nhc) cp(s->nhc, s->ck_nhc, s->nhc_groups * sizeof(NhcState));
+}
+
 // Kinetic energy of every thermostat group into s->nhc_ke.
 void group_ke(tmd_system *s) {
   launch_kinetic(s->n, s->v, s->elem, s->m->d_mass, s->ke, s->st, s->launches);
@@ -451,7 +484,9 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
   // launch (including the conditional rebuild kernels) is replayed with its
   // arguments fixed at capture; buffers, box, atom count and dt key the graph.
   const bool use_graph = !s->prof;
-  if (use_graph && (!s->step_exec || s->step_dt != dt || s->step_nvt != (nvt != nullptr))) {
+  auto ensure_graph = [&]() -> int {
+    if (!use_graph || (s->step_exec && s->step_dt == dt && s->step_nvt == (nvt != nullptr)))
+      return TMD_OK;
     drop_graph(s);
     cudaGraph_t g;
     long l0 = s->launches;
@@ -468,34 +503,65 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
     s->launches = l0;
     s->step_dt = dt;
     s->step_nvt = nvt != nullptr;
-  }
-  for (int step = 1; step <= nsteps; step++) {
-    if (use_graph) {
-      TMD_CUDA(cudaGraphLaunch(s->step_exec, s->st));
-      s->launches += s->step_launches;
-    } else {
-      md_step();
+    return TMD_OK;
+  };
+  rc = ensure_graph();
+  if (rc) return rc;
+  // Steps run in chunks from a device checkpoint (x, v, f, image flags,
+  // thermostat).  A neighbor row that outgrew its capacity during a chunk
+  // truncated that step's list, so the chunk is rolled back, the capacity
+  // grown and the chunk run again: the trajectory is the one a large enough
+  // list gives.
+  constexpr int kChunk = 256;
+  rc = checkpoint_reserve(s);
+  if (rc) return rc;
+  for (int s0 = 1, retries = 0; s0 <= nsteps;) {
+    const int s1 = std::min(nsteps, s0 + kChunk - 1);
+    const int row0 = row;
+    checkpoint_copy(s, true);
+    for (int step = s0; step <= s1; step++) {
+      if (use_graph) {
+        TMD_CUDA(cudaGraphLaunch(s->step_exec, s->st));
+        s->launches += s->step_launches;
+      } else {
+        md_step();
+      }
+      if (want_thermo && (step % thermo_every == 0 || step == nsteps)) {
+        prof_begin(s);
+        thermo_row(s, row++);
+        prof_end(s, 6);
+      }
     }
-    if (want_thermo && (step % thermo_every == 0 || step == nsteps)) {
-      prof_begin(s);
-      thermo_row(s, row++);
-      prof_end(s, 6);
+    launch_check_finite(n, s->f, nullptr, s->status, s->st, s->launches);
+    TMD_CUDA(cudaGetLastError());
+    rc = read_status(s);
+    if (rc) return rc;
+    const int st = s->h_status[0];
+    if (st & kStatusOverflow) {
+      if (++retries > 8) return fail(TMD_ERR_CAPACITY, "neighbor list kept overflowing");
+      // size the rows for the longest one any rebuild of the chunk needed
+      // (the restored positions may not need it yet), then rebuild there
+      const int need = s->h_status[1];
+      checkpoint_copy(s, false);
+      rc = alloc_neighbors(s, std::max(need + need / 4 + 32, s->cap + 32));  // drops the graph
+      if (rc) return rc;
+      rc = rebuild_now(s);
+      if (rc) return rc;
+      rc = ensure_graph();
+      if (rc) return rc;
+      row = row0;
+      continue;
     }
+    if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
+    if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
+    if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite force during the run");
+    s0 = s1 + 1;
   }
-  launch_check_finite(n, s->f, nullptr, s->status, s->st, s->launches);
-  TMD_CUDA(cudaGetLastError());
-  if (want_thermo && thermo_count > 0)
+  if (want_thermo && thermo_count > 0) {
     TMD_CUDA(cudaMemcpyAsync(thermo, s->thermo_d, thermo_count * sizeof(double),
                              cudaMemcpyDeviceToHost, s->st));
-  rc = read_status(s);
-  if (rc) return rc;
-  int st = s->h_status[0];
-  if (st & kStatusOverflow)
-    return fail(TMD_ERR_CAPACITY, "neighbor list overflow during the run (raise the "
-                                  "capacity by calling set_atoms again)");
-  if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
-  if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
-  if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite force during the run");
+    TMD_CUDA(cudaStreamSynchronize(s->st));
+  }
   s->forces_valid = true;
   return TMD_OK;
 }
@@ -726,7 +792,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   A(P, N * h.nelt * h.K * h.D); A(G, N * h.nin); A(dEdG, N * h.nin); A(E, N);
   A(wv, 6 * N); A(eatom, N); A(vatom, 6 * N); A(ke, N);
   A(partial, 1024 * 8); A(scal, 8);
-  A(flag, 1); A(status, 2); A(maxneed, 1);
+  A(flag, 1); A(status, 2);
   A(perm, N); A(tiles, 3 * (N / 32 + h.nelt + 1));
 #undef A
   if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&s->h_scal), 8 * sizeof(double));
@@ -734,7 +800,6 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   if (e == cudaSuccess) e = cudaMemset(s->v, 0, 3 * N * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(s->image, 0, 3 * N * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(s->status, 0, 2 * sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(s->maxneed, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(s->flag, 0, sizeof(int));
   if (e != cudaSuccess) {
     tmd_system_free(s);
@@ -754,10 +819,11 @@ void tmd_system_free(tmd_system *s) {
   dfree(s->cell_atoms); dfree(s->tmp); dfree(s->nbr); dfree(s->nraw); dfree(s->boff);
   dfree(s->rev); dfree(s->P); dfree(s->G); dfree(s->dEdG); dfree(s->E); dfree(s->pdf);
   dfree(s->wv); dfree(s->eatom); dfree(s->vatom); dfree(s->ke); dfree(s->partial);
-  dfree(s->scal); dfree(s->flag); dfree(s->status); dfree(s->maxneed); dfree(s->perm);
+  dfree(s->scal); dfree(s->flag); dfree(s->status); dfree(s->perm);
   dfree(s->tiles); dfree(s->thermo_d);
   dfree(s->cbox); dfree(s->cgeom); dfree(s->acell); dfree(s->coff); dfree(s->cell_out);
   dfree(s->nhc); dfree(s->nhc_ke);
+  dfree(s->ck_x); dfree(s->ck_v); dfree(s->ck_f); dfree(s->ck_img); dfree(s->ck_nhc);
   if (s->h_scal) cudaFreeHost(s->h_scal);
   if (s->h_status) cudaFreeHost(s->h_status);
   for (auto &p : s->ev_pending) {

@@ -65,7 +65,7 @@ struct tmd_system {
   float4 *pdf = nullptr;
   double *wv = nullptr, *eatom = nullptr, *vatom = nullptr, *ke = nullptr;
   double *partial = nullptr, *scal = nullptr;  // scal: [0] pe, [1..6] virial, [7] ke
-  int *flag = nullptr, *status = nullptr, *maxneed = nullptr;
+  int *flag = nullptr, *status = nullptr;  // status[0] bits, status[1] longest row needed
   int *perm = nullptr, *tiles = nullptr;
   int ntiles = 0;
   double *thermo_d = nullptr;
@@ -92,6 +92,11 @@ struct tmd_system {
   double *nhc_ke = nullptr;
   int nhc_alloc = 0, nhc_groups = 0;
   bool nhc_valid = false;
+  // checkpoint of the dynamic state at the start of each chunk of MD steps
+  double *ck_x = nullptr, *ck_v = nullptr, *ck_f = nullptr;
+  int *ck_img = nullptr;
+  tmd::NhcState *ck_nhc = nullptr;
+  int ck_nhc_alloc = 0;
 };
 
 namespace tmd {

@@ -161,6 +161,34 @@ def test_nve_matches_oracle(fcc4k):
     assert th[-1, 0] + th[-1, 1] == pytest.approx(tho[-1, 0] + tho[-1, 1], abs=2e-7 * len(x))
 
 
+def test_nve_list_outgrows_its_capacity(tmp_path):
+    """An imploding cell (density 0.02 A^-3 at the start, velocities toward
+    the centre) outgrows the neighbor capacity sized at set_atoms during the
+    run; the chunk is rolled back, the list grown and the steps rerun, so the
+    run ends normally and follows the oracle, which has no capacity limit."""
+    p = tmp_path / "pot.npz"
+    syms = synth.gaussian_potential(p, nelt=1, num_filters=16, rc=6.0, max_moment=3,
+                                    hidden=(32, 32), actfn=2, seed=21)
+    a = 0.02 ** (-1.0 / 3.0)
+    x, t, box, _ = synth.build_system("sc", a, (6, 6, 6), sigma=0.05, seed=3)
+    c = box[3:6] / 2.0
+    v = -30.0 * (x - c)  # 40% of the distance to the centre after 20 fs
+    m = TensorMDModel(f"{p} {' '.join(syms)}")
+    s = TensorMDSystem(m, len(x), 1.0)
+    s.set_box(box)
+    s.set_atoms(x, t, v)
+    cap0 = max(np.diff(s.neighbor_list(m.cutmax + 1.0)[0]))
+    th = s.nve_run(20, 0.001, thermo_every=10)
+    cap1 = max(np.diff(s.neighbor_list(m.cutmax + 1.0)[0]))
+    assert cap1 > 2 * cap0  # the rows grew well beyond the first estimate
+    xo, vo, fo, tho = Oracle(str(p)).nve(x, v, t - 1, box, [1, 1, 1], 0.001, 20, skin=1.0)
+    xg = s.get()[0]
+    L = box[3:6]
+    dx = (xg - xo) - np.round((xg - xo) / L) * L
+    assert np.abs(dx).max() < 1e-5
+    np.testing.assert_allclose(th[-1], tho[-1], rtol=1e-5)
+
+
 def test_nve_energy_drift(fcc4k):
     """Total energy over 1,000 steps of 1 fs stays within 1e-5 eV/atom."""
     p, syms, x, t, box, v = fcc4k
