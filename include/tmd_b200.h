@@ -39,7 +39,7 @@ extern "C" {
  * FP64 cutoff test, energy/virial sums and position update). */
 #define TMD_PREC_FP32 0
 #define TMD_PREC_BF16 1
-#define TMD_PREC_FP8 2
+#define TMD_PREC_FP8 2    /* e4m3 tensor-core MLP, per-layer weight and per-row operand scales */
 #define TMD_PREC_BF16X3 3 /* split BF16 products: FP32-class accuracy */
 
 typedef struct tmd_model tmd_model;

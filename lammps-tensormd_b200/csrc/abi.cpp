@@ -277,7 +277,8 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
     ta.G = s->G; ta.dEdG = s->dEdG; ta.E = s->E; ta.layers = m->d_tc_layers;
     ta.status = s->status; ta.smem = m->tc_smem; ta.dz_bf16 = m->tc_dz_bf16 ? 1 : 0;
     ta.np = m->tc_np;
-    launch_mlp_tc(ta, s->st, s->launches);
+    if (m->tc_fp8) launch_mlp_fp8(ta, s->st, s->launches);
+    else launch_mlp_tc(ta, s->st, s->launches);
   } else {
     launch_mlp_fp32(ma, s->st, s->launches);
   }
@@ -658,19 +659,24 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
   }
   mlp_fp32_prepare(m->mlp_tr, m->mlp_smem);
   for (int l = 1; l < h.nl; l++) m->maxh = std::max(m->maxh, h.sizes[l]);
-  if (h.precision == TMD_PREC_BF16 || h.precision == TMD_PREC_BF16X3) {
+  if (h.precision == TMD_PREC_BF16 || h.precision == TMD_PREC_BF16X3 ||
+      h.precision == TMD_PREC_FP8) {
+    const bool fp8 = h.precision == TMD_PREC_FP8;
     const int np = h.precision == TMD_PREC_BF16X3 ? 3 : 1;
     m->tc_np = np;
+    m->tc_fp8 = fp8;
     // tcgen05 MLP: 128-atom tiles, widths in multiples of the 64-column chunk
     bool shape_ok = h.nin % 64 == 0 && h.nin <= 1024;
     for (int l = 1; l < h.nl; l++) shape_ok = shape_ok && h.sizes[l] % 64 == 0 && h.sizes[l] <= 128;
     if (!shape_ok) {
       tmd_model_free(m);
-      return fail(TMD_ERR_MODEL, "precision bf16 needs nelt*k*m and hidden widths that are "
-                                 "multiples of 64, hidden widths <= 128");
+      return fail(TMD_ERR_MODEL, "precision bf16/fp8 needs nelt*k*m and hidden widths that "
+                                 "are multiples of 64, hidden widths <= 128");
     }
-    size_t sm32 = mlp_tc_smem(h.nl, m->maxh, h.resnet, false, np);
-    size_t sm16 = mlp_tc_smem(h.nl, m->maxh, h.resnet, true, np);
+    size_t sm32 = fp8 ? mlp_fp8_smem(h.nl, m->maxh, h.resnet, false)
+                      : mlp_tc_smem(h.nl, m->maxh, h.resnet, false, np);
+    size_t sm16 = fp8 ? mlp_fp8_smem(h.nl, m->maxh, h.resnet, true)
+                      : mlp_tc_smem(h.nl, m->maxh, h.resnet, true, np);
     const size_t kSmemMax = 227 * 1024;
     if (sm32 <= kSmemMax / 2 || (sm32 <= kSmemMax && sm16 > kSmemMax / 2)) {
       m->tc_smem = sm32; m->tc_dz_bf16 = false;
@@ -690,7 +696,27 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
         T.b = F.b;
         T.wd = F.Wd;
         T.bd = F.bd;
-        if (l < h.nl - 1) {
+        T.wscale = 1.f;
+        if (l < h.nl - 1 && fp8) {
+          // one scale per layer: s_w = 448 / max|W| (e4m3 range)
+          const int K = T.K, N = T.N;
+          const std::vector<float> &W = h.W[el][l];
+          float wmax = 0.f;
+          for (float w : W) wmax = std::max(wmax, std::fabs(w));
+          T.wscale = wmax > 0.f ? 448.f / wmax : 1.f;
+          std::vector<uint8_t> pf((size_t)N * K), pb((size_t)K * N);
+          pack_core_chunks_fp8(W.data(), N, K, 1, N, T.wscale, pf.data());  // W^T
+          pack_core_chunks_fp8(W.data(), K, N, N, 1, T.wscale, pb.data());  // W
+          for (auto *vec : {&pf, &pb}) {
+            uint8_t *d = nullptr;
+            if (e == cudaSuccess) e = dalloc(&d, vec->size());
+            if (e == cudaSuccess) {
+              m->d_buf.push_back(reinterpret_cast<float *>(d));
+              e = cudaMemcpy(d, vec->data(), vec->size(), cudaMemcpyHostToDevice);
+            }
+            if (vec == &pf) T.Wf = d; else T.Wb = d;
+          }
+        } else if (l < h.nl - 1) {
           const int K = T.K, N = T.N;
           const size_t nf = (size_t)N * K, nbk = (size_t)K * N;
           std::vector<uint16_t> pf(nf * np), pb(nbk * np);
@@ -724,13 +750,12 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
                      cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
       tmd_model_free(m);
-      return fail(TMD_ERR_CUDA, std::string("bf16 weight upload: ") + cudaGetErrorString(e));
+      return fail(TMD_ERR_CUDA, std::string("tensor-core weight upload: ") +
+                                    cudaGetErrorString(e));
     }
-    mlp_tc_prepare(m->tc_smem, m->tc_dz_bf16, np);
+    if (fp8) mlp_fp8_prepare(m->tc_smem, m->tc_dz_bf16);
+    else mlp_tc_prepare(m->tc_smem, m->tc_dz_bf16, np);
     m->mlp_tr = 128;
-  } else if (h.precision != TMD_PREC_FP32) {
-    tmd_model_free(m);
-    return fail(TMD_ERR_MODEL, "precision fp8 is not available in this build");
   }
   *out = m;
   return TMD_OK;

@@ -24,6 +24,7 @@ struct tmd_model {
   size_t tc_smem = 0;
   bool tc_dz_bf16 = false;
   int tc_np = 1;
+  bool tc_fp8 = false;   // FP8 (e4m3) tensor-core MLP
   int maxh = 1;
   double *d_mass = nullptr;     // per element
   int mlp_tr = 64;

@@ -102,6 +102,7 @@ struct MlpTcLayer {
   const float *b;    // [N] bias (hidden layers)
   const double *wd;  // output layer weights (FP64), last layer only
   const double *bd;  // output bias (FP64) or nullptr, last layer only
+  float wscale;      // FP8 form: packed weights are e4m3(W * wscale); 1 otherwise
 };
 struct MlpTcArgs {
   int nl, actfn, resnet, nin, maxh, ntiles;
@@ -123,6 +124,14 @@ void mlp_tc_prepare(size_t smem, bool dz_bf16, int np);
 // into 64-column chunks of 8x8 BF16 core matrices, K-major.
 void pack_core_chunks(const float *src, int rows, int cols, long ld_r, long ld_k,
                       uint16_t *dst);
+
+// FP8 (e4m3) form of the tensor-core MLP (mlp_fp8.cu): same arguments, packed
+// weights e4m3(W * wscale) in 8x16 core matrices, per-row operand scales.
+void launch_mlp_fp8(const MlpTcArgs &a, cudaStream_t st, long &launches);
+size_t mlp_fp8_smem(int nl, int maxh, int resnet, bool dz_bf16);
+void mlp_fp8_prepare(size_t smem, bool dz_bf16);
+void pack_core_chunks_fp8(const float *src, int rows, int cols, long ld_r, long ld_k,
+                          float scale, uint8_t *dst);
 
 // dE/dP: S[n][B][K][D] = 2 P sum_m T[m][d] dEdG'[b][k][m] (dEdG'0 =
 // 0.5 dEdG0 / G0), written over P in place.
