@@ -140,6 +140,26 @@ int tmd_neighbor_list(tmd_system *sys, double cut, int *counts, int *entries,
  * compute_tensormd_density.cpp:129-200) of the last compute, in atom order. */
 int tmd_get_descriptors(tmd_system *sys, double *G);
 
+/* Kernel forms of the pair loops.  The reference has one implementation per
+ * phase (kernel.cu); here a phase may have several kernels that compute the
+ * same quantities with different thread mappings, and the fastest depends on
+ * the potential's shape (filters, monomials, elements) and the neighbor
+ * count.  Family TMD_TUNE_FORCE (the pair-force loop, kernel.cu:541-631):
+ *   0  K/4 lanes per atom, 4 filters per lane, partial forces summed over lanes
+ *   1  8 lanes per atom, one whole pair per lane, dE/dP staged in shared memory
+ *   2  16 lanes per atom, as 1
+ *   3  32 lanes per atom, as 1
+ * The forms agree to FP32 rounding (summation order).  set_variant picks one;
+ * autotune runs one evaluation, times reps launches of every form of the
+ * family on the system's current atoms, keeps the fastest and recomputes the
+ * forces with it; ms[TMD_TUNE_VARIANTS] (may be NULL) receives the mean
+ * device milliseconds per launch of each form. */
+#define TMD_TUNE_FORCE 0
+#define TMD_TUNE_VARIANTS 4
+int tmd_system_set_variant(tmd_system *sys, int family, int variant);
+int tmd_system_get_variant(tmd_system *sys, int family, int *variant);
+int tmd_system_autotune(tmd_system *sys, int family, int reps, double *ms);
+
 /* CUDA stream of the system (cudaStream_t as void*), for event timing. */
 int tmd_system_stream(tmd_system *sys, void **stream);
 

@@ -253,6 +253,23 @@ int rebuild_now(tmd_system *s) {
 }
 
 // Force evaluation on the current (valid) list.
+int default_force_variant(const tmd_model *m) {
+  // measured on the B200 (tmd_system_autotune): whole pairs per lane beat 4
+  // filters per lane by 1.2-1.6x; 16 lanes per atom for one element block
+  // (~70 pairs per block), 8 when the pairs split over several blocks
+  return m->kp.B > 1 ? kForcePairLane8 : kForcePairLane16;
+}
+
+ForceArgs force_args(tmd_system *s, float scale, int variant) {
+  ForceArgs fa{};
+  fa.n = s->n; fa.cap = s->cap; fa.kp = s->m->kp; fa.box = s->box; fa.scale = scale;
+  fa.x = s->x; fa.elem = s->elem; fa.nbr = s->nbr; fa.boff = s->boff; fa.S = s->P;
+  fa.pdf = s->pdf; fa.wv = s->wv;
+  fa.cbox = s->ncells ? s->cbox : nullptr; fa.acell = s->acell;
+  fa.variant = variant;
+  return fa;
+}
+
 void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   const tmd_model *m = s->m;
   DescArgs d{};
@@ -286,11 +303,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   prof_begin(s);
   launch_dedp(s->n, m->kp, s->P, s->G, s->dEdG, s->st, s->launches);  // P becomes S
   prof_end(s, 7);
-  ForceArgs fa{};
-  fa.n = s->n; fa.cap = s->cap; fa.kp = m->kp; fa.box = s->box; fa.scale = scale;
-  fa.x = s->x; fa.elem = s->elem; fa.nbr = s->nbr; fa.boff = s->boff; fa.S = s->P;
-  fa.pdf = s->pdf; fa.wv = s->wv;
-  fa.cbox = d.cbox; fa.acell = s->acell;
+  const ForceArgs fa = force_args(s, scale, s->force_variant);
   prof_begin(s);
   launch_force(fa, s->st, s->launches);
   prof_end(s, 3);
@@ -806,6 +819,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   s->m = m;
   s->natoms_cap = natoms_cap;
   s->skin = skin;
+  s->force_variant = default_force_variant(m);
   const HostModel &h = m->h;
   size_t N = natoms_cap;
   cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
@@ -1098,6 +1112,64 @@ int tmd_get_descriptors(tmd_system *s, double *G) {
   }
   for (size_t i = 0; i < cnt; i++) G[i] = tmp[i];
   return TMD_OK;
+}
+
+int tmd_system_set_variant(tmd_system *s, int family, int variant) {
+  if (!s) return fail(TMD_ERR_ARG, "null system");
+  if (family != TMD_TUNE_FORCE) return fail(TMD_ERR_ARG, "unknown kernel family");
+  if (variant < 0 || variant >= kForceVariants) return fail(TMD_ERR_ARG, "unknown variant");
+  if (variant != s->force_variant) {
+    TMD_CUDA(cudaStreamSynchronize(s->st));
+    drop_graph(s);  // the captured step holds the old kernel
+    s->force_variant = variant;
+  }
+  return TMD_OK;
+}
+
+int tmd_system_get_variant(tmd_system *s, int family, int *variant) {
+  if (!s || !variant) return fail(TMD_ERR_ARG, "null argument");
+  if (family != TMD_TUNE_FORCE) return fail(TMD_ERR_ARG, "unknown kernel family");
+  *variant = s->force_variant;
+  return TMD_OK;
+}
+
+int tmd_system_autotune(tmd_system *s, int family, int reps, double *ms) {
+  if (!s) return fail(TMD_ERR_ARG, "null system");
+  if (family != TMD_TUNE_FORCE) return fail(TMD_ERR_ARG, "unknown kernel family");
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before autotune");
+  if (reps < 1) reps = 1;
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  // a full evaluation leaves S = dE/dP and the list current for the force loop
+  int rc = tmd_compute(s, 0, 0, 1.0, nullptr, nullptr, nullptr, nullptr, nullptr);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  TMD_CUDA(cudaEventCreate(&e0));
+  TMD_CUDA(cudaEventCreate(&e1));
+  int best = s->force_variant;
+  float best_ms = 0.f;
+  cudaError_t err = cudaSuccess;
+  for (int v = 0; v < kForceVariants && err == cudaSuccess; v++) {
+    const ForceArgs fa = force_args(s, 1.0f, v);
+    launch_force(fa, s->st, s->launches);  // warm-up
+    err = cudaEventRecord(e0, s->st);
+    for (int r = 0; r < reps && err == cudaSuccess; r++) launch_force(fa, s->st, s->launches);
+    if (err == cudaSuccess) err = cudaEventRecord(e1, s->st);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    if (err == cudaSuccess) err = cudaGetLastError();
+    float t = 0.f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
+    t /= reps;
+    if (ms) ms[v] = t;
+    if (err == cudaSuccess && (v == 0 || t < best_ms)) { best = v; best_ms = t; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess)
+    return fail(TMD_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(err));
+  rc = tmd_system_set_variant(s, family, best);
+  if (rc) return rc;
+  // forces of the chosen form (the forms round differently)
+  return tmd_compute(s, 0, 0, 1.0, nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 
 int tmd_system_stream(tmd_system *s, void **stream) {

@@ -188,9 +188,19 @@ void launch_force_tpa(const ForceArgs &a, cudaStream_t st) {
 #undef TMD_FORCE_ARGS
 }
 
+}  // namespace tmd
+
+#include "force_pl.cuh"
+
+namespace tmd {
+
 // One radial kind and box mode per translation unit (parallel compilation).
 template <int RK, bool MULTI>
 void launch_force_rk(const ForceArgs &a, cudaStream_t st) {
+  if (a.variant != kForceFilterLane) {
+    launch_force_pl<RK, MULTI>(a, st);
+    return;
+  }
   switch (a.kp.K / 4) {
     case 1: launch_force_tpa<1, RK, MULTI>(a, st); break;
     case 2: launch_force_tpa<2, RK, MULTI>(a, st); break;

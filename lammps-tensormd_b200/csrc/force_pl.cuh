@@ -1,0 +1,243 @@
+// force_pl.cuh -- pair-per-lane form of the pair-force kernel.
+//
+// Same mathematics and outputs as k_force (force_impl.cuh): for every active
+// pair of atom i, V_d = sum_k S[k,d] H_k, W_d = sum_k S[k,d] dH_k,
+// df = (sum_d M_d W_d) u + grad Q(V) / r, scaled, into pdf[i*cap + t]; FP64
+// per-atom virial into wv[i].
+//
+// k_force gives each lane 4 filters of an atom and sums the lanes' partial
+// forces, so every lane of the atom's group evaluates the monomials, the
+// gradient of Q and the force expression of every pair.  Here W lanes share
+// one atom and each lane takes whole pairs: S of the current element block
+// (K x D floats) is staged once in shared memory and read by all lanes of the
+// group as broadcast vectors, and the monomials, grad Q and the force of a
+// pair are computed once.  Pairs are queued by the same PairRing as k_force
+// (W entries' geometry per step, active ones compacted in row order); lane c
+// of the group takes pair c of each chunk, so only the last chunk of a block
+// leaves lanes idle.
+#pragma once
+
+#include <algorithm>
+
+#include "descriptor_impl.cuh"
+
+namespace tmd {
+
+// Shared-memory layout of k_force_pl (floats): radial parameters [3][K] (none
+// for the table kind), then per atom group an S block [K][D4] + 4 (the extra
+// 4 floats put consecutive groups' blocks in different banks).
+template <int D>
+struct PlLayout {
+  static constexpr int D4 = (D + 3) / 4 * 4;
+  static __host__ __device__ inline int params(int K, int rk) { return rk == kRadTable ? 0 : 3 * K; }
+  static __host__ __device__ inline int group(int K) { return K * D4 + 4; }
+  static __host__ inline size_t bytes(int K, int rk, int groups) {
+    return sizeof(float) * ((size_t)params(K, rk) + (size_t)groups * group(K));
+  }
+};
+
+template <int W, int D, int RK, bool MULTI>
+__global__ void __launch_bounds__(kPairThreads, 4)
+k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
+           const double *__restrict__ x, const int *__restrict__ elem,
+           const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
+           const float *__restrict__ S, float4 *__restrict__ pdf,
+           double *__restrict__ wv, const BoxP *__restrict__ cbox,
+           const int *__restrict__ acell) {
+  using L = PlLayout<D>;
+  constexpr int D4 = L::D4;
+  constexpr int P2 = D4 / 2;  // FP32 pairs per S row (pad columns hold 0)
+  extern __shared__ float4 pl_dyn[];
+  __shared__ GeoSlot geo[2 * kPairThreads];
+  const int K = kp.K, B = kp.B;
+  float *rp = reinterpret_cast<float *>(pl_dyn);
+  if (RK != kRadTable) {
+    for (int i = threadIdx.x; i < K; i += blockDim.x) {
+      rp[i] = RK == kRadGauss ? kp.p1[i] : kp.p0[i];
+      rp[K + i] = RK == kRadGauss ? kp.p1lo[i] : kp.p1[i];
+      rp[2 * K + i] = RK == kRadGauss ? kp.gc[i] : kp.p2[i];
+    }
+  }
+  __syncthreads();
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = gt / W;
+  const int sub = gt % W;
+  if (a >= n) return;
+  const unsigned live = live_lanes(gt, (long)n * W);
+  const int lane = threadIdx.x & 31;
+  PairRing<W> pr;
+  pr.sub = sub;
+  pr.gshift = lane & ~(W - 1);
+  pr.gmask = PairRing<W>::kBits << pr.gshift;
+  pr.ring = geo + 2 * (threadIdx.x - sub);
+  const unsigned gmask = pr.gmask;
+  float *Sg = rp + L::params(K, RK) + (threadIdx.x / W) * L::group(K);
+  const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
+  const double xi = x[3 * a], yi = x[3 * a + 1], zi = x[3 * a + 2];
+  const uint32_t *row = nbr + (size_t)a * cap;
+  const int *bo = boff + (size_t)a * (B + 1);
+  float4 *pdf_row = pdf + (size_t)a * cap;
+  double w6[6] = {0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < B; b++) {
+    if (b > 0) __syncwarp(live);  // keep the warp's groups on the same block
+    const int s0 = bo[b], s1 = bo[b + 1];
+    if (s0 == s1) continue;
+    // stage S of (atom, block) as [K][D4] rows
+    __syncwarp(gmask);
+    const float *Sp = S + ((size_t)a * B + b) * K * D;
+    if constexpr (D == D4) {
+      const float4 *S4 = reinterpret_cast<const float4 *>(Sp);
+      float4 *G4 = reinterpret_cast<float4 *>(Sg);
+      for (int i = sub; i < K * D / 4; i += W) G4[i] = __ldg(S4 + i);
+    } else {
+      for (int i = sub; i < K * D4; i += W) {
+        const int k = i / D4, d = i - k * D4;
+        Sg[i] = d < D ? __ldg(Sp + k * D + d) : 0.f;
+      }
+    }
+    __syncwarp(gmask);
+    pr.begin(x, row, s0, s1);
+    for (;;) {
+      const int cnt = pr.feed(kp, bx, xi, yi, zi, x, row, pdf_row);
+      if (cnt == 0) break;
+      if (sub < cnt) {
+        const GeoSlot *sl = pr.slot(sub);
+        const PairGeo g = geo_load(sl);
+        const int t = __float_as_int(sl->c.y);
+        float2 V2[P2], W2[P2];
+#pragma unroll
+        for (int p = 0; p < P2; p++) {
+          V2[p] = make_float2(0.f, 0.f);
+          W2[p] = make_float2(0.f, 0.f);
+        }
+        const bool on = RK != kRadTable || (g.ti > 0 && g.ti < kp.tab_n - 2);
+        for (int k0 = 0; on && k0 < K; k0 += 4) {
+          Radial4<RK> R;
+          R.k0 = k0;
+          if (RK != kRadTable) {
+            const float4 pa = *reinterpret_cast<const float4 *>(rp + k0);
+            const float4 pb = *reinterpret_cast<const float4 *>(rp + K + k0);
+            const float4 pc = *reinterpret_cast<const float4 *>(rp + 2 * K + k0);
+            const float va[4] = {pa.x, pa.y, pa.z, pa.w}, vb[4] = {pb.x, pb.y, pb.z, pb.w},
+                        vc[4] = {pc.x, pc.y, pc.z, pc.w};
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+              if (RK == kRadGauss) { R.b[q] = va[q]; R.blo[q] = vb[q]; R.gc[q] = vc[q]; }
+              if (RK == kRadGeneric) { R.a[q] = va[q]; R.b[q] = vb[q]; R.c[q] = vc[q]; }
+            }
+          }
+          float H[4], dH[4];
+          radial4<RK, true>(kp, R, g, H, dH);
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const float2 h2 = make_float2(H[q], H[q]);
+            const float2 d2 = make_float2(dH[q], dH[q]);
+            const float4 *Sk = reinterpret_cast<const float4 *>(Sg + (k0 + q) * D4);
+#pragma unroll
+            for (int v = 0; v < D4 / 4; v++) {
+              const float4 s = Sk[v];
+              const float2 lo = make_float2(s.x, s.y), hi = make_float2(s.z, s.w);
+              V2[2 * v] = __ffma2_rn(lo, h2, V2[2 * v]);
+              W2[2 * v] = __ffma2_rn(lo, d2, W2[2 * v]);
+              V2[2 * v + 1] = __ffma2_rn(hi, h2, V2[2 * v + 1]);
+              W2[2 * v + 1] = __ffma2_rn(hi, d2, W2[2 * v + 1]);
+            }
+          }
+        }
+        float M[D4];
+        moments<D>(g.ux, g.uy, g.uz, M);
+#pragma unroll
+        for (int d = D; d < D4; d++) M[d] = 0.f;
+        float2 fa = make_float2(0.f, 0.f), fb = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int p = 0; p < P2; p += 2) {
+          fa = __ffma2_rn(make_float2(M[2 * p], M[2 * p + 1]), W2[p], fa);
+          if (p + 1 < P2)
+            fb = __ffma2_rn(make_float2(M[2 * p + 2], M[2 * p + 3]), W2[p + 1], fb);
+        }
+        const float f1 = (fa.x + fb.x) + (fa.y + fb.y);
+        float V[D4];
+#pragma unroll
+        for (int p = 0; p < P2; p++) { V[2 * p] = V2[p].x; V[2 * p + 1] = V2[p].y; }
+        float gq[3], nvm;
+        poly_grad<D>(V, g.ux, g.uy, g.uz, gq, nvm);
+        const float rinv = 1.f / g.r;
+        const float fx = (f1 * g.ux + (gq[0] - g.ux * nvm) * rinv) * scale;
+        const float fy = (f1 * g.uy + (gq[1] - g.uy * nvm) * rinv) * scale;
+        const float fz = (f1 * g.uz + (gq[2] - g.uz * nvm) * rinv) * scale;
+        pdf_row[t] = make_float4(fx, fy, fz, 0.f);
+        const double rr = (double)g.r + (double)g.rlo;
+        const double rx = (double)g.ux * rr, ry = (double)g.uy * rr, rz = (double)g.uz * rr;
+        w6[0] -= rx * fx;
+        w6[1] -= ry * fy;
+        w6[2] -= rz * fz;
+        w6[3] -= rx * fy;
+        w6[4] -= rx * fz;
+        w6[5] -= ry * fz;
+      }
+      pr.pop(cnt);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 6; c++) {
+#pragma unroll
+    for (int o = W >> 1; o > 0; o >>= 1) w6[c] += __shfl_xor_sync(gmask, w6[c], o, W);
+  }
+  if (sub == 0) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) wv[(size_t)a * 6 + c] = w6[c];
+  }
+}
+
+// Atom groups per block: as many as fit 128 threads and 48 KB of shared
+// memory (the static ring plus the dynamic parameters and S blocks).
+inline int force_pl_groups(int W, int K, int D4, int rk) {
+  const size_t per = sizeof(float) * ((size_t)K * D4 + 4);
+  const size_t base = sizeof(float) * (rk == kRadTable ? 0 : 3 * (size_t)K) +
+                      sizeof(GeoSlot) * 2 * kPairThreads;
+  int g = kPairThreads / W;
+  while (g > 1 && base + g * per > 48 * 1024) g--;
+  return g;
+}
+
+template <int W, int RK, bool MULTI>
+void launch_force_pl_w(const ForceArgs &a, cudaStream_t st) {
+#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.S, a.pdf, a.wv, a.cbox, a.acell
+#define TMD_PL_CASE(DV)                                                                     \
+  case DV: {                                                                                \
+    const int g = force_pl_groups(W, a.kp.K, PlLayout<DV>::D4, RK);                         \
+    const int T = g * W;                                                                    \
+    const long threads = (long)a.n * W;                                                     \
+    const int grid = (int)std::max(1L, (threads + T - 1) / T);                              \
+    k_force_pl<W, DV, RK, MULTI><<<grid, T, PlLayout<DV>::bytes(a.kp.K, RK, g), st>>>(      \
+        TMD_FORCE_ARGS);                                                                    \
+    break;                                                                                  \
+  }
+  switch (a.kp.D) {
+    TMD_PL_CASE(1)
+    TMD_PL_CASE(4)
+    TMD_PL_CASE(10)
+    default: {
+      const int g = force_pl_groups(W, a.kp.K, PlLayout<20>::D4, RK);
+      const int T = g * W;
+      const long threads = (long)a.n * W;
+      const int grid = (int)std::max(1L, (threads + T - 1) / T);
+      k_force_pl<W, 20, RK, MULTI><<<grid, T, PlLayout<20>::bytes(a.kp.K, RK, g), st>>>(
+          TMD_FORCE_ARGS);
+      break;
+    }
+  }
+#undef TMD_PL_CASE
+#undef TMD_FORCE_ARGS
+}
+
+template <int RK, bool MULTI>
+void launch_force_pl(const ForceArgs &a, cudaStream_t st) {
+  switch (a.variant) {
+    case kForcePairLane8: launch_force_pl_w<8, RK, MULTI>(a, st); break;
+    case kForcePairLane32: launch_force_pl_w<32, RK, MULTI>(a, st); break;
+    default: launch_force_pl_w<16, RK, MULTI>(a, st); break;
+  }
+}
+
+}  // namespace tmd

@@ -75,6 +75,9 @@ struct tmd_system {
   std::vector<int> h_elem;
   double *h_scal = nullptr;  // pinned [8]
   int *h_status = nullptr;   // pinned [2]
+  // kernel form of the pair-force loop (kForce*), set by the default rule,
+  // tmd_system_set_variant or tmd_system_autotune
+  int force_variant = 0;
   // kernel timing
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -134,6 +137,9 @@ int read_status(tmd_system *s);
 int clear_status(tmd_system *s);
 int rebuild_now(tmd_system *s);
 void launch_force_eval(tmd_system *s, float scale, bool want_vatom);
+ForceArgs force_args(tmd_system *s, float scale, int variant);
+// Kernel form of the force loop used when nothing chose one.
+int default_force_variant(const tmd_model *m);
 NbArgs nb_args(tmd_system *s);
 // LAMMPS types (1-based) -> potential elements; TMD_ERR_ARG for unmapped types.
 int map_types(const tmd_model *m, int n, const int *type, std::vector<int> &elem);

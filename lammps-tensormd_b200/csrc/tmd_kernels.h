@@ -139,6 +139,13 @@ void launch_dedp(int n, const KParams &kp, float *P, const float *G, const float
                  cudaStream_t st, long &launches);
 
 // Force: per-pair dE_i/dx_j into pdf, per-atom virial partials.
+// Kernel forms: K/4 lanes per atom with 4 filters each (k_force), or W lanes
+// per atom with whole pairs per lane (k_force_pl, W = 8, 16, 32).
+constexpr int kForceFilterLane = 0;
+constexpr int kForcePairLane8 = 1;
+constexpr int kForcePairLane16 = 2;
+constexpr int kForcePairLane32 = 3;
+constexpr int kForceVariants = 4;
 struct ForceArgs {
   int n, cap;
   KParams kp;
@@ -153,6 +160,7 @@ struct ForceArgs {
   double *wv;  // [n][6] per-atom sum of -r_ij (x) df over own pairs
   const BoxP *cbox;   // multi-cell mode (as DescArgs)
   const int *acell;
+  int variant;        // kForce*
 };
 void launch_force(const ForceArgs &a, cudaStream_t st, long &launches);
 

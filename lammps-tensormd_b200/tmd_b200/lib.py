@@ -37,6 +37,9 @@ SIGNATURES = [
     ("tmd_nvt_energy", _c_int, [_vp, _pd]),
     ("tmd_neighbor_list", _c_int, [_vp, _c_double, _pi, _pi, _c_long, _pl]),
     ("tmd_get_descriptors", _c_int, [_vp, _pd]),
+    ("tmd_system_set_variant", _c_int, [_vp, _c_int, _c_int]),
+    ("tmd_system_get_variant", _c_int, [_vp, _c_int, _pi]),
+    ("tmd_system_autotune", _c_int, [_vp, _c_int, _c_int, _pd]),
     ("tmd_system_stream", _c_int, [_vp, ctypes.POINTER(_vp)]),
     ("tmd_system_launches", _c_long, [_vp]),
     ("tmd_profile_enable", _c_int, [_vp, _c_int]),

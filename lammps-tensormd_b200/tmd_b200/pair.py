@@ -166,6 +166,25 @@ class TensorMDSystem:
         check(self.lib.tmd_get_descriptors(self.h, _dp(G)))
         return G
 
+    # kernel forms of the force loop (tmd_system_set_variant, family 0)
+    FORCE_VARIANTS = ("filter_lane", "pair_lane8", "pair_lane16", "pair_lane32")
+
+    def set_force_variant(self, variant):
+        v = self.FORCE_VARIANTS.index(variant) if isinstance(variant, str) else int(variant)
+        check(self.lib.tmd_system_set_variant(self.h, 0, v))
+
+    def force_variant(self) -> str:
+        v = ctypes.c_int()
+        check(self.lib.tmd_system_get_variant(self.h, 0, ctypes.byref(v)))
+        return self.FORCE_VARIANTS[v.value]
+
+    def autotune(self, reps: int = 5):
+        """Time every force-loop form on the current atoms, keep the fastest;
+        returns {form: ms per launch}."""
+        ms = np.zeros(len(self.FORCE_VARIANTS))
+        check(self.lib.tmd_system_autotune(self.h, 0, int(reps), _dp(ms)))
+        return dict(zip(self.FORCE_VARIANTS, ms.tolist()))
+
     def stream(self) -> int:
         p = ctypes.c_void_p()
         check(self.lib.tmd_system_stream(self.h, ctypes.byref(p)))
