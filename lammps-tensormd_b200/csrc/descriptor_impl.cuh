@@ -31,13 +31,13 @@ constexpr int kPairThreads = 128;  // block size of the pair kernels
 struct GeoSlot {
   float4 a;  // r, rlo, ux, uy
   float4 b;  // uz, fc, dfc, tq
-  float4 c;  // ti (bits), neighbor slot t (bits), unused
+  float4 c;  // ti (bits), neighbor slot t (bits), 1/r, unused
 };
 
 __device__ inline void geo_store(GeoSlot *s, const PairGeo &g, int t) {
   s->a = make_float4(g.r, g.rlo, g.ux, g.uy);
   s->b = make_float4(g.uz, g.fc, g.dfc, g.tq);
-  s->c = make_float4(__int_as_float(g.ti), __int_as_float(t), 0.f, 0.f);
+  s->c = make_float4(__int_as_float(g.ti), __int_as_float(t), g.rinv, 0.f);
 }
 
 __device__ inline PairGeo geo_load(const GeoSlot *s) {
@@ -45,7 +45,9 @@ __device__ inline PairGeo geo_load(const GeoSlot *s) {
   float4 a = s->a, b = s->b;
   g.r = a.x; g.rlo = a.y; g.ux = a.z; g.uy = a.w;
   g.uz = b.x; g.fc = b.y; g.dfc = b.z; g.tq = b.w;
-  g.ti = __float_as_int(s->c.x);
+  const float4 c = s->c;
+  g.ti = __float_as_int(c.x);
+  g.rinv = c.z;
   return g;
 }
 

@@ -129,7 +129,7 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
         for (int p = 0; p < D2; p++) { V[2 * p] = V2[p].x; V[2 * p + 1] = V2[p].y; }
         float gq[3], nvm;
         poly_grad<D>(V, g.ux, g.uy, g.uz, gq, nvm);
-        const float rinv = 1.f / g.r;
+        const float rinv = g.rinv;
         float fx = f1 * g.ux + (gq[0] - g.ux * nvm) * rinv;
         float fy = f1 * g.uy + (gq[1] - g.uy * nvm) * rinv;
         float fz = f1 * g.uz + (gq[2] - g.uz * nvm) * rinv;

@@ -23,13 +23,13 @@
 
 namespace tmd {
 
-// Shared-memory layout of k_force_pl (floats): radial parameters [3][K] (none
+// Shared-memory layout of k_force_pl (floats): radial parameters [4][K] (none
 // for the table kind), then per atom group an S block [K][D4] + 4 (the extra
 // 4 floats put consecutive groups' blocks in different banks).
 template <int D>
 struct PlLayout {
   static constexpr int D4 = (D + 3) / 4 * 4;
-  static __host__ __device__ inline int params(int K, int rk) { return rk == kRadTable ? 0 : 3 * K; }
+  static __host__ __device__ inline int params(int K, int rk) { return rk == kRadTable ? 0 : 4 * K; }
   static __host__ __device__ inline int group(int K) { return K * D4 + 4; }
   static __host__ inline size_t bytes(int K, int rk, int groups) {
     return sizeof(float) * ((size_t)params(K, rk) + (size_t)groups * group(K));
@@ -56,6 +56,7 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
       rp[i] = RK == kRadGauss ? kp.p1[i] : kp.p0[i];
       rp[K + i] = RK == kRadGauss ? kp.p1lo[i] : kp.p1[i];
       rp[2 * K + i] = RK == kRadGauss ? kp.gc[i] : kp.p2[i];
+      rp[3 * K + i] = RK == kRadGauss ? kp.gcl[i] : 0.f;
     }
   }
   __syncthreads();
@@ -77,7 +78,7 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
   const uint32_t *row = nbr + (size_t)a * cap;
   const int *bo = boff + (size_t)a * (B + 1);
   float4 *pdf_row = pdf + (size_t)a * cap;
-  double w6[6] = {0, 0, 0, 0, 0, 0};
+  float w6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   for (int b = 0; b < B; b++) {
     if (b > 0) __syncwarp(live);  // keep the warp's groups on the same block
     const int s0 = bo[b], s1 = bo[b + 1];
@@ -118,11 +119,15 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
             const float4 pa = *reinterpret_cast<const float4 *>(rp + k0);
             const float4 pb = *reinterpret_cast<const float4 *>(rp + K + k0);
             const float4 pc = *reinterpret_cast<const float4 *>(rp + 2 * K + k0);
+            const float4 pd = RK == kRadGauss ? *reinterpret_cast<const float4 *>(rp + 3 * K + k0)
+                                              : make_float4(0.f, 0.f, 0.f, 0.f);
             const float va[4] = {pa.x, pa.y, pa.z, pa.w}, vb[4] = {pb.x, pb.y, pb.z, pb.w},
-                        vc[4] = {pc.x, pc.y, pc.z, pc.w};
+                        vc[4] = {pc.x, pc.y, pc.z, pc.w}, vd[4] = {pd.x, pd.y, pd.z, pd.w};
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-              if (RK == kRadGauss) { R.b[q] = va[q]; R.blo[q] = vb[q]; R.gc[q] = vc[q]; }
+              if (RK == kRadGauss) {
+                R.b[q] = va[q]; R.blo[q] = vb[q]; R.gc[q] = vc[q]; R.gl[q] = vd[q];
+              }
               if (RK == kRadGeneric) { R.a[q] = va[q]; R.b[q] = vb[q]; R.c[q] = vc[q]; }
             }
           }
@@ -161,13 +166,14 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
         for (int p = 0; p < P2; p++) { V[2 * p] = V2[p].x; V[2 * p + 1] = V2[p].y; }
         float gq[3], nvm;
         poly_grad<D>(V, g.ux, g.uy, g.uz, gq, nvm);
-        const float rinv = 1.f / g.r;
+        const float rinv = g.rinv;
         const float fx = (f1 * g.ux + (gq[0] - g.ux * nvm) * rinv) * scale;
         const float fy = (f1 * g.uy + (gq[1] - g.uy * nvm) * rinv) * scale;
         const float fz = (f1 * g.uz + (gq[2] - g.uz * nvm) * rinv) * scale;
         pdf_row[t] = make_float4(fx, fy, fz, 0.f);
-        const double rr = (double)g.r + (double)g.rlo;
-        const double rx = (double)g.ux * rr, ry = (double)g.uy * rr, rz = (double)g.uz * rr;
+        // per-pair virial in FP32 (df itself is FP32), summed in FP32 over
+        // the lane's few pairs of the atom, then in FP64 over lanes and atoms
+        const float rx = g.ux * g.r, ry = g.uy * g.r, rz = g.uz * g.r;
         w6[0] -= rx * fx;
         w6[1] -= ry * fy;
         w6[2] -= rz * fz;
@@ -178,14 +184,16 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
       pr.pop(cnt);
     }
   }
+  double w6d[6];
 #pragma unroll
   for (int c = 0; c < 6; c++) {
+    w6d[c] = (double)w6[c];
 #pragma unroll
-    for (int o = W >> 1; o > 0; o >>= 1) w6[c] += __shfl_xor_sync(gmask, w6[c], o, W);
+    for (int o = W >> 1; o > 0; o >>= 1) w6d[c] += __shfl_xor_sync(gmask, w6d[c], o, W);
   }
   if (sub == 0) {
 #pragma unroll
-    for (int c = 0; c < 6; c++) wv[(size_t)a * 6 + c] = w6[c];
+    for (int c = 0; c < 6; c++) wv[(size_t)a * 6 + c] = w6d[c];
   }
 }
 

@@ -394,7 +394,10 @@ void fill_kparams(const HostModel &h, KParams &kp) {
       kp.p1lo[k] = float(h.p1[k] - double(kp.p1[k]));
     }
     if (!h.p2.empty()) kp.p2[k] = float(h.p2[k]);
-    if (!h.p0.empty()) kp.gc[k] = float(h.p0[k] / (h.rmax * h.rmax));
+    if (!h.p0.empty()) {
+      kp.gc[k] = float(h.p0[k] / (h.rmax * h.rmax));
+      kp.gcl[k] = float(h.p0[k] / (h.rmax * h.rmax) * 1.4426950408889634);  // log2(e)
+    }
   }
   // element blocks: tensormd.cpp:165-176
   for (int i = 0; i < h.nelt; i++) {

@@ -17,6 +17,7 @@ struct PairGeo {
   float ux, uy, uz;     // unit vector (x_j - x_i) / r
   float fc, dfc;        // analytic cutoff and derivative
   float tq;             // table: offset inside the interval
+  float rinv;           // 1 / r (FP32)
   int ti;               // table interval (0 for analytic), -1 when inactive
 };
 
@@ -53,7 +54,7 @@ __device__ inline void pair_geometry(const KParams &kp, const BoxP &box, double 
                                      double yi, double zi, const NbPos &p,
                                      PairGeo &g) {
   g.ti = -1;
-  g.r = g.rlo = g.ux = g.uy = g.uz = g.fc = g.dfc = g.tq = 0.f;
+  g.r = g.rlo = g.ux = g.uy = g.uz = g.fc = g.dfc = g.tq = g.rinv = 0.f;
   if (p.code < 0) return;
   int sx, sy, sz;
   shift_decode(p.code, sx, sy, sz);
@@ -66,6 +67,7 @@ __device__ inline void pair_geometry(const KParams &kp, const BoxP &box, double 
   float rf = float(r);
   float rinv = 1.0f / rf;
   g.r = rf;
+  g.rinv = rinv;
   g.rlo = float(r - double(rf));
   g.ux = float(dx) * rinv;
   g.uy = float(dy) * rinv;
@@ -105,6 +107,7 @@ __device__ inline PairGeo shfl_geo(unsigned mask, const PairGeo &g, int src,
   o.fc = __shfl_sync(mask, g.fc, src, width);
   o.dfc = __shfl_sync(mask, g.dfc, src, width);
   o.tq = __shfl_sync(mask, g.tq, src, width);
+  o.rinv = __shfl_sync(mask, g.rinv, src, width);
   o.ti = __shfl_sync(mask, g.ti, src, width);
   return o;
 }
@@ -124,7 +127,7 @@ template <int RK>
 struct Radial4 {
   float a[RK == kRadGeneric ? 4 : 1], b[RK == kRadTable ? 1 : 4],
       c[RK == kRadGeneric ? 4 : 1], blo[RK == kRadGauss ? 4 : 1],
-      gc[RK == kRadGauss ? 4 : 1];
+      gc[RK == kRadGauss ? 4 : 1], gl[RK == kRadGauss ? 4 : 1];
   int k0;
 };
 
@@ -142,6 +145,7 @@ __device__ inline Radial4<RK> load_radial4(const KParams &kp, int k0) {
     if (RK == kRadGauss) {
       R.blo[t] = kp.p1lo[k0 + t];
       R.gc[t] = kp.gc[k0 + t];
+      R.gl[t] = kp.gcl[k0 + t];
     }
   }
   return R;
@@ -173,7 +177,7 @@ __device__ inline void radial4(const KParams &kp, const Radial4<RK> &R, const Pa
       float c1 = c1s[t], c2 = c2s[t], s = ss[t];
       float c3 = fabsf(c2 * rr);
       float c4 = c3 + fabsf(c1 * q);
-      if (c4 > 0.f) c3 /= c4;
+      if (c4 > 0.f) c3 = __fdividef(c3, c4);  // weight in [0, 1]: 2-ulp quotient
       c4 = c2 + c3 * (c1 - c2);
       H[t] = ys[t] + q * (s - rr * c4);
       if (DERIV) dH[t] = s + (q - rr) * c4 + dx * (c4 - c2) * (1.f - c3);
@@ -188,7 +192,7 @@ __device__ inline void radial4(const KParams &kp, const Radial4<RK> &R, const Pa
       // (r - omega) from the hi/lo pairs of both: no systematic rounding of
       // the Gaussian centre
       float d = (r - R.b[t]) + (g.rlo - R.blo[t]);
-      f = expf(-R.gc[t] * d * d);
+      f = exp2f(-R.gl[t] * d * d);
       df = -2.f * R.gc[t] * d * f;
     } else {
       const float a = R.a[t], b = R.b[t], c = R.c[t];

@@ -29,6 +29,7 @@ struct KParams {
   // Gaussian SF: exp(-gc (r - omega)^2) with gc = eta / rc^2 rounded once
   // from FP64, omega = p1 + p1lo (FP32 hi/lo pair)
   float gc[kMaxK], p1lo[kMaxK];
+  float gcl[kMaxK];     // gc * log2(e): exp(-gc d^2) evaluated as exp2(-gcl d^2)
   int eltij[kMaxElt * kMaxElt];  // element block of (elt_i, elt_j)
   const float *table;   // [tab_n][4][K] : y, s, c1, c2
   int tab_n;
