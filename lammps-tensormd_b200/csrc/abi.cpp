@@ -283,7 +283,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   ma.nl = m->h.nl; ma.actfn = m->h.actfn; ma.resnet = m->h.resnet; ma.nin = m->h.nin;
   int maxh = 1;
   for (int l = 1; l < m->h.nl; l++) maxh = std::max(maxh, m->h.sizes[l]);
-  ma.maxh = maxh; ma.tr = m->mlp_tr; ma.smem = m->mlp_smem;
+  ma.maxh = maxh; ma.tr = m->mlp_tr; ma.smem = m->mlp_smem; ma.resident = m->mlp_resident;
   ma.ntiles = s->ntiles; ma.tiles = s->tiles; ma.perm = s->perm; ma.G = s->G;
   ma.dEdG = s->dEdG; ma.E = s->E; ma.layers = m->d_layers;
   prof_begin(s);
@@ -659,10 +659,17 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     tmd_model_free(m);
     return fail(TMD_ERR_CUDA, std::string("model upload: ") + cudaGetErrorString(e));
   }
-  // MLP tile: 64 atoms when the shared-memory footprint allows, else 32
+  // MLP: the resident-weight form (one persistent CTA per SM) when the
+  // element's hidden weights and a tile's activations fit in shared memory,
+  // else weights streamed in chunks with 64- or 32-atom tiles
   size_t s64 = mlp_fp32_smem(h.nl, h.sizes.data(), 64);
   size_t s32 = mlp_fp32_smem(h.nl, h.sizes.data(), 32);
-  if (s64 <= 110 * 1024) {
+  const size_t sres = mlp_fp32r_smem(h.nl, h.sizes.data());
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+  if (h.nl >= 2 && sres <= 227 * 1024 && nsm > 0) {
+    m->mlp_tr = mlp_fp32r_tile(); m->mlp_smem = sres; m->mlp_resident = nsm;
+  } else if (s64 <= 110 * 1024) {
     m->mlp_tr = 64; m->mlp_smem = s64;
   } else if (s32 <= 220 * 1024) {
     m->mlp_tr = 32; m->mlp_smem = s32;
@@ -670,7 +677,7 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     tmd_model_free(m);
     return fail(TMD_ERR_MODEL, "MLP too wide for the shared-memory tile");
   }
-  mlp_fp32_prepare(m->mlp_tr, m->mlp_smem);
+  mlp_fp32_prepare(m->mlp_tr, m->mlp_smem, m->mlp_resident > 0);
   for (int l = 1; l < h.nl; l++) m->maxh = std::max(m->maxh, h.sizes[l]);
   if (h.precision == TMD_PREC_BF16 || h.precision == TMD_PREC_BF16X3 ||
       h.precision == TMD_PREC_FP8) {

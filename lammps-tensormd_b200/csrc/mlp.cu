@@ -231,7 +231,298 @@ k_mlp_fp32(MlpArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Resident-weight form.  The hidden layers' W of the current element stay in
+// shared memory (row-major, row stride ldw = 32*ceil(N/32) + 4 floats, zero
+// padding) for the whole life of a persistent CTA, which walks the tiles
+// (sorted by element) with a grid stride and reloads the weights only when the
+// element changes.  The forward GEMM reads W rows as float4 over 4 output
+// columns (as tile_gemm); the backward GEMM contracts over the output width,
+// so a thread owns outputs k = k0 + tx + 16 j and reads the rows W[k][c..c+3]
+// as float4 (row stride = 4 mod 32 words: the 8 threads of a phase hit
+// distinct banks).  Same FP32 arithmetic in the same order as k_mlp_fp32.
+// ---------------------------------------------------------------------------
+constexpr int kResTR = 128;       // atoms per tile of the resident form
+constexpr int kResThreads = 512;  // 16 warps: a 4 x 4 register tile per thread
+
+struct ResLayout {
+  int woff[kMaxLayers], ldw[kMaxLayers], boff[kMaxLayers], dzoff[kMaxLayers];
+  int wsf, wsd, act0, act1, total;  // floats
+};
+
+__host__ __device__ inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// sizes[0..nl]: n_in, layer widths.
+__host__ __device__ inline ResLayout res_layout(int nl, const int *sizes, int tr) {
+  ResLayout r{};
+  const int ldt = tr + 4;
+  int maxh = 1;
+  for (int l = 1; l < nl; l++) maxh = maxh > sizes[l] ? maxh : sizes[l];
+  int o = 0;
+  for (int l = 0; l < nl - 1; l++) {
+    r.ldw[l] = round_up(sizes[l + 1], 32) + 4;
+    r.woff[l] = o;
+    o += sizes[l] * r.ldw[l];
+  }
+  for (int l = 0; l < nl - 1; l++) { r.boff[l] = o; o += round_up(sizes[l + 1], 4); }
+  r.wsf = o; o += round_up(sizes[nl - 1], 4);
+  o = round_up(o, 2);
+  r.wsd = o; o += 2 * round_up(sizes[nl - 1], 2);  // doubles
+  const int w0 = sizes[0] > maxh ? sizes[0] : maxh;
+  r.act0 = o; o += round_up(w0, 4) * ldt;
+  r.act1 = o; o += round_up(maxh, 4) * ldt;
+  for (int l = 0; l < nl - 1; l++) { r.dzoff[l] = o; o += round_up(sizes[l + 1], 4) * ldt; }
+  r.total = round_up(o, 4);
+  return r;
+}
+
+// Forward: out(r, c) = sum_k inT[k][r] W[k][c] for c < N, r < TR.
+template <int TR, int NT, class Epi>
+__device__ inline void res_gemm_fwd(const float *inT, int Kd, const float *W, int ldw, int N,
+                                    Epi epi) {
+  constexpr int LDT = TR + 4, RT = TR / (NT / 16);
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int N4 = round_up(N, 4);
+  for (int c0 = 0; c0 < N4; c0 += 64) {
+    const int cc = c0 + 4 * tx;
+    if (cc >= N4) continue;
+    float acc[RT][4];
+#pragma unroll
+    for (int i = 0; i < RT; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+    const float *wp = W + cc;
+    const float *xp = inT + ty * RT;
+#pragma unroll 4
+    for (int k = 0; k < Kd; k++) {
+      const float4 w = *reinterpret_cast<const float4 *>(wp + k * ldw);
+      float xv[RT];
+      if (RT == 4) {
+        const float4 t = *reinterpret_cast<const float4 *>(xp + k * LDT);
+        xv[0] = t.x; xv[1] = t.y; xv[2 % RT] = t.z; xv[3 % RT] = t.w;
+      } else {
+        const float2 t = *reinterpret_cast<const float2 *>(xp + k * LDT);
+        xv[0] = t.x; xv[1 % RT] = t.y;
+      }
+#pragma unroll
+      for (int i = 0; i < RT; i++) {
+        acc[i][0] = fmaf(xv[i], w.x, acc[i][0]);
+        acc[i][1] = fmaf(xv[i], w.y, acc[i][1]);
+        acc[i][2] = fmaf(xv[i], w.z, acc[i][2]);
+        acc[i][3] = fmaf(xv[i], w.w, acc[i][3]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < RT; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (cc + j < N) epi(ty * RT + i, cc + j, acc[i][j]);
+  }
+}
+
+// Backward: out(r, k) = sum_c gzT[c][r] W[k][c] for k < Kout, r < TR; gzT
+// has round_up(Nc, 4) rows (padding rows finite), W zero beyond column Nc.
+template <int TR, int NT, class Epi>
+__device__ inline void res_gemm_bwd(const float *gzT, int Nc, const float *W, int ldw, int Kout,
+                                    Epi epi) {
+  constexpr int LDT = TR + 4, RT = TR / (NT / 16);
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int Nc4 = round_up(Nc, 4);
+  for (int k0 = 0; k0 < Kout; k0 += 64) {
+    float acc[RT][4];
+#pragma unroll
+    for (int i = 0; i < RT; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+    bool kv[4];
+    const float *wr[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int k = k0 + tx + 16 * j;
+      kv[j] = k < Kout;
+      wr[j] = W + (size_t)(kv[j] ? k : 0) * ldw;
+    }
+    const float *gp = gzT + ty * RT;
+#pragma unroll 2
+    for (int c = 0; c < Nc4; c += 4) {
+      float4 wj[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        wj[j] = kv[j] ? *reinterpret_cast<const float4 *>(wr[j] + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+      float g[4][RT];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (RT == 4) {
+          const float4 t = *reinterpret_cast<const float4 *>(gp + (c + q) * LDT);
+          g[q][0] = t.x; g[q][1] = t.y; g[q][2 % RT] = t.z; g[q][3 % RT] = t.w;
+        } else {
+          const float2 t = *reinterpret_cast<const float2 *>(gp + (c + q) * LDT);
+          g[q][0] = t.x; g[q][1 % RT] = t.y;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < RT; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          acc[i][j] = fmaf(g[0][i], wj[j].x, acc[i][j]);
+          acc[i][j] = fmaf(g[1][i], wj[j].y, acc[i][j]);
+          acc[i][j] = fmaf(g[2][i], wj[j].z, acc[i][j]);
+          acc[i][j] = fmaf(g[3][i], wj[j].w, acc[i][j]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < RT; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (kv[j]) epi(ty * RT + i, k0 + tx + 16 * j, acc[i][j]);
+  }
+}
+
+template <int TR, int NT>
+__global__ void __launch_bounds__(NT, 1)
+k_mlp_fp32r(MlpArgs a) {
+  extern __shared__ float4 smr4[];
+  float *sm = reinterpret_cast<float *>(smr4);
+  constexpr int LDT = TR + 4;
+  const int L = a.nl, nin = a.nin;
+  int sizes[kMaxLayers + 1];
+  sizes[0] = nin;
+  const MlpLayer *L0 = a.layers;
+  for (int l = 0; l < L; l++) sizes[l + 1] = L0[l].N;
+  const ResLayout lay = res_layout(L, sizes, TR);
+  float *act0 = sm + lay.act0, *act1 = sm + lay.act1;
+  float *wsf = sm + lay.wsf;
+  double *wsd = reinterpret_cast<double *>(sm + lay.wsd);
+  __shared__ int rows[TR];
+  const int tid = threadIdx.x;
+  const int Klast = sizes[L - 1];
+  // padding rows of the activation-gradient buffers are read by the backward
+  // GEMM (times zero weights): keep them finite
+  for (int l = 0; l < L - 1; l++) {
+    const int N = sizes[l + 1], N4 = round_up(N, 4);
+    for (int idx = tid; idx < (N4 - N) * LDT; idx += NT) sm[lay.dzoff[l] + N * LDT + idx] = 0.f;
+  }
+  int cur_elt = -1;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const int elt = a.tiles[3 * tile], start = a.tiles[3 * tile + 1],
+              count = a.tiles[3 * tile + 2];
+    __syncthreads();  // the previous tile is done with every buffer
+    if (elt != cur_elt) {
+      cur_elt = elt;
+      const MlpLayer *Ls = a.layers + (size_t)elt * L;
+      for (int l = 0; l < L - 1; l++) {
+        const int K = Ls[l].K, N = Ls[l].N, ldw = lay.ldw[l];
+        float *Wd = sm + lay.woff[l];
+        for (int idx = tid; idx < K * ldw; idx += NT) {
+          const int k = idx / ldw, c = idx - k * ldw;
+          Wd[idx] = c < N ? __ldg(Ls[l].W + (size_t)k * N + c) : 0.f;
+        }
+        float *bd = sm + lay.boff[l];
+        for (int c = tid; c < N; c += NT) bd[c] = Ls[l].b ? __ldg(Ls[l].b + c) : 0.f;
+      }
+      const MlpLayer lo = Ls[L - 1];
+      for (int k = tid; k < lo.K; k += NT) {
+        double sd = 0.0;
+        float sf = 0.f;
+        for (int o2 = 0; o2 < lo.N; o2++) {
+          sd += __ldg(lo.Wd + (size_t)k * lo.N + o2);
+          sf += __ldg(lo.W + (size_t)k * lo.N + o2);
+        }
+        wsd[k] = sd;
+        wsf[k] = sf;
+      }
+    }
+    if (tid < TR) rows[tid] = tid < count ? a.perm[start + tid] : -1;
+    __syncthreads();
+    // G tile, transposed
+    for (int idx = tid; idx < TR * nin; idx += NT) {
+      const int r = idx / nin, k = idx - r * nin;
+      const int at = rows[r];
+      act0[(size_t)k * LDT + r] = at >= 0 ? __ldg(a.G + (size_t)at * nin + k) : 0.f;
+    }
+    __syncthreads();
+    float *in = act0, *out = act1;
+    for (int l = 0; l < L - 1; l++) {
+      const int K = sizes[l], N = sizes[l + 1];
+      float *dz = sm + lay.dzoff[l];
+      const float *bias = sm + lay.boff[l];
+      const bool res = a.resnet && l > 0 && K == N;
+      const int actfn = a.actfn;
+      float *o = out;
+      const float *ip = in;
+      res_gemm_fwd<TR, NT>(in, K, sm + lay.woff[l], lay.ldw[l], N, [&](int r, int c, float v) {
+        const float z = v + bias[c];
+        float d;
+        float y = act_fwd(actfn, z, d);
+        if (res) y += ip[(size_t)c * LDT + r];
+        o[(size_t)c * LDT + r] = y;
+        dz[(size_t)c * LDT + r] = d;
+      });
+      __syncthreads();
+      float *t = in; in = out; out = t;
+    }
+    // output layer in FP64
+    {
+      const MlpLayer lo = a.layers[(size_t)elt * L + L - 1];
+      const int per = NT / TR;
+      const int r = tid / per, part = tid % per;
+      double s = 0.0;
+      for (int k = part; k < Klast; k += per) s = fma((double)in[(size_t)k * LDT + r], wsd[k], s);
+      for (int o2 = per >> 1; o2 > 0; o2 >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o2);
+      if (part == 0 && rows[r] >= 0) {
+        double e = s;
+        if (lo.bd)
+          for (int o2 = 0; o2 < lo.N; o2++) e += __ldg(lo.bd + o2);
+        a.E[rows[r]] = e;
+      }
+    }
+    // backward seed: g of the last hidden output = row sums of W_L, times act'
+    {
+      float *dz = sm + lay.dzoff[L - 2 >= 0 ? L - 2 : 0];
+      float *g = out;
+      for (int idx = tid; idx < Klast * TR; idx += NT) {
+        const int k = idx / TR, r = idx - k * TR;
+        g[(size_t)k * LDT + r] = wsf[k];
+        if (L >= 2) dz[(size_t)k * LDT + r] *= wsf[k];
+      }
+    }
+    __syncthreads();
+    float *gcur = out, *gnext = in;
+    for (int l = L - 2; l >= 0; l--) {
+      const int K = sizes[l], N = sizes[l + 1];
+      const float *gz = sm + lay.dzoff[l];
+      const float *Wl = sm + lay.woff[l];
+      if (l == 0) {
+        const int *rw = rows;
+        float *dE = a.dEdG;
+        res_gemm_bwd<TR, NT>(gz, N, Wl, lay.ldw[l], K, [&](int r, int k, float v) {
+          const int at = rw[r];
+          if (at >= 0) dE[(size_t)at * nin + k] = v;
+        });
+      } else {
+        const bool res = a.resnet && K == N;
+        float *dzn = sm + lay.dzoff[l - 1];
+        const float *gc = gcur;
+        float *gn = gnext;
+        res_gemm_bwd<TR, NT>(gz, N, Wl, lay.ldw[l], K, [&](int r, int k, float v) {
+          const float gv = v + (res ? gc[(size_t)k * LDT + r] : 0.f);
+          gn[(size_t)k * LDT + r] = gv;
+          dzn[(size_t)k * LDT + r] *= gv;
+        });
+        __syncthreads();
+        float *t = gcur; gcur = gnext; gnext = t;
+      }
+    }
+  }
+}
+
 }  // namespace
+
+size_t mlp_fp32r_smem(int nl, const int *sizes) {
+  return sizeof(float) * (size_t)res_layout(nl, sizes, kResTR).total;
+}
+
+int mlp_fp32r_tile() { return kResTR; }
 
 size_t mlp_fp32_smem(int nl, const int *sizes, int tr) {
   // sizes[0..nl]: n_in, layer widths
@@ -248,6 +539,11 @@ size_t mlp_fp32_smem(int nl, const int *sizes, int tr) {
 void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches) {
   if (a.ntiles <= 0) return;
   launches += 1;
+  if (a.resident > 0) {
+    const int grid = a.ntiles < a.resident ? a.ntiles : a.resident;
+    k_mlp_fp32r<kResTR, kResThreads><<<grid, kResThreads, a.smem, st>>>(a);
+    return;
+  }
   if (a.tr == 64) {
     k_mlp_fp32<64><<<a.ntiles, kThreads, a.smem, st>>>(a);
   } else {
@@ -255,8 +551,11 @@ void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches) {
   }
 }
 
-void mlp_fp32_prepare(int tr, size_t smem) {
-  if (tr == 64)
+void mlp_fp32_prepare(int tr, size_t smem, bool resident) {
+  if (resident)
+    cudaFuncSetAttribute(k_mlp_fp32r<kResTR, kResThreads>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  else if (tr == 64)
     cudaFuncSetAttribute(k_mlp_fp32<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   else
     cudaFuncSetAttribute(k_mlp_fp32<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -29,6 +29,7 @@ struct tmd_model {
   double *d_mass = nullptr;     // per element
   int mlp_tr = 64;
   size_t mlp_smem = 0;
+  int mlp_resident = 0;    // > 0: resident-weight MLP, persistent grid size
   int nsys = 0;            // systems created from this model and not yet freed
   bool released = false;   // tmd_model_free called while nsys > 0
 };

@@ -79,6 +79,7 @@ struct MlpArgs {
   int nl, actfn, resnet, nin, maxh;
   int tr;             // atoms per CTA (32 or 64)
   size_t smem;        // dynamic shared memory bytes
+  int resident;       // > 0: resident-weight form, persistent grid of this many CTAs
   int ntiles;
   const int *tiles;   // [ntiles][3] = (element, start, count) into perm
   const int *perm;    // atom indices grouped by element
@@ -90,7 +91,10 @@ struct MlpArgs {
 };
 void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches);
 size_t mlp_fp32_smem(int nl, const int *sizes, int tr);
-void mlp_fp32_prepare(int tr, size_t smem);
+// Resident-weight form: shared memory per CTA and atoms per tile.
+size_t mlp_fp32r_smem(int nl, const int *sizes);
+int mlp_fp32r_tile();
+void mlp_fp32_prepare(int tr, size_t smem, bool resident);
 
 // Tensor-core (tcgen05) MLP, BF16 operands.  Weights are packed on the host
 // in 64-column chunks of the K-major core-matrix layout (pack_core_chunks).
