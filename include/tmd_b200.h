@@ -172,7 +172,8 @@ long tmd_system_launches(const tmd_system *sys);
  * tmd_nve_run; tmd_profile_read returns, per family, the number of launches
  * and the summed device milliseconds since the last reset.  Families:
  * 0 neighbor build, 1 descriptor, 2 mlp, 3 force, 4 gather, 5 nve+check,
- * 6 reductions, 7 dE/dP.  Arrays hold TMD_NPROF entries. */
+ * 6 reductions, 7 dE/dP (no launches: the force kernels form dE/dP per
+ * atom).  Arrays hold TMD_NPROF entries. */
 #define TMD_NPROF 8
 int tmd_profile_enable(tmd_system *sys, int enable);
 int tmd_profile_read(tmd_system *sys, long *launches, double *ms, int reset);

@@ -263,7 +263,8 @@ int default_force_variant(const tmd_model *m) {
 ForceArgs force_args(tmd_system *s, float scale, int variant) {
   ForceArgs fa{};
   fa.n = s->n; fa.cap = s->cap; fa.kp = s->m->kp; fa.box = s->box; fa.scale = scale;
-  fa.x = s->x; fa.elem = s->elem; fa.nbr = s->nbr; fa.boff = s->boff; fa.S = s->P;
+  fa.x = s->x; fa.elem = s->elem; fa.nbr = s->nbr; fa.boff = s->boff;
+  fa.P = s->P; fa.G = s->G; fa.dEdG = s->dEdG;
   fa.pdf = s->pdf; fa.wv = s->wv;
   fa.cbox = s->ncells ? s->cbox : nullptr; fa.acell = s->acell;
   fa.variant = variant;
@@ -300,9 +301,6 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
     launch_mlp_fp32(ma, s->st, s->launches);
   }
   prof_end(s, 2);
-  prof_begin(s);
-  launch_dedp(s->n, m->kp, s->P, s->G, s->dEdG, s->st, s->launches);  // P becomes S
-  prof_end(s, 7);
   const ForceArgs fa = force_args(s, scale, s->force_variant);
   prof_begin(s);
   launch_force(fa, s->st, s->launches);

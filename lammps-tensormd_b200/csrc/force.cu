@@ -29,70 +29,6 @@ void launch_force(const ForceArgs &a, cudaStream_t st, long &launches) {
 }
 
 // ---------------------------------------------------------------------
-// dE/dP (kernel2_GPU, kernel.cu:730-848; tensor_ops.cpp:633-674): one thread
-// per (atom, block, filter) row; the row's D values of P are read and S
-// written over them with vector accesses, T is indexed by the loop counter
-// (the same for every lane, a broadcast).  Keeping this small contraction out
-// of k_force keeps the force kernel's code compact (its pair loop runs out of
-// the instruction cache) for any number of elements.
-// ---------------------------------------------------------------------
-template <int D, int M>
-__global__ void k_dedp(long nrows, KParams kp, float *__restrict__ P,
-                       const float *__restrict__ G, const float *__restrict__ dEdG) {
-  const long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= nrows) return;
-  // G and dE/dG rows are [n*B*K][M]
-  float gp[M];
-#pragma unroll
-  for (int m = 0; m < M; m++) gp[m] = __ldg(dEdG + row * M + m);
-  const float g0 = __ldg(G + row * M);
-  gp[0] = fabsf(g0) < 1e-8f ? 0.f : gp[0] / g0 * 0.5f;
-  float p[D];
-  float *pr = P + row * D;
-  if constexpr (D % 4 == 0) {
-#pragma unroll
-    for (int v = 0; v < D / 4; v++) {
-      const float4 q = reinterpret_cast<const float4 *>(pr)[v];
-      p[4 * v] = q.x; p[4 * v + 1] = q.y; p[4 * v + 2] = q.z; p[4 * v + 3] = q.w;
-    }
-  } else {
-#pragma unroll
-    for (int d = 0; d < D; d++) p[d] = pr[d];
-  }
-#pragma unroll
-  for (int d = 0; d < D; d++) {
-    float t = 0.f;
-#pragma unroll
-    for (int m = 0; m < M; m++) t = fmaf(gp[m], kp.T[m * D + d], t);
-    p[d] = 2.f * t * p[d];
-  }
-  if constexpr (D % 4 == 0) {
-#pragma unroll
-    for (int v = 0; v < D / 4; v++)
-      reinterpret_cast<float4 *>(pr)[v] = make_float4(p[4 * v], p[4 * v + 1], p[4 * v + 2],
-                                                      p[4 * v + 3]);
-  } else {
-#pragma unroll
-    for (int d = 0; d < D; d++) pr[d] = p[d];
-  }
-}
-
-void launch_dedp(int n, const KParams &kp, float *P, const float *G, const float *dEdG,
-                 cudaStream_t st, long &launches) {
-  const long nrows = (long)n * kp.B * kp.K;
-  if (nrows == 0) return;
-  const int T = 128;
-  const unsigned grid = (unsigned)((nrows + T - 1) / T);
-  switch (kp.D) {
-    case 1: k_dedp<1, 1><<<grid, T, 0, st>>>(nrows, kp, P, G, dEdG); break;
-    case 4: k_dedp<4, 2><<<grid, T, 0, st>>>(nrows, kp, P, G, dEdG); break;
-    case 10: k_dedp<10, 3><<<grid, T, 0, st>>>(nrows, kp, P, G, dEdG); break;
-    default: k_dedp<20, 4><<<grid, T, 0, st>>>(nrows, kp, P, G, dEdG); break;
-  }
-  launches += 1;
-}
-
-// ---------------------------------------------------------------------
 // Gather: f_i = sum over own slots of (df_ij - df_ji), FP64, fixed order.
 // df_ji is read from the partner slot rev[t] written by atom j, so every
 // atom sums its own row and no two threads write the same force.  8 lanes

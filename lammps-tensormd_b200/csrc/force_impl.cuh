@@ -7,7 +7,7 @@
 //   U_k = sum_d S[k,d] M_d, V_d = sum_k S[k,d] H_k
 //   df = (sum_k U_k dH_k) u + sum_d V_d dM_d/dx_j     (F1 + F2, kernel.cu:541-631,
 //                                                       tensor_ops.cpp:126-190,470-535)
-// S is formed by k_dedp (force.cu) over P in place; this kernel loads it.
+// S of an (atom, block) is formed when the kernel reaches the block (dedp_row).
 // The reference writes U, V, F1 and F2 per padded slot and scatters df with
 // FP64 atomics (kernel.cu:1639-1758).  Here S stays in registers (4 filters x D
 // per lane as FP32 pairs, TPA = K/4 lanes per atom), U and V are packed FP32x2
@@ -27,12 +27,33 @@
 
 namespace tmd {
 
+// dE/dG' of one (atom, block, filter) row (kernel2_GPU, kernel.cu:730-848;
+// tensor_ops.cpp:633-674): dE/dG'_m = dE/dG_m for m > 0 and
+// dE/dG'_0 = 0.5 dE/dG_0 / G_0 (0 when |G_0| < 1e-8); then
+// S[k][d] = 2 P[k][d] sum_m T[m][d] dE/dG'_m, m ascending.
+__device__ inline void dedp_row_g(const float *__restrict__ G, const float *__restrict__ dEdG,
+                                  size_t row, int M, float gp[4]) {
+#pragma unroll
+  for (int m = 0; m < 4; m++) gp[m] = m < M ? __ldg(dEdG + row * M + m) : 0.f;
+  const float g0 = __ldg(G + row * M);
+  gp[0] = fabsf(g0) < 1e-8f ? 0.f : gp[0] / g0 * 0.5f;
+}
+__device__ inline float dedp_elem(const float gp[4], const float *T, int D, int M, int d,
+                                  float p) {
+  float t = 0.f;
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+    if (m < M) t = fmaf(gp[m], T[m * D + d], t);
+  return 2.f * t * p;
+}
+
 template <int TPA, int D, int RK, bool MULTI>
 __global__ void __launch_bounds__(kPairThreads, 3)
 k_force(KParams kp, BoxP box, int n, int cap, float scale,
         const double *__restrict__ x, const int *__restrict__ elem,
         const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
-        const float *__restrict__ S, float4 *__restrict__ pdf,
+        const float *__restrict__ P, const float *__restrict__ G,
+        const float *__restrict__ dEdG, float4 *__restrict__ pdf,
         double *__restrict__ wv, const BoxP *__restrict__ cbox,
         const int *__restrict__ acell) {
   constexpr int D2 = (D + 1) / 2;
@@ -65,24 +86,28 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
     if (b > 0) __syncwarp(live);
     const int s0 = bo[b], s1 = bo[b + 1];
     if (s0 == s1) continue;
-    // S = dE/dP of this lane's 4 filters (4 x D contiguous floats), as FP32
-    // pairs over d
+    // S = dE/dP of this lane's 4 filters as FP32 pairs over d, formed here
+    // (a rolled loop: the pair loop below must stay in the instruction cache)
     float2 S2[4][D2];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int p = 0; p < D2; p++) S2[q][p] = make_float2(0.f, 0.f);
     {
-      const float *Sp = S + (((size_t)a * B + b) * K + k0) * D;
-      if constexpr (D % 2 == 0) {
-        const float2 *S2p = reinterpret_cast<const float2 *>(Sp);
+      const size_t row0 = ((size_t)a * B + b) * K + k0;
 #pragma unroll
-        for (int q = 0; q < 4; q++)
+      for (int q = 0; q < 4; q++) {
+        float gp[4];
+        dedp_row_g(G, dEdG, row0 + q, kp.M, gp);
+        const float *Pp = P + (row0 + q) * D;
 #pragma unroll
-          for (int p = 0; p < D2; p++) S2[q][p] = __ldg(S2p + q * D2 + p);
-      } else {
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-#pragma unroll
-          for (int p = 0; p < D2; p++)
-            S2[q][p] = make_float2(__ldg(Sp + q * D + 2 * p),
-                                   2 * p + 1 < D ? __ldg(Sp + q * D + 2 * p + 1) : 0.f);
+        for (int p = 0; p < D2; p++) {
+          const float s0 = dedp_elem(gp, kp.T, D, kp.M, 2 * p, __ldg(Pp + 2 * p));
+          const float s1 = 2 * p + 1 < D
+                               ? dedp_elem(gp, kp.T, D, kp.M, 2 * p + 1, __ldg(Pp + 2 * p + 1))
+                               : 0.f;
+          S2[q][p] = make_float2(s0, s1);
+        }
       }
     }
     float4 *pdf_row = pdf + (size_t)a * cap;
@@ -178,7 +203,7 @@ void launch_force_tpa(const ForceArgs &a, cudaStream_t st) {
   long threads = (long)a.n * TPA;
   int grid = (int)((threads + T - 1) / T);
   if (grid < 1) grid = 1;
-#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.S, a.pdf, a.wv, a.cbox, a.acell
+#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.dEdG, a.pdf, a.wv, a.cbox, a.acell
   switch (a.kp.D) {
     case 1: k_force<TPA, 1, RK, MULTI><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;
     case 4: k_force<TPA, 4, RK, MULTI><<<grid, T, 0, st>>>(TMD_FORCE_ARGS); break;

@@ -1,6 +1,8 @@
 // force_pl.cuh -- pair-per-lane form of the pair-force kernel.
 //
-// Same mathematics and outputs as k_force (force_impl.cuh): for every active
+// Same mathematics and outputs as k_force (force_impl.cuh): S = dE/dP of each
+// (atom, element block) formed from P, G and dE/dG when the group reaches the
+// block (dedp_row_g / dedp_elem), then for every active
 // pair of atom i, V_d = sum_k S[k,d] H_k, W_d = sum_k S[k,d] dH_k,
 // df = (sum_d M_d W_d) u + grad Q(V) / r, scaled, into pdf[i*cap + t]; FP64
 // per-atom virial into wv[i].
@@ -24,13 +26,16 @@
 namespace tmd {
 
 // Shared-memory layout of k_force_pl (floats): radial parameters [4][K] (none
-// for the table kind), then per atom group an S block [K][D4] + 4 (the extra
-// 4 floats put consecutive groups' blocks in different banks).
+// for the table kind) and T [4][D4], then per atom group an S block [K][D4]
+// + 4 (the extra 4 floats put consecutive groups' blocks in different banks)
+// and the dE/dG' rows [K][4].
 template <int D>
 struct PlLayout {
   static constexpr int D4 = (D + 3) / 4 * 4;
-  static __host__ __device__ inline int params(int K, int rk) { return rk == kRadTable ? 0 : 4 * K; }
-  static __host__ __device__ inline int group(int K) { return K * D4 + 4; }
+  static __host__ __device__ inline int params(int K, int rk) {
+    return (rk == kRadTable ? 0 : 4 * K) + 4 * D4;
+  }
+  static __host__ __device__ inline int group(int K) { return K * D4 + 4 + 4 * K; }
   static __host__ inline size_t bytes(int K, int rk, int groups) {
     return sizeof(float) * ((size_t)params(K, rk) + (size_t)groups * group(K));
   }
@@ -41,7 +46,8 @@ __global__ void __launch_bounds__(kPairThreads, 4)
 k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
            const double *__restrict__ x, const int *__restrict__ elem,
            const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
-           const float *__restrict__ S, float4 *__restrict__ pdf,
+           const float *__restrict__ P, const float *__restrict__ G,
+           const float *__restrict__ dEdG, float4 *__restrict__ pdf,
            double *__restrict__ wv, const BoxP *__restrict__ cbox,
            const int *__restrict__ acell) {
   using L = PlLayout<D>;
@@ -49,8 +55,13 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
   constexpr int P2 = D4 / 2;  // FP32 pairs per S row (pad columns hold 0)
   extern __shared__ float4 pl_dyn[];
   __shared__ GeoSlot geo[2 * kPairThreads];
-  const int K = kp.K, B = kp.B;
+  const int K = kp.K, B = kp.B, M = kp.M;
   float *rp = reinterpret_cast<float *>(pl_dyn);
+  float *Ts = rp + (RK == kRadTable ? 0 : 4 * K);  // T[m][d], rows of D4
+  for (int i = threadIdx.x; i < 4 * D4; i += blockDim.x) {
+    const int m = i / D4, d = i - m * D4;
+    Ts[i] = (m < M && d < D) ? kp.T[m * D + d] : 0.f;
+  }
   if (RK != kRadTable) {
     for (int i = threadIdx.x; i < K; i += blockDim.x) {
       rp[i] = RK == kRadGauss ? kp.p1[i] : kp.p0[i];
@@ -73,6 +84,7 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
   pr.ring = geo + 2 * (threadIdx.x - sub);
   const unsigned gmask = pr.gmask;
   float *Sg = rp + L::params(K, RK) + (threadIdx.x / W) * L::group(K);
+  float *gpg = Sg + K * D4 + 4;  // dE/dG' rows [K][4]
   const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
   const double xi = x[3 * a], yi = x[3 * a + 1], zi = x[3 * a + 2];
   const uint32_t *row = nbr + (size_t)a * cap;
@@ -83,17 +95,54 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
     if (b > 0) __syncwarp(live);  // keep the warp's groups on the same block
     const int s0 = bo[b], s1 = bo[b + 1];
     if (s0 == s1) continue;
-    // stage S of (atom, block) as [K][D4] rows
+    // S = dE/dP of (atom, block) as [K][D4] rows: dE/dG' rows first, then
+    // one element per lane step (same arithmetic and order as dedp_elem)
     __syncwarp(gmask);
-    const float *Sp = S + ((size_t)a * B + b) * K * D;
-    if constexpr (D == D4) {
-      const float4 *S4 = reinterpret_cast<const float4 *>(Sp);
-      float4 *G4 = reinterpret_cast<float4 *>(Sg);
-      for (int i = sub; i < K * D / 4; i += W) G4[i] = __ldg(S4 + i);
-    } else {
-      for (int i = sub; i < K * D4; i += W) {
-        const int k = i / D4, d = i - k * D4;
-        Sg[i] = d < D ? __ldg(Sp + k * D + d) : 0.f;
+    const size_t row0 = ((size_t)a * B + b) * K;
+    for (int k = sub; k < K; k += W) {
+      float gp[4];
+      dedp_row_g(G, dEdG, row0 + k, M, gp);
+      *reinterpret_cast<float4 *>(gpg + 4 * k) = make_float4(gp[0], gp[1], gp[2], gp[3]);
+    }
+    __syncwarp(gmask);
+    {
+      // 4-column units of the [K][D4] block, kBatch P loads in flight per lane
+      constexpr int kBatch = 4;
+      const int nv = K * D4 / 4;
+      for (int v0 = sub; v0 < nv; v0 += W * kBatch) {
+        float4 pv[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; u++) {
+          const int v = v0 + u * W;
+          pv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (v < nv) {
+            const int k = (4 * v) / D4, d0 = 4 * v - k * D4;
+            const float *Pr = P + (row0 + k) * D;
+            if constexpr (D == D4) {
+              pv[u] = __ldg(reinterpret_cast<const float4 *>(Pr + d0));
+            } else {
+              pv[u].x = d0 < D ? __ldg(Pr + d0) : 0.f;
+              pv[u].y = d0 + 1 < D ? __ldg(Pr + d0 + 1) : 0.f;
+              pv[u].z = d0 + 2 < D ? __ldg(Pr + d0 + 2) : 0.f;
+              pv[u].w = d0 + 3 < D ? __ldg(Pr + d0 + 3) : 0.f;
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; u++) {
+          const int v = v0 + u * W;
+          if (v < nv) {
+            const int k = (4 * v) / D4, d0 = 4 * v - k * D4;
+            const float4 g4 = *reinterpret_cast<const float4 *>(gpg + 4 * k);
+            const float gp[4] = {g4.x, g4.y, g4.z, g4.w};
+            const float p[4] = {pv[u].x, pv[u].y, pv[u].z, pv[u].w};
+            float s[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+              s[j] = d0 + j < D ? dedp_elem(gp, Ts, D4, M, d0 + j, p[j]) : 0.f;
+            *reinterpret_cast<float4 *>(Sg + 4 * v) = make_float4(s[0], s[1], s[2], s[3]);
+          }
+        }
       }
     }
     __syncwarp(gmask);
@@ -199,9 +248,10 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
 
 // Atom groups per block: as many as fit 128 threads and 48 KB of shared
 // memory (the static ring plus the dynamic parameters and S blocks).
-inline int force_pl_groups(int W, int K, int D4, int rk) {
-  const size_t per = sizeof(float) * ((size_t)K * D4 + 4);
-  const size_t base = sizeof(float) * (rk == kRadTable ? 0 : 3 * (size_t)K) +
+template <int D>
+inline int force_pl_groups(int W, int K, int rk) {
+  const size_t per = sizeof(float) * (size_t)PlLayout<D>::group(K);
+  const size_t base = sizeof(float) * (size_t)PlLayout<D>::params(K, rk) +
                       sizeof(GeoSlot) * 2 * kPairThreads;
   int g = kPairThreads / W;
   while (g > 1 && base + g * per > 48 * 1024) g--;
@@ -210,10 +260,10 @@ inline int force_pl_groups(int W, int K, int D4, int rk) {
 
 template <int W, int RK, bool MULTI>
 void launch_force_pl_w(const ForceArgs &a, cudaStream_t st) {
-#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.S, a.pdf, a.wv, a.cbox, a.acell
+#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.dEdG, a.pdf, a.wv, a.cbox, a.acell
 #define TMD_PL_CASE(DV)                                                                     \
   case DV: {                                                                                \
-    const int g = force_pl_groups(W, a.kp.K, PlLayout<DV>::D4, RK);                         \
+    const int g = force_pl_groups<DV>(W, a.kp.K, RK);                         \
     const int T = g * W;                                                                    \
     const long threads = (long)a.n * W;                                                     \
     const int grid = (int)std::max(1L, (threads + T - 1) / T);                              \
@@ -226,7 +276,7 @@ void launch_force_pl_w(const ForceArgs &a, cudaStream_t st) {
     TMD_PL_CASE(4)
     TMD_PL_CASE(10)
     default: {
-      const int g = force_pl_groups(W, a.kp.K, PlLayout<20>::D4, RK);
+      const int g = force_pl_groups<20>(W, a.kp.K, RK);
       const int T = g * W;
       const long threads = (long)a.n * W;
       const int grid = (int)std::max(1L, (threads + T - 1) / T);

@@ -137,11 +137,6 @@ void mlp_fp8_prepare(size_t smem, bool dz_bf16);
 void pack_core_chunks_fp8(const float *src, int rows, int cols, long ld_r, long ld_k,
                           float scale, uint8_t *dst);
 
-// dE/dP: S[n][B][K][D] = 2 P sum_m T[m][d] dEdG'[b][k][m] (dEdG'0 =
-// 0.5 dEdG0 / G0), written over P in place.
-void launch_dedp(int n, const KParams &kp, float *P, const float *G, const float *dEdG,
-                 cudaStream_t st, long &launches);
-
 // Force: per-pair dE_i/dx_j into pdf, per-atom virial partials.
 // Kernel forms: K/4 lanes per atom with 4 filters each (k_force), or W lanes
 // per atom with whole pairs per lane (k_force_pl, W = 8, 16, 32).
@@ -159,7 +154,9 @@ struct ForceArgs {
   const int *elem;
   const uint32_t *nbr;
   const int *boff;
-  const float *S;     // dE/dP [n][B][K][D] (launch_dedp)
+  // S = dE/dP is formed per (atom, block) from the descriptor moments P
+  // [n][B][K][D] and the MLP rows G, dE/dG [n*B*K][M] (dedp_row)
+  const float *P, *G, *dEdG;
   float4 *pdf;
   double *wv;  // [n][6] per-atom sum of -r_ij (x) df over own pairs
   const BoxP *cbox;   // multi-cell mode (as DescArgs)
