@@ -189,9 +189,12 @@ def run_ours(args, rank, world, local):
     sys_ = TensorMDSystem(model, n, 1.0)
     sys_.set_box(box)
     sys_.set_atoms(x, t, v)
-    # setup, outside the timed region: pick the force-loop form for this shape
+    # setup, outside the timed region: pick the kernel forms for this shape
     tune_ms = sys_.autotune(reps=5)
-    force_form = {"chosen": sys_.force_variant(), "ms_per_launch": tune_ms}
+    tune_dms = sys_.autotune(reps=5, family="descriptor")
+    force_form = {"chosen": sys_.force_variant(), "ms_per_launch": tune_ms,
+                  "descriptor_chosen": sys_.descriptor_variant(),
+                  "descriptor_ms_per_launch": tune_dms}
     stream = torch.cuda.ExternalStream(sys_.stream(), device=dev)
     if world > 1:
         import torch.distributed as dist
@@ -412,6 +415,7 @@ def run_cells(args, rank, world, local, dev, barrier):
     b.set_cells(data["boxes"])
     b.set_atoms(data["x"], data["types"], data["v"])
     tune_ms = b.system().autotune(reps=3)
+    tune_dms = b.system().autotune(reps=3, family="descriptor")
     n = b.n
     dt = 0.001
     stream = torch.cuda.ExternalStream(b.system().stream(), device=dev)
@@ -445,7 +449,9 @@ def run_cells(args, rank, world, local, dev, barrier):
            "ms_per_step": ms / args.cells_steps, "steps": args.cells_steps,
            "natoms": n, "ncells": c["ncells"], "gpu_launches": launches,
            "max_cell_energy_drift_eV_per_atom": drift,
-           "force_form": {"chosen": sv.force_variant(), "ms_per_launch": tune_ms},
+           "force_form": {"chosen": sv.force_variant(), "ms_per_launch": tune_ms,
+                          "descriptor_chosen": sv.descriptor_variant(),
+                          "descriptor_ms_per_launch": tune_dms},
            "kernel_ms": {k: (cnt, t / max(cnt, 1)) for k, (cnt, t) in prof.items()},
            "config": {k: v for k, v in c.items() if k != "pot"} | {"potential": c["pot"]}}
     b.close()
@@ -471,6 +477,7 @@ def run_w23k(args, rank, world, local, dev, barrier):
     s.set_box(box)
     s.set_atoms(x, t, v)
     tune_ms = s.autotune(reps=5)
+    tune_dms = s.autotune(reps=5, family="descriptor")
     stream = torch.cuda.ExternalStream(s.stream(), device=dev)
     s.nvt_run(max(args.warmup, 3), 0.001, 300.0, 300.0, 0.1)
     s.set_atoms(x, t, v)
@@ -492,7 +499,8 @@ def run_w23k(args, rank, world, local, dev, barrier):
         dist.all_reduce(ms, op=dist.ReduceOp.MAX)
     ms = float(ms.item())
     value = n * 100 * world / (ms / 1000.0)
-    form = {"chosen": s.force_variant(), "ms_per_launch": tune_ms}
+    form = {"chosen": s.force_variant(), "ms_per_launch": tune_ms,
+            "descriptor_chosen": s.descriptor_variant(), "descriptor_ms_per_launch": tune_dms}
     s.close()
     model.close()
     return {"value": value, "unit": UNIT, "ms_per_step": ms / 100, "natoms": n, "steps": 100,

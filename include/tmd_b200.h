@@ -149,12 +149,19 @@ int tmd_get_descriptors(tmd_system *sys, double *G);
  *   1  8 lanes per atom, one whole pair per lane, dE/dP staged in shared memory
  *   2  16 lanes per atom, as 1
  *   3  32 lanes per atom, as 1
+ * Family TMD_TUNE_DESCRIPTOR (the moment contraction P = sum H M,
+ * kernel.cu:1105, with G = T P^2):
+ *   0  K/4 lanes per atom, 4 filters per lane
+ *   1  min(K, 32) lanes per atom, K/min(K, 32) filters per lane, monomials of
+ *      a pair computed once and shared through shared memory
  * The forms agree to FP32 rounding (summation order).  set_variant picks one;
  * autotune runs one evaluation, times reps launches of every form of the
  * family on the system's current atoms, keeps the fastest and recomputes the
- * forces with it; ms[TMD_TUNE_VARIANTS] (may be NULL) receives the mean
- * device milliseconds per launch of each form. */
+ * results with it; ms (may be NULL) receives the mean device milliseconds per
+ * launch of each form (4 force forms, 2 descriptor forms; at most
+ * TMD_TUNE_VARIANTS). */
 #define TMD_TUNE_FORCE 0
+#define TMD_TUNE_DESCRIPTOR 1
 #define TMD_TUNE_VARIANTS 4
 int tmd_system_set_variant(tmd_system *sys, int family, int variant);
 int tmd_system_get_variant(tmd_system *sys, int family, int *variant);

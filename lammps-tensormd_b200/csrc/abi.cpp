@@ -253,6 +253,22 @@ int rebuild_now(tmd_system *s) {
 }
 
 // Force evaluation on the current (valid) list.
+DescArgs desc_args(tmd_system *s, int variant) {
+  DescArgs d{};
+  d.n = s->n; d.cap = s->cap; d.kp = s->m->kp; d.box = s->box; d.x = s->x;
+  d.elem = s->elem; d.nbr = s->nbr; d.boff = s->boff; d.P = s->P; d.G = s->G;
+  d.cbox = s->ncells ? s->cbox : nullptr; d.acell = s->acell;
+  d.variant = variant;
+  return d;
+}
+
+int default_desc_variant(const tmd_model *m) {
+  // measured on the B200 (tmd_system_autotune): the wide form is 1.25-1.33x
+  // faster at K = 16 and equal at K = 32
+  (void)m;
+  return kDescWide;
+}
+
 int default_force_variant(const tmd_model *m) {
   // measured on the B200 (tmd_system_autotune): whole pairs per lane beat 4
   // filters per lane by 1.2-1.6x; 16 lanes per atom for one element block
@@ -273,10 +289,7 @@ ForceArgs force_args(tmd_system *s, float scale, int variant) {
 
 void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   const tmd_model *m = s->m;
-  DescArgs d{};
-  d.n = s->n; d.cap = s->cap; d.kp = m->kp; d.box = s->box; d.x = s->x;
-  d.elem = s->elem; d.nbr = s->nbr; d.boff = s->boff; d.P = s->P; d.G = s->G;
-  d.cbox = s->ncells ? s->cbox : nullptr; d.acell = s->acell;
+  const DescArgs d = desc_args(s, s->desc_variant);
   prof_begin(s);
   launch_descriptor(d, s->st, s->launches);
   prof_end(s, 1);
@@ -825,6 +838,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   s->natoms_cap = natoms_cap;
   s->skin = skin;
   s->force_variant = default_force_variant(m);
+  s->desc_variant = default_desc_variant(m);
   const HostModel &h = m->h;
   size_t N = natoms_cap;
   cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
@@ -1119,45 +1133,59 @@ int tmd_get_descriptors(tmd_system *s, double *G) {
   return TMD_OK;
 }
 
+namespace {
+int family_forms(int family) {
+  return family == TMD_TUNE_FORCE ? kForceVariants
+                                  : (family == TMD_TUNE_DESCRIPTOR ? kDescVariants : 0);
+}
+int &family_slot(tmd_system *s, int family) {
+  return family == TMD_TUNE_FORCE ? s->force_variant : s->desc_variant;
+}
+}  // namespace
+
 int tmd_system_set_variant(tmd_system *s, int family, int variant) {
   if (!s) return fail(TMD_ERR_ARG, "null system");
-  if (family != TMD_TUNE_FORCE) return fail(TMD_ERR_ARG, "unknown kernel family");
-  if (variant < 0 || variant >= kForceVariants) return fail(TMD_ERR_ARG, "unknown variant");
-  if (variant != s->force_variant) {
+  if (family_forms(family) == 0) return fail(TMD_ERR_ARG, "unknown kernel family");
+  if (variant < 0 || variant >= family_forms(family)) return fail(TMD_ERR_ARG, "unknown variant");
+  if (variant != family_slot(s, family)) {
     TMD_CUDA(cudaStreamSynchronize(s->st));
     drop_graph(s);  // the captured step holds the old kernel
-    s->force_variant = variant;
+    family_slot(s, family) = variant;
   }
   return TMD_OK;
 }
 
 int tmd_system_get_variant(tmd_system *s, int family, int *variant) {
   if (!s || !variant) return fail(TMD_ERR_ARG, "null argument");
-  if (family != TMD_TUNE_FORCE) return fail(TMD_ERR_ARG, "unknown kernel family");
-  *variant = s->force_variant;
+  if (family_forms(family) == 0) return fail(TMD_ERR_ARG, "unknown kernel family");
+  *variant = family_slot(s, family);
   return TMD_OK;
 }
 
 int tmd_system_autotune(tmd_system *s, int family, int reps, double *ms) {
   if (!s) return fail(TMD_ERR_ARG, "null system");
-  if (family != TMD_TUNE_FORCE) return fail(TMD_ERR_ARG, "unknown kernel family");
+  const int nforms = family_forms(family);
+  if (nforms == 0) return fail(TMD_ERR_ARG, "unknown kernel family");
   if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before autotune");
   if (reps < 1) reps = 1;
   TMD_CUDA(cudaSetDevice(s->m->device));
-  // a full evaluation leaves S = dE/dP and the list current for the force loop
+  // a full evaluation leaves the list, P, G and dE/dG current for either loop
   int rc = tmd_compute(s, 0, 0, 1.0, nullptr, nullptr, nullptr, nullptr, nullptr);
   if (rc) return rc;
   cudaEvent_t e0, e1;
   TMD_CUDA(cudaEventCreate(&e0));
   TMD_CUDA(cudaEventCreate(&e1));
-  int best = s->force_variant;
+  int best = family_slot(s, family);
   float best_ms = 0.f;
   cudaError_t err = cudaSuccess;
-  for (int v = 0; v < kForceVariants && err == cudaSuccess; v++) {
-    const ForceArgs fa = force_args(s, 1.0f, v);
-    launch_force(fa, s->st, s->launches);  // warm-up
+  for (int v = 0; v < nforms && err == cudaSuccess; v++) {
+    auto launch = [&]() {
+      if (family == TMD_TUNE_FORCE) launch_force(force_args(s, 1.0f, v), s->st, s->launches);
+      else launch_descriptor(desc_args(s, v), s->st, s->launches);
+    };
+    launch();  // warm-up
     err = cudaEventRecord(e0, s->st);
-    for (int r = 0; r < reps && err == cudaSuccess; r++) launch_force(fa, s->st, s->launches);
+    for (int r = 0; r < reps && err == cudaSuccess; r++) launch();
     if (err == cudaSuccess) err = cudaEventRecord(e1, s->st);
     if (err == cudaSuccess) err = cudaEventSynchronize(e1);
     if (err == cudaSuccess) err = cudaGetLastError();
@@ -1173,7 +1201,7 @@ int tmd_system_autotune(tmd_system *s, int family, int reps, double *ms) {
     return fail(TMD_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(err));
   rc = tmd_system_set_variant(s, family, best);
   if (rc) return rc;
-  // forces of the chosen form (the forms round differently)
+  // results of the chosen form (the forms round differently)
   return tmd_compute(s, 0, 0, 1.0, nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 

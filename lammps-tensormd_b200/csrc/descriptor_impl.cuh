@@ -111,6 +111,15 @@ struct PairRing {
   __device__ inline int feed(const KParams &kp, const BoxP &box, double xi, double yi,
                              double zi, const double *__restrict__ x,
                              const uint32_t *__restrict__ row, float4 *__restrict__ pdf_row) {
+    return feed_with(kp, box, xi, yi, zi, x, row, pdf_row, [](int, const PairGeo &) {});
+  }
+  // As feed; extra(slot index, geometry) runs for every queued pair, on the
+  // lane that computed it (per-pair data kept beside the ring).
+  template <class Extra>
+  __device__ inline int feed_with(const KParams &kp, const BoxP &box, double xi, double yi,
+                                  double zi, const double *__restrict__ x,
+                                  const uint32_t *__restrict__ row,
+                                  float4 *__restrict__ pdf_row, Extra extra) {
     while (qn < TPA && t < s1) {
       const NbPos pc = pnext;
       pnext = load_nb(x, enext, t + TPA + sub < s1);
@@ -119,8 +128,11 @@ struct PairRing {
       pair_geometry(kp, box, xi, yi, zi, pc, g);
       const bool act = g.ti >= 0;
       const unsigned bal = (__ballot_sync(gmask, act) >> gshift) & kBits;
-      if (act) geo_store(slot(qn + __popc(bal & ((1u << sub) - 1u))), g, t + sub);
-      else if (pdf_row != nullptr && t + sub < s1)
+      if (act) {
+        const int c = qn + __popc(bal & ((1u << sub) - 1u));
+        geo_store(slot(c), g, t + sub);
+        extra((head + c) & (kSlots - 1), g);
+      } else if (pdf_row != nullptr && t + sub < s1)
         pdf_row[t + sub] = make_float4(0.f, 0.f, 0.f, 0.f);
       qn += __popc(bal);
       t += TPA;
@@ -208,6 +220,120 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
   }
 }
 
+// Wide-group form: W = min(K, 32) lanes per atom, FPL = K / W filters per
+// lane.  With K = 16 the 4-filter form packs 8 atoms into a warp whose groups
+// fetch, test and queue their rows at different rates, so much of the warp
+// idles; here a warp holds one or two atoms.  The lane that computes a pair's
+// geometry also computes its D monomials once and keeps them beside the ring
+// slot; every lane then reads them as broadcast vectors and accumulates
+// P[k][d] for its own filters in the same order (pairs in row order, FP32
+// pairs over d) as k_descriptor.
+template <int W, int FPL, int D, int RK, bool MULTI>
+__global__ void __launch_bounds__(kPairThreads, 6)
+k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
+               const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
+               float *__restrict__ P, const BoxP *__restrict__ cbox,
+               const int *__restrict__ acell) {
+  constexpr int D4 = (D + 3) / 4 * 4;
+  constexpr int P2 = D4 / 2;
+  __shared__ GeoSlot geo[2 * kPairThreads];
+  __shared__ __align__(16) float mono[2 * kPairThreads * D4];
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = gt / W;
+  const int sub = gt % W;
+  if (a >= n) return;
+  const int lane = threadIdx.x & 31;
+  PairRing<W> pr;
+  pr.sub = sub;
+  pr.gshift = lane & ~(W - 1);
+  pr.gmask = PairRing<W>::kBits << pr.gshift;
+  pr.ring = geo + 2 * (threadIdx.x - sub);
+  float *mr = mono + 2 * (threadIdx.x - sub) * D4;  // monomials of the group's slots
+  const int B = kp.B, K = kp.K;
+  const int kf = sub * FPL;
+  Radial1<RK> R[FPL];
+#pragma unroll
+  for (int f = 0; f < FPL; f++) R[f] = load_radial1<RK>(kp, kf + f);
+  const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
+  const double xi = x[3 * a], yi = x[3 * a + 1], zi = x[3 * a + 2];
+  const uint32_t *row = nbr + (size_t)a * cap;
+  const int *bo = boff + (size_t)a * (B + 1);
+  const unsigned live = live_lanes(gt, (long)n * W);
+  auto keep_monomials = [&](int idx, const PairGeo &g) {
+    float M[D4];
+    moments<D>(g.ux, g.uy, g.uz, M);
+#pragma unroll
+    for (int d = D; d < D4; d++) M[d] = 0.f;
+    float4 *dst = reinterpret_cast<float4 *>(mr + idx * D4);
+#pragma unroll
+    for (int v = 0; v < D4 / 4; v++)
+      dst[v] = make_float4(M[4 * v], M[4 * v + 1], M[4 * v + 2], M[4 * v + 3]);
+  };
+  for (int b = 0; b < B; b++) {
+    if (b > 0) __syncwarp(live);
+    float2 acc[FPL][P2];
+#pragma unroll
+    for (int f = 0; f < FPL; f++)
+#pragma unroll
+      for (int p = 0; p < P2; p++) acc[f][p] = make_float2(0.f, 0.f);
+    pr.begin(x, row, bo[b], bo[b + 1]);
+    for (;;) {
+      const int cnt = pr.feed_with(kp, bx, xi, yi, zi, x, row, nullptr, keep_monomials);
+      if (cnt == 0) break;
+      for (int c = 0; c < cnt; c++) {
+        const PairGeo g = geo_load(pr.slot(c));
+        const float4 *ms = reinterpret_cast<const float4 *>(
+            mr + ((pr.head + c) & (PairRing<W>::kSlots - 1)) * D4);
+        float2 h2[FPL];
+#pragma unroll
+        for (int f = 0; f < FPL; f++) {
+          const float h = radial1<RK>(kp, R[f], g);
+          h2[f] = make_float2(h, h);
+        }
+#pragma unroll
+        for (int v = 0; v < D4 / 4; v++) {
+          const float4 m4 = ms[v];
+          const float2 lo = make_float2(m4.x, m4.y), hi = make_float2(m4.z, m4.w);
+#pragma unroll
+          for (int f = 0; f < FPL; f++) {
+            acc[f][2 * v] = __ffma2_rn(h2[f], lo, acc[f][2 * v]);
+            acc[f][2 * v + 1] = __ffma2_rn(h2[f], hi, acc[f][2 * v + 1]);
+          }
+        }
+      }
+      pr.pop(cnt);
+    }
+    float *Pp = P + (((size_t)a * B + b) * K + kf) * D;
+#pragma unroll
+    for (int f = 0; f < FPL; f++) {
+      if constexpr (D % 2 == 0) {
+        float2 *P2p = reinterpret_cast<float2 *>(Pp + f * D);
+#pragma unroll
+        for (int p = 0; p < D / 2; p++) P2p[p] = acc[f][p];
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; d++) Pp[f * D + d] = (d & 1) ? acc[f][d >> 1].y : acc[f][d >> 1].x;
+      }
+    }
+  }
+}
+
+template <int W, int FPL, int RK, bool MULTI>
+void launch_descriptor_w(const DescArgs &a, cudaStream_t st) {
+  const int T = kPairThreads;
+  const long threads = (long)a.n * W;
+  int grid = (int)((threads + T - 1) / T);
+  if (grid < 1) grid = 1;
+#define TMD_DESCW_ARGS a.kp, a.box, a.n, a.cap, a.x, a.nbr, a.boff, a.P, a.cbox, a.acell
+  switch (a.kp.D) {
+    case 1: k_descriptor_w<W, FPL, 1, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
+    case 4: k_descriptor_w<W, FPL, 4, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
+    case 10: k_descriptor_w<W, FPL, 10, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
+    default: k_descriptor_w<W, FPL, 20, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
+  }
+#undef TMD_DESCW_ARGS
+}
+
 // G[b,k,m] = sum_d T[m,d] P[b,k,d]^2, G[b,k,0] = sign(P0) sqrt(.)
 // (kernel_1_fused_device, kernel.cu:1028-1061): one thread per output, the D
 // values of the row from L1, coalesced writes in the MLP row layout.
@@ -265,6 +391,17 @@ void launch_descriptor_tpa(const DescArgs &a, cudaStream_t st) {
 // own translation unit so the variants compile in parallel.
 template <int RK, bool MULTI>
 void launch_descriptor_rk(const DescArgs &a, cudaStream_t st) {
+  if (a.variant == kDescWide) {
+    switch (a.kp.K) {
+      case 4: launch_descriptor_w<4, 1, RK, MULTI>(a, st); break;
+      case 8: launch_descriptor_w<8, 1, RK, MULTI>(a, st); break;
+      case 16: launch_descriptor_w<16, 1, RK, MULTI>(a, st); break;
+      case 32: launch_descriptor_w<32, 1, RK, MULTI>(a, st); break;
+      case 64: launch_descriptor_w<32, 2, RK, MULTI>(a, st); break;
+      default: launch_descriptor_w<32, 4, RK, MULTI>(a, st); break;
+    }
+    return;
+  }
   switch (a.kp.K / 4) {
     case 1: launch_descriptor_tpa<1, RK, MULTI>(a, st); break;
     case 2: launch_descriptor_tpa<2, RK, MULTI>(a, st); break;

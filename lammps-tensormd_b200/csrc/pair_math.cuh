@@ -217,6 +217,61 @@ __device__ inline void radial4(const KParams &kp, const Radial4<RK> &R, const Pa
   }
 }
 
+// Radial parameters of one filter k, loaded once per kernel by the lane that
+// owns the filter (the wide-group descriptor form).
+template <int RK>
+struct Radial1 {
+  float a, b, c, blo, gc, gl;
+  int k;
+};
+
+template <int RK>
+__device__ inline Radial1<RK> load_radial1(const KParams &kp, int k) {
+  Radial1<RK> R{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, k};
+  if (RK == kRadGeneric) { R.a = kp.p0[k]; R.c = kp.p2[k]; }
+  if (RK != kRadTable) R.b = kp.p1[k];
+  if (RK == kRadGauss) { R.blo = kp.p1lo[k]; R.gc = kp.gc[k]; R.gl = kp.gcl[k]; }
+  return R;
+}
+
+// H_k of one filter: the expressions of radial4 for a single k.
+template <int RK>
+__device__ inline float radial1(const KParams &kp, const Radial1<RK> &R, const PairGeo &g) {
+  if (RK == kRadTable) {
+    if (g.ti <= 0 || g.ti >= kp.tab_n - 2) return 0.f;
+    const int K = kp.K;
+    const float *row = kp.table + (size_t)g.ti * 4 * K + R.k;
+    const float y = __ldg(row), s = __ldg(row + K), c1 = __ldg(row + 2 * K),
+                c2 = __ldg(row + 3 * K);
+    const float q = g.tq, dx = kp.tab_dx, rr = dx - q;
+    float c3 = fabsf(c2 * rr);
+    float c4 = c3 + fabsf(c1 * q);
+    if (c4 > 0.f) c3 = __fdividef(c3, c4);
+    c4 = c2 + c3 * (c1 - c2);
+    return y + q * (s - rr * c4);
+  }
+  float f;
+  if (RK == kRadGauss) {
+    float d = (g.r - R.b) + (g.rlo - R.blo);
+    f = exp2f(-R.gl * d * d);
+  } else {
+    const float r = g.r, a = R.a, b = R.b, c = R.c;
+    if (kp.method == 0) {
+      float xr = r / a;
+      float pw = powf(xr, b);
+      f = expf(-pw);
+    } else if (kp.method == 1) {
+      float gdr = b * (r - c);
+      float e1 = expf(-gdr), e2 = expf(-2.f * gdr);
+      f = a * (e2 - 2.f * e1);
+    } else {
+      float z = -b * ((r - c) / c);
+      f = a * expf(z);
+    }
+  }
+  return g.fc * f;
+}
+
 template <int D>
 __device__ inline void moments(float x, float y, float z, float M[D]) {
   M[0] = 1.f;

@@ -79,6 +79,7 @@ struct tmd_system {
   // kernel form of the pair-force loop (kForce*), set by the default rule,
   // tmd_system_set_variant or tmd_system_autotune
   int force_variant = 0;
+  int desc_variant = 0;    // kDesc*, the same way
   // kernel timing
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -139,6 +140,8 @@ int clear_status(tmd_system *s);
 int rebuild_now(tmd_system *s);
 void launch_force_eval(tmd_system *s, float scale, bool want_vatom);
 ForceArgs force_args(tmd_system *s, float scale, int variant);
+DescArgs desc_args(tmd_system *s, int variant);
+int default_desc_variant(const tmd_model *m);
 // Kernel form of the force loop used when nothing chose one.
 int default_force_variant(const tmd_model *m);
 NbArgs nb_args(tmd_system *s);

@@ -52,6 +52,12 @@ void launch_neighbor_check(int n, const double *x, const double *xbuild,
 void launch_set_flag(int *flag, cudaStream_t st, long &launches);
 
 // Descriptor: P[n][B][K][D], G[n][B*K*M].
+// Kernel forms: K/4 lanes per atom with 4 filters each (k_descriptor), or
+// min(K, 32) lanes per atom with K/min(K, 32) filters each and the monomials
+// of each pair computed once (k_descriptor_w).
+constexpr int kDescFilter4 = 0;
+constexpr int kDescWide = 1;
+constexpr int kDescVariants = 2;
 struct DescArgs {
   int n, cap;
   KParams kp;
@@ -63,6 +69,7 @@ struct DescArgs {
   float *P, *G;
   const BoxP *cbox;   // multi-cell mode: box of each cell, else nullptr
   const int *acell;   // multi-cell mode: cell of each atom
+  int variant;        // kDesc*
 };
 void launch_descriptor(const DescArgs &a, cudaStream_t st, long &launches);
 

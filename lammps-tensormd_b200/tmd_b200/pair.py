@@ -178,12 +178,26 @@ class TensorMDSystem:
         check(self.lib.tmd_system_get_variant(self.h, 0, ctypes.byref(v)))
         return self.FORCE_VARIANTS[v.value]
 
-    def autotune(self, reps: int = 5):
-        """Time every force-loop form on the current atoms, keep the fastest;
-        returns {form: ms per launch}."""
-        ms = np.zeros(len(self.FORCE_VARIANTS))
-        check(self.lib.tmd_system_autotune(self.h, 0, int(reps), _dp(ms)))
-        return dict(zip(self.FORCE_VARIANTS, ms.tolist()))
+    # kernel forms of the descriptor (family 1)
+    DESC_VARIANTS = ("filter4", "wide")
+
+    def set_descriptor_variant(self, variant):
+        v = self.DESC_VARIANTS.index(variant) if isinstance(variant, str) else int(variant)
+        check(self.lib.tmd_system_set_variant(self.h, 1, v))
+
+    def descriptor_variant(self) -> str:
+        v = ctypes.c_int()
+        check(self.lib.tmd_system_get_variant(self.h, 1, ctypes.byref(v)))
+        return self.DESC_VARIANTS[v.value]
+
+    def autotune(self, reps: int = 5, family: str = "force"):
+        """Time every form of a kernel family ("force" or "descriptor") on the
+        current atoms, keep the fastest; returns {form: ms per launch}."""
+        names = self.FORCE_VARIANTS if family == "force" else self.DESC_VARIANTS
+        ms = np.zeros(4)
+        check(self.lib.tmd_system_autotune(self.h, 0 if family == "force" else 1, int(reps),
+                                           _dp(ms)))
+        return dict(zip(names, ms[:len(names)].tolist()))
 
     def stream(self) -> int:
         p = ctypes.c_void_p()

@@ -1,6 +1,7 @@
-"""Kernel forms of the pair-force loop (tmd_system_set_variant / autotune).
+"""Kernel forms of the pair-force loop and of the descriptor
+(tmd_system_set_variant / autotune).
 
-Every form must meet the plain-form tolerances against the FP64 oracle
+Every combination of forms must meet the plain-form tolerances against the FP64 oracle
 (force relative RMS 1e-5, energy 1e-7 eV/atom on the benchmark shape and
 5e-7 on the others, virial 1e-5) on every radial kind (Gaussian, rational
 table, the generic analytic forms), every monomial count (D = 1, 4, 10, 20),
@@ -17,6 +18,7 @@ from tmd_testutil import GOLDEN, frac_wrap, read_data, rel_rms
 pytestmark = pytest.mark.gpu
 
 FORMS = TensorMDSystem.FORCE_VARIANTS
+DFORMS = TensorMDSystem.DESC_VARIANTS
 
 
 def _check(out, ref, n, e_tol, f_tol=1e-5):
@@ -32,12 +34,15 @@ def _forms(args, x, t, box, pbc=(1, 1, 1)):
     s.set_box(box, pbc)
     s.set_atoms(x, t)
     outs = {}
-    for v in FORMS:
-        s.set_force_variant(v)
-        assert s.force_variant() == v
-        outs[v] = s.compute(1, 1, 1.0)
-        again = s.compute(1, 1, 1.0)
-        assert np.array_equal(outs[v]["f"], again["f"]), v
+    for dv in DFORMS:
+        s.set_descriptor_variant(dv)
+        assert s.descriptor_variant() == dv
+        for v in FORMS:
+            s.set_force_variant(v)
+            assert s.force_variant() == v
+            outs[(dv, v)] = s.compute(1, 1, 1.0)
+            again = s.compute(1, 1, 1.0)
+            assert np.array_equal(outs[(dv, v)]["f"], again["f"]), (dv, v)
     return outs
 
 
@@ -82,9 +87,28 @@ def test_forms_on_benchmark_shape(fcc4k):
     p, syms, x, t, box = fcc4k
     outs = _forms(f"{p} {' '.join(syms)}", x, t, box)
     ref = Oracle(p).compute(x, t - 1, box, [1, 1, 1], skin=1.0)
+    first = outs[(DFORMS[0], FORMS[0])]
     for v, out in outs.items():
         _check(out, ref, len(x), 1e-7)
-        assert rel_rms(out["f"], outs[FORMS[0]]["f"]) <= 1e-6, v
+        assert rel_rms(out["f"], first["f"]) <= 1e-6, v
+
+
+def test_descriptor_forms_agree(fcc4k):
+    """Both descriptor forms give the same G = T P^2 rows to FP32 rounding."""
+    p, syms, x, t, box = fcc4k
+    m = TensorMDModel(f"{p} {' '.join(syms)}")
+    s = TensorMDSystem(m, len(x), 1.0)
+    s.set_box(box, [1, 1, 1])
+    s.set_atoms(x, t)
+    G = {}
+    for dv in DFORMS:
+        s.set_descriptor_variant(dv)
+        s.compute(1, 1, 1.0)
+        G[dv] = s.descriptors()
+    ref = Oracle(p).compute(x, t - 1, box, [1, 1, 1], skin=1.0, want_G=True)["G"]
+    for dv, g in G.items():
+        assert rel_rms(g, ref) <= 1e-6, (dv, rel_rms(g, ref))
+    assert rel_rms(G[DFORMS[1]], G[DFORMS[0]]) <= 1e-6
 
 
 @pytest.mark.parametrize("D,mm", [(1, 0), (4, 1), (10, 2)])
@@ -147,9 +171,11 @@ def test_forms_in_a_batch(tmp_path):
     b.set_atoms(np.concatenate([c[0] for c in cells]), np.concatenate([c[1] for c in cells]))
     sysv = b.system()
     res = {}
-    for v in FORMS:
-        sysv.set_force_variant(v)
-        res[v] = b.compute()
+    for dv in DFORMS:
+        sysv.set_descriptor_variant(dv)
+        for v in FORMS:
+            sysv.set_force_variant(v)
+            res[(dv, v)] = b.compute()
     off = 0
     for c, (x, t, box) in enumerate(cells):
         ref = Oracle(load_npz(p)).compute(x, t - 1, box, [1, 1, 1], skin=1.0)
@@ -168,6 +194,10 @@ def test_autotune_picks_the_fastest(fcc4k):
     s.set_atoms(x, t)
     ms = s.autotune(reps=3)
     assert set(ms) == set(FORMS) and all(v > 0 for v in ms.values())
+    assert s.force_variant() == min(ms, key=ms.get)
+    md = s.autotune(reps=3, family="descriptor")
+    assert set(md) == set(DFORMS) and all(v > 0 for v in md.values())
+    assert s.descriptor_variant() == min(md, key=md.get)
     assert s.force_variant() == min(ms, key=ms.get)
     out = s.compute(1, 1, 1.0)
     ref = Oracle(p).compute(x, t - 1, box, [1, 1, 1], skin=1.0)
