@@ -168,12 +168,13 @@ int alloc_neighbors(tmd_system *s, int cap) {
   drop_graph(s);
   cap = (cap + 31) / 32 * 32;
   if (cap > 4096) return fail(TMD_ERR_CAPACITY, "more than 4096 neighbors per atom");
-  dfree(s->tmp); dfree(s->nbr); dfree(s->rev); dfree(s->pdf);
+  dfree(s->tmp); dfree(s->nbr); dfree(s->rev); dfree(s->pdf); dfree(s->pgeo);
   size_t tot = (size_t)s->natoms_cap * cap;
   TMD_CUDA(dalloc(&s->tmp, tot));
   TMD_CUDA(dalloc(&s->nbr, tot));
   TMD_CUDA(dalloc(&s->rev, tot));
   TMD_CUDA(dalloc(&s->pdf, tot));
+  TMD_CUDA(dalloc(&s->pgeo, 2 * tot));
   s->cap = cap;
   s->capp = pow2_at_least(cap);
   return TMD_OK;
@@ -259,6 +260,7 @@ DescArgs desc_args(tmd_system *s, int variant) {
   d.elem = s->elem; d.nbr = s->nbr; d.boff = s->boff; d.P = s->P; d.G = s->G;
   d.cbox = s->ncells ? s->cbox : nullptr; d.acell = s->acell;
   d.variant = variant;
+  d.pdf = s->pdf; d.pgeo = s->pgeo; d.pcnt = s->pcnt;
   return d;
 }
 
@@ -271,9 +273,9 @@ int default_desc_variant(const tmd_model *m) {
 
 int default_force_variant(const tmd_model *m) {
   // measured on the B200 (tmd_system_autotune): whole pairs per lane beat 4
-  // filters per lane by 1.2-1.6x; 16 lanes per atom for one element block
-  // (~70 pairs per block), 8 when the pairs split over several blocks
-  return m->kp.B > 1 ? kForcePairLane8 : kForcePairLane16;
+  // filters per lane by 1.3-2x; 8 lanes per atom up to 16 filters, 16 lanes
+  // above (the per-atom dE/dP staging grows with K)
+  return m->kp.K <= 16 ? kForcePairLane8 : kForcePairLane16;
 }
 
 ForceArgs force_args(tmd_system *s, float scale, int variant) {
@@ -284,6 +286,7 @@ ForceArgs force_args(tmd_system *s, float scale, int variant) {
   fa.pdf = s->pdf; fa.wv = s->wv;
   fa.cbox = s->ncells ? s->cbox : nullptr; fa.acell = s->acell;
   fa.variant = variant;
+  fa.pgeo = s->pgeo; fa.pcnt = s->pcnt;
   return fa;
 }
 
@@ -846,7 +849,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   A(x, 3 * N); A(v, 3 * N); A(f, 3 * N); A(xbuild, 3 * N);
   A(image, 3 * N); A(elem, N);
   A(cell_of, N); A(cell_atoms, N);
-  A(nraw, N); A(boff, N * (h.nelt + 1));
+  A(nraw, N); A(boff, N * (h.nelt + 1)); A(pcnt, N * h.nelt);
   A(P, N * h.nelt * h.K * h.D); A(G, N * h.nin); A(dEdG, N * h.nin); A(E, N);
   A(wv, 6 * N); A(eatom, N); A(vatom, 6 * N); A(ke, N);
   A(partial, 1024 * 8); A(scal, 8);
@@ -876,6 +879,7 @@ void tmd_system_free(tmd_system *s) {
   dfree(s->cell_of); dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_cursor);
   dfree(s->cell_atoms); dfree(s->tmp); dfree(s->nbr); dfree(s->nraw); dfree(s->boff);
   dfree(s->rev); dfree(s->P); dfree(s->G); dfree(s->dEdG); dfree(s->E); dfree(s->pdf);
+  dfree(s->pgeo); dfree(s->pcnt);
   dfree(s->wv); dfree(s->eatom); dfree(s->vatom); dfree(s->ke); dfree(s->partial);
   dfree(s->scal); dfree(s->flag); dfree(s->status); dfree(s->perm);
   dfree(s->tiles); dfree(s->thermo_d);

@@ -148,13 +148,40 @@ struct PairRing {
   }
 };
 
+// Compact geometry of an active pair, written by the descriptor kernels for
+// the pair-lane force kernel (two float4: r, rlo, ux, uy | uz, fc, dfc, t for
+// analytic radial kinds; uz, tq, ti, t for the table), so that the force
+// kernel reads the active pairs instead of testing every list entry again.
+template <int RK>
+__device__ inline void store_pair_geo(const GeoSlot *s, float4 *__restrict__ dst) {
+  const float4 a = s->a, b = s->b, c = s->c;
+  dst[0] = a;
+  dst[1] = RK == kRadTable ? make_float4(b.x, b.w, c.x, c.y) : make_float4(b.x, b.y, b.z, c.y);
+}
+
+template <int RK>
+__device__ inline PairGeo load_pair_geo(const float4 *__restrict__ src, int &t) {
+  const float4 a = __ldg(src), b = __ldg(src + 1);
+  PairGeo g;
+  g.r = a.x; g.rlo = a.y; g.ux = a.z; g.uy = a.w; g.uz = b.x;
+  if (RK == kRadTable) {
+    g.tq = b.y; g.ti = __float_as_int(b.z); g.fc = g.dfc = 0.f;
+  } else {
+    g.fc = b.y; g.dfc = b.z; g.ti = 0; g.tq = 0.f;
+  }
+  t = __float_as_int(b.w);
+  g.rinv = __frcp_rn(g.r);  // 1/r rounded to nearest, as pair_geometry
+  return g;
+}
+
 template <int TPA, int D, int RK, bool MULTI>
 __global__ void __launch_bounds__(kPairThreads, 4)
 k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
              const int *__restrict__ elem, const uint32_t *__restrict__ nbr,
              const int *__restrict__ boff, float *__restrict__ P,
              float *__restrict__ G, const BoxP *__restrict__ cbox,
-             const int *__restrict__ acell) {
+             const int *__restrict__ acell, float4 *__restrict__ pdf,
+             float4 *__restrict__ pgeo, int *__restrict__ pcnt) {
   constexpr int D2 = (D + 1) / 2;
   __shared__ GeoSlot geo[2 * kPairThreads];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -175,9 +202,13 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
   const uint32_t *row = nbr + (size_t)a * cap;
   const int *bo = boff + (size_t)a * (B + 1);
   const unsigned live = live_lanes(gt, (long)n * TPA);
+  float4 *pdf_row = pdf + (size_t)a * cap;
+  float4 *pg_row = pgeo + (size_t)a * cap * 2;
+  int nact = 0;
   for (int b = 0; b < B; b++) {
     // keep the warp's groups on the same element block (see k_force)
     if (b > 0) __syncwarp(live);
+    const int nact0 = nact;
     float2 acc[4][D2];
 #pragma unroll
     for (int q = 0; q < 4; q++)
@@ -185,8 +216,10 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
       for (int p = 0; p < D2; p++) acc[q][p] = make_float2(0.f, 0.f);
     pr.begin(x, row, bo[b], bo[b + 1]);
     for (;;) {
-      const int cnt = pr.feed(kp, bx, xi, yi, zi, x, row, nullptr);
+      const int cnt = pr.feed(kp, bx, xi, yi, zi, x, row, pdf_row);
       if (cnt == 0) break;
+      if (sub < cnt) store_pair_geo<RK>(pr.slot(sub), pg_row + 2 * (nact + sub));
+      nact += cnt;
       for (int c = 0; c < cnt; c++) {
         const PairGeo g = geo_load(pr.slot(c));
         float H[4], dH[4];
@@ -202,6 +235,7 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
       }
       pr.pop(cnt);
     }
+    if (sub == 0) pcnt[(size_t)a * B + b] = nact - nact0;
     // P rows of this lane: 4 filters x D values, contiguous (G = T P^2 is
     // formed by k_invariants)
     float *Pp = P + (((size_t)a * B + b) * K + k0) * D;
@@ -233,7 +267,8 @@ __global__ void __launch_bounds__(kPairThreads, 6)
 k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
                const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
                float *__restrict__ P, const BoxP *__restrict__ cbox,
-               const int *__restrict__ acell) {
+               const int *__restrict__ acell, float4 *__restrict__ pdf,
+               float4 *__restrict__ pgeo, int *__restrict__ pcnt) {
   constexpr int D4 = (D + 3) / 4 * 4;
   constexpr int P2 = D4 / 2;
   __shared__ GeoSlot geo[2 * kPairThreads];
@@ -269,8 +304,12 @@ k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ 
     for (int v = 0; v < D4 / 4; v++)
       dst[v] = make_float4(M[4 * v], M[4 * v + 1], M[4 * v + 2], M[4 * v + 3]);
   };
+  float4 *pdf_row = pdf + (size_t)a * cap;
+  float4 *pg_row = pgeo + (size_t)a * cap * 2;
+  int nact = 0;
   for (int b = 0; b < B; b++) {
     if (b > 0) __syncwarp(live);
+    const int nact0 = nact;
     float2 acc[FPL][P2];
 #pragma unroll
     for (int f = 0; f < FPL; f++)
@@ -278,8 +317,10 @@ k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ 
       for (int p = 0; p < P2; p++) acc[f][p] = make_float2(0.f, 0.f);
     pr.begin(x, row, bo[b], bo[b + 1]);
     for (;;) {
-      const int cnt = pr.feed_with(kp, bx, xi, yi, zi, x, row, nullptr, keep_monomials);
+      const int cnt = pr.feed_with(kp, bx, xi, yi, zi, x, row, pdf_row, keep_monomials);
       if (cnt == 0) break;
+      if (sub < cnt) store_pair_geo<RK>(pr.slot(sub), pg_row + 2 * (nact + sub));
+      nact += cnt;
       for (int c = 0; c < cnt; c++) {
         const PairGeo g = geo_load(pr.slot(c));
         const float4 *ms = reinterpret_cast<const float4 *>(
@@ -303,6 +344,7 @@ k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ 
       }
       pr.pop(cnt);
     }
+    if (sub == 0) pcnt[(size_t)a * B + b] = nact - nact0;
     float *Pp = P + (((size_t)a * B + b) * K + kf) * D;
 #pragma unroll
     for (int f = 0; f < FPL; f++) {
@@ -324,7 +366,7 @@ void launch_descriptor_w(const DescArgs &a, cudaStream_t st) {
   const long threads = (long)a.n * W;
   int grid = (int)((threads + T - 1) / T);
   if (grid < 1) grid = 1;
-#define TMD_DESCW_ARGS a.kp, a.box, a.n, a.cap, a.x, a.nbr, a.boff, a.P, a.cbox, a.acell
+#define TMD_DESCW_ARGS a.kp, a.box, a.n, a.cap, a.x, a.nbr, a.boff, a.P, a.cbox, a.acell, a.pdf, a.pgeo, a.pcnt
   switch (a.kp.D) {
     case 1: k_descriptor_w<W, FPL, 1, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
     case 4: k_descriptor_w<W, FPL, 4, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
@@ -377,7 +419,7 @@ void launch_descriptor_tpa(const DescArgs &a, cudaStream_t st) {
   long threads = (long)a.n * TPA;
   int grid = (int)((threads + T - 1) / T);
   if (grid < 1) grid = 1;
-#define TMD_DESC_ARGS a.kp, a.box, a.n, a.cap, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.cbox, a.acell
+#define TMD_DESC_ARGS a.kp, a.box, a.n, a.cap, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.cbox, a.acell, a.pdf, a.pgeo, a.pcnt
   switch (a.kp.D) {
     case 1: k_descriptor<TPA, 1, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;
     case 4: k_descriptor<TPA, 4, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESC_ARGS); break;

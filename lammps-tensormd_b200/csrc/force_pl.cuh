@@ -13,9 +13,10 @@
 // one atom and each lane takes whole pairs: S of the current element block
 // (K x D floats) is staged once in shared memory and read by all lanes of the
 // group as broadcast vectors, and the monomials, grad Q and the force of a
-// pair are computed once.  Pairs are queued by the same PairRing as k_force
-// (W entries' geometry per step, active ones compacted in row order); lane c
-// of the group takes pair c of each chunk, so only the last chunk of a block
+// pair are computed once.  The pairs are the compact list of active pairs
+// that the descriptor step wrote (pgeo, pcnt: geometry computed once per
+// step, skin-shell entries already given a zero pair force); lane c of the
+// group takes pair c of each chunk of W, so only the last chunk of a block
 // leaves lanes idle.
 #pragma once
 
@@ -49,12 +50,12 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
            const float *__restrict__ P, const float *__restrict__ G,
            const float *__restrict__ dEdG, float4 *__restrict__ pdf,
            double *__restrict__ wv, const BoxP *__restrict__ cbox,
-           const int *__restrict__ acell) {
+           const int *__restrict__ acell, const float4 *__restrict__ pgeo,
+           const int *__restrict__ pcnt) {
   using L = PlLayout<D>;
   constexpr int D4 = L::D4;
   constexpr int P2 = D4 / 2;  // FP32 pairs per S row (pad columns hold 0)
   extern __shared__ float4 pl_dyn[];
-  __shared__ GeoSlot geo[2 * kPairThreads];
   const int K = kp.K, B = kp.B, M = kp.M;
   float *rp = reinterpret_cast<float *>(pl_dyn);
   float *Ts = rp + (RK == kRadTable ? 0 : 4 * K);  // T[m][d], rows of D4
@@ -77,24 +78,17 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
   if (a >= n) return;
   const unsigned live = live_lanes(gt, (long)n * W);
   const int lane = threadIdx.x & 31;
-  PairRing<W> pr;
-  pr.sub = sub;
-  pr.gshift = lane & ~(W - 1);
-  pr.gmask = PairRing<W>::kBits << pr.gshift;
-  pr.ring = geo + 2 * (threadIdx.x - sub);
-  const unsigned gmask = pr.gmask;
+  const unsigned gmask = PairRing<W>::kBits << (lane & ~(W - 1));
   float *Sg = rp + L::params(K, RK) + (threadIdx.x / W) * L::group(K);
   float *gpg = Sg + K * D4 + 4;  // dE/dG' rows [K][4]
-  const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
-  const double xi = x[3 * a], yi = x[3 * a + 1], zi = x[3 * a + 2];
-  const uint32_t *row = nbr + (size_t)a * cap;
-  const int *bo = boff + (size_t)a * (B + 1);
+  const float4 *pg_row = pgeo + (size_t)a * cap * 2;
   float4 *pdf_row = pdf + (size_t)a * cap;
   float w6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  int pos = 0;  // first active pair of the block in the compact list
   for (int b = 0; b < B; b++) {
     if (b > 0) __syncwarp(live);  // keep the warp's groups on the same block
-    const int s0 = bo[b], s1 = bo[b + 1];
-    if (s0 == s1) continue;
+    const int np = pcnt[(size_t)a * B + b];
+    if (np == 0) continue;
     // S = dE/dP of (atom, block) as [K][D4] rows: dE/dG' rows first, then
     // one element per lane step (same arithmetic and order as dedp_elem)
     __syncwarp(gmask);
@@ -146,14 +140,11 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
       }
     }
     __syncwarp(gmask);
-    pr.begin(x, row, s0, s1);
-    for (;;) {
-      const int cnt = pr.feed(kp, bx, xi, yi, zi, x, row, pdf_row);
-      if (cnt == 0) break;
-      if (sub < cnt) {
-        const GeoSlot *sl = pr.slot(sub);
-        const PairGeo g = geo_load(sl);
-        const int t = __float_as_int(sl->c.y);
+    for (int c0 = 0; c0 < np; c0 += W) {
+      const int c = c0 + sub;
+      if (c < np) {
+        int t;
+        const PairGeo g = load_pair_geo<RK>(pg_row + 2 * (pos + c), t);
         float2 V2[P2], W2[P2];
 #pragma unroll
         for (int p = 0; p < P2; p++) {
@@ -230,8 +221,8 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
         w6[4] -= rx * fz;
         w6[5] -= ry * fz;
       }
-      pr.pop(cnt);
     }
+    pos += np;
   }
   double w6d[6];
 #pragma unroll
@@ -247,12 +238,11 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
 }
 
 // Atom groups per block: as many as fit 128 threads and 48 KB of shared
-// memory (the static ring plus the dynamic parameters and S blocks).
+// memory (the dynamic parameters and S blocks).
 template <int D>
 inline int force_pl_groups(int W, int K, int rk) {
   const size_t per = sizeof(float) * (size_t)PlLayout<D>::group(K);
-  const size_t base = sizeof(float) * (size_t)PlLayout<D>::params(K, rk) +
-                      sizeof(GeoSlot) * 2 * kPairThreads;
+  const size_t base = sizeof(float) * (size_t)PlLayout<D>::params(K, rk);
   int g = kPairThreads / W;
   while (g > 1 && base + g * per > 48 * 1024) g--;
   return g;
@@ -260,7 +250,7 @@ inline int force_pl_groups(int W, int K, int rk) {
 
 template <int W, int RK, bool MULTI>
 void launch_force_pl_w(const ForceArgs &a, cudaStream_t st) {
-#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.dEdG, a.pdf, a.wv, a.cbox, a.acell
+#define TMD_FORCE_ARGS a.kp, a.box, a.n, a.cap, a.scale, a.x, a.elem, a.nbr, a.boff, a.P, a.G, a.dEdG, a.pdf, a.wv, a.cbox, a.acell, a.pgeo, a.pcnt
 #define TMD_PL_CASE(DV)                                                                     \
   case DV: {                                                                                \
     const int g = force_pl_groups<DV>(W, a.kp.K, RK);                         \

@@ -289,22 +289,21 @@ __device__ inline void moments(float x, float y, float z, float M[D]) {
 
 // Gradient of Q(u) = sum_d V_d M_d(u) with respect to u, and sum_d n_d V_d M_d
 // (n_d = rank of monomial d).  Then dQ/dx_j = (gradQ - u * nVM) / r, which
-// is sum_d V_d dM_d/dx_j (tensor_ops.cpp calculate_dM_{p,d,f}).
+// is sum_d V_d dM_d/dx_j (tensor_ops.cpp calculate_dM_{p,d,f}).  Each M_d is
+// homogeneous of degree n_d, so u . grad M_d = n_d M_d (Euler) and nVM is
+// formed as u . gradQ.
 template <int D>
 __device__ inline void poly_grad(const float V[D], float x, float y, float z,
                                  float gq[3], float &nvm) {
-  float gx = 0.f, gy = 0.f, gz = 0.f, s = 0.f;
+  float gx = 0.f, gy = 0.f, gz = 0.f;
   if (D > 1) {
     gx += V[1]; gy += V[2]; gz += V[3];
-    s += V[1] * x + V[2] * y + V[3] * z;
   }
   if (D > 4) {
     // xx, xy, xz, yy, yz, zz
     gx += 2.f * V[4] * x + V[5] * y + V[6] * z;
     gy += V[5] * x + 2.f * V[7] * y + V[8] * z;
     gz += V[6] * x + V[8] * y + 2.f * V[9] * z;
-    s += 2.f * (V[4] * x * x + V[5] * x * y + V[6] * x * z + V[7] * y * y +
-                V[8] * y * z + V[9] * z * z);
     if (D > 10) {
       float xx = x * x, xy = x * y, xz = x * z, yy = y * y, yz = y * z, zz = z * z;
       // xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
@@ -314,13 +313,10 @@ __device__ inline void poly_grad(const float V[D], float x, float y, float z,
             2.f * V[17] * yz + V[18] * zz;
       gz += V[12] * xx + V[14] * xy + 2.f * V[15] * xz + V[17] * yy +
             2.f * V[18] * yz + 3.f * V[19] * zz;
-      s += 3.f * (V[10] * xx * x + V[11] * xx * y + V[12] * xx * z + V[13] * xy * y +
-                  V[14] * xy * z + V[15] * xz * z + V[16] * yy * y + V[17] * yy * z +
-                  V[18] * yz * z + V[19] * zz * z);
     }
   }
   gq[0] = gx; gq[1] = gy; gq[2] = gz;
-  nvm = s;
+  nvm = x * gx + y * gy + z * gz;
 }
 
 }  // namespace tmd

@@ -65,6 +65,8 @@ struct tmd_system {
   float *P = nullptr, *G = nullptr, *dEdG = nullptr;
   double *E = nullptr;
   float4 *pdf = nullptr;
+  float4 *pgeo = nullptr;   // [natoms_cap][cap][2] active-pair geometry (descriptor step)
+  int *pcnt = nullptr;      // [natoms_cap][B] active pairs per (atom, element block)
   double *wv = nullptr, *eatom = nullptr, *vatom = nullptr, *ke = nullptr;
   double *partial = nullptr, *scal = nullptr;  // scal: [0] pe, [1..6] virial, [7] ke
   int *flag = nullptr, *status = nullptr;  // status[0] bits, status[1] longest row needed

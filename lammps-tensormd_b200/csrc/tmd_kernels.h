@@ -70,6 +70,12 @@ struct DescArgs {
   const BoxP *cbox;   // multi-cell mode: box of each cell, else nullptr
   const int *acell;   // multi-cell mode: cell of each atom
   int variant;        // kDesc*
+  // per-pair outputs for the force step: zero pair force of every list entry
+  // beyond rc (pdf[n][cap]), compact geometry of the active pairs
+  // (pgeo[n][cap][2], element block by element block) and their number per
+  // (atom, block) (pcnt[n][B])
+  float4 *pdf, *pgeo;
+  int *pcnt;
 };
 void launch_descriptor(const DescArgs &a, cudaStream_t st, long &launches);
 
@@ -169,6 +175,8 @@ struct ForceArgs {
   const BoxP *cbox;   // multi-cell mode (as DescArgs)
   const int *acell;
   int variant;        // kForce*
+  const float4 *pgeo;  // active pairs from the descriptor step (pair-lane forms)
+  const int *pcnt;
 };
 void launch_force(const ForceArgs &a, cudaStream_t st, long &launches);
 
