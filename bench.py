@@ -49,6 +49,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-bf16", action="store_true")
+    ap.add_argument("--profile-step", type=int, default=0, metavar="N",
+                    help="profiler target: set up the headline workload with the default "
+                         "kernel forms, run N force evaluations, print nothing else")
+    ap.add_argument("--main-only", action="store_true",
+                    help="only the headline workload (no precision forms, cells, serving, "
+                         "reference-workload or CPU lines): for profiler launch lists")
     ap.add_argument("--cells-steps", type=int, default=500,
                     help="NVE steps of the 4,096-cell batch line (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=2000.0,
@@ -149,32 +155,40 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(config):
-    """Per-launch DRAM bytes (read + write) of the force kernel, from the
-    committed ncu summary of the same workload (profiles/), or None."""
-    p = ROOT / "profiles" / f"force_descriptor_{config}.md"
+def ncu_traffic(config, kernel):
+    """Per-launch DRAM bytes (read + write) of a kernel, from the committed ncu
+    summary of the same workload (profiles/step_kernels_<config>.md, line
+    `traffic_bytes_per_launch <kernel>: N`), or None."""
+    p = ROOT / "profiles" / f"step_kernels_{config}.md"
     if not p.exists():
         return None
+    key = f"traffic_bytes_per_launch {kernel}:"
     for line in p.read_text().splitlines():
-        if "traffic_bytes_per_launch:" in line:
+        if key in line:
             try:
-                return int(line.split("traffic_bytes_per_launch:")[1].split()[0])
+                return int(line.split(key)[1].split()[0])
             except ValueError:
                 return None
     return None
 
 
-def algorithmic(cfg, npairs_rc, nlist, B, K, D, nin):
+def algorithmic(cfg, npairs_rc, nlist, B, K, D, nin, form):
     """Algorithmic FLOPs and HBM bytes per launch of the force kernel.
 
     FLOPs: the U and V contractions, 2 x (2 K D) per pair inside rc
-    (tensor_ops.cpp kernel_U / kernel_V).  Bytes: each input read once and
-    each output written once: x (24 B/atom), neighbor row (4 B/entry), P
-    (4 B K D B), G and dE/dG (2 x 4 nin), pair forces (16 B/entry), virial
-    partials (48 B/atom)."""
+    (tensor_ops.cpp kernel_U / kernel_V).  Bytes, each input read once and
+    each output written once: P (4 B K D B/atom), G and dE/dG (2 x 4 nin),
+    virial partials (48 B/atom), and per pair either (pair-lane forms) the
+    descriptor step's compact pair geometry (32 B per pair inside rc) and the
+    pair force (16 B), or (filter-lane form) x (24 B/atom), the neighbor row
+    (4 B/entry) and the pair force of every entry (16 B)."""
     n = cfg["natoms"]
     flops = 4.0 * K * D * npairs_rc
-    bytes_ = n * (24 + 4 * B * K * D + 8 * nin + 48) + nlist * (4 + 16)
+    per_atom = 4 * B * K * D + 8 * nin + 48
+    if form == "filter_lane":
+        bytes_ = n * (24 + per_atom) + nlist * (4 + 16)
+    else:
+        bytes_ = n * (per_atom + 4 * B) + npairs_rc * (32 + 16)
     return flops, bytes_
 
 
@@ -243,18 +257,19 @@ def run_ours(args, rank, world, local):
     npairs_rc = len(ent)
     nlist = len(sys_.neighbor_list(model.cutmax + 1.0)[1])
     B, K, D = model.nelt, model.num_filters, {1: 1, 2: 4, 3: 10, 4: 20}[model.mmax]
-    flops, abytes = algorithmic(cfg, npairs_rc, nlist, B, K, D, model.n_desc)
+    flops, abytes = algorithmic(cfg, npairs_rc, nlist, B, K, D, model.n_desc,
+                                sys_.force_variant())
     fcnt, fms = prof["force"]
     force_ms = fms / max(fcnt, 1)
     hbm_peak, peak_kind = measured_peaks()
     clocks = clk.summary()
     sm_mhz = clocks["sm_mhz"] or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
-    traffic = ncu_traffic(args.config)
-    ach_gbs = abytes / (force_ms / 1000.0) / 1e9
-    ach_tf = flops / (force_ms / 1000.0) / 1e12
     kname = {"filter_lane": "k_force", "pair_lane8": "k_force_pl<8>",
              "pair_lane16": "k_force_pl<16>", "pair_lane32": "k_force_pl<32>"}[sys_.force_variant()]
+    traffic = ncu_traffic(args.config, kname)
+    ach_gbs = abytes / (force_ms / 1000.0) / 1e9
+    ach_tf = flops / (force_ms / 1000.0) / 1e12
     roofline = {"kernel": kname, "bound": "hbm", "achieved": ach_gbs,
                 "peak": hbm_peak, "unit": "GB/s", "frac": ach_gbs / hbm_peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
@@ -313,7 +328,7 @@ def run_ours(args, rank, world, local):
     # tensor-core MLP forms of the same workload (same steps, same timing)
     forms = {"fp32": {"value": value, "ms_per_step": ms_max / args.steps,
                       "mlp_ms": prof["mlp"][1] / max(prof["mlp"][0], 1)}}
-    for prec in ([] if args.no_bf16 else ["bf16x3", "bf16"]):
+    for prec in ([] if (args.no_bf16 or args.main_only) else ["bf16x3", "bf16"]):
         try:
             mb = TensorMDModel(f"{pot} {' '.join(syms)} precision {prec}", device=local)
             sb = TensorMDSystem(mb, n, 1.0)
@@ -358,15 +373,15 @@ def run_ours(args, rank, world, local):
             forms[prec] = {"error": str(exc)}
 
     cells = None
-    if args.cells_steps > 0:
+    if args.cells_steps > 0 and not args.main_only:
         cells = run_cells(args, rank, world, local, dev, barrier)
     serving = None
-    if args.serve_window > 0:
+    if args.serve_window > 0 and not args.main_only:
         serving = run_serving(args, rank, local)
-    w23k = run_w23k(args, rank, world, local, dev, barrier)
+    w23k = None if args.main_only else run_w23k(args, rank, world, local, dev, barrier)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not (args.no_cpu_baseline or args.main_only):
         cpu = cpu_baseline(args.config, samples=2)
 
     if rank == 0:
@@ -634,9 +649,29 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def profile_step(args):
+    """A short, fixed launch sequence for ncu captures: the headline workload,
+    args.profile_step force evaluations (each: neighbor check, descriptor,
+    invariants, MLP, force, gather)."""
+    from tmd_b200 import TensorMDModel, TensorMDSystem
+    pot, syms, x, t, box, v, cfg = workload(args.config, seed=42)
+    model = TensorMDModel(f"{pot} {' '.join(syms)}")
+    s = TensorMDSystem(model, len(x), 1.0)
+    s.set_box(box)
+    s.set_atoms(x, t, v)
+    for _ in range(args.profile_step):
+        s.compute(1, 1, 1.0)
+    print(json.dumps({"profile_step": args.profile_step, "config": args.config,
+                      "force_form": s.force_variant(),
+                      "descriptor_form": s.descriptor_variant()}), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.profile_step > 0:
+        profile_step(args)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -25,8 +25,12 @@ void launch_descriptor(const DescArgs &a, cudaStream_t st, long &launches) {
       if (cells) launch_descriptor_generic_cells(a, st); else launch_descriptor_generic(a, st);
       break;
   }
-  launch_invariants(a, st);
-  launches += 2;
+  if (a.variant == kDescWide) {
+    launches += 1;  // G formed inside k_descriptor_w
+  } else {
+    launch_invariants(a, st);
+    launches += 2;
+  }
 }
 
 }  // namespace tmd

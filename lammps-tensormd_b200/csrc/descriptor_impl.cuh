@@ -261,15 +261,18 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
 // geometry also computes its D monomials once and keeps them beside the ring
 // slot; every lane then reads them as broadcast vectors and accumulates
 // P[k][d] for its own filters in the same order (pairs in row order, FP32
-// pairs over d) as k_descriptor.
+// pairs over d) as k_descriptor, then forms its filters' G rows from the P
+// rows it holds (no k_invariants pass).
 template <int W, int FPL, int D, int RK, bool MULTI>
 __global__ void __launch_bounds__(kPairThreads, 6)
 k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
                const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
-               float *__restrict__ P, const BoxP *__restrict__ cbox,
+               float *__restrict__ P, float *__restrict__ G,
+               const BoxP *__restrict__ cbox,
                const int *__restrict__ acell, float4 *__restrict__ pdf,
                float4 *__restrict__ pgeo, int *__restrict__ pcnt) {
   constexpr int D4 = (D + 3) / 4 * 4;
+  constexpr int M = D == 1 ? 1 : (D == 4 ? 2 : (D == 10 ? 3 : 4));
   constexpr int P2 = D4 / 2;
   __shared__ GeoSlot geo[2 * kPairThreads];
   __shared__ __align__(16) float mono[2 * kPairThreads * D4];
@@ -346,6 +349,7 @@ k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ 
     }
     if (sub == 0) pcnt[(size_t)a * B + b] = nact - nact0;
     float *Pp = P + (((size_t)a * B + b) * K + kf) * D;
+    float *Gp = G + (((size_t)a * B + b) * K + kf) * M;
 #pragma unroll
     for (int f = 0; f < FPL; f++) {
       if constexpr (D % 2 == 0) {
@@ -355,6 +359,18 @@ k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ 
       } else {
 #pragma unroll
         for (int d = 0; d < D; d++) Pp[f * D + d] = (d & 1) ? acc[f][d >> 1].y : acc[f][d >> 1].x;
+      }
+      // G row of the filter, in the order of k_invariants
+#pragma unroll
+      for (int m = 0; m < M; m++) {
+        float s = 0.f;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          const float pv = (d & 1) ? acc[f][d >> 1].y : acc[f][d >> 1].x;
+          s = fmaf(kp.T[m * D + d], pv * pv, s);
+        }
+        if (m == 0) s = copysignf(1.f, acc[f][0].x) * sqrtf(s);
+        Gp[f * M + m] = s;
       }
     }
   }
@@ -366,7 +382,7 @@ void launch_descriptor_w(const DescArgs &a, cudaStream_t st) {
   const long threads = (long)a.n * W;
   int grid = (int)((threads + T - 1) / T);
   if (grid < 1) grid = 1;
-#define TMD_DESCW_ARGS a.kp, a.box, a.n, a.cap, a.x, a.nbr, a.boff, a.P, a.cbox, a.acell, a.pdf, a.pgeo, a.pcnt
+#define TMD_DESCW_ARGS a.kp, a.box, a.n, a.cap, a.x, a.nbr, a.boff, a.P, a.G, a.cbox, a.acell, a.pdf, a.pgeo, a.pcnt
   switch (a.kp.D) {
     case 1: k_descriptor_w<W, FPL, 1, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
     case 4: k_descriptor_w<W, FPL, 4, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
