@@ -153,7 +153,8 @@ int tmd_get_descriptors(tmd_system *sys, double *G);
  * kernel.cu:1105, with G = T P^2):
  *   0  K/4 lanes per atom, 4 filters per lane
  *   1  min(K, 32) lanes per atom, K/min(K, 32) filters per lane, monomials of
- *      a pair computed once and shared through shared memory
+ *      a pair computed once and shared through shared memory, G formed in
+ *      the same kernel
  * The forms agree to FP32 rounding (summation order).  set_variant picks one;
  * autotune runs one evaluation, times reps launches of every form of the
  * family on the system's current atoms, keeps the fastest and recomputes the

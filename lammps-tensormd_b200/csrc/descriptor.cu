@@ -25,7 +25,7 @@ void launch_descriptor(const DescArgs &a, cudaStream_t st, long &launches) {
       if (cells) launch_descriptor_generic_cells(a, st); else launch_descriptor_generic(a, st);
       break;
   }
-  if (a.variant == kDescWide) {
+  if (a.variant != kDescFilter4) {
     launches += 1;  // G formed inside k_descriptor_w
   } else {
     launch_invariants(a, st);

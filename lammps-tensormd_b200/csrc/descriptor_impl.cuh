@@ -460,6 +460,7 @@ void launch_descriptor_rk(const DescArgs &a, cudaStream_t st) {
     }
     return;
   }
+
   switch (a.kp.K / 4) {
     case 1: launch_descriptor_tpa<1, RK, MULTI>(a, st); break;
     case 2: launch_descriptor_tpa<2, RK, MULTI>(a, st); break;

@@ -34,6 +34,7 @@ void launch_force(const ForceArgs &a, cudaStream_t st, long &launches) {
 // atom sums its own row and no two threads write the same force.  8 lanes
 // per atom.
 // ---------------------------------------------------------------------
+template <bool VATOM>
 __global__ void k_gather(int n, int cap, int B, const int *__restrict__ boff,
                          const float4 *__restrict__ pdf, const int *__restrict__ rev,
                          const uint32_t *__restrict__ nbr, const double *__restrict__ x,
@@ -49,14 +50,37 @@ __global__ void k_gather(int n, int cap, int B, const int *__restrict__ boff,
   double fx = 0, fy = 0, fz = 0;
   double v6[6] = {0, 0, 0, 0, 0, 0};
   const size_t base = (size_t)a * cap;
-  for (int t = sub; t < cnt; t += 8) {
+  int t0 = sub;
+  if (!VATOM) {
+    // four of the lane's entries per round: their rev slots and own pair
+    // forces, then the partners' pair forces, all in flight together; the
+    // sums run in the same order as the one-entry loop below
+    for (; t0 + 24 < cnt; t0 += 32) {
+      int rv[4];
+      float4 p[4], q[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        rv[u] = rev[base + t0 + 8 * u];
+        p[u] = pdf[base + t0 + 8 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) q[u] = rv[u] >= 0 ? pdf[rv[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        fx += (double)p[u].x - (double)q[u].x;
+        fy += (double)p[u].y - (double)q[u].y;
+        fz += (double)p[u].z - (double)q[u].z;
+      }
+    }
+  }
+  for (int t = t0; t < cnt; t += 8) {
     float4 p = pdf[base + t];
     int rv = rev[base + t];
     float4 q = rv >= 0 ? pdf[rv] : make_float4(0.f, 0.f, 0.f, 0.f);
     fx += (double)p.x - (double)q.x;
     fy += (double)p.y - (double)q.y;
     fz += (double)p.z - (double)q.z;
-    if (vatom) {
+    if (VATOM) {
       uint32_t e = nbr[base + t];
       int j = e & kAtomMask;
       int sx, sy, sz;
@@ -79,7 +103,7 @@ __global__ void k_gather(int n, int cap, int B, const int *__restrict__ boff,
     fy += __shfl_xor_sync(gmask, fy, o, 8);
     fz += __shfl_xor_sync(gmask, fz, o, 8);
   }
-  if (vatom) {
+  if (VATOM) {
 #pragma unroll
     for (int c = 0; c < 6; c++)
 #pragma unroll
@@ -89,7 +113,7 @@ __global__ void k_gather(int n, int cap, int B, const int *__restrict__ boff,
     f[3 * a] = fx;
     f[3 * a + 1] = fy;
     f[3 * a + 2] = fz;
-    if (vatom) {
+    if (VATOM) {
 #pragma unroll
       for (int c = 0; c < 6; c++) vatom[6 * a + c] = 0.5 * (wv[6 * a + c] + v6[c]);
     }
@@ -101,8 +125,12 @@ void launch_gather(const GatherArgs &a, cudaStream_t st, long &launches) {
   long threads = (long)a.n * 8;
   int grid = (int)((threads + T - 1) / T);
   if (grid < 1) grid = 1;
-  k_gather<<<grid, T, 0, st>>>(a.n, a.cap, a.B, a.boff, a.pdf, a.rev, a.nbr, a.x,
-                               a.box, a.wv, a.f, a.vatom, a.cbox, a.acell);
+  if (a.vatom)
+    k_gather<true><<<grid, T, 0, st>>>(a.n, a.cap, a.B, a.boff, a.pdf, a.rev, a.nbr, a.x,
+                                       a.box, a.wv, a.f, a.vatom, a.cbox, a.acell);
+  else
+    k_gather<false><<<grid, T, 0, st>>>(a.n, a.cap, a.B, a.boff, a.pdf, a.rev, a.nbr, a.x,
+                                        a.box, a.wv, a.f, a.vatom, a.cbox, a.acell);
   launches += 1;
 }
 
