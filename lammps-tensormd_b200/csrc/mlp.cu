@@ -434,11 +434,42 @@ k_mlp_fp32r(MlpArgs a) {
     }
     if (tid < TR) rows[tid] = tid < count ? a.perm[start + tid] : -1;
     __syncthreads();
-    // G tile, transposed
-    for (int idx = tid; idx < TR * nin; idx += NT) {
-      const int r = idx / nin, k = idx - r * nin;
-      const int at = rows[r];
-      act0[(size_t)k * LDT + r] = at >= 0 ? __ldg(a.G + (size_t)at * nin + k) : 0.f;
+    // G tile, transposed.  The whole CTA waits on these loads, so with rows
+    // a multiple of 4 wide they go as float4, four per thread in flight, a
+    // warp covering 32 rows of one column quad (conflict-free stores)
+    if ((nin & 3) == 0) {
+      const int nq = nin >> 2, total = TR * nq;
+      for (int base = tid; base < total; base += 4 * NT) {
+        float4 gv[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int idx = base + u * NT;
+          gv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (idx < total) {
+            const int q = idx / TR, r = idx - q * TR;
+            const int at = rows[r];
+            if (at >= 0) gv[u] = __ldg(reinterpret_cast<const float4 *>(a.G + (size_t)at * nin) + q);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int idx = base + u * NT;
+          if (idx < total) {
+            const int q = idx / TR, r = idx - q * TR;
+            float *dst = act0 + (size_t)(4 * q) * LDT + r;
+            dst[0] = gv[u].x;
+            dst[LDT] = gv[u].y;
+            dst[2 * LDT] = gv[u].z;
+            dst[3 * LDT] = gv[u].w;
+          }
+        }
+      }
+    } else {
+      for (int idx = tid; idx < TR * nin; idx += NT) {
+        const int r = idx / nin, k = idx - r * nin;
+        const int at = rows[r];
+        act0[(size_t)k * LDT + r] = at >= 0 ? __ldg(a.G + (size_t)at * nin + k) : 0.f;
+      }
     }
     __syncthreads();
     float *in = act0, *out = act1;
