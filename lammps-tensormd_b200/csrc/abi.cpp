@@ -581,6 +581,7 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
       continue;
     }
     if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
+    if (st & kStatusLaunch) return fail(TMD_ERR_CUDA, "neighbor build launched without its shared memory");
     if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
     if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite force during the run");
     s0 = s1 + 1;
@@ -1018,6 +1019,7 @@ int tmd_compute(tmd_system *s, int eflag, int vflag, double scale, double *energ
     return tmd_compute(s, eflag, vflag, scale, energy, virial, f, eatom, vatom);
   }
   if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
+  if (st & kStatusLaunch) return fail(TMD_ERR_CUDA, "neighbor build launched without its shared memory");
   if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
   if (st & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside a non-periodic boundary");
   if (energy) *energy = s->h_scal[0];

@@ -202,6 +202,7 @@ int tmd_batch_compute(tmd_batch *b, double *energy, double *virial, double *f) {
     return tmd_batch_compute(b, energy, virial, f);
   }
   if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
+  if (st & kStatusLaunch) return fail(TMD_ERR_CUDA, "neighbor build launched without its shared memory");
   if (st & kStatusShift) return fail(TMD_ERR_ARG, "a cell is too small for the cutoff");
   if (st & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside a non-periodic boundary");
   for (int c = 0; c < C; c++) {

@@ -189,8 +189,16 @@ __device__ inline double rsq_nofma(double dx, double dy, double dz) {
                    __dmul_rn(dz, dz));
 }
 
-// One warp per atom; lanes walk stencil cells, two passes (count, write)
-// give a deterministic order.
+// One warp per atom; lanes walk stencil cells.  Each lane keeps the passing
+// candidates of its cell (up to kNbKeep) in shared memory while it counts
+// them, then writes them at its prefix position: the order is deterministic
+// (lane order, then cell order) and the distances are computed once; a cell
+// with more passing candidates than that is walked a second time.
+constexpr int kNbKeep = 16;
+constexpr int kNbKeepStride = kNbKeep + 1;  // odd stride: lanes in distinct banks
+
+// Dynamic shared memory a launch of k_nb_build with `threads` threads needs.
+size_t nb_build_smem(int threads) { return sizeof(uint32_t) * (size_t)threads * kNbKeepStride; }
 __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
                            BinP bin, const int *__restrict__ cell_of,
                            const int *__restrict__ cell_start,
@@ -199,7 +207,19 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
                            int *__restrict__ nraw, int *status, int *maxneed,
                            const int *flag) {
   if (!*flag) return;
+  extern __shared__ uint32_t nb_keep[];
+  {
+    // a launch without the keep buffers (nb_build_smem) would write past the
+    // dynamic shared memory: refuse with a status bit instead
+    uint32_t dyn;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    if (dyn < sizeof(uint32_t) * blockDim.x * kNbKeepStride) {
+      if (threadIdx.x == 0) atomicOr(status, kStatusLaunch);
+      return;
+    }
+  }
   const int lane = threadIdx.x & 31;
+  uint32_t *keep = nb_keep + (size_t)threadIdx.x * kNbKeepStride;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
   const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
@@ -239,6 +259,7 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
       a1 = cell_start[c + 1];
     }
     const bool self_cell = (sh[0] == 0 && sh[1] == 0 && sh[2] == 0);
+    const int code = shift_code(sh[0], sh[1], sh[2]);
     for (int p = a0; p < a1; p++) {
       int j = cell_atoms[p];
       if (j == i && self_cell) continue;
@@ -246,7 +267,10 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
       image_of(box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sh[0], sh[1], sh[2],
                gx, gy, gz);
       double r2 = rsq_nofma(xi - gx, yi - gy, zi - gz);
-      if (r2 <= cutsq) cnt++;
+      if (r2 <= cutsq) {
+        if (cnt < kNbKeep) keep[cnt] = nb_pack(j, code);
+        cnt++;
+      }
     }
     int incl = cnt;
     for (int o = 1; o < 32; o <<= 1) {
@@ -255,8 +279,10 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
     }
     int total = __shfl_sync(0xffffffffu, incl, 31);
     int pos = out + incl - cnt;
-    if (cnt > 0) {
-      int code = shift_code(sh[0], sh[1], sh[2]);
+    if (cnt > 0 && cnt <= kNbKeep) {
+      for (int q = 0; q < cnt; q++)
+        if (pos + q < cap) row[pos + q] = keep[q];
+    } else if (cnt > kNbKeep) {
       for (int p = a0; p < a1; p++) {
         int j = cell_atoms[p];
         if (j == i && self_cell) continue;
@@ -424,6 +450,81 @@ __global__ void k_nb_sort(int n, int B, KParams kp, const int *__restrict__ elem
   }
 }
 
+// The same sort for rows of up to 32*NQ entries, keys in registers: element
+// e = q*32 + lane of the row is key q of the lane.  Network stages with a
+// stride of 32 or more compare two keys of one lane; smaller strides compare
+// with the partner lane through a shuffle (the lower element keeps the
+// minimum of an ascending pair).  Same network as k_nb_sort, so the same
+// order.
+template <int NQ>
+__global__ void k_nb_sort_reg(int n, int B, KParams kp, const int *__restrict__ elem,
+                              int cap, const uint32_t *__restrict__ tmp,
+                              const int *__restrict__ nraw, uint32_t *__restrict__ nbr,
+                              int *__restrict__ boff, const int *flag) {
+  if (!*flag) return;
+  constexpr int CAPP = 32 * NQ;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+    const int cnt = min(nraw[i], cap);
+    const int ei = elem[i];
+    const uint32_t *row = tmp + (size_t)i * cap;
+    unsigned long long v[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      const int t = q * 32 + lane;
+      v[q] = ~0ull;
+      if (t < cnt) {
+        const uint32_t e = row[t];
+        const int b = kp.eltij[ei * kMaxElt + elem[e & kAtomMask]];
+        v[q] = ((unsigned long long)b << 32) | e;
+      }
+    }
+#pragma unroll
+    for (int k = 2; k <= CAPP; k <<= 1) {
+#pragma unroll
+      for (int jj = k >> 1; jj > 0; jj >>= 1) {
+        if (jj >= 32) {
+#pragma unroll
+          for (int q = 0; q < NQ; q++) {
+            const int p = q ^ (jj >> 5);
+            if (p > q) {
+              const bool up = ((q * 32) & k) == 0;
+              const unsigned long long a = v[q], c = v[p];
+              if ((a > c) == up) { v[q] = c; v[p] = a; }
+            }
+          }
+        } else {
+          const bool lower = (lane & jj) == 0;
+#pragma unroll
+          for (int q = 0; q < NQ; q++) {
+            const unsigned long long o = __shfl_xor_sync(0xffffffffu, v[q], jj);
+            const bool up = ((q * 32 + lane) & k) == 0;
+            const unsigned long long lo = v[q] < o ? v[q] : o, hi = v[q] < o ? o : v[q];
+            v[q] = (lower == up) ? lo : hi;
+          }
+        }
+      }
+    }
+    uint32_t *orow = nbr + (size_t)i * cap;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      const int t = q * 32 + lane;
+      if (t < cnt) orow[t] = (uint32_t)(v[q] & 0xffffffffu);
+    }
+    for (int b = 0; b <= B; b++) {
+      int c = 0;
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        const int t = q * 32 + lane;
+        c += (t < cnt && (int)(v[q] >> 32) < b) ? 1 : 0;
+      }
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if (lane == 0) boff[(size_t)i * (B + 1) + b] = c;
+    }
+  }
+}
+
 // Partner slot of every entry: (j -> i, -shift) found by binary search in the
 // sorted block of atom j.
 __global__ void k_nb_rev(int n, int B, KParams kp, const int *__restrict__ elem,
@@ -496,15 +597,28 @@ void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
                                   a.cell_cursor, a.flag);
     k_nb_fill<<<gn, T, 0, st>>>(a.n, a.cell_of, a.cell_cursor, a.cell_atoms, a.flag);
     k_nb_cellsort<<<gc, T, 0, st>>>(a.bin.ncell, a.cell_start, a.cell_atoms, a.flag);
-    k_nb_build<<<gw, T, 0, st>>>(a.n, a.x, a.box, a.bin, a.cell_of, a.cell_start,
-                                 a.cell_atoms, a.cutsq, a.cap, a.tmp, a.nraw,
-                                 a.status, a.maxneed, a.flag);
+    k_nb_build<<<gw, T, nb_build_smem(T), st>>>(
+        a.n, a.x, a.box, a.bin, a.cell_of, a.cell_start, a.cell_atoms, a.cutsq, a.cap,
+        a.tmp, a.nraw, a.status, a.maxneed, a.flag);
     launches += 6;
   }
-  int wpb = a.capp >= 1024 ? 1 : (a.capp >= 512 ? 2 : 4);
-  size_t smem = (size_t)wpb * a.capp * sizeof(unsigned long long);
-  k_nb_sort<<<cap_grid((a.n + wpb - 1) / wpb), 32 * wpb, smem, st>>>(
-      a.n, a.B, a.kp, a.elem, a.cap, a.capp, a.tmp, a.nraw, a.nbr, a.boff, a.flag);
+  if (a.capp <= 256) {
+#define TMD_SORT_REG(NQ)                                                                  \
+  k_nb_sort_reg<NQ><<<gw, T, 0, st>>>(a.n, a.B, a.kp, a.elem, a.cap, a.tmp, a.nraw, a.nbr, \
+                                      a.boff, a.flag)
+    switch (a.capp) {
+      case 32: TMD_SORT_REG(1); break;
+      case 64: TMD_SORT_REG(2); break;
+      case 128: TMD_SORT_REG(4); break;
+      default: TMD_SORT_REG(8); break;
+    }
+#undef TMD_SORT_REG
+  } else {
+    int wpb = a.capp >= 1024 ? 1 : (a.capp >= 512 ? 2 : 4);
+    size_t smem = (size_t)wpb * a.capp * sizeof(unsigned long long);
+    k_nb_sort<<<cap_grid((a.n + wpb - 1) / wpb), 32 * wpb, smem, st>>>(
+        a.n, a.B, a.kp, a.elem, a.cap, a.capp, a.tmp, a.nraw, a.nbr, a.boff, a.flag);
+  }
   k_nb_rev<<<gw, T, 0, st>>>(a.n, a.B, a.kp, a.elem, a.cap, a.nbr, a.boff, a.rev,
                              a.flag);
   k_nb_finish<<<gn, T, 0, st>>>(a.n, a.x, a.xbuild, a.flag);

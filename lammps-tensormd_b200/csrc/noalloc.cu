@@ -42,6 +42,7 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box, BinP b
                            uint32_t *__restrict__ tmp, int *__restrict__ nraw, int *status,
                            int *maxneed, const int *flag);
 __global__ void k_set_flag(int *flag);
+size_t nb_build_smem(int threads);
 void set_last_error(const std::string &msg);
 
 namespace {
@@ -178,7 +179,7 @@ extern "C" int tmd_neighbor_list_noalloc(const double *x_dev, int n, const doubl
   k_nb_scan<<<1, 1024, 0, st>>>(bin.ncell, cell_count, cell_start, cell_cursor, flag);
   k_nb_fill<<<grid((n + T - 1) / T), T, 0, st>>>(n, cell_of, cell_cursor, cell_atoms, flag);
   k_nb_cellsort<<<grid((bin.ncell + T - 1) / T), T, 0, st>>>(bin.ncell, cell_start, cell_atoms, flag);
-  k_nb_build<<<grid(((long)n * 32 + T - 1) / T), T, 0, st>>>(
+  k_nb_build<<<grid(((long)n * 32 + T - 1) / T), T, nb_build_smem(T), st>>>(
       n, x_dev, b, bin, cell_of, cell_start, cell_atoms, cut * cut, cap,
       reinterpret_cast<uint32_t *>(rows_dev), counts_dev, status, maxneed, flag);
   e = cudaGetLastError();
@@ -188,6 +189,7 @@ extern "C" int tmd_neighbor_list_noalloc(const double *x_dev, int n, const doubl
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return fail(TMD_ERR_CUDA, std::string("status read: ") + cudaGetErrorString(e));
   if (h[0] & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside the periodic cell (wrap positions first)");
+  if (h[0] & kStatusLaunch) return fail(TMD_ERR_CUDA, "neighbor build launched without its shared memory");
   if (h[0] & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
   if (h[0] & kStatusOverflow)
     return fail(TMD_ERR_CAPACITY, "a row needs " + std::to_string(h[2]) + " entries, cap is " +

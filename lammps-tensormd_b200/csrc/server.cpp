@@ -201,6 +201,7 @@ int read_cells(tmd_server *sv) {
   const int st = s->h_status[0];
   if (st & kStatusOverflow) return fail(TMD_ERR_CAPACITY, "neighbor list overflow");
   if (st & kStatusTimeout) return fail(TMD_ERR_TIMEOUT, "a tensor-core wait timed out");
+  if (st & kStatusLaunch) return fail(TMD_ERR_CUDA, "neighbor build launched without its shared memory");
   if (st & kStatusShift) return fail(TMD_ERR_ARG, "a cell is too small for the cutoff");
   return TMD_OK;
 }

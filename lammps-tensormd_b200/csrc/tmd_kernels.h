@@ -11,6 +11,7 @@ constexpr int kStatusShift = 2;      // image shift beyond +-3 cells
 constexpr int kStatusOutside = 4;    // atom outside a non-periodic boundary
 constexpr int kStatusNonfinite = 8;  // NaN/Inf energy or force
 constexpr int kStatusTimeout = 16;   // a bounded device wait gave up
+constexpr int kStatusLaunch = 32;    // a kernel launched without its shared memory
 
 // Per-cell constants of the multi-cell neighbor build: perpendicular widths
 // and the largest image shift per axis (0 on non-periodic axes).
