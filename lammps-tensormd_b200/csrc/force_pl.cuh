@@ -67,8 +67,8 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
     for (int i = threadIdx.x; i < K; i += blockDim.x) {
       rp[i] = RK == kRadGauss ? kp.p1[i] : kp.p0[i];
       rp[K + i] = RK == kRadGauss ? kp.p1lo[i] : kp.p1[i];
-      rp[2 * K + i] = RK == kRadGauss ? kp.gc[i] : kp.p2[i];
-      rp[3 * K + i] = RK == kRadGauss ? kp.gcl[i] : 0.f;
+      rp[2 * K + i] = RK == kRadGauss ? -2.f * kp.gc[i] : kp.p2[i];
+      rp[3 * K + i] = RK == kRadGauss ? -kp.gcl[i] : 0.f;
     }
   }
   __syncthreads();

@@ -122,7 +122,9 @@ inline int radial_kind(const KParams &kp) {
   return kp.method == 3 ? kRadGauss : kRadGeneric;
 }
 
-// Radial parameters of a lane's 4 filters, loaded once per kernel.
+// Radial parameters of a lane's 4 filters, loaded once per kernel.  For the
+// Gaussian kind gc holds -2 gc and gl holds -gcl (signs and the factor 2
+// applied once at load, exactly).
 template <int RK>
 struct Radial4 {
   float a[RK == kRadGeneric ? 4 : 1], b[RK == kRadTable ? 1 : 4],
@@ -144,8 +146,8 @@ __device__ inline Radial4<RK> load_radial4(const KParams &kp, int k0) {
     if (RK != kRadTable) R.b[t] = kp.p1[k0 + t];
     if (RK == kRadGauss) {
       R.blo[t] = kp.p1lo[k0 + t];
-      R.gc[t] = kp.gc[k0 + t];
-      R.gl[t] = kp.gcl[k0 + t];
+      R.gc[t] = -2.f * kp.gc[k0 + t];
+      R.gl[t] = -kp.gcl[k0 + t];
     }
   }
   return R;
@@ -192,8 +194,8 @@ __device__ inline void radial4(const KParams &kp, const Radial4<RK> &R, const Pa
       // (r - omega) from the hi/lo pairs of both: no systematic rounding of
       // the Gaussian centre
       float d = (r - R.b[t]) + (g.rlo - R.blo[t]);
-      f = exp2f(-R.gl[t] * d * d);
-      df = -2.f * R.gc[t] * d * f;
+      f = exp2f(R.gl[t] * d * d);
+      df = R.gc[t] * d * f;
     } else {
       const float a = R.a[t], b = R.b[t], c = R.c[t];
       if (kp.method == 0) {
@@ -295,25 +297,34 @@ __device__ inline void moments(float x, float y, float z, float M[D]) {
 template <int D>
 __device__ inline void poly_grad(const float V[D], float x, float y, float z,
                                  float gq[3], float &nvm) {
+  // Horner form: grad_a Q = V_a + x P_a + y Q_a + z R_a, with P, Q, R the
+  // coefficients of x, y, z once the linear terms are taken out (three short
+  // independent chains instead of one long sum per component)
   float gx = 0.f, gy = 0.f, gz = 0.f;
   if (D > 1) {
-    gx += V[1]; gy += V[2]; gz += V[3];
-  }
-  if (D > 4) {
-    // xx, xy, xz, yy, yz, zz
-    gx += 2.f * V[4] * x + V[5] * y + V[6] * z;
-    gy += V[5] * x + 2.f * V[7] * y + V[8] * z;
-    gz += V[6] * x + V[8] * y + 2.f * V[9] * z;
-    if (D > 10) {
-      float xx = x * x, xy = x * y, xz = x * z, yy = y * y, yz = y * z, zz = z * z;
-      // xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
-      gx += 3.f * V[10] * xx + 2.f * V[11] * xy + 2.f * V[12] * xz + V[13] * yy +
-            V[14] * yz + V[15] * zz;
-      gy += V[11] * xx + 2.f * V[13] * xy + V[14] * xz + 3.f * V[16] * yy +
-            2.f * V[17] * yz + V[18] * zz;
-      gz += V[12] * xx + V[14] * xy + 2.f * V[15] * xz + V[17] * yy +
-            2.f * V[18] * yz + 3.f * V[19] * zz;
+    float Px = 0.f, Qx = 0.f, Rx = 0.f, Py = 0.f, Qy = 0.f, Ry = 0.f, Pz = 0.f, Qz = 0.f,
+          Rz = 0.f;
+    if (D > 4) {
+      // xx, xy, xz, yy, yz, zz
+      Px = 2.f * V[4]; Qx = V[5]; Rx = V[6];
+      Py = V[5]; Qy = 2.f * V[7]; Ry = V[8];
+      Pz = V[6]; Qz = V[8]; Rz = 2.f * V[9];
+      if (D > 10) {
+        // xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
+        Px = fmaf(3.f * V[10], x, fmaf(2.f * V[11], y, fmaf(2.f * V[12], z, Px)));
+        Qx = fmaf(V[13], y, fmaf(V[14], z, Qx));
+        Rx = fmaf(V[15], z, Rx);
+        Py = fmaf(V[11], x, fmaf(2.f * V[13], y, fmaf(V[14], z, Py)));
+        Qy = fmaf(3.f * V[16], y, fmaf(2.f * V[17], z, Qy));
+        Ry = fmaf(V[18], z, Ry);
+        Pz = fmaf(V[12], x, fmaf(V[14], y, fmaf(2.f * V[15], z, Pz)));
+        Qz = fmaf(V[17], y, fmaf(2.f * V[18], z, Qz));
+        Rz = fmaf(3.f * V[19], z, Rz);
+      }
     }
+    gx = fmaf(x, Px, fmaf(y, Qx, fmaf(z, Rx, V[1])));
+    gy = fmaf(x, Py, fmaf(y, Qy, fmaf(z, Ry, V[2])));
+    gz = fmaf(x, Pz, fmaf(y, Qz, fmaf(z, Rz, V[3])));
   }
   gq[0] = gx; gq[1] = gy; gq[2] = gz;
   nvm = x * gx + y * gy + z * gz;
