@@ -311,6 +311,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
     ta.G = s->G; ta.dEdG = s->dEdG; ta.E = s->E; ta.layers = m->d_tc_layers;
     ta.status = s->status; ta.smem = m->tc_smem; ta.dz_bf16 = m->tc_dz_bf16 ? 1 : 0;
     ta.np = m->tc_np;
+    ta.persistent = m->tc_persistent; ta.smem_p = m->tc_smem_p;
     if (m->tc_fp8) launch_mlp_fp8(ta, s->st, s->launches);
     else launch_mlp_tc(ta, s->st, s->launches);
   } else {
@@ -790,6 +791,18 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     }
     if (fp8) mlp_fp8_prepare(m->tc_smem, m->tc_dz_bf16);
     else mlp_tc_prepare(m->tc_smem, m->tc_dz_bf16, np);
+    // weight-resident persistent form when the hidden weights, one tile's
+    // operands and act' fit in shared memory (next to ~3 KB of static data)
+    if (!fp8) {
+      const size_t sp = mlp_tcp_smem(h.nl, h.sizes.data(), h.resnet, np);
+      int nsm = 0;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+      if (sp > 0 && sp <= 227 * 1024 - 3 * 1024 && nsm > 0) {
+        m->tc_persistent = nsm;
+        m->tc_smem_p = sp;
+        mlp_tcp_prepare(sp, np);
+      }
+    }
     m->mlp_tr = 128;
   }
   *out = m;

@@ -276,6 +276,22 @@ __host__ __device__ inline ResLayout res_layout(int nl, const int *sizes, int tr
   return r;
 }
 
+// RT consecutive floats of one k-row of a transposed tile (16-byte aligned
+// for RT >= 4).
+template <int RT>
+__device__ inline void load_rows(const float *src, float v[RT]) {
+  if constexpr (RT % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < RT / 4; q++) {
+      const float4 t = reinterpret_cast<const float4 *>(src)[q];
+      v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+    }
+  } else {
+    const float2 t = *reinterpret_cast<const float2 *>(src);
+    v[0] = t.x; v[1 % RT] = t.y;
+  }
+}
+
 // Forward: out(r, c) = sum_k inT[k][r] W[k][c] for c < N, r < TR.
 template <int TR, int NT, class Epi>
 __device__ inline void res_gemm_fwd(const float *inT, int Kd, const float *W, int ldw, int N,
@@ -297,13 +313,7 @@ __device__ inline void res_gemm_fwd(const float *inT, int Kd, const float *W, in
     for (int k = 0; k < Kd; k++) {
       const float4 w = *reinterpret_cast<const float4 *>(wp + k * ldw);
       float xv[RT];
-      if (RT == 4) {
-        const float4 t = *reinterpret_cast<const float4 *>(xp + k * LDT);
-        xv[0] = t.x; xv[1] = t.y; xv[2 % RT] = t.z; xv[3 % RT] = t.w;
-      } else {
-        const float2 t = *reinterpret_cast<const float2 *>(xp + k * LDT);
-        xv[0] = t.x; xv[1 % RT] = t.y;
-      }
+      load_rows<RT>(xp + k * LDT, xv);
 #pragma unroll
       for (int i = 0; i < RT; i++) {
         acc[i][0] = fmaf(xv[i], w.x, acc[i][0]);
@@ -351,15 +361,7 @@ __device__ inline void res_gemm_bwd(const float *gzT, int Nc, const float *W, in
         wj[j] = kv[j] ? *reinterpret_cast<const float4 *>(wr[j] + c) : make_float4(0.f, 0.f, 0.f, 0.f);
       float g[4][RT];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        if (RT == 4) {
-          const float4 t = *reinterpret_cast<const float4 *>(gp + (c + q) * LDT);
-          g[q][0] = t.x; g[q][1] = t.y; g[q][2 % RT] = t.z; g[q][3 % RT] = t.w;
-        } else {
-          const float2 t = *reinterpret_cast<const float2 *>(gp + (c + q) * LDT);
-          g[q][0] = t.x; g[q][1 % RT] = t.y;
-        }
-      }
+      for (int q = 0; q < 4; q++) load_rows<RT>(gp + (c + q) * LDT, g[q]);
 #pragma unroll
       for (int i = 0; i < RT; i++)
 #pragma unroll

@@ -270,6 +270,277 @@ k_mlp_tc(MlpTcArgs a) {
                  "r"(TMEM_COLS));
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form for MLPs whose packed hidden weights fit in shared memory
+// next to one tile's operand and act' buffers (no residual layers).  One CTA
+// of 256 threads per SM walks the tiles (sorted by element) with a grid
+// stride; the element's packed W^T and W blocks (hi, and lo for the split
+// form) stay in shared memory until the element changes, so the GEMMs read
+// only shared memory.  Thread t owns tile row 32 (w % 4) + lane (its TMEM
+// lane) and, with warp w / 4, one half of every 64-column group of the
+// accumulator: two threads share a row's epilogue.  Operands are written as
+// whole 16-byte core rows, act' column-major ([layer][column][row]) so a
+// warp's stores are contiguous.  MMAs, commit and the bounded waits are as in
+// k_mlp_tc.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kTcpThreads = 256;
+
+// 8 consecutive values as one 16-byte core row of BF16 (and the lo residuals)
+template <int NP>
+__device__ inline void put_core_row(__nv_bfloat16 *buf, size_t lo_stride, int off,
+                                    const float *v) {
+  uint4 hi, lo;
+  uint32_t *h = reinterpret_cast<uint32_t *>(&hi), *l = reinterpret_cast<uint32_t *>(&lo);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const __nv_bfloat162 hb = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+    h[q] = *reinterpret_cast<const uint32_t *>(&hb);
+    if (NP == 3) {
+      const __nv_bfloat162 lb = __floats2bfloat162_rn(v[2 * q] - __low2float(hb),
+                                                      v[2 * q + 1] - __high2float(hb));
+      l[q] = *reinterpret_cast<const uint32_t *>(&lb);
+    }
+  }
+  *reinterpret_cast<uint4 *>(buf + off) = hi;
+  if (NP == 3) *reinterpret_cast<uint4 *>(buf + lo_stride + off) = lo;
+}
+
+// Elements of the resident weight blocks of one element's hidden layers.
+__host__ __device__ inline size_t tcp_weight_elems(int nl, const int *sizes, int nb) {
+  size_t w = 0;
+  for (int l = 0; l < nl - 1; l++) w += 2 * (size_t)nb * sizes[l] * sizes[l + 1];
+  return w;
+}
+}  // namespace
+
+template <int NP>
+__global__ void __launch_bounds__(kTcpThreads, 1)
+k_mlp_tcp(MlpTcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int rows_s[TM];
+  __shared__ double epart[2][TM];
+  typedef __nv_bfloat16 T;
+  constexpr int NB = NP == 3 ? 2 : 1;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quad = warp & 3, half = warp >> 2;
+  const int row = quad * 32 + lane;
+  const int L = a.nl, nin = a.nin, maxh = a.maxh;
+  const int maxw = nin > maxh ? nin : maxh;
+  int sizes[kMaxLayers + 1];
+  sizes[0] = nin;
+  for (int l = 0; l < L; l++) sizes[l + 1] = a.layers[l].N;
+  T *wsm = reinterpret_cast<T *>(smraw);
+  T *actb = wsm + tcp_weight_elems(L, sizes, NB);
+  const size_t act_lo = (size_t)TM * maxw;
+  float *dzb = reinterpret_cast<float *>(actb + NB * act_lo);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16);
+  uint32_t phase = 0;
+  bool ok = true;
+
+  // D[TM x nout] = A[TM x kred] . B^T; A = actb laid out with kfull columns,
+  // B rows n0..n0+nout-1 of a resident packed block of brows rows (hi, then
+  // lo bsize elements later).
+  auto gemm = [&](int kfull, int kred, const T *B, int brows, int n0, int nout) {
+    const size_t bsize = (size_t)brows * kred;
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t id = idesc_bf16(nout);
+      const uint64_t a_lo = (uint64_t)((act_lo * 2) >> 4);
+      const uint64_t b_lo = (uint64_t)((bsize * 2) >> 4);
+      for (int c = 0; c < kred / KCH; c++) {
+#pragma unroll
+        for (int s = 0; s < KCH / KSTEP; s++) {
+          const uint64_t da = sdesc(smem_u32(actb) + (uint32_t)((c * KCH + s * KSTEP) / EPC) * 128u,
+                                    128u, (uint32_t)(kfull / EPC) * 128u);
+          const uint64_t db = sdesc(smem_u32(B + ((size_t)c * brows + n0) * KCH) +
+                                        (uint32_t)(s * KSTEP / EPC) * 128u,
+                                    128u, (uint32_t)(KCH / EPC) * 128u);
+          mma_bf16(tmem, da, db, id, (c > 0 || s > 0) ? 1u : 0u);
+          if (NP == 3) {
+            mma_bf16(tmem, da, db + b_lo, id, 1u);  // hi * lo'
+            mma_bf16(tmem, da + a_lo, db, id, 1u);  // lo * hi'
+          }
+        }
+      }
+      commit(&mbar);
+    }
+    const bool done = mbar_wait(&mbar, phase);
+    ok = __syncthreads_and(done ? 1 : 0) != 0;
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+  };
+  // operand writes visible to the tensor core, TMEM reads done, then barrier
+  auto publish = [&]() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+  };
+
+  int cur_elt = -1;
+  for (int tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x) {
+    const int elt = a.tiles[3 * tile], start = a.tiles[3 * tile + 1],
+              count = a.tiles[3 * tile + 2];
+    const MlpTcLayer *Ls = a.layers + (size_t)elt * L;
+    __syncthreads();  // the previous tile is done with every buffer
+    if (elt != cur_elt) {
+      cur_elt = elt;
+      T *w = wsm;
+      for (int l = 0; l < L - 1; l++) {
+        const size_t nblk = (size_t)NB * sizes[l] * sizes[l + 1];  // elements per direction
+        for (int dir = 0; dir < 2; dir++) {
+          const uint4 *src = reinterpret_cast<const uint4 *>(dir == 0 ? Ls[l].Wf : Ls[l].Wb);
+          uint4 *dst = reinterpret_cast<uint4 *>(w);
+          const int nvec = (int)(nblk * sizeof(T) / 16);
+          for (int i = tid; i < nvec; i += kTcpThreads) dst[i] = __ldg(src + i);
+          w += nblk;
+        }
+      }
+    }
+    if (tid < TM) rows_s[tid] = tid < count ? a.perm[start + tid] : -1;
+    __syncthreads();
+    // G tile as BF16 operand (kfull = nin), one 16-byte core row per step
+    {
+      const int nq = nin / 8;
+      for (int idx = tid; idx < TM * nq; idx += kTcpThreads) {
+        const int r = idx / nq, k8 = idx - r * nq;
+        const int at = rows_s[r];
+        float v[8];
+        if (at >= 0) {
+          const float4 *g = reinterpret_cast<const float4 *>(a.G + (size_t)at * nin + 8 * k8);
+          const float4 p = __ldg(g), q = __ldg(g + 1);
+          v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w;
+          v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 8; j++) v[j] = 0.f;
+        }
+        put_core_row<NP>(actb, act_lo, core_off(r, 8 * k8, nin), v);
+      }
+    }
+    publish();
+    const int row_atom = rows_s[row];
+
+    // ---------------- forward ----------------
+    double E = 0.0;
+    const T *wl = wsm;
+    for (int l = 0; l < L - 1 && ok; l++) {
+      const MlpTcLayer ly = Ls[l];
+      const int K = sizes[l], N = sizes[l + 1];
+      gemm(l == 0 ? nin : maxh, K, wl, N, 0, N);
+      wl += 2 * (size_t)NB * K * N;
+      if (!ok) break;
+      const bool last = (l == L - 2);
+      const double *wout = Ls[L - 1].wd;
+      float *dz = dzb + (size_t)l * maxh * TM;
+      for (int c0 = 32 * half; c0 < N; c0 += 64) {
+        float v[32];
+        tmem_ld32(trow + c0, v);
+#pragma unroll 4
+        for (int j = 0; j < 32; j++) {
+          const int c = c0 + j;
+          const float z = v[j] + __ldg(ly.b + c);
+          float d;
+          const float y = act_fwd(a.actfn, z, d);
+          if (!last) {
+            dz[(size_t)c * TM + row] = d;
+            v[j] = y;
+          } else {
+            // output layer in FP64; gradient seed g = w_out, gz = g * act'
+            const double w = __ldg(wout + c);
+            E = fma((double)y, w, E);
+            v[j] = (float)w * d;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) put_core_row<NP>(actb, act_lo, core_off(row, c0 + 8 * q, maxh), v + 8 * q);
+      }
+      publish();
+    }
+    if (!ok) break;
+    epart[half][row] = E;
+    __syncthreads();
+    if (half == 0 && row_atom >= 0)
+      a.E[row_atom] = (epart[0][row] + epart[1][row]) + (Ls[L - 1].bd ? *Ls[L - 1].bd : 0.0);
+
+    // ---------------- backward ----------------
+    for (int l = L - 2; l >= 0 && ok; l--) {
+      size_t woff = 0;
+      for (int q = 0; q < l; q++) woff += 2 * (size_t)NB * sizes[q] * sizes[q + 1];
+      const int K = sizes[l], N = sizes[l + 1];
+      const T *wb = wsm + woff + (size_t)NB * K * N;  // W block after the W^T block
+      if (l == 0) {
+        for (int n0 = 0; n0 < K && ok; n0 += 128) {
+          const int nout = min(128, K - n0);
+          gemm(maxh, N, wb, K, n0, nout);
+          if (!ok) break;
+          for (int c0 = 32 * half; c0 < nout; c0 += 64) {
+            float v[32];
+            tmem_ld32(trow + c0, v);
+            if (row_atom >= 0) {
+              float4 *dst = reinterpret_cast<float4 *>(a.dEdG + (size_t)row_atom * nin + n0 + c0);
+#pragma unroll
+              for (int j = 0; j < 8; j++)
+                dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+            }
+          }
+          asm volatile("tcgen05.fence::before_thread_sync;");
+          __syncthreads();
+        }
+      } else {
+        gemm(maxh, N, wb, K, 0, K);
+        if (!ok) break;
+        const float *dzn = dzb + (size_t)(l - 1) * maxh * TM;
+        for (int c0 = 32 * half; c0 < K; c0 += 64) {
+          float v[32];
+          tmem_ld32(trow + c0, v);
+#pragma unroll
+          for (int j = 0; j < 32; j++) v[j] *= dzn[(size_t)(c0 + j) * TM + row];
+#pragma unroll
+          for (int q = 0; q < 4; q++) put_core_row<NP>(actb, act_lo, core_off(row, c0 + 8 * q, maxh), v + 8 * q);
+        }
+        publish();
+      }
+    }
+  }
+  if (!ok && tid == 0) atomicOr(a.status, kStatusTimeout);
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS));
+}
+
+size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np) {
+  if (resnet || nl < 2) return 0;
+  const size_t nb = np == 3 ? 2 : 1;
+  int maxh = 1;
+  for (int l = 1; l < nl; l++) maxh = maxh > sizes[l] ? maxh : sizes[l];
+  const int maxw = sizes[0] > maxh ? sizes[0] : maxh;
+  size_t b = tcp_weight_elems(nl, sizes, (int)nb) * 2;  // resident W^T and W blocks
+  b += nb * (size_t)TM * maxw * 2;                      // operand buffer
+  b += (size_t)(nl - 1) * maxh * TM * 4;                // act' (FP32)
+  return b;
+}
+
 void pack_core_chunks(const float *src, int rows, int cols, long ld_r, long ld_k,
                       uint16_t *dst) {
   // chunk c holds columns [64c, 64c + 64) of every row; inside a chunk the
@@ -310,8 +581,21 @@ void mlp_tc_prepare(size_t smem, bool dz_bf16, int np) {
   }
 }
 
+void mlp_tcp_prepare(size_t smem, int np) {
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (np == 3) cudaFuncSetAttribute(k_mlp_tcp<3>, at, (int)smem);
+  else cudaFuncSetAttribute(k_mlp_tcp<1>, at, (int)smem);
+}
+
 void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches) {
   if (a.ntiles <= 0) return;
+  if (a.persistent > 0) {
+    const int grid = a.ntiles < a.persistent ? a.ntiles : a.persistent;
+    if (a.np == 3) k_mlp_tcp<3><<<grid, kTcpThreads, a.smem_p, st>>>(a);
+    else k_mlp_tcp<1><<<grid, kTcpThreads, a.smem_p, st>>>(a);
+    launches += 1;
+    return;
+  }
   if (a.np == 3) {
     if (a.dz_bf16) k_mlp_tc<__nv_bfloat16, 3><<<a.ntiles, TM, a.smem, st>>>(a);
     else k_mlp_tc<float, 3><<<a.ntiles, TM, a.smem, st>>>(a);
