@@ -51,6 +51,26 @@ __device__ inline PairGeo geo_load(const GeoSlot *s) {
   return g;
 }
 
+// The fields of a slot that the radial basis reads (r, r_lo, f_c for the
+// analytic kinds; interval and offset for the table).
+template <int RK>
+__device__ inline PairGeo geo_load_radial(const GeoSlot *s) {
+  PairGeo g;
+  g.ux = g.uy = g.uz = g.dfc = g.rinv = 0.f;
+  if (RK == kRadTable) {
+    g.r = g.rlo = g.fc = 0.f;
+    g.tq = s->b.w;
+    g.ti = __float_as_int(s->c.x);
+  } else {
+    const float2 rr = *reinterpret_cast<const float2 *>(&s->a);
+    g.r = rr.x; g.rlo = rr.y;
+    g.fc = s->b.y;
+    g.tq = 0.f;
+    g.ti = 0;
+  }
+  return g;
+}
+
 // Lanes of thread gt's warp whose global thread index is below nthreads
 // (threads past the last atom return at kernel entry).
 __device__ inline unsigned live_lanes(int gt, long nthreads) {
@@ -324,8 +344,9 @@ k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ 
       if (cnt == 0) break;
       if (sub < cnt) store_pair_geo<RK>(pr.slot(sub), pg_row + 2 * (nact + sub));
       nact += cnt;
+#pragma unroll 2
       for (int c = 0; c < cnt; c++) {
-        const PairGeo g = geo_load(pr.slot(c));
+        const PairGeo g = geo_load_radial<RK>(pr.slot(c));
         const float4 *ms = reinterpret_cast<const float4 *>(
             mr + ((pr.head + c) & (PairRing<W>::kSlots - 1)) * D4);
         float2 h2[FPL];
