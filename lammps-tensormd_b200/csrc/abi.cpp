@@ -213,6 +213,7 @@ NbArgs nb_args(tmd_system *s) {
   a.xbuild = s->xbuild; a.flag = s->flag; a.status = s->status; a.maxneed = s->status + 1;
   a.ncells = s->ncells; a.cbox = s->cbox; a.cgeom = s->cgeom; a.acell = s->acell;
   a.coff = s->coff;
+  a.cflag = s->ncells ? s->cflag : nullptr;
   return a;
 }
 
@@ -495,7 +496,8 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
     prof_begin(s);
     if (nvt) launch_nhc_half(G, s->nhc, nullptr, n, acell, s->v, s->st, s->launches);
     launch_nve_initial(n, s->x, s->v, s->f, s->elem, s->m->d_mass, dtf, dt, s->st, s->launches);
-    launch_neighbor_check(n, s->x, s->xbuild, trigsq, s->flag, s->st, s->launches);
+    launch_neighbor_check(n, s->x, s->xbuild, trigsq, s->flag, s->st, s->launches, s->acell,
+                          s->ncells ? s->cflag : nullptr);
     prof_end(s, 5);
     prof_begin(s);
     launch_neighbor_build(nb_args(s), s->st, s->launches);
@@ -898,6 +900,7 @@ void tmd_system_free(tmd_system *s) {
   dfree(s->scal); dfree(s->flag); dfree(s->status); dfree(s->perm);
   dfree(s->tiles); dfree(s->thermo_d);
   dfree(s->cbox); dfree(s->cgeom); dfree(s->acell); dfree(s->coff); dfree(s->cell_out);
+  dfree(s->cflag);
   dfree(s->nhc); dfree(s->nhc_ke);
   dfree(s->ck_x); dfree(s->ck_v); dfree(s->ck_f); dfree(s->ck_img); dfree(s->ck_nhc);
   if (s->h_scal) cudaFreeHost(s->h_scal);
@@ -979,7 +982,8 @@ int tmd_system_set_positions(tmd_system *s, const double *x) {
   TMD_CUDA(cudaMemcpyAsync(s->x, x, 3 * s->n * sizeof(double), cudaMemcpyHostToDevice, s->st));
   s->forces_valid = false;
   double half = 0.5 * s->skin;
-  launch_neighbor_check(s->n, s->x, s->xbuild, half * half, s->flag, s->st, s->launches);
+  launch_neighbor_check(s->n, s->x, s->xbuild, half * half, s->flag, s->st, s->launches,
+                        s->acell, s->ncells ? s->cflag : nullptr);
   launch_neighbor_build(nb_args(s), s->st, s->launches);
   return TMD_OK;
 }

@@ -30,6 +30,8 @@ int cells_alloc(tmd_system *s, int max_cells) {
   if (e == cudaSuccess) e = dalloc(&s->acell, s->natoms_cap);
   if (e == cudaSuccess) e = dalloc(&s->coff, max_cells + 1);
   if (e == cudaSuccess) e = dalloc(&s->cell_out, 8 * (size_t)max_cells);
+  if (e == cudaSuccess) e = dalloc(&s->cflag, max_cells);
+  if (e == cudaSuccess) e = cudaMemset(s->cflag, 0, sizeof(int) * (size_t)max_cells);
   if (e != cudaSuccess)
     return fail(TMD_ERR_CUDA, std::string("batch allocation: ") + cudaGetErrorString(e));
   s->max_cells = max_cells;

@@ -37,6 +37,35 @@ __global__ void k_nb_check(int n, const double *__restrict__ x,
   if (rsq > trigsq) atomicOr(flag, 1);
 }
 
+// Multi-cell mode rebuilds only the cells whose atoms moved (cflag[c] set by
+// k_nbc_check), as separate systems would; bit 2 of the flag (a forced
+// rebuild) rebuilds every cell.  Single-box mode passes cflag = nullptr.
+__device__ inline bool nb_rebuild(const int *flag, const int *__restrict__ cflag,
+                                  const int *__restrict__ acell, int i) {
+  return cflag == nullptr || (*flag & 2) || cflag[acell[i]];
+}
+
+__global__ void k_nbc_check(int n, const double *__restrict__ x,
+                            const double *__restrict__ xbuild, double trigsq,
+                            const int *__restrict__ acell, int *__restrict__ cflag, int *flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double dx = x[3 * i] - xbuild[3 * i];
+  double dy = x[3 * i + 1] - xbuild[3 * i + 1];
+  double dz = x[3 * i + 2] - xbuild[3 * i + 2];
+  double rsq = dx * dx + dy * dy + dz * dz;
+  if (rsq > trigsq) {
+    cflag[acell[i]] = 1;
+    atomicOr(flag, 1);
+  }
+}
+
+__global__ void k_nbc_clear(int ncells, int *__restrict__ cflag, const int *flag) {
+  if (!*flag) return;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x)
+    cflag[c] = 0;
+}
+
 __device__ inline void frac_of(const BoxP &b, double px, double py, double pz,
                                double &fx, double &fy, double &fz) {
   double dx = px - b.lo[0], dy = py - b.lo[1], dz = pz - b.lo[2];
@@ -322,10 +351,11 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
 // ---------------------------------------------------------------------
 __global__ void k_nbc_wrap(int n, double *__restrict__ x, int *__restrict__ image,
                            const BoxP *__restrict__ cbox, const int *__restrict__ acell,
-                           int *status, const int *flag) {
+                           const int *__restrict__ cflag, int *status, const int *flag) {
   if (!*flag) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
+    if (!nb_rebuild(flag, cflag, acell, i)) continue;
     const BoxP &box = cbox[acell[i]];
     double px, py, pz, f[3];
     wrap_atom(box, i, x, image, px, py, pz);
@@ -342,11 +372,12 @@ __global__ void k_nbc_build(int n, const double *__restrict__ x,
                             const int *__restrict__ acell, const int *__restrict__ coff,
                             double cut, double cutsq, int cap, uint32_t *__restrict__ tmp,
                             int *__restrict__ nraw, int *status, int *maxneed,
-                            const int *flag) {
+                            const int *__restrict__ cflag, const int *flag) {
   if (!*flag) return;
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+    if (!nb_rebuild(flag, cflag, acell, i)) continue;
     const int c = acell[i];
     const BoxP &box = cbox[c];
     const CellGeom &cg = cgeom[c];
@@ -401,12 +432,14 @@ __global__ void k_nb_sort(int n, int B, KParams kp, const int *__restrict__ elem
                           int cap, int capp, const uint32_t *__restrict__ tmp,
                           const int *__restrict__ nraw,
                           uint32_t *__restrict__ nbr, int *__restrict__ boff,
+                          const int *__restrict__ acell, const int *__restrict__ cflag,
                           const int *flag) {
   if (!*flag) return;
   extern __shared__ unsigned long long sbuf[];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   for (int i = blockIdx.x * wpb + wib; i < n; i += gridDim.x * wpb) {
+  if (!nb_rebuild(flag, cflag, acell, i)) continue;
   unsigned long long *s = sbuf + (size_t)wib * capp;
   __syncwarp();
   int cnt = min(nraw[i], cap);
@@ -460,12 +493,14 @@ template <int NQ>
 __global__ void k_nb_sort_reg(int n, int B, KParams kp, const int *__restrict__ elem,
                               int cap, const uint32_t *__restrict__ tmp,
                               const int *__restrict__ nraw, uint32_t *__restrict__ nbr,
-                              int *__restrict__ boff, const int *flag) {
+                              int *__restrict__ boff, const int *__restrict__ acell,
+                              const int *__restrict__ cflag, const int *flag) {
   if (!*flag) return;
   constexpr int CAPP = 32 * NQ;
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+    if (!nb_rebuild(flag, cflag, acell, i)) continue;
     const int cnt = min(nraw[i], cap);
     const int ei = elem[i];
     const uint32_t *row = tmp + (size_t)i * cap;
@@ -530,11 +565,13 @@ __global__ void k_nb_sort_reg(int n, int B, KParams kp, const int *__restrict__ 
 __global__ void k_nb_rev(int n, int B, KParams kp, const int *__restrict__ elem,
                          int cap, const uint32_t *__restrict__ nbr,
                          const int *__restrict__ boff, int *__restrict__ rev,
+                         const int *__restrict__ acell, const int *__restrict__ cflag,
                          const int *flag) {
   if (!*flag) return;
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+  if (!nb_rebuild(flag, cflag, acell, i)) continue;
   int cnt = boff[(size_t)i * (B + 1) + B];
   int ei = elem[i];
   for (int t = lane; t < cnt; t += 32) {
@@ -558,10 +595,12 @@ __global__ void k_nb_rev(int n, int B, KParams kp, const int *__restrict__ elem,
 }
 
 __global__ void k_nb_finish(int n, const double *__restrict__ x,
-                            double *__restrict__ xbuild, int *flag) {
+                            double *__restrict__ xbuild, const int *__restrict__ acell,
+                            const int *__restrict__ cflag, int *flag) {
   if (!*flag) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
+    if (!nb_rebuild(flag, cflag, acell, i)) continue;
     xbuild[3 * i] = x[3 * i];
     xbuild[3 * i + 1] = x[3 * i + 1];
     xbuild[3 * i + 2] = x[3 * i + 2];
@@ -570,7 +609,7 @@ __global__ void k_nb_finish(int n, const double *__restrict__ x,
 
 __global__ void k_nb_clear(int *flag) { *flag = 0; }
 
-__global__ void k_set_flag(int *flag) { *flag = 1; }
+__global__ void k_set_flag(int *flag) { *flag = 3; }  // rebuild, every cell
 
 // Host driver: the whole rebuild sequence on `st`.  All launches are
 // conditional on *flag; `launches` counts them.
@@ -583,10 +622,11 @@ void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
   int gn = cap_grid((a.n + T - 1) / T);
   int gw = cap_grid(((long)a.n * 32 + T - 1) / T);
   if (a.ncells > 0) {
-    k_nbc_wrap<<<gn, T, 0, st>>>(a.n, a.x, a.image, a.cbox, a.acell, a.status, a.flag);
+    k_nbc_wrap<<<gn, T, 0, st>>>(a.n, a.x, a.image, a.cbox, a.acell, a.cflag, a.status,
+                                 a.flag);
     k_nbc_build<<<gw, T, 0, st>>>(a.n, a.x, a.cbox, a.cgeom, a.acell, a.coff,
                                   std::sqrt(a.cutsq), a.cutsq, a.cap, a.tmp, a.nraw,
-                                  a.status, a.maxneed, a.flag);
+                                  a.status, a.maxneed, a.cflag, a.flag);
     launches += 2;
   } else {
     int gc = cap_grid((a.bin.ncell + T - 1) / T);
@@ -605,7 +645,7 @@ void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
   if (a.capp <= 256) {
 #define TMD_SORT_REG(NQ)                                                                  \
   k_nb_sort_reg<NQ><<<gw, T, 0, st>>>(a.n, a.B, a.kp, a.elem, a.cap, a.tmp, a.nraw, a.nbr, \
-                                      a.boff, a.flag)
+                                      a.boff, a.acell, a.cflag, a.flag)
     switch (a.capp) {
       case 32: TMD_SORT_REG(1); break;
       case 64: TMD_SORT_REG(2); break;
@@ -617,20 +657,28 @@ void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
     int wpb = a.capp >= 1024 ? 1 : (a.capp >= 512 ? 2 : 4);
     size_t smem = (size_t)wpb * a.capp * sizeof(unsigned long long);
     k_nb_sort<<<cap_grid((a.n + wpb - 1) / wpb), 32 * wpb, smem, st>>>(
-        a.n, a.B, a.kp, a.elem, a.cap, a.capp, a.tmp, a.nraw, a.nbr, a.boff, a.flag);
+        a.n, a.B, a.kp, a.elem, a.cap, a.capp, a.tmp, a.nraw, a.nbr, a.boff, a.acell, a.cflag,
+        a.flag);
   }
-  k_nb_rev<<<gw, T, 0, st>>>(a.n, a.B, a.kp, a.elem, a.cap, a.nbr, a.boff, a.rev,
-                             a.flag);
-  k_nb_finish<<<gn, T, 0, st>>>(a.n, a.x, a.xbuild, a.flag);
+  k_nb_rev<<<gw, T, 0, st>>>(a.n, a.B, a.kp, a.elem, a.cap, a.nbr, a.boff, a.rev, a.acell,
+                             a.cflag, a.flag);
+  k_nb_finish<<<gn, T, 0, st>>>(a.n, a.x, a.xbuild, a.acell, a.cflag, a.flag);
+  if (a.cflag) {
+    k_nbc_clear<<<cap_grid((a.ncells + T - 1) / T), T, 0, st>>>(a.ncells, a.cflag, a.flag);
+    launches += 1;
+  }
   k_nb_clear<<<1, 1, 0, st>>>(a.flag);
   launches += 4;
 }
 
 void launch_neighbor_check(int n, const double *x, const double *xbuild,
                            double trigsq, int *flag, cudaStream_t st,
-                           long &launches) {
+                           long &launches, const int *acell, int *cflag) {
   const int T = 256;
-  k_nb_check<<<(n + T - 1) / T, T, 0, st>>>(n, x, xbuild, trigsq, flag);
+  if (cflag)
+    k_nbc_check<<<(n + T - 1) / T, T, 0, st>>>(n, x, xbuild, trigsq, acell, cflag, flag);
+  else
+    k_nb_check<<<(n + T - 1) / T, T, 0, st>>>(n, x, xbuild, trigsq, flag);
   launches += 1;
 }
 

@@ -316,7 +316,8 @@ int tick(tmd_server *sv) {
   for (int k = 0; k < sv->steps_per_tick; k++) {
     launch_srv_pre(s->n, s->ncells, s->acell, s->coff, sv->ctl, s->x, s->v, s->f, s->elem,
                    s->m->d_mass, sv->pw, sv->csum, s->st, s->launches);
-    launch_neighbor_check(s->n, s->x, s->xbuild, half * half, s->flag, s->st, s->launches);
+    launch_neighbor_check(s->n, s->x, s->xbuild, half * half, s->flag, s->st, s->launches,
+                          s->acell, s->cflag);
     launch_neighbor_build(nb_args(s), s->st, s->launches);
     launch_force_eval(s, 1.0f, false);
     launch_srv_post(s->n, s->ncells, s->acell, s->coff, sv->ctl, s->v, s->f, s->elem,

@@ -57,6 +57,7 @@ struct tmd_system {
   tmd::CellGeom *cgeom = nullptr;
   int *acell = nullptr, *coff = nullptr;
   double *cell_out = nullptr;  // [ncells][8]: energy, virial[6], spare
+  int *cflag = nullptr;        // [max_cells] cells whose list must be rebuilt
   // device state
   double *x = nullptr, *v = nullptr, *f = nullptr, *xbuild = nullptr;
   int *image = nullptr, *elem = nullptr;

@@ -44,12 +44,15 @@ struct NbArgs {
   int *rev;
   double *xbuild;
   int *flag, *status, *maxneed;
+  int *cflag;  // multi-cell mode: cells to rebuild (k_nbc_check), else nullptr
 };
 
 void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches);
+// Displacement check: sets flag when an atom moved more than sqrt(trigsq)
+// since the last build; in multi-cell mode (cflag) also marks the atom's cell.
 void launch_neighbor_check(int n, const double *x, const double *xbuild,
                            double trigsq, int *flag, cudaStream_t st,
-                           long &launches);
+                           long &launches, const int *acell = nullptr, int *cflag = nullptr);
 void launch_set_flag(int *flag, cudaStream_t st, long &launches);
 
 // Descriptor: P[n][B][K][D], G[n][B*K*M].
