@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--profile-step", type=int, default=0, metavar="N",
                     help="profiler target: set up the headline workload with the default "
                          "kernel forms, run N force evaluations, print nothing else")
+    ap.add_argument("--profile-precision", default="fp32", choices=["fp32", "bf16x3", "bf16"],
+                    help="MLP precision form of the --profile-step target")
     ap.add_argument("--main-only", action="store_true",
                     help="only the headline workload (no precision forms, cells, serving, "
                          "reference-workload or CPU lines): for profiler launch lists")
@@ -660,13 +662,15 @@ def profile_step(args):
     invariants, MLP, force, gather)."""
     from tmd_b200 import TensorMDModel, TensorMDSystem
     pot, syms, x, t, box, v, cfg = workload(args.config, seed=42)
-    model = TensorMDModel(f"{pot} {' '.join(syms)}")
+    prec = "" if args.profile_precision == "fp32" else f" precision {args.profile_precision}"
+    model = TensorMDModel(f"{pot} {' '.join(syms)}{prec}")
     s = TensorMDSystem(model, len(x), 1.0)
     s.set_box(box)
     s.set_atoms(x, t, v)
     for _ in range(args.profile_step):
         s.compute(1, 1, 1.0)
     print(json.dumps({"profile_step": args.profile_step, "config": args.config,
+                      "precision": args.profile_precision,
                       "force_form": s.force_variant(),
                       "descriptor_form": s.descriptor_variant()}), flush=True)
 

@@ -286,25 +286,29 @@ k_mlp_tc(MlpTcArgs a) {
 namespace {
 constexpr int kTcpThreads = 256;
 
-// 8 consecutive values as one 16-byte core row of BF16 (and the lo residuals)
-template <int NP>
-__device__ inline void put_core_row(__nv_bfloat16 *buf, size_t lo_stride, int off,
-                                    const float *v) {
-  uint4 hi, lo;
-  uint32_t *h = reinterpret_cast<uint32_t *>(&hi), *l = reinterpret_cast<uint32_t *>(&lo);
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const __nv_bfloat162 hb = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
-    h[q] = *reinterpret_cast<const uint32_t *>(&hb);
-    if (NP == 3) {
-      const __nv_bfloat162 lb = __floats2bfloat162_rn(v[2 * q] - __low2float(hb),
-                                                      v[2 * q + 1] - __high2float(hb));
-      l[q] = *reinterpret_cast<const uint32_t *>(&lb);
-    }
-  }
-  *reinterpret_cast<uint4 *>(buf + off) = hi;
-  if (NP == 3) *reinterpret_cast<uint4 *>(buf + lo_stride + off) = lo;
+// Two values as a BF16 pair (bits), and their lo residuals for the split form.
+__device__ inline uint32_t bf16x2_bits(float a, float b, uint32_t &lo_bits) {
+  const __nv_bfloat162 hb = __floats2bfloat162_rn(a, b);
+  const __nv_bfloat162 lb = __floats2bfloat162_rn(a - __low2float(hb), b - __high2float(hb));
+  lo_bits = *reinterpret_cast<const uint32_t *>(&lb);
+  return *reinterpret_cast<const uint32_t *>(&hb);
 }
+
+// 8 consecutive values as one 16-byte core row of BF16 (and the lo residuals).
+// The values come as scalars so that the caller's arrays stay in registers.
+template <int NP>
+__device__ inline void put_core_row(__nv_bfloat16 *buf, size_t lo_stride, int off, float v0,
+                                    float v1, float v2, float v3, float v4, float v5, float v6,
+                                    float v7) {
+  uint32_t l0, l1, l2, l3;
+  const uint4 hi = make_uint4(bf16x2_bits(v0, v1, l0), bf16x2_bits(v2, v3, l1),
+                              bf16x2_bits(v4, v5, l2), bf16x2_bits(v6, v7, l3));
+  *reinterpret_cast<uint4 *>(buf + off) = hi;
+  if (NP == 3) *reinterpret_cast<uint4 *>(buf + lo_stride + off) = make_uint4(l0, l1, l2, l3);
+}
+#define TMD_PUT_ROW(NP, buf, lo, off, v, b)                                                \
+  put_core_row<NP>(buf, lo, off, v[b], v[b + 1], v[b + 2], v[b + 3], v[b + 4], v[b + 5], \
+                   v[b + 6], v[b + 7])
 
 // Elements of the resident weight blocks of one element's hidden layers.
 __host__ __device__ inline size_t tcp_weight_elems(int nl, const int *sizes, int nb) {
@@ -432,7 +436,7 @@ k_mlp_tcp(MlpTcArgs a) {
 #pragma unroll
           for (int j = 0; j < 8; j++) v[j] = 0.f;
         }
-        put_core_row<NP>(actb, act_lo, core_off(r, 8 * k8, nin), v);
+        TMD_PUT_ROW(NP, actb, act_lo, core_off(r, 8 * k8, nin), v, 0);
       }
     }
     publish();
@@ -453,7 +457,7 @@ k_mlp_tcp(MlpTcArgs a) {
       for (int c0 = 32 * half; c0 < N; c0 += 64) {
         float v[32];
         tmem_ld32(trow + c0, v);
-#pragma unroll 4
+#pragma unroll
         for (int j = 0; j < 32; j++) {
           const int c = c0 + j;
           const float z = v[j] + __ldg(ly.b + c);
@@ -470,7 +474,7 @@ k_mlp_tcp(MlpTcArgs a) {
           }
         }
 #pragma unroll
-        for (int q = 0; q < 4; q++) put_core_row<NP>(actb, act_lo, core_off(row, c0 + 8 * q, maxh), v + 8 * q);
+        for (int q = 0; q < 4; q++) TMD_PUT_ROW(NP, actb, act_lo, core_off(row, c0 + 8 * q, maxh), v, 8 * q);
       }
       publish();
     }
@@ -514,7 +518,7 @@ k_mlp_tcp(MlpTcArgs a) {
 #pragma unroll
           for (int j = 0; j < 32; j++) v[j] *= dzn[(size_t)(c0 + j) * TM + row];
 #pragma unroll
-          for (int q = 0; q < 4; q++) put_core_row<NP>(actb, act_lo, core_off(row, c0 + 8 * q, maxh), v + 8 * q);
+          for (int q = 0; q < 4; q++) TMD_PUT_ROW(NP, actb, act_lo, core_off(row, c0 + 8 * q, maxh), v, 8 * q);
         }
         publish();
       }
