@@ -467,10 +467,49 @@ def run_cells(args, rank, world, local, dev, barrier):
     sv.profile(False)
     etot = th.sum(-1)  # rows x cells
     drift = float(np.abs(etot[-1] - etot[0]).max() / c["natoms"])
+    # BF16 MLP forms on the same cells: a shorter timed NVE run each, and the
+    # force error of one evaluation against the FP32 form at the starting state
+    forms = {}
+    if not args.no_bf16:
+        b.set_atoms(data["x"], data["types"], data["v"])
+        f32 = b.compute()["f"]
+        nsteps_f = max(50, args.cells_steps // 5)
+        for prec in ("bf16x3", "bf16"):
+            try:
+                mb = TensorMDModel(f"{pot} {' '.join(syms)} precision {prec}", device=local)
+                bb = TensorMDBatch(mb, data["natoms"], 1.0)
+                bb.set_cells(data["boxes"])
+                bb.set_atoms(data["x"], data["types"], data["v"])
+                fe = bb.compute()["f"]
+                err = float(np.sqrt(((fe - f32) ** 2).mean()))
+                st_b = torch.cuda.ExternalStream(bb.system().stream(), device=dev)
+                bb.nve_run(max(args.warmup, 3), dt)
+                torch.cuda.synchronize()
+                barrier()
+                q0 = torch.cuda.Event(enable_timing=True)
+                q1 = torch.cuda.Event(enable_timing=True)
+                q0.record(st_b)
+                bb.nve_run(nsteps_f, dt)
+                q1.record(st_b)
+                torch.cuda.synchronize()
+                barrier()
+                msb = torch.tensor([q0.elapsed_time(q1)], device=dev, dtype=torch.float64)
+                if world > 1:
+                    import torch.distributed as dist
+                    dist.all_reduce(msb, op=dist.ReduceOp.MAX)
+                msb = float(msb.item())
+                forms[prec] = {"value": n * nsteps_f * world / (msb / 1000.0),
+                               "ms_per_step": msb / nsteps_f, "steps": nsteps_f,
+                               "force_rms_err_vs_fp32_eV_per_A": err}
+                bb.close()
+                mb.close()
+            except Exception as exc:  # report, do not hide
+                forms[prec] = {"error": str(exc)}
     out = {"value": n * args.cells_steps * world / (ms / 1000.0), "unit": UNIT,
            "ms_per_step": ms / args.cells_steps, "steps": args.cells_steps,
            "natoms": n, "ncells": c["ncells"], "gpu_launches": launches,
            "max_cell_energy_drift_eV_per_atom": drift,
+           "forms": forms,
            "force_form": {"chosen": sv.force_variant(), "ms_per_launch": tune_ms,
                           "descriptor_chosen": sv.descriptor_variant(),
                           "descriptor_ms_per_launch": tune_dms},

@@ -313,6 +313,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
     ta.status = s->status; ta.smem = m->tc_smem; ta.dz_bf16 = m->tc_dz_bf16 ? 1 : 0;
     ta.np = m->tc_np;
     ta.persistent = m->tc_persistent; ta.smem_p = m->tc_smem_p;
+    ta.dz_bf16_p = m->tc_dz_bf16_p ? 1 : 0;
     if (m->tc_fp8) launch_mlp_fp8(ta, s->st, s->launches);
     else launch_mlp_tc(ta, s->st, s->launches);
   } else {
@@ -796,13 +797,21 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     // weight-resident persistent form when the hidden weights, one tile's
     // operands and act' fit in shared memory (next to ~3 KB of static data)
     if (!fp8) {
-      const size_t sp = mlp_tcp_smem(h.nl, h.sizes.data(), h.resnet, np);
+      // act' in FP32; the BF16 form falls back to BF16 act' when that is what fits
+      const size_t kLimit = 227 * 1024 - 3 * 1024;
+      size_t sp = mlp_tcp_smem(h.nl, h.sizes.data(), h.resnet, np, false);
+      bool dzb = false;
+      if ((sp == 0 || sp > kLimit) && np == 1) {
+        sp = mlp_tcp_smem(h.nl, h.sizes.data(), h.resnet, np, true);
+        dzb = true;
+      }
       int nsm = 0;
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
-      if (sp > 0 && sp <= 227 * 1024 - 3 * 1024 && nsm > 0) {
+      if (sp > 0 && sp <= kLimit && nsm > 0) {
         m->tc_persistent = nsm;
         m->tc_smem_p = sp;
-        mlp_tcp_prepare(sp, np);
+        m->tc_dz_bf16_p = dzb;
+        mlp_tcp_prepare(sp, np, dzb);
       }
     }
     m->mlp_tr = 128;

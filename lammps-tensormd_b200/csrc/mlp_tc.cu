@@ -318,7 +318,7 @@ __host__ __device__ inline size_t tcp_weight_elems(int nl, const int *sizes, int
 }
 }  // namespace
 
-template <int NP>
+template <int NP, typename DZ>
 __global__ void __launch_bounds__(kTcpThreads, 1)
 k_mlp_tcp(MlpTcArgs a) {
   extern __shared__ __align__(1024) unsigned char smraw[];
@@ -339,7 +339,12 @@ k_mlp_tcp(MlpTcArgs a) {
   T *wsm = reinterpret_cast<T *>(smraw);
   T *actb = wsm + tcp_weight_elems(L, sizes, NB);
   const size_t act_lo = (size_t)TM * maxw;
-  float *dzb = reinterpret_cast<float *>(actb + NB * act_lo);
+  DZ *dzb = reinterpret_cast<DZ *>(actb + NB * act_lo);  // act' [layer][column][row]
+  size_t dzoff[kMaxLayers];
+  {
+    size_t o = 0;
+    for (int l = 0; l < L - 1; l++) { dzoff[l] = o; o += (size_t)sizes[l + 1] * TM; }
+  }
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -453,7 +458,7 @@ k_mlp_tcp(MlpTcArgs a) {
       if (!ok) break;
       const bool last = (l == L - 2);
       const double *wout = Ls[L - 1].wd;
-      float *dz = dzb + (size_t)l * maxh * TM;
+      DZ *dz = dzb + dzoff[l];
       for (int c0 = 32 * half; c0 < N; c0 += 64) {
         float v[32];
         tmem_ld32(trow + c0, v);
@@ -464,7 +469,7 @@ k_mlp_tcp(MlpTcArgs a) {
           float d;
           const float y = act_fwd(a.actfn, z, d);
           if (!last) {
-            dz[(size_t)c * TM + row] = d;
+            dz[(size_t)c * TM + row] = dz_store<DZ>(d);
             v[j] = y;
           } else {
             // output layer in FP64; gradient seed g = w_out, gz = g * act'
@@ -511,12 +516,12 @@ k_mlp_tcp(MlpTcArgs a) {
       } else {
         gemm(maxh, N, wb, K, 0, K);
         if (!ok) break;
-        const float *dzn = dzb + (size_t)(l - 1) * maxh * TM;
+        const DZ *dzn = dzb + dzoff[l - 1];
         for (int c0 = 32 * half; c0 < K; c0 += 64) {
           float v[32];
           tmem_ld32(trow + c0, v);
 #pragma unroll
-          for (int j = 0; j < 32; j++) v[j] *= dzn[(size_t)(c0 + j) * TM + row];
+          for (int j = 0; j < 32; j++) v[j] *= (float)dzn[(size_t)(c0 + j) * TM + row];
 #pragma unroll
           for (int q = 0; q < 4; q++) TMD_PUT_ROW(NP, actb, act_lo, core_off(row, c0 + 8 * q, maxh), v, 8 * q);
         }
@@ -533,7 +538,7 @@ k_mlp_tcp(MlpTcArgs a) {
                  "r"(TMEM_COLS));
 }
 
-size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np) {
+size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np, bool dz_bf16) {
   if (resnet || nl < 2) return 0;
   const size_t nb = np == 3 ? 2 : 1;
   int maxh = 1;
@@ -541,7 +546,7 @@ size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np) {
   const int maxw = sizes[0] > maxh ? sizes[0] : maxh;
   size_t b = tcp_weight_elems(nl, sizes, (int)nb) * 2;  // resident W^T and W blocks
   b += nb * (size_t)TM * maxw * 2;                      // operand buffer
-  b += (size_t)(nl - 1) * maxh * TM * 4;                // act' (FP32)
+  for (int l = 1; l < nl; l++) b += (size_t)sizes[l] * TM * (dz_bf16 ? 2 : 4);  // act'
   return b;
 }
 
@@ -585,18 +590,20 @@ void mlp_tc_prepare(size_t smem, bool dz_bf16, int np) {
   }
 }
 
-void mlp_tcp_prepare(size_t smem, int np) {
+void mlp_tcp_prepare(size_t smem, int np, bool dz_bf16) {
   const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  if (np == 3) cudaFuncSetAttribute(k_mlp_tcp<3>, at, (int)smem);
-  else cudaFuncSetAttribute(k_mlp_tcp<1>, at, (int)smem);
+  if (np == 3) cudaFuncSetAttribute(k_mlp_tcp<3, float>, at, (int)smem);
+  else if (dz_bf16) cudaFuncSetAttribute(k_mlp_tcp<1, __nv_bfloat16>, at, (int)smem);
+  else cudaFuncSetAttribute(k_mlp_tcp<1, float>, at, (int)smem);
 }
 
 void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches) {
   if (a.ntiles <= 0) return;
   if (a.persistent > 0) {
     const int grid = a.ntiles < a.persistent ? a.ntiles : a.persistent;
-    if (a.np == 3) k_mlp_tcp<3><<<grid, kTcpThreads, a.smem_p, st>>>(a);
-    else k_mlp_tcp<1><<<grid, kTcpThreads, a.smem_p, st>>>(a);
+    if (a.np == 3) k_mlp_tcp<3, float><<<grid, kTcpThreads, a.smem_p, st>>>(a);
+    else if (a.dz_bf16_p) k_mlp_tcp<1, __nv_bfloat16><<<grid, kTcpThreads, a.smem_p, st>>>(a);
+    else k_mlp_tcp<1, float><<<grid, kTcpThreads, a.smem_p, st>>>(a);
     launches += 1;
     return;
   }

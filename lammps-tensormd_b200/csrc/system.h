@@ -27,6 +27,7 @@ struct tmd_model {
   bool tc_fp8 = false;   // FP8 (e4m3) tensor-core MLP
   int tc_persistent = 0; // > 0: weight-resident persistent tensor-core MLP (grid size)
   size_t tc_smem_p = 0;
+  bool tc_dz_bf16_p = false;
   int maxh = 1;
   double *d_mass = nullptr;     // per element
   int mlp_tr = 64;

@@ -138,14 +138,15 @@ struct MlpTcArgs {
   int np;  // 1: BF16 products; 3: split BF16 (hi*hi + hi*lo + lo*hi)
   int persistent;     // > 0: weight-resident persistent form on this many CTAs
   size_t smem_p;      // its dynamic shared memory
+  int dz_bf16_p;      // its act' in BF16 (BF16 form only, when FP32 does not fit)
 };
 void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches);
 size_t mlp_tc_smem(int nl, int maxh, int resnet, bool dz_bf16, int np);
 void mlp_tc_prepare(size_t smem, bool dz_bf16, int np);
 // Persistent form: dynamic shared memory for sizes[0..nl], 0 if unsupported
 // (residual layers).
-size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np);
-void mlp_tcp_prepare(size_t smem, int np);
+size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np, bool dz_bf16);
+void mlp_tcp_prepare(size_t smem, int np, bool dz_bf16);
 
 // Host: pack a rows x cols matrix (element (r, k) = src[r * ld_r + k * ld_k])
 // into 64-column chunks of 8x8 BF16 core matrices, K-major.
