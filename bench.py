@@ -384,6 +384,17 @@ def run_ours(args, rank, world, local):
     serving = None
     if args.serve_window > 0 and not args.main_only:
         serving = run_serving(args, rank, local)
+        if not args.no_bf16:
+            # the same job stream (same seeds) with the MLP in the BF16 forms
+            serving["forms"] = {}
+            for prec in ("bf16x3", "bf16"):
+                try:
+                    sf = run_serving(args, rank, local, precision=prec)
+                    serving["forms"][prec] = {k: sf[k] for k in (
+                        "solves_per_s", "p50_ms", "p99_ms", "atom_steps_per_s", "makespan_s",
+                        "by_kind")}
+                except Exception as exc:  # report, do not hide
+                    serving["forms"][prec] = {"error": str(exc)}
     w23k = None if args.main_only else run_w23k(args, rank, world, local, dev, barrier)
 
     cpu = None
@@ -570,7 +581,7 @@ def run_w23k(args, rank, world, local, dev, barrier):
                       "fix nvt temp 300 300 0.1, skin 1.0, dt 1 fs"}
 
 
-def run_serving(args, rank, local):
+def run_serving(args, rank, local, precision="fp32"):
     """Serving: Poisson arrivals (rate args.serve_rate per s over
     args.serve_window s) of jobs with N log-uniform in [32, 4096] atoms, FCC /
     BCC lattices or random packings (0.085 A^-3, dmin 2 A), 1-4 elements; 60%
@@ -583,7 +594,8 @@ def run_serving(args, rank, local):
     pot = f"/tmp/tmd_bench_serve_{rank}.npz"
     syms = synth.gaussian_potential(pot, seed=4242, nelt=4, num_filters=16, rc=6.0,
                                     max_moment=3, hidden=(64, 64), actfn=2)
-    model = TensorMDModel(f"{pot} {' '.join(syms)}", device=local)
+    prec = "" if precision == "fp32" else f" precision {precision}"
+    model = TensorMDModel(f"{pot} {' '.join(syms)}{prec}", device=local)
     sizes = np.unique(np.round(np.geomspace(32, 4096, 12)).astype(int))
     packings = {int(n): synth.random_packing(int(n), rng) for n in sizes}
     t_arr = np.cumsum(rng.exponential(1.0 / args.serve_rate,
@@ -624,7 +636,7 @@ def run_serving(args, rank, local):
     model.close()
     lat = np.array([d["latency"] for d in done]) * 1000.0
     natoms = np.array([len(j[0]) for j in jobs])
-    out = {"jobs": len(jobs), "arrival_rate_per_s": args.serve_rate,
+    out = {"precision": precision, "jobs": len(jobs), "arrival_rate_per_s": args.serve_rate,
            "window_s": args.serve_window, "makespan_s": t_end - t_start,
            "solves_per_s": len(jobs) / (t_end - t_start),
            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),

@@ -51,6 +51,25 @@ def test_single_point_jobs_equal_separate_systems(model4):
     srv.close()
 
 
+def test_bf16_single_point_jobs_equal_separate_systems(tmp_path):
+    """The tensor-core MLP forms too: a job's result does not depend on the
+    other jobs in the batch (MMA rows are independent atoms)."""
+    p = tmp_path / "serve_bf16.npz"
+    syms = synth.gaussian_potential(p, seed=31, nelt=4, num_filters=16, rc=6.0,
+                                    max_moment=3, hidden=(64, 64), actfn=2)
+    m = TensorMDModel(f"{p} {' '.join(syms)} precision bf16")
+    rng = np.random.default_rng(5)
+    srv = TensorMDServer(m, max_atoms=200000, max_cells=256)
+    jobs = [synth.serving_job(rng, kind=0, nmax=900) for _ in range(8)]
+    tickets = [srv.submit(0, x, t, box) for x, t, box, _ in jobs]
+    for tk, (x, t, box, _) in zip(tickets, jobs):
+        out = srv.wait(tk, timeout=120)
+        ref = _separate(m, x, t, box).compute(1, 1)
+        assert np.array_equal(out["f"], ref["f"])
+        assert out["energy"] == pytest.approx(ref["energy"], rel=1e-12, abs=1e-10)
+    srv.close()
+
+
 def test_nve_job_matches_system_run(model4):
     rng = np.random.default_rng(2)
     x, t, box, v = synth.serving_job(rng, kind=1, nmin=500, nmax=600)
