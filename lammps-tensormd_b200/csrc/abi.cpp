@@ -180,8 +180,31 @@ int alloc_neighbors(tmd_system *s, int cap) {
   return TMD_OK;
 }
 
-int initial_cap(tmd_system *s) {
+int adopt_rows(tmd_system *s, int cap, uint32_t *nbr, int *rev) {
+  if (cap > 4096) return fail(TMD_ERR_CAPACITY, "more than 4096 neighbors per atom");
+  TMD_CUDA(cudaStreamSynchronize(s->st));  // the rows were filled on s->st
+  drop_graph(s);
+  dfree(s->tmp); dfree(s->nbr); dfree(s->rev); dfree(s->pdf); dfree(s->pgeo);
+  s->nbr = nbr;
+  s->rev = rev;
+  size_t tot = (size_t)s->natoms_cap * cap;
+  TMD_CUDA(dalloc(&s->tmp, tot));
+  TMD_CUDA(dalloc(&s->pdf, tot));
+  TMD_CUDA(dalloc(&s->pgeo, 2 * tot));
+  s->cap = cap;
+  s->capp = pow2_at_least(cap);
+  return TMD_OK;
+}
+
+int cap_for_density(const tmd_system *s, double dens) {
   double cut = s->m->h.rmax + s->skin;
+  double est = dens * 4.0 / 3.0 * M_PI * cut * cut * cut;
+  int cap = (int)std::ceil(1.3 * est) + 32;
+  if (cap < 64) cap = 64;
+  return cap;
+}
+
+int initial_cap(tmd_system *s) {
   double dens = 0.0;
   if (s->ncells > 0) {
     for (int c = 0; c < s->ncells; c++) {
@@ -192,10 +215,7 @@ int initial_cap(tmd_system *s) {
   } else {
     dens = s->n / (s->box.xprd * s->box.yprd * s->box.zprd);
   }
-  double est = dens * 4.0 / 3.0 * M_PI * cut * cut * cut;
-  int cap = (int)std::ceil(1.3 * est) + 32;
-  if (cap < 64) cap = 64;
-  return cap;
+  return cap_for_density(s, dens);
 }
 
 NbArgs nb_args(tmd_system *s) {
@@ -679,15 +699,19 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     return fail(TMD_ERR_CUDA, std::string("model upload: ") + cudaGetErrorString(e));
   }
   // MLP: the resident-weight form (one persistent CTA per SM) when the
-  // element's hidden weights and a tile's activations fit in shared memory,
-  // else weights streamed in chunks with 64- or 32-atom tiles
+  // element's hidden weights and a tile's activations fit in shared memory
+  // (128-atom tiles, else 64), else weights streamed in chunks with 64- or
+  // 32-atom tiles
   size_t s64 = mlp_fp32_smem(h.nl, h.sizes.data(), 64);
   size_t s32 = mlp_fp32_smem(h.nl, h.sizes.data(), 32);
-  const size_t sres = mlp_fp32r_smem(h.nl, h.sizes.data());
+  const size_t sres = mlp_fp32r_smem(h.nl, h.sizes.data(), 128);
+  const size_t sres64 = mlp_fp32r_smem(h.nl, h.sizes.data(), 64);
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
   if (h.nl >= 2 && sres <= 227 * 1024 && nsm > 0) {
-    m->mlp_tr = mlp_fp32r_tile(); m->mlp_smem = sres; m->mlp_resident = nsm;
+    m->mlp_tr = 128; m->mlp_smem = sres; m->mlp_resident = nsm;
+  } else if (h.nl >= 2 && sres64 <= 227 * 1024 && nsm > 0) {
+    m->mlp_tr = 64; m->mlp_smem = sres64; m->mlp_resident = nsm;
   } else if (s64 <= 110 * 1024) {
     m->mlp_tr = 64; m->mlp_smem = s64;
   } else if (s32 <= 220 * 1024) {

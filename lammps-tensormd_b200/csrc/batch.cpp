@@ -64,29 +64,37 @@ int cells_layout(tmd_system *s, int ncells, const int *natoms) {
   return TMD_OK;
 }
 
+int cell_setup(const tmd_system *s, const double bx[9], const int pbc[3], BoxP &b,
+               CellGeom &g, std::string &why) {
+  const double cut = s->m->h.rmax + s->skin;
+  if (!(bx[3] > 0 && bx[4] > 0 && bx[5] > 0)) {
+    why = "box lengths must be > 0";
+    return TMD_ERR_ARG;
+  }
+  box_setup(b, bx, pbc);
+  g = CellGeom{};
+  widths(b, g.w);
+  for (int a = 0; a < 3; a++) {
+    g.m[a] = 0;
+    if (!b.pbc[a]) continue;
+    // the largest shift whose slab can come within cut of an atom
+    g.m[a] = (int)std::ceil(cut * (1.0 + 1e-9) / g.w[a] + 1e-6);
+    if (g.m[a] > kShiftR) {
+      why = "too small for the cutoff: more than 3 images per axis would be needed";
+      return TMD_ERR_ARG;
+    }
+  }
+  return TMD_OK;
+}
+
 int cells_geometry(tmd_system *s, const double *boxes, const int *pbc) {
   const int C = s->ncells;
-  const double cut = s->m->h.rmax + s->skin;
   std::vector<BoxP> hb(C);
   std::vector<CellGeom> hg(C);
+  std::string why;
   for (int c = 0; c < C; c++) {
-    const double *bx = boxes + 9 * (size_t)c;
-    if (!(bx[3] > 0 && bx[4] > 0 && bx[5] > 0))
-      return fail(TMD_ERR_ARG, "cell " + std::to_string(c) + ": box lengths must be > 0");
-    box_setup(hb[c], bx, pbc + 3 * (size_t)c);
-    CellGeom g{};
-    widths(hb[c], g.w);
-    for (int a = 0; a < 3; a++) {
-      g.m[a] = 0;
-      if (!hb[c].pbc[a]) continue;
-      // the largest shift whose slab can come within cut of an atom
-      g.m[a] = (int)std::ceil(cut * (1.0 + 1e-9) / g.w[a] + 1e-6);
-      if (g.m[a] > kShiftR)
-        return fail(TMD_ERR_ARG, "cell " + std::to_string(c) +
-                                     " is too small for the cutoff: more than 3 images "
-                                     "per axis would be needed");
-    }
-    hg[c] = g;
+    int rc = cell_setup(s, boxes + 9 * (size_t)c, pbc + 3 * (size_t)c, hb[c], hg[c], why);
+    if (rc) return fail(rc, "cell " + std::to_string(c) + ": " + why);
   }
   drop_graph(s);
   TMD_CUDA(cudaMemcpyAsync(s->cbox, hb.data(), C * sizeof(BoxP), cudaMemcpyHostToDevice, s->st));

@@ -242,8 +242,9 @@ k_mlp_fp32(MlpArgs a) {
 // as float4 (row stride = 4 mod 32 words: the 8 threads of a phase hit
 // distinct banks).  Same FP32 arithmetic in the same order as k_mlp_fp32.
 // ---------------------------------------------------------------------------
-constexpr int kResTR = 128;       // atoms per tile of the resident form
-constexpr int kResThreads = 512;  // 16 warps: a 4 x 4 register tile per thread
+// Tiles of 128 atoms on 16 warps, or of 64 atoms on 8 warps when an input
+// width as large as 4 elements x 16 filters x 4 moments needs the smaller
+// activation buffers: a 4 x 4 register tile per thread either way.
 
 struct ResLayout {
   int woff[kMaxLayers], ldw[kMaxLayers], boff[kMaxLayers], dzoff[kMaxLayers];
@@ -551,11 +552,9 @@ k_mlp_fp32r(MlpArgs a) {
 
 }  // namespace
 
-size_t mlp_fp32r_smem(int nl, const int *sizes) {
-  return sizeof(float) * (size_t)res_layout(nl, sizes, kResTR).total;
+size_t mlp_fp32r_smem(int nl, const int *sizes, int tr) {
+  return sizeof(float) * (size_t)res_layout(nl, sizes, tr).total;
 }
-
-int mlp_fp32r_tile() { return kResTR; }
 
 size_t mlp_fp32_smem(int nl, const int *sizes, int tr) {
   // sizes[0..nl]: n_in, layer widths
@@ -574,7 +573,10 @@ void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches) {
   launches += 1;
   if (a.resident > 0) {
     const int grid = a.ntiles < a.resident ? a.ntiles : a.resident;
-    k_mlp_fp32r<kResTR, kResThreads><<<grid, kResThreads, a.smem, st>>>(a);
+    if (a.tr == 128)
+      k_mlp_fp32r<128, 512><<<grid, 512, a.smem, st>>>(a);
+    else
+      k_mlp_fp32r<64, 256><<<grid, 256, a.smem, st>>>(a);
     return;
   }
   if (a.tr == 64) {
@@ -585,9 +587,12 @@ void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches) {
 }
 
 void mlp_fp32_prepare(int tr, size_t smem, bool resident) {
-  if (resident)
-    cudaFuncSetAttribute(k_mlp_fp32r<kResTR, kResThreads>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (resident && tr == 128)
+    cudaFuncSetAttribute(k_mlp_fp32r<128, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+  else if (resident)
+    cudaFuncSetAttribute(k_mlp_fp32r<64, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
   else if (tr == 64)
     cudaFuncSetAttribute(k_mlp_fp32<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   else

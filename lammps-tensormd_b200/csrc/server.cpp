@@ -41,6 +41,7 @@ struct Job {
   int n = 0;
   std::vector<double> x, v;
   std::vector<int> elem;
+  std::vector<int> ecount;  // atoms per potential element
   double box[9];
   int pbc[3];
   int nsteps = 0;
@@ -80,10 +81,13 @@ struct tmd_server {
   std::vector<JobP> active;            // cell order
   std::vector<CellCtl> h_ctl;          // host copy of the cells' control blocks
   std::vector<double> h_cell;          // [cells][8] energy, virial
-  double *x2 = nullptr, *v2 = nullptr, *f2 = nullptr;
-  int *img2 = nullptr;
+  // second copies of the per-atom arrays a relayout moves into
+  double *x2 = nullptr, *v2 = nullptr, *f2 = nullptr, *xb2 = nullptr;
+  int *img2 = nullptr, *elem2 = nullptr, *boff2 = nullptr;
+  int *rev2 = nullptr;  // natoms x cap, allocated with the rows
   double *stage_x = nullptr, *stage_v = nullptr;
-  int *src = nullptr;
+  int *stage_e = nullptr;
+  int *src = nullptr, *fresh = nullptr, *estart = nullptr;
   CellCtl *ctl = nullptr;
   double *pw = nullptr, *csum = nullptr, *fsq = nullptr, *cfmax = nullptr;
 };
@@ -111,8 +115,91 @@ CellCtl initial_ctl(const Job &j) {
   return q;
 }
 
-// Lay the cells of `next` out on the device (continuing jobs gathered from
-// the current layout, new ones from staging), then rebuild the lists.
+// Move every atom into the layout described by sv->src / sv->fresh (already
+// on the device, with acell and coff) with neighbor rows of cap1 entries, and
+// swap the moved arrays in.  Rows of the same length go through the build
+// scratch (tmp) and sv->rev2; longer rows get new arrays.
+int move_cells(tmd_server *sv, int n, int cap1) {
+  tmd_system *s = sv->s;
+  if (cap1 > 4096) return fail(TMD_ERR_CAPACITY, "more than 4096 neighbors per atom");
+  const bool same = cap1 == s->cap && s->nbr && s->tmp && sv->rev2;
+  uint32_t *nbr2 = same ? s->tmp : nullptr;
+  int *rev2 = same ? sv->rev2 : nullptr;
+  if (!same) {
+    const size_t tot = (size_t)s->natoms_cap * cap1;
+    cudaError_t e = dalloc(&nbr2, tot);
+    if (e == cudaSuccess) e = dalloc(&rev2, tot);
+    if (e != cudaSuccess) {
+      dfree(nbr2);
+      dfree(rev2);
+      return fail(TMD_ERR_CUDA, std::string("neighbor rows: ") + cudaGetErrorString(e));
+    }
+  }
+  SrvMove m{};
+  m.n = n;
+  m.B = s->m->h.nelt;
+  m.cap0 = s->cap > 0 ? s->cap : 1;
+  m.cap1 = cap1;
+  m.acell = s->acell; m.coff = s->coff; m.src = sv->src; m.fresh = sv->fresh;
+  m.x = s->x; m.v = s->v; m.f = s->f; m.xb = s->xbuild;
+  m.img = s->image; m.elem = s->elem; m.boff = s->boff; m.rev = s->rev; m.nbr = s->nbr;
+  m.sx = sv->stage_x; m.sv = sv->stage_v; m.selem = sv->stage_e;
+  m.x2 = sv->x2; m.v2 = sv->v2; m.f2 = sv->f2; m.xb2 = sv->xb2;
+  m.img2 = sv->img2; m.elem2 = sv->elem2; m.boff2 = sv->boff2; m.rev2 = rev2; m.nbr2 = nbr2;
+  launch_srv_move(m, s->st, s->launches);
+  TMD_CUDA(cudaGetLastError());
+  std::swap(s->x, sv->x2);
+  std::swap(s->v, sv->v2);
+  std::swap(s->f, sv->f2);
+  std::swap(s->xbuild, sv->xb2);
+  std::swap(s->image, sv->img2);
+  std::swap(s->elem, sv->elem2);
+  std::swap(s->boff, sv->boff2);
+  if (same) {
+    std::swap(s->nbr, s->tmp);
+    std::swap(s->rev, sv->rev2);
+    return TMD_OK;
+  }
+  int rc = adopt_rows(s, cap1, nbr2, rev2);  // synchronises, frees the old rows
+  if (rc) return rc;
+  dfree(sv->rev2);
+  TMD_CUDA(dalloc(&sv->rev2, (size_t)s->natoms_cap * cap1));
+  return TMD_OK;
+}
+
+// Neighbor lists of the fresh cells (the others kept theirs).  An overflow
+// lengthens every row in place (each cell moves onto itself) and builds the
+// fresh cells again.
+int build_fresh(tmd_server *sv) {
+  tmd_system *s = sv->s;
+  for (int attempt = 0; attempt < 4; attempt++) {
+    int rc = clear_status(s);
+    if (rc) return rc;
+    launch_srv_mark(s->ncells, sv->fresh, s->cflag, s->flag, s->st, s->launches);
+    launch_neighbor_build(nb_args(s), s->st, s->launches);
+    TMD_CUDA(cudaGetLastError());
+    rc = read_status(s);
+    if (rc) return rc;
+    const int st = s->h_status[0];
+    if (st & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
+    if (st & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside a non-periodic boundary");
+    if (!(st & kStatusOverflow)) return TMD_OK;
+    const int need = s->h_status[1];
+    const int cap1 = (need + need / 4 + 32 + 31) / 32 * 32;
+    std::vector<int> self(s->h_coff.begin(), s->h_coff.end() - 1);
+    TMD_CUDA(cudaMemcpyAsync(sv->src, self.data(), self.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, s->st));
+    rc = move_cells(sv, s->n, cap1);
+    if (rc) return rc;
+  }
+  return fail(TMD_ERR_CAPACITY, "neighbor list did not fit after resizing");
+}
+
+// Lay the cells of `next` out on the device: continuing jobs move from the
+// current layout with their neighbor lists (a cell's list is rebuilt only
+// when its own atoms trigger it, as for a separate system), new ones come
+// from staging and get their lists built.  Host work is per cell; per-atom
+// work (cell index, element grouping) runs on the device.
 int relayout(tmd_server *sv, const std::vector<JobP> &next) {
   tmd_system *s = sv->s;
   const int C = (int)next.size();
@@ -122,65 +209,104 @@ int relayout(tmd_server *sv, const std::vector<JobP> &next) {
     s->n = 0;
     return TMD_OK;
   }
+  const int B = s->m->h.nelt, tr = s->m->mlp_tr;
   std::unordered_map<const Job *, int> old_cell;
   for (size_t c = 0; c < sv->active.size(); c++) old_cell[sv->active[c].get()] = (int)c;
-  const std::vector<int> old_off = s->h_coff;
-  std::vector<int> natoms(C), srcv(C), elem;
+  std::vector<int> coff(C + 1, 0), srcv(C), fresh(C, 0), total(B, 0), selem;
   std::vector<double> boxes(9 * (size_t)C), sx, svel;
   std::vector<int> pbc(3 * (size_t)C);
   std::vector<CellCtl> ctl(C);
   int staged = 0;
   for (int c = 0; c < C; c++) {
     const Job &j = *next[c];
-    natoms[c] = j.n;
+    coff[c + 1] = coff[c] + j.n;
     std::memcpy(&boxes[9 * (size_t)c], j.box, sizeof j.box);
     std::memcpy(&pbc[3 * (size_t)c], j.pbc, sizeof j.pbc);
-    elem.insert(elem.end(), j.elem.begin(), j.elem.end());
+    for (int e = 0; e < B; e++) total[e] += j.ecount[e];
     auto it = old_cell.find(&j);
     if (it != old_cell.end()) {
-      srcv[c] = old_off[it->second];
+      srcv[c] = s->h_coff[it->second];
       ctl[c] = sv->h_ctl[it->second];
     } else {
       srcv[c] = -staged - 1;
       sx.insert(sx.end(), j.x.begin(), j.x.end());
       svel.insert(svel.end(), j.v.begin(), j.v.end());
+      selem.insert(selem.end(), j.elem.begin(), j.elem.end());
       staged += j.n;
       ctl[c] = initial_ctl(j);
+      fresh[c] = 1;
     }
   }
+  const int n = coff[C];
+  if (n > s->natoms_cap) return fail(TMD_ERR_CAPACITY, "atoms exceed the batch capacity");
+  // MLP element grouping (set_elements' order): element e from start[e],
+  // cell by cell; tiles of up to mlp_tr atoms of one element
+  std::vector<int> cur(B, 0), estart((size_t)C * B), tiles;
+  for (int e = 1; e < B; e++) cur[e] = cur[e - 1] + total[e - 1];
+  for (int e = 0; e < B; e++)
+    for (int o = 0; o < total[e]; o += tr) {
+      tiles.push_back(e);
+      tiles.push_back(cur[e] + o);
+      tiles.push_back(std::min(tr, total[e] - o));
+    }
+  for (int c = 0; c < C; c++)
+    for (int e = 0; e < B; e++) {
+      estart[(size_t)c * B + e] = cur[e];
+      cur[e] += next[c]->ecount[e];
+    }
+  s->ncells = C;
+  int rc = cells_geometry(s, boxes.data(), pbc.data());
+  if (rc) return rc;
+  s->h_coff = coff;
+  s->h_acell.clear();
+  TMD_CUDA(cudaMemcpyAsync(s->coff, coff.data(), (C + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                           s->st));
+  TMD_CUDA(cudaMemcpyAsync(sv->src, srcv.data(), C * sizeof(int), cudaMemcpyHostToDevice,
+                           s->st));
+  TMD_CUDA(cudaMemcpyAsync(sv->fresh, fresh.data(), C * sizeof(int), cudaMemcpyHostToDevice,
+                           s->st));
+  TMD_CUDA(cudaMemcpyAsync(sv->ctl, ctl.data(), C * sizeof(CellCtl), cudaMemcpyHostToDevice,
+                           s->st));
+  TMD_CUDA(cudaMemcpyAsync(sv->estart, estart.data(), estart.size() * sizeof(int),
+                           cudaMemcpyHostToDevice, s->st));
+  if (!tiles.empty())
+    TMD_CUDA(cudaMemcpyAsync(s->tiles, tiles.data(), tiles.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, s->st));
   if (staged > 0) {
     TMD_CUDA(cudaMemcpyAsync(sv->stage_x, sx.data(), sx.size() * sizeof(double),
                              cudaMemcpyHostToDevice, s->st));
     TMD_CUDA(cudaMemcpyAsync(sv->stage_v, svel.data(), svel.size() * sizeof(double),
                              cudaMemcpyHostToDevice, s->st));
+    TMD_CUDA(cudaMemcpyAsync(sv->stage_e, selem.data(), selem.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, s->st));
   }
-  TMD_CUDA(cudaMemcpyAsync(sv->src, srcv.data(), C * sizeof(int), cudaMemcpyHostToDevice,
-                           s->st));
-  TMD_CUDA(cudaMemcpyAsync(sv->ctl, ctl.data(), C * sizeof(CellCtl), cudaMemcpyHostToDevice,
-                           s->st));
-  int rc = cells_layout(s, C, natoms.data());  // new acell/coff (synchronises)
+  launch_srv_acell(C, s->coff, s->acell, s->st, s->launches);
+  // row length: the current one unless a fresh cell is denser than it allows
+  int cap1 = s->cap;
+  if (staged > 0) {
+    double dens = 0.0;
+    for (int c = 0; c < C; c++)
+      if (fresh[c]) {
+        const BoxP &bx = s->h_cbox[c];
+        dens = std::max(dens, (coff[c + 1] - coff[c]) / (bx.xprd * bx.yprd * bx.zprd));
+      }
+    cap1 = std::max(cap1, (cap_for_density(s, dens) + 31) / 32 * 32);
+  }
+  rc = move_cells(sv, n, cap1);
   if (rc) return rc;
-  const int n = s->h_coff[C];
-  launch_srv_gather(n, s->acell, s->coff, sv->src, s->x, s->v, s->f, s->image, sv->stage_x,
-                    sv->stage_v, sv->x2, sv->v2, sv->f2, sv->img2, s->st, s->launches);
+  launch_srv_perm(C, B, s->coff, s->elem, sv->estart, s->perm, s->st, s->launches);
   TMD_CUDA(cudaGetLastError());
-  std::swap(s->x, sv->x2);
-  std::swap(s->v, sv->v2);
-  std::swap(s->f, sv->f2);
-  std::swap(s->image, sv->img2);
-  rc = cells_geometry(s, boxes.data(), pbc.data());
-  if (rc) return rc;
-  rc = set_elements(s, n, elem.data());
-  if (rc) return rc;
+  s->n = n;
+  s->ntiles = (int)tiles.size() / 3;
+  s->h_elem.clear();
+  s->have_atoms = true;
+  s->forces_valid = false;
+  s->nhc_valid = false;
   sv->active = next;
   sv->h_ctl = ctl;
-  s->have_atoms = true;
-  int cap = initial_cap(s);
-  if (cap > s->cap) {
-    rc = alloc_neighbors(s, cap);
-    if (rc) return rc;
-  }
-  return rebuild_now(s);
+  if (staged > 0) return build_fresh(sv);  // synchronises
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  return TMD_OK;
 }
 
 // Per-cell energy/virial sums and control blocks to the host.
@@ -401,9 +527,15 @@ int tmd_server_create(const tmd_model *m, int max_atoms, int max_cells, double s
   if (e == cudaSuccess) e = dalloc(&sv->v2, 3 * N);
   if (e == cudaSuccess) e = dalloc(&sv->f2, 3 * N);
   if (e == cudaSuccess) e = dalloc(&sv->img2, 3 * N);
+  if (e == cudaSuccess) e = dalloc(&sv->xb2, 3 * N);
+  if (e == cudaSuccess) e = dalloc(&sv->elem2, N);
+  if (e == cudaSuccess) e = dalloc(&sv->boff2, N * (m->h.nelt + 1));
   if (e == cudaSuccess) e = dalloc(&sv->stage_x, 3 * N);
   if (e == cudaSuccess) e = dalloc(&sv->stage_v, 3 * N);
+  if (e == cudaSuccess) e = dalloc(&sv->stage_e, N);
   if (e == cudaSuccess) e = dalloc(&sv->src, C);
+  if (e == cudaSuccess) e = dalloc(&sv->fresh, C);
+  if (e == cudaSuccess) e = dalloc(&sv->estart, C * m->h.nelt);
   if (e == cudaSuccess) e = dalloc(&sv->ctl, C);
   if (e == cudaSuccess) e = dalloc(&sv->pw, 3 * N);
   if (e == cudaSuccess) e = dalloc(&sv->csum, 4 * C);
@@ -429,7 +561,9 @@ void tmd_server_free(tmd_server *sv) {
   if (sv->worker.joinable()) sv->worker.join();
   if (sv->s) cudaSetDevice(sv->s->m->device);
   dfree(sv->x2); dfree(sv->v2); dfree(sv->f2); dfree(sv->img2);
-  dfree(sv->stage_x); dfree(sv->stage_v); dfree(sv->src); dfree(sv->ctl);
+  dfree(sv->xb2); dfree(sv->elem2); dfree(sv->boff2); dfree(sv->rev2);
+  dfree(sv->stage_x); dfree(sv->stage_v); dfree(sv->stage_e); dfree(sv->src);
+  dfree(sv->fresh); dfree(sv->estart); dfree(sv->ctl);
   dfree(sv->pw); dfree(sv->csum); dfree(sv->fsq); dfree(sv->cfmax);
   tmd_system_free(sv->s);
   delete sv;
@@ -446,7 +580,13 @@ int tmd_server_submit(tmd_server *sv, int kind, int n, const double *x, const in
     return fail(TMD_ERR_ARG, "NVE and FIRE jobs need nsteps >= 1 and dt > 0");
   if (kind == kJobFire && !(fmax > 0)) return fail(TMD_ERR_ARG, "FIRE jobs need fmax > 0");
   if (n > sv->max_atoms) return fail(TMD_ERR_CAPACITY, "job larger than the server's atom budget");
-  if (!(box[3] > 0 && box[4] > 0 && box[5] > 0)) return fail(TMD_ERR_ARG, "box lengths must be > 0");
+  {
+    BoxP b;
+    CellGeom g;
+    std::string why;
+    int rc = cell_setup(sv->s, box, pbc, b, g, why);
+    if (rc) return fail(rc, "job box: " + why);
+  }
   auto j = std::make_shared<Job>();
   j->kind = kind;
   j->n = n;
@@ -455,6 +595,8 @@ int tmd_server_submit(tmd_server *sv, int kind, int n, const double *x, const in
   if (v) j->v.assign(v, v + 3 * (size_t)n);
   int rc = map_types(sv->m, n, type, j->elem);
   if (rc) return rc;
+  j->ecount.assign(sv->m->h.nelt, 0);
+  for (int e : j->elem) j->ecount[e]++;
   std::memcpy(j->box, box, sizeof j->box);
   std::memcpy(j->pbc, pbc, sizeof j->pbc);
   j->nsteps = nsteps;

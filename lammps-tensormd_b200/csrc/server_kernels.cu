@@ -26,44 +26,131 @@ __device__ inline bool fire_active(const CellCtl &c) {
 }
 }  // namespace
 
-__global__ void k_srv_gather(int n, const int *__restrict__ acell, const int *__restrict__ coff,
-                             const int *__restrict__ src, const double *__restrict__ x_old,
-                             const double *__restrict__ v_old, const double *__restrict__ f_old,
-                             const int *__restrict__ img_old,
-                             const double *__restrict__ x_stage,
-                             const double *__restrict__ v_stage, double *__restrict__ x,
-                             double *__restrict__ v, double *__restrict__ f,
-                             int *__restrict__ img) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n) return;
-  const int c = acell[a];
-  const int k = a - coff[c];
-  const int s = src[c];
-  for (int d = 0; d < 3; d++) {
+// One warp per atom of the new layout.  A moved atom brings its state and,
+// unless its cell is about to be rebuilt, its neighbor row: entries keep
+// their shift code and move their atom index with the cell (every partner
+// of a cell's atom is in the same cell), partner slots j*cap0 + t become
+// (j + delta)*cap1 + t.  The row keeps its sorted order since one delta
+// moves every index.  A new atom gets an empty row.
+__global__ void k_srv_move(SrvMove m) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int B1 = m.B + 1;
+  for (int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < m.n; a += nw) {
+    const int c = m.acell[a];
+    const int k = a - m.coff[c];
+    const int s = m.src[c];
     if (s >= 0) {
-      const long o = 3L * (s + k) + d;
-      x[3L * a + d] = x_old[o];
-      v[3L * a + d] = v_old[o];
-      f[3L * a + d] = f_old[o];
-      img[3L * a + d] = img_old[o];
+      const long o = (long)s + k;
+      if (lane < 3) {
+        m.x2[3L * a + lane] = m.x[3 * o + lane];
+        m.v2[3L * a + lane] = m.v[3 * o + lane];
+        m.f2[3L * a + lane] = m.f[3 * o + lane];
+        m.xb2[3L * a + lane] = m.xb[3 * o + lane];
+        m.img2[3L * a + lane] = m.img[3 * o + lane];
+      } else if (lane == 3) {
+        m.elem2[a] = m.elem[o];
+      }
+      if (m.fresh[c]) {
+        for (int b = lane; b < B1; b += 32) m.boff2[(long)a * B1 + b] = 0;
+        continue;
+      }
+      for (int b = lane; b < B1; b += 32) m.boff2[(long)a * B1 + b] = m.boff[o * B1 + b];
+      int cnt = m.boff[o * B1 + m.B];
+      cnt = min(cnt, min(m.cap0, m.cap1));
+      const int delta = m.coff[c] - s;
+      const uint32_t *row = m.nbr + o * m.cap0;
+      const int *rrow = m.rev + o * m.cap0;
+      uint32_t *row2 = m.nbr2 + (long)a * m.cap1;
+      int *rrow2 = m.rev2 + (long)a * m.cap1;
+      for (int t = lane; t < cnt; t += 32) {
+        const uint32_t e = row[t];
+        row2[t] = (e & ~kAtomMask) | uint32_t((int)(e & kAtomMask) + delta);
+        const int r = rrow[t];
+        rrow2[t] = r < 0 ? -1 : (int)((long)(r / m.cap0 + delta) * m.cap1 + r % m.cap0);
+      }
     } else {
-      const long o = 3L * (-s - 1 + k) + d;
-      x[3L * a + d] = x_stage[o];
-      v[3L * a + d] = v_stage[o];
-      f[3L * a + d] = 0.0;
-      img[3L * a + d] = 0;
+      const long o = (long)(-s - 1) + k;
+      if (lane < 3) {
+        m.x2[3L * a + lane] = m.sx[3 * o + lane];
+        m.v2[3L * a + lane] = m.sv[3 * o + lane];
+        m.f2[3L * a + lane] = 0.0;
+        m.xb2[3L * a + lane] = m.sx[3 * o + lane];
+        m.img2[3L * a + lane] = 0;
+      } else if (lane == 3) {
+        m.elem2[a] = m.selem[o];
+      }
+      for (int b = lane; b < B1; b += 32) m.boff2[(long)a * B1 + b] = 0;
     }
   }
 }
 
-void launch_srv_gather(int n, const int *acell, const int *coff, const int *src,
-                       const double *x_old, const double *v_old, const double *f_old,
-                       const int *img_old, const double *x_stage, const double *v_stage,
-                       double *x, double *v, double *f, int *img, cudaStream_t st,
-                       long &launches) {
-  if (n <= 0) return;
-  k_srv_gather<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(
-      n, acell, coff, src, x_old, v_old, f_old, img_old, x_stage, v_stage, x, v, f, img);
+void launch_srv_move(const SrvMove &m, cudaStream_t st, long &launches) {
+  if (m.n <= 0) return;
+  long g = ((long)m.n * 32 + kThreads - 1) / kThreads;
+  if (g > 148 * 16) g = 148 * 16;
+  k_srv_move<<<(int)g, kThreads, 0, st>>>(m);
+  launches += 1;
+}
+
+__global__ void k_srv_acell(int ncells, const int *__restrict__ coff, int *__restrict__ acell) {
+  for (int c = blockIdx.x; c < ncells; c += gridDim.x)
+    for (int a = coff[c] + threadIdx.x; a < coff[c + 1]; a += blockDim.x) acell[a] = c;
+}
+
+void launch_srv_acell(int ncells, const int *coff, int *acell, cudaStream_t st,
+                      long &launches) {
+  if (ncells <= 0) return;
+  const int g = ncells < 148 * 16 ? ncells : 148 * 16;
+  k_srv_acell<<<g, kThreads, 0, st>>>(ncells, coff, acell);
+  launches += 1;
+}
+
+// One warp per cell: a ballot per 32 atoms and element places the cell's
+// atoms of each element at its slots in perm, in atom order.
+__global__ void k_srv_perm(int ncells, int B, const int *__restrict__ coff,
+                           const int *__restrict__ elem, const int *__restrict__ estart,
+                           int *__restrict__ perm) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncells; c += nw) {
+    const int a0 = coff[c], a1 = coff[c + 1];
+    for (int e = 0; e < B; e++) {
+      int pos = estart[(long)c * B + e];
+      for (int ab = a0; ab < a1; ab += 32) {
+        const int a = ab + lane;
+        const bool hit = a < a1 && elem[a] == e;
+        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) perm[pos + __popc(bal & below)] = a;
+        pos += __popc(bal);
+      }
+    }
+  }
+}
+
+void launch_srv_perm(int ncells, int B, const int *coff, const int *elem, const int *estart,
+                     int *perm, cudaStream_t st, long &launches) {
+  if (ncells <= 0) return;
+  long g = ((long)ncells * 32 + kThreads - 1) / kThreads;
+  if (g > 148 * 16) g = 148 * 16;
+  k_srv_perm<<<(int)g, kThreads, 0, st>>>(ncells, B, coff, elem, estart, perm);
+  launches += 1;
+}
+
+__global__ void k_srv_mark(int ncells, const int *__restrict__ fresh, int *__restrict__ cflag,
+                           int *flag) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x)
+    cflag[c] = fresh[c];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *flag = 1;
+}
+
+void launch_srv_mark(int ncells, const int *fresh, int *cflag, int *flag, cudaStream_t st,
+                     long &launches) {
+  int g = (ncells + kThreads - 1) / kThreads;
+  if (g > 148 * 8) g = 148 * 8;
+  if (g < 1) g = 1;
+  k_srv_mark<<<g, kThreads, 0, st>>>(ncells, fresh, cflag, flag);
   launches += 1;
 }
 

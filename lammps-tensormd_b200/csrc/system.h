@@ -140,7 +140,13 @@ void drop_graph(tmd_system *s);
 void box_setup(BoxP &b, const double bx[9], const int pbc[3]);
 void widths(const BoxP &b, double w[3]);
 int alloc_neighbors(tmd_system *s, int cap);
+// Take nbr/rev (natoms_cap x cap entries, filled on s->st) as the neighbor
+// rows and re-allocate the per-entry scratch arrays (tmp, pdf, pgeo) at cap.
+int adopt_rows(tmd_system *s, int cap, uint32_t *nbr, int *rev);
 int initial_cap(tmd_system *s);
+// Neighbor entries per atom for a number density (atoms / A^3): the atoms in
+// the (rc + skin) sphere with a 30% margin plus 32, at least 64.
+int cap_for_density(const tmd_system *s, double dens);
 int read_status(tmd_system *s);
 int clear_status(tmd_system *s);
 int rebuild_now(tmd_system *s);
@@ -161,6 +167,10 @@ int set_elements(tmd_system *s, int n, const int *elem);
 int cells_alloc(tmd_system *s, int max_cells);
 int cells_layout(tmd_system *s, int ncells, const int *natoms);
 int cells_geometry(tmd_system *s, const double *boxes, const int *pbc);
+// Box and image-shift range of one cell; TMD_ERR_ARG with the reason in `why`
+// for a degenerate box or one too small for the cutoff.
+int cell_setup(const tmd_system *s, const double bx[9], const int pbc[3], BoxP &b,
+               CellGeom &g, std::string &why);
 // Make sure s->thermo_d holds count doubles.
 int thermo_reserve(tmd_system *s, long count);
 // fix nvt parameters, one target ramp per thermostat group (cell or system).

@@ -94,7 +94,7 @@ struct MlpLayer {
 };
 struct MlpArgs {
   int nl, actfn, resnet, nin, maxh;
-  int tr;             // atoms per CTA (32 or 64)
+  int tr;             // atoms per tile (32 or 64 streamed, 64 or 128 resident)
   size_t smem;        // dynamic shared memory bytes
   int resident;       // > 0: resident-weight form, persistent grid of this many CTAs
   int ntiles;
@@ -108,9 +108,9 @@ struct MlpArgs {
 };
 void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches);
 size_t mlp_fp32_smem(int nl, const int *sizes, int tr);
-// Resident-weight form: shared memory per CTA and atoms per tile.
-size_t mlp_fp32r_smem(int nl, const int *sizes);
-int mlp_fp32r_tile();
+// Resident-weight form: shared memory per CTA for tiles of tr atoms (128
+// atoms on 512 threads, or 64 on 256 when the wider tile does not fit).
+size_t mlp_fp32r_smem(int nl, const int *sizes, int tr);
 void mlp_fp32_prepare(int tr, size_t smem, bool resident);
 
 // Tensor-core (tcgen05) MLP, BF16 operands.  Weights are packed on the host
@@ -244,11 +244,34 @@ struct CellCtl {
 // New layout of a server batch: atom a of new cell c comes from old atom
 // src[c] + (a - coff[c]) when src[c] >= 0, else from staging slot
 // -src[c] - 1 + (a - coff[c]) (new requests; image counters start at 0).
-void launch_srv_gather(int n, const int *acell, const int *coff, const int *src,
-                       const double *x_old, const double *v_old, const double *f_old,
-                       const int *img_old, const double *x_stage, const double *v_stage,
-                       double *x, double *v, double *f, int *img, cudaStream_t st,
-                       long &launches);
+// A moved cell keeps its neighbor list: rows (cap0 entries per atom in the
+// old arrays, cap1 in the new ones) are copied with their atom indices and
+// partner slots re-based to the new offsets, unless fresh[c] is set (the
+// cell is about to be rebuilt).
+struct SrvMove {
+  int n, B, cap0, cap1;
+  const int *acell, *coff, *src, *fresh;
+  const double *x, *v, *f, *xb;
+  const int *img, *elem, *boff, *rev;
+  const uint32_t *nbr;
+  const double *sx, *sv;
+  const int *selem;
+  double *x2, *v2, *f2, *xb2;
+  int *img2, *elem2, *boff2, *rev2;
+  uint32_t *nbr2;
+};
+void launch_srv_move(const SrvMove &m, cudaStream_t st, long &launches);
+// acell[a] = c for every atom of cell c.
+void launch_srv_acell(int ncells, const int *coff, int *acell, cudaStream_t st,
+                      long &launches);
+// MLP element grouping of a batch: perm lists the atoms of element 0 in cell
+// order, then element 1, ...; estart[c*B + e] is where cell c's atoms of
+// element e begin (the order a counting sort over all atoms gives).
+void launch_srv_perm(int ncells, int B, const int *coff, const int *elem, const int *estart,
+                     int *perm, cudaStream_t st, long &launches);
+// Rebuild request for the fresh cells: cflag[c] = fresh[c], *flag = 1.
+void launch_srv_mark(int ncells, const int *fresh, int *cflag, int *flag, cudaStream_t st,
+                     long &launches);
 // One serving step, before the force evaluation: FIRE power (F.v, v.v, F.F)
 // summed per cell, FIRE state update, then the position update of NVE (half
 // kick + drift) and FIRE (mix + semi-implicit Euler) cells.

@@ -10,7 +10,10 @@
   FIRE jobs          end with every |F_i| <= fmax and a lower energy
   concurrency        mixed jobs from several threads all complete; results
                      do not depend on what else was in flight
-  errors             unknown kind, job beyond the atom budget, wait timeout"""
+  mix independence   NVE and FIRE end states bitwise the same with other jobs
+                     retiring and entering around them
+  errors             unknown kind, job beyond the atom budget, box too small
+                     for the cutoff, wait timeout"""
 import threading
 
 import numpy as np
@@ -91,6 +94,42 @@ def test_nve_job_matches_system_run(model4):
     srv.close()
 
 
+def test_trajectory_independent_of_the_mix(model4):
+    """An NVE and a FIRE job give bitwise the same end state run together
+    and inside a batch whose other cells retire and are admitted while they
+    run (three cells at most in flight, so retirements move them and admit
+    queued jobs).  Moved cells keep their neighbor lists; a cell's list is rebuilt
+    only when its own atoms trigger it."""
+    rng = np.random.default_rng(6)
+    a = synth.serving_job(rng, kind=1, nmin=400, nmax=500)
+    fj = synth.serving_job(rng, kind=2, nmin=150, nmax=250)
+    fillers = [(int(k), synth.serving_job(rng, kind=int(k), nmin=50, nmax=700))
+               for k in (1, 0, 1, 2, 0, 1, 0, 1, 1, 0)]
+
+    def run(mixed):
+        srv = TensorMDServer(model4, max_atoms=100000, max_cells=3, steps_per_tick=4)
+        subs = [(1, a, 60), (2, fj, 80)]
+        if mixed:
+            subs = [(k, j, 5 + 7 * i) for i, (k, j) in enumerate(fillers[:3])] + subs[:1] \
+                + [(k, j, 3 + 5 * i) for i, (k, j) in enumerate(fillers[3:7])] + subs[1:] \
+                + [(k, j, 9 + 4 * i) for i, (k, j) in enumerate(fillers[7:])]
+        tks = [(k, nst, srv.submit(k, x, t, box, v=v, nsteps=max(nst, 1), dt=0.002, fmax=1e-4))
+               for k, (x, t, box, v), nst in subs]
+        outs = [srv.wait(tk, timeout=300) for _, _, tk in tks]
+        srv.close()
+        pick = [o for (k, nst, _), o in zip(tks, outs) if (k, nst) in ((1, 60), (2, 80))]
+        assert len(pick) == 2
+        return pick
+
+    alone, mixed = run(False), run(True)
+    for o1, o2 in zip(alone, mixed):
+        assert o1["steps"] == o2["steps"]
+        for key in ("x", "v", "f"):
+            assert np.array_equal(o1[key], o2[key]), key
+        assert o1["energy"] == o2["energy"]
+        assert np.array_equal(o1["virial"], o2["virial"])
+
+
 def test_fire_job_relaxes(model4):
     rng = np.random.default_rng(3)
     x, t, box, _ = synth.serving_job(rng, kind=2, nmin=100, nmax=200)
@@ -161,6 +200,14 @@ def test_server_errors(model4):
     with pytest.raises(TmdError) as e:
         srv.submit(0, big, tb, boxb)
     assert e.value.code == -4
+    # a periodic box too small for the cutoff (rc + skin = 7 A needs more
+    # than 3 images of a 2 A box) is refused at submit; the server goes on
+    tiny = np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0]])
+    with pytest.raises(TmdError) as e:
+        srv.submit(0, tiny, np.array([1, 1]), np.array([0, 0, 0, 2.0, 2.0, 2.0, 0, 0, 0]))
+    assert e.value.code == -1 and "cutoff" in str(e.value)
+    out = srv.wait(srv.submit(0, x, t, box), timeout=120)
+    assert np.isfinite(out["energy"])
     tk = srv.submit(1, x, t, box, nsteps=200000, dt=0.001)
     with pytest.raises(TmdError) as e:
         srv.wait(tk, timeout=0.0)
