@@ -4,14 +4,16 @@
 //
 // Cells are concatenated: atoms of cell c are coff[c]..coff[c+1]-1, every
 // atom records its cell, and a pair never leaves its cell (images are taken
-// in the cell's own box).  The neighbor build tests each atom against the
-// atoms of its cell under the image shifts that can reach the cutoff; the
-// descriptor, MLP, force and gather kernels are the single-system kernels
-// with the box read per atom.  Energies and virials are summed per cell in a
+// in the cell's own box).  The neighbor build bins every cell in its own grid
+// of fractional-coordinate bins and walks a stencil of bins and image shifts
+// around each atom; the descriptor, MLP, force and gather kernels are the
+// single-system kernels with the box read per atom.  Energies and virials are summed per cell in a
 // fixed order.  The reference evaluates one LAMMPS system per process
 // (pair_tensormd.cpp:141-184); a batch of C cells gives the same per-cell
 // results as C separate systems.
+#include <algorithm>
 #include <cmath>
+#include <string>
 #include <vector>
 
 #include "system.h"
@@ -87,16 +89,50 @@ int cell_setup(const tmd_system *s, const double bx[9], const int pbc[3], BoxP &
   return TMD_OK;
 }
 
+void cell_bins(const BoxP &b, int natoms, double cut, CellGeom &g) {
+  // bins slightly wider than cut/2 (as the single-box grid), at most about
+  // two per atom so a sparse cell does not hold a large empty grid
+  for (int a = 0; a < 3; a++) {
+    int nb = (int)std::floor(g.w[a] / (0.5 * cut * (1.0 + 1e-6)));
+    g.nb[a] = std::max(1, std::min(nb, 1024));
+  }
+  const long most = std::max(8L, 2L * natoms);
+  while ((long)g.nb[0] * g.nb[1] * g.nb[2] > most) {
+    const int a = (g.nb[0] >= g.nb[1] && g.nb[0] >= g.nb[2]) ? 0 : (g.nb[1] >= g.nb[2] ? 1 : 2);
+    g.nb[a] = (g.nb[a] + 1) / 2;
+  }
+  for (int a = 0; a < 3; a++) {
+    int ns = (int)std::ceil(cut * (1.0 + 1e-9) / (g.w[a] / g.nb[a]));
+    if (!b.pbc[a] && ns > g.nb[a]) ns = g.nb[a];
+    g.ns[a] = std::max(ns, 1);
+  }
+}
+
 int cells_geometry(tmd_system *s, const double *boxes, const int *pbc) {
   const int C = s->ncells;
+  const double cut = s->m->h.rmax + s->skin;
   std::vector<BoxP> hb(C);
   std::vector<CellGeom> hg(C);
   std::string why;
+  long nbins = 0;
   for (int c = 0; c < C; c++) {
     int rc = cell_setup(s, boxes + 9 * (size_t)c, pbc + 3 * (size_t)c, hb[c], hg[c], why);
     if (rc) return fail(rc, "cell " + std::to_string(c) + ": " + why);
+    cell_bins(hb[c], s->h_coff[c + 1] - s->h_coff[c], cut, hg[c]);
+    hg[c].bin0 = (int)nbins;
+    nbins += (long)hg[c].nb[0] * hg[c].nb[1] * hg[c].nb[2];
   }
+  if (nbins > (1L << 30)) return fail(TMD_ERR_CAPACITY, "too many neighbor bins");
   drop_graph(s);
+  if (nbins > s->ncell_alloc) {
+    dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_cursor);
+    s->ncell_alloc = 0;
+    TMD_CUDA(dalloc(&s->cell_count, nbins));
+    TMD_CUDA(dalloc(&s->cell_start, nbins + 1));
+    TMD_CUDA(dalloc(&s->cell_cursor, nbins));
+    s->ncell_alloc = (int)nbins;
+  }
+  s->nbins = (int)nbins;
   TMD_CUDA(cudaMemcpyAsync(s->cbox, hb.data(), C * sizeof(BoxP), cudaMemcpyHostToDevice, s->st));
   TMD_CUDA(cudaMemcpyAsync(s->cgeom, hg.data(), C * sizeof(CellGeom), cudaMemcpyHostToDevice,
                            s->st));

@@ -340,82 +340,235 @@ __global__ void k_nb_build(int n, const double *__restrict__ x, BoxP box,
 // ---------------------------------------------------------------------
 // Multi-cell batches: many small periodic cells, each in its own box.  Atoms
 // of cell c are coff[c]..coff[c+1]-1 and see only atoms of their own cell
-// and its images.  Cells hold a few hundred atoms, so instead of bins each
-// atom tests every atom of its cell under every image shift that can reach
-// the cutoff.  A shift s on axis a is skipped when the slab of fractional
-// coordinates [s, s + 1) lies farther than cut from atom i along a: the
-// distance between planes of constant fractional coordinate is |df_a| w_a
-// (w_a = perpendicular width), a lower bound of the true distance.  The
-// kept set is the same (j, shift) set as the binned build, with the same
-// FP64 image construction and no-FMA rsq.
+// and its images.  Every cell has its own grid of bins in fractional
+// coordinates (CellGeom: nb bins per axis, at least cut/2 wide, a +-ns
+// stencil reaching the cutoff); the bins of all cells share one set of bin
+// arrays, cell c's from bin0.  A stencil bin beyond the grid is a bin of an
+// image (shift = floor division by nb), so a cell narrower than the cutoff
+// is walked under every image shift that can reach it.  The kept set is the
+// same (j, shift) set as the single-box binned build, with the same FP64
+// image construction and no-FMA rsq.  Only cells flagged for a rebuild are
+// zeroed, binned, scanned, sorted and walked: a cell's binned atoms occupy
+// its own atom range coff[c].., so the scan runs per cell, and a bin's atoms
+// are cell_atoms[cell_start[b] .. cell_cursor[b]) once the fill has advanced
+// the cursors (the next bin's start may belong to a cell left as it was).
 // ---------------------------------------------------------------------
-__global__ void k_nbc_wrap(int n, double *__restrict__ x, int *__restrict__ image,
-                           const BoxP *__restrict__ cbox, const int *__restrict__ acell,
-                           const int *__restrict__ cflag, int *status, const int *flag) {
+__device__ inline bool nbc_cell_flagged(const int *flag, const int *__restrict__ cflag, int c) {
+  return (*flag & 2) || cflag[c];
+}
+
+__device__ inline int nbc_cell_bins(const CellGeom &g) { return g.nb[0] * g.nb[1] * g.nb[2]; }
+
+// One block per flagged cell: zero its bin counts.
+__global__ void k_nbc_zero(int ncells, const CellGeom *__restrict__ cgeom,
+                           const int *__restrict__ cflag, int *__restrict__ cell_count,
+                           const int *flag) {
+  if (!*flag) return;
+  for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
+    if (!nbc_cell_flagged(flag, cflag, c)) continue;
+    const CellGeom &g = cgeom[c];
+    const int nbc = nbc_cell_bins(g);
+    for (int b = threadIdx.x; b < nbc; b += blockDim.x) cell_count[g.bin0 + b] = 0;
+  }
+}
+
+// One warp per flagged cell: exclusive scan of its bin counts from coff[c].
+__global__ void k_nbc_scan(int ncells, const CellGeom *__restrict__ cgeom,
+                           const int *__restrict__ coff, const int *__restrict__ cflag,
+                           const int *__restrict__ cell_count, int *__restrict__ cell_start,
+                           int *__restrict__ cell_cursor, const int *flag) {
+  if (!*flag) return;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncells; c += nw) {
+    if (!nbc_cell_flagged(flag, cflag, c)) continue;
+    const CellGeom &g = cgeom[c];
+    const int nbc = nbc_cell_bins(g);
+    int base = coff[c];
+    for (int b0 = 0; b0 < nbc; b0 += 32) {
+      const int b = b0 + lane;
+      const int v = b < nbc ? cell_count[g.bin0 + b] : 0;
+      int incl = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (b < nbc) {
+        cell_start[g.bin0 + b] = base + incl - v;
+        cell_cursor[g.bin0 + b] = base + incl - v;
+      }
+      base += __shfl_sync(0xffffffffu, incl, 31);
+    }
+  }
+}
+
+// One block per flagged cell, a thread per bin: order each bin's atoms by
+// index so the build is deterministic.
+__global__ void k_nbc_cellsort(int ncells, const CellGeom *__restrict__ cgeom,
+                               const int *__restrict__ cflag,
+                               const int *__restrict__ cell_start,
+                               const int *__restrict__ cell_cursor,
+                               int *__restrict__ cell_atoms, const int *flag) {
+  if (!*flag) return;
+  for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
+    if (!nbc_cell_flagged(flag, cflag, c)) continue;
+    const CellGeom &g = cgeom[c];
+    const int nbc = nbc_cell_bins(g);
+    for (int b = threadIdx.x; b < nbc; b += blockDim.x) {
+      const int s0 = cell_start[g.bin0 + b], s1 = cell_cursor[g.bin0 + b];
+      for (int a = s0 + 1; a < s1; a++) {
+        const int v = cell_atoms[a];
+        int q = a - 1;
+        while (q >= s0 && cell_atoms[q] > v) {
+          cell_atoms[q + 1] = cell_atoms[q];
+          q--;
+        }
+        cell_atoms[q + 1] = v;
+      }
+    }
+  }
+}
+
+__global__ void k_nbc_bin(int n, double *__restrict__ x, int *__restrict__ image,
+                          const BoxP *__restrict__ cbox, const CellGeom *__restrict__ cgeom,
+                          const int *__restrict__ acell, const int *__restrict__ cflag,
+                          int *__restrict__ cell_of, int *__restrict__ cell_count,
+                          int *status, const int *flag) {
   if (!*flag) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
     if (!nb_rebuild(flag, cflag, acell, i)) continue;
-    const BoxP &box = cbox[acell[i]];
+    const int c = acell[i];
+    const BoxP &box = cbox[c];
+    const CellGeom &g = cgeom[c];
     double px, py, pz, f[3];
     wrap_atom(box, i, x, image, px, py, pz);
     frac_of(box, px, py, pz, f[0], f[1], f[2]);
-    for (int a = 0; a < 3; a++)
+    int q[3];
+    for (int a = 0; a < 3; a++) {
       if (!box.pbc[a] && (f[a] < 0.0 || f[a] > 1.0)) atomicOr(status, kStatusOutside);
+      int v = (int)floor(f[a] * g.nb[a]);
+      q[a] = v < 0 ? 0 : (v >= g.nb[a] ? g.nb[a] - 1 : v);
+    }
+    const int bin = g.bin0 + (q[2] * g.nb[1] + q[1]) * g.nb[0] + q[0];
+    cell_of[i] = bin;
+    atomicAdd(&cell_count[bin], 1);
   }
 }
 
-// One warp per atom; entries in (shift, j) order, compacted with a ballot.
+__global__ void k_nbc_fill(int n, const int *__restrict__ cell_of,
+                           const int *__restrict__ acell, const int *__restrict__ cflag,
+                           int *__restrict__ cell_cursor, int *__restrict__ cell_atoms,
+                           const int *flag) {
+  if (!*flag) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    if (!nb_rebuild(flag, cflag, acell, i)) continue;
+    const int pos = atomicAdd(&cell_cursor[cell_of[i]], 1);
+    cell_atoms[pos] = i;
+  }
+}
+
+// One warp per atom, lanes over the stencil bins with per-lane keep buffers
+// (as k_nb_build), the box and grid of the atom's cell.
 __global__ void k_nbc_build(int n, const double *__restrict__ x,
                             const BoxP *__restrict__ cbox,
                             const CellGeom *__restrict__ cgeom,
-                            const int *__restrict__ acell, const int *__restrict__ coff,
-                            double cut, double cutsq, int cap, uint32_t *__restrict__ tmp,
-                            int *__restrict__ nraw, int *status, int *maxneed,
-                            const int *__restrict__ cflag, const int *flag) {
+                            const int *__restrict__ acell, const int *__restrict__ cell_of,
+                            const int *__restrict__ cell_start,
+                            const int *__restrict__ cell_end,
+                            const int *__restrict__ cell_atoms, double cutsq, int cap,
+                            uint32_t *__restrict__ tmp, int *__restrict__ nraw, int *status,
+                            int *maxneed, const int *__restrict__ cflag, const int *flag) {
   if (!*flag) return;
+  extern __shared__ uint32_t nb_keep[];
+  {
+    uint32_t dyn;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    if (dyn < sizeof(uint32_t) * blockDim.x * kNbKeepStride) {
+      if (threadIdx.x == 0) atomicOr(status, kStatusLaunch);
+      return;
+    }
+  }
   const int lane = threadIdx.x & 31;
+  uint32_t *keep = nb_keep + (size_t)threadIdx.x * kNbKeepStride;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
     if (!nb_rebuild(flag, cflag, acell, i)) continue;
-    const int c = acell[i];
-    const BoxP &box = cbox[c];
-    const CellGeom &cg = cgeom[c];
-    const int j0 = coff[c], j1 = coff[c + 1];
+    const int cidx = acell[i];
+    const BoxP &box = cbox[cidx];
+    const CellGeom &g = cgeom[cidx];
     const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
-    double fi[3];
-    frac_of(box, xi, yi, zi, fi[0], fi[1], fi[2]);
-    // shift range per axis: keep s unless the slab [s, s+1) is beyond cut
-    int lo[3], hi[3];
-    const double reach = cut * (1.0 + 1e-9), eps = 1e-6;
-    for (int a = 0; a < 3; a++) {
-      lo[a] = 0; hi[a] = 0;
-      if (!box.pbc[a]) continue;
-      lo[a] = -cg.m[a]; hi[a] = cg.m[a];
-      while (lo[a] < 0 && (fi[a] - (lo[a] + 1) - eps) * cg.w[a] > reach) lo[a]++;
-      while (hi[a] > 0 && (hi[a] - fi[a] - eps) * cg.w[a] > reach) hi[a]--;
-    }
-    uint32_t *row = tmp + (size_t)i * cap;
+    const int ci = cell_of[i] - g.bin0;
+    const int cx = ci % g.nb[0], cy = (ci / g.nb[0]) % g.nb[1], cz = ci / (g.nb[0] * g.nb[1]);
+    const int wx = 2 * g.ns[0] + 1, wy = 2 * g.ns[1] + 1, wz = 2 * g.ns[2] + 1;
+    const int S = wx * wy * wz;
     int out = 0;
-    for (int sz = lo[2]; sz <= hi[2]; sz++)
-      for (int sy = lo[1]; sy <= hi[1]; sy++)
-        for (int sx = lo[0]; sx <= hi[0]; sx++) {
-          const bool self_img = (sx == 0 && sy == 0 && sz == 0);
-          const int code = shift_code(sx, sy, sz);
-          for (int jb = j0; jb < j1; jb += 32) {
-            const int j = jb + lane;
-            bool hit = false;
-            if (j < j1 && !(self_img && j == i)) {
-              double gx, gy, gz;
-              image_of(box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sx, sy, sz, gx, gy, gz);
-              hit = rsq_nofma(xi - gx, yi - gy, zi - gz) <= cutsq;
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            const int pos = out + __popc(bal & ((1u << lane) - 1u));
-            if (hit && pos < cap) row[pos] = nb_pack(j, code);
-            out += __popc(bal);
+    uint32_t *row = tmp + (size_t)i * cap;
+    for (int base = 0; base < S; base += 32) {
+      const int sidx = base + lane;
+      int c = -1, sh[3] = {0, 0, 0};
+      if (sidx < S) {
+        const int o[3] = {sidx % wx - g.ns[0], (sidx / wx) % wy - g.ns[1],
+                          sidx / (wx * wy) - g.ns[2]};
+        const int cc[3] = {cx + o[0], cy + o[1], cz + o[2]};
+        int w3[3];
+        bool ok = true;
+        for (int a = 0; a < 3; a++) {
+          const int q = cc[a], nb = g.nb[a];
+          const int sa = q >= 0 ? q / nb : -((-q + nb - 1) / nb);
+          w3[a] = q - sa * nb;
+          sh[a] = sa;
+          if (!box.pbc[a] && sa != 0) ok = false;
+          if (sa > kShiftR || sa < -kShiftR) {
+            ok = false;
+            atomicOr(status, kStatusShift);
           }
         }
+        if (ok) c = g.bin0 + (w3[2] * g.nb[1] + w3[1]) * g.nb[0] + w3[0];
+      }
+      int cnt = 0, a0 = 0, a1 = 0;
+      if (c >= 0) {
+        a0 = cell_start[c];
+        a1 = cell_end[c];
+      }
+      const bool self_img = (sh[0] == 0 && sh[1] == 0 && sh[2] == 0);
+      const int code = shift_code(sh[0], sh[1], sh[2]);
+      for (int p = a0; p < a1; p++) {
+        const int j = cell_atoms[p];
+        if (j == i && self_img) continue;
+        double gx, gy, gz;
+        image_of(box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sh[0], sh[1], sh[2], gx, gy, gz);
+        if (rsq_nofma(xi - gx, yi - gy, zi - gz) <= cutsq) {
+          if (cnt < kNbKeep) keep[cnt] = nb_pack(j, code);
+          cnt++;
+        }
+      }
+      int incl = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      int pos = out + incl - cnt;
+      if (cnt > 0 && cnt <= kNbKeep) {
+        for (int q = 0; q < cnt; q++)
+          if (pos + q < cap) row[pos + q] = keep[q];
+      } else if (cnt > kNbKeep) {
+        for (int p = a0; p < a1; p++) {
+          const int j = cell_atoms[p];
+          if (j == i && self_img) continue;
+          double gx, gy, gz;
+          image_of(box, x[3 * j], x[3 * j + 1], x[3 * j + 2], sh[0], sh[1], sh[2], gx, gy,
+                   gz);
+          if (rsq_nofma(xi - gx, yi - gy, zi - gz) <= cutsq) {
+            if (pos < cap) row[pos] = nb_pack(j, code);
+            pos++;
+          }
+        }
+      }
+      out += total;
+    }
     if (lane == 0) {
       nraw[i] = out;
       if (out > cap) {
@@ -622,12 +775,21 @@ void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
   int gn = cap_grid((a.n + T - 1) / T);
   int gw = cap_grid(((long)a.n * 32 + T - 1) / T);
   if (a.ncells > 0) {
-    k_nbc_wrap<<<gn, T, 0, st>>>(a.n, a.x, a.image, a.cbox, a.acell, a.cflag, a.status,
-                                 a.flag);
-    k_nbc_build<<<gw, T, 0, st>>>(a.n, a.x, a.cbox, a.cgeom, a.acell, a.coff,
-                                  std::sqrt(a.cutsq), a.cutsq, a.cap, a.tmp, a.nraw,
-                                  a.status, a.maxneed, a.cflag, a.flag);
-    launches += 2;
+    const int gc = cap_grid(a.ncells);
+    const int gcw = cap_grid(((long)a.ncells * 32 + T - 1) / T);
+    k_nbc_zero<<<gc, T, 0, st>>>(a.ncells, a.cgeom, a.cflag, a.cell_count, a.flag);
+    k_nbc_bin<<<gn, T, 0, st>>>(a.n, a.x, a.image, a.cbox, a.cgeom, a.acell, a.cflag,
+                                a.cell_of, a.cell_count, a.status, a.flag);
+    k_nbc_scan<<<gcw, T, 0, st>>>(a.ncells, a.cgeom, a.coff, a.cflag, a.cell_count,
+                                  a.cell_start, a.cell_cursor, a.flag);
+    k_nbc_fill<<<gn, T, 0, st>>>(a.n, a.cell_of, a.acell, a.cflag, a.cell_cursor,
+                                 a.cell_atoms, a.flag);
+    k_nbc_cellsort<<<gc, T, 0, st>>>(a.ncells, a.cgeom, a.cflag, a.cell_start, a.cell_cursor,
+                                     a.cell_atoms, a.flag);
+    k_nbc_build<<<gw, T, nb_build_smem(T), st>>>(
+        a.n, a.x, a.cbox, a.cgeom, a.acell, a.cell_of, a.cell_start, a.cell_cursor,
+        a.cell_atoms, a.cutsq, a.cap, a.tmp, a.nraw, a.status, a.maxneed, a.cflag, a.flag);
+    launches += 6;
   } else {
     int gc = cap_grid((a.bin.ncell + T - 1) / T);
     k_nb_zero<<<gc, T, 0, st>>>(a.bin.ncell, a.cell_count, a.flag);

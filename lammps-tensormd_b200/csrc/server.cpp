@@ -255,10 +255,10 @@ int relayout(tmd_server *sv, const std::vector<JobP> &next) {
       cur[e] += next[c]->ecount[e];
     }
   s->ncells = C;
-  int rc = cells_geometry(s, boxes.data(), pbc.data());
-  if (rc) return rc;
   s->h_coff = coff;
   s->h_acell.clear();
+  int rc = cells_geometry(s, boxes.data(), pbc.data());
+  if (rc) return rc;
   TMD_CUDA(cudaMemcpyAsync(s->coff, coff.data(), (C + 1) * sizeof(int), cudaMemcpyHostToDevice,
                            s->st));
   TMD_CUDA(cudaMemcpyAsync(sv->src, srcv.data(), C * sizeof(int), cudaMemcpyHostToDevice,

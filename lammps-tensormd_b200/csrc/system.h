@@ -52,6 +52,7 @@ struct tmd_system {
   // multi-cell batch (ncells > 0): cell c holds atoms coff[c]..coff[c+1]-1
   // in its own periodic box; box/bin above are unused
   int ncells = 0, max_cells = 0;
+  int nbins = 0;  // neighbor bins of all cells (CellGeom::bin0 numbering)
   std::vector<int> h_coff, h_acell;
   std::vector<tmd::BoxP> h_cbox;
   tmd::BoxP *cbox = nullptr;
@@ -166,6 +167,7 @@ int set_elements(tmd_system *s, int n, const int *elem);
 // cell layout (atoms per cell, concatenated), per-cell boxes.
 int cells_alloc(tmd_system *s, int max_cells);
 int cells_layout(tmd_system *s, int ncells, const int *natoms);
+// Needs ncells and h_coff of the layout (bins per cell scale with its atoms).
 int cells_geometry(tmd_system *s, const double *boxes, const int *pbc);
 // Box and image-shift range of one cell; TMD_ERR_ARG with the reason in `why`
 // for a degenerate box or one too small for the cutoff.

@@ -13,12 +13,16 @@ constexpr int kStatusNonfinite = 8;  // NaN/Inf energy or force
 constexpr int kStatusTimeout = 16;   // a bounded device wait gave up
 constexpr int kStatusLaunch = 32;    // a kernel launched without its shared memory
 
-// Per-cell constants of the multi-cell neighbor build: perpendicular widths
-// and the largest image shift per axis (0 on non-periodic axes).
+// Per-cell constants of the multi-cell neighbor build: perpendicular widths,
+// the largest image shift per axis (0 on non-periodic axes) and the cell's
+// grid of bins in fractional coordinates: nb bins per axis, a +-ns stencil
+// reaching the cutoff, bins numbered from bin0 in the batch-wide bin arrays.
 struct CellGeom {
   double w[3];
   int m[3];
-  int pad;
+  int nb[3];
+  int ns[3];
+  int bin0;
 };
 
 struct NbArgs {
@@ -35,7 +39,7 @@ struct NbArgs {
   int *nraw;
   uint32_t *nbr;
   // multi-cell mode (ncells > 0): atoms of cell c are coff[c]..coff[c+1]-1,
-  // each cell periodic in its own box; bins are not used
+  // each cell periodic in its own box with its own bins (CellGeom)
   int ncells;
   const BoxP *cbox;
   const CellGeom *cgeom;
