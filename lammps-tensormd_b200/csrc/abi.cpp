@@ -334,6 +334,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
     ta.np = m->tc_np;
     ta.persistent = m->tc_persistent; ta.smem_p = m->tc_smem_p;
     ta.dz_bf16_p = m->tc_dz_bf16_p ? 1 : 0;
+    ta.streamed = m->tc_streamed; ta.smem_s = m->tc_smem_s; ta.stages = m->tc_stages;
     if (m->tc_fp8) launch_mlp_fp8(ta, s->st, s->launches);
     else launch_mlp_tc(ta, s->st, s->launches);
   } else {
@@ -836,6 +837,15 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
         m->tc_smem_p = sp;
         m->tc_dz_bf16_p = dzb;
         mlp_tcp_prepare(sp, np, dzb);
+      }
+      // weights too large to stay resident: the streamed-weight form
+      int stages = 0;
+      const size_t ss = mlp_tcs_smem(h.nl, h.sizes.data(), h.resnet, np, &stages);
+      if (m->tc_persistent == 0 && ss > 0 && nsm > 0) {
+        m->tc_streamed = nsm;
+        m->tc_smem_s = ss;
+        m->tc_stages = stages;
+        mlp_tcs_prepare(ss, np);
       }
     }
     m->mlp_tr = 128;

@@ -538,6 +538,452 @@ k_mlp_tcp(MlpTcArgs a) {
                  "r"(TMEM_COLS));
 }
 
+// ---------------------------------------------------------------------------
+// Streamed-weight persistent form for MLPs whose weights do not fit in shared
+// memory (e.g. 512-128-128-128 per element with four elements: 393 KB of
+// BF16 W^T and W blocks per element).  One CTA of 256 threads per SM walks
+// the tiles with a grid stride.  The weight chunks every tile needs (64
+// reduction columns x the GEMM's rows, contiguous in the packed blocks) are a
+// fixed schedule; thread 0 streams them from global memory (L2-resident)
+// into a ring of S shared-memory stages with cp.async.bulk copies that
+// complete on a per-stage mbarrier, up to S - 1 chunks ahead of the MMAs and
+// across layer and tile boundaries, and issues every MMA; a tcgen05.commit
+// per chunk frees its stage.  The G tile is converted to BF16 in 64-column
+// chunks by all threads into two slots (written while the previous chunk's
+// MMAs run), which alias the activation buffer of the hidden layers.  act'
+// of the hidden layers stays in tensor memory (tcgen05.st) next to the
+// accumulator: TMEM columns [0, accw) accumulate, then one block of act'
+// columns per hidden layer; the final dE/dG GEMM (nin output columns) runs in
+// 128-column blocks, up to four at a time, over all 512 columns once every
+// act' has been used.  The epilogue thread mapping, operand writes, bounded
+// waits and error path are those of k_mlp_tcp; on an error thread 0 also
+// waits (bounded) for the copies still in flight before TMEM is released.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kTcsThreads = 512;
+constexpr int kTcsParts = kTcsThreads / 128;  // threads per tile row (column parts)
+constexpr int kTcsMaxChunks = 192;
+constexpr int kTcsMaxBias = 512;
+constexpr int kTcsMaxStages = 8;
+constexpr int kTcsTmemCols = 512;
+
+struct TcsChunk {  // one weight chunk of the per-tile schedule
+  short l, dir, c, n0, nrows;
+};
+
+__device__ inline void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+      "[%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+__device__ inline void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+__device__ inline void tmem_st32(uint32_t taddr, const float v[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+      "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(
+          taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15])), "r"(__float_as_uint(v[16])), "r"(__float_as_uint(v[17])),
+      "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])), "r"(__float_as_uint(v[20])),
+      "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])), "r"(__float_as_uint(v[23])),
+      "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])), "r"(__float_as_uint(v[26])),
+      "r"(__float_as_uint(v[27])), "r"(__float_as_uint(v[28])), "r"(__float_as_uint(v[29])),
+      "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
+      : "memory");
+}
+
+// Shared-memory plan of the streamed form: elements (BF16) of one stage and
+// of the operand region (per hi/lo part), TMEM accumulator width.
+struct TcsPlan {
+  int maxrows, stage_elems, a_elems, accw;
+};
+__host__ __device__ inline TcsPlan tcs_plan(int nin, int maxh, int nb) {
+  TcsPlan p;
+  p.maxrows = maxh > 128 ? maxh : 128;
+  p.stage_elems = nb * p.maxrows * KCH;
+  const int g2 = 2 * TM * KCH, h = TM * maxh;
+  p.a_elems = g2 > h ? g2 : h;
+  p.accw = p.maxrows;
+  (void)nin;
+  return p;
+}
+}  // namespace
+
+template <int NP>
+__global__ void __launch_bounds__(kTcsThreads, 1)
+k_mlp_tcs(MlpTcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  __shared__ __align__(8) uint64_t full_b[kTcsMaxStages], empty_b[kTcsMaxStages], gbar[2],
+      accb[4], drainb;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int rows_s[TM];
+  __shared__ double epart[kTcsParts][TM];
+  __shared__ TcsChunk sched[kTcsMaxChunks];
+  __shared__ int nq_s, sz_s[kMaxLayers + 1], act_s[kMaxLayers], bo_s[kMaxLayers];
+  __shared__ float bias_s[kTcsMaxBias];   // hidden biases of the current element
+  __shared__ double wout_s[256];          // its output-layer weights
+  typedef __nv_bfloat16 T;
+  constexpr int NB = NP == 3 ? 2 : 1;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quad = warp & 3, part = warp >> 2;
+  const int row = quad * 32 + lane;
+  const int L = a.nl, nin = a.nin, maxh = a.maxh, S = a.stages;
+  const TcsPlan pl = tcs_plan(nin, maxh, NB);
+  T *stage0 = reinterpret_cast<T *>(smraw);
+  T *abuf = stage0 + (size_t)S * pl.stage_elems;
+  const uint64_t a_lo_u = (uint64_t)(((size_t)pl.a_elems * 2) >> 4);  // lo part, 16-B units
+  const uint64_t b_lo_u = (uint64_t)(((size_t)pl.maxrows * KCH * 2) >> 4);
+
+  if (tid == 0) {
+    // layer widths, act' TMEM columns and bias offsets per hidden layer
+    sz_s[0] = nin;
+    for (int l = 0; l < L; l++) sz_s[l + 1] = a.layers[l].N;
+    int o = pl.accw, ob = 0;
+    for (int l = 0; l < L - 1; l++) {
+      act_s[l] = o;
+      bo_s[l] = ob;
+      o += sz_s[l + 1];
+      ob += sz_s[l + 1];
+    }
+    const int *sizes = sz_s;
+    int k = 0;
+    for (int l = 0; l < L - 1; l++)
+      for (int c = 0; c < sizes[l] / KCH; c++)
+        sched[k++] = TcsChunk{(short)l, 0, (short)c, 0, (short)sizes[l + 1]};
+    for (int l = L - 2; l >= 1; l--)
+      for (int c = 0; c < sizes[l + 1] / KCH; c++)
+        sched[k++] = TcsChunk{(short)l, 1, (short)c, 0, (short)sizes[l]};
+    for (int n0 = 0; n0 < sizes[0]; n0 += 128)
+      for (int c = 0; c < sizes[1] / KCH; c++)
+        sched[k++] = TcsChunk{0, 1, (short)c, (short)n0, (short)min(128, sizes[0] - n0)};
+    nq_s = k;
+    for (int s = 0; s < S; s++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full_b[s])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty_b[s])));
+    }
+    for (int j = 0; j < 2; j++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&gbar[j])));
+    for (int j = 0; j < 4; j++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accb[j])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&drainb)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(kTcsTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16);
+  const int nq = nq_s;
+  const int *sizes = sz_s;
+  const int ntile_cta =
+      blockIdx.x < a.ntiles ? (a.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  const int q_end = ntile_cta * nq;
+  int q_issue = 0, q_mma = 0;  // thread 0: next chunk to copy / to multiply
+  bool ok0 = true;             // thread 0: its own waits
+  bool ok = true;
+  uint32_t gk[2] = {0, 0}, ak[4] = {0, 0, 0, 0};  // completions consumed per barrier
+
+  // thread 0: copy chunks up to (not including) qlim into their stages
+  auto issue_to = [&](int qlim) {
+    while (ok0 && q_issue < qlim && q_issue < q_end) {
+      const int s = q_issue % S;
+      if (q_issue >= S && !mbar_wait(&empty_b[s], (uint32_t)((q_issue / S) - 1) & 1u)) {
+        ok0 = false;
+        break;
+      }
+      const int t = blockIdx.x + (q_issue / nq) * gridDim.x;
+      const TcsChunk ch = sched[q_issue % nq];
+      const MlpTcLayer &ly = a.layers[(size_t)a.tiles[3 * t] * L + ch.l];
+      const int K = sizes[ch.l], N = sizes[ch.l + 1];
+      const int brows = ch.dir ? K : N;
+      const T *src = reinterpret_cast<const T *>(ch.dir ? ly.Wb : ly.Wf) +
+                     ((size_t)ch.c * brows + ch.n0) * KCH;
+      const uint32_t bytes = (uint32_t)ch.nrows * KCH * 2;
+      const uint32_t bar = smem_u32(&full_b[s]);
+      T *dst = stage0 + (size_t)s * pl.stage_elems;
+      mbar_expect_tx(bar, bytes * NB);
+      bulk_g2s(smem_u32(dst), src, bytes, bar);
+      if (NP == 3) bulk_g2s(smem_u32(dst + (size_t)pl.maxrows * KCH), src + (size_t)K * N, bytes, bar);
+      q_issue++;
+    }
+  };
+  // thread 0: the MMAs of the next chunk into TMEM column tcol; A at a_addr
+  // (hi part) with 8-row group stride a_sbo bytes
+  auto mma_next = [&](uint32_t a_addr, uint32_t a_sbo, uint32_t tcol, bool first) {
+    if (!ok0) return;
+    const int q = q_mma;
+    const int s = q % S;
+    if (!mbar_wait(&full_b[s], (uint32_t)(q / S) & 1u)) {
+      ok0 = false;
+      return;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const TcsChunk ch = sched[q % nq];
+    const uint32_t id = idesc_bf16(ch.nrows);
+    const uint32_t bbase = smem_u32(stage0 + (size_t)s * pl.stage_elems);
+#pragma unroll
+    for (int ks = 0; ks < KCH / KSTEP; ks++) {
+      const uint64_t da = sdesc(a_addr + (uint32_t)(ks * KSTEP / EPC) * 128u, 128u, a_sbo);
+      const uint64_t db = sdesc(bbase + (uint32_t)(ks * KSTEP / EPC) * 128u, 128u,
+                                (uint32_t)(KCH / EPC) * 128u);
+      mma_bf16(tmem + tcol, da, db, id, (!first || ks > 0) ? 1u : 0u);
+      if (NP == 3) {
+        mma_bf16(tmem + tcol, da, db + b_lo_u, id, 1u);  // hi * lo'
+        mma_bf16(tmem + tcol, da + a_lo_u, db, id, 1u);  // lo * hi'
+      }
+    }
+    commit(&empty_b[s]);
+    q_mma++;
+    issue_to(q_mma + S - 1);
+  };
+  // every thread: wait for completion number k of barrier b (bounded)
+  auto wait_all = [&](uint64_t *b, uint32_t &k) {
+    const bool done = mbar_wait(b, k & 1u);
+    k++;
+    ok = __syncthreads_and((done && ok && (tid != 0 || ok0)) ? 1 : 0) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+  };
+  auto publish = [&]() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    ok = __syncthreads_and((ok && (tid != 0 || ok0)) ? 1 : 0) != 0;
+  };
+  const uint32_t a_sbo_h = (uint32_t)(maxh / EPC) * 128u;   // activation buffer
+  const uint32_t a_sbo_g = (uint32_t)(KCH / EPC) * 128u;    // G chunk slot
+  const uint32_t abase = smem_u32(abuf);
+
+  int cur_elt = -1;
+  if (tid == 0) issue_to(S - 1);
+  for (int tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x) {
+    const int elt = a.tiles[3 * tile], start = a.tiles[3 * tile + 1],
+              count = a.tiles[3 * tile + 2];
+    const MlpTcLayer *Ls = a.layers + (size_t)elt * L;
+    if (tid < TM) rows_s[tid] = tid < count ? a.perm[start + tid] : -1;
+    if (elt != cur_elt) {  // the element's biases and output weights
+      cur_elt = elt;
+      for (int l = 0; l < L - 1; l++)
+        for (int c = tid; c < sizes[l + 1]; c += kTcsThreads)
+          bias_s[bo_s[l] + c] = __ldg(Ls[l].b + c);
+      for (int c = tid; c < sizes[L - 1]; c += kTcsThreads) wout_s[c] = __ldg(Ls[L - 1].wd + c);
+    }
+    __syncthreads();
+    const int row_atom = rows_s[row];
+
+    // ---------------- layer 0: G chunks through two slots ----------------
+    for (int c = 0; c < nin / KCH && ok; c++) {
+      const int slot = c & 1;
+      T *gs = abuf + (size_t)slot * TM * KCH;
+      if (c >= 2) wait_all(&gbar[slot], gk[slot]);  // the MMAs of chunk c - 2 are done
+      if (!ok) break;
+      for (int idx = tid; idx < TM * (KCH / 8); idx += kTcsThreads) {
+        const int r = idx / (KCH / 8), k8 = idx - r * (KCH / 8);
+        const int at = rows_s[r];
+        float v[8];
+        if (at >= 0) {
+          const float4 *g = reinterpret_cast<const float4 *>(a.G + (size_t)at * nin + c * KCH + 8 * k8);
+          const float4 p = __ldg(g), q = __ldg(g + 1);
+          v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w;
+          v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 8; j++) v[j] = 0.f;
+        }
+        TMD_PUT_ROW(NP, gs, pl.a_elems, core_off(r, 8 * k8, KCH), v, 0);
+      }
+      publish();
+      if (!ok) break;
+      if (tid == 0) {
+        mma_next(smem_u32(gs), a_sbo_g, 0, c == 0);
+        commit(&gbar[slot]);
+      }
+    }
+    if (!ok) break;
+    if (tid == 0) commit(&accb[0]);
+    wait_all(&accb[0], ak[0]);
+    if (!ok) break;
+    // each slot used this tile has one completion not yet consumed (its last
+    // chunk, done by now): consume it so the parities stay in step
+    for (int slot = 0; slot < 2; slot++)
+      if ((nin / KCH - slot + 1) / 2 > 0) wait_all(&gbar[slot], gk[slot]);
+    if (!ok) break;
+
+    // ---------------- forward epilogues and hidden layers ----------------
+    double E = 0.0;
+    for (int l = 0; l < L - 1 && ok; l++) {
+      const int K = sizes[l], N = sizes[l + 1];
+      const float *bl = bias_s + bo_s[l];
+      const int actl = act_s[l];
+      if (l > 0) {
+        if (tid == 0) {
+          for (int c = 0; c < K / KCH; c++)
+            mma_next(abase + (uint32_t)(c * KCH / EPC) * 128u, a_sbo_h, 0, c == 0);
+          commit(&accb[0]);
+        }
+        wait_all(&accb[0], ak[0]);
+        if (!ok) break;
+      }
+      const bool last = (l == L - 2);
+      for (int c0 = 32 * part; c0 < N; c0 += 32 * kTcsParts) {
+        float v[32], d[32];
+        tmem_ld32(trow + c0, v);
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          const int cc = c0 + j;
+          const float z = v[j] + bl[cc];
+          const float y = act_fwd(a.actfn, z, d[j]);
+          if (!last) {
+            v[j] = y;
+          } else {
+            // output layer in FP64; gradient seed g = w_out, gz = g * act'
+            const double w = wout_s[cc];
+            E = fma((double)y, w, E);
+            v[j] = (float)w * d[j];
+          }
+        }
+        if (!last) tmem_st32(trow + actl + c0, d);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          TMD_PUT_ROW(NP, abuf, pl.a_elems, core_off(row, c0 + 8 * q, maxh), v, 8 * q);
+      }
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      publish();
+    }
+    if (!ok) break;
+    epart[part][row] = E;
+    __syncthreads();
+    if (part == 0 && row_atom >= 0)
+      a.E[row_atom] = ((epart[0][row] + epart[1][row]) + (epart[2][row] + epart[3][row])) +
+                      (Ls[L - 1].bd ? *Ls[L - 1].bd : 0.0);
+
+    // ---------------- backward through the hidden layers ----------------
+    for (int l = L - 2; l >= 1 && ok; l--) {
+      const int K = sizes[l], N = sizes[l + 1];
+      if (tid == 0) {
+        for (int c = 0; c < N / KCH; c++)
+          mma_next(abase + (uint32_t)(c * KCH / EPC) * 128u, a_sbo_h, 0, c == 0);
+        commit(&accb[0]);
+      }
+      wait_all(&accb[0], ak[0]);
+      if (!ok) break;
+      const int actp = act_s[l - 1];
+      for (int c0 = 32 * part; c0 < K; c0 += 32 * kTcsParts) {
+        float v[32], d[32];
+        tmem_ld32(trow + c0, v);
+        tmem_ld32(trow + actp + c0, d);
+#pragma unroll
+        for (int j = 0; j < 32; j++) v[j] *= d[j];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          TMD_PUT_ROW(NP, abuf, pl.a_elems, core_off(row, c0 + 8 * q, maxh), v, 8 * q);
+      }
+      publish();
+    }
+    if (!ok) break;
+
+    // ---------------- dE/dG = gz . W_0^T in 128-column blocks ----------------
+    {
+      const int N0 = sizes[1];
+      const int nblk = (nin + 127) / 128;
+      for (int b0 = 0; b0 < nblk && ok; b0 += 4) {
+        const int b1 = min(nblk, b0 + 4);
+        if (tid == 0) {
+          for (int b = b0; b < b1; b++) {
+            for (int c = 0; c < N0 / KCH; c++)
+              mma_next(abase + (uint32_t)(c * KCH / EPC) * 128u, a_sbo_h,
+                       (uint32_t)(128 * (b - b0)), c == 0);
+            commit(&accb[b - b0]);
+          }
+        }
+        for (int b = b0; b < b1 && ok; b++) {
+          wait_all(&accb[b - b0], ak[b - b0]);
+          if (!ok) break;
+          const int n0 = 128 * b, nout = min(128, nin - n0);
+          for (int c0 = 32 * part; c0 < nout; c0 += 32 * kTcsParts) {
+            float v[32];
+            tmem_ld32(trow + (uint32_t)(128 * (b - b0)) + c0, v);
+            if (row_atom >= 0) {
+              float4 *dst = reinterpret_cast<float4 *>(a.dEdG + (size_t)row_atom * nin + n0 + c0);
+#pragma unroll
+              for (int j = 0; j < 8; j++)
+                dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+            }
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        ok = __syncthreads_and(ok ? 1 : 0) != 0;
+      }
+    }
+  }
+  // drain: copies still in flight (error path) and every MMA, then free TMEM
+  if (tid == 0) {
+    bool fine = ok && ok0;
+    for (int q = q_mma; q < q_issue; q++)
+      if (!mbar_wait(&full_b[q % S], (uint32_t)(q / S) & 1u)) fine = false;
+    commit(&drainb);
+    if (!mbar_wait(&drainb, 0)) fine = false;
+    if (!fine) atomicOr(a.status, kStatusTimeout);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcsTmemCols));
+}
+
+size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int *stages) {
+  *stages = 0;
+  if (resnet || nl < 2 || nl - 1 > kMaxLayers) return 0;
+  const int nin = sizes[0];
+  int maxh = 1, acts = 0;
+  for (int l = 1; l < nl; l++) {
+    if (sizes[l] % KCH != 0 || sizes[l] > 256) return 0;
+    maxh = maxh > sizes[l] ? maxh : sizes[l];
+    acts += sizes[l];
+  }
+  if (nin % KCH != 0) return 0;
+  const int nb = np == 3 ? 2 : 1;
+  const TcsPlan pl = tcs_plan(nin, maxh, nb);
+  if (pl.accw + acts > kTcsTmemCols) return 0;
+  // chunk schedule length
+  int nq = 0;
+  for (int l = 0; l < nl - 1; l++) nq += sizes[l] / KCH;
+  for (int l = nl - 2; l >= 1; l--) nq += sizes[l + 1] / KCH;
+  nq += ((nin + 127) / 128) * (sizes[1] / KCH);
+  if (nq > kTcsMaxChunks) return 0;
+  // as many stages as fit next to the operand region and ~12 KB of static data
+  const size_t limit = 227 * 1024 - 12 * 1024;
+  const size_t abytes = (size_t)nb * pl.a_elems * 2, sbytes = (size_t)pl.stage_elems * 2;
+  if (abytes + 2 * sbytes > limit) return 0;
+  int S = (int)((limit - abytes) / sbytes);
+  if (S > kTcsMaxStages) S = kTcsMaxStages;
+  *stages = S;
+  return abytes + (size_t)S * sbytes;
+}
+
+void mlp_tcs_prepare(size_t smem, int np) {
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (np == 3) cudaFuncSetAttribute(k_mlp_tcs<3>, at, (int)smem);
+  else cudaFuncSetAttribute(k_mlp_tcs<1>, at, (int)smem);
+}
+
 size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np, bool dz_bf16) {
   if (resnet || nl < 2) return 0;
   const size_t nb = np == 3 ? 2 : 1;
@@ -599,6 +1045,13 @@ void mlp_tcp_prepare(size_t smem, int np, bool dz_bf16) {
 
 void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches) {
   if (a.ntiles <= 0) return;
+  if (a.streamed > 0) {
+    const int grid = a.ntiles < a.streamed ? a.ntiles : a.streamed;
+    if (a.np == 3) k_mlp_tcs<3><<<grid, kTcsThreads, a.smem_s, st>>>(a);
+    else k_mlp_tcs<1><<<grid, kTcsThreads, a.smem_s, st>>>(a);
+    launches += 1;
+    return;
+  }
   if (a.persistent > 0) {
     const int grid = a.ntiles < a.persistent ? a.ntiles : a.persistent;
     if (a.np == 3) k_mlp_tcp<3, float><<<grid, kTcpThreads, a.smem_p, st>>>(a);

@@ -28,6 +28,9 @@ struct tmd_model {
   int tc_persistent = 0; // > 0: weight-resident persistent tensor-core MLP (grid size)
   size_t tc_smem_p = 0;
   bool tc_dz_bf16_p = false;
+  int tc_streamed = 0;   // > 0: streamed-weight persistent tensor-core MLP (grid size)
+  size_t tc_smem_s = 0;
+  int tc_stages = 0;
   int maxh = 1;
   double *d_mass = nullptr;     // per element
   int mlp_tr = 64;

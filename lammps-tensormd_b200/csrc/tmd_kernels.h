@@ -143,6 +143,9 @@ struct MlpTcArgs {
   int persistent;     // > 0: weight-resident persistent form on this many CTAs
   size_t smem_p;      // its dynamic shared memory
   int dz_bf16_p;      // its act' in BF16 (BF16 form only, when FP32 does not fit)
+  int streamed;       // > 0: streamed-weight persistent form on this many CTAs
+  size_t smem_s;      // its dynamic shared memory
+  int stages;         // its weight-chunk stages
 };
 void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches);
 size_t mlp_tc_smem(int nl, int maxh, int resnet, bool dz_bf16, int np);
@@ -151,6 +154,12 @@ void mlp_tc_prepare(size_t smem, bool dz_bf16, int np);
 // (residual layers).
 size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np, bool dz_bf16);
 void mlp_tcp_prepare(size_t smem, int np, bool dz_bf16);
+// Streamed-weight persistent form (weights too large to stay in shared
+// memory): dynamic shared memory and weight stages, 0 if unsupported
+// (residual layers, widths not multiples of 64 or above 256, act' beyond 512
+// TMEM columns).
+size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int *stages);
+void mlp_tcs_prepare(size_t smem, int np);
 
 // Host: pack a rows x cols matrix (element (r, k) = src[r * ld_r + k * ld_k])
 // into 64-column chunks of 8x8 BF16 core matrices, K-major.

@@ -78,6 +78,43 @@ def test_tc_residual_wide_descriptor(prec):
     _assert_bounds(prec, _errors(out, ref, len(x)))
 
 
+def _alloy_pot(path):
+    """The precision config's potential shape: 4 elements, 32 filters, rc 6.5,
+    512-128-128-128-1 softplus (too large to keep its weights in shared
+    memory: the streamed-weight tensor-core form)."""
+    c = synth.config("alloy432k")
+    return synth.gaussian_potential(path, seed=99, **c["pot"])
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "bf16"])
+def test_tc_streamed_weights_alloy(tmp_path, prec):
+    p = tmp_path / "alloy.npz"
+    syms = _alloy_pot(p)
+    x, t, box, _ = synth.build_system("fcc", 3.6, (8, 8, 8), sigma=0.05, nelt=4, seed=7)
+    _, out = _run(f"{p} {' '.join(syms)}", prec, x, t, box)
+    ref = Oracle(load_npz(p)).compute(x, t - 1, box, [1, 1, 1], skin=1.0)
+    _assert_bounds(prec, _errors(out, ref, len(x)))
+
+
+def test_tc_streamed_weights_many_tiles(tmp_path):
+    """More 128-atom tiles than SMs: each persistent CTA walks several tiles
+    of several elements while the weight chunks stream ahead.  The split form
+    against the plain FP32 form, and bitwise the same run to run."""
+    p = tmp_path / "alloy.npz"
+    syms = _alloy_pot(p)
+    x, t, box, _ = synth.build_system("fcc", 3.6, (18, 18, 16), sigma=0.05, nelt=4, seed=8)
+    args = f"{p} {' '.join(syms)}"
+    s32 = TensorMDSystem(TensorMDModel(args), len(x), 1.0)
+    s32.set_box(box)
+    s32.set_atoms(x, t)
+    ref = s32.compute(1, 1)
+    s, out = _run(args, "bf16x3", x, t, box)
+    frms, de, vr = _errors(out, ref, len(x))
+    assert frms <= 1e-3 and de <= 1e-4 and vr <= 1e-2, (frms, de, vr)
+    again = s.compute(1, 1, peratom=True)
+    assert np.array_equal(again["f"], out["f"]) and again["energy"] == out["energy"]
+
+
 def test_tc_deterministic(fcc4k):
     p, syms, x, t, box, _ = fcc4k
     s, a = _run(f"{p} {' '.join(syms)}", "bf16", x, t, box)
