@@ -787,26 +787,42 @@ k_mlp_tcs(MlpTcArgs a) {
     const int row_atom = rows_s[row];
 
     // ---------------- layer 0: G chunks through two slots ----------------
+    // each thread converts kGRows core rows (8 columns of one atom row) per
+    // chunk; the rows of chunk c + 1 are loaded while chunk c is published
+    // and multiplied
+    constexpr int kGRows = TM * (KCH / 8) / kTcsThreads;
+    static_assert(kGRows * kTcsThreads == TM * (KCH / 8), "G chunk split");
+    float4 gv[kGRows][2];
+    auto load_g = [&](int c) {
+#pragma unroll
+      for (int u = 0; u < kGRows; u++) {
+        const int idx = tid + u * kTcsThreads;
+        const int r = idx / (KCH / 8), k8 = idx - r * (KCH / 8);
+        const int at = rows_s[r];
+        if (at >= 0) {
+          const float4 *g = reinterpret_cast<const float4 *>(a.G + (size_t)at * nin + c * KCH + 8 * k8);
+          gv[u][0] = __ldg(g);
+          gv[u][1] = __ldg(g + 1);
+        } else {
+          gv[u][0] = gv[u][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+    };
+    load_g(0);
     for (int c = 0; c < nin / KCH && ok; c++) {
       const int slot = c & 1;
       T *gs = abuf + (size_t)slot * TM * KCH;
       if (c >= 2) wait_all(&gbar[slot], gk[slot]);  // the MMAs of chunk c - 2 are done
       if (!ok) break;
-      for (int idx = tid; idx < TM * (KCH / 8); idx += kTcsThreads) {
-        const int r = idx / (KCH / 8), k8 = idx - r * (KCH / 8);
-        const int at = rows_s[r];
-        float v[8];
-        if (at >= 0) {
-          const float4 *g = reinterpret_cast<const float4 *>(a.G + (size_t)at * nin + c * KCH + 8 * k8);
-          const float4 p = __ldg(g), q = __ldg(g + 1);
-          v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w;
-          v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
-        } else {
 #pragma unroll
-          for (int j = 0; j < 8; j++) v[j] = 0.f;
-        }
+      for (int u = 0; u < kGRows; u++) {
+        const int idx = tid + u * kTcsThreads;
+        const int r = idx / (KCH / 8), k8 = idx - r * (KCH / 8);
+        const float v[8] = {gv[u][0].x, gv[u][0].y, gv[u][0].z, gv[u][0].w,
+                            gv[u][1].x, gv[u][1].y, gv[u][1].z, gv[u][1].w};
         TMD_PUT_ROW(NP, gs, pl.a_elems, core_off(r, 8 * k8, KCH), v, 0);
       }
+      if (c + 1 < nin / KCH) load_g(c + 1);
       publish();
       if (!ok) break;
       if (tid == 0) {
@@ -847,7 +863,7 @@ k_mlp_tcs(MlpTcArgs a) {
         for (int j = 0; j < 32; j++) {
           const int cc = c0 + j;
           const float z = v[j] + bl[cc];
-          const float y = act_fwd(a.actfn, z, d[j]);
+          const float y = tc::act_fwd_fast(a.actfn, z, d[j]);
           if (!last) {
             v[j] = y;
           } else {

@@ -97,6 +97,41 @@ __device__ inline float act_fwd(int actfn, float z, float &d) {
   }
 }
 
+// The same activations from fast intrinsics (__expf, __logf, __frcp_rn),
+// for the tensor-core forms whose operands are BF16: absolute errors of a
+// few 1e-7, far below the operand rounding.  Where a closed form loses
+// relative accuracy the Taylor series takes over: log(1 + e) = e - e^2/2 +
+// e^3/3 for e < 1e-3 (softplus of z < -6.9), tanh a = a - a^3/3 for a <
+// 4e-3.  Same thresholds as act_fwd for the large-argument branches.
+__device__ inline float act_fwd_fast(int actfn, float z, float &d) {
+  switch (actfn) {
+    case 0:
+      d = z > 0.f ? 1.f : 0.f;
+      return z > 0.f ? z : 0.f;
+    case 1: {
+      const float ex = __expf(fminf(z, 80.f));
+      d = ex * __frcp_rn(1.f + ex);
+      const float lg = ex < 1e-3f ? ex * (1.f - ex * (0.5f - ex * (1.f / 3.f)))
+                                  : __logf(1.f + ex);
+      return z < 13.942385152878742f ? lg : z;
+    }
+    case 2: {
+      const float a = fabsf(z);
+      const float t = __expf(-2.f * fminf(a, 40.f));
+      const float y0 = a < 4e-3f ? a - a * a * a * (1.f / 3.f) : (1.f - t) * __frcp_rn(1.f + t);
+      const float y = copysignf(y0, z);
+      d = 1.f - y * y;
+      return y;
+    }
+    default: {
+      const float q = sqrtf(z * z + 4.f);
+      const float y = z >= 0.f ? 0.5f * (z + q) : 2.f * __frcp_rn(q - z);
+      d = y * __frcp_rn(q);
+      return y;
+    }
+  }
+}
+
 // element offset of (r, k) in a K-major core-matrix operand with kfull
 // columns and epc elements per 16-byte core row
 template <int EPC>
