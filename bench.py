@@ -59,6 +59,8 @@ def parse():
                          "reference-workload or CPU lines): for profiler launch lists")
     ap.add_argument("--cells-steps", type=int, default=500,
                     help="NVE steps of the 4,096-cell batch line (0 skips it)")
+    ap.add_argument("--precision-steps", type=int, default=20,
+                    help="NVE steps per MLP form of the 432,000-atom precision line (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=2000.0,
                     help="serving line: Poisson arrival rate (jobs/s)")
     ap.add_argument("--serve-window", type=float, default=2.0,
@@ -396,6 +398,12 @@ def run_ours(args, rank, world, local):
                 except Exception as exc:  # report, do not hide
                     serving["forms"][prec] = {"error": str(exc)}
     w23k = None if args.main_only else run_w23k(args, rank, world, local, dev, barrier)
+    alloy = None
+    if args.precision_steps > 0 and not args.main_only:
+        try:
+            alloy = run_alloy(args, rank, world, local, dev, barrier)
+        except Exception as exc:  # report, do not hide
+            alloy = {"error": str(exc)}
 
     cpu = None
     if rank == 0 and world == 1 and not (args.no_cpu_baseline or args.main_only):
@@ -421,6 +429,7 @@ def run_ours(args, rank, world, local):
             "force_form": force_form,
             "forms": forms,
             "cells4096": cells,
+            "alloy432k": alloy,
             "serving": serving,
             "reference_workload_w23k": w23k,
             "cpu_baseline": cpu,
@@ -429,6 +438,66 @@ def run_ours(args, rank, world, local):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_alloy(args, rank, world, local, dev, barrier):
+    """Precision config: 4-element random FCC alloy a = 3.6 A, 60x60x30 cells =
+    432,000 atoms, 32 Gaussians rc 6.5 A, MLP 512-128-128-128-1 softplus.
+    Each MLP form (plain FP32, split BF16, BF16) runs the same NVE steps,
+    timed with CUDA events on its system stream after 3 warm-up steps; MLP
+    time per step from a profiled pass; force and energy error of the BF16
+    forms against the FP32 form on the starting positions."""
+    import torch
+    from tmd_b200 import TensorMDModel, TensorMDSystem, synth
+    pot, syms, x, t, box, v, cfg = workload("alloy432k", seed=42)
+    n, dt = len(x), 0.001
+    out = {"natoms": n, "steps": args.precision_steps, "config": cfg, "forms": {}}
+    ref = None
+    for prec in ("fp32", "bf16x3", "bf16"):
+        suffix = "" if prec == "fp32" else f" precision {prec}"
+        m = TensorMDModel(f"{pot} {' '.join(syms)}{suffix}", device=local)
+        s_ = TensorMDSystem(m, n, 1.0)
+        s_.set_box(box)
+        s_.set_atoms(x, t, v)
+        s_.autotune(reps=3)
+        s_.autotune(reps=3, family="descriptor")
+        r = s_.compute(1, 1)
+        row = {"force_form": s_.force_variant(), "descriptor_form": s_.descriptor_variant()}
+        if ref is None:
+            ref = r
+        else:
+            row["force_rms_err_vs_fp32_eV_per_A"] = float(np.sqrt(np.mean((r["f"] - ref["f"]) ** 2)))
+            row["energy_err_vs_fp32_eV_per_atom"] = abs(r["energy"] - ref["energy"]) / n
+        s_.nve_run(3, dt)
+        stream = torch.cuda.ExternalStream(s_.stream(), device=dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s_.nve_run(args.precision_steps, dt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        ms = float(ms.item())
+        s_.profile(True)
+        s_.profile_read(reset=True)
+        s_.nve_run(5, dt)
+        prof = s_.profile_read(reset=True)
+        row.update({"value": n * args.precision_steps * world / (ms / 1000.0),
+                    "ms_per_step": ms / args.precision_steps,
+                    "kernel_ms": {k: c_t[1] / max(c_t[0], 1) for k, c_t in prof.items()
+                                  if c_t[0] > 0}})
+        out["forms"][prec] = row
+        s_.close()
+        m.close()
+    f32 = out["forms"]["fp32"]["value"]
+    for prec in ("bf16x3", "bf16"):
+        out["forms"][prec]["speedup_vs_fp32"] = out["forms"][prec]["value"] / f32
+    return out
 
 
 def run_cells(args, rank, world, local, dev, barrier):

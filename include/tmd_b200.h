@@ -237,11 +237,17 @@ int tmd_batch_nvt_run(tmd_batch *batch, int nsteps, double dt, const double *t_s
  *   TMD_JOB_FIRE    FIRE relaxation (Bitzek et al. 2006, semi-implicit Euler,
  *                   initial step dt, dt_max = 10 dt) until every force
  *                   component norm |F_i| <= fmax or nsteps iterations ran
+ * tmd_server_submit returns TMD_ERR_ARG for a box that is degenerate or too
+ * small for the cutoff (more than 3 images per axis) and TMD_ERR_CAPACITY for
+ * a job larger than max_atoms.  A job's results do not depend on the other
+ * jobs in flight: when jobs join or leave, the continuing ones move on the
+ * device together with their neighbor lists, and a job's list is rebuilt
+ * only when its own atoms trigger it, as for a separate system.
  * tmd_server_wait blocks up to timeout_s seconds (< 0: no limit) and returns
  * TMD_ERR_TIMEOUT if the job is not done (the ticket stays valid); on
  * completion it fills the non-NULL outputs: energy, virial[6], final x / v /
- * f [n*3] (positions wrapped into the box), steps run, latency from submit to
- * completion, and releases the ticket. */
+ * f [n*3] (positions as wrapped at the job's last neighbor rebuild), steps
+ * run, latency from submit to completion, and releases the ticket. */
 #define TMD_JOB_ENERGY 0
 #define TMD_JOB_NVE 1
 #define TMD_JOB_FIRE 2
@@ -261,8 +267,9 @@ int tmd_server_wait(tmd_server *server, long ticket, double timeout_s,
 int tmd_server_stats(tmd_server *server, long *submitted, long *completed,
                      long *active_atoms, double *atom_steps, double *busy_s);
 /* Worker seconds by phase since creation: seconds[0] relayout (admission and
- * retirement, with the neighbor rebuild), [1] force evaluations of newly
- * admitted jobs, [2] integrator steps, [3] copying results out. */
+ * retirement: moving the cells, neighbor lists of the new jobs), [1] force
+ * evaluations of newly admitted jobs, [2] integrator steps, [3] copying
+ * results out. */
 int tmd_server_timing(tmd_server *server, double *seconds);
 
 /* Full neighbor list without allocating any memory.  This entry point has no
