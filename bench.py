@@ -1,7 +1,7 @@
 """Benchmark of the B200 pair_style tensormd path: MD atom-steps/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config bcc128k|fcc4k|alloy432k]
+                    [--config bcc128k|fcc4k|alloy432k|alloy55k]
 
 Workload (default): BCC a = 2.87 A, 40x40x40 cells = 128,000 atoms, Gaussian
 displacements sigma = 0.08 A, 600 K Maxwell velocities, one element, 16

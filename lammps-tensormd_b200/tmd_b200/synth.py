@@ -282,4 +282,8 @@ def config(name):
         return dict(kind="fcc", a=3.6, cells=(60, 60, 30), sigma=0.05, T=300.0, nelt=4,
                     pot=dict(nelt=4, num_filters=32, rc=6.5, max_moment=3,
                              hidden=(128, 128, 128), actfn=1))
+    if name == "alloy55k":  # the precision config's potential on 55,296 atoms (profiling)
+        c = config("alloy432k")
+        c["cells"] = (24, 24, 24)
+        return c
     raise KeyError(name)
