@@ -322,6 +322,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   int maxh = 1;
   for (int l = 1; l < m->h.nl; l++) maxh = std::max(maxh, m->h.sizes[l]);
   ma.maxh = maxh; ma.tr = m->mlp_tr; ma.smem = m->mlp_smem; ma.resident = m->mlp_resident;
+  ma.streamed = m->mlp_streamed; ma.stages = m->mlp_stages; ma.status = s->status;
   ma.ntiles = s->ntiles; ma.tiles = s->tiles; ma.perm = s->perm; ma.G = s->G;
   ma.dEdG = s->dEdG; ma.E = s->E; ma.layers = m->d_layers;
   prof_begin(s);
@@ -701,7 +702,9 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
   }
   // MLP: the resident-weight form (one persistent CTA per SM) when the
   // element's hidden weights and a tile's activations fit in shared memory
-  // (128-atom tiles, else 64), else weights streamed in chunks with 64- or
+  // (128-atom tiles, else 64); else the persistent streamed-weight form
+  // (64-atom tiles, weight chunks copied through a stage ring); else, for
+  // residual MLPs, weights staged per chunk by the threads with 64- or
   // 32-atom tiles
   size_t s64 = mlp_fp32_smem(h.nl, h.sizes.data(), 64);
   size_t s32 = mlp_fp32_smem(h.nl, h.sizes.data(), 32);
@@ -713,6 +716,30 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     m->mlp_tr = 128; m->mlp_smem = sres; m->mlp_resident = nsm;
   } else if (h.nl >= 2 && sres64 <= 227 * 1024 && nsm > 0) {
     m->mlp_tr = 64; m->mlp_smem = sres64; m->mlp_resident = nsm;
+  } else if (int stages = 0;
+             nsm > 0 && (m->mlp_smem = mlp_fp32s_smem(h.nl, h.sizes.data(), h.resnet, &stages)) > 0) {
+    // weights streamed through shared memory in chunks (64-atom tiles):
+    // pack each hidden layer's W and W^T into the chunk layouts
+    m->mlp_tr = 64; m->mlp_streamed = nsm; m->mlp_stages = stages;
+    for (int el = 0; el < h.nelt && e == cudaSuccess; el++)
+      for (int l = 0; l + 1 < h.nl && e == cudaSuccess; l++) {
+        MlpLayer &Ly = layers[(size_t)el * h.nl + l];
+        std::vector<float> pf, pb;
+        mlp_fp32s_pack(h.W[el][l].data(), h.sizes[l], h.sizes[l + 1], pf, pb);
+        float *df = nullptr, *db = nullptr;
+        e = up(pf, &df);
+        if (e == cudaSuccess) e = up(pb, &db);
+        Ly.Wp = df;
+        Ly.Wtp = db;
+      }
+    if (e == cudaSuccess)
+      e = cudaMemcpy(m->d_layers, layers.data(), layers.size() * sizeof(MlpLayer),
+                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      tmd_model_free(m);
+      return fail(TMD_ERR_CUDA, std::string("model upload: ") + cudaGetErrorString(e));
+    }
+    mlp_fp32s_prepare(m->mlp_smem);
   } else if (s64 <= 110 * 1024) {
     m->mlp_tr = 64; m->mlp_smem = s64;
   } else if (s32 <= 220 * 1024) {
@@ -721,7 +748,7 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     tmd_model_free(m);
     return fail(TMD_ERR_MODEL, "MLP too wide for the shared-memory tile");
   }
-  mlp_fp32_prepare(m->mlp_tr, m->mlp_smem, m->mlp_resident > 0);
+  if (m->mlp_streamed == 0) mlp_fp32_prepare(m->mlp_tr, m->mlp_smem, m->mlp_resident > 0);
   for (int l = 1; l < h.nl; l++) m->maxh = std::max(m->maxh, h.sizes[l]);
   if (h.precision == TMD_PREC_BF16 || h.precision == TMD_PREC_BF16X3 ||
       h.precision == TMD_PREC_FP8) {

@@ -15,6 +15,9 @@
 // tile per 64-column pass.
 #include <float.h>
 
+#include <vector>
+
+#include "tc_util.cuh"
 #include "tmd_kernels.h"
 
 namespace tmd {
@@ -550,10 +553,339 @@ k_mlp_fp32r(MlpArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Streamed-weight form (k_mlp_fp32s) for MLPs whose weights do not fit in
+// shared memory (e.g. 512-128-128-128 per element: 393 KB of FP32 W per
+// direction).  Persistent CTAs of 256 threads walk 64-atom tiles.  Every GEMM
+// of a tile is a sequence of chunks: 32 reduction rows x a 128-column output
+// block of a weight array packed on the host as [block][rows][128] (forward:
+// W, blocks over N; backward: W^T, blocks over K), so a chunk is one
+// contiguous 16 KB that thread 0 copies with cp.async.bulk into a ring of S
+// shared-memory stages, S - 1 chunks ahead (across layers and tiles), each
+// completing on its stage's mbarrier.  Layer 0 reads G in 32-column chunks,
+// gathered and transposed by all threads into the chunk's stage (the next
+// chunk's G rows are loaded while the current chunk is multiplied).  Hidden
+// activations, gradients and act' stay in shared memory (k-major, stride
+// 64 + 4), as in the resident form.  Thread (ty, tx) of the 16 x 16 grid owns
+// rows 4ty..4ty+3 and columns 4tx..4tx+3, 64+4tx..64+4tx+3 of a block: per
+// reduction row one float4 of A, two of W and 16 FFMA2.  Products and sums
+// per output in the same order as the other FP32 forms (reduction index
+// ascending); the output layer in FP64.
+// ---------------------------------------------------------------------------
+constexpr int kFsTR = 64;
+constexpr int kFsThreads = 256;
+constexpr int kFsKC = 32;
+constexpr int kFsCB = 128;
+constexpr int kFsLDT = kFsTR + 4;
+constexpr int kFsMaxStages = 6;
+constexpr int kFsMaxChunks = 512;
+
+struct FsChunk {
+  short l, dir, blk, r0;
+};
+
+struct FsLayout {  // offsets in floats
+  int stage;       // floats per stage: W chunk [32][128], then G chunk [32][68]
+  int h0, h1, bias, wout, total;
+  int dzoff[kMaxLayers], boff[kMaxLayers];
+};
+
+__host__ __device__ inline FsLayout fs_layout(int nl, const int *sizes, int S) {
+  FsLayout f{};
+  int maxh = 1;
+  for (int l = 1; l < nl; l++) maxh = maxh > sizes[l] ? maxh : sizes[l];
+  f.stage = kFsKC * kFsCB + kFsKC * kFsLDT;
+  int o = S * f.stage;
+  f.h0 = o; o += maxh * kFsLDT;
+  f.h1 = o; o += maxh * kFsLDT;
+  for (int l = 0; l + 2 < nl; l++) { f.dzoff[l] = o; o += sizes[l + 1] * kFsLDT; }
+  f.bias = o;
+  int ob = 0;
+  for (int l = 0; l + 1 < nl; l++) { f.boff[l] = ob; ob += sizes[l + 1]; }
+  o += round_up(ob, 4);
+  f.wout = round_up(o, 4);  // doubles from here
+  o = f.wout + 2 * round_up(sizes[nl - 1], 2);
+  f.total = round_up(o, 4);
+  return f;
+}
+
+__global__ void __launch_bounds__(kFsThreads, 1)
+k_mlp_fp32s(MlpArgs a) {
+  extern __shared__ float4 fs4[];
+  float *sm = reinterpret_cast<float *>(fs4);
+  __shared__ __align__(8) uint64_t fullb[kFsMaxStages];
+  __shared__ int rows_s[kFsTR];
+  __shared__ FsChunk sched[kFsMaxChunks];
+  __shared__ int nq_s, sz_s[kMaxLayers + 1];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int L = a.nl, nin = a.nin, S = a.stages;
+  if (tid == 0) {
+    sz_s[0] = nin;
+    for (int l = 0; l < L; l++) sz_s[l + 1] = a.layers[l].N;
+    int k = 0;
+    for (int l = 0; l < L - 1; l++)
+      for (int nb = 0; nb * kFsCB < sz_s[l + 1]; nb++)
+        for (int r0 = 0; r0 < sz_s[l]; r0 += kFsKC) sched[k++] = FsChunk{(short)l, 0, (short)nb, (short)r0};
+    for (int l = L - 2; l >= 0; l--)
+      for (int kb = 0; kb * kFsCB < sz_s[l]; kb++)
+        for (int r0 = 0; r0 < sz_s[l + 1]; r0 += kFsKC) sched[k++] = FsChunk{(short)l, 1, (short)kb, (short)r0};
+    nq_s = k;
+    for (int s = 0; s < S; s++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_u32(&fullb[s])));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  __syncthreads();
+  const int *sizes = sz_s;
+  const int nq = nq_s;
+  const FsLayout lay = fs_layout(L, sizes, S);
+  float *bias_s = sm + lay.bias;
+  double *wout_s = reinterpret_cast<double *>(sm + lay.wout);
+  const int ntile_cta =
+      blockIdx.x < a.ntiles ? (a.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  const int q_end = ntile_cta * nq;
+  int q_issue = 0;  // thread 0: next chunk to copy
+  bool ok = true;
+
+  auto issue_to = [&](int qlim) {  // thread 0
+    while (q_issue < qlim && q_issue < q_end) {
+      const int t = blockIdx.x + (q_issue / nq) * gridDim.x;
+      const FsChunk ch = sched[q_issue % nq];
+      const MlpLayer &ly = a.layers[(size_t)a.tiles[3 * t] * L + ch.l];
+      const int rows = ch.dir ? ly.N : ly.K;
+      const float *src = (ch.dir ? ly.Wtp : ly.Wp) + ((size_t)ch.blk * rows + ch.r0) * kFsCB;
+      const uint32_t bar = tc::smem_u32(&fullb[q_issue % S]);
+      const uint32_t bytes = kFsKC * kFsCB * 4;
+      tc::mbar_expect_tx(bar, bytes);
+      tc::bulk_g2s(tc::smem_u32(sm + (size_t)(q_issue % S) * lay.stage), src, bytes, bar);
+      q_issue++;
+    }
+  };
+  if (tid == 0) issue_to(S - 1);
+
+  int q = 0, cur_elt = -1;
+  float4 gr[2];
+  // G rows of reduction columns k0..k0+31 of this tile, into registers
+  auto load_g = [&](int k0) {
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int idx = tid + u * kFsThreads, r = idx >> 3, q4 = idx & 7;
+      const int at = rows_s[r];
+      gr[u] = at >= 0 ? __ldg(reinterpret_cast<const float4 *>(a.G + (size_t)at * nin + k0 + 4 * q4))
+                      : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  // wait for chunk q, free the previous stage for chunk q + S - 1
+  auto next_chunk = [&]() -> float * {
+    bool okc = true;
+    if (tid == 0) okc = tc::mbar_wait(&fullb[q % S], (uint32_t)(q / S) & 1u);
+    ok = __syncthreads_and(okc && ok) != 0;
+    if (tid == 0 && ok) issue_to(q + S);
+    return sm + (size_t)(q % S) * lay.stage;
+  };
+  auto fma_chunk = [&](const float *A, const float *Bw, float2 (&acc)[4][4]) {
+#pragma unroll 4
+    for (int k = 0; k < kFsKC; k++) {
+      const float4 av = *reinterpret_cast<const float4 *>(A + k * kFsLDT + 4 * ty);
+      const float4 b0 = *reinterpret_cast<const float4 *>(Bw + k * kFsCB + 4 * tx);
+      const float4 b1 = *reinterpret_cast<const float4 *>(Bw + k * kFsCB + 64 + 4 * tx);
+      const float2 bb[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w),
+                            make_float2(b1.x, b1.y), make_float2(b1.z, b1.w)};
+      const float ar[4] = {av.x, av.y, av.z, av.w};
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const float2 a2 = make_float2(ar[i], ar[i]);
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = __ffma2_rn(a2, bb[j], acc[i][j]);
+      }
+    }
+  };
+  auto col_of = [&](int blk, int j) { return blk * kFsCB + (j < 4 ? 4 * tx + j : 64 + 4 * tx + j - 4); };
+  auto acc_at = [&](const float2 (&acc)[4][4], int i, int j) {
+    const float2 v = acc[i][j >> 1];
+    return (j & 1) ? v.y : v.x;
+  };
+
+  for (int tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x) {
+    const int elt = a.tiles[3 * tile], start = a.tiles[3 * tile + 1],
+              count = a.tiles[3 * tile + 2];
+    const MlpLayer *Ls = a.layers + (size_t)elt * L;
+    if (tid < kFsTR) rows_s[tid] = tid < count ? a.perm[start + tid] : -1;
+    if (elt != cur_elt) {
+      cur_elt = elt;
+      for (int l = 0; l < L - 1; l++)
+        for (int c = tid; c < sizes[l + 1]; c += kFsThreads)
+          bias_s[lay.boff[l] + c] = Ls[l].b ? __ldg(Ls[l].b + c) : 0.f;
+      for (int c = tid; c < sizes[L - 1]; c += kFsThreads) wout_s[c] = __ldg(Ls[L - 1].Wd + c);
+    }
+    __syncthreads();
+    float *hin = sm + lay.h0, *hout = sm + lay.h1;
+    double ep[4] = {0.0, 0.0, 0.0, 0.0};
+    load_g(0);
+
+    // ---------------- forward ----------------
+    for (int l = 0; l < L - 1 && ok; l++) {
+      const int K = sizes[l], N = sizes[l + 1];
+      const bool last = (l == L - 2);
+      const float *bl = bias_s + lay.boff[l];
+      float *dz = last ? nullptr : sm + lay.dzoff[l];
+      for (int nb = 0; nb * kFsCB < N && ok; nb++) {
+        float2 acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) acc[i][j] = make_float2(0.f, 0.f);
+        for (int k0 = 0; k0 < K; k0 += kFsKC) {
+          float *stW = sm + (size_t)(q % S) * lay.stage, *stG = stW + kFsKC * kFsCB;
+          if (l == 0) {
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+              const int idx = tid + u * kFsThreads, r = idx >> 3, q4 = idx & 7;
+              const float v[4] = {gr[u].x, gr[u].y, gr[u].z, gr[u].w};
+#pragma unroll
+              for (int j = 0; j < 4; j++) stG[(4 * q4 + j) * kFsLDT + r] = v[j];
+            }
+          }
+          next_chunk();
+          if (!ok) break;
+          if (l == 0) {  // the next chunk's G rows
+            if (k0 + kFsKC < K) load_g(k0 + kFsKC);
+            else if ((nb + 1) * kFsCB < N) load_g(0);
+          }
+          fma_chunk(l == 0 ? stG : hin + (size_t)k0 * kFsLDT, stW, acc);
+          q++;
+        }
+        if (!ok) break;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int r = 4 * ty + i;
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const int c = col_of(nb, j);
+            if (c < N) {
+              float d;
+              const float y = act_fwd(a.actfn, acc_at(acc, i, j) + bl[c], d);
+              if (!last) {
+                hout[(size_t)c * kFsLDT + r] = y;
+                dz[(size_t)c * kFsLDT + r] = d;
+              } else {
+                // output layer in FP64; gradient seed g = w_out, gz = g * act'
+                const double w = wout_s[c];
+                ep[i] = fma((double)y, w, ep[i]);
+                hout[(size_t)c * kFsLDT + r] = (float)w * d;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+      float *t = hin; hin = hout; hout = t;
+    }
+    if (!ok) break;
+    {
+      const MlpLayer lo = Ls[L - 1];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        double e = ep[i];
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o, 16);
+        const int at = rows_s[4 * ty + i];
+        if (tx == 0 && at >= 0) {
+          if (lo.bd)
+            for (int o2 = 0; o2 < lo.N; o2++) e += __ldg(lo.bd + o2);
+          a.E[at] = e;
+        }
+      }
+    }
+
+    // ---------------- backward ----------------
+    for (int l = L - 2; l >= 0 && ok; l--) {
+      const int K = sizes[l], N = sizes[l + 1];
+      const float *dzp = l > 0 ? sm + lay.dzoff[l - 1] : nullptr;
+      for (int kb = 0; kb * kFsCB < K && ok; kb++) {
+        float2 acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) acc[i][j] = make_float2(0.f, 0.f);
+        for (int n0 = 0; n0 < N; n0 += kFsKC) {
+          const float *stW = next_chunk();
+          if (!ok) break;
+          fma_chunk(hin + (size_t)n0 * kFsLDT, stW, acc);
+          q++;
+        }
+        if (!ok) break;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int r = 4 * ty + i;
+          if (l > 0) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              const int c = col_of(kb, j);
+              if (c < K) hout[(size_t)c * kFsLDT + r] = acc_at(acc, i, j) * dzp[(size_t)c * kFsLDT + r];
+            }
+          } else {
+            const int at = rows_s[r];
+            if (at >= 0) {
+              float *dst = a.dEdG + (size_t)at * nin;
+              const int c0 = kb * kFsCB + 4 * tx, c1 = c0 + 64;
+              if (c0 < K) *reinterpret_cast<float4 *>(dst + c0) =
+                  make_float4(acc[i][0].x, acc[i][0].y, acc[i][1].x, acc[i][1].y);
+              if (c1 < K) *reinterpret_cast<float4 *>(dst + c1) =
+                  make_float4(acc[i][2].x, acc[i][2].y, acc[i][3].x, acc[i][3].y);
+            }
+          }
+        }
+      }
+      __syncthreads();
+      float *t = hin; hin = hout; hout = t;
+    }
+  }
+  // copies still in flight (an error path leaves some): wait (bounded)
+  if (tid == 0) {
+    bool fine = ok;
+    for (int qq = q; qq < q_issue; qq++)
+      if (!tc::mbar_wait(&fullb[qq % S], (uint32_t)(qq / S) & 1u)) fine = false;
+    if (!fine && a.status) atomicOr(a.status, kStatusTimeout);
+  }
+}
+
 }  // namespace
 
 size_t mlp_fp32r_smem(int nl, const int *sizes, int tr) {
   return sizeof(float) * (size_t)res_layout(nl, sizes, tr).total;
+}
+
+size_t mlp_fp32s_smem(int nl, const int *sizes, int resnet, int *stages) {
+  *stages = 0;
+  if (resnet || nl < 2 || nl - 1 > kMaxLayers) return 0;
+  for (int l = 0; l < nl; l++)
+    if (sizes[l] % kFsKC != 0 || sizes[l] > 32767) return 0;
+  int nq = 0;
+  for (int l = 0; l < nl - 1; l++) {
+    const int K = sizes[l], N = sizes[l + 1];
+    nq += ((N + kFsCB - 1) / kFsCB) * (K / kFsKC) + ((K + kFsCB - 1) / kFsCB) * (N / kFsKC);
+  }
+  if (nq > kFsMaxChunks) return 0;
+  const size_t limit = 227 * 1024 - 6 * 1024;  // next to ~5 KB of static data
+  int S = kFsMaxStages;
+  while (S >= 2 && sizeof(float) * (size_t)fs_layout(nl, sizes, S).total > limit) S--;
+  if (S < 2) return 0;
+  *stages = S;
+  return sizeof(float) * (size_t)fs_layout(nl, sizes, S).total;
+}
+
+void mlp_fp32s_pack(const float *W, int K, int N, std::vector<float> &fwd, std::vector<float> &bwd) {
+  // forward [N blocks][K][128]: block nb row k = W[k][128 nb ..]; backward
+  // [K blocks][N][128]: block kb row n = W[128 kb ..][n]; zero beyond N / K
+  const int nbF = (N + kFsCB - 1) / kFsCB, kbB = (K + kFsCB - 1) / kFsCB;
+  fwd.assign((size_t)nbF * K * kFsCB, 0.f);
+  bwd.assign((size_t)kbB * N * kFsCB, 0.f);
+  for (int k = 0; k < K; k++)
+    for (int n = 0; n < N; n++) {
+      const float w = W[(size_t)k * N + n];
+      fwd[((size_t)(n / kFsCB) * K + k) * kFsCB + n % kFsCB] = w;
+      bwd[((size_t)(k / kFsCB) * N + n) * kFsCB + k % kFsCB] = w;
+    }
 }
 
 size_t mlp_fp32_smem(int nl, const int *sizes, int tr) {
@@ -571,6 +903,11 @@ size_t mlp_fp32_smem(int nl, const int *sizes, int tr) {
 void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches) {
   if (a.ntiles <= 0) return;
   launches += 1;
+  if (a.streamed > 0) {
+    const int grid = a.ntiles < a.streamed ? a.ntiles : a.streamed;
+    k_mlp_fp32s<<<grid, kFsThreads, a.smem, st>>>(a);
+    return;
+  }
   if (a.resident > 0) {
     const int grid = a.ntiles < a.resident ? a.ntiles : a.resident;
     if (a.tr == 128)
@@ -584,6 +921,10 @@ void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches) {
   } else {
     k_mlp_fp32<32><<<a.ntiles, kThreads, a.smem, st>>>(a);
   }
+}
+
+void mlp_fp32s_prepare(size_t smem) {
+  cudaFuncSetAttribute(k_mlp_fp32s, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 void mlp_fp32_prepare(int tr, size_t smem, bool resident) {

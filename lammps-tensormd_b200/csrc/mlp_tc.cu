@@ -38,6 +38,8 @@ using tc::commit;
 using tc::mbar_wait;
 using tc::tmem_ld32;
 using tc::act_fwd;
+using tc::bulk_g2s;
+using tc::mbar_expect_tx;
 constexpr int EPC = 8;       // BF16 elements per 16-byte core-matrix row
 constexpr int KSTEP = 16;    // MMA K of kind::f16
 
@@ -570,19 +572,6 @@ constexpr int kTcsTmemCols = 512;
 struct TcsChunk {  // one weight chunk of the per-tile schedule
   short l, dir, c, n0, nrows;
 };
-
-__device__ inline void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-      "[%3];" ::"r"(dst),
-      "l"(src), "r"(bytes), "r"(bar)
-      : "memory");
-}
-
-__device__ inline void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
 
 __device__ inline void tmem_st32(uint32_t taddr, const float v[32]) {
   asm volatile(

@@ -36,6 +36,8 @@ struct tmd_model {
   int mlp_tr = 64;
   size_t mlp_smem = 0;
   int mlp_resident = 0;    // > 0: resident-weight MLP, persistent grid size
+  int mlp_streamed = 0;    // > 0: streamed-weight FP32 MLP, persistent grid size
+  int mlp_stages = 0;
   int nsys = 0;            // systems created from this model and not yet freed
   bool released = false;   // tmd_model_free called while nsys > 0
 };

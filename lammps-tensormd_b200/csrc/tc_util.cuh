@@ -54,6 +54,22 @@ __device__ inline bool mbar_wait(uint64_t *mbar, uint32_t phase) {
   }
 }
 
+// Global -> shared bulk copy (no multicast) completing on mbarrier `bar`;
+// addresses 16-byte aligned, bytes a multiple of 16.
+__device__ inline void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+      "[%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+// Arrive on `bar` and add `bytes` to the transaction count of its phase.
+__device__ inline void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
 __device__ inline void tmem_ld32(uint32_t taddr, float v[32]) {
   uint32_t r[32];
   asm volatile(

@@ -1,6 +1,8 @@
 // tmd_kernels.h -- launch interfaces of the device kernels.
 #pragma once
 
+#include <vector>
+
 #include "tmd_internal.h"
 
 namespace tmd {
@@ -95,12 +97,19 @@ struct MlpLayer {
   // output layer only: FP64 copies, the atomic energy is formed in FP64
   const double *Wd;
   const double *bd;
+  // streamed-weight form only (hidden layers): W packed [N/128][K][128] and
+  // W^T packed [K/128][N][128] (mlp_fp32s_pack)
+  const float *Wp;
+  const float *Wtp;
 };
 struct MlpArgs {
   int nl, actfn, resnet, nin, maxh;
   int tr;             // atoms per tile (32 or 64 streamed, 64 or 128 resident)
   size_t smem;        // dynamic shared memory bytes
   int resident;       // > 0: resident-weight form, persistent grid of this many CTAs
+  int streamed;       // > 0: streamed-weight form, persistent grid of this many CTAs
+  int stages;         // its weight-chunk stages
+  int *status;        // timeout bit of the streamed form's bounded waits
   int ntiles;
   const int *tiles;   // [ntiles][3] = (element, start, count) into perm
   const int *perm;    // atom indices grouped by element
@@ -116,6 +125,13 @@ size_t mlp_fp32_smem(int nl, const int *sizes, int tr);
 // atoms on 512 threads, or 64 on 256 when the wider tile does not fit).
 size_t mlp_fp32r_smem(int nl, const int *sizes, int tr);
 void mlp_fp32_prepare(int tr, size_t smem, bool resident);
+// Streamed-weight form (weights too large for shared memory): dynamic shared
+// memory and weight stages, 0 if unsupported (residual layers, widths not
+// multiples of 32); host packing of one layer's W into its chunk layouts.
+size_t mlp_fp32s_smem(int nl, const int *sizes, int resnet, int *stages);
+void mlp_fp32s_pack(const float *W, int K, int N, std::vector<float> &fwd,
+                    std::vector<float> &bwd);
+void mlp_fp32s_prepare(size_t smem);
 
 // Tensor-core (tcgen05) MLP, BF16 operands.  Weights are packed on the host
 // in 64-column chunks of the K-major core-matrix layout (pack_core_chunks).

@@ -117,6 +117,21 @@ def test_three_elements_against_oracle():
     assert out["energy"] * pub["replicas"] == pytest.approx(pub["energy_total"], abs=1.0)
 
 
+def test_wide_mlp_streamed_weights_against_oracle(tmp_path):
+    """The precision config's potential (4 elements, 32 filters, rc 6.5,
+    512-128-128-128-1 softplus): its FP32 weights do not fit in shared
+    memory, so the plain form streams them in chunks.  10,976 atoms = 172
+    tiles of 64 atoms, more than one per SM."""
+    p = tmp_path / "alloy.npz"
+    syms = synth.gaussian_potential(p, seed=99, **synth.config("alloy432k")["pot"])
+    x, t, box, _ = synth.build_system("fcc", 3.6, (14, 14, 14), sigma=0.05, nelt=4, seed=7)
+    _, s, out = _run(f"{p} {' '.join(syms)}", x, t, box)
+    ref = Oracle(load_npz(p)).compute(x, t - 1, box, [1, 1, 1], skin=1.0)
+    _check(out, ref, len(x))
+    again = s.compute(1, 1, 1.0)
+    assert np.array_equal(again["f"], out["f"]) and again["energy"] == out["energy"]
+
+
 @pytest.mark.parametrize("kw", [dict(actfn=1, resnet=1, hidden=(32, 32, 32)),
                                 dict(actfn=3, resnet=0, hidden=(32, 32), fctype=1),
                                 dict(actfn=2, resnet=0, hidden=(64, 64), max_moment=2),
