@@ -254,6 +254,21 @@ int tmd_batch_nvt_run(tmd_batch *batch, int nsteps, double dt, const double *t_s
 typedef struct tmd_server tmd_server;
 int tmd_server_create(const tmd_model *model, int max_atoms, int max_cells,
                       double skin, int steps_per_tick, tmd_server **out);
+/* Admission by HBM footprint: a server sized from a device-memory budget.
+ * The neighbor rows are given the length the densest admissible job needs
+ * (max_density atoms per A^3, the same 30% + 32 margin as any system), and
+ * max_atoms is the number of atoms whose arrays (positions, velocities,
+ * forces, descriptors, MLP rows, neighbor rows, relayout copies, bins) fit in
+ * hbm_bytes at that length.  Jobs are then admitted while their atoms fit, so
+ * the batch never holds more than the budget; tmd_server_submit refuses a job
+ * denser than max_density (TMD_ERR_CAPACITY) instead of growing the rows. */
+int tmd_server_create_bytes(const tmd_model *model, size_t hbm_bytes, double max_density,
+                            int max_cells, double skin, int steps_per_tick,
+                            tmd_server **out);
+/* Device bytes the server's arrays hold at its current neighbor-row length,
+ * its atom capacity and that row length (entries per atom). */
+int tmd_server_footprint(const tmd_server *server, size_t *device_bytes, int *max_atoms,
+                         int *row_length);
 void tmd_server_free(tmd_server *server);
 int tmd_server_submit(tmd_server *server, int kind, int n, const double *x,
                       const int *type, const double *v, const double box[9],

@@ -18,6 +18,7 @@
 // system per process (pair_tensormd.cpp:141-184); the batch gives each cell
 // the results that system would give.
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -64,6 +65,7 @@ struct tmd_server {
   const tmd_model *m = nullptr;
   tmd_system *s = nullptr;
   int max_atoms = 0, max_cells = 0, steps_per_tick = 8;
+  int max_cap = 0;  // > 0: longest neighbor row the HBM budget allows (byte-budget servers)
   // shared with callers
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -115,6 +117,30 @@ CellCtl initial_ctl(const Job &j) {
   return q;
 }
 
+// Device bytes per atom of a server whose neighbor rows hold `cap` entries:
+// the system's and the server's per-atom arrays, cap x 64 B of rows (tmp,
+// nbr, rev and the relayout copy of rev: 4 B each; pair forces 16 B; pair
+// geometry 32 B) and the neighbor bins (at most about two per atom).
+size_t server_bytes_per_atom(const tmd_model *m, int cap) {
+  const HostModel &h = m->h;
+  const size_t B = h.nelt, nin = h.nin;
+  size_t a = 4 * 24 + 12 + 4;          // x, v, f, xbuild; image; element
+  a += 3 * 4;                          // bin of atom, binned atoms, raw row length
+  a += 4 * (B + 1) + 4 * B;            // row block offsets, active pairs per block
+  a += 4 * B * h.K * h.D + 2 * 4 * nin;  // P; G and dE/dG
+  a += 8 + 48 + 8 + 48 + 8 + 4 + 4;    // E, virial partials, eatom, vatom, ke, perm, cell
+  a += 4 * 24 + 12 + 4 + 4 * (B + 1);  // relayout copies: x v f xbuild, image, element, offsets
+  a += 48 + 4 + 24 + 8;                // staging x v, staging element, FIRE power, |F|^2
+  a += 2 * 12;                         // bins: count, start, cursor
+  a += (size_t)cap * 64;
+  return a;
+}
+
+// Row length (a multiple of 32) a job of n atoms in box volume vol needs.
+int job_cap(const tmd_server *sv, int n, double vol) {
+  return (cap_for_density(sv->s, n / vol) + 31) / 32 * 32;
+}
+
 // Move every atom into the layout described by sv->src / sv->fresh (already
 // on the device, with acell and coff) with neighbor rows of cap1 entries, and
 // swap the moved arrays in.  Rows of the same length go through the build
@@ -122,6 +148,8 @@ CellCtl initial_ctl(const Job &j) {
 int move_cells(tmd_server *sv, int n, int cap1) {
   tmd_system *s = sv->s;
   if (cap1 > 4096) return fail(TMD_ERR_CAPACITY, "more than 4096 neighbors per atom");
+  if (sv->max_cap > 0 && cap1 > sv->max_cap)
+    return fail(TMD_ERR_CAPACITY, "neighbor rows beyond the server's HBM budget");
   const bool same = cap1 == s->cap && s->nbr && s->tmp && sv->rev2;
   uint32_t *nbr2 = same ? s->tmp : nullptr;
   int *rev2 = same ? sv->rev2 : nullptr;
@@ -282,7 +310,8 @@ int relayout(tmd_server *sv, const std::vector<JobP> &next) {
   }
   launch_srv_acell(C, s->coff, s->acell, s->st, s->launches);
   // row length: the current one unless a fresh cell is denser than it allows
-  int cap1 = s->cap;
+  // (a byte-budget server holds rows of its full length from the start)
+  int cap1 = std::max(s->cap, sv->max_cap);
   if (staged > 0) {
     double dens = 0.0;
     for (int c = 0; c < C; c++)
@@ -551,6 +580,40 @@ int tmd_server_create(const tmd_model *m, int max_atoms, int max_cells, double s
   return TMD_OK;
 }
 
+int tmd_server_create_bytes(const tmd_model *m, size_t hbm_bytes, double max_density,
+                            int max_cells, double skin, int steps_per_tick, tmd_server **out) {
+  if (!m || !out || !(max_density > 0) || !(skin >= 0) || max_cells < 1)
+    return fail(TMD_ERR_ARG, "bad server arguments");
+  *out = nullptr;
+  // the row length of the densest admissible job, then as many atoms as fit
+  const double cut = m->h.rmax + skin;
+  const double est = max_density * 4.0 / 3.0 * M_PI * cut * cut * cut;
+  int cap = std::max((int)std::ceil(1.3 * est) + 32, 64);
+  cap = (cap + 31) / 32 * 32;
+  if (cap > 4096) return fail(TMD_ERR_CAPACITY, "density needs more than 4096 neighbors per atom");
+  const size_t per = server_bytes_per_atom(m, cap);
+  const size_t cell_bytes = (size_t)max_cells * 160;  // boxes, geometry, sums, controls
+  if (hbm_bytes <= cell_bytes + per) return fail(TMD_ERR_CAPACITY, "HBM budget below one atom");
+  const size_t atoms = (hbm_bytes - cell_bytes) / per;
+  if (atoms > (size_t)kMaxAtoms) return fail(TMD_ERR_CAPACITY, "HBM budget beyond the atom index range");
+  int rc = tmd_server_create(m, (int)atoms, max_cells, skin, steps_per_tick, out);
+  if (rc) return rc;
+  (*out)->max_cap = cap;
+  return TMD_OK;
+}
+
+int tmd_server_footprint(const tmd_server *sv, size_t *device_bytes, int *max_atoms,
+                         int *row_length) {
+  if (!sv) return fail(TMD_ERR_ARG, "null server");
+  const int cap = std::max(sv->s->cap, sv->max_cap);
+  if (device_bytes)
+    *device_bytes = (size_t)sv->max_atoms * server_bytes_per_atom(sv->m, cap) +
+                    (size_t)sv->max_cells * 160;
+  if (max_atoms) *max_atoms = sv->max_atoms;
+  if (row_length) *row_length = cap;
+  return TMD_OK;
+}
+
 void tmd_server_free(tmd_server *sv) {
   if (!sv) return;
   {
@@ -586,6 +649,8 @@ int tmd_server_submit(tmd_server *sv, int kind, int n, const double *x, const in
     std::string why;
     int rc = cell_setup(sv->s, box, pbc, b, g, why);
     if (rc) return fail(rc, "job box: " + why);
+    if (sv->max_cap > 0 && job_cap(sv, n, b.xprd * b.yprd * b.zprd) > sv->max_cap)
+      return fail(TMD_ERR_CAPACITY, "job denser than the server's HBM budget allows");
   }
   auto j = std::make_shared<Job>();
   j->kind = kind;

@@ -62,6 +62,9 @@ SIGNATURES = [
     ("tmd_server_wait", _c_int, [_vp, _c_long, _c_double, _pd, _pd, _pd, _pd, _pd, _pi, _pd]),
     ("tmd_server_stats", _c_int, [_vp, _pl, _pl, _pl, _pd, _pd]),
     ("tmd_server_timing", _c_int, [_vp, _pd]),
+    ("tmd_server_create_bytes", _c_int, [_vp, ctypes.c_size_t, _c_double, _c_int, _c_double,
+                                         _c_int, ctypes.POINTER(_vp)]),
+    ("tmd_server_footprint", _c_int, [_vp, ctypes.POINTER(ctypes.c_size_t), _pi, _pi]),
     ("tmd_neighbor_list_noalloc", _c_int, [_vp, _c_int, _pd, _pi, _c_double, _c_int, _vp,
                                            _vp, _vp]),
 ]

@@ -317,15 +317,31 @@ class TensorMDServer:
 
     ENERGY, NVE, FIRE = 0, 1, 2
 
-    def __init__(self, model: TensorMDModel, max_atoms: int, max_cells: int = 8192,
-                 skin: float = 1.0, steps_per_tick: int = 8):
+    def __init__(self, model: TensorMDModel, max_atoms: int = 0, max_cells: int = 8192,
+                 skin: float = 1.0, steps_per_tick: int = 8, hbm_bytes: int = 0,
+                 max_density: float = 0.0):
+        """Capacity either as max_atoms, or as an HBM budget (hbm_bytes) for
+        jobs up to max_density atoms per A^3 (tmd_server_create_bytes)."""
         self.model = model
         self.lib = model.lib
         h = ctypes.c_void_p()
-        check(self.lib.tmd_server_create(model.h, int(max_atoms), int(max_cells), float(skin),
-                                         int(steps_per_tick), ctypes.byref(h)))
+        if hbm_bytes:
+            check(self.lib.tmd_server_create_bytes(model.h, int(hbm_bytes), float(max_density),
+                                                   int(max_cells), float(skin),
+                                                   int(steps_per_tick), ctypes.byref(h)))
+        else:
+            check(self.lib.tmd_server_create(model.h, int(max_atoms), int(max_cells),
+                                             float(skin), int(steps_per_tick), ctypes.byref(h)))
         self.h = h
         self._n = {}
+
+    def footprint(self):
+        """dict(device_bytes, max_atoms, row_length) (tmd_server_footprint)."""
+        b = ctypes.c_size_t()
+        na, cap = ctypes.c_int(), ctypes.c_int()
+        check(self.lib.tmd_server_footprint(self.h, ctypes.byref(b), ctypes.byref(na),
+                                            ctypes.byref(cap)))
+        return dict(device_bytes=b.value, max_atoms=na.value, row_length=cap.value)
 
     def close(self):
         if getattr(self, "h", None):

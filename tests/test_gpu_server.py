@@ -94,12 +94,23 @@ def test_nve_job_matches_system_run(model4):
     srv.close()
 
 
-def test_trajectory_independent_of_the_mix(model4):
+@pytest.fixture(scope="module")
+def model4_bf16(tmp_path_factory):
+    p = tmp_path_factory.mktemp("pot") / "serve16.npz"
+    syms = synth.gaussian_potential(p, seed=31, nelt=4, num_filters=16, rc=6.0,
+                                    max_moment=3, hidden=(64, 64), actfn=2)
+    return TensorMDModel(f"{p} {' '.join(syms)} precision bf16")
+
+
+@pytest.mark.parametrize("form", ["fp32", "bf16"])
+def test_trajectory_independent_of_the_mix(model4, model4_bf16, form):
     """An NVE and a FIRE job give bitwise the same end state run together
     and inside a batch whose other cells retire and are admitted while they
     run (three cells at most in flight, so retirements move them and admit
-    queued jobs).  Moved cells keep their neighbor lists; a cell's list is rebuilt
-    only when its own atoms trigger it."""
+    queued jobs).  Moved cells keep their neighbor lists; a cell's list is
+    rebuilt only when its own atoms trigger it; the MLP rows (FP32 or
+    tensor-core) are independent atoms."""
+    model4 = model4 if form == "fp32" else model4_bf16
     rng = np.random.default_rng(6)
     a = synth.serving_job(rng, kind=1, nmin=400, nmax=500)
     fj = synth.serving_job(rng, kind=2, nmin=150, nmax=250)
@@ -187,6 +198,32 @@ def test_concurrent_mixed_jobs(model4):
             assert results[i]["steps"] == 40
     st = srv.stats()
     assert st["submitted"] == 30 and st["completed"] == 30 and st["atom_steps"] > 0
+    srv.close()
+
+
+def test_hbm_budget_admission(model4):
+    """A server sized from an HBM budget: its arrays fit the budget, jobs are
+    admitted while their atoms fit (a queue forms beyond that), every job
+    completes, and a job denser than the budget's row length is refused."""
+    budget = 512 << 20
+    srv = TensorMDServer(model4, hbm_bytes=budget, max_density=0.09, max_cells=64,
+                         steps_per_tick=4)
+    fp = srv.footprint()
+    assert fp["device_bytes"] <= budget and fp["max_atoms"] > 5000
+    rng = np.random.default_rng(9)
+    jobs = [synth.serving_job(rng, kind=1, nmin=2000, nmax=4000) for _ in range(12)]
+    assert sum(len(j[0]) for j in jobs) > fp["max_atoms"]  # not all fit at once
+    tks = [srv.submit(1, x, t, box, v=v, nsteps=12, dt=0.001) for x, t, box, v in jobs]
+    for tk in tks:
+        assert srv.wait(tk, timeout=300)["steps"] == 12
+    st = srv.stats()
+    assert st["completed"] == 12 and st["active_atoms"] <= fp["max_atoms"]
+    # a compressed lattice (about 0.34 atoms/A^3) needs longer rows than the budget
+    x, t, box, _ = synth.build_system("fcc", 2.3, (4, 4, 4), sigma=0.0, nelt=1, seed=1)
+    with pytest.raises(TmdError) as e:
+        srv.submit(0, x, t, box)
+    assert e.value.code == -4
+    assert srv.footprint()["row_length"] == fp["row_length"]
     srv.close()
 
 
