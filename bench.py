@@ -739,10 +739,28 @@ def cpu_baseline(cfg_name, samples=2):
     o.nve(x, v, t - 1, box, [1, 1, 1], 0.001, samples - 1, skin=1.0)
     t1 = time.perf_counter()
     val = len(x) * samples / (t1 - t0)
-    return {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{samples} full MD steps (neighbor rebuild + FP64 force) of the "
-                      f"{cfg['natoms']}-atom workload, oracle/tmd_oracle.c, OpenMP "
-                      f"{cores} threads"}
+    out = {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"{samples} full MD steps (neighbor rebuild + FP64 force) of the "
+                     f"{cfg['natoms']}-atom workload, oracle/tmd_oracle.c, OpenMP "
+                     f"{cores} threads"}
+    # one thread, on the 4,000-atom FCC config (2 MD steps: about 2 s)
+    try:
+        import ctypes
+        gomp = ctypes.CDLL("libgomp.so.1")  # the OpenMP runtime the oracle runs on
+        pot1, syms1, x1, t1_, box1, v1, cfg1 = workload("fcc4k", seed=42)
+        o1 = Oracle(load_npz(pot1))
+        gomp.omp_set_num_threads(1)
+        o1.nve(x1[:8], v1[:8], (t1_ - 1)[:8], box1, [1, 1, 1], 0.001, 1)
+        s0 = time.perf_counter()
+        o1.nve(x1, v1, t1_ - 1, box1, [1, 1, 1], 0.001, 1, skin=1.0)
+        s1 = time.perf_counter()
+        gomp.omp_set_num_threads(cores)
+        out["single_thread"] = {"value": len(x1) * 2 / (s1 - s0), "unit": UNIT, "cores": 1,
+                                "sample": "2 full MD steps of the 4,000-atom FCC config "
+                                          "(fcc4k), 1 OpenMP thread"}
+    except OSError as exc:  # no libgomp under that name: report, do not hide
+        out["single_thread"] = {"error": str(exc)}
+    return out
 
 
 def run_reference(args, rank, world):
