@@ -125,12 +125,14 @@ int cells_geometry(tmd_system *s, const double *boxes, const int *pbc) {
   if (nbins > (1L << 30)) return fail(TMD_ERR_CAPACITY, "too many neighbor bins");
   drop_graph(s);
   if (nbins > s->ncell_alloc) {
+    // with headroom: a server's layouts grow a little at a time
+    const long alloc = std::min(nbins + nbins / 2 + 1024, 1L << 30);
     dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_cursor);
     s->ncell_alloc = 0;
-    TMD_CUDA(dalloc(&s->cell_count, nbins));
-    TMD_CUDA(dalloc(&s->cell_start, nbins + 1));
-    TMD_CUDA(dalloc(&s->cell_cursor, nbins));
-    s->ncell_alloc = (int)nbins;
+    TMD_CUDA(dalloc(&s->cell_count, alloc));
+    TMD_CUDA(dalloc(&s->cell_start, alloc + 1));
+    TMD_CUDA(dalloc(&s->cell_cursor, alloc));
+    s->ncell_alloc = (int)alloc;
   }
   s->nbins = (int)nbins;
   TMD_CUDA(cudaMemcpyAsync(s->cbox, hb.data(), C * sizeof(BoxP), cudaMemcpyHostToDevice, s->st));

@@ -528,12 +528,27 @@ void worker_main(tmd_server *sv) {
   }
 }
 
+int server_create(const tmd_model *m, int max_atoms, int max_cells, double skin,
+                  int steps_per_tick, int row_cap, tmd_server **out);
+
 }  // namespace
 
 extern "C" {
 
 int tmd_server_create(const tmd_model *m, int max_atoms, int max_cells, double skin,
                       int steps_per_tick, tmd_server **out) {
+  return server_create(m, max_atoms, max_cells, skin, steps_per_tick, 0, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// row_cap > 0: neighbor rows of exactly this length for the server's life
+// (byte-budget servers); 0: rows for jobs up to 0.09 atoms/A^3, longer when
+// a denser job comes
+int server_create(const tmd_model *m, int max_atoms, int max_cells, double skin,
+                  int steps_per_tick, int row_cap, tmd_server **out) {
   if (!m || !out || max_atoms < 1 || max_cells < 1 || steps_per_tick < 1)
     return fail(TMD_ERR_ARG, "bad server arguments");
   *out = nullptr;
@@ -575,10 +590,22 @@ int tmd_server_create(const tmd_model *m, int max_atoms, int max_cells, double s
     return fail(TMD_ERR_CUDA, std::string("server allocation: ") + cudaGetErrorString(e));
   }
   s->have_box = true;
+  // neighbor rows up front, so that admissions move data instead of
+  // allocating it
+  sv->max_cap = row_cap;
+  rc = move_cells(sv, 0, row_cap > 0 ? row_cap : (cap_for_density(s, 0.09) + 31) / 32 * 32);
+  if (rc) {
+    tmd_server_free(sv);
+    return rc;
+  }
   sv->worker = std::thread(worker_main, sv);
   *out = sv;
   return TMD_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int tmd_server_create_bytes(const tmd_model *m, size_t hbm_bytes, double max_density,
                             int max_cells, double skin, int steps_per_tick, tmd_server **out) {
@@ -596,10 +623,7 @@ int tmd_server_create_bytes(const tmd_model *m, size_t hbm_bytes, double max_den
   if (hbm_bytes <= cell_bytes + per) return fail(TMD_ERR_CAPACITY, "HBM budget below one atom");
   const size_t atoms = (hbm_bytes - cell_bytes) / per;
   if (atoms > (size_t)kMaxAtoms) return fail(TMD_ERR_CAPACITY, "HBM budget beyond the atom index range");
-  int rc = tmd_server_create(m, (int)atoms, max_cells, skin, steps_per_tick, out);
-  if (rc) return rc;
-  (*out)->max_cap = cap;
-  return TMD_OK;
+  return server_create(m, (int)atoms, max_cells, skin, steps_per_tick, cap, out);
 }
 
 int tmd_server_footprint(const tmd_server *sv, size_t *device_bytes, int *max_atoms,
