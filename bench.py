@@ -75,6 +75,23 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(value, world, device):
+    """The largest of every rank's value, on every rank (the slowest replica's
+    time is the job's time)."""
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(atoms_per_rank, steps, world, ms_max):
+    """Whole-job atom-steps/s of `world` replicas of `atoms_per_rank` atoms that
+    each ran `steps` steps, timed by the slowest one (ms_max milliseconds)."""
+    return atoms_per_rank * steps * world / (ms_max / 1000.0)
+
+
 def workload(cfg_name, seed):
     from tmd_b200 import synth
     c = synth.config(cfg_name)
@@ -216,7 +233,9 @@ def run_ours(args, rank, world, local):
     stream = torch.cuda.ExternalStream(sys_.stream(), device=dev)
     if world > 1:
         import torch.distributed as dist
-        dist.init_process_group("nccl", device_id=dev)
+        import datetime
+        # ranks that wait for one another end with an error within minutes
+        dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(seconds=300))
     dt = 0.001
 
     def barrier():
@@ -241,12 +260,8 @@ def run_ours(args, rank, world, local):
     barrier()
     ms = e0.elapsed_time(e1)
     launches = sys_.launches() - l0
-    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = n * args.steps * world / (ms_max / 1000.0)
+    ms_max = max_over_ranks(ms, world, dev)
+    value = replicas_value(n, args.steps, world, ms_max)
 
     # per-kernel device times of the same step sequence (a second, profiled pass)
     sys_.profile(True)
@@ -327,11 +342,8 @@ def run_ours(args, rank, world, local):
     for _ in range(args.e2e_steps):
         e2e_step()
     t1 = time.perf_counter()
-    e2e_s = torch.tensor([t1 - t0], device=dev, dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
-    e2e_val = n * args.e2e_steps * world / float(e2e_s.item())
+    e2e_val = replicas_value(n, args.e2e_steps, world,
+                             1000.0 * max_over_ranks(t1 - t0, world, dev))
 
     # tensor-core MLP forms of the same workload (same steps, same timing)
     forms = {"fp32": {"value": value, "ms_per_step": ms_max / args.steps,
@@ -361,11 +373,7 @@ def run_ours(args, rank, world, local):
             sb.nve_run(args.steps, dt)
             b1.record(sb_stream)
             torch.cuda.synchronize()
-            bms = torch.tensor([b0.elapsed_time(b1)], device=dev, dtype=torch.float64)
-            if world > 1:
-                import torch.distributed as dist
-                dist.all_reduce(bms, op=dist.ReduceOp.MAX)
-            bms = float(bms.item())
+            bms = max_over_ranks(b0.elapsed_time(b1), world, dev)
             sb.profile(True)
             sb.profile_read(reset=True)
             sb.nve_run(nprof, dt)
@@ -478,11 +486,7 @@ def run_alloy(args, rank, world, local, dev, barrier):
         s_.nve_run(args.precision_steps, dt)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
-        if world > 1:
-            import torch.distributed as dist
-            dist.all_reduce(ms, op=dist.ReduceOp.MAX)
-        ms = float(ms.item())
+        ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
         s_.profile(True)
         s_.profile_read(reset=True)
         s_.nve_run(5, dt)
@@ -534,11 +538,7 @@ def run_cells(args, rank, world, local, dev, barrier):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    ms = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
-    ms = float(ms.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
     launches = sv.launches() - l0
     sv.profile(True)
     sv.profile_read(reset=True)
@@ -573,11 +573,7 @@ def run_cells(args, rank, world, local, dev, barrier):
                 q1.record(st_b)
                 torch.cuda.synchronize()
                 barrier()
-                msb = torch.tensor([q0.elapsed_time(q1)], device=dev, dtype=torch.float64)
-                if world > 1:
-                    import torch.distributed as dist
-                    dist.all_reduce(msb, op=dist.ReduceOp.MAX)
-                msb = float(msb.item())
+                msb = max_over_ranks(q0.elapsed_time(q1), world, dev)
                 forms[prec] = {"value": n * nsteps_f * world / (msb / 1000.0),
                                "ms_per_step": msb / nsteps_f, "steps": nsteps_f,
                                "force_rms_err_vs_fp32_eV_per_A": err}
@@ -634,11 +630,7 @@ def run_w23k(args, rank, world, local, dev, barrier):
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     barrier()
-    ms = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
-    ms = float(ms.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
     value = n * 100 * world / (ms / 1000.0)
     form = {"chosen": s.force_variant(), "ms_per_launch": tune_ms,
             "descriptor_chosen": s.descriptor_variant(), "descriptor_ms_per_launch": tune_dms}
