@@ -80,6 +80,36 @@ def test_batch_equals_separate_systems(pot2):
         np.testing.assert_allclose(out["virial"][c], ref["virial"], rtol=1e-12, atol=1e-10)
 
 
+def test_batch_non_periodic_cells(pot2):
+    """A slab (periodic in x and y, the box 10 A taller than the atoms), a
+    cluster (periodic in no direction) and a periodic cell in one batch: each
+    cell's bin grid takes no image shift along its non-periodic axes.  Forces
+    bit-identical to separate systems with the same boundaries."""
+    p, syms = pot2
+    args = f"{p} {' '.join(syms)}"
+    x, t, box, _ = synth.build_system("fcc", 3.6, (3, 3, 3), sigma=0.05, nelt=2, seed=11)
+    slab_box = box.copy()
+    slab_box[5] += 10.0
+    cl_box = box.copy()
+    cl_box[3:6] += 12.0
+    cells = [(x + np.array([0.0, 0.0, 5.0]), t, slab_box, (1, 1, 0)),
+             (x + 6.0, t, cl_box, (0, 0, 0)),
+             (x, t, box, (1, 1, 1))]
+    m = TensorMDModel(args)
+    b = TensorMDBatch(m, [len(c[0]) for c in cells], 1.0)
+    b.set_cells(np.stack([c[2] for c in cells]), np.array([c[3] for c in cells]))
+    b.set_atoms(np.concatenate([c[0] for c in cells]), np.concatenate([c[1] for c in cells]))
+    out = b.compute()
+    off = b.offsets
+    for c, (xc, tc, bc, pbc) in enumerate(cells):
+        s = TensorMDSystem(m, len(xc), 1.0)
+        s.set_box(bc, pbc)
+        s.set_atoms(xc, tc)
+        ref = s.compute(1, 1)
+        assert np.array_equal(out["f"][off[c]:off[c + 1]], ref["f"]), c
+        assert out["energy"][c] == pytest.approx(ref["energy"], rel=1e-12, abs=1e-10)
+
+
 def test_batch_against_oracle(pot2):
     p, syms = pot2
     cells = _cells()

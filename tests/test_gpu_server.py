@@ -15,6 +15,7 @@
   errors             unknown kind, job beyond the atom budget, box too small
                      for the cutoff, wait timeout"""
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -139,6 +140,36 @@ def test_trajectory_independent_of_the_mix(model4, model4_bf16, form):
             assert np.array_equal(o1[key], o2[key]), key
         assert o1["energy"] == o2["energy"]
         assert np.array_equal(o1["virial"], o2["virial"])
+
+
+def test_rows_grow_under_running_jobs(model4):
+    """A job denser than the rows were sized for (FCC a = 3.3 A: 0.11
+    atoms/A^3) arrives while an NVE job runs: every cell's rows move to the
+    longer length (atom indices and partner slots re-based), and the running
+    job's end state is bitwise the one it has without the dense neighbour."""
+    rng = np.random.default_rng(12)
+    a = synth.serving_job(rng, kind=1, nmin=400, nmax=500)
+    dense = synth.build_system("fcc", 3.3, (3, 3, 3), sigma=0.05, nelt=2, seed=4)
+
+    def run(with_dense):
+        srv = TensorMDServer(model4, max_atoms=50000, max_cells=8, steps_per_tick=4)
+        row0 = srv.footprint()["row_length"]
+        x, t, box, v = a
+        tk = srv.submit(1, x, t, box, v=v, nsteps=40, dt=0.002)
+        if with_dense:
+            while srv.stats()["active_atoms"] == 0:  # the first job is in flight
+                time.sleep(0.0005)
+            xd, td, boxd, vd = dense
+            srv.wait(srv.submit(1, xd, td, boxd, v=vd, nsteps=8, dt=0.001), timeout=120)
+            assert srv.footprint()["row_length"] > row0
+        out = srv.wait(tk, timeout=120)
+        srv.close()
+        return out
+
+    o1, o2 = run(False), run(True)
+    for key in ("x", "v", "f"):
+        assert np.array_equal(o1[key], o2[key]), key
+    assert o1["energy"] == o2["energy"]
 
 
 def test_fire_job_relaxes(model4):
