@@ -196,15 +196,21 @@ def ncu_traffic(config, kernel):
 def algorithmic(cfg, npairs_rc, nlist, B, K, D, nin, form):
     """Algorithmic FLOPs and HBM bytes per launch of the force kernel.
 
-    FLOPs: the U and V contractions, 2 x (2 K D) per pair inside rc
-    (tensor_ops.cpp kernel_U / kernel_V).  Bytes, each input read once and
+    FLOPs, the per-atom work of the force step (everything after the MLP but
+    the gather): per pair inside rc the U and V contractions 2 x (2 K D)
+    (tensor_ops.cpp kernel_U / kernel_V), the radial functions and their
+    derivatives 10 K, F1 2 K + 3, F2 2 D + 3 and the monomial derivatives 6 D;
+    per atom and element block dE/dP (2 M + 1) D K (M invariants per filter,
+    tensor_ops.cpp kernel_dEdS).  Bytes, each input read once and
     each output written once: P (4 B K D B/atom), G and dE/dG (2 x 4 nin),
     virial partials (48 B/atom), and per pair either (pair-lane forms) the
     descriptor step's compact pair geometry (32 B per pair inside rc) and the
     pair force (16 B), or (filter-lane form) x (24 B/atom), the neighbor row
     (4 B/entry) and the pair force of every entry (16 B)."""
     n = cfg["natoms"]
-    flops = 4.0 * K * D * npairs_rc
+    M = {1: 1, 4: 2, 10: 3, 20: 4}[D]
+    flops = npairs_rc * (4.0 * K * D + 10.0 * K + (2 * K + 3) + (2 * D + 3) + 6.0 * D) \
+        + n * B * (2 * M + 1) * D * K
     per_atom = 4 * B * K * D + 8 * nin + 48
     if form == "filter_lane":
         bytes_ = n * (24 + per_atom) + nlist * (4 + 16)
