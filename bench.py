@@ -305,6 +305,41 @@ def run_ours(args, rank, world, local):
                                     "(no FP32 figure in MEASURED_PEAKS.json)",
                      "algorithmic_flops_per_launch": flops}
     kernel_ms = {k: (c, t / max(c, 1)) for k, (c, t) in prof.items()}
+    # the other step kernels against their bounds (same profiled pass);
+    # algorithmic work per launch, per the survey's per-atom figures
+    Minv = {1: 1, 4: 2, 10: 3, 20: 4}[D]
+    sz = cfg["mlp"]
+    mlp_macs = sum(a * b for a, b in zip(sz[:-1], sz[1:])) \
+        + sum(a * b for a, b in zip(sz[:-2], sz[1:-1]))
+
+    def kms(name):
+        c, tt = prof[name]
+        return tt / max(c, 1)
+
+    def fp32_row(name, fl):
+        ms_ = kms(name)
+        tf = fl / (ms_ / 1000.0) / 1e12
+        return {"ms": ms_, "bound": "fp32", "flops": fl, "achieved_tflops": tf,
+                "frac": tf / fp32_peak}
+
+    desc_flops = npairs_rc * (2.0 * K * D + 10.0 * K + D) + n * B * (2 * Minv + 1) * D * K
+    # each pair force is read twice (as an atom's own and as its partner's)
+    # but needs to leave HBM once
+    gather_bytes = nlist * (16 + 4) + n * (24 + 4)
+    g_ms = kms("gather")
+    kernel_roofline = {
+        "descriptor": fp32_row("descriptor", desc_flops),
+        "mlp": fp32_row("mlp", 2.0 * n * mlp_macs),
+        "force": fp32_row("force", flops),
+        "gather": {"ms": g_ms, "bound": "hbm", "bytes": gather_bytes,
+                   "achieved_gbs": gather_bytes / (g_ms / 1000.0) / 1e9,
+                   "frac": gather_bytes / (g_ms / 1000.0) / 1e9 / hbm_peak},
+        "work": "descriptor: per pair inside rc P 2KD + radial 10K + monomials D, per atom "
+                "and block G (2M+1)DK; mlp: 2 x (forward + backward MACs) per atom; force: "
+                "as roofline_fp32; gather: per list entry its pair force (16 B, read "
+                "once; the partner read is the same array) and partner slot (4 B), per atom "
+                "force (24 B) and row length",
+    }
 
     # e2e through the reference-facing call pattern (host buffers)
     sys_.set_atoms(x, t, v)
@@ -439,6 +474,7 @@ def run_ours(args, rank, world, local):
             "clocks": clocks,
             "roofline": roofline,
             "roofline_fp32": roofline_fp32,
+            "kernel_roofline": kernel_roofline,
             "kernel_ms": kernel_ms,
             "force_form": force_form,
             "forms": forms,
