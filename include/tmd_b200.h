@@ -228,7 +228,8 @@ int tmd_batch_nvt_run(tmd_batch *batch, int nsteps, double dt, const double *t_s
  * A job server on one GPU: callers submit independent small systems from any
  * thread; one library thread keeps every job in flight as a cell of one
  * multi-cell batch and advances all of them together (continuous batching:
- * finished jobs leave and queued jobs join between ticks, FIFO, within
+ * finished jobs leave and queued jobs join between ticks, single-point jobs
+ * ahead of the queue (they hold atoms for one tick only), the others FIFO, within
  * max_atoms / max_cells; each tick runs steps_per_tick steps).  There is no
  * counterpart in the reference, which runs one LAMMPS system per process.
  * Job kinds:

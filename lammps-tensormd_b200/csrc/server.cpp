@@ -4,11 +4,10 @@
 // Callers submit jobs from any thread (tmd_server_submit) and collect results
 // (tmd_server_wait).  One worker thread owns the device: it keeps every job
 // in flight as a cell of one multi-cell system (batch.cpp) and repeats ticks:
-//   1. retire finished cells and admit queued jobs (FIFO, up to the atom and
-//      cell budget), re-laying the cells out on the device (positions,
-//      velocities, forces and image counters of continuing cells gathered
-//      into the new order, new jobs appended from a staging upload), then a
-//      neighbor rebuild;
+//   1. retire finished cells and admit queued jobs (single-point jobs first,
+//      then FIFO, up to the atom and cell budget), re-laying the cells out on
+//      the device: continuing cells move with their state and neighbor lists,
+//      new jobs come from a staging upload and get their lists built;
 //   2. one force evaluation: single-point jobs are finished by it, FIRE jobs
 //      that already satisfy fmax too; these leave before the steps;
 //   3. steps_per_tick steps of the mixed integrator (server_kernels.cu) for the rest;
@@ -403,8 +402,9 @@ std::vector<JobP> survivors(tmd_server *sv, const std::vector<char> &gone) {
 
 int tick(tmd_server *sv) {
   tmd_system *s = sv->s;
-  // 1. admission (FIFO within the budget); jobs finished by the last tick's
-  // steps leave with the same relayout
+  // 1. admission within the budget: queued single-point jobs first (they
+  // hold atoms only for the tick that evaluates them), then the others FIFO;
+  // jobs finished by the last tick's steps leave with the same relayout
   std::vector<JobP> next;
   long atoms = 0;
   for (auto &j : sv->active)
@@ -416,11 +416,23 @@ int tick(tmd_server *sv) {
   size_t nadm = 0;
   {
     std::lock_guard<std::mutex> lk(sv->mu);
-    while (!sv->queue.empty()) {
-      const JobP &j = sv->queue.front();
-      if (atoms + j->n > sv->max_atoms || (int)next.size() >= sv->max_cells) break;
-      atoms += j->n;
-      next.push_back(j);
+    auto fits = [&](const Job &j) {
+      return atoms + j.n <= sv->max_atoms && (int)next.size() < sv->max_cells;
+    };
+    std::deque<JobP> rest;
+    for (auto &j : sv->queue) {
+      if (j->kind == kJobEnergy && fits(*j)) {
+        atoms += j->n;
+        next.push_back(j);
+        nadm++;
+      } else {
+        rest.push_back(j);
+      }
+    }
+    sv->queue.swap(rest);
+    while (!sv->queue.empty() && fits(*sv->queue.front())) {
+      atoms += sv->queue.front()->n;
+      next.push_back(sv->queue.front());
       sv->queue.pop_front();
       nadm++;
     }
