@@ -4,10 +4,9 @@ A batch of C cells must give, cell by cell, what C separate systems give:
   forces        bit-identical to the separate systems (same neighbor rows after
                 sorting, same per-pair arithmetic, same per-atom MLP rows)
   energy/virial per-cell FP64 sums in another fixed order: relative 1e-12
-  NVE thermo    1e-12 at step 0; per cell within 1e-6 relative of separate
-                runs after 60 steps (the batch rebuilds all cells when any
-                atom of any cell needs it, and wrapping at a rebuild moves the
-                FP64 rounding of positions)
+  NVE runs     per cell bitwise the positions, velocities, forces and image
+                counters of separate runs (a cell's list is rebuilt when its
+                own atoms trigger it); thermo sums 1e-12 relative
 and the FP64 oracle, cell by cell, within the plain-form tolerances
 (force relative RMS 1e-5, energy 5e-7 eV/atom, virial 1e-5).
 Cells cover FCC and BCC lattices, a triclinic cell and cells smaller than the
@@ -152,16 +151,19 @@ def test_batch_nve_matches_separate_runs(pot2):
     _, b = _batch(args, cells, v=data["v"])
     th = b.nve_run(60, 0.001, thermo_every=20)
     assert th.shape == (4, 6, 2)
+    bx, bv, bf, bimg = b.get()
+    off = b.offsets
     for c, (x, t, box, v) in enumerate(data["cells"]):
         _, s = _separate(args, x, t, box, v=v)
         ref = s.nve_run(60, 0.001, thermo_every=20)
-        # the starting state agrees to the order of the FP64 sums; after a
-        # rebuild the FP64 image construction rounds differently (positions
-        # wrapped at other steps), an FP32 distance occasionally lands one ulp
-        # apart and the difference grows over the run (2.5e-8 relative seen at
-        # step 60)
-        np.testing.assert_allclose(th[0, c, :], ref[0], rtol=1e-12)
-        np.testing.assert_allclose(th[:, c, :], ref, rtol=1e-6, atol=1e-6)
+        # a cell rebuilds its list exactly when its own atoms trigger it, as
+        # the separate system does, so the trajectories are the same bit for
+        # bit; the thermo sums run in another order
+        sx, sv, sf, simg = s.get()
+        sl = slice(off[c], off[c + 1])
+        assert np.array_equal(bx[sl], sx) and np.array_equal(bv[sl], sv), c
+        assert np.array_equal(bf[sl], sf) and np.array_equal(bimg[sl], simg), c
+        np.testing.assert_allclose(th[:, c, :], ref, rtol=1e-12, atol=1e-12)
     # total energy per cell is conserved over the run
     etot = th.sum(-1)
     assert np.abs(etot - etot[0]).max() < 1e-3 * 256
