@@ -88,7 +88,10 @@ int tmd_system_set_atoms(tmd_system *sys, int n, const double *x,
                          const int *type, const double *v);
 
 /* Replace positions only (same n and types); the cheap per-step upload of
- * the LAMMPS drop-in.  Triggers a rebuild check on the next compute. */
+ * the LAMMPS drop-in.  The positions may be in any periodic frame (wrapped by
+ * the caller at its own times, or never): each atom takes the periodic image
+ * nearest its position at the last neighbor build, so the list stays valid
+ * and only real motion (more than skin/2) triggers a rebuild. */
 int tmd_system_set_positions(tmd_system *sys, const double *x);
 
 /* Download state; NULL pointers are skipped.  image[n*3] are the periodic

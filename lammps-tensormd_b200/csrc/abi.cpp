@@ -1050,6 +1050,8 @@ int tmd_system_set_positions(tmd_system *s, const double *x) {
   if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms first");
   if (s->n == 0) return TMD_OK;
   TMD_CUDA(cudaMemcpyAsync(s->x, x, 3 * s->n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  launch_nearest_image(s->n, s->x, s->xbuild, s->box, s->ncells ? s->cbox : nullptr, s->acell,
+                       s->st, s->launches);
   s->forces_valid = false;
   double half = 0.5 * s->skin;
   launch_neighbor_check(s->n, s->x, s->xbuild, half * half, s->flag, s->st, s->launches,

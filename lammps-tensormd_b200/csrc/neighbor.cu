@@ -760,6 +760,45 @@ __global__ void k_nb_finish(int n, const double *__restrict__ x,
   }
 }
 
+// Positions handed over by a caller each step (tmd_system_set_positions) are
+// in the caller's periodic frame, which wraps atoms at other times than the
+// list build does (LAMMPS wraps at its own reneighboring, a caller's
+// integrator may never wrap).  Each atom takes the periodic image of its new
+// position nearest to its position at the last build, so the list's image
+// shifts stay valid and the displacement check sees the atom's motion rather
+// than a box vector.  Shifts beyond 3 cells per axis are left alone (the
+// check then rebuilds).  Image counters keep counting the device's own wraps.
+__global__ void k_nearest_image(int n, double *__restrict__ x,
+                                const double *__restrict__ xbuild, BoxP box,
+                                const BoxP *__restrict__ cbox, const int *__restrict__ acell) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const BoxP &b = cbox ? cbox[acell[i]] : box;
+  double f[3], g[3];
+  frac_of(b, x[3 * i], x[3 * i + 1], x[3 * i + 2], f[0], f[1], f[2]);
+  frac_of(b, xbuild[3 * i], xbuild[3 * i + 1], xbuild[3 * i + 2], g[0], g[1], g[2]);
+  int k[3] = {0, 0, 0};
+  for (int a = 0; a < 3; a++) {
+    if (!b.pbc[a]) continue;
+    const double d = rint(f[a] - g[a]);
+    if (fabs(d) <= kShiftR) k[a] = (int)d;
+  }
+  if (k[0] || k[1] || k[2]) {
+    double ox, oy, oz;
+    image_of(b, x[3 * i], x[3 * i + 1], x[3 * i + 2], -k[0], -k[1], -k[2], ox, oy, oz);
+    x[3 * i] = ox;
+    x[3 * i + 1] = oy;
+    x[3 * i + 2] = oz;
+  }
+}
+
+void launch_nearest_image(int n, double *x, const double *xbuild, const BoxP &box,
+                          const BoxP *cbox, const int *acell, cudaStream_t st, long &launches) {
+  if (n <= 0) return;
+  k_nearest_image<<<(n + 255) / 256, 256, 0, st>>>(n, x, xbuild, box, cbox, acell);
+  launches += 1;
+}
+
 __global__ void k_nb_clear(int *flag) { *flag = 0; }
 
 __global__ void k_set_flag(int *flag) { *flag = 3; }  // rebuild, every cell

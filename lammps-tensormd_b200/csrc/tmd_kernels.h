@@ -60,6 +60,10 @@ void launch_neighbor_check(int n, const double *x, const double *xbuild,
                            double trigsq, int *flag, cudaStream_t st,
                            long &launches, const int *acell = nullptr, int *cflag = nullptr);
 void launch_set_flag(int *flag, cudaStream_t st, long &launches);
+// Positions from a caller's frame: each atom to the periodic image nearest its
+// position at the last list build (cbox/acell in multi-cell mode, else box).
+void launch_nearest_image(int n, double *x, const double *xbuild, const BoxP &box,
+                          const BoxP *cbox, const int *acell, cudaStream_t st, long &launches);
 
 // Descriptor: P[n][B][K][D], G[n][B*K*M].
 // Kernel forms: K/4 lanes per atom with 4 filters each (k_descriptor), or

@@ -145,6 +145,25 @@ def test_activation_and_rank_variants(tmp_path, kw):
     _check(out, ref, len(x), e_tol=E_PER_ATOM_OTHER)
 
 
+def test_set_positions_any_periodic_frame(fcc4k):
+    """Positions handed over in another periodic frame (every atom shifted by
+    -1, 0 or +1 box vectors per axis, as a caller that wraps at other times
+    would hand them over) give the forces and energy of the original frame,
+    to the FP64 rounding of the shift."""
+    p, syms, x, t, box, _ = fcc4k
+    m = TensorMDModel(f"{p} {' '.join(syms)}")
+    s = TensorMDSystem(m, len(x), 1.0)
+    s.set_box(box)
+    s.set_atoms(x, t)
+    ref = s.compute(1, 1)
+    k = np.random.default_rng(3).integers(-1, 2, size=(len(x), 3))
+    s.set_positions(x + k * np.array([box[3], box[4], box[5]]))
+    out = s.compute(1, 1)
+    assert rel_rms(out["f"], ref["f"]) <= 1e-12
+    assert out["energy"] == pytest.approx(ref["energy"], rel=1e-12)
+    np.testing.assert_allclose(out["virial"], ref["virial"], rtol=1e-10, atol=1e-10)
+
+
 def test_deterministic_bitwise(fcc4k):
     p, syms, x, t, box, _ = fcc4k
     m = TensorMDModel(f"{p} {' '.join(syms)}")
