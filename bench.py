@@ -306,7 +306,7 @@ def run_ours(args, rank, world, local):
                      "algorithmic_flops_per_launch": flops}
     kernel_ms = {k: (c, t / max(c, 1)) for k, (c, t) in prof.items()}
     # the other step kernels against their bounds (same profiled pass);
-    # algorithmic work per launch, per the survey's per-atom figures
+    # algorithmic work per launch: the per-atom operation counts of each step
     Minv = {1: 1, 4: 2, 10: 3, 20: 4}[D]
     sz = cfg["mlp"]
     mlp_macs = sum(a * b for a, b in zip(sz[:-1], sz[1:])) \
