@@ -176,6 +176,27 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def fp32_peak_tflops(lib, device):
+    """FP32 issue peak measured in this run: the library's packed-FMA (FFMA2)
+    microkernel on every SM, best of 5 event-timed launches."""
+    import ctypes
+    from tmd_b200.lib import check
+    tf = ctypes.c_double()
+    check(lib.tmd_fp32_peak(int(device), 5, ctypes.byref(tf)))
+    return tf.value
+
+
+def step_bytes_s8d(n, nlist, nin, rebuild_period):
+    """Algorithmic HBM bytes of one MD step as the survey's roofline section
+    defines them for a fused design: read x (24 B) and type (4 B), write f
+    (24 B), read and write v (48 B), write x (24 B), read the neighbor list
+    (4 B per entry) and write it once per rebuild period, and the MLP staging
+    G + dE/dG written and read (4 x 2 x 2 x nin B).  The design's own staging
+    between kernels is not counted."""
+    per_atom = 24 + 4 + 24 + 48 + 24 + 16 * nin
+    return n * per_atom + nlist * 4 * (1.0 + 1.0 / max(rebuild_period, 1.0))
+
+
 def ncu_traffic(config, kernel):
     """Per-launch DRAM bytes (read + write) of a kernel, from the committed ncu
     summary of the same workload (profiles/step_kernels_<config>.md, line
@@ -249,23 +270,29 @@ def run_ours(args, rank, world, local):
             import torch.distributed as dist
             dist.barrier()
 
+    # clocks are sampled from before the warm-up to the end of the profiled
+    # pass (nvidia-smi every 200 ms; the timed region alone can be shorter)
+    clk = ClockSampler(local).__enter__()
+    # measured FP32 issue peak, the denominator of the FP32 rooflines
+    fp32_peak = fp32_peak_tflops(sys_.lib, local)
     # warm-up
     sys_.nve_run(max(args.warmup, 3), dt)
     torch.cuda.synchronize()
     # timed region
     l0 = sys_.launches()
+    r0 = sys_.rebuilds()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        sys_.nve_run(args.steps, dt)
-        e1.record(stream)
-        torch.cuda.synchronize()
+    e0.record(stream)
+    sys_.nve_run(args.steps, dt)
+    e1.record(stream)
+    torch.cuda.synchronize()
     barrier()
     ms = e0.elapsed_time(e1)
     launches = sys_.launches() - l0
+    rebuilds = sys_.rebuilds() - r0
     ms_max = max_over_ranks(ms, world, dev)
     value = replicas_value(n, args.steps, world, ms_max)
 
@@ -273,9 +300,12 @@ def run_ours(args, rank, world, local):
     sys_.profile(True)
     sys_.profile_read(reset=True)
     nprof = max(10, min(args.steps, 50))
+    rp0 = sys_.rebuilds()
     sys_.nve_run(nprof, dt)
     prof = sys_.profile_read(reset=True)
     sys_.profile(False)
+    prof_rebuilds = sys_.rebuilds() - rp0
+    clk.__exit__(None, None, None)
 
     # force-kernel roofline
     off, ent = sys_.neighbor_list(model.cutmax)
@@ -288,22 +318,25 @@ def run_ours(args, rank, world, local):
     force_ms = fms / max(fcnt, 1)
     hbm_peak, peak_kind = measured_peaks()
     clocks = clk.summary()
-    sm_mhz = clocks["sm_mhz"] or 1965.0
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
     kname = {"filter_lane": "k_force", "pair_lane8": "k_force_pl<8>",
              "pair_lane16": "k_force_pl<16>", "pair_lane32": "k_force_pl<32>"}[sys_.force_variant()]
     traffic = ncu_traffic(args.config, kname)
     ach_gbs = abytes / (force_ms / 1000.0) / 1e9
     ach_tf = flops / (force_ms / 1000.0) / 1e12
-    roofline = {"kernel": kname, "bound": "hbm", "achieved": ach_gbs,
-                "peak": hbm_peak, "unit": "GB/s", "frac": ach_gbs / hbm_peak,
-                "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "algorithmic_bytes_per_launch": abytes, "launch_ms": force_ms}
-    roofline_fp32 = {"kernel": kname, "bound": "fp32", "achieved": ach_tf,
-                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach_tf / fp32_peak,
-                     "peak_source": "148 SMs x 128 FP32 lanes x 2 x sampled SM clock "
-                                    "(no FP32 figure in MEASURED_PEAKS.json)",
-                     "algorithmic_flops_per_launch": flops}
+    # the force kernel is bound by FP32 issue (its DRAM traffic is ~20% of
+    # peak): the headline roofline is its algorithmic FLOP/s against the FP32
+    # peak measured in this run; the HBM view of the same launch beside it
+    roofline = {"kernel": kname, "bound": "fp32", "achieved": ach_tf,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach_tf / fp32_peak,
+                "traffic": traffic,
+                "peak_source": "measured in this run (tmd_fp32_peak: FFMA2 microkernel, "
+                               "2 FLOP per FMA, best of 5)",
+                "algorithmic_flops_per_launch": flops, "launch_ms": force_ms,
+                "hbm": {"achieved_gbs": ach_gbs, "peak_gbs": hbm_peak,
+                        "frac": ach_gbs / hbm_peak,
+                        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                        "bytes_per_launch": abytes,
+                        "traffic_over_bytes": (traffic / abytes) if traffic else None}}
     kernel_ms = {k: (c, t / max(c, 1)) for k, (c, t) in prof.items()}
     # the other step kernels against their bounds (same profiled pass);
     # algorithmic work per launch: the per-atom operation counts of each step
@@ -327,6 +360,26 @@ def run_ours(args, rank, world, local):
     # but needs to leave HBM once
     gather_bytes = nlist * (16 + 4) + n * (24 + 4)
     g_ms = kms("gather")
+    # the whole step against the survey's algorithmic bytes (x, type, list,
+    # f, v, MLP staging) and the DRAM bytes the step's kernels move (sum of
+    # the committed ncu per-launch traffic of the step kernels)
+    steps_all = args.steps + nprof
+    period = steps_all / max(rebuilds + prof_rebuilds, 1)
+    sbytes = step_bytes_s8d(n, nlist, model.n_desc, period)
+    step_traffic = 0
+    for kn in ("k_descriptor_w", "k_mlp_fp32r", kname, "k_gather"):
+        tr = ncu_traffic(args.config, kn)
+        step_traffic = None if (tr is None or step_traffic is None) else step_traffic + tr
+    step_roofline = {
+        "algorithmic_bytes_per_step": sbytes,
+        "algorithmic_bytes_per_atom": sbytes / n,
+        "traffic_bytes_per_step": step_traffic,
+        "traffic_over_algorithmic": (step_traffic / sbytes) if step_traffic else None,
+        "rebuild_period_steps": period,
+        "flops_per_step": None,  # filled below
+        "note": "bytes as the survey defines them for a fused design; traffic = "
+                "committed ncu DRAM bytes per launch of descriptor, MLP, force and gather",
+    }
     kernel_roofline = {
         "descriptor": fp32_row("descriptor", desc_flops),
         "mlp": fp32_row("mlp", 2.0 * n * mlp_macs),
@@ -334,12 +387,17 @@ def run_ours(args, rank, world, local):
         "gather": {"ms": g_ms, "bound": "hbm", "bytes": gather_bytes,
                    "achieved_gbs": gather_bytes / (g_ms / 1000.0) / 1e9,
                    "frac": gather_bytes / (g_ms / 1000.0) / 1e9 / hbm_peak},
+        "fp32_peak_tflops": fp32_peak,
         "work": "descriptor: per pair inside rc P 2KD + radial 10K + monomials D, per atom "
                 "and block G (2M+1)DK; mlp: 2 x (forward + backward MACs) per atom; force: "
-                "as roofline_fp32; gather: per list entry its pair force (16 B, read "
+                "as roofline; gather: per list entry its pair force (16 B, read "
                 "once; the partner read is the same array) and partner slot (4 B), per atom "
                 "force (24 B) and row length",
     }
+
+    step_roofline["flops_per_step"] = desc_flops + 2.0 * n * mlp_macs + flops
+    step_roofline["fp32_frac_of_step"] = (step_roofline["flops_per_step"]
+                                          / (ms_max / args.steps / 1000.0) / 1e12 / fp32_peak)
 
     # e2e through the reference-facing call pattern (host buffers)
     sys_.set_atoms(x, t, v)
@@ -471,9 +529,10 @@ def run_ours(args, rank, world, local):
                     "timing": "host wall clock, includes the host velocity Verlet "
                               "(multithreaded in-place CPU tensor ops)"},
             "gpu_launches": launches,
+            "neighbor_rebuilds_in_timed_region": rebuilds,
             "clocks": clocks,
             "roofline": roofline,
-            "roofline_fp32": roofline_fp32,
+            "step_roofline": step_roofline,
             "kernel_roofline": kernel_roofline,
             "kernel_ms": kernel_ms,
             "force_form": force_form,

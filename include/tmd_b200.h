@@ -177,6 +177,18 @@ int tmd_system_stream(tmd_system *sys, void **stream);
 /* Number of kernels the library launched since the system was created. */
 long tmd_system_launches(const tmd_system *sys);
 
+/* Neighbor-list rebuilds the system has run since it was created (forced
+ * ones at set_atoms included, and the displacement-triggered ones inside MD
+ * runs: LAMMPS's "Neighbor list builds" count).  Waits for the stream. */
+int tmd_system_rebuilds(tmd_system *sys, long *count);
+
+/* Measured FP32 issue peak of a device: a packed-FMA (FFMA2) kernel with
+ * eight independent chains per thread on every SM, `reps` timed launches
+ * (CUDA events) after one warm-up, best of them, in TFLOP/s (2 FLOP per
+ * FMA).  The denominator of the FP32 rooflines; no reference counterpart.
+ * Uses its own stream and returns after it has finished. */
+int tmd_fp32_peak(int device, int reps, double *tflops);
+
 /* Kernel timing (TensorMDTimer's phase report, tensormd_timer.h:25-46, with
  * CUDA events instead of host clocks).  enable != 0 records an event pair
  * around every kernel family on the system stream during tmd_compute and
@@ -292,10 +304,13 @@ int tmd_server_stats(tmd_server *server, long *submitted, long *completed,
 int tmd_server_timing(tmd_server *server, double *seconds);
 
 /* Full neighbor list without allocating any memory.  This entry point has no
- * counterpart in the reference.  It is meant for callers that must not call
- * cudaMalloc: code that records into a CUDA graph (allocation is not allowed
- * while a stream is being captured), and hosts that give a library no device
- * memory of its own because they manage every byte through their own pool.
+ * counterpart in the reference.  It is meant for host programs that must not
+ * let a library call cudaMalloc: programs that manage every byte of device
+ * memory through their own pool, or that reserve the whole device up front,
+ * so that an allocation inside the library would fail or escape their
+ * accounting.  The call is synchronous: it waits for `stream` to finish and
+ * reads a status word back to the host, so it must be made outside any
+ * stream capture.
  *
  * x_dev[n*3]: device positions, already inside the periodic cell (no
  * wrapping is done; atoms outside a periodic cell give TMD_ERR_ARG).
@@ -313,7 +328,7 @@ int tmd_server_timing(tmd_server *server, double *seconds);
  * cells (larger requests give TMD_ERR_CAPACITY).  All calls share that one
  * array: calls whose work overlaps on the GPU race and corrupt each other, so
  * serialise them.  The first call on each device looks the array up
- * (cudaGetSymbolAddress); make that first call before any stream capture. */
+ * (cudaGetSymbolAddress) with that device current. */
 #define TMD_NOALLOC_MAX_ATOMS 262144
 #define TMD_NOALLOC_MAX_CELLS 131072
 int tmd_neighbor_list_noalloc(const double *x_dev, int n, const double box[9],

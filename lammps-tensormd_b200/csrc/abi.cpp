@@ -939,7 +939,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   A(P, N * h.nelt * h.K * h.D); A(G, N * h.nin); A(dEdG, N * h.nin); A(E, N);
   A(wv, 6 * N); A(eatom, N); A(vatom, 6 * N); A(ke, N);
   A(partial, 1024 * 8); A(scal, 8);
-  A(flag, 1); A(status, 2);
+  A(flag, 2); A(status, 2);  // flag[0] rebuild pending, flag[1] rebuilds done
   A(perm, N); A(tiles, 3 * (N / 32 + h.nelt + 1));
 #undef A
   if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&s->h_scal), 8 * sizeof(double));
@@ -947,7 +947,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   if (e == cudaSuccess) e = cudaMemset(s->v, 0, 3 * N * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(s->image, 0, 3 * N * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(s->status, 0, 2 * sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(s->flag, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(s->flag, 0, 2 * sizeof(int));
   if (e != cudaSuccess) {
     tmd_system_free(s);
     return fail(TMD_ERR_CUDA, std::string("system allocation: ") + cudaGetErrorString(e));
@@ -1307,6 +1307,15 @@ int tmd_system_stream(tmd_system *s, void **stream) {
 }
 
 long tmd_system_launches(const tmd_system *s) { return s ? s->launches : 0; }
+
+int tmd_system_rebuilds(tmd_system *s, long *count) {
+  if (!s || !count) return fail(TMD_ERR_ARG, "null argument");
+  int h[2] = {0, 0};
+  TMD_CUDA(cudaMemcpyAsync(h, s->flag, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  *count = h[1];
+  return TMD_OK;
+}
 
 int tmd_profile_enable(tmd_system *s, int enable) {
   if (!s) return fail(TMD_ERR_ARG, "null system");

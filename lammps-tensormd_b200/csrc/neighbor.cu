@@ -799,7 +799,12 @@ void launch_nearest_image(int n, double *x, const double *xbuild, const BoxP &bo
   launches += 1;
 }
 
-__global__ void k_nb_clear(int *flag) { *flag = 0; }
+// End of the rebuild sequence: count a rebuild that ran (flag[1]) and clear
+// the pending flag.
+__global__ void k_nb_clear(int *flag) {
+  if (flag[0]) flag[1] += 1;
+  flag[0] = 0;
+}
 
 __global__ void k_set_flag(int *flag) { *flag = 3; }  // rebuild, every cell
 

@@ -1,12 +1,14 @@
 // noalloc.cu -- tmd_neighbor_list_noalloc: the full neighbor list built with
 // no device allocation at all.
 //
-// Who needs it: code that records its work into a CUDA graph cannot call
-// cudaMalloc while the stream is being captured, and some host programs hand
-// a library no device memory of its own because they account for every byte
-// through their own pool.  Those callers pass the positions and the output
-// rows in memory they own; the cell-binning scratch below is the only other
-// memory the call touches.
+// Who needs it: host programs that give a library no device memory of its
+// own, because they account for every byte through their own pool or have
+// reserved the whole device up front (a cudaMalloc inside the library would
+// then fail or break their accounting).  Those callers pass the positions and
+// the output rows in memory they own; the cell-binning scratch below is the
+// only other memory the call touches.  The call is synchronous: it waits for
+// its stream and reads a status word back to the host, so it must be made
+// outside any stream capture.
 //
 // The scratch is one static device array of 4 MiB that every GPU loading this
 // library keeps until the process exits.  Its device address is looked up
@@ -58,8 +60,10 @@ __device__ __align__(256) int g_scratch[kScratchInts];
 std::mutex g_mu;
 int *g_addr[64] = {nullptr};  // device address of g_scratch per device
 
-// Bin atoms by fractional coordinate without moving them; an atom outside a
-// periodic cell is an error here (the caller's positions are read-only).
+// Bin atoms by fractional coordinate without moving them; an atom outside the
+// cell is an error here (the caller's positions are read-only).  As in the
+// system build (k_nb_bin), a periodic axis needs 0 <= f < 1 and a
+// non-periodic one 0 <= f <= 1 (an atom on a shrink-wrapped upper face is in).
 __global__ void k_bin_inplace(int n, const double *__restrict__ x, BoxP box, BinP bin,
                               int *__restrict__ cell_of, int *__restrict__ cell_count,
                               int *status) {
@@ -72,7 +76,7 @@ __global__ void k_bin_inplace(int n, const double *__restrict__ x, BoxP box, Bin
     f[0] = (dx - f[1] * box.xy - f[2] * box.xz) / box.xprd;
     int c3[3];
     for (int a = 0; a < 3; a++) {
-      if (f[a] < 0.0 || f[a] >= 1.0) atomicOr(status, kStatusOutside);
+      if (f[a] < 0.0 || (box.pbc[a] ? f[a] >= 1.0 : f[a] > 1.0)) atomicOr(status, kStatusOutside);
       int q = (int)floor(f[a] * bin.nb[a]);
       q = q < 0 ? 0 : (q >= bin.nb[a] ? bin.nb[a] - 1 : q);
       c3[a] = q;
@@ -107,8 +111,11 @@ extern "C" int tmd_neighbor_list_noalloc(const double *x_dev, int n, const doubl
   if (n == 0) return TMD_OK;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 64)
+  if (e != cudaSuccess)
     return fail(TMD_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64)
+    return fail(TMD_ERR_ARG, "device index " + std::to_string(dev) +
+                                 " exceeds the no-alloc address table (64 devices)");
   int *base = nullptr;
   {
     // set-up, once per device, with that device current
@@ -157,6 +164,7 @@ extern "C" int tmd_neighbor_list_noalloc(const double *x_dev, int n, const doubl
     int a = (bin.nb[0] >= bin.nb[1] && bin.nb[0] >= bin.nb[2]) ? 0 : (bin.nb[1] >= bin.nb[2] ? 1 : 2);
     bin.nb[a] = (bin.nb[a] + 1) / 2;
     bin.ns[a] = (int)std::ceil(cut * (1.0 + 1e-9) / (w[a] / bin.nb[a]));
+    if (!b.pbc[a] && bin.ns[a] > bin.nb[a]) bin.ns[a] = bin.nb[a];
     ncell = (long)bin.nb[0] * bin.nb[1] * bin.nb[2];
   }
   bin.ncell = (int)ncell;
@@ -188,7 +196,8 @@ extern "C" int tmd_neighbor_list_noalloc(const double *x_dev, int n, const doubl
   e = cudaMemcpyAsync(h, status, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return fail(TMD_ERR_CUDA, std::string("status read: ") + cudaGetErrorString(e));
-  if (h[0] & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside the periodic cell (wrap positions first)");
+  if (h[0] & kStatusOutside)
+    return fail(TMD_ERR_ARG, "atom outside the cell (wrap positions into it first)");
   if (h[0] & kStatusLaunch) return fail(TMD_ERR_CUDA, "neighbor build launched without its shared memory");
   if (h[0] & kStatusShift) return fail(TMD_ERR_ARG, "periodic cell is too small for the cutoff");
   if (h[0] & kStatusOverflow)

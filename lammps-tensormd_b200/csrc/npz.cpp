@@ -63,9 +63,6 @@ NpyArray parse_npy(const unsigned char *p, size_t n, const std::string &key) {
   a.kind = descr[1];
   a.itemsize = std::stoi(descr.substr(2));
   if (endian == '>') fail("npz: big-endian arrays are not supported (" + key + ")");
-  if (h.find("'fortran_order': True") != std::string::npos && a.itemsize > 0) {
-    // Only 1-D / scalar arrays are order-independent; 2-D weights must be C.
-  }
   bool fortran = h.find("'fortran_order': True") != std::string::npos;
   auto spos = h.find('(', h.find("'shape'"));
   auto send = h.find(')', spos);

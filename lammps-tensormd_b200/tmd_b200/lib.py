@@ -42,6 +42,8 @@ SIGNATURES = [
     ("tmd_system_autotune", _c_int, [_vp, _c_int, _c_int, _pd]),
     ("tmd_system_stream", _c_int, [_vp, ctypes.POINTER(_vp)]),
     ("tmd_system_launches", _c_long, [_vp]),
+    ("tmd_system_rebuilds", _c_int, [_vp, _pl]),
+    ("tmd_fp32_peak", _c_int, [_c_int, _c_int, _pd]),
     ("tmd_profile_enable", _c_int, [_vp, _c_int]),
     ("tmd_profile_read", _c_int, [_vp, _pl, _pd, _c_int]),
     ("tmd_last_error", _c_int, [ctypes.c_char_p, _c_int]),

@@ -207,6 +207,12 @@ class TensorMDSystem:
     def launches(self) -> int:
         return int(self.lib.tmd_system_launches(self.h))
 
+    def rebuilds(self) -> int:
+        """Neighbor-list rebuilds run since the system was created."""
+        c = ctypes.c_long()
+        check(self.lib.tmd_system_rebuilds(self.h, ctypes.byref(c)))
+        return int(c.value)
+
     PROFILE_FAMILIES = ("neighbor", "descriptor", "mlp", "force", "gather", "nve", "reduce",
                         "dedp")
 

@@ -6,8 +6,9 @@ oracle restatement); nothing in the product links it.
 
     python oracle/build_ref.py [--force]
 
-Needs the reference tree; without it the build is skipped and the tests that
-use the library are skipped too.  Output goes only to oracle/_ref/.
+Needs the reference tree (TMD_REFERENCE_TREE, see oracle/reftree.py);
+without it the build is skipped and the tests that use the library are
+skipped too.  Output goes only to oracle/_ref/.
 """
 from __future__ import annotations
 
@@ -16,7 +17,11 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = Path("/root/reference/src/ML-TENSORMD")
+if str(HERE) not in sys.path:
+    sys.path.insert(0, str(HERE))
+from reftree import reference_tree  # noqa: E402
+
+REF_SRC = reference_tree() / "src" / "ML-TENSORMD"
 OUT_DIR = HERE / "_ref"
 LIB = OUT_DIR / "libtmdref.so"
 

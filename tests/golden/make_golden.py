@@ -1,6 +1,8 @@
 """Regenerate tests/golden/ from the reference tree (run where it is mounted).
 
-    python tests/golden/make_golden.py /path/to/lammps-tensormd
+    python tests/golden/make_golden.py [/path/to/lammps-tensormd]
+
+(default: TMD_REFERENCE_TREE, see oracle/reftree.py)
 
 Copies three shipped potentials and two data files, and extracts the
 published step-0 results of the reference (LAMMPS thermo lines and the
@@ -99,4 +101,6 @@ def main(ref: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    sys.path.insert(0, str(HERE.parent.parent / "oracle"))
+    from reftree import reference_tree
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else reference_tree())

@@ -1,0 +1,131 @@
+"""Parity at the sizes the benchmark times, through the C ABI, against the
+FP64 oracle on the same positions.
+
+  bcc128k   128,000-atom BCC (a = 2.87 A, 40^3 cells, sigma 0.08 A, 600 K),
+            16 Gaussians rc 6 A, rank <= 3, MLP 64-64-64-1 tanh: 1,000 NVE
+            steps of 1 fs on the device; every 100 steps the device state is
+            read back and forces, energy and virial on those positions are
+            compared with the oracle.  At this size the persistent MLP walks
+            about seven 128-atom tiles per CTA and every kernel runs its
+            multi-wave grid.
+  alloy432k 432,000-atom 4-element random FCC alloy (a = 3.6 A, 60x60x30
+            cells), 32 Gaussians rc 6.5 A, MLP 512-128-128-128-1 softplus:
+            one evaluation per MLP form against one oracle evaluation.
+  cells4096 4,096 cells x 256 atoms (half FCC, half BCC, 2 elements): 16
+            sampled cells against the oracle cell by cell, at the start and
+            after the benchmark's 500 NVE steps.
+
+Bars (the plain-form bars of the other parity tests): force relative RMS
+<= 1e-5, |dE|/N <= 1e-7 eV/atom, virial relative <= 1e-5; the BF16 MLP forms
+force RMS <= 1e-3 eV/A against the oracle.
+"""
+import numpy as np
+import pytest
+
+from pack import Oracle, load_npz
+from tmd_b200 import TensorMDBatch, TensorMDModel, TensorMDSystem, synth
+from tmd_testutil import frac_wrap, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+FORCE_RRMS = 1e-5
+E_PER_ATOM = 1e-7
+VIR_REL = 1e-5
+BF16_FORCE_RMS = 1e-3  # eV/A against the FP64 oracle
+
+
+def _errors(out, ref, n):
+    return {"force_rel_rms": rel_rms(out["f"], ref["f"]),
+            "force_rms": float(np.sqrt(np.mean((out["f"] - ref["f"]) ** 2))),
+            "energy_per_atom": abs(out["energy"] - ref["energy"]) / n,
+            "virial_rel": float(np.linalg.norm(out["virial"] - ref["virial"])
+                                / np.linalg.norm(ref["virial"]))}
+
+
+def _assert_plain(err):
+    assert err["force_rel_rms"] <= FORCE_RRMS, err
+    assert err["energy_per_atom"] <= E_PER_ATOM, err
+    assert err["virial_rel"] <= VIR_REL, err
+
+
+def _system(cfg_name, seed=42, precision=""):
+    c = synth.config(cfg_name)
+    import tempfile
+    from pathlib import Path
+    p = Path(tempfile.mkdtemp(prefix="tmdtimed")) / f"{cfg_name}.npz"
+    syms = synth.gaussian_potential(p, seed=1234, **c["pot"])
+    x, t, box, v = synth.build_system(c["kind"], c["a"], c["cells"], sigma=c["sigma"],
+                                      T=c["T"], nelt=c["nelt"], seed=seed)
+    return str(p), syms, x, t, box, v
+
+
+def test_bcc128k_1000_steps_checked_every_100():
+    p, syms, x, t, box, v = _system("bcc128k")
+    n = len(x)
+    m = TensorMDModel(f"{p} {' '.join(syms)}")
+    s = TensorMDSystem(m, n, 1.0)
+    s.set_box(box)
+    s.set_atoms(x, t, v)
+    o = Oracle(load_npz(p))
+    worst = {}
+    for chunk in range(11):
+        if chunk:
+            s.nve_run(100, 0.001)
+        xs = s.get()[0]
+        out = s.compute(1, 1)
+        ref = o.compute(frac_wrap(xs, box), t - 1, box, [1, 1, 1])
+        err = _errors(out, ref, n)
+        _assert_plain(err)
+        for k, val in err.items():
+            worst[k] = max(worst.get(k, 0.0), val)
+    print("bcc128k worst over 11 checkpoints:", worst)
+
+
+def test_alloy432k_every_form_against_the_oracle():
+    p, syms, x, t, box, _ = _system("alloy432k")
+    n = len(x)
+    ref = Oracle(load_npz(p)).compute(x, t - 1, box, [1, 1, 1])
+    for prec in ("fp32", "bf16x3", "bf16"):
+        suffix = "" if prec == "fp32" else f" precision {prec}"
+        m = TensorMDModel(f"{p} {' '.join(syms)}{suffix}")
+        s = TensorMDSystem(m, n, 1.0)
+        s.set_box(box)
+        s.set_atoms(x, t)
+        err = _errors(s.compute(1, 1), ref, n)
+        if prec == "fp32":
+            _assert_plain(err)
+        else:
+            assert err["force_rms"] <= BF16_FORCE_RMS, (prec, err)
+        s.close()
+        m.close()
+
+
+def test_cells4096_sampled_cells_against_the_oracle(tmp_path):
+    c = synth.config("cells4096")
+    p = tmp_path / "cells.npz"
+    syms = synth.gaussian_potential(p, seed=2024, **c["pot"])
+    data = synth.batch_cells(c["ncells"], c["natoms"], nelt=c["nelt"], sigma=c["sigma"],
+                             t_range=c["t_range"], seed=99)
+    m = TensorMDModel(f"{p} {' '.join(syms)}")
+    b = TensorMDBatch(m, data["natoms"], 1.0)
+    b.set_cells(data["boxes"])
+    b.set_atoms(data["x"], data["types"], data["v"])
+    o = Oracle(load_npz(p))
+    sample = np.linspace(0, c["ncells"] - 1, 16).astype(int)
+    boxes = np.asarray(data["boxes"]).reshape(-1, 9)
+    types = np.asarray(data["types"])
+    for phase in ("start", "after 500 NVE steps"):
+        if phase != "start":
+            b.nve_run(500, 0.001)
+        xs = b.get()[0]
+        out = b.compute()
+        for cidx in sample:
+            a0, a1 = b.offsets[cidx], b.offsets[cidx + 1]
+            ref = o.compute(frac_wrap(xs[a0:a1], boxes[cidx]), types[a0:a1] - 1,
+                            boxes[cidx], [1, 1, 1])
+            cell = {"f": out["f"][a0:a1], "energy": out["energy"][cidx],
+                    "virial": out["virial"][cidx]}
+            err = _errors(cell, ref, a1 - a0)
+            assert err["force_rel_rms"] <= FORCE_RRMS, (phase, cidx, err)
+            assert err["energy_per_atom"] <= E_PER_ATOM, (phase, cidx, err)
+            assert err["virial_rel"] <= VIR_REL, (phase, cidx, err)

@@ -1,16 +1,16 @@
 """The LAMMPS-side binding (pair style tensormd/b200 and its plugin entry)
 compiles against the LAMMPS headers of the reference tree (syntax check with
 the serial MPI stubs).  Skipped where that tree is not mounted."""
-import os
 import shutil
 import subprocess
 from pathlib import Path
 
 import pytest
 
+from reftree import reference_tree
 from tmd_testutil import ROOT
 
-LAMMPS_SRC = Path(os.environ.get("TMD_LAMMPS_SRC", "/root/reference/src"))
+LAMMPS_SRC = reference_tree() / "src"
 
 
 @pytest.mark.skipif(not (LAMMPS_SRC / "pair.h").exists() or shutil.which("g++") is None,

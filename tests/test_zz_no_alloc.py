@@ -1,14 +1,16 @@
-"""tmd_neighbor_list_noalloc: the neighbor list for callers that may not
-allocate device memory (code recorded into a CUDA graph, where cudaMalloc is
-not allowed during capture, and hosts that manage all device memory through
-their own pool).  The entry point uses only the buffers the caller passes and
-the library's static 4 MiB scratch array.
+"""tmd_neighbor_list_noalloc: the neighbor list for host programs that may not
+let a library allocate device memory (they manage every byte through their
+own pool, or reserve the whole device up front).  The entry point uses only
+the buffers the caller passes and the library's static 4 MiB scratch array;
+it is synchronous and is called outside any stream capture.
 
 Checked through the C ABI against the existing entry point
 (tmd_system_* + tmd_neighbor_list): the same (i, j, image) set, bit for bit,
 as every neighbor-set test here requires, on two calls in a row (the second
-call finds the previous call's contents in the shared scratch array).  This
-file sorts last so a failure here cannot hide the other tests."""
+call finds the previous call's contents in the shared scratch array), for
+periodic, slab and cluster cells and for a sparse box whose bins must be
+merged to fit the scratch array's cell limit.  This file sorts last so a
+failure here cannot hide the other tests."""
 import ctypes
 
 import numpy as np
@@ -39,7 +41,7 @@ def _decode(counts, rows, cap):
     return off, ent
 
 
-def _noalloc(x, box, pbc, cut, cap):
+def _noalloc(x, box, pbc, cut, cap, expect=0):
     import torch
     lib = load_library()
     n = len(x)
@@ -53,7 +55,7 @@ def _noalloc(x, box, pbc, cut, cap):
                                        pb.ctypes.data_as(_pi), cut, cap,
                                        ctypes.c_void_p(counts.data_ptr()),
                                        ctypes.c_void_p(rows.data_ptr()), None)
-    assert rc == 0, rc
+    assert rc == expect, rc
     return counts.cpu().numpy(), rows.cpu().numpy().view(np.uint32)
 
 
@@ -67,23 +69,60 @@ def _existing(pot_args, x, t, box, pbc, skin):
     return canonical_pairs(*s.neighbor_list(cut)), xs, cut
 
 
-@pytest.mark.parametrize("case", ["fcc864", "triclinic16"])
+def _small_pot(tmp_path, rc=5.0):
+    p = tmp_path / "pot.npz"
+    syms = synth.gaussian_potential(p, nelt=1, num_filters=8, rc=rc, hidden=(8, 8))
+    return f"{p} {' '.join(syms)}"
+
+
+@pytest.mark.parametrize("case", ["fcc864", "triclinic16", "slab", "cluster", "sparse"])
 def test_noalloc_list_equals_system_list(tmp_path, case):
-    if case == "fcc864":
-        p = tmp_path / "pot.npz"
-        syms = synth.gaussian_potential(p, nelt=1, num_filters=8, rc=5.0, hidden=(8, 8))
-        x, t, box, _ = synth.build_system("fcc", 3.6, (6, 6, 6), sigma=0.1, seed=9)
-        args = f"{p} {' '.join(syms)}"
-    else:
+    pbc = (1, 1, 1)
+    if case == "triclinic16":
         x, t, box = read_data(GOLDEN / "Mo8_Ni8_id3210.data")
         x = frac_wrap(x, box)
         args = f"{GOLDEN}/MoNi_m3.npz Mo Ni interp 0.0001"
-    ref, xs, cut = _existing(args, x, t, box, (1, 1, 1), 1.0)
+    elif case == "sparse":
+        # 3,000 atoms in a periodic 200 A cube: bins of cut/2 would give
+        # 57^3 = 185,193 cells, more than the scratch array holds, so the
+        # call merges bins until the grid fits
+        args = _small_pot(tmp_path, rc=6.0)
+        rng = np.random.default_rng(5)
+        box = np.array([0, 0, 0, 200.0, 200.0, 200.0, 0, 0, 0])
+        x = rng.uniform(0.0, 200.0, size=(3000, 3))
+        t = np.ones(len(x), dtype=np.int32)
+    else:
+        args = _small_pot(tmp_path)
+        x, t, box, _ = synth.build_system("fcc", 3.6, (6, 6, 6), sigma=0.1, seed=9)
+        if case != "fcc864":
+            # non-periodic axes: a box 2 A wider than the atoms on each side;
+            # one atom sits exactly on the upper face of the first free axis
+            pbc = (1, 1, 0) if case == "slab" else (0, 0, 0)
+            box = box.copy()
+            for a in range(3):
+                if not pbc[a]:
+                    lo = x[:, a].min() - 2.0
+                    box[a], box[3 + a] = lo, x[:, a].max() + 2.0 - lo
+            a = 2
+            x = x.copy()
+            x[0, a] = box[a] + box[3 + a]
+    ref, xs, cut = _existing(args, x, t, box, pbc, 1.0)
     cap = 512
     for _ in range(2):  # second call reuses the scratch left by the first
-        counts, rows = _noalloc(xs, box, (1, 1, 1), cut, cap)
+        counts, rows = _noalloc(xs, box, pbc, cut, cap)
         got = canonical_pairs(*_decode(counts, rows, cap))
         assert np.array_equal(got, ref)
+
+
+def test_noalloc_row_overflow_reports_needed_length(tmp_path):
+    args = _small_pot(tmp_path)
+    x, t, box, _ = synth.build_system("fcc", 3.6, (6, 6, 6), sigma=0.1, seed=9)
+    ref, xs, cut = _existing(args, x, t, box, (1, 1, 1), 1.0)
+    longest = int(np.bincount(ref[:, 0]).max())
+    _noalloc(xs, box, (1, 1, 1), cut, 16, expect=-4)
+    buf = ctypes.create_string_buffer(256)
+    load_library().tmd_last_error(buf, 256)
+    assert f"needs {longest} entries".encode() in buf.value, buf.value
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit():
