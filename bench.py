@@ -54,6 +54,9 @@ def parse():
                          "kernel forms, run N force evaluations, print nothing else")
     ap.add_argument("--profile-precision", default="fp32", choices=["fp32", "bf16x3", "bf16"],
                     help="MLP precision form of the --profile-step target")
+    ap.add_argument("--profile-desc", default="", choices=["", "filter4", "wide", "wide2"],
+                    help="descriptor form of the --profile-step target (default: the "
+                         "library's default form)")
     ap.add_argument("--main-only", action="store_true",
                     help="only the headline workload (no precision forms, cells, serving, "
                          "reference-workload or CPU lines): for profiler launch lists")
@@ -63,6 +66,9 @@ def parse():
                     help="NVE steps per MLP form of the 432,000-atom precision line (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=2000.0,
                     help="serving line: Poisson arrival rate (jobs/s)")
+    ap.add_argument("--serve-sweep", default="250,500,1000",
+                    help="serving line: further arrival rates (jobs/s, comma separated; "
+                         "empty skips), each served by every MLP form")
     ap.add_argument("--serve-window", type=float, default=2.0,
                     help="serving line: seconds of arrivals (0 skips it)")
     return ap.parse_args()
@@ -165,7 +171,8 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window": "the whole bench run (every leg), nvidia-smi every 200 ms"}
 
 
 def measured_peaks():
@@ -241,6 +248,17 @@ def algorithmic(cfg, npairs_rc, nlist, B, K, D, nin, form):
 
 
 def run_ours(args, rank, world, local):
+    # clocks and throttle reasons sampled (nvidia-smi, every 200 ms) over the
+    # whole run: the headline's timed region alone is often shorter than one
+    # sampling interval
+    clk = ClockSampler(local).__enter__()
+    try:
+        run_ours_sampled(args, rank, world, local, clk)
+    finally:
+        clk.__exit__(None, None, None)
+
+
+def run_ours_sampled(args, rank, world, local, clk):
     import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -270,9 +288,6 @@ def run_ours(args, rank, world, local):
             import torch.distributed as dist
             dist.barrier()
 
-    # clocks are sampled from before the warm-up to the end of the profiled
-    # pass (nvidia-smi every 200 ms; the timed region alone can be shorter)
-    clk = ClockSampler(local).__enter__()
     # measured FP32 issue peak, the denominator of the FP32 rooflines
     fp32_peak = fp32_peak_tflops(sys_.lib, local)
     # warm-up
@@ -305,7 +320,6 @@ def run_ours(args, rank, world, local):
     prof = sys_.profile_read(reset=True)
     sys_.profile(False)
     prof_rebuilds = sys_.rebuilds() - rp0
-    clk.__exit__(None, None, None)
 
     # force-kernel roofline
     off, ent = sys_.neighbor_list(model.cutmax)
@@ -317,7 +331,6 @@ def run_ours(args, rank, world, local):
     fcnt, fms = prof["force"]
     force_ms = fms / max(fcnt, 1)
     hbm_peak, peak_kind = measured_peaks()
-    clocks = clk.summary()
     kname = {"filter_lane": "k_force", "pair_lane8": "k_force_pl<8>",
              "pair_lane16": "k_force_pl<16>", "pair_lane32": "k_force_pl<32>"}[sys_.force_variant()]
     traffic = ncu_traffic(args.config, kname)
@@ -493,17 +506,34 @@ def run_ours(args, rank, world, local):
     serving = None
     if args.serve_window > 0 and not args.main_only:
         serving = run_serving(args, rank, local)
-        if not args.no_bf16:
+        keys = ("solves_per_s", "p50_ms", "p99_ms", "atom_steps_per_s", "makespan_s",
+                "by_kind", "fire_converged_frac")
+        precs = [] if args.no_bf16 else ["bf16x3", "bf16"]
+        if precs:
             # the same job stream (same seeds) with the MLP in the BF16 forms
             serving["forms"] = {}
-            for prec in ("bf16x3", "bf16"):
+            for prec in precs:
                 try:
                     sf = run_serving(args, rank, local, precision=prec)
-                    serving["forms"][prec] = {k: sf[k] for k in (
-                        "solves_per_s", "p50_ms", "p99_ms", "atom_steps_per_s", "makespan_s",
-                        "by_kind")}
+                    serving["forms"][prec] = {k: sf[k] for k in keys}
                 except Exception as exc:  # report, do not hide
                     serving["forms"][prec] = {"error": str(exc)}
+        # latency against throughput: lower arrival rates, every form
+        rates = [float(r) for r in args.serve_sweep.split(",") if r.strip()]
+        serving["rate_sweep"] = {}
+        for rate in rates:
+            row = {}
+            for prec in ["fp32"] + precs:
+                try:
+                    sf = run_serving(args, rank, local, precision=prec, rate=rate)
+                    row[prec] = {k: sf[k] for k in keys}
+                except Exception as exc:  # report, do not hide
+                    row[prec] = {"error": str(exc)}
+            serving["rate_sweep"][f"{rate:g}"] = row
+        try:
+            serving["fire_trained"] = run_fire_trained(rank, local)
+        except Exception as exc:  # report, do not hide
+            serving["fire_trained"] = {"error": str(exc)}
     w23k = None if args.main_only else run_w23k(args, rank, world, local, dev, barrier)
     alloy = None
     if args.precision_steps > 0 and not args.main_only:
@@ -516,6 +546,7 @@ def run_ours(args, rank, world, local):
     if rank == 0 and world == 1 and not (args.no_cpu_baseline or args.main_only):
         cpu = cpu_baseline(args.config, samples=2)
 
+    clocks = clk.summary()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -743,15 +774,62 @@ def run_w23k(args, rank, world, local, dev, barrier):
                       "fix nvt temp 300 300 0.1, skin 1.0, dt 1 fs"}
 
 
-def run_serving(args, rank, local, precision="fp32"):
-    """Serving: Poisson arrivals (rate args.serve_rate per s over
+def run_fire_trained(rank, local, njobs=64):
+    """FIRE jobs on a trained potential, whose lattices are real minima (the
+    random-weight serving potential has none: its cells collapse under any
+    minimiser, so its FIRE jobs run to the iteration cap): the reference's
+    MoNi_m3 potential, Mo8Ni8 cells replicated 1-3 times per axis (16-432
+    atoms), positions displaced by sigma 0.1 A, min_style fire to max |F_i|
+    < 0.01 eV/A, at most 1000 iterations, all submitted at once."""
+    from tmd_b200 import TensorMDModel, TensorMDServer
+    from tmd_b200.synth import frac_wrap, read_data
+    GOLDEN = ROOT / "tests" / "golden"
+    x0, t0, box0 = read_data(GOLDEN / "Mo8_Ni8_id3210.data")
+    x0 = frac_wrap(x0, box0)
+    rng = np.random.default_rng(515 + rank)
+    model = TensorMDModel(f"{GOLDEN}/MoNi_m3.npz Mo Ni interp 0.0001", device=local)
+    srv = TensorMDServer(model, max_atoms=200000, max_cells=256, steps_per_tick=8)
+    a = np.array(box0[3:6])
+    tilt = np.array(box0[6:9])
+    jobs = []
+    for _ in range(njobs):
+        r = rng.integers(1, 4, size=3)
+        sh = np.stack(np.meshgrid(*(np.arange(k) for k in r), indexing="ij"), -1).reshape(-1, 3)
+        off = np.stack([sh[:, 0] * a[0] + sh[:, 1] * tilt[0] + sh[:, 2] * tilt[1],
+                        sh[:, 1] * a[1] + sh[:, 2] * tilt[2], sh[:, 2] * a[2]], -1)
+        x = (x0[None, :, :] + off[:, None, :]).reshape(-1, 3)
+        t = np.tile(t0, len(sh))
+        box = np.concatenate([box0[:3], a * r, [tilt[0] * r[1], tilt[1] * r[2],
+                                                tilt[2] * r[2]]])
+        x = x + rng.normal(0.0, 0.1, size=x.shape)
+        jobs.append((x, t, box))
+    t_start = time.perf_counter()
+    tickets = [srv.submit(2, x, t, box, nsteps=1000, dt=0.001, fmax=0.01) for x, t, box in jobs]
+    done = [srv.wait(tk, timeout=600) for tk in tickets]
+    t_end = time.perf_counter()
+    srv.close()
+    model.close()
+    it = np.array([d["steps"] for d in done])
+    fmax = np.array([np.linalg.norm(d["f"], axis=1).max() for d in done])
+    lat = np.array([d["latency"] for d in done]) * 1000.0
+    return {"jobs": njobs, "potential": "MoNi_m3.npz interp 0.0001 (trained, shipped)",
+            "natoms_range": [int(min(len(j[0]) for j in jobs)), int(max(len(j[0]) for j in jobs))],
+            "converged_frac": float(np.mean(fmax < 0.01)), "iteration_cap": 1000,
+            "iterations_p50": float(np.percentile(it, 50)),
+            "iterations_max": int(it.max()), "makespan_s": t_end - t_start,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+
+
+def run_serving(args, rank, local, precision="fp32", rate=None):
+    """Serving: Poisson arrivals (rate jobs/s, default args.serve_rate, over
     args.serve_window s) of jobs with N log-uniform in [32, 4096] atoms, FCC /
     BCC lattices or random packings (0.085 A^-3, dmin 2 A), 1-4 elements; 60%
-    single-point, 25% 200-step NVE, 15% FIRE to fmax 0.01 eV/A (at most 1000
-    iterations).  Jobs go through tmd_server_submit / tmd_server_wait; latency
-    is submit -> completion on the host clock."""
+    single-point, 25% 200-step NVE, 15% FIRE (min_style fire) to max |F_i| <
+    0.01 eV/A (at most 1000 iterations).  Jobs go through tmd_server_submit /
+    tmd_server_wait; latency is submit -> completion on the host clock."""
     import threading
     from tmd_b200 import TensorMDModel, TensorMDServer, synth
+    rate = args.serve_rate if rate is None else rate
     rng = np.random.default_rng(77 + rank)
     pot = f"/tmp/tmd_bench_serve_{rank}.npz"
     syms = synth.gaussian_potential(pot, seed=4242, nelt=4, num_filters=16, rc=6.0,
@@ -760,8 +838,7 @@ def run_serving(args, rank, local, precision="fp32"):
     model = TensorMDModel(f"{pot} {' '.join(syms)}{prec}", device=local)
     sizes = np.unique(np.round(np.geomspace(32, 4096, 12)).astype(int))
     packings = {int(n): synth.random_packing(int(n), rng) for n in sizes}
-    t_arr = np.cumsum(rng.exponential(1.0 / args.serve_rate,
-                                      size=int(args.serve_rate * args.serve_window * 1.5)))
+    t_arr = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * args.serve_window * 1.5) + 8))
     t_arr = t_arr[t_arr < args.serve_window]
     kinds = rng.choice(3, size=len(t_arr), p=[0.60, 0.25, 0.15])
     jobs = [synth.serving_job(rng, kind=int(k), packings=packings) for k in kinds]
@@ -798,7 +875,7 @@ def run_serving(args, rank, local, precision="fp32"):
     model.close()
     lat = np.array([d["latency"] for d in done]) * 1000.0
     natoms = np.array([len(j[0]) for j in jobs])
-    out = {"precision": precision, "jobs": len(jobs), "arrival_rate_per_s": args.serve_rate,
+    out = {"precision": precision, "jobs": len(jobs), "arrival_rate_per_s": rate,
            "window_s": args.serve_window, "makespan_s": t_end - t_start,
            "solves_per_s": len(jobs) / (t_end - t_start),
            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
@@ -808,6 +885,7 @@ def run_serving(args, rank, local, precision="fp32"):
            "worker_seconds_by_phase": phases,
            "fire_converged_frac": float(np.mean([d["steps"] < 1000 for d, k in
                                                  zip(done, kinds) if k == 2] or [1.0])),
+           "fire_iteration_cap": 1000,
            "by_kind": {}}
     for k, name in enumerate(("single_point", "nve200", "fire")):
         sel = kinds == k
@@ -898,6 +976,8 @@ def profile_step(args):
     s = TensorMDSystem(model, len(x), 1.0)
     s.set_box(box)
     s.set_atoms(x, t, v)
+    if args.profile_desc:
+        s.set_descriptor_variant(args.profile_desc)
     for _ in range(args.profile_step):
         s.compute(1, 1, 1.0)
     print(json.dumps({"profile_step": args.profile_step, "config": args.config,

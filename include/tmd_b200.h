@@ -94,6 +94,29 @@ int tmd_system_set_atoms(tmd_system *sys, int n, const double *x,
  * and only real motion (more than skin/2) triggers a rebuild. */
 int tmd_system_set_positions(tmd_system *sys, const double *x);
 
+/* Ghost-aware mode for domain-decomposed (multi-rank) LAMMPS runs, in place
+ * of tmd_system_set_box + tmd_system_set_atoms.  x[nall*3], type[nall] with
+ * nall = nlocal + nghost are LAMMPS's atom->x and atom->type: the rank's
+ * local atoms first, then its ghosts (copies of other ranks' atoms and
+ * periodic images, placed by LAMMPS's border exchange out to the ghost
+ * cutoff, which must reach cutmax + skin).  The reference evaluates the
+ * local atoms over LAMMPS's full list with ghosts
+ * (pair_tensormd.cpp:141-184,321-330) and writes forces on local and ghost
+ * atoms for reverse communication (kernel.cu:1760-1789); here the system
+ * becomes non-periodic (its box is the atoms' bounding box plus cutmax +
+ * skin on each side), neighbor rows are built for all nall atoms (the same
+ * neighbor set as LAMMPS's list of the local atoms) and evaluated for the
+ * local ones.  tmd_compute then fills f[nall*3] (forces on the ghosts
+ * included, for LAMMPS to reverse-communicate), the energy of the local
+ * atoms, the virial of their pairs (LAMMPS's fdotr sum over local and ghost
+ * atoms), eatom[nall] (ghosts 0) and vatom[nall*6].  Until the next call,
+ * tmd_system_set_positions takes nall positions in the same order (LAMMPS's
+ * forward communication between reneighborings).  tmd_nve_run and
+ * tmd_nvt_run are refused in this mode (LAMMPS integrates); tmd_system_
+ * set_atoms leaves it. */
+int tmd_system_set_atoms_ghost(tmd_system *sys, int nlocal, int nghost, const double *x,
+                               const int *type);
+
 /* Download state; NULL pointers are skipped.  image[n*3] are the periodic
  * image counters accumulated by wrapping (Domain::pbc image flags). */
 int tmd_system_get(tmd_system *sys, double *x, double *v, double *f,
@@ -140,7 +163,10 @@ int tmd_neighbor_list(tmd_system *sys, double cut, int *counts, int *entries,
                       long cap, long *total);
 
 /* Per-atom descriptors G[n * n_desc] (compute tensormd/density,
- * compute_tensormd_density.cpp:129-200) of the last compute, in atom order. */
+ * compute_tensormd_density.cpp:129-200: array_atom[i] = the atom's MLP input
+ * row, b*k*m order) of the current positions, in atom order; the descriptor
+ * kernel runs for the call.  In ghost-aware mode, the nlocal local atoms'
+ * rows only. */
 int tmd_get_descriptors(tmd_system *sys, double *G);
 
 /* Kernel forms of the pair loops.  The reference has one implementation per
@@ -158,11 +184,13 @@ int tmd_get_descriptors(tmd_system *sys, double *G);
  *   1  min(K, 32) lanes per atom, K/min(K, 32) filters per lane, monomials of
  *      a pair computed once and shared through shared memory, G formed in
  *      the same kernel
+ *   2  as 1, the atom's lanes split into two streams that take alternate
+ *      pairs, 2K/min(K, 32) filters per lane (K = 4..64; other K run form 1)
  * The forms agree to FP32 rounding (summation order).  set_variant picks one;
  * autotune runs one evaluation, times reps launches of every form of the
  * family on the system's current atoms, keeps the fastest and recomputes the
  * results with it; ms (may be NULL) receives the mean device milliseconds per
- * launch of each form (4 force forms, 2 descriptor forms; at most
+ * launch of each form (4 force forms, 3 descriptor forms; at most
  * TMD_TUNE_VARIANTS). */
 #define TMD_TUNE_FORCE 0
 #define TMD_TUNE_DESCRIPTOR 1
@@ -181,6 +209,15 @@ long tmd_system_launches(const tmd_system *sys);
  * ones at set_atoms included, and the displacement-triggered ones inside MD
  * runs: LAMMPS's "Neighbor list builds" count).  Waits for the stream. */
 int tmd_system_rebuilds(tmd_system *sys, long *count);
+
+/* Failure-detection hook for tests (no reference counterpart).  With
+ * cycles > 0 the system's tensor-core MLP kernels (precision bf16, bf16x3,
+ * fp8) start every CTA with a wait of at most `cycles` clock cycles on one
+ * of their mbarriers, before any MMA or copy is issued; nothing arrives on
+ * it, so each CTA takes its timeout path (no asynchronous work in flight,
+ * TMEM freed) and tmd_compute returns TMD_ERR_TIMEOUT with the context still
+ * usable.  cycles = 0 (the default) turns it off; the FP32 MLP has no waits. */
+int tmd_system_set_wait_probe(tmd_system *sys, long long cycles);
 
 /* Measured FP32 issue peak of a device: a packed-FMA (FFMA2) kernel with
  * eight independent chains per thread on every SM, `reps` timed launches
@@ -250,9 +287,13 @@ int tmd_batch_nvt_run(tmd_batch *batch, int nsteps, double dt, const double *t_s
  * Job kinds:
  *   TMD_JOB_ENERGY  one force evaluation (energy, virial, forces)
  *   TMD_JOB_NVE     nsteps of velocity Verlet with step dt (as tmd_nve_run)
- *   TMD_JOB_FIRE    FIRE relaxation (Bitzek et al. 2006, semi-implicit Euler,
- *                   initial step dt, dt_max = 10 dt) until every force
- *                   component norm |F_i| <= fmax or nsteps iterations ran
+ *   TMD_JOB_FIRE    energy minimisation as LAMMPS's min_style fire at its
+ *                   defaults (min.cpp:63-72, min_fire.cpp:149-619: Euler
+ *                   implicit, half step back, dmax 0.1 A, delaystep 20,
+ *                   alpha0 0.25, tmax 10, tmin 0.02; initial step dt, v = 0
+ *                   at the start) until max_i |F_i| < fmax after an iteration
+ *                   (min_modify norm max) or nsteps iterations ran; a step
+ *                   back costs one more force evaluation of its cell
  * tmd_server_submit returns TMD_ERR_ARG for a box that is degenerate or too
  * small for the cutoff (more than 3 images per axis) and TMD_ERR_CAPACITY for
  * a job larger than max_atoms.  A job's results do not depend on the other

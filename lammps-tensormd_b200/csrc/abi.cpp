@@ -234,6 +234,7 @@ NbArgs nb_args(tmd_system *s) {
   a.ncells = s->ncells; a.cbox = s->cbox; a.cgeom = s->cgeom; a.acell = s->acell;
   a.coff = s->coff;
   a.cflag = s->ncells ? s->cflag : nullptr;
+  a.nlocal = s->n - s->nghost; a.pdf = s->pdf; a.wv = s->wv;
   return a;
 }
 
@@ -277,7 +278,7 @@ int rebuild_now(tmd_system *s) {
 // Force evaluation on the current (valid) list.
 DescArgs desc_args(tmd_system *s, int variant) {
   DescArgs d{};
-  d.n = s->n; d.cap = s->cap; d.kp = s->m->kp; d.box = s->box; d.x = s->x;
+  d.n = s->n - s->nghost; d.cap = s->cap; d.kp = s->m->kp; d.box = s->box; d.x = s->x;
   d.elem = s->elem; d.nbr = s->nbr; d.boff = s->boff; d.P = s->P; d.G = s->G;
   d.cbox = s->ncells ? s->cbox : nullptr; d.acell = s->acell;
   d.variant = variant;
@@ -301,7 +302,7 @@ int default_force_variant(const tmd_model *m) {
 
 ForceArgs force_args(tmd_system *s, float scale, int variant) {
   ForceArgs fa{};
-  fa.n = s->n; fa.cap = s->cap; fa.kp = s->m->kp; fa.box = s->box; fa.scale = scale;
+  fa.n = s->n - s->nghost; fa.cap = s->cap; fa.kp = s->m->kp; fa.box = s->box; fa.scale = scale;
   fa.x = s->x; fa.elem = s->elem; fa.nbr = s->nbr; fa.boff = s->boff;
   fa.P = s->P; fa.G = s->G; fa.dEdG = s->dEdG;
   fa.pdf = s->pdf; fa.wv = s->wv;
@@ -336,6 +337,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
     ta.persistent = m->tc_persistent; ta.smem_p = m->tc_smem_p;
     ta.dz_bf16_p = m->tc_dz_bf16_p ? 1 : 0;
     ta.streamed = m->tc_streamed; ta.smem_s = m->tc_smem_s; ta.stages = m->tc_stages;
+    ta.probe_wait = s->wait_probe;
     if (m->tc_fp8) launch_mlp_fp8(ta, s->st, s->launches);
     else launch_mlp_tc(ta, s->st, s->launches);
   } else {
@@ -377,11 +379,13 @@ int set_elements(tmd_system *s, int n, const int *elem) {
   s->nhc_valid = false;  // new atoms: a fresh thermostat
   // atoms grouped by element (TensorMD::calc_tensor_density i2row order),
   // MLP tiles of up to mlp_tr atoms of one element
+  // (ghost atoms, the last s->nghost, have no MLP rows)
+  const int ne = n - s->nghost;
   std::vector<int> cnt(h.nelt, 0), start(h.nelt + 1, 0);
-  for (int i = 0; i < n; i++) cnt[elem[i]]++;
+  for (int i = 0; i < ne; i++) cnt[elem[i]]++;
   for (int e = 0; e < h.nelt; e++) start[e + 1] = start[e] + cnt[e];
   std::vector<int> perm(n > 0 ? n : 1), fill(start.begin(), start.end() - 1);
-  for (int i = 0; i < n; i++) perm[fill[elem[i]]++] = i;
+  for (int i = 0; i < ne; i++) perm[fill[elem[i]]++] = i;
   std::vector<int> tiles;
   for (int e = 0; e < h.nelt; e++)
     for (int o = 0; o < cnt[e]; o += s->m->mlp_tr) {
@@ -1022,6 +1026,7 @@ int tmd_system_set_atoms(tmd_system *s, int n, const double *x, const int *type,
   std::vector<int> elem;
   int rc = map_types(s->m, n, type, elem);
   if (rc) return rc;
+  s->nghost = 0;
   rc = set_elements(s, n, elem.data());
   if (rc) return rc;
   if (n > 0) {
@@ -1038,6 +1043,61 @@ int tmd_system_set_atoms(tmd_system *s, int n, const double *x, const int *type,
   s->forces_valid = false;
   if (n == 0) return TMD_OK;
   int cap = initial_cap(s);
+  if (cap > s->cap) {
+    rc = alloc_neighbors(s, cap);
+    if (rc) return rc;
+  }
+  return rebuild_now(s);
+}
+
+int tmd_system_set_atoms_ghost(tmd_system *s, int nlocal, int nghost, const double *x,
+                               const int *type) {
+  if (!s || !x || !type || nlocal < 0 || nghost < 0) return fail(TMD_ERR_ARG, "null argument");
+  const long nall = (long)nlocal + nghost;
+  if (nall > s->natoms_cap) return fail(TMD_ERR_CAPACITY, "nlocal + nghost exceeds the system capacity");
+  if (s->ncells > 0) return fail(TMD_ERR_STATE, "a batch has no ghost atoms");
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  drop_graph(s);
+  const int n = (int)nall;
+  // a non-periodic box around every atom: the bounding box of the atoms with
+  // a margin of cutoff + skin on each side (atoms move less than skin/2
+  // between LAMMPS's reneighborings, when the caller sets the atoms anew)
+  double lo[3] = {0.0, 0.0, 0.0}, hi[3] = {1.0, 1.0, 1.0};
+  for (int a = 0; a < 3 && n > 0; a++) {
+    lo[a] = hi[a] = x[a];
+    for (int i = 1; i < n; i++) {
+      lo[a] = std::min(lo[a], x[3 * (size_t)i + a]);
+      hi[a] = std::max(hi[a], x[3 * (size_t)i + a]);
+    }
+  }
+  const double margin = s->m->h.rmax + s->skin;
+  const double bx[9] = {lo[0] - margin, lo[1] - margin, lo[2] - margin,
+                        hi[0] - lo[0] + 2 * margin, hi[1] - lo[1] + 2 * margin,
+                        hi[2] - lo[2] + 2 * margin, 0.0, 0.0, 0.0};
+  const int pbc[3] = {0, 0, 0};
+  box_setup(s->box, bx, pbc);
+  s->have_box = true;
+  int rc = bin_setup(s);
+  if (rc) return rc;
+  std::vector<int> elem;
+  rc = map_types(s->m, n, type, elem);
+  if (rc) return rc;
+  s->nghost = nghost;
+  rc = set_elements(s, n, elem.data());
+  if (rc) return rc;
+  if (n > 0) {
+    TMD_CUDA(cudaMemcpyAsync(s->x, x, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    TMD_CUDA(cudaMemsetAsync(s->v, 0, 3 * (size_t)n * sizeof(double), s->st));
+    TMD_CUDA(cudaMemsetAsync(s->image, 0, 3 * (size_t)n * sizeof(int), s->st));
+  }
+  TMD_CUDA(cudaStreamSynchronize(s->st));
+  s->have_atoms = true;
+  s->forces_valid = false;
+  if (n == 0) return TMD_OK;
+  // rows for the density inside the atoms' own bounding box
+  double vol = 1.0;
+  for (int a = 0; a < 3; a++) vol *= std::max(hi[a] - lo[a], 1.0);
+  const int cap = cap_for_density(s, n / vol);
   if (cap > s->cap) {
     rc = alloc_neighbors(s, cap);
     if (rc) return rc;
@@ -1085,18 +1145,25 @@ int tmd_compute(tmd_system *s, int eflag, int vflag, double scale, double *energ
   }
   int rc;
   bool want_vatom = vatom != nullptr;
+  // energies and virial partials belong to the evaluated (local) atoms;
+  // forces and per-atom virials to every atom, ghosts included
+  const int nl = n - s->nghost;
   launch_force_eval(s, (float)scale, want_vatom);
   if (eflag || energy)
-    launch_reduce_scaled(s->E, n, s->partial, s->scal, scale, s->st, s->launches);
+    launch_reduce_scaled(s->E, nl, s->partial, s->scal, scale, s->st, s->launches);
   if (vflag || virial)
-    launch_reduce_f64(s->wv, n, 6, s->partial, s->scal + 1, s->st, s->launches);
+    launch_reduce_f64(s->wv, nl, 6, s->partial, s->scal + 1, s->st, s->launches);
   launch_check_finite(n, s->f, (eflag || energy) ? s->scal : nullptr, s->status, s->st,
                       s->launches);
   TMD_CUDA(cudaGetLastError());
-  if (eatom) launch_scale_copy(s->E, n, scale, s->eatom, s->st, s->launches);
+  if (eatom && nl > 0) launch_scale_copy(s->E, nl, scale, s->eatom, s->st, s->launches);
   TMD_CUDA(cudaMemcpyAsync(s->h_scal, s->scal, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
   if (f) TMD_CUDA(cudaMemcpyAsync(f, s->f, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
-  if (eatom) TMD_CUDA(cudaMemcpyAsync(eatom, s->eatom, n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  if (eatom) {
+    if (nl > 0)
+      TMD_CUDA(cudaMemcpyAsync(eatom, s->eatom, nl * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    for (int i = nl; i < n; i++) eatom[i] = 0.0;  // ghosts carry no energy
+  }
   if (vatom) TMD_CUDA(cudaMemcpyAsync(vatom, s->vatom, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
   rc = read_status(s);
   if (rc) return rc;
@@ -1121,6 +1188,7 @@ int tmd_compute(tmd_system *s, int eflag, int vflag, double scale, double *energ
 int tmd_nve_run(tmd_system *s, int nsteps, double dt, int thermo_every, double *thermo) {
   if (!s || nsteps < 0 || !(dt > 0)) return fail(TMD_ERR_ARG, "bad nve arguments");
   if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before nve_run");
+  if (s->nghost > 0) return fail(TMD_ERR_STATE, "ghost atoms: the caller integrates");
   if (thermo && thermo_every < 1) return fail(TMD_ERR_ARG, "thermo_every must be >= 1");
   int rows = thermo ? 1 + nsteps / thermo_every + ((nsteps % thermo_every) ? 1 : 0) : 0;
   // row r: potential energy, kinetic energy of the whole system
@@ -1138,6 +1206,7 @@ int tmd_nvt_run(tmd_system *s, int nsteps, double dt, double t_start, double t_s
   if (!(t_start > 0) || !(t_stop > 0) || !(t_damp > 0))
     return fail(TMD_ERR_ARG, "fix nvt needs t_start, t_stop and t_damp > 0");
   if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before nvt_run");
+  if (s->nghost > 0) return fail(TMD_ERR_STATE, "ghost atoms: the caller integrates");
   if (s->ncells > 0) return fail(TMD_ERR_STATE, "a batch runs nvt through tmd_batch_nvt_run");
   if (thermo && thermo_every < 1) return fail(TMD_ERR_ARG, "thermo_every must be >= 1");
   int rows = thermo ? 1 + nsteps / thermo_every + ((nsteps % thermo_every) ? 1 : 0) : 0;
@@ -1218,12 +1287,26 @@ int tmd_neighbor_list(tmd_system *s, double cut, int *counts, int *entries, long
 
 int tmd_get_descriptors(tmd_system *s, double *G) {
   if (!s || !G) return fail(TMD_ERR_ARG, "null argument");
-  size_t cnt = (size_t)s->n * s->m->h.nin;
-  std::vector<float> tmp(cnt);
-  if (cnt) {
-    TMD_CUDA(cudaMemcpyAsync(tmp.data(), s->G, cnt * sizeof(float), cudaMemcpyDeviceToHost, s->st));
-    TMD_CUDA(cudaStreamSynchronize(s->st));
+  if (!s->have_atoms) return fail(TMD_ERR_STATE, "set_atoms before get_descriptors");
+  TMD_CUDA(cudaSetDevice(s->m->device));
+  const int nl = s->n - s->nghost;
+  size_t cnt = (size_t)nl * s->m->h.nin;
+  if (cnt == 0) return TMD_OK;
+  // the descriptor of the current positions (compute tensormd/density runs
+  // between force evaluations, after LAMMPS moved the atoms)
+  for (int attempt = 0; attempt < 2; attempt++) {
+    launch_descriptor(desc_args(s, s->desc_variant), s->st, s->launches);
+    TMD_CUDA(cudaGetLastError());
+    int rc = read_status(s);
+    if (rc) return rc;
+    if (!(s->h_status[0] & kStatusOverflow)) break;
+    rc = rebuild_now(s);  // positions outgrew the rows: rebuild larger, redo
+    if (rc) return rc;
   }
+  if (s->h_status[0] & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside a non-periodic boundary");
+  std::vector<float> tmp(cnt);
+  TMD_CUDA(cudaMemcpyAsync(tmp.data(), s->G, cnt * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+  TMD_CUDA(cudaStreamSynchronize(s->st));
   for (size_t i = 0; i < cnt; i++) G[i] = tmp[i];
   return TMD_OK;
 }
@@ -1307,6 +1390,13 @@ int tmd_system_stream(tmd_system *s, void **stream) {
 }
 
 long tmd_system_launches(const tmd_system *s) { return s ? s->launches : 0; }
+
+int tmd_system_set_wait_probe(tmd_system *s, long long cycles) {
+  if (!s || cycles < 0) return fail(TMD_ERR_ARG, "bad wait probe");
+  drop_graph(s);  // a captured step holds the old kernel parameters
+  s->wait_probe = cycles;
+  return TMD_OK;
+}
 
 int tmd_system_rebuilds(tmd_system *s, long *count) {
   if (!s || !count) return fail(TMD_ERR_ARG, "null argument");

@@ -180,8 +180,7 @@ __device__ inline void store_pair_geo(const GeoSlot *s, float4 *__restrict__ dst
 }
 
 template <int RK>
-__device__ inline PairGeo load_pair_geo(const float4 *__restrict__ src, int &t) {
-  const float4 a = __ldg(src), b = __ldg(src + 1);
+__device__ inline PairGeo decode_pair_geo(const float4 a, const float4 b, int &t) {
   PairGeo g;
   g.r = a.x; g.rlo = a.y; g.ux = a.z; g.uy = a.w; g.uz = b.x;
   if (RK == kRadTable) {
@@ -192,6 +191,11 @@ __device__ inline PairGeo load_pair_geo(const float4 *__restrict__ src, int &t) 
   t = __float_as_int(b.w);
   g.rinv = __frcp_rn(g.r);  // 1/r rounded to nearest, as pair_geometry
   return g;
+}
+
+template <int RK>
+__device__ inline PairGeo load_pair_geo(const float4 *__restrict__ src, int &t) {
+  return decode_pair_geo<RK>(__ldg(src), __ldg(src + 1), t);
 }
 
 template <int TPA, int D, int RK, bool MULTI>
@@ -397,6 +401,156 @@ k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ 
   }
 }
 
+// Two-stream wide form: W lanes per atom as two pair streams of FL = W/2
+// lanes, FPL = K/FL filters per lane.  The geometry ring is k_descriptor_w's;
+// of each chunk of queued pairs, stream 0 takes the even and stream 1 the odd
+// ones, so every monomial vector read from shared memory feeds 2 * FPL packed
+// FMAs instead of 2 (the read and the radial of a pair are shared by more
+// filters per lane) while a warp still holds W = min(K, 32) lanes per atom.
+// The streams' partial P are added (stream 0 + stream 1) by a shuffle at the
+// end of each element block; each stream then forms and writes half of the
+// lane's filters' P and G rows.
+template <int W, int FPL, int D, int RK, bool MULTI>
+__global__ void __launch_bounds__(kPairThreads, 4)
+k_descriptor_w2(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
+                const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
+                float *__restrict__ P, float *__restrict__ G,
+                const BoxP *__restrict__ cbox,
+                const int *__restrict__ acell, float4 *__restrict__ pdf,
+                float4 *__restrict__ pgeo, int *__restrict__ pcnt) {
+  constexpr int FL = W / 2;
+  constexpr int D4 = (D + 3) / 4 * 4;
+  constexpr int M = D == 1 ? 1 : (D == 4 ? 2 : (D == 10 ? 3 : 4));
+  constexpr int P2 = D4 / 2;
+  __shared__ GeoSlot geo[2 * kPairThreads];
+  __shared__ __align__(16) float mono[2 * kPairThreads * D4];
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = gt / W;
+  const int sub = gt % W;
+  if (a >= n) return;
+  const int lane = threadIdx.x & 31;
+  const int stream = sub / FL, fl = sub % FL;
+  PairRing<W> pr;
+  pr.sub = sub;
+  pr.gshift = lane & ~(W - 1);
+  pr.gmask = PairRing<W>::kBits << pr.gshift;
+  pr.ring = geo + 2 * (threadIdx.x - sub);
+  float *mr = mono + 2 * (threadIdx.x - sub) * D4;  // monomials of the group's slots
+  const int B = kp.B, K = kp.K;
+  const int kf = fl * FPL;
+  Radial1<RK> R[FPL];
+#pragma unroll
+  for (int f = 0; f < FPL; f++) R[f] = load_radial1<RK>(kp, kf + f);
+  const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
+  const double xi = x[3 * a], yi = x[3 * a + 1], zi = x[3 * a + 2];
+  const uint32_t *row = nbr + (size_t)a * cap;
+  const int *bo = boff + (size_t)a * (B + 1);
+  const unsigned live = live_lanes(gt, (long)n * W);
+  auto keep_monomials = [&](int idx, const PairGeo &g) {
+    float Mv[D4];
+    moments<D>(g.ux, g.uy, g.uz, Mv);
+#pragma unroll
+    for (int d = D; d < D4; d++) Mv[d] = 0.f;
+    float4 *dst = reinterpret_cast<float4 *>(mr + idx * D4);
+#pragma unroll
+    for (int v = 0; v < D4 / 4; v++)
+      dst[v] = make_float4(Mv[4 * v], Mv[4 * v + 1], Mv[4 * v + 2], Mv[4 * v + 3]);
+  };
+  float4 *pdf_row = pdf + (size_t)a * cap;
+  float4 *pg_row = pgeo + (size_t)a * cap * 2;
+  int nact = 0;
+  for (int b = 0; b < B; b++) {
+    if (b > 0) __syncwarp(live);
+    const int nact0 = nact;
+    float2 acc[FPL][P2];
+#pragma unroll
+    for (int f = 0; f < FPL; f++)
+#pragma unroll
+      for (int p = 0; p < P2; p++) acc[f][p] = make_float2(0.f, 0.f);
+    pr.begin(x, row, bo[b], bo[b + 1]);
+    for (;;) {
+      const int cnt = pr.feed_with(kp, bx, xi, yi, zi, x, row, pdf_row, keep_monomials);
+      if (cnt == 0) break;
+      if (sub < cnt) store_pair_geo<RK>(pr.slot(sub), pg_row + 2 * (nact + sub));
+      nact += cnt;
+      for (int c = stream; c < cnt; c += 2) {
+        const PairGeo g = geo_load_radial<RK>(pr.slot(c));
+        const float4 *ms = reinterpret_cast<const float4 *>(
+            mr + ((pr.head + c) & (PairRing<W>::kSlots - 1)) * D4);
+        float2 h2[FPL];
+#pragma unroll
+        for (int f = 0; f < FPL; f++) {
+          const float h = radial1<RK>(kp, R[f], g);
+          h2[f] = make_float2(h, h);
+        }
+#pragma unroll
+        for (int v = 0; v < D4 / 4; v++) {
+          const float4 m4 = ms[v];
+          const float2 lo = make_float2(m4.x, m4.y), hi = make_float2(m4.z, m4.w);
+#pragma unroll
+          for (int f = 0; f < FPL; f++) {
+            acc[f][2 * v] = __ffma2_rn(h2[f], lo, acc[f][2 * v]);
+            acc[f][2 * v + 1] = __ffma2_rn(h2[f], hi, acc[f][2 * v + 1]);
+          }
+        }
+      }
+      pr.pop(cnt);
+    }
+    if (sub == 0) pcnt[(size_t)a * B + b] = nact - nact0;
+    // P = stream 0 + stream 1 (both streams hold the sum afterwards)
+#pragma unroll
+    for (int f = 0; f < FPL; f++)
+#pragma unroll
+      for (int p = 0; p < P2; p++) {
+        const float ox = __shfl_xor_sync(pr.gmask, acc[f][p].x, FL, W);
+        const float oy = __shfl_xor_sync(pr.gmask, acc[f][p].y, FL, W);
+        acc[f][p] = stream == 0 ? make_float2(acc[f][p].x + ox, acc[f][p].y + oy)
+                                : make_float2(ox + acc[f][p].x, oy + acc[f][p].y);
+      }
+    float *Pp = P + (((size_t)a * B + b) * K + kf) * D;
+    float *Gp = G + (((size_t)a * B + b) * K + kf) * M;
+#pragma unroll
+    for (int f = 0; f < FPL; f++) {
+      if ((f & 1) != stream) continue;  // each stream writes half the filters
+      if constexpr (D % 2 == 0) {
+        float2 *P2p = reinterpret_cast<float2 *>(Pp + f * D);
+#pragma unroll
+        for (int p = 0; p < D / 2; p++) P2p[p] = acc[f][p];
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; d++) Pp[f * D + d] = (d & 1) ? acc[f][d >> 1].y : acc[f][d >> 1].x;
+      }
+#pragma unroll
+      for (int m = 0; m < M; m++) {
+        float sacc = 0.f;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          const float pv = (d & 1) ? acc[f][d >> 1].y : acc[f][d >> 1].x;
+          sacc = fmaf(kp.T[m * D + d], pv * pv, sacc);
+        }
+        if (m == 0) sacc = copysignf(1.f, acc[f][0].x) * sqrtf(sacc);
+        Gp[f * M + m] = sacc;
+      }
+    }
+  }
+}
+
+template <int W, int FPL, int RK, bool MULTI>
+void launch_descriptor_w2(const DescArgs &a, cudaStream_t st) {
+  const int T = kPairThreads;
+  const long threads = (long)a.n * W;
+  int grid = (int)((threads + T - 1) / T);
+  if (grid < 1) grid = 1;
+#define TMD_DESCW_ARGS a.kp, a.box, a.n, a.cap, a.x, a.nbr, a.boff, a.P, a.G, a.cbox, a.acell, a.pdf, a.pgeo, a.pcnt
+  switch (a.kp.D) {
+    case 1: k_descriptor_w2<W, FPL, 1, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
+    case 4: k_descriptor_w2<W, FPL, 4, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
+    case 10: k_descriptor_w2<W, FPL, 10, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
+    default: k_descriptor_w2<W, FPL, 20, RK, MULTI><<<grid, T, 0, st>>>(TMD_DESCW_ARGS); break;
+  }
+#undef TMD_DESCW_ARGS
+}
+
 template <int W, int FPL, int RK, bool MULTI>
 void launch_descriptor_w(const DescArgs &a, cudaStream_t st) {
   const int T = kPairThreads;
@@ -470,7 +624,17 @@ void launch_descriptor_tpa(const DescArgs &a, cudaStream_t st) {
 // own translation unit so the variants compile in parallel.
 template <int RK, bool MULTI>
 void launch_descriptor_rk(const DescArgs &a, cudaStream_t st) {
-  if (a.variant == kDescWide) {
+  if (a.variant == kDescWide2 && a.kp.K >= 4 && a.kp.K <= 64) {
+    switch (a.kp.K) {
+      case 4: launch_descriptor_w2<4, 2, RK, MULTI>(a, st); return;
+      case 8: launch_descriptor_w2<8, 2, RK, MULTI>(a, st); return;
+      case 16: launch_descriptor_w2<16, 2, RK, MULTI>(a, st); return;
+      case 32: launch_descriptor_w2<32, 2, RK, MULTI>(a, st); return;
+      case 64: launch_descriptor_w2<32, 4, RK, MULTI>(a, st); return;
+      default: break;  // other filter counts: the one-stream wide form
+    }
+  }
+  if (a.variant == kDescWide || a.variant == kDescWide2) {
     switch (a.kp.K) {
       case 4: launch_descriptor_w<4, 1, RK, MULTI>(a, st); break;
       case 8: launch_descriptor_w<8, 1, RK, MULTI>(a, st); break;

@@ -140,11 +140,22 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
       }
     }
     __syncwarp(gmask);
+    // the lane's next pair's geometry is loaded while the current one runs
+    float4 nga = make_float4(0.f, 0.f, 0.f, 0.f), ngb = nga;
+    if (sub < np) {
+      nga = __ldg(pg_row + 2 * (pos + sub));
+      ngb = __ldg(pg_row + 2 * (pos + sub) + 1);
+    }
     for (int c0 = 0; c0 < np; c0 += W) {
       const int c = c0 + sub;
+      const float4 cga = nga, cgb = ngb;
+      if (c + W < np) {
+        nga = __ldg(pg_row + 2 * (pos + c + W));
+        ngb = __ldg(pg_row + 2 * (pos + c + W) + 1);
+      }
       if (c < np) {
         int t;
-        const PairGeo g = load_pair_geo<RK>(pg_row + 2 * (pos + c), t);
+        const PairGeo g = decode_pair_geo<RK>(cga, cgb, t);
         float2 V2[P2], W2[P2];
 #pragma unroll
         for (int p = 0; p < P2; p++) {

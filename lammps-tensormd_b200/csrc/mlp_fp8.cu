@@ -113,6 +113,12 @@ k_mlp_fp8(MlpTcArgs a) {
   const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
   uint32_t phase = 0;
   bool ok = true;
+  if (a.probe_wait > 0) {
+    // failure-detection hook: a bounded wait on a barrier nothing arrives on
+    // yet, before any MMA or copy is issued
+    const bool done = mbar_wait(&mbar, 0u, a.probe_wait);
+    ok = __syncthreads_and(done ? 1 : 0) != 0;
+  }
   float sa = rsc[tid];  // scale of this thread's row of the current A operand
 
   // D[TM x nout] = A[TM x kred] . B^T, B rows n0..n0+nout-1 of a packed block

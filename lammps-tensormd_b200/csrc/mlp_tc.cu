@@ -122,6 +122,12 @@ k_mlp_tc(MlpTcArgs a) {
   const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
   uint32_t phase = 0;
   bool ok = true;
+  if (a.probe_wait > 0) {
+    // failure-detection hook: a bounded wait on a barrier nothing arrives on
+    // yet, before any MMA or copy is issued
+    const bool done = mbar_wait(&mbar, 0u, a.probe_wait);
+    ok = __syncthreads_and(done ? 1 : 0) != 0;
+  }
 
   // D[TM x nout] (TMEM columns 0..nout-1) = A[TM x kred] . B^T with B rows
   // n0..n0+nout-1 of a packed weight block of brows rows.
@@ -365,6 +371,12 @@ k_mlp_tcp(MlpTcArgs a) {
   const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16);
   uint32_t phase = 0;
   bool ok = true;
+  if (a.probe_wait > 0) {
+    // failure-detection hook: a bounded wait on a barrier nothing arrives on
+    // yet, before any MMA or copy is issued
+    const bool done = mbar_wait(&mbar, 0u, a.probe_wait);
+    ok = __syncthreads_and(done ? 1 : 0) != 0;
+  }
 
   // D[TM x nout] = A[TM x kred] . B^T; A = actb laid out with kfull columns,
   // B rows n0..n0+nout-1 of a resident packed block of brows rows (hi, then
@@ -687,6 +699,13 @@ k_mlp_tcs(MlpTcArgs a) {
   int q_issue = 0, q_mma = 0;  // thread 0: next chunk to copy / to multiply
   bool ok0 = true;             // thread 0: its own waits
   bool ok = true;
+  if (a.probe_wait > 0) {
+    // failure-detection hook: a bounded wait on a barrier nothing arrives on
+    // yet, before any MMA or copy is issued
+    const bool done = mbar_wait(&drainb, 0u, a.probe_wait);
+    ok = __syncthreads_and(done ? 1 : 0) != 0;
+  }
+  if (!ok) ok0 = false;
   uint32_t gk[2] = {0, 0}, ak[4] = {0, 0, 0, 0};  // completions consumed per barrier
 
   // thread 0: copy chunks up to (not including) qlim into their stages

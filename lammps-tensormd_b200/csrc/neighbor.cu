@@ -799,6 +799,21 @@ void launch_nearest_image(int n, double *x, const double *xbuild, const BoxP &bo
   launches += 1;
 }
 
+// Ghost-aware mode: rows of ghost atoms are built (their partner slots serve
+// the local atoms' gather) but never evaluated, so after a build their pair
+// forces and virial partials are set to zero once.
+__global__ void k_nb_zero_ghost(int n, int nlocal, int cap, float4 *__restrict__ pdf,
+                                double *__restrict__ wv, const int *flag) {
+  if (!*flag) return;
+  const long e0 = (long)nlocal * cap, e1 = (long)n * cap;
+  for (long e = e0 + blockIdx.x * (long)blockDim.x + threadIdx.x; e < e1;
+       e += (long)gridDim.x * blockDim.x)
+    pdf[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (long e = 6L * nlocal + blockIdx.x * (long)blockDim.x + threadIdx.x; e < 6L * n;
+       e += (long)gridDim.x * blockDim.x)
+    wv[e] = 0.0;
+}
+
 // End of the rebuild sequence: count a rebuild that ran (flag[1]) and clear
 // the pending flag.
 __global__ void k_nb_clear(int *flag) {
@@ -871,6 +886,11 @@ void launch_neighbor_build(const NbArgs &a, cudaStream_t st, long &launches) {
   k_nb_finish<<<gn, T, 0, st>>>(a.n, a.x, a.xbuild, a.acell, a.cflag, a.flag);
   if (a.cflag) {
     k_nbc_clear<<<cap_grid((a.ncells + T - 1) / T), T, 0, st>>>(a.ncells, a.cflag, a.flag);
+    launches += 1;
+  }
+  if (a.pdf && a.nlocal < a.n) {
+    k_nb_zero_ghost<<<cap_grid(((long)(a.n - a.nlocal) * a.cap + T - 1) / T), T, 0, st>>>(
+        a.n, a.nlocal, a.cap, a.pdf, a.wv, a.flag);
     launches += 1;
   }
   k_nb_clear<<<1, 1, 0, st>>>(a.flag);

@@ -8,8 +8,9 @@
 //      then FIFO, up to the atom and cell budget), re-laying the cells out on
 //      the device: continuing cells move with their state and neighbor lists,
 //      new jobs come from a staging upload and get their lists built;
-//   2. one force evaluation: single-point jobs are finished by it, FIRE jobs
-//      that already satisfy fmax too; these leave before the steps;
+//   2. one force evaluation: single-point jobs are finished by it and leave
+//      before the steps (FIRE jobs test convergence only after an iteration,
+//      as LAMMPS does);
 //   3. steps_per_tick steps of the mixed integrator (server_kernels.cu) for the rest;
 //   4. per-cell status to the host; finished NVE / FIRE jobs are copied out.
 // A job waits at most one tick before it enters the batch, and every step
@@ -90,7 +91,8 @@ struct tmd_server {
   int *stage_e = nullptr;
   int *src = nullptr, *fresh = nullptr, *estart = nullptr;
   CellCtl *ctl = nullptr;
-  double *pw = nullptr, *csum = nullptr, *fsq = nullptr, *cfmax = nullptr;
+  double *pw = nullptr, *pm = nullptr, *csum = nullptr, *cmax = nullptr, *fsq = nullptr,
+         *cfmax = nullptr;
 };
 
 namespace {
@@ -110,8 +112,9 @@ CellCtl initial_ctl(const Job &j) {
   q.mode = j.kind;
   q.left = j.kind == kJobEnergy ? 0 : j.nsteps;
   q.dt = j.dt;
-  q.dtmax = 10.0 * j.dt;
-  q.alpha = 0.1;
+  q.dtmax = 10.0 * j.dt;   // min_style fire tmax 10
+  q.dtmin = 0.02 * j.dt;   // tmin 0.02
+  q.alpha = 0.25;          // alpha0
   q.fmax2 = j.fmax * j.fmax;
   return q;
 }
@@ -129,7 +132,7 @@ size_t server_bytes_per_atom(const tmd_model *m, int cap) {
   a += 4 * B * h.K * h.D + 2 * 4 * nin;  // P; G and dE/dG
   a += 8 + 48 + 8 + 48 + 8 + 4 + 4;    // E, virial partials, eatom, vatom, ke, perm, cell
   a += 4 * 24 + 12 + 4 + 4 * (B + 1);  // relayout copies: x v f xbuild, image, element, offsets
-  a += 48 + 4 + 24 + 8;                // staging x v, staging element, FIRE power, |F|^2
+  a += 48 + 4 + 40 + 8;                // staging x v, staging element, FIRE power and maxima, |F|^2
   a += 2 * 12;                         // bins: count, start, cursor
   a += (size_t)cap * 64;
   return a;
@@ -482,7 +485,7 @@ int tick(tmd_server *sv) {
   const double half = 0.5 * s->skin;
   for (int k = 0; k < sv->steps_per_tick; k++) {
     launch_srv_pre(s->n, s->ncells, s->acell, s->coff, sv->ctl, s->x, s->v, s->f, s->elem,
-                   s->m->d_mass, sv->pw, sv->csum, s->st, s->launches);
+                   s->m->d_mass, sv->pw, sv->pm, sv->csum, sv->cmax, s->st, s->launches);
     launch_neighbor_check(s->n, s->x, s->xbuild, half * half, s->flag, s->st, s->launches,
                           s->acell, s->cflag);
     launch_neighbor_build(nb_args(s), s->st, s->launches);
@@ -594,7 +597,9 @@ int server_create(const tmd_model *m, int max_atoms, int max_cells, double skin,
   if (e == cudaSuccess) e = dalloc(&sv->estart, C * m->h.nelt);
   if (e == cudaSuccess) e = dalloc(&sv->ctl, C);
   if (e == cudaSuccess) e = dalloc(&sv->pw, 3 * N);
+  if (e == cudaSuccess) e = dalloc(&sv->pm, 2 * N);
   if (e == cudaSuccess) e = dalloc(&sv->csum, 4 * C);
+  if (e == cudaSuccess) e = dalloc(&sv->cmax, 2 * C);
   if (e == cudaSuccess) e = dalloc(&sv->fsq, N);
   if (e == cudaSuccess) e = dalloc(&sv->cfmax, C);
   if (e != cudaSuccess) {
@@ -663,7 +668,8 @@ void tmd_server_free(tmd_server *sv) {
   dfree(sv->xb2); dfree(sv->elem2); dfree(sv->boff2); dfree(sv->rev2);
   dfree(sv->stage_x); dfree(sv->stage_v); dfree(sv->stage_e); dfree(sv->src);
   dfree(sv->fresh); dfree(sv->estart); dfree(sv->ctl);
-  dfree(sv->pw); dfree(sv->csum); dfree(sv->fsq); dfree(sv->cfmax);
+  dfree(sv->pw); dfree(sv->pm); dfree(sv->csum); dfree(sv->cmax); dfree(sv->fsq);
+  dfree(sv->cfmax);
   tmd_system_free(sv->s);
   delete sv;
 }
@@ -693,7 +699,8 @@ int tmd_server_submit(tmd_server *sv, int kind, int n, const double *x, const in
   j->n = n;
   j->x.assign(x, x + 3 * (size_t)n);
   j->v.assign(3 * (size_t)n, 0.0);
-  if (v) j->v.assign(v, v + 3 * (size_t)n);
+  // FIRE starts from v = 0 (MinFire::setup_style); the caller's v is ignored
+  if (v && kind != kJobFire) j->v.assign(v, v + 3 * (size_t)n);
   int rc = map_types(sv->m, n, type, j->elem);
   if (rc) return rc;
   j->ecount.assign(sv->m->h.nelt, 0);

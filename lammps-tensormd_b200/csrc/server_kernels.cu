@@ -3,12 +3,18 @@
 //
 // Every cell carries a CellCtl.  NVE cells follow FixNVE (fix_nve.cpp:64-141,
 // metal units, products and sums rounded separately like integrate.cu).
-// FIRE cells follow Bitzek et al., PRL 97, 170201 (2006) with a semi-implicit
-// Euler step: from the current v and F of the cell, P = F.v; P > 0 mixes
-// v <- (1 - a) v + a |v| F/|F| and, after more than Nmin such steps in a row,
-// grows dt (x finc, capped at dtmax) and shrinks a (x fa); P <= 0 zeroes v,
-// resets a and, past the first Nmin iterations, halves dt.  Then
-// v <- v + dt F/m and x <- x + dt v.  Convergence: max_i |F_i| <= fmax.
+// FIRE cells follow LAMMPS's min_style fire at its defaults (min.cpp:63-72,
+// MinFire::run_iterate<EULERIMPLICIT> in min_fire.cpp:149-619): per cell
+// P = F.v; P > 0 mixes v <- (1 - a) v + a sqrt(v.v / F.F) F after the Euler
+// kick and, more than delaystep (20) iterations after the last P <= 0, grows
+// dt by 1.1 (at most 10 dt0) and shrinks a by 0.99; P <= 0 (after the first
+// 20 iterations) resets a to 0.25 and halves dt (not below 0.02 dt0), steps
+// the atoms back by dt v / 2 and zeroes v, after which the forces of the new
+// positions are evaluated (one more force evaluation of the batch) before the
+// step continues from v = 0.  The step is limited so that no atom moves more
+// than dmax = 0.1 A along an axis; then v += dt F / m and x += dt v.  An
+// iteration ends with the force evaluation after its move; the cell has
+// converged when max_i |F_i|^2 < fmax^2 (min_modify norm max) at that point.
 #include <cmath>
 
 #include "tmd_kernels.h"
@@ -17,8 +23,11 @@ namespace tmd {
 
 namespace {
 constexpr double kFtm2v = 1.0 / 1.0364269e-4;  // metal units, update.cpp:187-206
-constexpr int kFireNmin = 5;
-constexpr double kFireFinc = 1.1, kFireFdec = 0.5, kFireAlpha0 = 0.1, kFireFalpha = 0.99;
+// min_style fire defaults (min.cpp:63-72)
+constexpr int kFireDelay = 20;
+constexpr double kFireGrow = 1.1, kFireShrink = 0.5, kFireAlpha0 = 0.25, kFireAlphaShrink = 0.99;
+constexpr double kFireDmax = 0.1;
+constexpr int kFireMaxNeg = 2000;  // max_vdotf_negatif
 constexpr int kThreads = 256;
 
 __device__ inline bool fire_active(const CellCtl &c) {
@@ -154,48 +163,120 @@ void launch_srv_mark(int ncells, const int *fresh, int *cflag, int *flag, cudaSt
   launches += 1;
 }
 
-// (F.v, v.v, F.F) per atom of active FIRE cells, 0 elsewhere.
+// Per atom of active FIRE cells (0 elsewhere): (F.v, v.v, F.F) into pw and
+// (max_k |v_k|, max_k |F_k| / m) into pm, for the per-cell sums and maxima.
 __global__ void k_srv_power(int n, const int *__restrict__ acell,
                             const CellCtl *__restrict__ ctl, const double *__restrict__ v,
-                            const double *__restrict__ f, double *__restrict__ pw) {
+                            const double *__restrict__ f, const int *__restrict__ elem,
+                            const double *__restrict__ mass_e, double *__restrict__ pw,
+                            double *__restrict__ pm) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
-  double p = 0, vv = 0, ff = 0;
+  double p = 0, vv = 0, ff = 0, vm = 0, fm = 0;
   if (fire_active(ctl[acell[a]])) {
     for (int d = 0; d < 3; d++) {
       const double vd = v[3L * a + d], fd = f[3L * a + d];
-      p += fd * vd;
+      p += vd * fd;
       vv += vd * vd;
       ff += fd * fd;
+      vm = fmax(vm, fabs(vd));
+      fm = fmax(fm, fabs(fd));
     }
+    fm /= mass_e[elem[a]];
   }
   pw[3L * a] = p;
   pw[3L * a + 1] = vv;
   pw[3L * a + 2] = ff;
+  pm[2L * a] = vm;
+  pm[2L * a + 1] = fm;
 }
 
-// FIRE state of every active cell from its (P, v.v, F.F) sums.
+// Per-cell maxima of two interleaved per-atom values (one block per cell).
+__global__ void k_cell_max2(int ncells, const int *__restrict__ coff,
+                            const double *__restrict__ in, double *__restrict__ out) {
+  __shared__ double sh[2][kThreads];
+  for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
+    double m0 = 0.0, m1 = 0.0;
+    for (int a = coff[c] + threadIdx.x; a < coff[c + 1]; a += blockDim.x) {
+      m0 = fmax(m0, in[2L * a]);
+      m1 = fmax(m1, in[2L * a + 1]);
+    }
+    sh[0][threadIdx.x] = m0;
+    sh[1][threadIdx.x] = m1;
+    __syncthreads();
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) {
+        sh[0][threadIdx.x] = fmax(sh[0][threadIdx.x], sh[0][threadIdx.x + s]);
+        sh[1][threadIdx.x] = fmax(sh[1][threadIdx.x], sh[1][threadIdx.x + s]);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      out[2L * c] = sh[0][0];
+      out[2L * c + 1] = sh[1][0];
+    }
+    __syncthreads();
+  }
+}
+
+// Step limit so that no atom moves more than dmax along an axis, for the
+// largest velocity component vmax (min_fire.cpp, dtvone).
+__device__ inline double fire_limit(double dt, double vmax) {
+  return dt * vmax > kFireDmax ? kFireDmax / vmax : dt;
+}
+
+// FIRE plan of every active cell for this step, from its (P, v.v, F.F) sums
+// and (max |v_k|, max |F_k| / m) maxima.
 __global__ void k_srv_fire_update(int ncells, CellCtl *__restrict__ ctl,
-                                  const double *__restrict__ csum) {
+                                  const double *__restrict__ csum,
+                                  const double *__restrict__ cmax) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncells) return;
   CellCtl q = ctl[c];
-  if (!fire_active(q)) return;
+  if (!fire_active(q)) {
+    q.plan = kFirePlanNone;
+    ctl[c] = q;
+    return;
+  }
   const double P = csum[4L * c], vv = csum[4L * c + 1], ff = csum[4L * c + 2];
-  if (P > 0.0) {
-    q.mix1 = 1.0 - q.alpha;
-    q.mix2 = ff > 0.0 ? q.alpha * sqrt(vv / ff) : 0.0;
-    q.npos++;
-    if (q.npos > kFireNmin) {
-      q.dt = fmin(q.dt * kFireFinc, q.dtmax);
-      q.alpha *= kFireFalpha;
-    }
+  const double vmax = cmax[2L * c], fmm = cmax[2L * c + 1];
+  if (q.phase == 1) {
+    // forces of the stepped-back positions are in: v = dt F / m estimates the
+    // step limit, then the move starts from v = 0
+    q.phase = 0;
+    q.plan = kFirePlanReset;
+    q.dtv = fire_limit(q.dt, q.dt * kFtm2v * fmm);
   } else {
-    q.mix1 = 0.0;
-    q.mix2 = 0.0;
-    q.npos = 0;
-    q.alpha = kFireAlpha0;
-    if (q.it >= kFireNmin) q.dt *= kFireFdec;
+    q.it++;
+    if (P > 0.0) {
+      q.nneg = 0;
+      q.mix1 = 1.0 - q.alpha;
+      q.mix2 = ff <= 1e-20 ? 0.0 : q.alpha * sqrt(vv / ff);
+      if (q.it - q.last_neg > kFireDelay) {
+        q.dt = fmin(q.dt * kFireGrow, q.dtmax);
+        q.alpha *= kFireAlphaShrink;
+      }
+      q.plan = kFirePlanMix;
+      q.dtv = fire_limit(q.dt, vmax);
+    } else {
+      q.last_neg = q.it;
+      if (q.it >= kFireDelay) {
+        q.alpha = kFireAlpha0;
+        if (q.dt * kFireShrink >= q.dtmin) q.dt *= kFireShrink;
+      }
+      if (++q.nneg > kFireMaxNeg) {
+        q.conv = 2;  // stuck in a basin (LAMMPS: "max iterations with v.f negative")
+        q.plan = kFirePlanNone;
+      } else if (vv > 0.0) {
+        q.plan = kFirePlanBack;
+        q.phase = 1;
+      } else {
+        // v is already zero: the step back moves nothing and the forces in
+        // hand are those of the current positions
+        q.plan = kFirePlanReset;
+        q.dtv = fire_limit(q.dt, q.dt * kFtm2v * fmm);
+      }
+    }
   }
   ctl[c] = q;
 }
@@ -216,30 +297,38 @@ __global__ void k_srv_initial(int n, const int *__restrict__ acell,
       v[3L * a + d] = vd;
       x[3L * a + d] = __dadd_rn(x[3L * a + d], __dmul_rn(q.dt, vd));
     }
-  } else if (fire_active(q)) {
-    const double dtfm = q.dt * kFtm2v / m;
+  } else if (q.mode == kJobFire && q.plan == kFirePlanBack) {
+    for (int d = 0; d < 3; d++) {
+      x[3L * a + d] -= 0.5 * q.dt * v[3L * a + d];
+      v[3L * a + d] = 0.0;
+    }
+  } else if (q.mode == kJobFire && (q.plan == kFirePlanMix || q.plan == kFirePlanReset)) {
+    const double dtfm = q.dtv * kFtm2v / m;
+    const bool mix = q.plan == kFirePlanMix;
     for (int d = 0; d < 3; d++) {
       const double fd = f[3L * a + d];
-      double vd = q.mix1 * v[3L * a + d] + q.mix2 * fd;
-      vd += dtfm * fd;
+      double vd = (mix ? v[3L * a + d] : 0.0) + dtfm * fd;
+      if (mix) vd = q.mix1 * vd + q.mix2 * fd;
       v[3L * a + d] = vd;
-      x[3L * a + d] += q.dt * vd;
+      x[3L * a + d] += q.dtv * vd;
     }
   }
 }
 
 void launch_srv_pre(int n, int ncells, const int *acell, const int *coff, CellCtl *ctl,
                     double *x, double *v, const double *f, const int *elem,
-                    const double *mass_e, double *pw, double *csum, cudaStream_t st,
-                    long &launches) {
+                    const double *mass_e, double *pw, double *pm, double *csum,
+                    double *cmax, cudaStream_t st, long &launches) {
   if (n <= 0) return;
   const int g = (n + kThreads - 1) / kThreads;
-  k_srv_power<<<g, kThreads, 0, st>>>(n, acell, ctl, v, f, pw);
+  k_srv_power<<<g, kThreads, 0, st>>>(n, acell, ctl, v, f, elem, mass_e, pw, pm);
   launch_cell_sum(ncells, coff, pw, 3, 1.0, csum, 4, st, launches);
+  const int gc = ncells < 148 * 16 ? ncells : 148 * 16;
+  k_cell_max2<<<gc, kThreads, 0, st>>>(ncells, coff, pm, cmax);
   k_srv_fire_update<<<(ncells + kThreads - 1) / kThreads, kThreads, 0, st>>>(ncells, ctl,
-                                                                             csum);
+                                                                             csum, cmax);
   k_srv_initial<<<g, kThreads, 0, st>>>(n, acell, ctl, x, v, f, elem, mass_e);
-  launches += 3;
+  launches += 4;
 }
 
 // NVE second half kick; |F|^2 per atom.
@@ -286,11 +375,12 @@ __global__ void k_srv_cell_end(int ncells, CellCtl *__restrict__ ctl,
   if (q.mode == kJobNve) {
     if (count && q.left > 0) q.left--;
   } else if (q.mode == kJobFire && !q.conv && q.left > 0) {
-    if (count) {
+    // an iteration ends with the force evaluation after its move (not after
+    // a step back); only then is convergence tested, as LAMMPS does
+    if (count && (q.plan == kFirePlanMix || q.plan == kFirePlanReset)) {
       q.left--;
-      q.it++;
+      if (cfmax[c] < q.fmax2) q.conv = 1;
     }
-    if (cfmax[c] <= q.fmax2) q.conv = 1;
   }
   ctl[c] = q;
 }

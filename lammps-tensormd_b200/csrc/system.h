@@ -47,6 +47,9 @@ struct tmd_system {
   cudaStream_t st = nullptr;
   long launches = 0;
   int natoms_cap = 0, n = 0;
+  // ghost-aware mode (tmd_system_set_atoms_ghost): the last nghost of the n
+  // atoms are LAMMPS ghosts, partners only (rows built, never evaluated)
+  int nghost = 0;
   double skin = 1.0;
   bool have_box = false, have_atoms = false, have_v = false;
   bool forces_valid = false;
@@ -92,6 +95,7 @@ struct tmd_system {
   // tmd_system_set_variant or tmd_system_autotune
   int force_variant = 0;
   int desc_variant = 0;    // kDesc*, the same way
+  long long wait_probe = 0;  // tmd_system_set_wait_probe (failure-detection tests)
   // kernel timing
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;

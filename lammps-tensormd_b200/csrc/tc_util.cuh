@@ -37,8 +37,9 @@ __device__ inline void commit(uint64_t *mbar) {
           smem_u32(mbar)));
 }
 
-// Bounded wait for the mbarrier phase; false on timeout.
-__device__ inline bool mbar_wait(uint64_t *mbar, uint32_t phase) {
+// Bounded wait for the mbarrier phase; false on timeout (after `limit`
+// clock cycles).
+__device__ inline bool mbar_wait(uint64_t *mbar, uint32_t phase, long long limit = kWaitCycles) {
   const uint32_t a = smem_u32(mbar);
   const long long t0 = clock64();
   while (true) {
@@ -50,7 +51,7 @@ __device__ inline bool mbar_wait(uint64_t *mbar, uint32_t phase) {
         : "r"(a), "r"(phase)
         : "memory");
     if (ok) return true;
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   }
 }
 
@@ -100,9 +101,11 @@ __device__ inline float act_fwd(int actfn, float z, float &d) {
       return z < 13.942385152878742f ? log1pf(ex) : z;
     }
     case 2: {
-      float y = tanhf(z);
-      d = 1.f - y * y;
-      return y;
+      // sech^2 z = 4 e / (1 + e)^2, e = exp(-2|z|): no 1 - tanh^2 cancellation
+      const float e = expf(-2.f * fabsf(z));
+      const float u = 1.f + e;
+      d = 4.f * e / (u * u);
+      return tanhf(z);
     }
     default: {
       float q = sqrtf(z * z + 4.f);
@@ -136,7 +139,8 @@ __device__ inline float act_fwd_fast(int actfn, float z, float &d) {
       const float t = __expf(-2.f * fminf(a, 40.f));
       const float y0 = a < 4e-3f ? a - a * a * a * (1.f / 3.f) : (1.f - t) * __frcp_rn(1.f + t);
       const float y = copysignf(y0, z);
-      d = 1.f - y * y;
+      const float u = 1.f + t;
+      d = 4.f * t * __frcp_rn(u * u);  // sech^2 z without 1 - tanh^2 cancellation
       return y;
     }
     default: {

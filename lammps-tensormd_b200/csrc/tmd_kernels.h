@@ -50,6 +50,11 @@ struct NbArgs {
   int *rev;
   double *xbuild;
   int *flag, *status, *maxneed;
+  // ghost-aware mode: atoms nlocal..n-1 are never evaluated; a build zeroes
+  // their pair forces and virial partials (read by the gather as partners)
+  int nlocal;
+  float4 *pdf;
+  double *wv;
   int *cflag;  // multi-cell mode: cells to rebuild (k_nbc_check), else nullptr
 };
 
@@ -71,7 +76,8 @@ void launch_nearest_image(int n, double *x, const double *xbuild, const BoxP &bo
 // of each pair computed once (k_descriptor_w).
 constexpr int kDescFilter4 = 0;
 constexpr int kDescWide = 1;
-constexpr int kDescVariants = 2;
+constexpr int kDescWide2 = 2;  // two pair streams per atom, 2+ filters per lane
+constexpr int kDescVariants = 3;
 struct DescArgs {
   int n, cap;
   KParams kp;
@@ -166,6 +172,11 @@ struct MlpTcArgs {
   int streamed;       // > 0: streamed-weight persistent form on this many CTAs
   size_t smem_s;      // its dynamic shared memory
   int stages;         // its weight-chunk stages
+  // > 0: failure-detection hook (tmd_system_set_wait_probe): every CTA first
+  // waits at most this many cycles on one of its mbarriers before issuing any
+  // MMA or copy; nothing arrives on it, so the kernel takes its timeout path
+  // with no asynchronous work in flight and reports kStatusTimeout
+  long long probe_wait;
 };
 void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches);
 size_t mlp_tc_smem(int nl, int maxh, int resnet, bool dz_bf16, int np);
@@ -258,21 +269,31 @@ void launch_scale_copy(const double *in, int n, double scale, double *out,
 // ---- serving: per-cell control of mixed jobs in one multi-cell system ----
 constexpr int kJobEnergy = 0;  // one force evaluation, atoms fixed
 constexpr int kJobNve = 1;     // velocity Verlet, `left` steps
-constexpr int kJobFire = 2;    // FIRE relaxation until max |F| <= fmax or `left` runs out
+constexpr int kJobFire = 2;    // FIRE relaxation until max |F| < fmax or `left` runs out
 
 struct CellCtl {
   int mode;      // kJob*
   int left;      // NVE steps / FIRE iterations still to run
-  int npos;      // FIRE: consecutive steps with P = F.v > 0
-  int conv;      // FIRE: converged (max |F|^2 <= fmax2)
-  int it;        // FIRE: iterations run
-  int pad;
+  int nneg;      // FIRE: iterations in a row with P = F.v <= 0
+  int conv;      // FIRE: converged (max |F|^2 < fmax2) or stopped
+  int it;        // FIRE: iterations begun
+  int phase;     // FIRE: 1 = stepped back, forces of the new positions pending
+  int last_neg;  // FIRE: last iteration with P <= 0
+  int plan;      // FIRE: move of the current step (kFirePlan*)
   double dt;     // NVE step; FIRE current step (ps)
-  double dtmax;  // FIRE
+  double dtmax, dtmin;  // FIRE step limits
   double alpha;  // FIRE mixing parameter
   double fmax2;  // FIRE convergence threshold, (eV/A)^2
   double mix1, mix2;  // FIRE velocity mixing of the current step
+  double dtv;    // FIRE step of the current move after the dmax limit
 };
+
+// FIRE moves of one step of a cell (server_kernels.cu)
+constexpr int kFirePlanNone = 0;
+constexpr int kFirePlanMix = 1;    // P > 0: Euler kick, mix, drift
+constexpr int kFirePlanBack = 2;   // P <= 0: half step back, v = 0 (forces re-evaluated)
+constexpr int kFirePlanReset = 3;  // after a reset: v = dt F / m, drift
+
 
 // New layout of a server batch: atom a of new cell c comes from old atom
 // src[c] + (a - coff[c]) when src[c] >= 0, else from staging slot
@@ -306,12 +327,14 @@ void launch_srv_perm(int ncells, int B, const int *coff, const int *elem, const 
 void launch_srv_mark(int ncells, const int *fresh, int *cflag, int *flag, cudaStream_t st,
                      long &launches);
 // One serving step, before the force evaluation: FIRE power (F.v, v.v, F.F)
-// summed per cell, FIRE state update, then the position update of NVE (half
-// kick + drift) and FIRE (mix + semi-implicit Euler) cells.
+// summed per cell and the largest velocity and force/mass components per
+// cell, the FIRE plan of each cell, then the position update of NVE (half
+// kick + drift) and FIRE (mix + Euler, or step back) cells.  pw: 3 doubles
+// per atom, pm: 2 per atom, csum: 4 per cell, cmax: 2 per cell.
 void launch_srv_pre(int n, int ncells, const int *acell, const int *coff, CellCtl *ctl,
                     double *x, double *v, const double *f, const int *elem,
-                    const double *mass_e, double *pw, double *csum, cudaStream_t st,
-                    long &launches);
+                    const double *mass_e, double *pw, double *pm, double *csum,
+                    double *cmax, cudaStream_t st, long &launches);
 // After the force evaluation: NVE second half kick (kick != 0), per-cell
 // max |F|^2, step bookkeeping (count != 0) and FIRE convergence.
 void launch_srv_post(int n, int ncells, const int *acell, const int *coff, CellCtl *ctl,

@@ -5,10 +5,24 @@
  * no arguments (:205-208); coeff() takes "* * file.npz El1 ... [keywords]"
  * (:214-317) and sets the per-type masses from the potential file (:303-312);
  * init_style() requires newton_pair on (:323-330); init_one() returns the
- * cutoff (:336-341); extract("scale") exposes the fix-adapt scale (:415-425).
- * compute() hands local positions and the box to the device, which builds its
- * own periodic neighbor list, and adds forces, energy and the virial (no
- * fdotr: the virial comes from the pair separations on the device).
+ * cutoff (:336-341); extract("scale") exposes the fix-adapt scale (:415-425),
+ * of which compute() uses scale[1][1] for every type, as the reference does
+ * (:168-170).  compute() runs in one of two modes:
+ *   one MPI rank   the local atoms and the periodic box go to the device,
+ *                  which builds its own periodic list (periodic images on the
+ *                  device, ghosts unused); forces on local atoms only;
+ *   several ranks  the ghost-aware mode: local and ghost atoms go to the
+ *                  device (tmd_system_set_atoms_ghost), which evaluates the
+ *                  local atoms over the same neighbor set as LAMMPS's full
+ *                  list and returns forces on local and ghost atoms, which
+ *                  LAMMPS's reverse communication sums (newton_pair on), as
+ *                  the reference does (kernel.cu:1760-1789).
+ * No LAMMPS neighbor list is requested: the device builds the list itself,
+ * and LAMMPS sets its neighbor and ghost cutoff to the pair cutoff + skin
+ * whether or not a list is requested (neighbor.cpp:337-376), so the ghost
+ * shell the device needs is always there; a full list would cost a host
+ * build at every reneighboring for nothing.  The virial comes from the pair
+ * separations on the device (no fdotr), energy and virial per rank.
  */
 #include "pair_tensormd_b200.h"
 
@@ -42,7 +56,9 @@ PairTensorMDB200::PairTensorMDB200(LAMMPS *lmp) : Pair(lmp)
   scale = nullptr;
   natoms_cap = 0;
   last_nlocal = -1;
+  last_nall = -1;
   last_box_stamp = -1;
+  ghost_mode = false;
 }
 
 PairTensorMDB200::~PairTensorMDB200()
@@ -121,9 +137,16 @@ void PairTensorMDB200::coeff(int narg, char **arg)
 void PairTensorMDB200::init_style()
 {
   if (force->newton_pair == 0) error->all(FLERR, "Pair style tensormd/b200 requires newton pair on");
-  if (comm->nprocs > 1)
-    error->all(FLERR, "Pair style tensormd/b200 runs on one MPI rank (periodic images on the GPU)");
   skin = neighbor->skin;
+  ghost_mode = comm->nprocs > 1;
+  last_nlocal = -1;
+  last_box_stamp = -1;
+  // one scale for all types, as PairTensorMD::compute (pair_tensormd.cpp:168-170)
+  const int n = atom->ntypes;
+  for (int i = 1; i <= n; i++)
+    for (int j = i; j <= n; j++)
+      if (setflag[i][j] && scale[i][j] != scale[1][1] && comm->me == 0)
+        error->warning(FLERR, "pair tensormd/b200 uses scale[1][1] for every type pair");
 }
 
 double PairTensorMDB200::init_one(int i, int j)
@@ -133,39 +156,60 @@ double PairTensorMDB200::init_one(int i, int j)
   return cutmax;
 }
 
-void PairTensorMDB200::compute(int eflag, int vflag)
+// Hand the current atoms to the device: the first call after LAMMPS
+// reneighbored (atoms migrated, re-sorted, ghosts rebuilt) uploads types and
+// order, the others positions only.
+void PairTensorMDB200::upload()
 {
-  ev_init(eflag, vflag);
-  const int n = atom->nlocal;
-  if (!sys || n > natoms_cap) {
+  const int nlocal = atom->nlocal;
+  const int nall = ghost_mode ? nlocal + atom->nghost : nlocal;
+  if (!sys || nall > natoms_cap) {
     if (sys) tmd_system_free(sys);
-    natoms_cap = n + n / 5 + 64;
+    natoms_cap = nall + nall / 5 + 64;
     check(tmd_system_create(model, natoms_cap, skin, &sys), "system");
     last_nlocal = -1;
     last_box_stamp = -1;
   }
-  double box[9] = {domain->boxlo[0], domain->boxlo[1], domain->boxlo[2],
-                   domain->xprd,     domain->yprd,     domain->zprd,
-                   domain->xy,       domain->xz,       domain->yz};
-  int pbc[3] = {domain->xperiodic, domain->yperiodic, domain->zperiodic};
-  bool box_changed = last_box_stamp < 0;
-  for (int c = 0; c < 9 && !box_changed; c++) box_changed = box[c] != last_box[c];
-  if (box_changed) {
-    check(tmd_system_set_box(sys, box, pbc), "box");
-    memcpy(last_box, box, sizeof(box));
-    last_box_stamp = 1;
-    last_nlocal = -1;
-  }
-  xbuf.assign(atom->x[0], atom->x[0] + 3 * (size_t)n);
-  // atoms migrate and LAMMPS re-sorts them on reneighboring steps: re-upload
-  // types and order then, positions only otherwise
-  if (n != last_nlocal || neighbor->ago == 0) {
-    tbuf.assign(atom->type, atom->type + n);
-    check(tmd_system_set_atoms(sys, n, xbuf.data(), tbuf.data(), nullptr), "atoms");
-    last_nlocal = n;
+  xbuf.assign(atom->x[0], atom->x[0] + 3 * (size_t)nall);
+  const bool reneighbored = nall != last_nall || nlocal != last_nlocal || neighbor->ago == 0;
+  if (ghost_mode) {
+    if (reneighbored) {
+      tbuf.assign(atom->type, atom->type + nall);
+      check(tmd_system_set_atoms_ghost(sys, nlocal, nall - nlocal, xbuf.data(), tbuf.data()),
+            "local and ghost atoms");
+    } else {
+      check(tmd_system_set_positions(sys, xbuf.data()), "positions");
+    }
   } else {
-    check(tmd_system_set_positions(sys, xbuf.data()), "positions");
+    double box[9] = {domain->boxlo[0], domain->boxlo[1], domain->boxlo[2],
+                     domain->xprd,     domain->yprd,     domain->zprd,
+                     domain->xy,       domain->xz,       domain->yz};
+    int pbc[3] = {domain->xperiodic, domain->yperiodic, domain->zperiodic};
+    bool box_changed = last_box_stamp < 0;
+    for (int c = 0; c < 9 && !box_changed; c++) box_changed = box[c] != last_box[c];
+    if (box_changed) {
+      check(tmd_system_set_box(sys, box, pbc), "box");
+      memcpy(last_box, box, sizeof(box));
+      last_box_stamp = 1;
+    }
+    if (reneighbored || box_changed) {
+      tbuf.assign(atom->type, atom->type + nlocal);
+      check(tmd_system_set_atoms(sys, nlocal, xbuf.data(), tbuf.data(), nullptr), "atoms");
+    } else {
+      check(tmd_system_set_positions(sys, xbuf.data()), "positions");
+    }
   }
+  last_nlocal = nlocal;
+  last_nall = nall;
+}
+
+void PairTensorMDB200::compute(int eflag, int vflag)
+{
+  ev_init(eflag, vflag);
+  upload();
+  // forces (and per-atom virials) on every atom the device holds: the local
+  // ones, and in the ghost-aware mode the ghosts for reverse communication
+  const int n = last_nall;
   fbuf.resize(3 * (size_t)n);
   double e = 0.0, v6[6] = {0, 0, 0, 0, 0, 0};
   double *ea = nullptr, *va = nullptr;
@@ -186,6 +230,19 @@ void PairTensorMDB200::compute(int eflag, int vflag)
   if (vflag_atom)
     for (int i = 0; i < n; i++)
       for (int c = 0; c < 6; c++) vatom[i][c] += vbuf[6 * i + c];
+}
+
+int PairTensorMDB200::descriptor_width()
+{
+  int nd = 0;
+  if (model) check(tmd_model_info(model, nullptr, nullptr, nullptr, &nd, nullptr, nullptr), "model info");
+  return nd;
+}
+
+void PairTensorMDB200::descriptors(double *G)
+{
+  upload();
+  check(tmd_get_descriptors(sys, G), "descriptors");
 }
 
 void *PairTensorMDB200::extract(const char *str, int &dim)

@@ -4,9 +4,11 @@
  *   pair_style tensormd/b200
  *   pair_coeff * * file.npz El1 El2 ... [interp dx] [cmax exact|default]
  *              [precision fp32|bf16|bf16x3]
- * The force evaluation runs in libtmd_b200.so (include/tmd_b200.h).  Periodic
- * images are handled on the device, so the style needs no LAMMPS neighbor list
- * and writes forces for local atoms only; it runs on one MPI rank.
+ * The force evaluation runs in libtmd_b200.so (include/tmd_b200.h), which
+ * builds its own neighbor list.  On one MPI rank the device handles the
+ * periodic images and the style writes forces on local atoms; on several
+ * ranks it hands local and ghost atoms over and writes forces on both, for
+ * LAMMPS's reverse communication.
  */
 #ifdef PAIR_CLASS
 // clang-format off
@@ -39,6 +41,11 @@ class PairTensorMDB200 : public Pair {
   void *extract(const char *, int &) override;
   double memory_usage() override;
 
+  // compute tensormd/density/b200: G rows of the local atoms at the current
+  // positions (G[nlocal][descriptor_width()])
+  int descriptor_width();
+  void descriptors(double *G);
+
  private:
   tmd_model *model;
   tmd_system *sys;
@@ -46,7 +53,8 @@ class PairTensorMDB200 : public Pair {
   double skin;
   double **scale;
   int natoms_cap;
-  int last_nlocal;
+  int last_nlocal, last_nall;
+  bool ghost_mode;
   int last_box_stamp;
   double last_box[9];
   std::vector<double> xbuf, fbuf, ebuf, vbuf;
@@ -54,6 +62,7 @@ class PairTensorMDB200 : public Pair {
 
   void allocate();
   void check(int rc, const char *what);
+  void upload();
 };
 
 }    // namespace LAMMPS_NS

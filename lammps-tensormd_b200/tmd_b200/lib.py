@@ -29,6 +29,7 @@ SIGNATURES = [
     ("tmd_system_set_box", _c_int, [_vp, _pd, _pi]),
     ("tmd_system_set_atoms", _c_int, [_vp, _c_int, _pd, _pi, _pd]),
     ("tmd_system_set_positions", _c_int, [_vp, _pd]),
+    ("tmd_system_set_atoms_ghost", _c_int, [_vp, _c_int, _c_int, _pd, _pi]),
     ("tmd_system_get", _c_int, [_vp, _pd, _pd, _pd, _pi]),
     ("tmd_compute", _c_int, [_vp, _c_int, _c_int, _c_double, _pd, _pd, _pd, _pd, _pd]),
     ("tmd_nve_run", _c_int, [_vp, _c_int, _c_double, _c_int, _pd]),
@@ -43,6 +44,7 @@ SIGNATURES = [
     ("tmd_system_stream", _c_int, [_vp, ctypes.POINTER(_vp)]),
     ("tmd_system_launches", _c_long, [_vp]),
     ("tmd_system_rebuilds", _c_int, [_vp, _pl]),
+    ("tmd_system_set_wait_probe", _c_int, [_vp, ctypes.c_longlong]),
     ("tmd_fp32_peak", _c_int, [_c_int, _c_int, _pd]),
     ("tmd_profile_enable", _c_int, [_vp, _c_int]),
     ("tmd_profile_read", _c_int, [_vp, _pl, _pd, _c_int]),

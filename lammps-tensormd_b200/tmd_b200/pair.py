@@ -96,11 +96,23 @@ class TensorMDSystem:
         t = np.ascontiguousarray(types, dtype=np.int32)
         vv = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         self.n = x.shape[0]
+        self.nlocal = self.n
         check(self.lib.tmd_system_set_atoms(self.h, self.n, _dp(x), _ip(t), _dp(vv)))
 
     def set_positions(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
         check(self.lib.tmd_system_set_positions(self.h, _dp(x)))
+
+    def set_atoms_ghost(self, nlocal, x, types):
+        """Ghost-aware mode (multi-rank LAMMPS): x[nall, 3] and types[nall]
+        hold the rank's local atoms first, then its ghosts; compute() then
+        returns forces for all nall atoms and the energy of the local ones."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        self.n = x.shape[0]
+        self.nlocal = int(nlocal)
+        check(self.lib.tmd_system_set_atoms_ghost(self.h, int(nlocal), self.n - int(nlocal),
+                                                  _dp(x), _ip(t)))
 
     def get(self):
         n = self.n
@@ -162,7 +174,7 @@ class TensorMDSystem:
         return off, ent[: tot.value]
 
     def descriptors(self):
-        G = np.zeros((self.n, self.model.n_desc))
+        G = np.zeros((getattr(self, "nlocal", self.n), self.model.n_desc))
         check(self.lib.tmd_get_descriptors(self.h, _dp(G)))
         return G
 
@@ -179,7 +191,7 @@ class TensorMDSystem:
         return self.FORCE_VARIANTS[v.value]
 
     # kernel forms of the descriptor (family 1)
-    DESC_VARIANTS = ("filter4", "wide")
+    DESC_VARIANTS = ("filter4", "wide", "wide2")
 
     def set_descriptor_variant(self, variant):
         v = self.DESC_VARIANTS.index(variant) if isinstance(variant, str) else int(variant)

@@ -278,6 +278,16 @@ class Oracle:
                                    ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double,
                                    ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+            L.tmdo_fire.restype = ctypes.c_int
+            L.tmdo_fire.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_int), ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                    ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double)]
             cls._lib = L
         return cls._lib
 
@@ -329,8 +339,12 @@ class Oracle:
         return off, ent[:tot]
 
     def compute(self, x, elem, box, pbc, nlist=None, skin=0.0, scale=1.0,
-                want_G=False, want_dEdG=False):
-        """Return dict(energy, eatom, f, virial, vatom[, G, dEdG])."""
+                want_G=False, want_dEdG=False, nlocal=None):
+        """Return dict(energy, eatom, f, virial, vatom[, G, dEdG]).
+
+        nlocal (ghost-aware evaluation, as a LAMMPS rank): only atoms
+        0..nlocal-1 are evaluated (their rows, energies); the others are
+        partners only and receive forces and per-atom virial halves."""
         L = self.lib()
         x = np.ascontiguousarray(x, dtype=np.float64)
         n = x.shape[0]
@@ -342,6 +356,10 @@ class Oracle:
         off, ent = nlist
         off = np.ascontiguousarray(off, dtype=np.int64)
         ent = np.ascontiguousarray(ent, dtype=np.int32)
+        if nlocal is not None and nlocal < n:
+            # ghosts keep no rows: the local rows are the first off[nlocal] entries
+            ent = np.ascontiguousarray(ent[:off[nlocal]])
+            off = np.concatenate([off[:nlocal + 1], np.full(n - nlocal, off[nlocal])])
         if ent.size == 0:
             ent = np.zeros((1, 4), dtype=np.int32)
         eatom = np.zeros(n)
@@ -356,6 +374,14 @@ class Oracle:
                            eatom.ctypes.data, f.ctypes.data, vir.ctypes.data,
                            vatom.ctypes.data, G.ctypes.data if G is not None else None,
                            dG.ctypes.data if dG is not None else None)
+        if nlocal is not None and nlocal < n:
+            # an atom without a row still has the energy of an isolated atom
+            e -= float(eatom[nlocal:].sum())
+            eatom[nlocal:] = 0.0
+            if G is not None:
+                G = G[:nlocal]
+            if dG is not None:
+                dG = dG[:nlocal]
         out = dict(energy=e, eatom=eatom, f=f, virial=vir, vatom=vatom)
         if G is not None:
             out["G"] = G
@@ -403,6 +429,25 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("oracle nvt failed")
         return x, v, f, th
+
+    def fire(self, x, elem, box, pbc, dt, ftol, maxiter, skin=1.0):
+        """min_style fire at LAMMPS's defaults (eulerimplicit, halfstepback),
+        stopped when max_i |F_i| < ftol or after maxiter iterations; returns
+        (x, f, energy, iterations)."""
+        L = self.lib()
+        x = np.array(x, dtype=np.float64, order="C")
+        n = x.shape[0]
+        el = np.ascontiguousarray(elem, dtype=np.int32)
+        bx = np.ascontiguousarray(box, dtype=np.float64)
+        pb = np.ascontiguousarray(pbc, dtype=np.int32)
+        ms = np.ascontiguousarray(self.masses, dtype=np.float64)
+        f = np.zeros((n, 3))
+        pe = np.zeros(1)
+        it = L.tmdo_fire(self.h, n, _p(x, ctypes.c_double), _p(el, ctypes.c_int),
+                         _p(ms, ctypes.c_double), _p(bx, ctypes.c_double),
+                         _p(pb, ctypes.c_int), dt, ftol, int(maxiter), skin,
+                         _p(f, ctypes.c_double), _p(pe, ctypes.c_double))
+        return x, f, float(pe[0]), int(it)
 
 
 if __name__ == "__main__":  # pragma: no cover

@@ -945,3 +945,124 @@ int tmdo_nvt(void *h, int n, double *x, double *v, const int *elem,
   free(ent);
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* min_style fire (FIRE 2.0 as LAMMPS runs it by default)              */
+/* ------------------------------------------------------------------ */
+
+/* Forces and energy at x: neighbor list at rmax + skin, then the force
+ * evaluation (a fresh list every call, as LAMMPS reneighbours). */
+static double om_eval(void *h, int n, const double *x, const int *elem, const double *boxv,
+                      const int *pbc, double skin, double *f)
+{
+  om_model *m = (om_model *)h;
+  double cut = m->rmax + skin;
+  int *cnt = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+  long *off = (long *)malloc(sizeof(long) * (n + 1));
+  long tot = tmdo_neighbors(n, x, boxv, pbc, cut, cnt, NULL, 0);
+  int *ent = (int *)malloc(sizeof(int) * 4 * (tot > 0 ? tot : 1));
+  tmdo_neighbors(n, x, boxv, pbc, cut, cnt, ent, tot);
+  off[0] = 0;
+  for (int i = 0; i < n; i++) off[i + 1] = off[i] + cnt[i];
+  double pe = tmdo_compute(h, n, x, elem, boxv, pbc, off, ent, 1.0, NULL, f, NULL, NULL,
+                           NULL, NULL);
+  free(cnt);
+  free(off);
+  free(ent);
+  return pe;
+}
+
+/* Energy minimisation with min_style fire at LAMMPS's defaults (min.cpp:63-72:
+ * dmax 0.1 A, delaystep 20, dtgrow 1.1, dtshrink 0.5, alpha0 0.25,
+ * alphashrink 0.99, tmax 10, tmin 0.02, integrator eulerimplicit,
+ * halfstepback yes, abcfire no), one iteration as MinFire::run_iterate
+ * (min_fire.cpp:149-619): P = v.f over the atoms; P > 0 mixes
+ * v <- (1 - a) v + a sqrt(v.v / f.f) f after the Euler kick and, more than
+ * delaystep iterations after the last P <= 0, grows dt (capped at tmax dt0)
+ * and shrinks a; P <= 0 (past the first delaystep iterations) resets a and
+ * halves dt (not below tmin dt0), steps x back by dt v / 2, zeroes v and
+ * re-evaluates the forces; then dt is limited so that no atom moves more than
+ * dmax along an axis, v += dt f / m (metal units), x += dt v, and the forces
+ * are evaluated.  Velocities start at zero (MinFire::setup_style).  The run
+ * stops after an iteration whose largest per-atom |F|^2 is below ftol^2
+ * (min_modify norm max) or after maxiter iterations.  x is
+ * remapped into the periodic box after each move.  Returns the iterations
+ * run; f receives the forces at the final x and *pe the energy. */
+int tmdo_fire(void *h, int n, double *x, const int *elem, const double *mass_e,
+              const double *boxv, const int *pbc, double dt0, double ftol, int maxiter,
+              double skin, double *f, double *pe)
+{
+  const double dmax = 0.1, dtgrow = 1.1, dtshrink = 0.5, alpha0 = 0.25, alphashrink = 0.99;
+  const int delaystep = 20;
+  const double dtmax = 10.0 * dt0, dtmin = 0.02 * dt0;
+  om_box b;
+  om_box_from(boxv, pbc, &b);
+  double *v = (double *)calloc(3 * (size_t)(n > 0 ? n : 1), sizeof(double));
+  double dt = dt0, alpha = alpha0;
+  int last_negative = 0, flagv0 = 1, iter = 0;
+  double e = om_eval(h, n, x, elem, boxv, pbc, skin, f);
+  for (iter = 1; iter <= maxiter; iter++) {
+    double vdotf = 0.0, scale1 = 0.0, scale2 = 0.0;
+    for (int i = 0; i < 3 * n; i++) vdotf += v[i] * f[i];
+    if (vdotf > 0.0) {
+      double vdotv = 0.0, fdotf = 0.0;
+      for (int i = 0; i < 3 * n; i++) {
+        vdotv += v[i] * v[i];
+        fdotf += f[i] * f[i];
+      }
+      scale1 = 1.0 - alpha;
+      scale2 = fdotf <= 1e-20 ? 0.0 : alpha * sqrt(vdotv / fdotf);
+      if (iter - last_negative > delaystep) {
+        dt = fmin(dt * dtgrow, dtmax);
+        alpha *= alphashrink;
+      }
+    } else {
+      last_negative = iter;
+      if (!(iter < delaystep)) {
+        alpha = alpha0;
+        if (dt * dtshrink >= dtmin) dt *= dtshrink;
+      }
+      for (int i = 0; i < 3 * n; i++) x[i] -= 0.5 * dt * v[i];
+      om_remap(&b, n, x);
+      for (int i = 0; i < 3 * n; i++) v[i] = 0.0;
+      flagv0 = 1;
+    }
+    if (flagv0) {
+      e = om_eval(h, n, x, elem, boxv, pbc, skin, f);
+      double dtf = dt * OM_FTM2V;
+      for (int i = 0; i < n; i++) {
+        double dtfm = dtf / mass_e[elem[i]];
+        for (int a = 0; a < 3; a++) v[3 * i + a] = dtfm * f[3 * i + a];
+      }
+    }
+    double dtv = dt;
+    for (int i = 0; i < n; i++) {
+      double vmax = fmax(fabs(v[3 * i]), fabs(v[3 * i + 1]));
+      vmax = fmax(vmax, fabs(v[3 * i + 2]));
+      if (dtv * vmax > dmax) dtv = dmax / vmax;
+    }
+    if (flagv0)
+      for (int i = 0; i < 3 * n; i++) v[i] = 0.0;
+    double dtf = dtv * OM_FTM2V;
+    for (int i = 0; i < n; i++) {
+      double dtfm = dtf / mass_e[elem[i]];
+      for (int a = 0; a < 3; a++) {
+        v[3 * i + a] += dtfm * f[3 * i + a];
+        if (vdotf > 0.0) v[3 * i + a] = scale1 * v[3 * i + a] + scale2 * f[3 * i + a];
+        x[3 * i + a] += dtv * v[3 * i + a];
+      }
+    }
+    om_remap(&b, n, x);
+    e = om_eval(h, n, x, elem, boxv, pbc, skin, f);
+    flagv0 = 0;
+    double fmax2 = 0.0;
+    for (int i = 0; i < n; i++) {
+      double s = f[3 * i] * f[3 * i] + f[3 * i + 1] * f[3 * i + 1] + f[3 * i + 2] * f[3 * i + 2];
+      if (s > fmax2) fmax2 = s;
+    }
+    if (fmax2 < ftol * ftol) break;
+  }
+  if (pe) *pe = e;
+  free(v);
+  return iter > maxiter ? maxiter : iter;
+}

@@ -6,7 +6,12 @@
                      virial to 1e-12 relative (sums in another order)
   NVE jobs           nsteps run; end state bitwise that of tmd_nve_run of the
                      same system (energy sums to 1e-12 relative)
-  FIRE jobs          end with every |F_i| <= fmax and a lower energy
+  FIRE jobs          LAMMPS min_style fire (its defaults) against the FP64
+                     oracle's restatement of min_fire.cpp: a 200-iteration
+                     trajectory on a random-weight potential (positions
+                     within 1e-4 A, energy 1e-6 eV/atom), and a relaxation on
+                     the trained MoNi potential to max |F_i| < 0.01 eV/A in
+                     the oracle's number of iterations
   concurrency        mixed jobs from several threads all complete; results
                      do not depend on what else was in flight
   mix independence   NVE and FIRE end states bitwise the same with other jobs
@@ -19,6 +24,8 @@ import time
 import numpy as np
 import pytest
 
+from pack import Oracle, load_npz
+from tmd_testutil import GOLDEN, frac_wrap, read_data
 from tmd_b200 import TensorMDModel, TensorMDServer, TensorMDSystem, TmdError, synth
 
 pytestmark = pytest.mark.gpu
@@ -29,7 +36,9 @@ def model4(tmp_path_factory):
     p = tmp_path_factory.mktemp("pot") / "serve.npz"
     syms = synth.gaussian_potential(p, seed=31, nelt=4, num_filters=16, rc=6.0,
                                     max_moment=3, hidden=(64, 64), actfn=2)
-    return TensorMDModel(f"{p} {' '.join(syms)}")
+    m = TensorMDModel(f"{p} {' '.join(syms)}")
+    m.npz_path = str(p)
+    return m
 
 
 def _separate(model, x, t, box, v=None):
@@ -177,26 +186,56 @@ def test_rows_grow_under_running_jobs(model4):
     assert o1["energy"] == o2["energy"]
 
 
-def test_fire_job_relaxes(model4):
-    rng = np.random.default_rng(3)
-    x, t, box, _ = synth.serving_job(rng, kind=2, nmin=100, nmax=200)
-    e0 = _separate(model4, x, t, box).compute(1, 1)["energy"]
-    srv = TensorMDServer(model4, max_atoms=100000, max_cells=64, steps_per_tick=16)
-    fmax = 0.05
-    tk = srv.submit(2, x, t, box, nsteps=3000, dt=0.001, fmax=fmax)
-    out = srv.wait(tk, timeout=300)
-    fnorm = np.linalg.norm(out["f"], axis=1).max()
-    assert out["steps"] < 3000, "FIRE did not converge"
-    assert fnorm <= fmax
+def test_fire_job_converges_as_the_oracle():
+    """FIRE on a trained potential (the reference's MoNi_m3, whose lattice is
+    a real minimum; the random-weight test potentials have none and collapse
+    under any minimiser): a perturbed 16-atom Mo8Ni8 cell relaxed to
+    max |F_i| < 0.01 eV/A in the server takes the oracle's number of
+    iterations and ends at its positions; the returned forces are those of
+    the returned positions."""
+    x, t, box = read_data(GOLDEN / "Mo8_Ni8_id3210.data")
+    x = frac_wrap(x, box) + np.random.default_rng(2).normal(0.0, 0.1, size=x.shape)
+    model = TensorMDModel(f"{GOLDEN}/MoNi_m3.npz Mo Ni interp 0.0001")
+    e0 = _separate(model, frac_wrap(x, box), t, box).compute(1, 1)["energy"]
+    srv = TensorMDServer(model, max_atoms=10000, max_cells=8, steps_per_tick=16)
+    fmax = 0.01
+    out = srv.wait(srv.submit(2, x, t, box, nsteps=1000, dt=0.001, fmax=fmax), timeout=300)
+    srv.close()
+    xo, fo, eo, it = Oracle(str(GOLDEN / "MoNi_m3.npz"), interp=1e-4).fire(
+        x, t - 1, box, [1, 1, 1], 0.001, fmax, 1000)
+    assert it < 1000 and out["steps"] == it
+    assert np.linalg.norm(out["f"], axis=1).max() < fmax
     assert out["energy"] < e0
-    # the returned state is consistent: forces of the returned positions.  A
-    # fresh system wraps atoms that crossed the box since the server's last
+    d = frac_wrap(out["x"], box) - frac_wrap(xo, box)
+    assert np.abs(d).max() < 1e-5, np.abs(d).max()
+    assert abs(out["energy"] - eo) / len(x) < 1e-6
+    # a fresh system wraps atoms that crossed the box since the server's last
     # rebuild, which reorders their list rows (and the FP32 sums) and moves
     # forces by ~1e-7 eV/A; forces of a neighbouring FIRE step would differ
-    # by ~1e-3
-    ref = _separate(model4, out["x"], t, box).compute(1, 1)
+    # by far more
+    ref = _separate(model, frac_wrap(out["x"], box), t, box).compute(1, 1)
     np.testing.assert_allclose(ref["f"], out["f"], rtol=0, atol=1e-6)
+
+
+def test_fire_trajectory_follows_the_oracle(model4):
+    """200 FIRE iterations of a 64-atom amorphous cell in the server against
+    the FP64 oracle's min_style fire (same defaults, same start, v = 0):
+    every P = F.v sign, step back and dt change must agree for the end
+    positions to agree."""
+    rng = np.random.default_rng(21)
+    x, box = synth.random_packing(64, rng)
+    t = rng.integers(1, 5, size=64).astype(np.int32)
+    srv = TensorMDServer(model4, max_atoms=10000, max_cells=8, steps_per_tick=16)
+    out = srv.wait(srv.submit(2, x, t, box, nsteps=200, dt=0.001, fmax=1e-9), timeout=300)
     srv.close()
+    o = Oracle(load_npz(model4.npz_path))
+    xo, fo, eo, it = o.fire(x, t - 1, box, [1, 1, 1], 0.001, 1e-9, 200)
+    assert out["steps"] == it == 200
+    L = box[3:6]
+    d = (out["x"] - xo) - np.round((out["x"] - xo) / L) * L
+    assert np.abs(d).max() < 1e-4, np.abs(d).max()
+    assert abs(out["energy"] - eo) / len(x) < 1e-6
+    assert eo < o.compute(x, t - 1, box, [1, 1, 1])["energy"]
 
 
 def test_concurrent_mixed_jobs(model4):

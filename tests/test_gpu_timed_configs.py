@@ -82,22 +82,35 @@ def test_bcc128k_1000_steps_checked_every_100():
 
 
 def test_alloy432k_every_form_against_the_oracle():
+    """The error table of the precision config: energy, force and virial of
+    every MLP form against one FP64 oracle evaluation on the same positions
+    (printed as one JSON line).  The FP8 form (e4m3, per-layer weight scale,
+    per-row activation scale) is reported, not held to the 1e-3 eV/A bar:
+    three mantissa bits in the first layer alone give a few percent error
+    in z on these random-weight potentials."""
+    import json
     p, syms, x, t, box, _ = _system("alloy432k")
     n = len(x)
     ref = Oracle(load_npz(p)).compute(x, t - 1, box, [1, 1, 1])
-    for prec in ("fp32", "bf16x3", "bf16"):
+    table = {"config": "alloy432k", "natoms": n,
+             "rms_force_eV_per_A": float(np.sqrt(np.mean(ref["f"] ** 2)))}
+    for prec in ("fp32", "bf16x3", "bf16", "fp8"):
         suffix = "" if prec == "fp32" else f" precision {prec}"
         m = TensorMDModel(f"{p} {' '.join(syms)}{suffix}")
         s = TensorMDSystem(m, n, 1.0)
         s.set_box(box)
         s.set_atoms(x, t)
         err = _errors(s.compute(1, 1), ref, n)
+        table[prec] = err
         if prec == "fp32":
             _assert_plain(err)
+        elif prec == "fp8":
+            assert np.isfinite(err["force_rms"]) and err["force_rms"] < 1.0, err
         else:
             assert err["force_rms"] <= BF16_FORCE_RMS, (prec, err)
         s.close()
         m.close()
+    print("errors_vs_fp64", json.dumps(table))
 
 
 def test_cells4096_sampled_cells_against_the_oracle(tmp_path):

@@ -15,7 +15,8 @@ LAMMPS_SRC = reference_tree() / "src"
 
 @pytest.mark.skipif(not (LAMMPS_SRC / "pair.h").exists() or shutil.which("g++") is None,
                     reason="LAMMPS headers not available")
-@pytest.mark.parametrize("src", ["pair_tensormd_b200.cpp", "tensormd_b200_plugin.cpp"])
+@pytest.mark.parametrize("src", ["pair_tensormd_b200.cpp", "tensormd_b200_plugin.cpp",
+                                 "compute_tensormd_density_b200.cpp"])
 def test_plugin_compiles_against_lammps_headers(src):
     plug = ROOT / "lammps-tensormd_b200" / "lammps"
     cmd = ["g++", "-std=c++17", "-fsyntax-only", "-DLAMMPS_SMALLBIG",

@@ -104,3 +104,24 @@ def test_table_tracks_analytic(tmp_path):
     table = Oracle(pot, interp=1e-4).compute(x, t - 1, box, [1, 1, 1])
     assert table["energy"] == pytest.approx(direct["energy"], rel=1e-8)
     assert np.abs(table["f"] - direct["f"]).max() < 1e-6 * max(1.0, np.abs(direct["f"]).max())
+
+
+def test_fire_restatement_relaxes_a_trained_cell():
+    """min_style fire (LAMMPS defaults) in the oracle relaxes a perturbed
+    Mo8Ni8 cell of the reference's trained MoNi potential to max |F_i| < 0.01
+    eV/A, lowering the energy; the returned forces are those of the returned
+    positions."""
+    from tmd_testutil import GOLDEN, frac_wrap, read_data
+    x, t, box = read_data(GOLDEN / "Mo8_Ni8_id3210.data")
+    x = frac_wrap(x, box) + np.random.default_rng(2).normal(0.0, 0.1, size=x.shape)
+    o = Oracle(str(GOLDEN / "MoNi_m3.npz"), interp=1e-4)
+    e0 = o.compute(frac_wrap(x, box), t - 1, box, [1, 1, 1])["energy"]
+    xo, fo, eo, it = o.fire(x, t - 1, box, [1, 1, 1], 0.001, 0.01, 1000)
+    assert it < 1000
+    assert np.linalg.norm(fo, axis=1).max() < 0.01
+    assert eo < e0
+    again = o.compute(xo, t - 1, box, [1, 1, 1])
+    assert np.abs(again["f"] - fo).max() < 1e-12
+    # capped run: exactly maxiter iterations when the tolerance is unreachable
+    _, _, _, it2 = o.fire(x, t - 1, box, [1, 1, 1], 0.001, 1e-12, 30)
+    assert it2 == 30
