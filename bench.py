@@ -54,7 +54,7 @@ def parse():
                          "kernel forms, run N force evaluations, print nothing else")
     ap.add_argument("--profile-precision", default="fp32", choices=["fp32", "bf16x3", "bf16"],
                     help="MLP precision form of the --profile-step target")
-    ap.add_argument("--profile-desc", default="", choices=["", "filter4", "wide", "wide2"],
+    ap.add_argument("--profile-desc", default="", choices=["", "filter4", "wide", "wide2", "split"],
                     help="descriptor form of the --profile-step target (default: the "
                          "library's default form)")
     ap.add_argument("--main-only", action="store_true",
@@ -64,6 +64,9 @@ def parse():
                     help="NVE steps of the 4,096-cell batch line (0 skips it)")
     ap.add_argument("--precision-steps", type=int, default=20,
                     help="NVE steps per MLP form of the 432,000-atom precision line (0 skips it)")
+    ap.add_argument("--decomp-steps", type=int, default=0,
+                    help="spatial decomposition line: NVE steps of the headline cell cut into "
+                         "one slab per rank (tmd_b200.decomp; 0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=2000.0,
                     help="serving line: Poisson arrival rate (jobs/s)")
     ap.add_argument("--serve-sweep", default="250,500,1000",
@@ -534,6 +537,12 @@ def run_ours_sampled(args, rank, world, local, clk):
             serving["fire_trained"] = run_fire_trained(rank, local)
         except Exception as exc:  # report, do not hide
             serving["fire_trained"] = {"error": str(exc)}
+    decomp = None
+    if args.decomp_steps > 0:
+        try:
+            decomp = run_decomp(args, rank, world, local, dev, barrier)
+        except Exception as exc:  # report, do not hide
+            decomp = {"error": str(exc)}
     w23k = None if args.main_only else run_w23k(args, rank, world, local, dev, barrier)
     alloy = None
     if args.precision_steps > 0 and not args.main_only:
@@ -572,6 +581,7 @@ def run_ours_sampled(args, rank, world, local, clk):
             "alloy432k": alloy,
             "serving": serving,
             "reference_workload_w23k": w23k,
+            "decomposition": decomp,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -724,6 +734,39 @@ def run_cells(args, rank, world, local, dev, barrier):
            "kernel_ms": {k: (cnt, t / max(cnt, 1)) for k, (cnt, t) in prof.items()},
            "config": {k: v for k, v in c.items() if k != "pot"} | {"potential": c["pot"]}}
     b.close()
+    model.close()
+    return out
+
+
+def run_decomp(args, rank, world, local, dev, barrier):
+    """One cell over all ranks: the headline workload cut into one slab per
+    rank along x (tmd_b200.decomp.SlabDecomposition over each rank's
+    ghost-aware device system; ghosts by all-gather, ghost forces home by
+    all-reduce, NCCL between GPUs), args.decomp_steps NVE steps with the
+    integrator on the host.  Strong scaling: the cell is fixed, the ranks
+    share it.  Host wall clock, max over ranks."""
+    from tmd_b200 import TensorMDModel, TensorMDSystem
+    from tmd_b200.decomp import SlabDecomposition
+    pot, syms, x, t, box, v, cfg = workload(args.config, seed=42)
+    model = TensorMDModel(f"{pot} {' '.join(syms)}", device=local)
+    n = len(x)
+    sysr = TensorMDSystem(model, int(3 * n / world) + 4096, 1.0)
+    dec = SlabDecomposition(box, model.cutmax + 1.0, 1.0, sysr, rank=rank, world=world,
+                            device=dev)
+    dec.set_atoms(x, t, v)
+    masses = np.asarray(model.type_mass, dtype=np.float64)
+    dec.nve_run(2, 0.001, masses)
+    barrier()
+    t0 = time.perf_counter()
+    dec.nve_run(args.decomp_steps, 0.001, masses)
+    wall = time.perf_counter() - t0
+    wall = max_over_ranks(wall, world, dev)
+    out = {"value": n * args.decomp_steps / wall, "unit": UNIT, "scaling": "strong",
+           "natoms": n, "ranks": world, "steps": args.decomp_steps,
+           "ms_per_step": 1000.0 * wall / args.decomp_steps,
+           "local_atoms_rank0": len(dec.x), "ghosts_rank0": dec.nghost,
+           "timing": "host wall clock (host integrator and exchange), max over ranks"}
+    sysr.close()
     model.close()
     return out
 

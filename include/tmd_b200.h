@@ -186,11 +186,14 @@ int tmd_get_descriptors(tmd_system *sys, double *G);
  *      the same kernel
  *   2  as 1, the atom's lanes split into two streams that take alternate
  *      pairs, 2K/min(K, 32) filters per lane (K = 4..64; other K run form 1)
+ *   3  split: the pair geometry of every list entry in a kernel of its own
+ *      (warp per atom, compact active pairs), then the contraction of form 1
+ *      over the compact pairs
  * The forms agree to FP32 rounding (summation order).  set_variant picks one;
  * autotune runs one evaluation, times reps launches of every form of the
  * family on the system's current atoms, keeps the fastest and recomputes the
  * results with it; ms (may be NULL) receives the mean device milliseconds per
- * launch of each form (4 force forms, 3 descriptor forms; at most
+ * launch of each form (4 force forms, 4 descriptor forms; at most
  * TMD_TUNE_VARIANTS). */
 #define TMD_TUNE_FORCE 0
 #define TMD_TUNE_DESCRIPTOR 1

@@ -25,7 +25,9 @@ void launch_descriptor(const DescArgs &a, cudaStream_t st, long &launches) {
       if (cells) launch_descriptor_generic_cells(a, st); else launch_descriptor_generic(a, st);
       break;
   }
-  if (a.variant != kDescFilter4) {
+  if (a.variant == kDescSplit) {
+    launches += 2;  // k_pair_geo + k_descriptor_c (G formed inside)
+  } else if (a.variant != kDescFilter4) {
     launches += 1;  // G formed inside k_descriptor_w
   } else {
     launch_invariants(a, st);

@@ -551,6 +551,220 @@ void launch_descriptor_w2(const DescArgs &a, cudaStream_t st) {
 #undef TMD_DESCW_ARGS
 }
 
+// ---------------------------------------------------------------------------
+// Split form: the pair geometry in a kernel of its own, the contraction in
+// another.  In the fused forms each lane computes the FP64 geometry of one
+// list entry at a time (a dependent chain: image, difference, squared
+// distance, square root, cutoff) and the atom's group waits on it before the
+// contraction can use the pair; at the registers the contraction needs, 16-24
+// warps per SM cannot hide that latency.  Here k_pair_geo runs with a warp
+// per atom and few registers (many warps per SM), tests every entry, and
+// writes the compact geometry of the active pairs block by block (the same
+// pgeo/pcnt the force kernel reads) and zero pair forces for the rest; the
+// contraction kernel then streams the compact pairs.
+
+// Warp per atom: entries of each element block in rounds of 32, active ones
+// compacted in row order (ballot + prefix count).
+template <int RK, bool MULTI>
+__global__ void __launch_bounds__(256)
+k_pair_geo(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
+           const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
+           const BoxP *__restrict__ cbox, const int *__restrict__ acell,
+           float4 *__restrict__ pdf, float4 *__restrict__ pgeo, int *__restrict__ pcnt) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int B = kp.B;
+  for (int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < n; a += nw) {
+    const BoxP &bx = box_of<MULTI>(box, cbox, acell, a);
+    const double xi = x[3 * a], yi = x[3 * a + 1], zi = x[3 * a + 2];
+    const uint32_t *row = nbr + (size_t)a * cap;
+    const int *bo = boff + (size_t)a * (B + 1);
+    float4 *pdf_row = pdf + (size_t)a * cap;
+    float4 *pg_row = pgeo + (size_t)a * cap * 2;
+    int nact = 0;
+    for (int b = 0; b < B; b++) {
+      const int s0 = bo[b], s1 = bo[b + 1];
+      int cnt = 0;
+      // positions of the next round's entries are loaded one round ahead
+      NbPos pn = load_nb(x, s0 + lane < s1 ? row[s0 + lane] : 0u, s0 + lane < s1);
+      for (int t0 = s0; t0 < s1; t0 += 32) {
+        const NbPos pc = pn;
+        const int tn = t0 + 32 + lane;
+        pn = load_nb(x, tn < s1 ? row[tn] : 0u, tn < s1);
+        PairGeo g;
+        pair_geometry(kp, bx, xi, yi, zi, pc, g);
+        const bool act = g.ti >= 0;
+        const unsigned bal = __ballot_sync(0xffffffffu, act);
+        const int t = t0 + lane;
+        if (act) {
+          const int c = nact + cnt + __popc(bal & ((1u << lane) - 1u));
+          float4 *dst = pg_row + 2 * c;
+          dst[0] = make_float4(g.r, g.rlo, g.ux, g.uy);
+          dst[1] = RK == kRadTable
+                       ? make_float4(g.uz, g.tq, __int_as_float(g.ti), __int_as_float(t))
+                       : make_float4(g.uz, g.fc, g.dfc, __int_as_float(t));
+        } else if (t < s1) {
+          pdf_row[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        cnt += __popc(bal);
+      }
+      if (lane == 0) pcnt[(size_t)a * B + b] = cnt;
+      nact += cnt;
+    }
+  }
+}
+
+// Contraction over the compact pairs: W = min(K, 32) lanes per atom, FPL =
+// K / W filters per lane.  Pairs come in chunks of W; lane c of the group
+// loads pair c's geometry (one chunk ahead), forms its D monomials and puts
+// them and the radial inputs in the group's shared-memory slots (two chunk
+// buffers, so one warp sync per chunk); every lane then accumulates its
+// filters over the chunk's pairs in row order, as k_descriptor_w.
+template <int W, int FPL, int D, int RK>
+__global__ void __launch_bounds__(kPairThreads, 8)
+k_descriptor_c(KParams kp, int n, int cap, float *__restrict__ P, float *__restrict__ G,
+               const float4 *__restrict__ pgeo, const int *__restrict__ pcnt) {
+  constexpr int D4 = (D + 3) / 4 * 4;
+  constexpr int M = D == 1 ? 1 : (D == 4 ? 2 : (D == 10 ? 3 : 4));
+  constexpr int P2 = D4 / 2;
+  constexpr int SL = D4 + 4;  // floats per slot: monomials, then (r, rlo, fc | tq, ti)
+  __shared__ __align__(16) float slots[2 * kPairThreads * SL];
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = gt / W;
+  const int sub = gt % W;
+  if (a >= n) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = PairRing<W>::kBits << (lane & ~(W - 1));
+  const unsigned live = live_lanes(gt, (long)n * W);
+  float *sg = slots + 2 * (threadIdx.x - sub) * SL;  // the group's 2 x W slots
+  const int B = kp.B, K = kp.K;
+  const int kf = sub * FPL;
+  Radial1<RK> R[FPL];
+#pragma unroll
+  for (int f = 0; f < FPL; f++) R[f] = load_radial1<RK>(kp, kf + f);
+  const float4 *pg_row = pgeo + (size_t)a * cap * 2;
+  int pos = 0, buf = 0;
+  for (int b = 0; b < B; b++) {
+    if (b > 0) __syncwarp(live);
+    const int np = pcnt[(size_t)a * B + b];
+    float2 acc[FPL][P2];
+#pragma unroll
+    for (int f = 0; f < FPL; f++)
+#pragma unroll
+      for (int p = 0; p < P2; p++) acc[f][p] = make_float2(0.f, 0.f);
+    float4 ga = make_float4(0.f, 0.f, 0.f, 0.f), gb = ga;
+    if (sub < np) {
+      ga = __ldg(pg_row + 2 * (pos + sub));
+      gb = __ldg(pg_row + 2 * (pos + sub) + 1);
+    }
+    for (int c0 = 0; c0 < np; c0 += W) {
+      const int cnt = min(W, np - c0);
+      float *slot = sg + (buf * W + sub) * SL;
+      if (sub < cnt) {
+        float Mv[D4];
+        moments<D>(ga.z, ga.w, gb.x, Mv);
+#pragma unroll
+        for (int d = D; d < D4; d++) Mv[d] = 0.f;
+#pragma unroll
+        for (int v = 0; v < D4 / 4; v++)
+          reinterpret_cast<float4 *>(slot)[v] =
+              make_float4(Mv[4 * v], Mv[4 * v + 1], Mv[4 * v + 2], Mv[4 * v + 3]);
+        // radial inputs: r, rlo, fc (analytic) or tq, interval (table)
+        reinterpret_cast<float4 *>(slot)[D4 / 4] =
+            RK == kRadTable ? make_float4(0.f, 0.f, gb.y, gb.z) : make_float4(ga.x, ga.y, gb.y, 0.f);
+      }
+      // next chunk's geometry in flight while this one is multiplied
+      const int cn = c0 + W + sub;
+      if (cn < np) {
+        ga = __ldg(pg_row + 2 * (pos + cn));
+        gb = __ldg(pg_row + 2 * (pos + cn) + 1);
+      }
+      __syncwarp(gmask);
+      const float *cs = sg + buf * W * SL;
+#pragma unroll 2
+      for (int c = 0; c < cnt; c++) {
+        const float4 *ms = reinterpret_cast<const float4 *>(cs + c * SL);
+        const float4 rr = ms[D4 / 4];
+        PairGeo g;
+        g.ux = g.uy = g.uz = g.dfc = g.rinv = 0.f;
+        if (RK == kRadTable) {
+          g.r = g.rlo = g.fc = 0.f;
+          g.tq = rr.z;
+          g.ti = __float_as_int(rr.w);
+        } else {
+          g.r = rr.x; g.rlo = rr.y; g.fc = rr.z; g.tq = 0.f; g.ti = 0;
+        }
+        float2 h2[FPL];
+#pragma unroll
+        for (int f = 0; f < FPL; f++) {
+          const float h = radial1<RK>(kp, R[f], g);
+          h2[f] = make_float2(h, h);
+        }
+#pragma unroll
+        for (int v = 0; v < D4 / 4; v++) {
+          const float4 m4 = ms[v];
+          const float2 lo = make_float2(m4.x, m4.y), hi = make_float2(m4.z, m4.w);
+#pragma unroll
+          for (int f = 0; f < FPL; f++) {
+            acc[f][2 * v] = __ffma2_rn(h2[f], lo, acc[f][2 * v]);
+            acc[f][2 * v + 1] = __ffma2_rn(h2[f], hi, acc[f][2 * v + 1]);
+          }
+        }
+      }
+      buf ^= 1;
+    }
+    pos += np;
+    float *Pp = P + (((size_t)a * B + b) * K + kf) * D;
+    float *Gp = G + (((size_t)a * B + b) * K + kf) * M;
+#pragma unroll
+    for (int f = 0; f < FPL; f++) {
+      if constexpr (D % 2 == 0) {
+        float2 *P2p = reinterpret_cast<float2 *>(Pp + f * D);
+#pragma unroll
+        for (int p = 0; p < D / 2; p++) P2p[p] = acc[f][p];
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; d++) Pp[f * D + d] = (d & 1) ? acc[f][d >> 1].y : acc[f][d >> 1].x;
+      }
+#pragma unroll
+      for (int m = 0; m < M; m++) {
+        float sacc = 0.f;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          const float pv = (d & 1) ? acc[f][d >> 1].y : acc[f][d >> 1].x;
+          sacc = fmaf(kp.T[m * D + d], pv * pv, sacc);
+        }
+        if (m == 0) sacc = copysignf(1.f, acc[f][0].x) * sqrtf(sacc);
+        Gp[f * M + m] = sacc;
+      }
+    }
+  }
+}
+
+template <int W, int FPL, int RK, bool MULTI>
+void launch_descriptor_split(const DescArgs &a, cudaStream_t st) {
+  {
+    const int T = 256;
+    long g = ((long)a.n * 32 + T - 1) / T;
+    if (g > 148 * 16) g = 148 * 16;
+    if (g < 1) g = 1;
+    k_pair_geo<RK, MULTI><<<(int)g, T, 0, st>>>(a.kp, a.box, a.n, a.cap, a.x, a.nbr, a.boff,
+                                               a.cbox, a.acell, a.pdf, a.pgeo, a.pcnt);
+  }
+  const int T = kPairThreads;
+  const long threads = (long)a.n * W;
+  int grid = (int)((threads + T - 1) / T);
+  if (grid < 1) grid = 1;
+#define TMD_DESCC_ARGS a.kp, a.n, a.cap, a.P, a.G, a.pgeo, a.pcnt
+  switch (a.kp.D) {
+    case 1: k_descriptor_c<W, FPL, 1, RK><<<grid, T, 0, st>>>(TMD_DESCC_ARGS); break;
+    case 4: k_descriptor_c<W, FPL, 4, RK><<<grid, T, 0, st>>>(TMD_DESCC_ARGS); break;
+    case 10: k_descriptor_c<W, FPL, 10, RK><<<grid, T, 0, st>>>(TMD_DESCC_ARGS); break;
+    default: k_descriptor_c<W, FPL, 20, RK><<<grid, T, 0, st>>>(TMD_DESCC_ARGS); break;
+  }
+#undef TMD_DESCC_ARGS
+}
+
 template <int W, int FPL, int RK, bool MULTI>
 void launch_descriptor_w(const DescArgs &a, cudaStream_t st) {
   const int T = kPairThreads;
@@ -624,6 +838,17 @@ void launch_descriptor_tpa(const DescArgs &a, cudaStream_t st) {
 // own translation unit so the variants compile in parallel.
 template <int RK, bool MULTI>
 void launch_descriptor_rk(const DescArgs &a, cudaStream_t st) {
+  if (a.variant == kDescSplit) {
+    switch (a.kp.K) {
+      case 4: launch_descriptor_split<4, 1, RK, MULTI>(a, st); break;
+      case 8: launch_descriptor_split<8, 1, RK, MULTI>(a, st); break;
+      case 16: launch_descriptor_split<16, 1, RK, MULTI>(a, st); break;
+      case 32: launch_descriptor_split<32, 1, RK, MULTI>(a, st); break;
+      case 64: launch_descriptor_split<32, 2, RK, MULTI>(a, st); break;
+      default: launch_descriptor_split<32, 4, RK, MULTI>(a, st); break;
+    }
+    return;
+  }
   if (a.variant == kDescWide2 && a.kp.K >= 4 && a.kp.K <= 64) {
     switch (a.kp.K) {
       case 4: launch_descriptor_w2<4, 2, RK, MULTI>(a, st); return;

@@ -77,7 +77,8 @@ void launch_nearest_image(int n, double *x, const double *xbuild, const BoxP &bo
 constexpr int kDescFilter4 = 0;
 constexpr int kDescWide = 1;
 constexpr int kDescWide2 = 2;  // two pair streams per atom, 2+ filters per lane
-constexpr int kDescVariants = 3;
+constexpr int kDescSplit = 3;  // geometry kernel + contraction kernel
+constexpr int kDescVariants = 4;
 struct DescArgs {
   int n, cap;
   KParams kp;

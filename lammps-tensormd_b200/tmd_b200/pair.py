@@ -191,7 +191,7 @@ class TensorMDSystem:
         return self.FORCE_VARIANTS[v.value]
 
     # kernel forms of the descriptor (family 1)
-    DESC_VARIANTS = ("filter4", "wide", "wide2")
+    DESC_VARIANTS = ("filter4", "wide", "wide2", "split")
 
     def set_descriptor_variant(self, variant):
         v = self.DESC_VARIANTS.index(variant) if isinstance(variant, str) else int(variant)

@@ -10,7 +10,8 @@ LAMMPS's reverse communication does with newton_pair on).  The result must
 equal the single periodic system's:
   forces        relative RMS <= 1e-6 (same pairs; rows, and with them the
                 FP32 summation order, differ)
-  energy        sum of the ranks' energies, 1e-9 relative
+  energy        sum of the ranks' energies, |dE|/N <= 1e-8 eV/atom (the
+                FP32 per-atom energies round differently with the row order)
   virial        sum of the ranks' virials, 1e-6 relative
   eatom/vatom   per atom after the reverse sum (ghost eatom is 0)
   descriptors   the local atoms' G rows (compute tensormd/density), 1e-5
@@ -102,7 +103,7 @@ def test_two_slab_ranks_equal_the_periodic_cell(cell):
         assert rel_rms(again["f"], out["f"]) <= 1e-12
         r.close()
     assert rel_rms(f, ref["f"]) <= 1e-6, rel_rms(f, ref["f"])
-    assert energy == pytest.approx(ref["energy"], rel=1e-9)
+    assert abs(energy - ref["energy"]) / n <= 1e-8
     assert np.linalg.norm(virial - ref["virial"]) <= 1e-6 * np.linalg.norm(ref["virial"])
     assert np.abs(eatom - ref["eatom"]).max() < 1e-6
     assert rel_rms(vatom, ref["vatom"]) <= 1e-5
@@ -145,7 +146,7 @@ def test_slab_decomposition_on_the_device(cell):
     f, e, vir = dec.compute()
     xg, vg, fg = dec.gather()
     assert rel_rms(fg, ref["f"]) <= 1e-6
-    assert e == pytest.approx(ref["energy"], rel=1e-9)
+    assert abs(e - ref["energy"]) / n <= 1e-8
     assert np.linalg.norm(vir - ref["virial"]) <= 1e-6 * np.linalg.norm(ref["virial"])
     dec.nve_run(10, 0.001, masses)
     s.nve_run(10, 0.001)

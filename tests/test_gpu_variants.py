@@ -7,7 +7,8 @@ Every combination of forms must meet the plain-form tolerances against the FP64 
 table, the generic analytic forms), every monomial count (D = 1, 4, 10, 20),
 more than one element and in multi-cell batches.  The forms sum in different
 orders, so between forms the forces agree to FP32 rounding (relative RMS
-1e-6), and each form is bitwise deterministic run to run."""
+5e-6 on the benchmark shape, where the two-stream descriptor adds its pairs
+as two partial sums), and each form is bitwise deterministic run to run."""
 import numpy as np
 import pytest
 
@@ -90,7 +91,8 @@ def test_forms_on_benchmark_shape(fcc4k):
     first = outs[(DFORMS[0], FORMS[0])]
     for v, out in outs.items():
         _check(out, ref, len(x), 1e-7)
-        assert rel_rms(out["f"], first["f"]) <= 1e-6, v
+        # the forms sum in different orders (pairs, filters, two pair streams)
+        assert rel_rms(out["f"], first["f"]) <= 5e-6, v
 
 
 def test_descriptor_forms_agree(fcc4k):
