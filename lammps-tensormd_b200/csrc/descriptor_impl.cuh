@@ -207,7 +207,7 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
              const int *__restrict__ acell, float4 *__restrict__ pdf,
              float4 *__restrict__ pgeo, int *__restrict__ pcnt) {
   constexpr int D2 = (D + 1) / 2;
-  __shared__ GeoSlot geo[2 * kPairThreads];
+  __shared__ GeoSlot geo[2 * kPairThreads + kPairThreads];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gt / TPA;
   const int sub = gt % TPA;
@@ -217,7 +217,9 @@ k_descriptor(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
   pr.sub = sub;
   pr.gshift = lane & ~(TPA - 1);
   pr.gmask = PairRing<TPA>::kBits << pr.gshift;
-  pr.ring = geo + 2 * (threadIdx.x - sub);  // the ring of this atom's group
+  // the ring of this atom's group; one spare slot per group puts the groups
+  // of a warp in different banks (their reads of slot c do not conflict)
+  pr.ring = geo + 2 * (threadIdx.x - sub) + threadIdx.x / TPA;
   const int B = kp.B, K = kp.K;
   const int k0 = 4 * sub;
   const Radial4<RK> R = load_radial4<RK>(kp, k0);
@@ -298,8 +300,8 @@ k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ 
   constexpr int D4 = (D + 3) / 4 * 4;
   constexpr int M = D == 1 ? 1 : (D == 4 ? 2 : (D == 10 ? 3 : 4));
   constexpr int P2 = D4 / 2;
-  __shared__ GeoSlot geo[2 * kPairThreads];
-  __shared__ __align__(16) float mono[2 * kPairThreads * D4];
+  __shared__ GeoSlot geo[2 * kPairThreads + kPairThreads / 4];
+  __shared__ __align__(16) float mono[2 * kPairThreads * D4 + kPairThreads];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gt / W;
   const int sub = gt % W;
@@ -309,8 +311,10 @@ k_descriptor_w(KParams kp, BoxP box, int n, int cap, const double *__restrict__ 
   pr.sub = sub;
   pr.gshift = lane & ~(W - 1);
   pr.gmask = PairRing<W>::kBits << pr.gshift;
-  pr.ring = geo + 2 * (threadIdx.x - sub);
-  float *mr = mono + 2 * (threadIdx.x - sub) * D4;  // monomials of the group's slots
+  // the group's ring and monomial slots, each group offset by one spare slot
+  // (12 words) and 4 words so that the groups of a warp read different banks
+  pr.ring = geo + 2 * (threadIdx.x - sub) + threadIdx.x / W;
+  float *mr = mono + 2 * (threadIdx.x - sub) * D4 + 4 * (threadIdx.x / W);
   const int B = kp.B, K = kp.K;
   const int kf = sub * FPL;
   Radial1<RK> R[FPL];
@@ -422,8 +426,8 @@ k_descriptor_w2(KParams kp, BoxP box, int n, int cap, const double *__restrict__
   constexpr int D4 = (D + 3) / 4 * 4;
   constexpr int M = D == 1 ? 1 : (D == 4 ? 2 : (D == 10 ? 3 : 4));
   constexpr int P2 = D4 / 2;
-  __shared__ GeoSlot geo[2 * kPairThreads];
-  __shared__ __align__(16) float mono[2 * kPairThreads * D4];
+  __shared__ GeoSlot geo[2 * kPairThreads + kPairThreads / 4];
+  __shared__ __align__(16) float mono[2 * kPairThreads * D4 + kPairThreads];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gt / W;
   const int sub = gt % W;
@@ -434,8 +438,10 @@ k_descriptor_w2(KParams kp, BoxP box, int n, int cap, const double *__restrict__
   pr.sub = sub;
   pr.gshift = lane & ~(W - 1);
   pr.gmask = PairRing<W>::kBits << pr.gshift;
-  pr.ring = geo + 2 * (threadIdx.x - sub);
-  float *mr = mono + 2 * (threadIdx.x - sub) * D4;  // monomials of the group's slots
+  // the group's ring and monomial slots, each group offset by one spare slot
+  // (12 words) and 4 words so that the groups of a warp read different banks
+  pr.ring = geo + 2 * (threadIdx.x - sub) + threadIdx.x / W;
+  float *mr = mono + 2 * (threadIdx.x - sub) * D4 + 4 * (threadIdx.x / W);
   const int B = kp.B, K = kp.K;
   const int kf = fl * FPL;
   Radial1<RK> R[FPL];
@@ -566,7 +572,7 @@ void launch_descriptor_w2(const DescArgs &a, cudaStream_t st) {
 // Warp per atom: entries of each element block in rounds of 32, active ones
 // compacted in row order (ballot + prefix count).
 template <int RK, bool MULTI>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 6)
 k_pair_geo(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
            const uint32_t *__restrict__ nbr, const int *__restrict__ boff,
            const BoxP *__restrict__ cbox, const int *__restrict__ acell,
@@ -585,12 +591,15 @@ k_pair_geo(KParams kp, BoxP box, int n, int cap, const double *__restrict__ x,
     for (int b = 0; b < B; b++) {
       const int s0 = bo[b], s1 = bo[b + 1];
       int cnt = 0;
-      // positions of the next round's entries are loaded one round ahead
+      // entries are loaded two rounds ahead and their positions one round
+      // ahead, so the dependent gather (entry, then position) overlaps work
       NbPos pn = load_nb(x, s0 + lane < s1 ? row[s0 + lane] : 0u, s0 + lane < s1);
+      uint32_t en = s0 + 32 + lane < s1 ? row[s0 + 32 + lane] : 0u;
       for (int t0 = s0; t0 < s1; t0 += 32) {
         const NbPos pc = pn;
         const int tn = t0 + 32 + lane;
-        pn = load_nb(x, tn < s1 ? row[tn] : 0u, tn < s1);
+        pn = load_nb(x, en, tn < s1);
+        en = tn + 32 < s1 ? row[tn + 32] : 0u;
         PairGeo g;
         pair_geometry(kp, bx, xi, yi, zi, pc, g);
         const bool act = g.ti >= 0;
@@ -628,7 +637,7 @@ k_descriptor_c(KParams kp, int n, int cap, float *__restrict__ P, float *__restr
   constexpr int M = D == 1 ? 1 : (D == 4 ? 2 : (D == 10 ? 3 : 4));
   constexpr int P2 = D4 / 2;
   constexpr int SL = D4 + 4;  // floats per slot: monomials, then (r, rlo, fc | tq, ti)
-  __shared__ __align__(16) float slots[2 * kPairThreads * SL];
+  __shared__ __align__(16) float slots[2 * kPairThreads * SL + kPairThreads];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gt / W;
   const int sub = gt % W;
@@ -636,7 +645,9 @@ k_descriptor_c(KParams kp, int n, int cap, float *__restrict__ P, float *__restr
   const int lane = threadIdx.x & 31;
   const unsigned gmask = PairRing<W>::kBits << (lane & ~(W - 1));
   const unsigned live = live_lanes(gt, (long)n * W);
-  float *sg = slots + 2 * (threadIdx.x - sub) * SL;  // the group's 2 x W slots
+  // the group's 2 x W slots, groups offset by 4 words: the groups of a warp
+  // read slot c from different banks
+  float *sg = slots + 2 * (threadIdx.x - sub) * SL + 4 * (threadIdx.x / W);
   const int B = kp.B, K = kp.K;
   const int kf = sub * FPL;
   Radial1<RK> R[FPL];
