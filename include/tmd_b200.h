@@ -213,6 +213,16 @@ long tmd_system_launches(const tmd_system *sys);
  * runs: LAMMPS's "Neighbor list builds" count).  Waits for the stream. */
 int tmd_system_rebuilds(tmd_system *sys, long *count);
 
+/* Temperature-dependent potentials (tdnp = 1 files, TDNP in tdnp.cpp): the
+ * electron temperature in eV (pair_coeff keyword etemp gives it in K, as
+ * pair_tensormd.cpp:245-246; fix tensormd/etemp sets pair->etemp between
+ * steps, fix_tensormd_etemp.cpp:80-89).  With such a potential tmd_compute's
+ * energy is the internal energy U and its forces those of the free energy
+ * A = U - T S (tdnp.cpp:167-226); tmd_system_tdnp_energies returns S and A
+ * of the last compute (PairTensorMD::eentropy, free_energy), times scale. */
+int tmd_system_set_etemp(tmd_system *sys, double etemp_ev);
+int tmd_system_tdnp_energies(tmd_system *sys, double *entropy, double *free_energy);
+
 /* Failure-detection hook for tests (no reference counterpart).  With
  * cycles > 0 the system's tensor-core MLP kernels (precision bf16, bf16x3,
  * fp8) start every CTA with a wait of at most `cycles` clock cycles on one

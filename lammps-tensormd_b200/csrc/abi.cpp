@@ -327,7 +327,21 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   ma.ntiles = s->ntiles; ma.tiles = s->tiles; ma.perm = s->perm; ma.G = s->G;
   ma.dEdG = s->dEdG; ma.E = s->E; ma.layers = m->d_layers;
   prof_begin(s);
-  if (m->d_tc_layers) {
+  if (m->h.tdnp) {
+    TdnpArgs td{};
+    td.n = s->n - s->nghost; td.nin = m->h.nin; td.ydim = m->h.ydim; td.maxw = m->tdnp_maxw;
+    td.nelt = m->h.nelt;
+    td.nl[0] = m->h.tH.nl; td.nl[1] = m->h.tU.nl; td.nl[2] = m->h.tS.nl;
+    td.actfn[0] = m->h.tH.actfn; td.actfn[1] = m->h.tU.actfn; td.actfn[2] = m->h.tS.actfn;
+    td.resnet[0] = m->h.tH.resnet; td.resnet[1] = m->h.tU.resnet; td.resnet[2] = m->h.tS.resnet;
+    td.layers = m->d_tdnp; td.elem = s->elem; td.G = s->G; td.dEdG = s->dEdG;
+    td.E = s->E; td.Sa = s->tdnp_s; td.Aa = s->tdnp_a;
+    td.T = (float)s->etemp;
+    td.c = (float)(m->h.sommerfeld ? s->etemp * s->etemp : s->etemp);
+    td.sommerfeld = m->h.sommerfeld;
+    td.warp_floats = m->tdnp_warp_floats;
+    launch_mlp_tdnp(td, s->st, s->launches);
+  } else if (m->d_tc_layers) {
     MlpTcArgs ta{};
     ta.nl = m->h.nl; ta.actfn = m->h.actfn; ta.resnet = m->h.resnet; ta.nin = m->h.nin;
     ta.maxh = m->maxh; ta.ntiles = s->ntiles; ta.tiles = s->tiles; ta.perm = s->perm;
@@ -704,6 +718,66 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     tmd_model_free(m);
     return fail(TMD_ERR_CUDA, std::string("model upload: ") + cudaGetErrorString(e));
   }
+  if (h.tdnp) {
+    // the H, U, S nets replace the MLP (k_mlp_tdnp); their layers as
+    // [net][element][kMaxLayers], W and W^T in FP32, output row sums of U
+    // and S in FP32 and FP64
+    const HostModel::Net *nets[3] = {&h.tH, &h.tU, &h.tS};
+    std::vector<TdnpLayer> tl((size_t)3 * h.nelt * kMaxLayers);
+    int maxw = std::max(h.nin, h.ydim);
+    for (int q = 0; q < 3 && e == cudaSuccess; q++)
+      for (int el = 0; el < h.nelt && e == cudaSuccess; el++)
+        for (int l = 0; l < nets[q]->nl && e == cudaSuccess; l++) {
+          const HostModel::Net &t = *nets[q];
+          TdnpLayer &L = tl[((size_t)q * h.nelt + el) * kMaxLayers + l];
+          L.K = t.sizes[l];
+          L.N = t.sizes[l + 1];
+          maxw = std::max(maxw, std::max(L.K, L.N));
+          const std::vector<double> &W = t.W[el][l];
+          std::vector<float> wf(W.begin(), W.end()), wt((size_t)L.K * L.N);
+          for (int k = 0; k < L.K; k++)
+            for (int n = 0; n < L.N; n++) wt[(size_t)n * L.K + k] = (float)W[(size_t)k * L.N + n];
+          float *dw = nullptr, *dwt = nullptr, *db = nullptr, *dwf = nullptr;
+          double *dwd = nullptr;
+          e = up(wf, &dw);
+          if (e == cudaSuccess) e = up(wt, &dwt);
+          if (e == cudaSuccess && !t.B[el][l].empty()) {
+            std::vector<float> bf(t.B[el][l].begin(), t.B[el][l].end());
+            e = up(bf, &db);
+          }
+          L.W = dw; L.WT = dwt; L.b = db; L.Wf = nullptr; L.Wd = nullptr; L.bd = 0.0;
+          if (q > 0 && l == t.nl - 1 && e == cudaSuccess) {
+            std::vector<double> rs(L.K, 0.0);
+            std::vector<float> rf(L.K, 0.f);
+            for (int k = 0; k < L.K; k++)
+              for (int n = 0; n < L.N; n++) {
+                rs[k] += W[(size_t)k * L.N + n];
+                rf[k] += (float)W[(size_t)k * L.N + n];
+              }
+            e = upd(rs, &dwd);
+            if (e == cudaSuccess) e = up(rf, &dwf);
+            for (double b : t.B[el][l]) L.bd += b;
+            L.Wf = dwf; L.Wd = dwd;
+          }
+        }
+    if (e == cudaSuccess) e = dalloc(&m->d_tdnp, tl.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(m->d_tdnp, tl.data(), tl.size() * sizeof(TdnpLayer), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      tmd_model_free(m);
+      return fail(TMD_ERR_CUDA, std::string("TDNP upload: ") + cudaGetErrorString(e));
+    }
+    const int nl[3] = {h.tH.nl, h.tU.nl, h.tS.nl};
+    m->tdnp_maxw = (maxw + 3) / 4 * 4;
+    m->tdnp_warp_floats = tdnp_warp_floats(nl, m->tdnp_maxw);
+    if (m->tdnp_warp_floats * sizeof(float) * 4 > 227 * 1024) {
+      tmd_model_free(m);
+      return fail(TMD_ERR_MODEL, "TDNP nets too wide for the shared-memory work space");
+    }
+    m->mlp_tr = 64;  // element grouping only (the TDNP kernel takes atoms directly)
+    *out = m;
+    return TMD_OK;
+  }
   // MLP: the resident-weight form (one persistent CTA per SM) when the
   // element's hidden weights and a tile's activations fit in shared memory
   // (128-atom tiles, else 64); else the persistent streamed-weight form
@@ -894,6 +968,7 @@ void tmd_model_free(tmd_model *m) {
   for (float *p : m->d_buf) cudaFree(p);
   if (m->d_layers) cudaFree(m->d_layers);
   if (m->d_tc_layers) cudaFree(m->d_tc_layers);
+  if (m->d_tdnp) cudaFree(m->d_tdnp);
   if (m->d_mass) cudaFree(m->d_mass);
   delete m;
 }
@@ -932,6 +1007,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   s->skin = skin;
   s->force_variant = default_force_variant(m);
   s->desc_variant = default_desc_variant(m);
+  s->etemp = m->h.etemp;
   const HostModel &h = m->h;
   size_t N = natoms_cap;
   cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
@@ -942,6 +1018,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   A(nraw, N); A(boff, N * (h.nelt + 1)); A(pcnt, N * h.nelt);
   A(P, N * h.nelt * h.K * h.D); A(G, N * h.nin); A(dEdG, N * h.nin); A(E, N);
   A(wv, 6 * N); A(eatom, N); A(vatom, 6 * N); A(ke, N);
+  if (h.tdnp) { A(tdnp_s, N); A(tdnp_a, N); A(tdnp_tot, 2); }
   A(partial, 1024 * 8); A(scal, 8);
   A(flag, 2); A(status, 2);  // flag[0] rebuild pending, flag[1] rebuilds done
   A(perm, N); A(tiles, 3 * (N / 32 + h.nelt + 1));
@@ -972,6 +1049,7 @@ void tmd_system_free(tmd_system *s) {
   dfree(s->pgeo); dfree(s->pcnt);
   dfree(s->wv); dfree(s->eatom); dfree(s->vatom); dfree(s->ke); dfree(s->partial);
   dfree(s->scal); dfree(s->flag); dfree(s->status); dfree(s->perm);
+  dfree(s->tdnp_s); dfree(s->tdnp_a); dfree(s->tdnp_tot);
   dfree(s->tiles); dfree(s->thermo_d);
   dfree(s->cbox); dfree(s->cgeom); dfree(s->acell); dfree(s->coff); dfree(s->cell_out);
   dfree(s->cflag);
@@ -1151,6 +1229,12 @@ int tmd_compute(tmd_system *s, int eflag, int vflag, double scale, double *energ
   launch_force_eval(s, (float)scale, want_vatom);
   if (eflag || energy)
     launch_reduce_scaled(s->E, nl, s->partial, s->scal, scale, s->st, s->launches);
+  if (s->m->h.tdnp) {
+    // entropy and free energy totals of the temperature-dependent model
+    // (TensorMD::run, tensormd.cpp:491-492: S and A times the pair scale)
+    launch_reduce_scaled(s->tdnp_s, nl, s->partial, s->tdnp_tot, scale, s->st, s->launches);
+    launch_reduce_scaled(s->tdnp_a, nl, s->partial, s->tdnp_tot + 1, scale, s->st, s->launches);
+  }
   if (vflag || virial)
     launch_reduce_f64(s->wv, nl, 6, s->partial, s->scal + 1, s->st, s->launches);
   launch_check_finite(n, s->f, (eflag || energy) ? s->scal : nullptr, s->status, s->st,
@@ -1180,6 +1264,13 @@ int tmd_compute(tmd_system *s, int eflag, int vflag, double scale, double *energ
   if (st & kStatusOutside) return fail(TMD_ERR_ARG, "atom outside a non-periodic boundary");
   if (energy) *energy = s->h_scal[0];
   if (virial) for (int c = 0; c < 6; c++) virial[c] = s->h_scal[1 + c];
+  if (s->m->h.tdnp) {
+    double t2[2] = {0.0, 0.0};
+    TMD_CUDA(cudaMemcpyAsync(t2, s->tdnp_tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    TMD_CUDA(cudaStreamSynchronize(s->st));
+    s->tdnp_S = t2[0];
+    s->tdnp_A = t2[1];
+  }
   s->forces_valid = true;
   if (st & kStatusNonfinite) return fail(TMD_ERR_NONFINITE, "non-finite energy or force");
   return TMD_OK;
@@ -1390,6 +1481,21 @@ int tmd_system_stream(tmd_system *s, void **stream) {
 }
 
 long tmd_system_launches(const tmd_system *s) { return s ? s->launches : 0; }
+
+int tmd_system_set_etemp(tmd_system *s, double etemp_ev) {
+  if (!s || !(etemp_ev >= 0)) return fail(TMD_ERR_ARG, "electron temperature must be >= 0");
+  if (etemp_ev != s->etemp) drop_graph(s);  // a captured step holds the old value
+  s->etemp = etemp_ev;
+  return TMD_OK;
+}
+
+int tmd_system_tdnp_energies(tmd_system *s, double *entropy, double *free_energy) {
+  if (!s) return fail(TMD_ERR_ARG, "null system");
+  if (!s->m->h.tdnp) return fail(TMD_ERR_STATE, "the potential is not temperature-dependent");
+  if (entropy) *entropy = s->tdnp_S;
+  if (free_energy) *free_energy = s->tdnp_A;
+  return TMD_OK;
+}
 
 int tmd_system_set_wait_probe(tmd_system *s, long long cycles) {
   if (!s || cycles < 0) return fail(TMD_ERR_ARG, "bad wait probe");

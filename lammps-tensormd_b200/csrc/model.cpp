@@ -213,7 +213,11 @@ HostModel parse_model(const std::string &coeff_args) {
       read_elt = false;
       i += 2;
     } else if (v == "etemp") {
-      bad("etemp (temperature-dependent TDNP model) is not supported");
+      // electron temperature in K, kept in eV (pair_tensormd.cpp:33,245-246)
+      h.etemp = std::strtod(value("etemp").c_str(), nullptr) / 11604.522060401008;
+      if (!(h.etemp >= 0)) bad("etemp must be >= 0");
+      read_elt = false;
+      i += 2;
     } else if (v == "cmax") {
       std::string c = value("cmax");
       if (c != "exact" && c != "default") bad("Unknown option for cmax");
@@ -239,8 +243,9 @@ HostModel parse_model(const std::string &coeff_args) {
 
   Npz z = load_npz(h.path);
   h.file_precision = has(z, "precision") ? need(z, "precision").iscalar() : 64;
-  if (has(z, "tdnp") && need(z, "tdnp").iscalar() == 1)
-    bad("TDNP potentials (tdnp = 1) are not supported");
+  h.tdnp = has(z, "tdnp") && need(z, "tdnp").iscalar() == 1;
+  if (h.tdnp && h.precision != 0)
+    bad("TDNP potentials run the plain FP32 form (no precision keyword)");
   h.rmax = need(z, "rmax").scalar();
   h.nelt = need(z, "nelt").iscalar();
   h.mm = need(z, "max_moment").iscalar();
@@ -302,7 +307,30 @@ HostModel parse_model(const std::string &coeff_args) {
   static const int nv[4] = {1, 4, 10, 20};
   h.D = nv[h.mm];
   h.M = h.mm + 1;
-  // NNP
+  if (h.tdnp) {
+    parse_tdnp(z, h);
+  } else {
+    parse_nnp(z, h);
+  }
+  if (h.interp_dx > 0) {
+    if (h.file_precision == 32)
+      build_table_t<float>(z, h, h.interp_dx);
+    else
+      build_table_t<double>(z, h, h.interp_dx);
+  }
+  // cutforcesq is a Scalar in TensorMD<Scalar> (tensormd.h:80)
+  if (h.file_precision == 32) {
+    float r = float(h.rmax);
+    h.rcsq = double(r * r);
+  } else {
+    h.rcsq = h.rmax * h.rmax;
+  }
+  return h;
+}
+
+namespace {
+// The NNP of a tdnp = 0 file (nnp.cpp:110-145).
+void parse_nnp_impl(const Npz &z, HostModel &h) {
   h.nl = need(z, "nlayers").iscalar();
   h.actfn = need(z, "actfn").iscalar();
   h.outbias = need(z, "apply_output_bias").iscalar();
@@ -342,21 +370,73 @@ HostModel parse_model(const std::string &coeff_args) {
         if (l == h.nl - 1) h.Bout[e] = b.d;
       }
     }
-  if (h.interp_dx > 0) {
-    if (h.file_precision == 32)
-      build_table_t<float>(z, h, h.interp_dx);
-    else
-      build_table_t<double>(z, h, h.interp_dx);
-  }
-  // cutforcesq is a Scalar in TensorMD<Scalar> (tensormd.h:80)
-  if (h.file_precision == 32) {
-    float r = float(h.rmax);
-    h.rcsq = double(r * r);
-  } else {
-    h.rcsq = h.rmax * h.rmax;
-  }
-  return h;
 }
+
+// The H, U, S nets of a tdnp = 1 file (tdnp.cpp:46-139): H maps the
+// descriptor to ydim - 1 values, to which the reference appends the
+// electron temperature (a zero weight column, tdnp.cpp:80-97); U and S map
+// the ydim values to an atom's internal energy and entropy.
+void parse_net(const Npz &z, const HostModel &h, const std::string &sc, int n_in,
+               HostModel::Net &t) {
+  t.nl = need(z, sc + "::nlayers").iscalar();
+  t.actfn = need(z, sc + "::actfn").iscalar();
+  t.outbias = need(z, sc + "::apply_output_bias").iscalar();
+  const int res_raw = need(z, sc + "::use_resnet_dt").iscalar();
+  const auto &ls = need(z, sc + "::layer_sizes");
+  if ((int)ls.size() != t.nl || t.nl < 1 || t.nl > kMaxLayers)
+    bad(sc + "::layer_sizes / nlayers unsupported");
+  t.sizes.assign(1, n_in);
+  for (size_t i = 0; i < ls.size(); i++) t.sizes.push_back(int(ls.d[i]));
+  for (int l = 0; l <= t.nl; l++)
+    if (t.sizes[l] < 1 || t.sizes[l] > 1024) bad(sc + " layer widths must be 1..1024");
+  int n_res = 0;
+  for (int l = 1; l < t.nl; l++)
+    if (t.sizes[l] == t.sizes[l + 1]) n_res++;
+  t.resnet = (res_raw && n_res > 0) ? 1 : 0;
+  t.W.assign(h.nelt, std::vector<std::vector<double>>(t.nl));
+  t.B.assign(h.nelt, std::vector<std::vector<double>>(t.nl));
+  for (int e = 0; e < h.nelt; e++)
+    for (int l = 0; l < t.nl; l++) {
+      const std::string key = "_" + std::to_string(e) + "_" + std::to_string(l);
+      const auto &w = need(z, sc + "::weights" + key);
+      if ((int)w.size() != t.sizes[l] * t.sizes[l + 1]) bad(sc + "::weights" + key + " has a wrong shape");
+      t.W[e][l] = w.d;
+      if (l < t.nl - 1 || t.outbias) {
+        const auto &b = need(z, sc + "::biases" + key);
+        if ((int)b.size() != t.sizes[l + 1]) bad(sc + "::biases" + key + " has a wrong shape");
+        t.B[e][l] = b.d;
+      }
+    }
+}
+
+void parse_tdnp_impl(const Npz &z, HostModel &h) {
+  h.sommerfeld = has(z, "tdnp::Sommerfeld") && need(z, "tdnp::Sommerfeld").iscalar() == 1;
+  const auto &w00 = need(z, "H::weights_0_0");
+  h.nin = w00.shape.empty() ? 1 : (int)w00.shape[0];
+  if (h.nin != h.nelt * h.K * h.M) bad("H::weights_0_0 rows != nelt*k*m");
+  parse_net(z, h, "H", h.nin, h.tH);
+  h.ydim = h.tH.sizes[h.tH.nl] + 1;
+  // the temperature column: zero weights and bias
+  const int L = h.tH.nl, K = h.tH.sizes[L - 1], N = h.ydim - 1;
+  for (int e = 0; e < h.nelt; e++) {
+    std::vector<double> w((size_t)K * (N + 1), 0.0);
+    for (int k = 0; k < K; k++)
+      for (int n = 0; n < N; n++) w[(size_t)k * (N + 1) + n] = h.tH.W[e][L - 1][(size_t)k * N + n];
+    h.tH.W[e][L - 1] = w;
+    if (!h.tH.B[e][L - 1].empty()) h.tH.B[e][L - 1].push_back(0.0);
+  }
+  h.tH.sizes[L] = h.ydim;
+  parse_net(z, h, "U", h.ydim, h.tU);
+  parse_net(z, h, "S", h.ydim, h.tS);
+  if ((int)need(z, "U::weights_0_0").shape[0] != h.ydim ||
+      (int)need(z, "S::weights_0_0").shape[0] != h.ydim)
+    bad("U and S must take the ydim outputs of H (with the temperature column)");
+}
+}  // namespace
+
+void parse_nnp(const Npz &z, HostModel &h) { parse_nnp_impl(z, h); }
+void parse_tdnp(const Npz &z, HostModel &h) { parse_tdnp_impl(z, h); }
+
 
 void fill_kparams(const HostModel &h, KParams &kp) {
   std::memset(&kp, 0, sizeof(kp));

@@ -39,11 +39,24 @@ struct HostModel {
   std::vector<int> sizes;                              // [nl+1]
   std::vector<std::vector<std::vector<float>>> W, Bs;  // [e][l]
   std::vector<std::vector<double>> Wout, Bout;         // [e] output layer, FP64
+  // temperature-dependent model (tdnp = 1, tdnp.cpp): nets H, U, S replace
+  // the MLP; etemp from pair_coeff (eV)
+  struct Net {
+    int nl = 0, actfn = 0, outbias = 0, resnet = 0;
+    std::vector<int> sizes;                         // [nl+1]
+    std::vector<std::vector<std::vector<double>>> W, B;  // [e][l], FP64 as read
+  };
+  int tdnp = 0, sommerfeld = 0, ydim = 0;
+  double etemp = 0.0;
+  Net tH, tU, tS;
 };
 
 // Parse "file.npz El1 El2 ... [interp dx] [cmax ...] [precision ...]" and the
 // file.  Throws ModelError / std::runtime_error.
 HostModel parse_model(const std::string &coeff_args);
+// The MLP of the file (tdnp = 0) or its TDNP nets (tdnp = 1), into h.
+void parse_nnp(const Npz &z, HostModel &h);
+void parse_tdnp(const Npz &z, HostModel &h);
 
 void fill_kparams(const HostModel &h, KParams &kp);
 

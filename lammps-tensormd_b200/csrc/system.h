@@ -38,6 +38,10 @@ struct tmd_model {
   int mlp_resident = 0;    // > 0: resident-weight MLP, persistent grid size
   int mlp_streamed = 0;    // > 0: streamed-weight FP32 MLP, persistent grid size
   int mlp_stages = 0;
+  // temperature-dependent model (tdnp = 1): the nets' layers on the device
+  tmd::TdnpLayer *d_tdnp = nullptr;
+  size_t tdnp_warp_floats = 0;
+  int tdnp_maxw = 0;
   int nsys = 0;            // systems created from this model and not yet freed
   bool released = false;   // tmd_model_free called while nsys > 0
 };
@@ -96,6 +100,11 @@ struct tmd_system {
   int force_variant = 0;
   int desc_variant = 0;    // kDesc*, the same way
   long long wait_probe = 0;  // tmd_system_set_wait_probe (failure-detection tests)
+  // temperature-dependent model: electron temperature (eV), per-atom
+  // entropy and free energy, and their totals of the last compute
+  double etemp = 0.0;
+  double *tdnp_s = nullptr, *tdnp_a = nullptr, *tdnp_tot = nullptr;  // tot: [2]
+  double tdnp_S = 0.0, tdnp_A = 0.0;
   // kernel timing
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;

@@ -180,6 +180,32 @@ struct MlpTcArgs {
   long long probe_wait;
 };
 void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches);
+
+// ---- temperature-dependent model (tdnp.cu) ----
+// One layer of a TDNP net: W (K x N), WT (N x K), b (N or null); for the
+// last layer of U and S also Wf (FP32) / Wd (FP64) row sums over the outputs
+// and bd the summed bias (FP64).
+struct TdnpLayer {
+  int K, N;
+  const float *W, *WT, *b, *Wf;
+  const double *Wd;
+  double bd;
+};
+struct TdnpArgs {
+  int n, nin, ydim, maxw, nelt;
+  int nl[3], actfn[3], resnet[3];    // H, U, S
+  const TdnpLayer *layers;           // [net][element][kMaxLayers]
+  const int *elem;
+  const float *G;
+  float *dEdG;
+  double *E, *Sa, *Aa;               // per atom: u, s, u - T s
+  float T, c;                        // electron temperature (eV); T or T^2 (Sommerfeld)
+  int sommerfeld;
+  size_t warp_floats;                // shared memory per warp (floats)
+};
+size_t tdnp_warp_floats(const int nl[3], int maxw);
+// 0, or -1 when the nets need more shared memory than a CTA has.
+int launch_mlp_tdnp(const TdnpArgs &a, cudaStream_t st, long &launches);
 size_t mlp_tc_smem(int nl, int maxh, int resnet, bool dz_bf16, int np);
 void mlp_tc_prepare(size_t smem, bool dz_bf16, int np);
 // Persistent form: dynamic shared memory for sizes[0..nl], 0 if unsupported

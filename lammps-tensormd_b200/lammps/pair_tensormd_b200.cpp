@@ -33,6 +33,7 @@
 #include "force.h"
 #include "memory.h"
 #include "neighbor.h"
+#include "utils.h"
 
 #include "tmd_b200.h"
 
@@ -59,6 +60,8 @@ PairTensorMDB200::PairTensorMDB200(LAMMPS *lmp) : Pair(lmp)
   last_nall = -1;
   last_box_stamp = -1;
   ghost_mode = false;
+  etemp = eentropy = free_energy = 0.0;
+  last_etemp = -1.0;
 }
 
 PairTensorMDB200::~PairTensorMDB200()
@@ -106,6 +109,9 @@ void PairTensorMDB200::coeff(int narg, char **arg)
   for (int i = 2; i < narg; i++) {
     if (i > 2) args += " ";
     args += arg[i];
+    // electron temperature in K, kept in eV (pair_tensormd.cpp:33,245-246)
+    if (strcmp(arg[i], "etemp") == 0 && i + 1 < narg)
+      etemp = utils::numeric(FLERR, arg[i + 1], false, lmp) / 11604.522060401008;
   }
   if (sys) { tmd_system_free(sys); sys = nullptr; }
   if (model) { tmd_model_free(model); model = nullptr; }
@@ -169,6 +175,7 @@ void PairTensorMDB200::upload()
     check(tmd_system_create(model, natoms_cap, skin, &sys), "system");
     last_nlocal = -1;
     last_box_stamp = -1;
+    last_etemp = -1.0;
   }
   xbuf.assign(atom->x[0], atom->x[0] + 3 * (size_t)nall);
   const bool reneighbored = nall != last_nall || nlocal != last_nlocal || neighbor->ago == 0;
@@ -215,7 +222,14 @@ void PairTensorMDB200::compute(int eflag, int vflag)
   double *ea = nullptr, *va = nullptr;
   if (eflag_atom) { ebuf.resize(n); ea = ebuf.data(); }
   if (vflag_atom) { vbuf.resize(6 * (size_t)n); va = vbuf.data(); }
+  if (etemp != last_etemp) {
+    check(tmd_system_set_etemp(sys, etemp), "electron temperature");
+    last_etemp = etemp;
+  }
   check(tmd_compute(sys, eflag, vflag, scale[1][1], &e, v6, fbuf.data(), ea, va), "compute");
+  // TDNP potentials: entropy and free energy (zero otherwise)
+  if (tmd_system_tdnp_energies(sys, &eentropy, &free_energy) != TMD_OK)
+    eentropy = free_energy = 0.0;
   double **f = atom->f;
   for (int i = 0; i < n; i++) {
     f[i][0] += fbuf[3 * i];
@@ -250,6 +264,10 @@ void *PairTensorMDB200::extract(const char *str, int &dim)
   if (strcmp(str, "scale") == 0) {
     dim = 2;
     return (void *) scale;
+  }
+  if (strcmp(str, "etemp") == 0) {
+    dim = 0;
+    return (void *) &etemp;
   }
   return nullptr;
 }

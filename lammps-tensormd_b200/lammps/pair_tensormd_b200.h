@@ -46,6 +46,11 @@ class PairTensorMDB200 : public Pair {
   int descriptor_width();
   void descriptors(double *G);
 
+  // temperature-dependent potentials (tdnp = 1), as PairTensorMD: the
+  // electron temperature in eV (pair_coeff etemp, fix tensormd/etemp through
+  // extract("etemp")), and the entropy and free energy of the last compute
+  double etemp, eentropy, free_energy;
+
  private:
   tmd_model *model;
   tmd_system *sys;
@@ -56,6 +61,7 @@ class PairTensorMDB200 : public Pair {
   int last_nlocal, last_nall;
   bool ghost_mode;
   int last_box_stamp;
+  double last_etemp;
   double last_box[9];
   std::vector<double> xbuf, fbuf, ebuf, vbuf;
   std::vector<int> tbuf;

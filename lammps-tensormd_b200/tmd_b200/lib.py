@@ -45,6 +45,8 @@ SIGNATURES = [
     ("tmd_system_launches", _c_long, [_vp]),
     ("tmd_system_rebuilds", _c_int, [_vp, _pl]),
     ("tmd_system_set_wait_probe", _c_int, [_vp, ctypes.c_longlong]),
+    ("tmd_system_set_etemp", _c_int, [_vp, _c_double]),
+    ("tmd_system_tdnp_energies", _c_int, [_vp, _pd, _pd]),
     ("tmd_fp32_peak", _c_int, [_c_int, _c_int, _pd]),
     ("tmd_profile_enable", _c_int, [_vp, _c_int]),
     ("tmd_profile_read", _c_int, [_vp, _pl, _pd, _c_int]),

@@ -219,6 +219,16 @@ class TensorMDSystem:
     def launches(self) -> int:
         return int(self.lib.tmd_system_launches(self.h))
 
+    def set_etemp(self, kelvin):
+        """Electron temperature of a tdnp = 1 potential, in K (fix tensormd/etemp)."""
+        check(self.lib.tmd_system_set_etemp(self.h, float(kelvin) / 11604.522060401008))
+
+    def tdnp_energies(self):
+        """(entropy, free energy) of the last compute of a tdnp = 1 potential."""
+        s_, a_ = ctypes.c_double(), ctypes.c_double()
+        check(self.lib.tmd_system_tdnp_energies(self.h, ctypes.byref(s_), ctypes.byref(a_)))
+        return s_.value, a_.value
+
     def rebuilds(self) -> int:
         """Neighbor-list rebuilds run since the system was created."""
         c = ctypes.c_long()

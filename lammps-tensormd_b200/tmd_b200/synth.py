@@ -71,6 +71,45 @@ def gaussian_potential(path, *, nelt=1, num_filters=16, rc=6.0, max_moment=3,
     return symbols
 
 
+def tdnp_potential(path, *, nelt=1, num_filters=8, rc=5.0, max_moment=3, h_hidden=(32,),
+                   ydim=8, u_hidden=(16,), s_hidden=(16,), actfn=1, sommerfeld=0, seed=77,
+                   symbols=None):
+    """Write a temperature-dependent (tdnp = 1) potential with random weights:
+    the Gaussian descriptor of gaussian_potential, and three nets per element
+    in the layout tdnp.cpp reads (H::*, U::*, S::*; tdnp::Sommerfeld): H maps
+    the descriptor to ydim - 1 values (the reference appends the electron
+    temperature as column ydim - 1), U and S map the ydim values to the
+    atom's internal energy and entropy.  No main NNP keys (TDNP replaces it)."""
+    rng = np.random.default_rng(seed)
+    symbols = gaussian_potential(path, nelt=nelt, num_filters=num_filters, rc=rc,
+                                 max_moment=max_moment, hidden=(4,), actfn=actfn,
+                                 seed=seed, symbols=symbols)
+    with np.load(path) as z:
+        d = {k: z[k] for k in z.files if not (k.startswith(("weights_", "biases_"))
+                                               or k in ("nlayers", "actfn", "layer_sizes",
+                                                        "use_resnet_dt", "apply_output_bias"))}
+    d["tdnp"] = np.int32(1)
+    d["tdnp::Sommerfeld"] = np.int32(sommerfeld)
+    nin = nelt * num_filters * (max_moment + 1)
+    nets = {"H": [nin] + list(h_hidden) + [ydim - 1],
+            "U": [ydim] + list(u_hidden) + [1],
+            "S": [ydim] + list(s_hidden) + [1]}
+    for scope, sizes in nets.items():
+        d[f"{scope}::nlayers"] = np.int32(len(sizes) - 1)
+        d[f"{scope}::layer_sizes"] = np.array(sizes[1:], dtype=np.int32)
+        d[f"{scope}::actfn"] = np.int32(actfn)
+        d[f"{scope}::use_resnet_dt"] = np.int32(0)
+        d[f"{scope}::apply_output_bias"] = np.int32(1)
+        for e in range(nelt):
+            for l in range(len(sizes) - 1):
+                w = rng.normal(0.0, 1.0 / np.sqrt(sizes[l]), size=(sizes[l], sizes[l + 1]))
+                d[f"{scope}::weights_{e}_{l}"] = (w if sizes[l + 1] > 1 else w[:, 0])
+                b = rng.normal(0.0, 0.1, size=sizes[l + 1])
+                d[f"{scope}::biases_{e}_{l}"] = b if sizes[l + 1] > 1 else b.reshape(())
+    np.savez(path, **d)
+    return symbols
+
+
 def _lattice_basis(kind):
     if kind == "fcc":
         return np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])

@@ -186,13 +186,19 @@ def pack_model(pot: dict, interp: float | None = None):
         K = int(np.asarray(pot[key]).size)
     if use_fnn and not interp:
         raise ValueError("FNN radial basis requires interp dx")
-    nl = int(pot["nlayers"])
-    sizes = [int(s) for s in np.asarray(pot["layer_sizes"]).ravel()]
-    n_in = int(np.asarray(pot["weights_0_0"]).shape[0])
+    tdnp = "tdnp" in pot and int(np.asarray(pot["tdnp"]).ravel()[0]) == 1
+    if tdnp:  # the TDNP nets replace the NNP (tensormd.cpp:129-132,471-484)
+        nl, sizes = 0, []
+        n_in = int(np.asarray(pot["H::weights_0_0"]).shape[0])
+    else:
+        nl = int(pot["nlayers"])
+        sizes = [int(s) for s in np.asarray(pot["layer_sizes"]).ravel()]
+        n_in = int(np.asarray(pot["weights_0_0"]).shape[0])
     ints = [1, nelt, mm, K, int(pot["fctype"]), 1 if interp else 0,
             int(pot.get("descriptor::method", 0)) if not use_fnn else 0,
-            int(pot.get("is_T_symmetric", 0)), nl, int(pot["actfn"]),
-            int(pot["use_resnet_dt"]), int(pot["apply_output_bias"]), n_in, 0]
+            int(pot.get("is_T_symmetric", 0)), nl, 0 if tdnp else int(pot["actfn"]),
+            0 if tdnp else int(pot["use_resnet_dt"]),
+            0 if tdnp else int(pot["apply_output_bias"]), n_in, 0]
     ints += sizes
     dbl = [float(np.asarray(pot["rmax"]).ravel()[0]), 0.0]
     p = np.zeros((3, K))
@@ -210,7 +216,7 @@ def pack_model(pot: dict, interp: float | None = None):
         tab = prm.astype(np.float64).ravel()
     parts = [np.asarray(dbl), p.ravel(), tab]
     full = [n_in] + sizes
-    outb = int(pot["apply_output_bias"])
+    outb = 0 if tdnp else int(pot["apply_output_bias"])
     for e in range(nelt):
         for l in range(nl):
             parts.append(np.asarray(pot[f"weights_{e}_{l}"], dtype=np.float64).ravel())
@@ -219,6 +225,41 @@ def pack_model(pot: dict, interp: float | None = None):
                                  f"expected {full[l]}x{full[l + 1]}")
             if l < nl - 1 or outb:
                 parts.append(np.asarray(pot[f"biases_{e}_{l}"], dtype=np.float64).ravel())
+    return np.asarray(ints, dtype=np.int32), np.concatenate(parts).astype(np.float64)
+
+
+def pack_tdnp(pot: dict):
+    """The H, U, S nets of a tdnp = 1 potential (tdnp.cpp:46-139) as the blob
+    of tmd_oracle.c tmdo_model_set_tdnp; H gets the zero weight column of the
+    electron temperature (tdnp.cpp:80-97)."""
+    nelt = int(pot["nelt"])
+    som = int(np.asarray(pot.get("tdnp::Sommerfeld", 0)).ravel()[0])
+    hs = [int(v) for v in np.asarray(pot["H::layer_sizes"]).ravel()]
+    ydim = hs[-1] + 1
+    ints = [som, ydim]
+    parts = []
+    for scope in ("H", "U", "S"):
+        nl = int(pot[f"{scope}::nlayers"])
+        ls = [int(v) for v in np.asarray(pot[f"{scope}::layer_sizes"]).ravel()]
+        n_in = int(np.asarray(pot[f"{scope}::weights_0_0"]).shape[0])
+        sizes = [n_in] + ls
+        if scope == "H":
+            sizes[-1] += 1
+        outb = int(pot[f"{scope}::apply_output_bias"])
+        ints += [nl, int(pot[f"{scope}::actfn"]), int(pot[f"{scope}::use_resnet_dt"]), outb]
+        ints += sizes
+        for e in range(nelt):
+            for l in range(nl):
+                w = np.asarray(pot[f"{scope}::weights_{e}_{l}"], dtype=np.float64)
+                w = w.reshape(sizes[l], -1)
+                if scope == "H" and l == nl - 1:
+                    w = np.concatenate([w, np.zeros((sizes[l], 1))], axis=1)
+                parts.append(w.ravel())
+                if l < nl - 1 or outb:
+                    b = np.asarray(pot[f"{scope}::biases_{e}_{l}"], dtype=np.float64).ravel()
+                    if scope == "H" and l == nl - 1:
+                        b = np.concatenate([b, [0.0]])
+                    parts.append(b)
     return np.asarray(ints, dtype=np.int32), np.concatenate(parts).astype(np.float64)
 
 
@@ -278,6 +319,12 @@ class Oracle:
                                    ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double,
                                    ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+            L.tmdo_model_set_tdnp.restype = ctypes.c_int
+            L.tmdo_model_set_tdnp.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.c_int]
+            L.tmdo_set_etemp.argtypes = [ctypes.c_void_p, ctypes.c_double]
+            L.tmdo_tdnp_totals.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
             L.tmdo_fire.restype = ctypes.c_int
             L.tmdo_fire.argtypes = [ctypes.c_void_p, ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_double),
@@ -291,7 +338,9 @@ class Oracle:
             cls._lib = L
         return cls._lib
 
-    def __init__(self, pot, interp: float | None = None):
+    def __init__(self, pot, interp: float | None = None, etemp: float = 0.0):
+        """etemp: electron temperature in K (pair_coeff keyword etemp, used by
+        tdnp = 1 potentials; converted to eV as pair_tensormd.cpp:33,246)."""
         if not isinstance(pot, dict):
             pot = load_npz(pot)
         self.pot = pot
@@ -302,11 +351,29 @@ class Oracle:
                                   _p(dbl, ctypes.c_double), dbl.size)
         if not self.h:
             raise ValueError("oracle rejected the model")
+        self.tdnp = "tdnp" in pot and int(np.asarray(pot["tdnp"]).ravel()[0]) == 1
+        if self.tdnp:
+            ti, td = pack_tdnp(pot)
+            self._tints, self._tdbl = ti, td
+            if L.tmdo_model_set_tdnp(self.h, _p(ti, ctypes.c_int), ti.size,
+                                     _p(td, ctypes.c_double), td.size) != 0:
+                raise ValueError("oracle rejected the TDNP nets")
+        self.set_etemp(etemp)
         dims = np.zeros(6, dtype=np.int32)
         L.tmdo_model_dims(self.h, _p(dims, ctypes.c_int))
         self.K, self.D, self.M, self.nelt, self.n_in, self.resnet = (int(v) for v in dims)
         self.rmax = float(np.asarray(pot["rmax"]).ravel()[0])
         self.masses = np.asarray(pot["masses"], dtype=np.float64).ravel()
+
+    def set_etemp(self, kelvin: float):
+        """Electron temperature (K) of a TDNP potential (fix tensormd/etemp)."""
+        self.lib().tmdo_set_etemp(self.h, float(kelvin) / 11604.522060401008)
+
+    def tdnp_totals(self):
+        """(entropy, free energy) of the last compute of a TDNP potential."""
+        out = np.zeros(2)
+        self.lib().tmdo_tdnp_totals(self.h, _p(out, ctypes.c_double))
+        return float(out[0]), float(out[1])
 
     def __del__(self):
         try:

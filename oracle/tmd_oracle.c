@@ -45,6 +45,14 @@
 #define OM_MAXE 8
 #define OM_MAXD 20
 
+/* One MLP of a TDNP model (tdnp.cpp setup_one): weights W[e][l] (K x N,
+ * row-major), biases b[e][l] (NULL for a last layer without output bias). */
+typedef struct {
+  int nl, actfn, resnet, outbias;
+  int sizes[OM_MAXL + 1];
+  const double *W[OM_MAXE][OM_MAXL], *b[OM_MAXE][OM_MAXL];
+} om_net;
+
 typedef struct {
   int nelt, max_moment, K, D, M, fctype, radial, desc_method, tsym;
   int nl, actfn, resnet, outbias, n_in, tab_n;
@@ -54,6 +62,14 @@ typedef struct {
   const double *dp0, *dp1, *dp2, *tab;
   const double *W[OM_MAXE][OM_MAXL], *b[OM_MAXE][OM_MAXL];
   double *store;
+  /* temperature-dependent model (tdnp.cpp): H maps G to y (ydim values, the
+   * last one the electron temperature), U and S map y to the atom's internal
+   * energy and entropy; the forces are those of A = U - T S */
+  int tdnp, sommerfeld, ydim;
+  double etemp;                  /* eV */
+  om_net H, U, S;
+  double *tstore;
+  double tdnp_S, tdnp_A;         /* totals of the last compute */
 } om_model;
 
 /* exponents (ax, ay, az) of monomial d, order of kernel.cu:1197-1232 */
@@ -148,7 +164,61 @@ void tmdo_model_free(void *h)
   om_model *m = (om_model *)h;
   if (!m) return;
   free(m->store);
+  free(m->tstore);
   free(m);
+}
+
+/* TDNP nets (blob of oracle/pack.py pack_tdnp): ints = [sommerfeld, ydim,
+ * then per net H, U, S: nl, actfn, resnet_raw, outbias, sizes[0..nl]];
+ * doubles = per net, element, layer: W (sizes[l] x sizes[l+1]) and, for
+ * hidden layers or with the output bias, b.  H's last layer has ydim
+ * outputs, the last column zero (tdnp.cpp:80-97). */
+int tmdo_model_set_tdnp(void *h, const int *ib, int ni, const double *db, int nd)
+{
+  (void)ni;
+  om_model *m = (om_model *)h;
+  m->tdnp = 1;
+  m->sommerfeld = ib[0];
+  m->ydim = ib[1];
+  m->tstore = (double *)malloc(sizeof(double) * (size_t)(nd > 0 ? nd : 1));
+  memcpy(m->tstore, db, sizeof(double) * (size_t)nd);
+  const int *q = ib + 2;
+  const double *p = m->tstore;
+  om_net *nets[3] = {&m->H, &m->U, &m->S};
+  for (int k = 0; k < 3; k++) {
+    om_net *t = nets[k];
+    t->nl = *q++;
+    t->actfn = *q++;
+    int res_raw = *q++;
+    t->outbias = *q++;
+    if (t->nl < 1 || t->nl > OM_MAXL) return -1;
+    for (int l = 0; l <= t->nl; l++) t->sizes[l] = *q++;
+    int n_res = 0;
+    for (int l = 1; l < t->nl; l++)
+      if (t->sizes[l] == t->sizes[l + 1]) n_res++;
+    t->resnet = (res_raw && n_res > 0) ? 1 : 0;
+    for (int e = 0; e < m->nelt; e++)
+      for (int l = 0; l < t->nl; l++) {
+        t->W[e][l] = p;
+        p += (size_t)t->sizes[l] * t->sizes[l + 1];
+        if (l < t->nl - 1 || t->outbias) {
+          t->b[e][l] = p;
+          p += t->sizes[l + 1];
+        } else {
+          t->b[e][l] = NULL;
+        }
+      }
+  }
+  return 0;
+}
+
+void tmdo_set_etemp(void *h, double etemp_ev) { ((om_model *)h)->etemp = etemp_ev; }
+
+void tmdo_tdnp_totals(void *h, double *out)
+{
+  om_model *m = (om_model *)h;
+  out[0] = m->tdnp_S;
+  out[1] = m->tdnp_A;
 }
 
 int tmdo_model_dims(void *h, int *out)
@@ -370,6 +440,106 @@ static double om_mlp(const om_model *m, int e, const double *g, double *grad,
   return E;
 }
 
+/* Forward of one TDNP net for element e: act[l] (width sizes[l], stride
+ * maxw) holds the input of layer l, dz[l] the act' of hidden layer l; the
+ * last layer is linear (nnp.cu:200-281).  Returns the sum of the outputs. */
+static double om_net_fwd(const om_net *t, int e, int actfn_ovr, double *act, double *dz,
+                         int maxw)
+{
+  (void)actfn_ovr;
+  int L = t->nl;
+  for (int l = 0; l < L; l++) {
+    int Kl = t->sizes[l], Nl = t->sizes[l + 1];
+    const double *W = t->W[e][l], *b = t->b[e][l];
+    double *x = act + (size_t)l * maxw, *y = act + (size_t)(l + 1) * maxw;
+    double *d = dz + (size_t)l * maxw;
+    for (int n = 0; n < Nl; n++) {
+      double z = 0.0;
+      for (int k = 0; k < Kl; k++) z += x[k] * W[(size_t)k * Nl + n];
+      if (b) z += b[n];
+      if (l < L - 1) {
+        double yy = om_act(t->actfn, z, &d[n]);
+        if (l > 0 && t->resnet && Kl == Nl) yy += x[n];
+        y[n] = yy;
+      } else {
+        y[n] = z;
+      }
+    }
+  }
+  double s = 0.0;
+  for (int n = 0; n < t->sizes[L]; n++) s += act[(size_t)L * maxw + n];
+  return s;
+}
+
+/* Backward of one net from the gradient gout of its outputs (NULL: 1 for
+ * every output, the gradient of their sum) to gin (width sizes[0]), with the
+ * activations of om_net_fwd (nnp.cu:149-198). */
+static void om_net_bwd(const om_net *t, int e, const double *gout, const double *dz, int maxw,
+                       double *gin)
+{
+  int L = t->nl;
+  double ga[1024], gb[1024];
+  double *gy = ga, *gx = gb;
+  {
+    int Kl = t->sizes[L - 1], Nl = t->sizes[L];
+    const double *W = t->W[e][L - 1];
+    for (int k = 0; k < Kl; k++) {
+      double s = 0.0;
+      for (int n = 0; n < Nl; n++) s += (gout ? gout[n] : 1.0) * W[(size_t)k * Nl + n];
+      gy[k] = s;
+    }
+  }
+  for (int l = L - 2; l >= 0; l--) {
+    int Kl = t->sizes[l], Nl = t->sizes[l + 1];
+    const double *W = t->W[e][l];
+    const double *d = dz + (size_t)l * maxw;
+    for (int k = 0; k < Kl; k++) {
+      double s = 0.0;
+      for (int n = 0; n < Nl; n++) s += gy[n] * d[n] * W[(size_t)k * Nl + n];
+      if (l > 0 && t->resnet && Kl == Nl) s += gy[k];
+      gx[k] = s;
+    }
+    double *tt = gy; gy = gx; gx = tt;
+  }
+  memcpy(gin, gy, sizeof(double) * t->sizes[0]);
+}
+
+/* TDNP atom (tdnp.cpp:167-226, nnp.cu:295-318): y = H(G), y[ydim-1] = T;
+ * u = U(y), s = S(y) (times T with the Sommerfeld form); the gradient of
+ * A = u - T s (T^2 s_net with Sommerfeld) back through H, the temperature
+ * column held fixed.  Returns u; *s_out, *a_out. */
+#define OM_TW 1024 /* widest TDNP layer */
+#define OM_TWORK (6 * (OM_MAXL + 1) * OM_TW + 3 * OM_TW)
+
+static double om_tdnp(const om_model *m, int e, const double *g, double *grad,
+                      double *s_out, double *a_out, double *work)
+{
+  enum { W = OM_TW };
+  double *actH = work, *dzH = actH + (OM_MAXL + 1) * W;
+  double *actU = dzH + (OM_MAXL + 1) * W, *dzU = actU + (OM_MAXL + 1) * W;
+  double *actS = dzU + (OM_MAXL + 1) * W, *dzS = actS + (OM_MAXL + 1) * W;
+  double *gu = dzS + (OM_MAXL + 1) * W, *gs = gu + W, *gyv = gs + W;
+  double T = m->etemp;
+  memcpy(actH, g, sizeof(double) * m->n_in);
+  om_net_fwd(&m->H, e, 0, actH, dzH, W);
+  double *y = actH + (size_t)m->H.nl * W;
+  y[m->ydim - 1] = T;
+  memcpy(actU, y, sizeof(double) * m->ydim);
+  memcpy(actS, y, sizeof(double) * m->ydim);
+  double u = om_net_fwd(&m->U, e, 0, actU, dzU, W);
+  double s = om_net_fwd(&m->S, e, 0, actS, dzS, W);
+  if (m->sommerfeld) s *= T;
+  om_net_bwd(&m->U, e, NULL, dzU, W, gu);
+  om_net_bwd(&m->S, e, NULL, dzS, W, gs);
+  double scale = m->sommerfeld ? T * T : T;
+  for (int k = 0; k < m->ydim; k++) gyv[k] = gu[k] - scale * gs[k];
+  gyv[m->ydim - 1] = 0.0;
+  om_net_bwd(&m->H, e, gyv, dzH, W, grad);
+  *s_out = s;
+  *a_out = u - T * s;
+  return u;
+}
+
 /* ------------------------------------------------------------------ */
 /* neighbor list                                                       */
 /* ------------------------------------------------------------------ */
@@ -545,6 +715,8 @@ double tmdo_compute(void *h, int n, const double *x, const int *elem,
   double *dfbuf = (double *)calloc((size_t)(npair > 0 ? npair : 1) * 3,
                                    sizeof(double));
   double *Ebuf = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double *Sbuf = (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+  double *Abuf = (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
   int eltij[OM_MAXE][OM_MAXE];
   for (int i = 0; i < B; i++) {
     int k = 1;
@@ -558,6 +730,7 @@ double tmdo_compute(void *h, int n, const double *x, const int *elem,
     double *G = (double *)malloc(sizeof(double) * nin);
     double *dG = (double *)malloc(sizeof(double) * (nin > 1024 ? nin : 1024));
     double *work = (double *)malloc(sizeof(double) * (size_t)(m->nl + 1) * maxw * 2);
+    double *twork = m->tdnp ? (double *)malloc(sizeof(double) * OM_TWORK) : NULL;
     double H[256], dH[256], Mv[OM_MAXD], dM[3 * OM_MAXD];
 #pragma omp for schedule(dynamic, 16)
     for (int i = 0; i < n; i++) {
@@ -592,7 +765,12 @@ double tmdo_compute(void *h, int n, const double *x, const int *elem,
           g0[0] = sqrt(g0[0]) * (Pk[0] < 0 ? -1.0 : 1.0);
         }
       if (Gout) memcpy(Gout + (size_t)i * nin, G, sizeof(double) * nin);
-      double E = om_mlp(m, ei, G, dG, work, maxw);
+      double E;
+      if (m->tdnp) {
+        E = om_tdnp(m, ei, G, dG, &Sbuf[i], &Abuf[i], twork);
+      } else {
+        E = om_mlp(m, ei, G, dG, work, maxw);
+      }
       Ebuf[i] = E;
       if (dEdGout) memcpy(dEdGout + (size_t)i * nin, dG, sizeof(double) * nin);
       /* dE/dG0 -> 0.5 dEdG0 / G0, then dE/dP */
@@ -641,7 +819,7 @@ double tmdo_compute(void *h, int n, const double *x, const int *elem,
           dfbuf[3 * s + a] = (f1 * u[a] + f2[a]) * scale;
       }
     }
-    free(P); free(S); free(G); free(dG); free(work);
+    free(P); free(S); free(G); free(dG); free(work); free(twork);
   }
 
   /* deterministic serial accumulation */
@@ -680,8 +858,17 @@ double tmdo_compute(void *h, int n, const double *x, const int *elem,
   }
   if (virial)
     for (int c = 0; c < 6; c++) virial[c] = vir[c];
+  double st = 0.0, at = 0.0;
+  for (int i = 0; i < n; i++) {
+    st += Sbuf[i] * scale;
+    at += Abuf[i] * scale;
+  }
+  m->tdnp_S = st;
+  m->tdnp_A = at;
   free(dfbuf);
   free(Ebuf);
+  free(Sbuf);
+  free(Abuf);
   return etot;
 }
 

@@ -61,8 +61,13 @@ def test_bad_arguments(libtmd, tmp_path):
     assert rc == -3 and "cmax" in msg
     rc, msg = _load(libtmd, f"{p} Cu Ni interp 0.001 stray")
     assert rc == -3 and "stray" in msg
-    rc, msg = _load(libtmd, f"{p} Cu Ni etemp 300")
+    rc, msg = _load(libtmd, f"{p} Cu Ni etemp -300")
     assert rc == -3 and "etemp" in msg
+    # temperature-dependent files run the plain FP32 form only
+    q = tmp_path / "t.npz"
+    synth.tdnp_potential(q, nelt=2, symbols=["Cu", "Ni"])
+    rc, msg = _load(libtmd, f"{q} Cu Ni etemp 3000 precision bf16")
+    assert rc == -3 and "TDNP" in msg
 
 
 def test_fnn_needs_interp(libtmd):

@@ -125,3 +125,29 @@ def test_fire_restatement_relaxes_a_trained_cell():
     # capped run: exactly maxiter iterations when the tolerance is unreachable
     _, _, _, it2 = o.fire(x, t - 1, box, [1, 1, 1], 0.001, 1e-12, 30)
     assert it2 == 30
+
+
+@pytest.mark.parametrize("sommerfeld", [0, 1])
+def test_tdnp_forces_are_the_free_energy_gradient(tmp_path, sommerfeld):
+    """TDNP restatement (tdnp.cpp, nnp.cu:295-318): the energy is the sum of
+    U, the forces are -dA/dx with A = U - T S (S scaled by T in the Sommerfeld
+    form), checked by central differences at T = 5000 K; A - U = -T S."""
+    p = tmp_path / "t.npz"
+    synth.tdnp_potential(p, nelt=2, sommerfeld=sommerfeld)
+    o = Oracle(load_npz(p), etemp=5000.0)
+    x, t, box, _ = synth.build_system("fcc", 3.6, (2, 2, 2), sigma=0.1, nelt=2, seed=3)
+    r = o.compute(x, t - 1, box, [1, 1, 1])
+    S, A = o.tdnp_totals()
+    T = 5000.0 / 11604.522060401008
+    assert A == pytest.approx(r["energy"] - T * S, rel=1e-12)
+    h = 1e-5
+    for i in (0, 17):
+        for a in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[i, a] += h
+            xm[i, a] -= h
+            o.compute(xp, t - 1, box, [1, 1, 1])
+            ap = o.tdnp_totals()[1]
+            o.compute(xm, t - 1, box, [1, 1, 1])
+            am = o.tdnp_totals()[1]
+            assert r["f"][i, a] == pytest.approx(-(ap - am) / (2 * h), rel=1e-6, abs=1e-8)
