@@ -552,19 +552,90 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
     }
     prof_end(s, 5);
   };
-  // Without kernel timing, the step runs as one captured CUDA graph: every
-  // launch (including the conditional rebuild kernels) is replayed with its
-  // arguments fixed at capture; buffers, box, atom count and dt key the graph.
+  // Without kernel timing, the step runs as one captured CUDA graph with its
+  // arguments fixed at capture; buffers, box, atom count and dt key the
+  // graph.  The rebuild kernels sit in the body of a conditional (IF) node
+  // whose value a one-thread kernel sets from the displacement check's flag
+  // (cudaGraphSetConditional), so a step without a rebuild launches none of
+  // them; where the runtime refuses conditional nodes, every rebuild kernel
+  // is captured and returns at once when no rebuild is pending.
   const bool use_graph = !s->prof;
+  auto md_step_conditional = [&](cudaGraph_t *g_out) -> cudaError_t {
+    long lb = 0;
+    cudaError_t e = cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    if (nvt) launch_nhc_half(G, s->nhc, nullptr, n, acell, s->v, s->st, s->launches);
+    launch_nve_initial(n, s->x, s->v, s->f, s->elem, s->m->d_mass, dtf, dt, s->st, s->launches);
+    launch_neighbor_check(n, s->x, s->xbuild, trigsq, s->flag, s->st, s->launches, s->acell,
+                          s->ncells ? s->cflag : nullptr);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraphConditionalHandle ch;
+    cudaGraphNode_t cn = nullptr;
+    e = cudaStreamGetCaptureInfo(s->st, &cs, nullptr, &cg, &deps, &ndeps);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&ch, cg, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+      launch_rebuild_cond(ch, s->flag, s->st, s->launches);
+      e = cudaStreamGetCaptureInfo(s->st, &cs, nullptr, &cg, &deps, &ndeps);
+    }
+    cudaGraphNodeParams cp = {};
+    if (e == cudaSuccess) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = ch;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&cn, cg, deps, ndeps, &cp);
+    }
+    if (e == cudaSuccess && !s->st_aux) e = cudaStreamCreateWithFlags(&s->st_aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+      e = cudaStreamBeginCaptureToGraph(s->st_aux, cp.conditional.phGraph_out[0], nullptr, nullptr,
+                                        0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const long l1 = s->launches;
+      launch_neighbor_build(nb_args(s), s->st_aux, s->launches);
+      lb = s->launches - l1;
+      s->launches = l1;
+      cudaGraph_t body;
+      e = cudaStreamEndCapture(s->st_aux, &body);
+    }
+    if (e == cudaSuccess)
+      e = cudaStreamUpdateCaptureDependencies(s->st, &cn, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+      launch_force_eval(s, 1.0f, false);
+      launch_nve_final(n, s->v, s->f, s->elem, s->m->d_mass, dtf, s->st, s->launches);
+      if (nvt) {
+        group_ke(s);
+        launch_nhc_half(G, s->nhc, s->nhc_ke, n, acell, s->v, s->st, s->launches);
+      }
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s->st, &g);
+    if (e == cudaSuccess) e = ee;
+    if (e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();  // a refused capture leaves no sticky error
+      return e;
+    }
+    s->rebuild_launches = lb;
+    *g_out = g;
+    return cudaSuccess;
+  };
   auto ensure_graph = [&]() -> int {
     if (!use_graph || (s->step_exec && s->step_dt == dt && s->step_nvt == (nvt != nullptr)))
       return TMD_OK;
     drop_graph(s);
-    cudaGraph_t g;
+    cudaGraph_t g = nullptr;
     long l0 = s->launches;
-    TMD_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-    md_step();
-    TMD_CUDA(cudaStreamEndCapture(s->st, &g));
+    s->rebuild_launches = 0;
+    if (md_step_conditional(&g) != cudaSuccess) {
+      s->launches = l0;
+      s->rebuild_launches = 0;
+      TMD_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+      md_step();
+      TMD_CUDA(cudaStreamEndCapture(s->st, &g));
+    }
     cudaError_t ie = cudaGraphInstantiate(&s->step_exec, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) {
@@ -587,6 +658,13 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
   constexpr int kChunk = 256;
   rc = checkpoint_reserve(s);
   if (rc) return rc;
+  // rebuilds before the run: the conditional rebuild kernels are counted
+  // once per rebuild that ran (flag[1])
+  int rb0[2] = {0, 0};
+  if (use_graph && s->rebuild_launches > 0) {
+    TMD_CUDA(cudaMemcpyAsync(rb0, s->flag, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    TMD_CUDA(cudaStreamSynchronize(s->st));
+  }
   for (int s0 = 1, retries = 0; s0 <= nsteps;) {
     const int s1 = std::min(nsteps, s0 + kChunk - 1);
     const int row0 = row;
@@ -634,6 +712,12 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
     TMD_CUDA(cudaMemcpyAsync(thermo, s->thermo_d, thermo_count * sizeof(double),
                              cudaMemcpyDeviceToHost, s->st));
     TMD_CUDA(cudaStreamSynchronize(s->st));
+  }
+  if (use_graph && s->rebuild_launches > 0) {
+    int rb1[2] = {0, 0};
+    TMD_CUDA(cudaMemcpyAsync(rb1, s->flag, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    TMD_CUDA(cudaStreamSynchronize(s->st));
+    s->launches += (long)(rb1[1] - rb0[1]) * s->rebuild_launches;
   }
   s->forces_valid = true;
   return TMD_OK;
@@ -1063,6 +1147,7 @@ void tmd_system_free(tmd_system *s) {
   }
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   if (s->st) cudaStreamDestroy(s->st);
+  if (s->st_aux) cudaStreamDestroy(s->st_aux);
   if (s->m) {
     tmd_model *m = const_cast<tmd_model *>(s->m);
     if (--m->nsys == 0 && m->released) tmd_model_free(m);

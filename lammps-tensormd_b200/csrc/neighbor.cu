@@ -908,6 +908,18 @@ void launch_neighbor_check(int n, const double *x, const double *xbuild,
   launches += 1;
 }
 
+// The MD step graph's rebuild condition: 1 when the displacement check (or a
+// forced rebuild) set the flag.
+__global__ void k_rebuild_cond(cudaGraphConditionalHandle h, const int *flag) {
+  cudaGraphSetConditional(h, flag[0] != 0 ? 1u : 0u);
+}
+
+void launch_rebuild_cond(cudaGraphConditionalHandle h, const int *flag, cudaStream_t st,
+                         long &launches) {
+  k_rebuild_cond<<<1, 1, 0, st>>>(h, flag);
+  launches += 1;
+}
+
 void launch_set_flag(int *flag, cudaStream_t st, long &launches) {
   k_set_flag<<<1, 1, 0, st>>>(flag);
   launches += 1;

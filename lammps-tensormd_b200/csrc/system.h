@@ -117,6 +117,8 @@ struct tmd_system {
   double step_dt = 0.0;
   bool step_nvt = false;
   long step_launches = 0;
+  long rebuild_launches = 0;      // kernels of the conditional rebuild body
+  cudaStream_t st_aux = nullptr;  // captures the rebuild body
   // fix nvt: one Nose-Hoover chain per group (cell, or the whole system);
   // kept between runs of the same atoms like the fix's state in LAMMPS
   tmd::NhcState *nhc = nullptr;

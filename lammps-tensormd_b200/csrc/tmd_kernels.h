@@ -65,6 +65,9 @@ void launch_neighbor_check(int n, const double *x, const double *xbuild,
                            double trigsq, int *flag, cudaStream_t st,
                            long &launches, const int *acell = nullptr, int *cflag = nullptr);
 void launch_set_flag(int *flag, cudaStream_t st, long &launches);
+// One thread: sets an IF node's condition of a captured graph to flag[0] != 0.
+void launch_rebuild_cond(cudaGraphConditionalHandle h, const int *flag, cudaStream_t st,
+                         long &launches);
 // Positions from a caller's frame: each atom to the periodic image nearest its
 // position at the last list build (cbox/acell in multi-cell mode, else box).
 void launch_nearest_image(int n, double *x, const double *xbuild, const BoxP &box,
