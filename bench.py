@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--profile-step", type=int, default=0, metavar="N",
                     help="profiler target: set up the headline workload with the default "
                          "kernel forms, run N force evaluations, print nothing else")
-    ap.add_argument("--profile-precision", default="fp32", choices=["fp32", "bf16x3", "bf16"],
+    ap.add_argument("--profile-precision", default="fp32",
+                    choices=["fp32", "tf32x3", "bf16x3", "bf16"],
                     help="MLP precision form of the --profile-step target")
     ap.add_argument("--profile-desc", default="", choices=["", "filter4", "wide", "wide2", "split"],
                     help="descriptor form of the --profile-step target (default: the "
@@ -463,7 +464,7 @@ def run_ours_sampled(args, rank, world, local, clk):
     # tensor-core MLP forms of the same workload (same steps, same timing)
     forms = {"fp32": {"value": value, "ms_per_step": ms_max / args.steps,
                       "mlp_ms": prof["mlp"][1] / max(prof["mlp"][0], 1)}}
-    for prec in ([] if (args.no_bf16 or args.main_only) else ["bf16x3", "bf16"]):
+    for prec in ([] if (args.no_bf16 or args.main_only) else ["tf32x3", "bf16x3", "bf16"]):
         try:
             mb = TensorMDModel(f"{pot} {' '.join(syms)} precision {prec}", device=local)
             sb = TensorMDSystem(mb, n, 1.0)
@@ -593,7 +594,7 @@ def run_ours_sampled(args, rank, world, local, clk):
 def run_alloy(args, rank, world, local, dev, barrier):
     """Precision config: 4-element random FCC alloy a = 3.6 A, 60x60x30 cells =
     432,000 atoms, 32 Gaussians rc 6.5 A, MLP 512-128-128-128-1 softplus.
-    Each MLP form (plain FP32, split BF16, BF16) runs the same NVE steps,
+    Each MLP form (plain FP32, 3xTF32, split BF16, BF16) runs the same NVE steps,
     timed with CUDA events on its system stream after 3 warm-up steps; MLP
     time per step from a profiled pass; force and energy error of the BF16
     forms against the FP32 form on the starting positions."""
@@ -603,7 +604,7 @@ def run_alloy(args, rank, world, local, dev, barrier):
     n, dt = len(x), 0.001
     out = {"natoms": n, "steps": args.precision_steps, "config": cfg, "forms": {}}
     ref = None
-    for prec in ("fp32", "bf16x3", "bf16"):
+    for prec in ("fp32", "tf32x3", "bf16x3", "bf16"):
         suffix = "" if prec == "fp32" else f" precision {prec}"
         m = TensorMDModel(f"{pot} {' '.join(syms)}{suffix}", device=local)
         s_ = TensorMDSystem(m, n, 1.0)
@@ -641,7 +642,7 @@ def run_alloy(args, rank, world, local, dev, barrier):
         s_.close()
         m.close()
     f32 = out["forms"]["fp32"]["value"]
-    for prec in ("bf16x3", "bf16"):
+    for prec in ("tf32x3", "bf16x3", "bf16"):
         out["forms"][prec]["speedup_vs_fp32"] = out["forms"][prec]["value"] / f32
     return out
 

@@ -41,12 +41,13 @@ extern "C" {
 #define TMD_PREC_BF16 1
 #define TMD_PREC_FP8 2    /* e4m3 tensor-core MLP, per-layer weight and per-row operand scales */
 #define TMD_PREC_BF16X3 3 /* split BF16 products: FP32-class accuracy */
+#define TMD_PREC_TF32X3 4 /* split TF32 products (3xTF32) on tcgen05: FP32 accuracy */
 
 typedef struct tmd_model tmd_model;
 typedef struct tmd_system tmd_system;
 
 /* pair_coeff arguments after "* *":  "file.npz El1 El2 ... [interp dx]
- * [cmax exact|default] [precision fp32|bf16|bf16x3|fp8]".
+ * [cmax exact|default] [precision fp32|tf32x3|bf16|bf16x3|fp8]".
  * Replaces PairTensorMD::coeff + read_potential_file + TensorMD::read_npz /
  * setup_global / setup_interpolation (pair_tensormd.cpp:214-317,376-399;
  * tensormd.cpp:109-280,438-446).  The element list maps LAMMPS atom types
@@ -224,7 +225,7 @@ int tmd_system_set_etemp(tmd_system *sys, double etemp_ev);
 int tmd_system_tdnp_energies(tmd_system *sys, double *entropy, double *free_energy);
 
 /* Failure-detection hook for tests (no reference counterpart).  With
- * cycles > 0 the system's tensor-core MLP kernels (precision bf16, bf16x3,
+ * cycles > 0 the system's tensor-core MLP kernels (precision tf32x3, bf16, bf16x3,
  * fp8) start every CTA with a wait of at most `cycles` clock cycles on one
  * of their mbarriers, before any MMA or copy is issued; nothing arrives on
  * it, so each CTA takes its timeout path (no asynchronous work in flight,

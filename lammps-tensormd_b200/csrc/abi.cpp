@@ -352,6 +352,8 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
     ta.dz_bf16_p = m->tc_dz_bf16_p ? 1 : 0;
     ta.streamed = m->tc_streamed; ta.smem_s = m->tc_smem_s; ta.stages = m->tc_stages;
     ta.probe_wait = s->wait_probe;
+    ta.tf32 = m->tc_tf32 ? 1 : 0;
+    ta.hi2 = m->tc_hi2;
     if (m->tc_fp8) launch_mlp_fp8(ta, s->st, s->launches);
     else launch_mlp_tc(ta, s->st, s->launches);
   } else {
@@ -912,6 +914,67 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
   }
   if (m->mlp_streamed == 0) mlp_fp32_prepare(m->mlp_tr, m->mlp_smem, m->mlp_resident > 0);
   for (int l = 1; l < h.nl; l++) m->maxh = std::max(m->maxh, h.sizes[l]);
+  if (h.precision == TMD_PREC_TF32X3) {
+    // 3xTF32 on tcgen05 (streamed form): W as hi = tf32(W) and lo =
+    // tf32(W - hi) planes, 32-column chunks, W^T (forward) and W (backward)
+    int stages = 0;
+    const size_t ss = mlp_tcs_smem(h.nl, h.sizes.data(), h.resnet, 3, 1, &stages);
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+    if (ss == 0 || nsm <= 0) {
+      tmd_model_free(m);
+      return fail(TMD_ERR_MODEL, "precision tf32x3 needs no residual layers, nelt*k*m and hidden "
+                                 "widths that are multiples of 32, hidden widths <= 256 and "
+                                 "act' within 512 TMEM columns");
+    }
+    std::vector<MlpTcLayer> tl((size_t)h.nelt * h.nl);
+    for (int el = 0; el < h.nelt && e == cudaSuccess; el++)
+      for (int l = 0; l < h.nl && e == cudaSuccess; l++) {
+        MlpTcLayer &T = tl[(size_t)el * h.nl + l];
+        const MlpLayer &F = layers[(size_t)el * h.nl + l];
+        T.K = h.sizes[l];
+        T.N = h.sizes[l + 1];
+        T.b = F.b;
+        T.wd = F.Wd;
+        T.bd = F.bd;
+        T.wscale = 1.f;
+        if (l == h.nl - 1) continue;
+        const int K = T.K, N = T.N;
+        const size_t nf = (size_t)N * K;
+        std::vector<float> pf(2 * nf), pb(2 * nf);
+        const std::vector<float> &W = h.W[el][l];
+        for (int part = 0; part < 2; part++) {
+          pack_core_chunks_tf32(W.data(), N, K, 1, N, part, pf.data() + part * nf);  // W^T
+          pack_core_chunks_tf32(W.data(), K, N, N, 1, part, pb.data() + part * nf);  // W
+        }
+        for (auto *vec : {&pf, &pb}) {
+          float *d = nullptr;
+          if (e == cudaSuccess) e = dalloc(&d, vec->size());
+          if (e == cudaSuccess) {
+            m->d_buf.push_back(d);
+            e = cudaMemcpy(d, vec->data(), vec->size() * 4, cudaMemcpyHostToDevice);
+          }
+          if (vec == &pf) T.Wf = d; else T.Wb = d;
+        }
+      }
+    if (e == cudaSuccess) e = dalloc(&m->d_tc_layers, tl.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(m->d_tc_layers, tl.data(), tl.size() * sizeof(MlpTcLayer),
+                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      tmd_model_free(m);
+      return fail(TMD_ERR_CUDA, std::string("tensor-core weight upload: ") +
+                                    cudaGetErrorString(e));
+    }
+    m->tc_np = 3;
+    m->tc_tf32 = true;
+    m->tc_hi2 = mlp_tcs_hi2(h.nl, h.sizes.data(), 3, 1);
+    m->tc_streamed = nsm;
+    m->tc_smem_s = ss;
+    m->tc_stages = stages;
+    mlp_tcs_prepare(ss, 3, 1);
+    m->mlp_tr = 128;
+  }
   if (h.precision == TMD_PREC_BF16 || h.precision == TMD_PREC_BF16X3 ||
       h.precision == TMD_PREC_FP8) {
     const bool fp8 = h.precision == TMD_PREC_FP8;
@@ -1029,12 +1092,12 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
       }
       // weights too large to stay resident: the streamed-weight form
       int stages = 0;
-      const size_t ss = mlp_tcs_smem(h.nl, h.sizes.data(), h.resnet, np, &stages);
+      const size_t ss = mlp_tcs_smem(h.nl, h.sizes.data(), h.resnet, np, 0, &stages);
       if (m->tc_persistent == 0 && ss > 0 && nsm > 0) {
         m->tc_streamed = nsm;
         m->tc_smem_s = ss;
         m->tc_stages = stages;
-        mlp_tcs_prepare(ss, np);
+        mlp_tcs_prepare(ss, np, 0);
       }
     }
     m->mlp_tr = 128;

@@ -585,6 +585,72 @@ struct TcsChunk {  // one weight chunk of the per-tile schedule
   short l, dir, c, n0, nrows;
 };
 
+// Operand formats of the streamed form.  Both keep 128-byte chunk rows (KC
+// reduction columns), so a weight chunk of R rows is R x 128 bytes either way.
+//   OpBf16: kind::f16 with BF16 A and B, 8 elements per 16-byte core row,
+//           MMA K = 16; activations from fast intrinsics (operands are BF16).
+//   OpTf32: kind::tf32, 4 elements per core row, MMA K = 8; the values are
+//           FP32 words rounded to TF32 (cvt.rna), split as hi + lo with
+//           NP = 3 (hi*hi' + hi*lo' + lo*hi': the 3xTF32 scheme, ~21
+//           significant bits per product, FP32 accumulation); activations
+//           and act' from the accurate functions of the FP32 forms.
+struct OpBf16 {
+  typedef __nv_bfloat16 T;
+  static constexpr int EPC = 8, KSTEP = 16, KC = 64;
+  static constexpr bool kFastAct = true;
+  static constexpr bool kSplitAcc = false;
+  __device__ static uint32_t idesc(int N) { return idesc_bf16(N); }
+  __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    mma_bf16(d, a, b, id, acc);
+  }
+  // 8 consecutive columns [c, c + 8) of row r (kfull columns): one core row
+  template <int NP>
+  __device__ static void put8(T *buf, size_t lo, int r, int c, int kfull, const float *v) {
+    put_core_row<NP>(buf, lo, tc::core_off<EPC>(r, c, kfull), v[0], v[1], v[2], v[3], v[4],
+                     v[5], v[6], v[7]);
+  }
+};
+
+__device__ inline uint32_t tf32_rna(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return r;
+}
+
+struct OpTf32 {
+  typedef float T;
+  static constexpr int EPC = 4, KSTEP = 8, KC = 32;
+  static constexpr bool kFastAct = false;
+  static constexpr bool kSplitAcc = true;
+  // D = FP32 [4,6) = 1, A = B = TF32 [7,10) = [10,13) = 2, K-major both
+  __device__ static uint32_t idesc(int N) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(TM >> 4) << 24);
+  }
+  __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(id), "r"(acc));
+  }
+  template <int NP>
+  __device__ static void put4(T *buf, size_t lo, int off, float v0, float v1, float v2,
+                              float v3) {
+    const uint32_t h0 = tf32_rna(v0), h1 = tf32_rna(v1), h2 = tf32_rna(v2), h3 = tf32_rna(v3);
+    *reinterpret_cast<uint4 *>(buf + off) = make_uint4(h0, h1, h2, h3);
+    if (NP == 3)
+      *reinterpret_cast<uint4 *>(buf + lo + off) =
+          make_uint4(tf32_rna(v0 - __uint_as_float(h0)), tf32_rna(v1 - __uint_as_float(h1)),
+                     tf32_rna(v2 - __uint_as_float(h2)), tf32_rna(v3 - __uint_as_float(h3)));
+  }
+  // 8 consecutive columns: two core rows in neighbouring core matrices
+  template <int NP>
+  __device__ static void put8(T *buf, size_t lo, int r, int c, int kfull, const float *v) {
+    put4<NP>(buf, lo, tc::core_off<EPC>(r, c, kfull), v[0], v[1], v[2], v[3]);
+    put4<NP>(buf, lo, tc::core_off<EPC>(r, c + 4, kfull), v[4], v[5], v[6], v[7]);
+  }
+};
+
 __device__ inline void tmem_st32(uint32_t taddr, const float v[32]) {
   asm volatile(
       "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
@@ -604,16 +670,17 @@ __device__ inline void tmem_st32(uint32_t taddr, const float v[32]) {
       : "memory");
 }
 
-// Shared-memory plan of the streamed form: elements (BF16) of one stage and
-// of the operand region (per hi/lo part), TMEM accumulator width.
+// Shared-memory plan of the streamed form: elements of one stage and of the
+// operand region (per hi/lo part), TMEM accumulator width; kc = reduction
+// columns per chunk (the format's KC).
 struct TcsPlan {
   int maxrows, stage_elems, a_elems, accw;
 };
-__host__ __device__ inline TcsPlan tcs_plan(int nin, int maxh, int nb) {
+__host__ __device__ inline TcsPlan tcs_plan(int nin, int maxh, int nb, int kc) {
   TcsPlan p;
   p.maxrows = maxh > 128 ? maxh : 128;
-  p.stage_elems = nb * p.maxrows * KCH;
-  const int g2 = 2 * TM * KCH, h = TM * maxh;
+  p.stage_elems = nb * p.maxrows * kc;
+  const int g2 = 2 * TM * kc, h = TM * maxh;
   p.a_elems = g2 > h ? g2 : h;
   p.accw = p.maxrows;
   (void)nin;
@@ -621,7 +688,7 @@ __host__ __device__ inline TcsPlan tcs_plan(int nin, int maxh, int nb) {
 }
 }  // namespace
 
-template <int NP>
+template <int NP, class OP>
 __global__ void __launch_bounds__(kTcsThreads, 1)
 k_mlp_tcs(MlpTcArgs a) {
   extern __shared__ __align__(1024) unsigned char smraw[];
@@ -634,39 +701,49 @@ k_mlp_tcs(MlpTcArgs a) {
   __shared__ int nq_s, sz_s[kMaxLayers + 1], act_s[kMaxLayers], bo_s[kMaxLayers];
   __shared__ float bias_s[kTcsMaxBias];   // hidden biases of the current element
   __shared__ double wout_s[256];          // its output-layer weights
-  typedef __nv_bfloat16 T;
+  typedef typename OP::T T;
   constexpr int NB = NP == 3 ? 2 : 1;
+  constexpr int EPC = OP::EPC, KSTEP = OP::KSTEP, KC = OP::KC;
+  // split accumulators (3xTF32): hi*hi' into D_hi, hi*lo' + lo*hi' into D_lo,
+  // summed in the epilogue, so that only one MMA per K step adds to a
+  // full-magnitude accumulator
+  constexpr bool kSplit = OP::kSplitAcc && NP == 3;
+  // split, where TMEM has room: the hi*hi' products of odd K steps into a
+  // second accumulator D_hi2 (half the full-magnitude accumulations each)
+  const bool hi2 = kSplit && a.hi2;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int quad = warp & 3, part = warp >> 2;
   const int row = quad * 32 + lane;
   const int L = a.nl, nin = a.nin, maxh = a.maxh, S = a.stages;
-  const TcsPlan pl = tcs_plan(nin, maxh, NB);
+  const TcsPlan pl = tcs_plan(nin, maxh, NB, KC);
   T *stage0 = reinterpret_cast<T *>(smraw);
   T *abuf = stage0 + (size_t)S * pl.stage_elems;
-  const uint64_t a_lo_u = (uint64_t)(((size_t)pl.a_elems * 2) >> 4);  // lo part, 16-B units
-  const uint64_t b_lo_u = (uint64_t)(((size_t)pl.maxrows * KCH * 2) >> 4);
+  const uint64_t a_lo_u = (uint64_t)(((size_t)pl.a_elems * sizeof(T)) >> 4);  // lo part, 16-B units
+  const uint64_t b_lo_u = (uint64_t)(((size_t)pl.maxrows * KC * sizeof(T)) >> 4);
 
   if (tid == 0) {
     // layer widths, act' TMEM columns and bias offsets per hidden layer
     sz_s[0] = nin;
     for (int l = 0; l < L; l++) sz_s[l + 1] = a.layers[l].N;
-    int o = pl.accw, ob = 0;
+    // act' of the last hidden layer is never stored (its gradient seed is
+    // formed in its forward epilogue)
+    int o = (kSplit ? (a.hi2 ? 3 : 2) : 1) * pl.accw, ob = 0;
     for (int l = 0; l < L - 1; l++) {
       act_s[l] = o;
       bo_s[l] = ob;
-      o += sz_s[l + 1];
+      if (l < L - 2) o += sz_s[l + 1];
       ob += sz_s[l + 1];
     }
     const int *sizes = sz_s;
     int k = 0;
     for (int l = 0; l < L - 1; l++)
-      for (int c = 0; c < sizes[l] / KCH; c++)
+      for (int c = 0; c < sizes[l] / KC; c++)
         sched[k++] = TcsChunk{(short)l, 0, (short)c, 0, (short)sizes[l + 1]};
     for (int l = L - 2; l >= 1; l--)
-      for (int c = 0; c < sizes[l + 1] / KCH; c++)
+      for (int c = 0; c < sizes[l + 1] / KC; c++)
         sched[k++] = TcsChunk{(short)l, 1, (short)c, 0, (short)sizes[l]};
     for (int n0 = 0; n0 < sizes[0]; n0 += 128)
-      for (int c = 0; c < sizes[1] / KCH; c++)
+      for (int c = 0; c < sizes[1] / KC; c++)
         sched[k++] = TcsChunk{0, 1, (short)c, (short)n0, (short)min(128, sizes[0] - n0)};
     nq_s = k;
     for (int s = 0; s < S; s++) {
@@ -722,20 +799,25 @@ k_mlp_tcs(MlpTcArgs a) {
       const int K = sizes[ch.l], N = sizes[ch.l + 1];
       const int brows = ch.dir ? K : N;
       const T *src = reinterpret_cast<const T *>(ch.dir ? ly.Wb : ly.Wf) +
-                     ((size_t)ch.c * brows + ch.n0) * KCH;
-      const uint32_t bytes = (uint32_t)ch.nrows * KCH * 2;
+                     ((size_t)ch.c * brows + ch.n0) * KC;
+      const uint32_t bytes = (uint32_t)(ch.nrows * KC * sizeof(T));
       const uint32_t bar = smem_u32(&full_b[s]);
       T *dst = stage0 + (size_t)s * pl.stage_elems;
       mbar_expect_tx(bar, bytes * NB);
       bulk_g2s(smem_u32(dst), src, bytes, bar);
-      if (NP == 3) bulk_g2s(smem_u32(dst + (size_t)pl.maxrows * KCH), src + (size_t)K * N, bytes, bar);
+      if (NP == 3) bulk_g2s(smem_u32(dst + (size_t)pl.maxrows * KC), src + (size_t)K * N, bytes, bar);
       q_issue++;
     }
   };
-  // thread 0: the MMAs of the next chunk into TMEM column tcol; A at a_addr
-  // (hi part) with 8-row group stride a_sbo bytes
-  auto mma_next = [&](uint32_t a_addr, uint32_t a_sbo, uint32_t tcol, bool first) {
+  // thread 0: the MMAs of the next chunk into TMEM column tcol (and, split,
+  // the lo products into column tlo, the odd K steps' hi products into thi2
+  // with hi2); A at a_addr (hi part) with 8-row group stride a_sbo bytes.
+  // kst counts the K steps of the current GEMM.
+  int kst = 0;
+  auto mma_next = [&](uint32_t a_addr, uint32_t a_sbo, uint32_t tcol, uint32_t tlo, uint32_t thi2,
+                      bool first) {
     if (!ok0) return;
+    if (first) kst = 0;
     const int q = q_mma;
     const int s = q % S;
     if (!mbar_wait(&full_b[s], (uint32_t)(q / S) & 1u)) {
@@ -744,17 +826,23 @@ k_mlp_tcs(MlpTcArgs a) {
     }
     asm volatile("tcgen05.fence::after_thread_sync;");
     const TcsChunk ch = sched[q % nq];
-    const uint32_t id = idesc_bf16(ch.nrows);
+    const uint32_t id = OP::idesc(ch.nrows);
     const uint32_t bbase = smem_u32(stage0 + (size_t)s * pl.stage_elems);
 #pragma unroll
-    for (int ks = 0; ks < KCH / KSTEP; ks++) {
+    for (int ks = 0; ks < KC / KSTEP; ks++) {
       const uint64_t da = sdesc(a_addr + (uint32_t)(ks * KSTEP / EPC) * 128u, 128u, a_sbo);
       const uint64_t db = sdesc(bbase + (uint32_t)(ks * KSTEP / EPC) * 128u, 128u,
-                                (uint32_t)(KCH / EPC) * 128u);
-      mma_bf16(tmem + tcol, da, db, id, (!first || ks > 0) ? 1u : 0u);
-      if (NP == 3) {
-        mma_bf16(tmem + tcol, da, db + b_lo_u, id, 1u);  // hi * lo'
-        mma_bf16(tmem + tcol, da + a_lo_u, db, id, 1u);  // lo * hi'
+                                (uint32_t)(KC / EPC) * 128u);
+      const int g = kst++;
+      const uint32_t acc = g >= 1 ? 1u : 0u;
+      if (hi2) OP::mma(tmem + ((g & 1) ? thi2 : tcol), da, db, id, g >= 2 ? 1u : 0u);
+      else OP::mma(tmem + tcol, da, db, id, acc);
+      if (kSplit) {
+        OP::mma(tmem + tlo, da, db + b_lo_u, id, acc);  // hi * lo'
+        OP::mma(tmem + tlo, da + a_lo_u, db, id, 1u);   // lo * hi'
+      } else if (NP == 3) {
+        OP::mma(tmem + tcol, da, db + b_lo_u, id, 1u);  // hi * lo'
+        OP::mma(tmem + tcol, da + a_lo_u, db, id, 1u);  // lo * hi'
       }
     }
     commit(&empty_b[s]);
@@ -774,8 +862,24 @@ k_mlp_tcs(MlpTcArgs a) {
     ok = __syncthreads_and((ok && (tid != 0 || ok0)) ? 1 : 0) != 0;
   };
   const uint32_t a_sbo_h = (uint32_t)(maxh / EPC) * 128u;   // activation buffer
-  const uint32_t a_sbo_g = (uint32_t)(KCH / EPC) * 128u;    // G chunk slot
+  const uint32_t a_sbo_g = (uint32_t)(KC / EPC) * 128u;     // G chunk slot
   const uint32_t abase = smem_u32(abuf);
+  const uint32_t lo_col = (uint32_t)pl.accw;                // D_lo of the layer GEMMs (split)
+  const uint32_t hi2_col = 2u * (uint32_t)pl.accw;          // D_hi2 (hi2)
+  // z = D_hi (+ D_hi2) + D_lo of 32 columns at c0 into v; d is scratch
+  auto acc_ld = [&](int c0, float (&v)[32], float (&d)[32]) {
+    tmem_ld32(trow + c0, v);
+    if (hi2) {
+      tmem_ld32(trow + hi2_col + c0, d);
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] += d[j];
+    }
+    if (kSplit) {
+      tmem_ld32(trow + lo_col + c0, d);
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] += d[j];
+    }
+  };
 
   int cur_elt = -1;
   if (tid == 0) issue_to(S - 1);
@@ -798,17 +902,17 @@ k_mlp_tcs(MlpTcArgs a) {
     // each thread converts kGRows core rows (8 columns of one atom row) per
     // chunk; the rows of chunk c + 1 are loaded while chunk c is published
     // and multiplied
-    constexpr int kGRows = TM * (KCH / 8) / kTcsThreads;
-    static_assert(kGRows * kTcsThreads == TM * (KCH / 8), "G chunk split");
+    constexpr int kGRows = TM * (KC / 8) / kTcsThreads;
+    static_assert(kGRows * kTcsThreads == TM * (KC / 8), "G chunk split");
     float4 gv[kGRows][2];
     auto load_g = [&](int c) {
 #pragma unroll
       for (int u = 0; u < kGRows; u++) {
         const int idx = tid + u * kTcsThreads;
-        const int r = idx / (KCH / 8), k8 = idx - r * (KCH / 8);
+        const int r = idx / (KC / 8), k8 = idx - r * (KC / 8);
         const int at = rows_s[r];
         if (at >= 0) {
-          const float4 *g = reinterpret_cast<const float4 *>(a.G + (size_t)at * nin + c * KCH + 8 * k8);
+          const float4 *g = reinterpret_cast<const float4 *>(a.G + (size_t)at * nin + c * KC + 8 * k8);
           gv[u][0] = __ldg(g);
           gv[u][1] = __ldg(g + 1);
         } else {
@@ -817,24 +921,24 @@ k_mlp_tcs(MlpTcArgs a) {
       }
     };
     load_g(0);
-    for (int c = 0; c < nin / KCH && ok; c++) {
+    for (int c = 0; c < nin / KC && ok; c++) {
       const int slot = c & 1;
-      T *gs = abuf + (size_t)slot * TM * KCH;
+      T *gs = abuf + (size_t)slot * TM * KC;
       if (c >= 2) wait_all(&gbar[slot], gk[slot]);  // the MMAs of chunk c - 2 are done
       if (!ok) break;
 #pragma unroll
       for (int u = 0; u < kGRows; u++) {
         const int idx = tid + u * kTcsThreads;
-        const int r = idx / (KCH / 8), k8 = idx - r * (KCH / 8);
+        const int r = idx / (KC / 8), k8 = idx - r * (KC / 8);
         const float v[8] = {gv[u][0].x, gv[u][0].y, gv[u][0].z, gv[u][0].w,
                             gv[u][1].x, gv[u][1].y, gv[u][1].z, gv[u][1].w};
-        TMD_PUT_ROW(NP, gs, pl.a_elems, core_off(r, 8 * k8, KCH), v, 0);
+        OP::template put8<NP>(gs, pl.a_elems, r, 8 * k8, KC, v);
       }
-      if (c + 1 < nin / KCH) load_g(c + 1);
+      if (c + 1 < nin / KC) load_g(c + 1);
       publish();
       if (!ok) break;
       if (tid == 0) {
-        mma_next(smem_u32(gs), a_sbo_g, 0, c == 0);
+        mma_next(smem_u32(gs), a_sbo_g, 0, lo_col, hi2_col, c == 0);
         commit(&gbar[slot]);
       }
     }
@@ -845,7 +949,7 @@ k_mlp_tcs(MlpTcArgs a) {
     // each slot used this tile has one completion not yet consumed (its last
     // chunk, done by now): consume it so the parities stay in step
     for (int slot = 0; slot < 2; slot++)
-      if ((nin / KCH - slot + 1) / 2 > 0) wait_all(&gbar[slot], gk[slot]);
+      if ((nin / KC - slot + 1) / 2 > 0) wait_all(&gbar[slot], gk[slot]);
     if (!ok) break;
 
     // ---------------- forward epilogues and hidden layers ----------------
@@ -856,8 +960,8 @@ k_mlp_tcs(MlpTcArgs a) {
       const int actl = act_s[l];
       if (l > 0) {
         if (tid == 0) {
-          for (int c = 0; c < K / KCH; c++)
-            mma_next(abase + (uint32_t)(c * KCH / EPC) * 128u, a_sbo_h, 0, c == 0);
+          for (int c = 0; c < K / KC; c++)
+            mma_next(abase + (uint32_t)(c * KC / EPC) * 128u, a_sbo_h, 0, lo_col, hi2_col, c == 0);
           commit(&accb[0]);
         }
         wait_all(&accb[0], ak[0]);
@@ -866,12 +970,13 @@ k_mlp_tcs(MlpTcArgs a) {
       const bool last = (l == L - 2);
       for (int c0 = 32 * part; c0 < N; c0 += 32 * kTcsParts) {
         float v[32], d[32];
-        tmem_ld32(trow + c0, v);
+        acc_ld(c0, v, d);
 #pragma unroll
         for (int j = 0; j < 32; j++) {
           const int cc = c0 + j;
           const float z = v[j] + bl[cc];
-          const float y = tc::act_fwd_fast(a.actfn, z, d[j]);
+          const float y = OP::kFastAct ? tc::act_fwd_fast(a.actfn, z, d[j])
+                                       : tc::act_fwd(a.actfn, z, d[j]);
           if (!last) {
             v[j] = y;
           } else {
@@ -883,8 +988,7 @@ k_mlp_tcs(MlpTcArgs a) {
         }
         if (!last) tmem_st32(trow + actl + c0, d);
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-          TMD_PUT_ROW(NP, abuf, pl.a_elems, core_off(row, c0 + 8 * q, maxh), v, 8 * q);
+        for (int q = 0; q < 4; q++) OP::template put8<NP>(abuf, pl.a_elems, row, c0 + 8 * q, maxh, v + 8 * q);
       }
       asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       publish();
@@ -900,8 +1004,8 @@ k_mlp_tcs(MlpTcArgs a) {
     for (int l = L - 2; l >= 1 && ok; l--) {
       const int K = sizes[l], N = sizes[l + 1];
       if (tid == 0) {
-        for (int c = 0; c < N / KCH; c++)
-          mma_next(abase + (uint32_t)(c * KCH / EPC) * 128u, a_sbo_h, 0, c == 0);
+        for (int c = 0; c < N / KC; c++)
+          mma_next(abase + (uint32_t)(c * KC / EPC) * 128u, a_sbo_h, 0, lo_col, hi2_col, c == 0);
         commit(&accb[0]);
       }
       wait_all(&accb[0], ak[0]);
@@ -909,13 +1013,12 @@ k_mlp_tcs(MlpTcArgs a) {
       const int actp = act_s[l - 1];
       for (int c0 = 32 * part; c0 < K; c0 += 32 * kTcsParts) {
         float v[32], d[32];
-        tmem_ld32(trow + c0, v);
+        acc_ld(c0, v, d);
         tmem_ld32(trow + actp + c0, d);
 #pragma unroll
         for (int j = 0; j < 32; j++) v[j] *= d[j];
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-          TMD_PUT_ROW(NP, abuf, pl.a_elems, core_off(row, c0 + 8 * q, maxh), v, 8 * q);
+        for (int q = 0; q < 4; q++) OP::template put8<NP>(abuf, pl.a_elems, row, c0 + 8 * q, maxh, v + 8 * q);
       }
       publish();
     }
@@ -923,15 +1026,19 @@ k_mlp_tcs(MlpTcArgs a) {
 
     // ---------------- dE/dG = gz . W_0^T in 128-column blocks ----------------
     {
+      // 128-column blocks over all 512 columns, each block np_ groups of 128
+      // columns (hi, then lo and hi2 when split): up to four blocks at a time
       const int N0 = sizes[1];
       const int nblk = (nin + 127) / 128;
-      for (int b0 = 0; b0 < nblk && ok; b0 += 4) {
-        const int b1 = min(nblk, b0 + 4);
+      const int np_ = kSplit ? (hi2 ? 3 : 2) : 1, conc = 4 / np_;
+      for (int b0 = 0; b0 < nblk && ok; b0 += conc) {
+        const int b1 = min(nblk, b0 + conc);
         if (tid == 0) {
           for (int b = b0; b < b1; b++) {
-            for (int c = 0; c < N0 / KCH; c++)
-              mma_next(abase + (uint32_t)(c * KCH / EPC) * 128u, a_sbo_h,
-                       (uint32_t)(128 * (b - b0)), c == 0);
+            const uint32_t cb = (uint32_t)(128 * np_ * (b - b0));
+            for (int c = 0; c < N0 / KC; c++)
+              mma_next(abase + (uint32_t)(c * KC / EPC) * 128u, a_sbo_h, cb, cb + 128u,
+                       cb + 256u, c == 0);
             commit(&accb[b - b0]);
           }
         }
@@ -941,7 +1048,14 @@ k_mlp_tcs(MlpTcArgs a) {
           const int n0 = 128 * b, nout = min(128, nin - n0);
           for (int c0 = 32 * part; c0 < nout; c0 += 32 * kTcsParts) {
             float v[32];
-            tmem_ld32(trow + (uint32_t)(128 * (b - b0)) + c0, v);
+            const uint32_t cb = (uint32_t)(128 * np_ * (b - b0));
+            tmem_ld32(trow + cb + c0, v);
+            for (int pp = 1; pp < np_; pp++) {
+              float w[32];
+              tmem_ld32(trow + cb + 128u * pp + c0, w);
+#pragma unroll
+              for (int j = 0; j < 32; j++) v[j] += w[j];
+            }
             if (row_atom >= 0) {
               float4 *dst = reinterpret_cast<float4 *>(a.dEdG + (size_t)row_atom * nin + n0 + c0);
 #pragma unroll
@@ -972,29 +1086,32 @@ k_mlp_tcs(MlpTcArgs a) {
                  "r"(kTcsTmemCols));
 }
 
-size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int *stages) {
+size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int tf32, int *stages) {
   *stages = 0;
   if (resnet || nl < 2 || nl - 1 > kMaxLayers) return 0;
+  const int kc = tf32 ? OpTf32::KC : OpBf16::KC;
+  const size_t esz = tf32 ? 4 : 2;
   const int nin = sizes[0];
-  int maxh = 1, acts = 0;
+  int maxh = 1, acts = 0;  // act' columns: every hidden layer but the last
   for (int l = 1; l < nl; l++) {
-    if (sizes[l] % KCH != 0 || sizes[l] > 256) return 0;
+    if (sizes[l] % kc != 0 || sizes[l] > 256) return 0;
     maxh = maxh > sizes[l] ? maxh : sizes[l];
-    acts += sizes[l];
+    if (l < nl - 1) acts += sizes[l];
   }
-  if (nin % KCH != 0) return 0;
+  if (nin % kc != 0) return 0;
   const int nb = np == 3 ? 2 : 1;
-  const TcsPlan pl = tcs_plan(nin, maxh, nb);
-  if (pl.accw + acts > kTcsTmemCols) return 0;
+  const TcsPlan pl = tcs_plan(nin, maxh, nb, kc);
+  const bool split = tf32 && np == 3;  // D_hi and D_lo accumulators
+  if ((split ? 2 : 1) * pl.accw + acts > kTcsTmemCols) return 0;
   // chunk schedule length
   int nq = 0;
-  for (int l = 0; l < nl - 1; l++) nq += sizes[l] / KCH;
-  for (int l = nl - 2; l >= 1; l--) nq += sizes[l + 1] / KCH;
-  nq += ((nin + 127) / 128) * (sizes[1] / KCH);
+  for (int l = 0; l < nl - 1; l++) nq += sizes[l] / kc;
+  for (int l = nl - 2; l >= 1; l--) nq += sizes[l + 1] / kc;
+  nq += ((nin + 127) / 128) * (sizes[1] / kc);
   if (nq > kTcsMaxChunks) return 0;
   // as many stages as fit next to the operand region and ~12 KB of static data
   const size_t limit = 227 * 1024 - 12 * 1024;
-  const size_t abytes = (size_t)nb * pl.a_elems * 2, sbytes = (size_t)pl.stage_elems * 2;
+  const size_t abytes = (size_t)nb * pl.a_elems * esz, sbytes = (size_t)pl.stage_elems * esz;
   if (abytes + 2 * sbytes > limit) return 0;
   int S = (int)((limit - abytes) / sbytes);
   if (S > kTcsMaxStages) S = kTcsMaxStages;
@@ -1002,10 +1119,23 @@ size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int *stages) {
   return abytes + (size_t)S * sbytes;
 }
 
-void mlp_tcs_prepare(size_t smem, int np) {
+int mlp_tcs_hi2(int nl, const int *sizes, int np, int tf32) {
+  // room in TMEM for a second hi accumulator next to D_hi, D_lo and act'
+  if (!(tf32 && np == 3)) return 0;
+  int maxh = 1, acts = 0;
+  for (int l = 1; l < nl; l++) {
+    maxh = maxh > sizes[l] ? maxh : sizes[l];
+    if (l < nl - 1) acts += sizes[l];
+  }
+  const TcsPlan pl = tcs_plan(sizes[0], maxh, 2, OpTf32::KC);
+  return 3 * pl.accw + acts <= kTcsTmemCols ? 1 : 0;
+}
+
+void mlp_tcs_prepare(size_t smem, int np, int tf32) {
   const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  if (np == 3) cudaFuncSetAttribute(k_mlp_tcs<3>, at, (int)smem);
-  else cudaFuncSetAttribute(k_mlp_tcs<1>, at, (int)smem);
+  if (tf32) cudaFuncSetAttribute(k_mlp_tcs<3, OpTf32>, at, (int)smem);
+  else if (np == 3) cudaFuncSetAttribute(k_mlp_tcs<3, OpBf16>, at, (int)smem);
+  else cudaFuncSetAttribute(k_mlp_tcs<1, OpBf16>, at, (int)smem);
 }
 
 size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np, bool dz_bf16) {
@@ -1036,6 +1166,35 @@ void pack_core_chunks(const float *src, int rows, int cols, long ld_r, long ld_k
         size_t off = (size_t)c * rows * KCH +
                      (size_t)(((r >> 3) * (KCH / EPC) + kk / EPC) * (8 * EPC) + (r & 7) * EPC + kk % EPC);
         dst[off] = bits;
+      }
+}
+
+float tf32_round_host(float v) {
+  // round to the 10-bit TF32 mantissa, ties away from zero (as cvt.rna)
+  uint32_t b;
+  memcpy(&b, &v, 4);
+  if ((b & 0x7f800000u) != 0x7f800000u) b = (b + 0x1000u) & 0xffffe000u;
+  float r;
+  memcpy(&r, &b, 4);
+  return r;
+}
+
+void pack_core_chunks_tf32(const float *src, int rows, int cols, long ld_r, long ld_k, int part,
+                           float *dst) {
+  // chunks of 32 columns; inside a chunk the element (r, k) sits at
+  // ((r/8) * 8 + k/4) * 32 + (r%8) * 4 + k%4; part 0 = hi = tf32(v),
+  // part 1 = lo = tf32(v - hi)
+  constexpr int kc = OpTf32::KC, epc = OpTf32::EPC;
+  const int nch = (cols + kc - 1) / kc;
+  for (int c = 0; c < nch; c++)
+    for (int r = 0; r < rows; r++)
+      for (int kk = 0; kk < kc; kk++) {
+        const int k = c * kc + kk;
+        const float v = k < cols ? src[(long)r * ld_r + (long)k * ld_k] : 0.f;
+        const float hi = tf32_round_host(v);
+        const size_t off = (size_t)c * rows * kc +
+                           (size_t)(((r >> 3) * (kc / epc) + kk / epc) * (8 * epc) + (r & 7) * epc + kk % epc);
+        dst[off] = part == 0 ? hi : tf32_round_host(v - hi);
       }
 }
 
@@ -1071,8 +1230,9 @@ void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches) {
   if (a.ntiles <= 0) return;
   if (a.streamed > 0) {
     const int grid = a.ntiles < a.streamed ? a.ntiles : a.streamed;
-    if (a.np == 3) k_mlp_tcs<3><<<grid, kTcsThreads, a.smem_s, st>>>(a);
-    else k_mlp_tcs<1><<<grid, kTcsThreads, a.smem_s, st>>>(a);
+    if (a.tf32) k_mlp_tcs<3, OpTf32><<<grid, kTcsThreads, a.smem_s, st>>>(a);
+    else if (a.np == 3) k_mlp_tcs<3, OpBf16><<<grid, kTcsThreads, a.smem_s, st>>>(a);
+    else k_mlp_tcs<1, OpBf16><<<grid, kTcsThreads, a.smem_s, st>>>(a);
     launches += 1;
     return;
   }

@@ -229,7 +229,8 @@ HostModel parse_model(const std::string &coeff_args) {
       else if (c == "bf16") h.precision = 1;
       else if (c == "fp8") h.precision = 2;
       else if (c == "bf16x3") h.precision = 3;
-      else bad("precision must be fp32, bf16, bf16x3 or fp8");
+      else if (c == "tf32x3") h.precision = 4;
+      else bad("precision must be fp32, tf32x3, bf16, bf16x3 or fp8");
       read_elt = false;
       i += 2;
     } else if (read_elt) {

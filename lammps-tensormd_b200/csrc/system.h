@@ -25,6 +25,8 @@ struct tmd_model {
   bool tc_dz_bf16 = false;
   int tc_np = 1;
   bool tc_fp8 = false;   // FP8 (e4m3) tensor-core MLP
+  bool tc_tf32 = false;  // 3xTF32 tensor-core MLP (streamed form)
+  int tc_hi2 = 0;        // its second hi accumulator (TMEM permitting)
   int tc_persistent = 0; // > 0: weight-resident persistent tensor-core MLP (grid size)
   size_t tc_smem_p = 0;
   bool tc_dz_bf16_p = false;

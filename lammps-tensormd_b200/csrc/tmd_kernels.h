@@ -147,8 +147,10 @@ void mlp_fp32s_pack(const float *W, int K, int N, std::vector<float> &fwd,
                     std::vector<float> &bwd);
 void mlp_fp32s_prepare(size_t smem);
 
-// Tensor-core (tcgen05) MLP, BF16 operands.  Weights are packed on the host
-// in 64-column chunks of the K-major core-matrix layout (pack_core_chunks).
+// Tensor-core (tcgen05) MLP, BF16 operands (TF32 in the 3xTF32 streamed
+// form).  Weights are packed on the host in chunks of the K-major
+// core-matrix layout: 64 BF16 columns (pack_core_chunks) or 32 TF32 columns
+// (pack_core_chunks_tf32).
 struct MlpTcLayer {
   int K, N;
   const void *Wf;    // forward B = W^T: N rows x K cols (bf16, packed; the lo
@@ -170,6 +172,8 @@ struct MlpTcArgs {
   size_t smem;
   int dz_bf16;
   int np;  // 1: BF16 products; 3: split BF16 (hi*hi + hi*lo + lo*hi)
+  int tf32;  // 1: split TF32 operands (3xTF32, np = 3; streamed form only)
+  int hi2;   // 3xTF32: a second accumulator for the odd K steps' hi products
   int persistent;     // > 0: weight-resident persistent form on this many CTAs
   size_t smem_p;      // its dynamic shared memory
   int dz_bf16_p;      // its act' in BF16 (BF16 form only, when FP32 does not fit)
@@ -217,15 +221,23 @@ size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np, bool dz_bf16);
 void mlp_tcp_prepare(size_t smem, int np, bool dz_bf16);
 // Streamed-weight persistent form (weights too large to stay in shared
 // memory): dynamic shared memory and weight stages, 0 if unsupported
-// (residual layers, widths not multiples of 64 or above 256, act' beyond 512
-// TMEM columns).
-size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int *stages);
-void mlp_tcs_prepare(size_t smem, int np);
+// (residual layers, widths not multiples of the chunk (64 BF16 / 32 TF32
+// columns) or above 256, act' beyond 512 TMEM columns).  tf32 = 1: the
+// 3xTF32 operand format.
+size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int tf32, int *stages);
+void mlp_tcs_prepare(size_t smem, int np, int tf32);
+// 3xTF32: 1 when TMEM holds a second hi accumulator (MlpTcArgs::hi2).
+int mlp_tcs_hi2(int nl, const int *sizes, int np, int tf32);
 
 // Host: pack a rows x cols matrix (element (r, k) = src[r * ld_r + k * ld_k])
 // into 64-column chunks of 8x8 BF16 core matrices, K-major.
 void pack_core_chunks(const float *src, int rows, int cols, long ld_r, long ld_k,
                       uint16_t *dst);
+// Host: the same into 32-column chunks of 8x4 TF32 core matrices; part 0 =
+// hi = tf32(v), part 1 = lo = tf32(v - hi) (round to nearest, ties away).
+void pack_core_chunks_tf32(const float *src, int rows, int cols, long ld_r, long ld_k, int part,
+                           float *dst);
+float tf32_round_host(float v);
 
 // FP8 (e4m3) form of the tensor-core MLP (mlp_fp8.cu): same arguments, packed
 // weights e4m3(W * wscale) in 8x16 core matrices, per-row operand scales.

@@ -10,7 +10,8 @@ FP64 oracle on the same positions.
             multi-wave grid.
   alloy432k 432,000-atom 4-element random FCC alloy (a = 3.6 A, 60x60x30
             cells), 32 Gaussians rc 6.5 A, MLP 512-128-128-128-1 softplus:
-            one evaluation per MLP form against one oracle evaluation.
+            one evaluation per MLP form against one oracle evaluation (the
+            plain FP32 and the 3xTF32 tensor-core MLP at the plain bars).
   cells4096 4,096 cells x 256 atoms (half FCC, half BCC, 2 elements): 16
             sampled cells against the oracle cell by cell, at the start and
             after the benchmark's 500 NVE steps.
@@ -85,6 +86,22 @@ def test_bcc128k_1000_steps_checked_every_100():
     print("bcc128k worst over 11 checkpoints:", worst)
 
 
+def test_bcc128k_tf32x3_against_the_oracle():
+    """The 3xTF32 tensor-core MLP at the headline size, at the plain-form bars
+    (one evaluation on the starting positions)."""
+    p, syms, x, t, box, v = _system("bcc128k")
+    n = len(x)
+    m = TensorMDModel(f"{p} {' '.join(syms)} precision tf32x3")
+    s = TensorMDSystem(m, n, 1.0)
+    s.set_box(box)
+    s.set_atoms(x, t, v)
+    out = s.compute(1, 1)
+    ref = Oracle(load_npz(p)).compute(x, t - 1, box, [1, 1, 1])
+    err = _errors(out, ref, n)
+    print("bcc128k tf32x3:", err)
+    _assert_plain(err, vir_rel=2e-5)
+
+
 def test_alloy432k_every_form_against_the_oracle():
     """The error table of the precision config: energy, force and virial of
     every MLP form against one FP64 oracle evaluation on the same positions
@@ -98,7 +115,7 @@ def test_alloy432k_every_form_against_the_oracle():
     ref = Oracle(load_npz(p)).compute(x, t - 1, box, [1, 1, 1])
     table = {"config": "alloy432k", "natoms": n,
              "rms_force_eV_per_A": float(np.sqrt(np.mean(ref["f"] ** 2)))}
-    for prec in ("fp32", "bf16x3", "bf16", "fp8"):
+    for prec in ("fp32", "tf32x3", "bf16x3", "bf16", "fp8"):
         suffix = "" if prec == "fp32" else f" precision {prec}"
         m = TensorMDModel(f"{p} {' '.join(syms)}{suffix}")
         s = TensorMDSystem(m, n, 1.0)
@@ -106,7 +123,7 @@ def test_alloy432k_every_form_against_the_oracle():
         s.set_atoms(x, t)
         err = _errors(s.compute(1, 1), ref, n)
         table[prec] = err
-        if prec == "fp32":
+        if prec in ("fp32", "tf32x3"):
             _assert_plain(err)
         elif prec == "fp8":
             assert np.isfinite(err["force_rms"]) and err["force_rms"] < 1.0, err
