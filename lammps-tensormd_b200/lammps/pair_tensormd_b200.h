@@ -3,7 +3,7 @@
  * Same input grammar as pair_style tensormd (src/ML-TENSORMD/pair_tensormd.h:16-83):
  *   pair_style tensormd/b200
  *   pair_coeff * * file.npz El1 El2 ... [interp dx] [cmax exact|default]
- *              [precision fp32|bf16|bf16x3]
+ *              [precision fp32|tf32x3|bf16|bf16x3|fp8]
  * The force evaluation runs in libtmd_b200.so (include/tmd_b200.h), which
  * builds its own neighbor list.  On one MPI rank the device handles the
  * periodic images and the style writes forces on local atoms; on several
