@@ -1085,7 +1085,10 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
       int nsm = 0;
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
       if (sp > 0 && sp <= kLimit && nsm > 0) {
-        m->tc_persistent = nsm;
+        // two CTAs per SM where both fit (228 KB per SM, 1 KB reserved and
+        // ~3 KB of static data per CTA): one CTA's epilogue and barriers
+        // overlap the other's MMAs
+        m->tc_persistent = 2 * (sp + 4 * 1024) <= 228 * 1024 ? 2 * nsm : nsm;
         m->tc_smem_p = sp;
         m->tc_dz_bf16_p = dzb;
         mlp_tcp_prepare(sp, np, dzb);

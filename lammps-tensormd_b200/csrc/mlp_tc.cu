@@ -348,10 +348,12 @@ k_mlp_tcp(MlpTcArgs a) {
   T *actb = wsm + tcp_weight_elems(L, sizes, NB);
   const size_t act_lo = (size_t)TM * maxw;
   DZ *dzb = reinterpret_cast<DZ *>(actb + NB * act_lo);  // act' [layer][column][row]
-  size_t dzoff[kMaxLayers];
+  // act' of every hidden layer but the last (whose act' is folded into the
+  // gradient seed in its forward epilogue)
+  size_t dzoff[kMaxLayers] = {};
   {
     size_t o = 0;
-    for (int l = 0; l < L - 1; l++) { dzoff[l] = o; o += (size_t)sizes[l + 1] * TM; }
+    for (int l = 0; l < L - 2; l++) { dzoff[l] = o; o += (size_t)sizes[l + 1] * TM; }
   }
 
   if (warp == 0) {
@@ -1146,7 +1148,7 @@ size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np, bool dz_bf16) 
   const int maxw = sizes[0] > maxh ? sizes[0] : maxh;
   size_t b = tcp_weight_elems(nl, sizes, (int)nb) * 2;  // resident W^T and W blocks
   b += nb * (size_t)TM * maxw * 2;                      // operand buffer
-  for (int l = 1; l < nl; l++) b += (size_t)sizes[l] * TM * (dz_bf16 ? 2 : 4);  // act'
+  for (int l = 1; l < nl - 1; l++) b += (size_t)sizes[l] * TM * (dz_bf16 ? 2 : 4);  // act'
   return b;
 }
 
