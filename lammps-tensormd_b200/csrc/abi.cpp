@@ -323,6 +323,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   int maxh = 1;
   for (int l = 1; l < m->h.nl; l++) maxh = std::max(maxh, m->h.sizes[l]);
   ma.maxh = maxh; ma.tr = m->mlp_tr; ma.smem = m->mlp_smem; ma.resident = m->mlp_resident;
+  ma.warped = m->mlp_warped;
   ma.streamed = m->mlp_streamed; ma.stages = m->mlp_stages; ma.status = s->status;
   ma.ntiles = s->ntiles; ma.tiles = s->tiles; ma.perm = s->perm; ma.G = s->G;
   ma.dEdG = s->dEdG; ma.E = s->E; ma.layers = m->d_layers;
@@ -864,7 +865,9 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     *out = m;
     return TMD_OK;
   }
-  // MLP: the resident-weight form (one persistent CTA per SM) when the
+  // MLP: with 64-wide hidden layers and no residual layers the warp-tile
+  // form (a warp per 32 atoms, the element's weights in shared memory);
+  // else the resident-weight form (one persistent CTA per SM) when the
   // element's hidden weights and a tile's activations fit in shared memory
   // (128-atom tiles, else 64); else the persistent streamed-weight form
   // (64-atom tiles, weight chunks copied through a stage ring); else, for
@@ -876,7 +879,18 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
   const size_t sres64 = mlp_fp32r_smem(h.nl, h.sizes.data(), 64);
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
-  if (h.nl >= 2 && sres <= 227 * 1024 && nsm > 0) {
+  int wt_warps = 0;
+  size_t swt = 0;
+  for (int nw = 16; nw >= 8 && wt_warps == 0; nw--) {
+    swt = mlp_fp32w_smem(h.nl, h.sizes.data(), h.resnet, nw);
+    if (swt > 0 && swt <= 227 * 1024) wt_warps = nw;
+  }
+  if (wt_warps > 0 && nsm > 0) {
+    // 64-wide hidden layers: the warp-tile form, one CTA of wt_warps warps
+    // per SM, tiles of mlp_fp32w_rows() atoms per warp
+    m->mlp_tr = mlp_fp32w_rows() * wt_warps; m->mlp_smem = swt; m->mlp_resident = nsm;
+    m->mlp_warped = wt_warps;
+  } else if (h.nl >= 2 && sres <= 227 * 1024 && nsm > 0) {
     m->mlp_tr = 128; m->mlp_smem = sres; m->mlp_resident = nsm;
   } else if (h.nl >= 2 && sres64 <= 227 * 1024 && nsm > 0) {
     m->mlp_tr = 64; m->mlp_smem = sres64; m->mlp_resident = nsm;
@@ -912,7 +926,8 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     tmd_model_free(m);
     return fail(TMD_ERR_MODEL, "MLP too wide for the shared-memory tile");
   }
-  if (m->mlp_streamed == 0) mlp_fp32_prepare(m->mlp_tr, m->mlp_smem, m->mlp_resident > 0);
+  if (m->mlp_warped > 0) mlp_fp32w_prepare(m->mlp_smem);
+  else if (m->mlp_streamed == 0) mlp_fp32_prepare(m->mlp_tr, m->mlp_smem, m->mlp_resident > 0);
   for (int l = 1; l < h.nl; l++) m->maxh = std::max(m->maxh, h.sizes[l]);
   if (h.precision == TMD_PREC_TF32X3) {
     // 3xTF32 on tcgen05 (streamed form): W as hi = tf32(W) and lo =

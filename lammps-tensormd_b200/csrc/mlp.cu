@@ -559,6 +559,322 @@ k_mlp_fp32r(MlpArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Warp-tile form (k_mlp_fp32w) for MLPs with 64-wide hidden layers and no
+// residual layers (the 64-64 nets of the benchmark, batch and serving
+// configs).  In the resident form a thread's 4 x 4 register tile takes two
+// 16-byte shared-memory loads per 16 FMAs, so the GEMMs wait on shared memory
+// about as long as on the FMA pipe, and 16 warps meet at a block barrier
+// after every layer.  Here each warp owns a tile of 16 atoms from start to
+// end (no block barrier except when the element changes): lane (ty, tx) =
+// (lane / 8, lane % 8) owns rows ty + 4 i (i < 4) and 8 columns of each
+// 64-column GEMM, a 4 x 8 register tile fed by three 16-byte loads per k step
+// for 32 FMAs.  Forward columns are 4 tx + j and 32 + 4 tx + j (j < 4: one
+// 128-byte row segment per warp load); backward outputs k = k0 + tx + 8 j (W
+// rows of the 8 tx lanes 4 banks apart).  The G rows of a tile are copied to
+// the warp's area with cp.async (zero-filled past the last atom; the next
+// tile's rows prefetched to L2 one tile ahead); every hidden output is formed
+// in registers before it overwrites the GEMM's input in place, and the
+// activation runs as a short loop over the lane's own four-column groups.
+// Each output is summed over the reduction index in ascending order with the
+// FMAs of the resident form (same dE/dG bits); the output layer in FP64,
+// summed over a lane's four columns and across the 8 lanes of a row, the two
+// column halves in order.
+// ---------------------------------------------------------------------------
+constexpr int kWtRI = 4;                 // rows per lane
+constexpr int kWtRows = 4 * kWtRI;       // atoms per warp tile
+constexpr int kWtThreads = 512;          // 16 warps per CTA
+constexpr int kWtWidth = 64;             // hidden width this form supports
+
+struct WtLayout {
+  int woff[kMaxLayers], ldw[kMaxLayers], boff[kMaxLayers];
+  int wsf, wsd, ef;  // FP32 / FP64 row sums of W_out; floats of the element block
+  int ldg, ldh, wf;  // G and hidden row strides; floats per warp area
+};
+
+__host__ __device__ inline WtLayout wt_layout(int nl, const int *sizes) {
+  WtLayout r{};
+  int o = 0;
+  for (int l = 0; l < nl - 1; l++) {
+    r.ldw[l] = sizes[l + 1] + 4;
+    r.woff[l] = o;
+    o += sizes[l] * r.ldw[l];
+  }
+  for (int l = 0; l < nl - 1; l++) { r.boff[l] = o; o += round_up(sizes[l + 1], 4); }
+  r.wsf = o; o += round_up(sizes[nl - 1], 4);
+  r.wsd = o; o += 2 * round_up(sizes[nl - 1], 2);
+  r.ef = round_up(o, 4);
+  r.ldg = round_up(sizes[0], 4) + 4;
+  r.ldh = kWtWidth + 4;
+  // G staging and the hidden buffers (output / gradient, then act' of every
+  // hidden layer but the last) share the warp area
+  const int gfl = kWtRows * r.ldg, hfl = (nl - 1) * kWtRows * r.ldh;
+  r.wf = round_up(gfl > hfl ? gfl : hfl, 4) + 2 * kWtRows;  // + FP64 row energies
+  return r;
+}
+
+// out(r_i, c0 + col_j) = sum_k A[r_i][k] W[k][c0 + col_j], k ascending.
+__device__ __forceinline__ void wt_gemm_fwd(const float *A, int lda, int K, const float *W,
+                                            int ldw, int ty, int tx, float (&acc)[kWtRI][8]) {
+  const float *ap = A + ty * lda;
+  const float *wp = W + 4 * tx;
+#pragma unroll 2
+  for (int k = 0; k < K; k += 4) {
+    float4 av[kWtRI], b0[4], b1[4];
+#pragma unroll
+    for (int i = 0; i < kWtRI; i++) av[i] = *reinterpret_cast<const float4 *>(ap + 4 * i * lda + k);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      b0[q] = *reinterpret_cast<const float4 *>(wp + (k + q) * ldw);
+      b1[q] = *reinterpret_cast<const float4 *>(wp + (k + q) * ldw + 32);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const float bq[8] = {b0[q].x, b0[q].y, b0[q].z, b0[q].w, b1[q].x, b1[q].y, b1[q].z, b1[q].w};
+#pragma unroll
+      for (int i = 0; i < kWtRI; i++) {
+        const float x = q == 0 ? av[i].x : (q == 1 ? av[i].y : (q == 2 ? av[i].z : av[i].w));
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(x, bq[j], acc[i][j]);
+      }
+    }
+  }
+}
+
+// out(r_i, k_j) = sum_c A[r_i][c] W[k_j][c], c ascending, k_j = k0 + tx + 8 j.
+__device__ __forceinline__ void wt_gemm_bwd(const float *A, int lda, int N, const float *W,
+                                            int ldw, int k0, int Kout, int ty, int tx,
+                                            float (&acc)[kWtRI][8]) {
+  const float *ap = A + ty * lda;
+  const float *wr[8];
+  bool kv[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int k = k0 + tx + 8 * j;
+    kv[j] = k < Kout;
+    wr[j] = W + (kv[j] ? k : 0) * ldw;
+  }
+#pragma unroll 2
+  for (int c = 0; c < N; c += 4) {
+    float4 av[kWtRI], wv[8];
+#pragma unroll
+    for (int i = 0; i < kWtRI; i++) av[i] = *reinterpret_cast<const float4 *>(ap + 4 * i * lda + c);
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+      wv[j] = kv[j] ? *reinterpret_cast<const float4 *>(wr[j] + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int i = 0; i < kWtRI; i++) {
+        const float x = q == 0 ? av[i].x : (q == 1 ? av[i].y : (q == 2 ? av[i].z : av[i].w));
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const float wq = q == 0 ? wv[j].x : (q == 1 ? wv[j].y : (q == 2 ? wv[j].z : wv[j].w));
+          acc[i][j] = fmaf(x, wq, acc[i][j]);
+        }
+      }
+  }
+}
+
+template <int ACT>
+__global__ void __launch_bounds__(kWtThreads, 1)
+k_mlp_fp32w(MlpArgs a) {
+  extern __shared__ float4 smw4[];
+  float *sm = reinterpret_cast<float *>(smw4);
+  const int L = a.nl, nin = a.nin;
+  int sizes[kMaxLayers + 1];
+  sizes[0] = nin;
+  for (int l = 0; l < L; l++) sizes[l + 1] = a.layers[l].N;
+  const WtLayout lay = wt_layout(L, sizes);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ty = lane >> 3, tx = lane & 7;
+  const int ldh = lay.ldh, ldg = lay.ldg;
+  float *wa = sm + lay.ef + w * lay.wf;  // this warp's area
+  float *x1 = wa;                        // hidden output / gradient [32][ldh]
+  float *dzb = wa + kWtRows * ldh;       // act' of hidden layer l at dzb + l * 32 * ldh
+  double *erow = reinterpret_cast<double *>(wa + lay.wf - 2 * kWtRows);  // row energies
+  const float *wsf = sm + lay.wsf;
+  const double *wsd = reinterpret_cast<const double *>(sm + lay.wsd);
+  int cur_elt = -1;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const int elt = a.tiles[3 * tile], start = a.tiles[3 * tile + 1],
+              count = a.tiles[3 * tile + 2];
+    if (elt != cur_elt) {  // the same for every warp of the block
+      __syncthreads();     // every warp is done with the previous element's weights
+      cur_elt = elt;
+      const MlpLayer *Ls = a.layers + (size_t)elt * L;
+      for (int l = 0; l < L - 1; l++) {
+        const int K = Ls[l].K, N = Ls[l].N, ldw = lay.ldw[l];
+        float *Wd = sm + lay.woff[l];
+        if ((reinterpret_cast<uintptr_t>(Ls[l].W) & 15) == 0) {
+          // rows of N = 64 floats as 16-byte vectors (the 4 pad columns unused)
+          const int n4 = N >> 2;
+          for (int idx = threadIdx.x; idx < K * n4; idx += blockDim.x) {
+            const int k = idx / n4, c4 = idx - k * n4;
+            *reinterpret_cast<float4 *>(Wd + k * ldw + 4 * c4) =
+                __ldg(reinterpret_cast<const float4 *>(Ls[l].W + (size_t)k * N) + c4);
+          }
+        } else {
+          for (int idx = threadIdx.x; idx < K * ldw; idx += blockDim.x) {
+            const int k = idx / ldw, c = idx - k * ldw;
+            Wd[idx] = c < N ? __ldg(Ls[l].W + (size_t)k * N + c) : 0.f;
+          }
+        }
+        float *bd = sm + lay.boff[l];
+        for (int c = threadIdx.x; c < N; c += blockDim.x) bd[c] = Ls[l].b ? __ldg(Ls[l].b + c) : 0.f;
+      }
+      const MlpLayer lo = Ls[L - 1];
+      double *wsdw = reinterpret_cast<double *>(sm + lay.wsd);
+      for (int k = threadIdx.x; k < lo.K; k += blockDim.x) {
+        double sd = 0.0;
+        float sf = 0.f;
+        for (int o2 = 0; o2 < lo.N; o2++) {
+          sd += __ldg(lo.Wd + (size_t)k * lo.N + o2);
+          sf += __ldg(lo.W + (size_t)k * lo.N + o2);
+        }
+        wsdw[k] = sd;
+        sm[lay.wsf + k] = sf;
+      }
+      __syncthreads();
+    }
+    const int r0 = kWtRows * w;  // the warp's first row of the tile
+    {
+      // the next tile's G rows of this warp into L2 while this one runs
+      const int nt = tile + gridDim.x;
+      if (nt < a.ntiles) {
+        const int ns = a.tiles[3 * nt + 1], nc = a.tiles[3 * nt + 2];
+        if (lane < kWtRows && r0 + lane < nc) {
+          const char *p = reinterpret_cast<const char *>(a.G + (size_t)a.perm[ns + r0 + lane] * nin);
+          for (int off = 0; off < nin * 4; off += 128)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(p + off));
+        }
+      }
+    }
+    if (r0 >= count) continue;
+    // lane r < kWtRows holds the atom of row r (-1 past the last atom)
+    const int prow = lane < kWtRows && r0 + lane < count ? a.perm[start + r0 + lane] : -1;
+    int at[kWtRI];
+#pragma unroll
+    for (int i = 0; i < kWtRI; i++) at[i] = __shfl_sync(0xffffffffu, prow, ty + 4 * i);
+    // G rows of the tile into the warp area (row stride ldg), zero past the
+    // last atom
+    {
+      const int nq = nin >> 2, total = kWtRows * nq;
+      for (int base = 0; base < total; base += 32) {  // the same trip count in every lane
+        const int idx = base + lane;
+        const int r = idx < total ? idx / nq : 0, q = idx - r * nq;
+        const int atr = __shfl_sync(0xffffffffu, prow, r);
+        if (idx < total) {
+          const float *src = a.G + (size_t)(atr >= 0 ? atr : 0) * nin + 4 * q;
+          const uint32_t dst = tc::smem_u32(wa + r * ldg + 4 * q);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+                       "r"(atr >= 0 ? 16 : 0));
+        }
+      }
+      asm volatile("cp.async.commit_group;");
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+      __syncwarp();
+    }
+    // ---------------- forward ----------------
+    for (int l = 0; l < L - 1; l++) {
+      float acc[kWtRI][8];
+#pragma unroll
+      for (int i = 0; i < kWtRI; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+      wt_gemm_fwd(wa, l == 0 ? ldg : ldh, sizes[l], sm + lay.woff[l], lay.ldw[l], ty, tx, acc);
+      __syncwarp();  // the input is read in full before the outputs overwrite it
+      const float *bias = sm + lay.boff[l];
+      // z = acc + b into the hidden buffer; the activation then runs as a
+      // short loop over the lane's own four-column groups (the unrolled
+      // register form would inline the activation 4 kWtRI times)
+#pragma unroll
+      for (int i = 0; i < kWtRI; i++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int r = ty + 4 * i, c = 32 * h + 4 * tx;
+          *reinterpret_cast<float4 *>(x1 + r * ldh + c) =
+              make_float4(acc[i][4 * h] + bias[c], acc[i][4 * h + 1] + bias[c + 1],
+                          acc[i][4 * h + 2] + bias[c + 2], acc[i][4 * h + 3] + bias[c + 3]);
+        }
+      const bool last = l == L - 2;
+      float *dz = dzb + (size_t)l * kWtRows * ldh;
+#pragma unroll 1
+      for (int ih = 0; ih < 2 * kWtRI; ih++) {
+        const int r = ty + 4 * (ih >> 1), c = 32 * (ih & 1) + 4 * tx;
+        const float4 z4 = *reinterpret_cast<const float4 *>(x1 + r * ldh + c);
+        float y[4], d[4];
+        y[0] = act_fwd(ACT, z4.x, d[0]);
+        y[1] = act_fwd(ACT, z4.y, d[1]);
+        y[2] = act_fwd(ACT, z4.z, d[2]);
+        y[3] = act_fwd(ACT, z4.w, d[3]);
+        if (!last) {
+          *reinterpret_cast<float4 *>(x1 + r * ldh + c) = make_float4(y[0], y[1], y[2], y[3]);
+          *reinterpret_cast<float4 *>(dz + r * ldh + c) = make_float4(d[0], d[1], d[2], d[3]);
+        } else {
+          // output layer in FP64 (the row's two column halves, each summed
+          // over the 8 lanes of the row); gradient seed = row sums of W_out
+          // times act'
+          double p = 0.0;
+#pragma unroll
+          for (int u = 0; u < 4; u++) p = fma((double)y[u], wsd[c + u], p);
+          p += __shfl_xor_sync(0xffffffffu, p, 1);
+          p += __shfl_xor_sync(0xffffffffu, p, 2);
+          p += __shfl_xor_sync(0xffffffffu, p, 4);
+          if (tx == 0) erow[r] = (ih & 1) ? erow[r] + p : p;
+          *reinterpret_cast<float4 *>(x1 + r * ldh + c) =
+              make_float4(d[0] * wsf[c], d[1] * wsf[c + 1], d[2] * wsf[c + 2], d[3] * wsf[c + 3]);
+        }
+      }
+      __syncwarp();
+    }
+    {
+      const MlpLayer lo = a.layers[(size_t)elt * L + L - 1];
+      double eb = 0.0;
+      if (lo.bd)
+        for (int o2 = 0; o2 < lo.N; o2++) eb += __ldg(lo.bd + o2);
+      if (prow >= 0) a.E[prow] = erow[lane] + eb;  // prow >= 0 only for lanes < kWtRows
+    }
+    // ---------------- backward ----------------
+    for (int l = L - 2; l >= 0; l--) {
+      const int K = sizes[l];
+      for (int k0 = 0; k0 < K; k0 += 64) {
+        float acc[kWtRI][8];
+#pragma unroll
+        for (int i = 0; i < kWtRI; i++)
+#pragma unroll
+          for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+        wt_gemm_bwd(x1, ldh, sizes[l + 1], sm + lay.woff[l], lay.ldw[l], k0, K, ty, tx, acc);
+        if (l == 0) {
+#pragma unroll
+          for (int i = 0; i < kWtRI; i++) {
+            if (at[i] < 0) continue;
+            float *dst = a.dEdG + (size_t)at[i] * nin;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              const int k = k0 + tx + 8 * j;
+              if (k < K) dst[k] = acc[i][j];
+            }
+          }
+        } else {
+          __syncwarp();  // the gradient is read in full before it is overwritten
+          const float *dz = dzb + (size_t)(l - 1) * kWtRows * ldh;
+#pragma unroll
+          for (int i = 0; i < kWtRI; i++) {
+            const int r = ty + 4 * i;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              const int k = tx + 8 * j;
+              x1[r * ldh + k] = dz[r * ldh + k] * acc[i][j];
+            }
+          }
+          __syncwarp();
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Streamed-weight form (k_mlp_fp32s) for MLPs whose weights do not fit in
 // shared memory (e.g. 512-128-128-128 per element: 393 KB of FP32 W per
 // direction).  Persistent CTAs of 256 threads walk 64-atom tiles.  Every GEMM
@@ -860,6 +1176,25 @@ size_t mlp_fp32r_smem(int nl, const int *sizes, int tr) {
   return sizeof(float) * (size_t)res_layout(nl, sizes, tr).total;
 }
 
+int mlp_fp32w_rows() { return kWtRows; }
+
+size_t mlp_fp32w_smem(int nl, const int *sizes, int resnet, int warps) {
+  if (resnet || nl < 2 || nl - 1 > kMaxLayers || warps < 1 || 32 * warps > kWtThreads) return 0;
+  if (sizes[0] % 4 != 0 || sizes[0] < 4) return 0;
+  for (int l = 1; l < nl; l++)
+    if (sizes[l] != kWtWidth) return 0;
+  const WtLayout w = wt_layout(nl, sizes);
+  return sizeof(float) * ((size_t)w.ef + (size_t)warps * w.wf);
+}
+
+void mlp_fp32w_prepare(size_t smem) {
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaFuncSetAttribute(k_mlp_fp32w<0>, at, (int)smem);
+  cudaFuncSetAttribute(k_mlp_fp32w<1>, at, (int)smem);
+  cudaFuncSetAttribute(k_mlp_fp32w<2>, at, (int)smem);
+  cudaFuncSetAttribute(k_mlp_fp32w<3>, at, (int)smem);
+}
+
 size_t mlp_fp32s_smem(int nl, const int *sizes, int resnet, int *stages) {
   *stages = 0;
   if (resnet || nl < 2 || nl - 1 > kMaxLayers) return 0;
@@ -911,6 +1246,17 @@ void launch_mlp_fp32(const MlpArgs &a, cudaStream_t st, long &launches) {
   if (a.streamed > 0) {
     const int grid = a.ntiles < a.streamed ? a.ntiles : a.streamed;
     k_mlp_fp32s<<<grid, kFsThreads, a.smem, st>>>(a);
+    return;
+  }
+  if (a.warped > 0) {
+    const int grid = a.ntiles < a.resident ? a.ntiles : a.resident;
+    const int T = 32 * a.warped;
+    switch (a.actfn) {
+      case 0: k_mlp_fp32w<0><<<grid, T, a.smem, st>>>(a); break;
+      case 1: k_mlp_fp32w<1><<<grid, T, a.smem, st>>>(a); break;
+      case 2: k_mlp_fp32w<2><<<grid, T, a.smem, st>>>(a); break;
+      default: k_mlp_fp32w<3><<<grid, T, a.smem, st>>>(a); break;
+    }
     return;
   }
   if (a.resident > 0) {

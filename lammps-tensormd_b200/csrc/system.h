@@ -38,6 +38,7 @@ struct tmd_model {
   int mlp_tr = 64;
   size_t mlp_smem = 0;
   int mlp_resident = 0;    // > 0: resident-weight MLP, persistent grid size
+  int mlp_warped = 0;      // > 0: warp-tile MLP, warps per CTA (grid mlp_resident)
   int mlp_streamed = 0;    // > 0: streamed-weight FP32 MLP, persistent grid size
   int mlp_stages = 0;
   // temperature-dependent model (tdnp = 1): the nets' layers on the device

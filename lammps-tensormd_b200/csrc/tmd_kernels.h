@@ -121,6 +121,7 @@ struct MlpArgs {
   int tr;             // atoms per tile (32 or 64 streamed, 64 or 128 resident)
   size_t smem;        // dynamic shared memory bytes
   int resident;       // > 0: resident-weight form, persistent grid of this many CTAs
+  int warped;         // > 0: warp-tile form, this many warps per CTA (tiles of 32 per warp)
   int streamed;       // > 0: streamed-weight form, persistent grid of this many CTAs
   int stages;         // its weight-chunk stages
   int *status;        // timeout bit of the streamed form's bounded waits
@@ -138,6 +139,11 @@ size_t mlp_fp32_smem(int nl, const int *sizes, int tr);
 // Resident-weight form: shared memory per CTA for tiles of tr atoms (128
 // atoms on 512 threads, or 64 on 256 when the wider tile does not fit).
 size_t mlp_fp32r_smem(int nl, const int *sizes, int tr);
+// Warp-tile form (64-wide hidden layers, no residual layers): shared memory
+// per CTA of `warps` warps, 0 if the form does not apply.
+size_t mlp_fp32w_smem(int nl, const int *sizes, int resnet, int warps);
+int mlp_fp32w_rows();  // atoms per warp tile
+void mlp_fp32w_prepare(size_t smem);
 void mlp_fp32_prepare(int tr, size_t smem, bool resident);
 // Streamed-weight form (weights too large for shared memory): dynamic shared
 // memory and weight stages, 0 if unsupported (residual layers, widths not
