@@ -27,24 +27,26 @@ namespace tmd {
 
 constexpr int kPairThreads = 128;  // block size of the pair kernels
 
-// Geometry slot in shared memory: three 16-byte vectors per lane.
+// Geometry slot in shared memory: three 16-byte vectors per lane; the inputs
+// of the radial basis (r, r_lo, f_c, table offset) share the first, so the
+// per-pair radial of the descriptor reads one vector.
 struct GeoSlot {
-  float4 a;  // r, rlo, ux, uy
-  float4 b;  // uz, fc, dfc, tq
+  float4 a;  // r, rlo, fc, tq
+  float4 b;  // ux, uy, uz, dfc
   float4 c;  // ti (bits), neighbor slot t (bits), 1/r, unused
 };
 
 __device__ inline void geo_store(GeoSlot *s, const PairGeo &g, int t) {
-  s->a = make_float4(g.r, g.rlo, g.ux, g.uy);
-  s->b = make_float4(g.uz, g.fc, g.dfc, g.tq);
+  s->a = make_float4(g.r, g.rlo, g.fc, g.tq);
+  s->b = make_float4(g.ux, g.uy, g.uz, g.dfc);
   s->c = make_float4(__int_as_float(g.ti), __int_as_float(t), g.rinv, 0.f);
 }
 
 __device__ inline PairGeo geo_load(const GeoSlot *s) {
   PairGeo g;
   float4 a = s->a, b = s->b;
-  g.r = a.x; g.rlo = a.y; g.ux = a.z; g.uy = a.w;
-  g.uz = b.x; g.fc = b.y; g.dfc = b.z; g.tq = b.w;
+  g.r = a.x; g.rlo = a.y; g.fc = a.z; g.tq = a.w;
+  g.ux = b.x; g.uy = b.y; g.uz = b.z; g.dfc = b.w;
   const float4 c = s->c;
   g.ti = __float_as_int(c.x);
   g.rinv = c.z;
@@ -59,12 +61,12 @@ __device__ inline PairGeo geo_load_radial(const GeoSlot *s) {
   g.ux = g.uy = g.uz = g.dfc = g.rinv = 0.f;
   if (RK == kRadTable) {
     g.r = g.rlo = g.fc = 0.f;
-    g.tq = s->b.w;
+    g.tq = s->a.w;
     g.ti = __float_as_int(s->c.x);
   } else {
-    const float2 rr = *reinterpret_cast<const float2 *>(&s->a);
-    g.r = rr.x; g.rlo = rr.y;
-    g.fc = s->b.y;
+    const float4 a = s->a;
+    g.r = a.x; g.rlo = a.y;
+    g.fc = a.z;
     g.tq = 0.f;
     g.ti = 0;
   }
@@ -175,8 +177,8 @@ struct PairRing {
 template <int RK>
 __device__ inline void store_pair_geo(const GeoSlot *s, float4 *__restrict__ dst) {
   const float4 a = s->a, b = s->b, c = s->c;
-  dst[0] = a;
-  dst[1] = RK == kRadTable ? make_float4(b.x, b.w, c.x, c.y) : make_float4(b.x, b.y, b.z, c.y);
+  dst[0] = make_float4(a.x, a.y, b.x, b.y);
+  dst[1] = RK == kRadTable ? make_float4(b.z, a.w, c.x, c.y) : make_float4(b.z, a.z, b.w, c.y);
 }
 
 template <int RK>

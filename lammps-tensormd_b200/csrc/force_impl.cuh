@@ -170,12 +170,11 @@ k_force(KParams kp, BoxP box, int n, int cap, float scale,
       // virial, with the separation as r (hi + lo) times u
       if (sub < cnt) {
         const GeoSlot *s = pr.slot(sub);
-        const float4 ga = s->a;
-        const float uz = s->b.x;
+        const float4 ga = s->a, gb = s->b;
         const int t = __float_as_int(s->c.y);
         pdf_row[t] = make_float4(mydf.x, mydf.y, mydf.z, 0.f);
         double rr = (double)ga.x + (double)ga.y;
-        double rx = (double)ga.z * rr, ry = (double)ga.w * rr, rz = (double)uz * rr;
+        double rx = (double)gb.x * rr, ry = (double)gb.y * rr, rz = (double)gb.z * rr;
         w6[0] -= rx * mydf.x;
         w6[1] -= ry * mydf.y;
         w6[2] -= rz * mydf.z;
