@@ -43,6 +43,16 @@ int fail(int code, const std::string &msg) {
 void drop_graph(tmd_system *s) {
   if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
   s->step_exec = nullptr;
+  if (s->pos_exec) cudaGraphExecDestroy(s->pos_exec);
+  s->pos_exec = nullptr;
+}
+
+// Rebuild kernels counted for the set_positions graphs launched since the
+// last read of the device rebuild counter (rb: its current value).
+void account_pos_rebuilds(tmd_system *s, int rb) {
+  if (s->pos_pending) s->launches += (long)(rb - s->rb_seen) * s->pos_rebuild_launches;
+  s->pos_pending = false;
+  s->rb_seen = rb;
 }
 
 namespace {
@@ -242,8 +252,63 @@ NbArgs nb_args(tmd_system *s) {
 int read_status(tmd_system *s) {
   TMD_CUDA(cudaMemcpyAsync(s->h_status, s->status, 2 * sizeof(int),
                            cudaMemcpyDeviceToHost, s->st));
+  TMD_CUDA(cudaMemcpyAsync(s->h_status + 2, s->flag + 1, sizeof(int),
+                           cudaMemcpyDeviceToHost, s->st));
   TMD_CUDA(cudaMemsetAsync(s->status, 0, 2 * sizeof(int), s->st));
   TMD_CUDA(cudaStreamSynchronize(s->st));
+  account_pos_rebuilds(s, s->h_status[2]);
+  return TMD_OK;
+}
+
+// The graph of set_positions' rebuild: a one-thread kernel sets an IF node
+// from the displacement check's flag; the node's body is the rebuild.
+int ensure_pos_graph(tmd_system *s) {
+  if (s->pos_exec) return TMD_OK;
+  if (!s->st_aux) TMD_CUDA(cudaStreamCreateWithFlags(&s->st_aux, cudaStreamNonBlocking));
+  long lcount = 0, lb = 0;
+  cudaError_t e = cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return fail(TMD_ERR_CUDA, cudaGetErrorString(e));
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  cudaGraphConditionalHandle ch;
+  cudaGraphNode_t cn = nullptr;
+  e = cudaStreamGetCaptureInfo(s->st, &cs, nullptr, &cg, &deps, &ndeps);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&ch, cg, 0, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) {
+    launch_rebuild_cond(ch, s->flag, s->st, lcount);
+    e = cudaStreamGetCaptureInfo(s->st, &cs, nullptr, &cg, &deps, &ndeps);
+  }
+  cudaGraphNodeParams cp = {};
+  if (e == cudaSuccess) {
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = ch;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&cn, cg, deps, ndeps, &cp);
+  }
+  if (e == cudaSuccess)
+    e = cudaStreamBeginCaptureToGraph(s->st_aux, cp.conditional.phGraph_out[0], nullptr, nullptr,
+                                      0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    launch_neighbor_build(nb_args(s), s->st_aux, lb);
+    cudaGraph_t body;
+    e = cudaStreamEndCapture(s->st_aux, &body);
+  }
+  if (e == cudaSuccess)
+    e = cudaStreamUpdateCaptureDependencies(s->st, &cn, 1, cudaStreamSetCaptureDependencies);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(s->st, &g);
+  if (e == cudaSuccess) e = ee;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&s->pos_exec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    s->pos_exec = nullptr;
+    cudaGetLastError();  // a refused capture leaves no sticky error
+    return fail(TMD_ERR_CUDA, cudaGetErrorString(e));
+  }
+  s->pos_rebuild_launches = lb;
   return TMD_OK;
 }
 
@@ -667,6 +732,7 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
   if (use_graph && s->rebuild_launches > 0) {
     TMD_CUDA(cudaMemcpyAsync(rb0, s->flag, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
     TMD_CUDA(cudaStreamSynchronize(s->st));
+    account_pos_rebuilds(s, rb0[1]);
   }
   for (int s0 = 1, retries = 0; s0 <= nsteps;) {
     const int s1 = std::min(nsteps, s0 + kChunk - 1);
@@ -721,6 +787,7 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
     TMD_CUDA(cudaMemcpyAsync(rb1, s->flag, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
     TMD_CUDA(cudaStreamSynchronize(s->st));
     s->launches += (long)(rb1[1] - rb0[1]) * s->rebuild_launches;
+    account_pos_rebuilds(s, rb1[1]);
   }
   s->forces_valid = true;
   return TMD_OK;
@@ -1189,7 +1256,7 @@ int tmd_system_create(const tmd_model *m, int natoms_cap, double skin,
   A(perm, N); A(tiles, 3 * (N / 32 + h.nelt + 1));
 #undef A
   if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&s->h_scal), 8 * sizeof(double));
-  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&s->h_status), 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&s->h_status), 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(s->v, 0, 3 * N * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(s->image, 0, 3 * N * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(s->status, 0, 2 * sizeof(int));
@@ -1360,7 +1427,16 @@ int tmd_system_set_positions(tmd_system *s, const double *x) {
   double half = 0.5 * s->skin;
   launch_neighbor_check(s->n, s->x, s->xbuild, half * half, s->flag, s->st, s->launches,
                         s->acell, s->ncells ? s->cflag : nullptr);
-  launch_neighbor_build(nb_args(s), s->st, s->launches);
+  // the rebuild only when the check asks for it (conditional graph node);
+  // where the graph cannot be made, every rebuild kernel is launched and
+  // returns at once when no rebuild is pending
+  if (!s->prof && ensure_pos_graph(s) == TMD_OK) {
+    TMD_CUDA(cudaGraphLaunch(s->pos_exec, s->st));
+    s->launches += 1;
+    s->pos_pending = true;
+  } else {
+    launch_neighbor_build(nb_args(s), s->st, s->launches);
+  }
   return TMD_OK;
 }
 

@@ -122,6 +122,14 @@ struct tmd_system {
   long step_launches = 0;
   long rebuild_launches = 0;      // kernels of the conditional rebuild body
   cudaStream_t st_aux = nullptr;  // captures the rebuild body
+  // tmd_system_set_positions: the list rebuild in a conditional graph node,
+  // launched only when the displacement check asks for it.  Its kernels are
+  // counted once per rebuild that ran, from the device rebuild counter
+  // (flag[1]) read with the status words.
+  cudaGraphExec_t pos_exec = nullptr;
+  long pos_rebuild_launches = 0;
+  bool pos_pending = false;  // launched since the rebuild counter was last read
+  int rb_seen = 0;           // the rebuild counter at that read
   // fix nvt: one Nose-Hoover chain per group (cell, or the whole system);
   // kept between runs of the same atoms like the fix's state in LAMMPS
   tmd::NhcState *nhc = nullptr;
