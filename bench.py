@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--decomp-steps", type=int, default=0,
                     help="spatial decomposition line: NVE steps of the headline cell cut into "
                          "one slab per rank (tmd_b200.decomp; 0 skips it)")
+    ap.add_argument("--drift-steps", type=int, default=0,
+                    help="energy-drift line: NVE steps of the shipped W_k32 potential on "
+                         "432,000 BCC atoms after 1,000 steps of fix nvt 300 K (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=2000.0,
                     help="serving line: Poisson arrival rate (jobs/s)")
     ap.add_argument("--serve-sweep", default="250,500,1000",
@@ -545,6 +548,12 @@ def run_ours_sampled(args, rank, world, local, clk):
         except Exception as exc:  # report, do not hide
             decomp = {"error": str(exc)}
     w23k = None if args.main_only else run_w23k(args, rank, world, local, dev, barrier)
+    drift = None
+    if args.drift_steps > 0:
+        try:
+            drift = run_w_drift(args, rank, local)
+        except Exception as exc:  # report, do not hide
+            drift = {"error": str(exc)}
     alloy = None
     if args.precision_steps > 0 and not args.main_only:
         try:
@@ -582,6 +591,7 @@ def run_ours_sampled(args, rank, world, local, clk):
             "alloy432k": alloy,
             "serving": serving,
             "reference_workload_w23k": w23k,
+            "w432k_nve_drift": drift,
             "decomposition": decomp,
             "cpu_baseline": cpu,
         }
@@ -816,6 +826,47 @@ def run_w23k(args, rank, world, local, dev, barrier):
             "host_wall_s": wall, "force_form": form, "published_a100": 3.221e6, "ratio_vs_published_a100": value / 3.221e6,
             "config": "W_k32_snapshot.npz interp 0.001, bcc 3.189 24x24x20, 300 K, "
                       "fix nvt temp 300 300 0.1, skin 1.0, dt 1 fs"}
+
+
+def run_w_drift(args, rank, local):
+    """Energy conservation on the reference's own trained potential:
+    W_k32_snapshot.npz (interp 0.001), BCC a = 3.189 A, 60^3 cells = 432,000
+    atoms, velocities 300 K (seeded), 1,000 steps of fix nvt temp 300 300 0.1
+    to equilibrate, then args.drift_steps NVE steps at dt = 1 fs with the total
+    energy sampled every 100 steps.  The synthetic random-weight potentials are
+    not stable lattices (their cells collapse within 10^4 steps), so their drift
+    would measure the collapse, not the integrator."""
+    from tmd_b200 import TensorMDModel, TensorMDSystem, synth
+    model = TensorMDModel(f"{ROOT}/tests/golden/W_k32_snapshot.npz W interp 0.001", device=local)
+    x, box = synth.lattice("bcc", 3.189, 60, 60, 60)
+    n = len(x)
+    t = np.ones(n, dtype=np.int32)
+    v = synth.maxwell(np.full(n, model.type_mass[1]), 300.0, np.random.default_rng(20250 + rank))
+    s = TensorMDSystem(model, n, 1.0)
+    s.set_box(box)
+    s.set_atoms(x, t, v)
+    s.autotune(reps=3)
+    s.autotune(reps=3, family="descriptor")
+    t0 = time.perf_counter()
+    s.nvt_run(1000, 0.001, 300.0, 300.0, 0.1)
+    every = 100
+    th = s.nve_run(args.drift_steps, 0.001, thermo_every=every)
+    wall = time.perf_counter() - t0
+    etot = (th[:, 0] + th[:, 1]) / n
+    steps = np.minimum(np.arange(len(etot)) * every, args.drift_steps)
+    slope = float(np.polyfit(steps * 1e-6, etot, 1)[0]) if len(etot) > 1 else 0.0  # eV/atom/ns
+    temp = 2.0 * th[:, 1] / ((3 * n - 3) * synth.BOLTZ)
+    s.close()
+    model.close()
+    return {"natoms": n, "nve_steps": args.drift_steps, "dt_fs": 1.0, "sample_every": every,
+            "max_abs_dE_eV_per_atom": float(np.abs(etot - etot[0]).max()),
+            "final_dE_eV_per_atom": float(etot[-1] - etot[0]),
+            "slope_eV_per_atom_per_ns": slope,
+            "T_first_K": float(temp[0]), "T_last_K": float(temp[-1]),
+            "T_mean_K": float(temp.mean()),
+            "wall_s": wall, "atom_steps_per_s_wall": n * (1000 + args.drift_steps) / wall,
+            "config": "W_k32_snapshot.npz interp 0.001, bcc 3.189 60x60x60, 300 K, "
+                      "fix nvt 300 300 0.1 for 1,000 steps, then NVE, skin 1.0, dt 1 fs"}
 
 
 def run_fire_trained(rank, local, njobs=64):
