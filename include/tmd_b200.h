@@ -92,7 +92,12 @@ int tmd_system_set_atoms(tmd_system *sys, int n, const double *x,
  * the LAMMPS drop-in.  The positions may be in any periodic frame (wrapped by
  * the caller at its own times, or never): each atom takes the periodic image
  * nearest its position at the last neighbor build, so the list stays valid
- * and only real motion (more than skin/2) triggers a rebuild. */
+ * and only real motion (more than skin/2) triggers a rebuild.  The upload,
+ * the displacement check and a rebuild are queued on the system's stream and
+ * the call returns without waiting (the rebuild sits in a conditional graph
+ * node: a call that needs none launches none of its kernels).  From pinned
+ * (page-locked) host memory the copy runs asynchronously: keep x unchanged
+ * until the next tmd_compute returns. */
 int tmd_system_set_positions(tmd_system *sys, const double *x);
 
 /* Ghost-aware mode for domain-decomposed (multi-rank) LAMMPS runs, in place
