@@ -206,7 +206,13 @@ __device__ inline void radial4(const KParams &kp, const Radial4<RK> &R, const Pa
       // the Gaussian centre
       float d = (r - R.b[t]) + (g.rlo - R.blo[t]);
       f = exp2_nonpos(R.gl[t] * d * d);
-      df = R.gc[t] * d * f;
+      if (DERIV) {
+        // dH = dfc f + fc (gc d f) = f (dfc + fc gc d): one FFMA and two FMULs
+        H[t] = g.fc * f;
+        dH[t] = f * fmaf(g.fc * R.gc[t], d, g.dfc);
+        continue;
+      }
+      df = 0.f;
     } else {
       const float a = R.a[t], b = R.b[t], c = R.c[t];
       if (kp.method == 0) {
