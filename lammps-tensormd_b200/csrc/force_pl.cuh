@@ -42,7 +42,10 @@ struct PlLayout {
   }
 };
 
-template <int W, int D, int RK, bool MULTI>
+// KC: the filter count when fixed at compile time (0: kp.K at run time); with
+// it the filter loop unrolls fully and the radial basis of the next filters
+// can be scheduled beside the contraction of the current ones.
+template <int W, int D, int RK, bool MULTI, int KC = 0>
 __global__ void __launch_bounds__(kPairThreads, 4)
 k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
            const double *__restrict__ x, const int *__restrict__ elem,
@@ -56,7 +59,7 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
   constexpr int D4 = L::D4;
   constexpr int P2 = D4 / 2;  // FP32 pairs per S row (pad columns hold 0)
   extern __shared__ float4 pl_dyn[];
-  const int K = kp.K, B = kp.B, M = kp.M;
+  const int K = KC > 0 ? KC : kp.K, B = kp.B, M = kp.M;
   float *rp = reinterpret_cast<float *>(pl_dyn);
   float *Ts = rp + (RK == kRadTable ? 0 : 4 * K);  // T[m][d], rows of D4
   for (int i = threadIdx.x; i < 4 * D4; i += blockDim.x) {
@@ -163,7 +166,9 @@ k_force_pl(KParams kp, BoxP box, int n, int cap, float scale,
           W2[p] = make_float2(0.f, 0.f);
         }
         const bool on = RK != kRadTable || (g.ti > 0 && g.ti < kp.tab_n - 2);
-        for (int k0 = 0; on && k0 < K; k0 += 4) {
+#pragma unroll
+        for (int k0 = 0; k0 < (KC > 0 ? KC : K); k0 += 4) {
+          if (!on) break;
           Radial4<RK> R;
           R.k0 = k0;
           if (RK != kRadTable) {
@@ -281,8 +286,13 @@ void launch_force_pl_w(const ForceArgs &a, cudaStream_t st) {
       const int T = g * W;
       const long threads = (long)a.n * W;
       const int grid = (int)std::max(1L, (threads + T - 1) / T);
-      k_force_pl<W, 20, RK, MULTI><<<grid, T, PlLayout<20>::bytes(a.kp.K, RK, g), st>>>(
-          TMD_FORCE_ARGS);
+      const size_t sm = PlLayout<20>::bytes(a.kp.K, RK, g);
+      if (a.kp.K == 16)
+        k_force_pl<W, 20, RK, MULTI, 16><<<grid, T, sm, st>>>(TMD_FORCE_ARGS);
+      else if (a.kp.K == 32)
+        k_force_pl<W, 20, RK, MULTI, 32><<<grid, T, sm, st>>>(TMD_FORCE_ARGS);
+      else
+        k_force_pl<W, 20, RK, MULTI><<<grid, T, sm, st>>>(TMD_FORCE_ARGS);
       break;
     }
   }
