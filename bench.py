@@ -387,7 +387,7 @@ def run_ours_sampled(args, rank, world, local, clk):
     period = steps_all / max(rebuilds + prof_rebuilds, 1)
     sbytes = step_bytes_s8d(n, nlist, model.n_desc, period)
     step_traffic = 0
-    for kn in ("k_descriptor_w", "k_mlp_fp32r", kname, "k_gather"):
+    for kn in ("k_descriptor_w", "k_mlp_fp32w", kname, "k_gather"):
         tr = ncu_traffic(args.config, kn)
         step_traffic = None if (tr is None or step_traffic is None) else step_traffic + tr
     step_roofline = {
