@@ -899,7 +899,7 @@ constexpr int kFsKC = 32;
 constexpr int kFsCB = 128;
 constexpr int kFsLDT = kFsTR + 4;
 constexpr int kFsMaxStages = 6;
-constexpr int kFsMaxChunks = 512;
+constexpr int kFsMaxChunks = 256;
 
 struct FsChunk {
   short l, dir, blk, r0;
@@ -907,11 +907,11 @@ struct FsChunk {
 
 struct FsLayout {  // offsets in floats
   int stage;       // floats per stage: W chunk [32][128], then G chunk [32][68]
-  int h0, h1, bias, wout, total;
+  int h0, h1, g, bias, wout, total;  // g: output gradients of residual MLPs
   int dzoff[kMaxLayers], boff[kMaxLayers];
 };
 
-__host__ __device__ inline FsLayout fs_layout(int nl, const int *sizes, int S) {
+__host__ __device__ inline FsLayout fs_layout(int nl, const int *sizes, int S, int resnet) {
   FsLayout f{};
   int maxh = 1;
   for (int l = 1; l < nl; l++) maxh = maxh > sizes[l] ? maxh : sizes[l];
@@ -919,6 +919,8 @@ __host__ __device__ inline FsLayout fs_layout(int nl, const int *sizes, int S) {
   int o = S * f.stage;
   f.h0 = o; o += maxh * kFsLDT;
   f.h1 = o; o += maxh * kFsLDT;
+  f.g = o;
+  if (resnet) o += maxh * kFsLDT;
   for (int l = 0; l + 2 < nl; l++) { f.dzoff[l] = o; o += sizes[l + 1] * kFsLDT; }
   f.bias = o;
   int ob = 0;
@@ -958,8 +960,10 @@ k_mlp_fp32s(MlpArgs a) {
   __syncthreads();
   const int *sizes = sz_s;
   const int nq = nq_s;
-  const FsLayout lay = fs_layout(L, sizes, S);
+  const FsLayout lay = fs_layout(L, sizes, S, a.resnet);
   float *bias_s = sm + lay.bias;
+  // residual MLPs: g = dE/dy of the current hidden layer's output, [c][r]
+  float *gres = sm + lay.g;
   double *wout_s = reinterpret_cast<double *>(sm + lay.wout);
   const int ntile_cta =
       blockIdx.x < a.ntiles ? (a.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
@@ -1047,6 +1051,7 @@ k_mlp_fp32s(MlpArgs a) {
     for (int l = 0; l < L - 1 && ok; l++) {
       const int K = sizes[l], N = sizes[l + 1];
       const bool last = (l == L - 2);
+      const bool res = a.resnet && l > 0 && K == N;  // y = act(z) + x (nnp.cpp:176-181)
       const float *bl = bias_s + lay.boff[l];
       float *dz = last ? nullptr : sm + lay.dzoff[l];
       for (int nb = 0; nb * kFsCB < N && ok; nb++) {
@@ -1084,7 +1089,8 @@ k_mlp_fp32s(MlpArgs a) {
             const int c = col_of(nb, j);
             if (c < N) {
               float d;
-              const float y = act_fwd(a.actfn, acc_at(acc, i, j) + bl[c], d);
+              float y = act_fwd(a.actfn, acc_at(acc, i, j) + bl[c], d);
+              if (res) y += hin[(size_t)c * kFsLDT + r];
               if (!last) {
                 hout[(size_t)c * kFsLDT + r] = y;
                 dz[(size_t)c * kFsLDT + r] = d;
@@ -1093,6 +1099,7 @@ k_mlp_fp32s(MlpArgs a) {
                 const double w = wout_s[c];
                 ep[i] = fma((double)y, w, ep[i]);
                 hout[(size_t)c * kFsLDT + r] = (float)w * d;
+                if (a.resnet) gres[(size_t)c * kFsLDT + r] = (float)w;
               }
             }
           }
@@ -1122,6 +1129,8 @@ k_mlp_fp32s(MlpArgs a) {
     for (int l = L - 2; l >= 0 && ok; l--) {
       const int K = sizes[l], N = sizes[l + 1];
       const float *dzp = l > 0 ? sm + lay.dzoff[l - 1] : nullptr;
+      // g_{l-1} = (g_l act'_l) W_l^T, plus g_l through a residual layer
+      const bool res = a.resnet && l > 0 && K == N;
       for (int kb = 0; kb * kFsCB < K && ok; kb++) {
         float2 acc[4][4];
 #pragma unroll
@@ -1142,7 +1151,12 @@ k_mlp_fp32s(MlpArgs a) {
 #pragma unroll
             for (int j = 0; j < 8; j++) {
               const int c = col_of(kb, j);
-              if (c < K) hout[(size_t)c * kFsLDT + r] = acc_at(acc, i, j) * dzp[(size_t)c * kFsLDT + r];
+              if (c < K) {
+                float g = acc_at(acc, i, j);
+                if (res) g += gres[(size_t)c * kFsLDT + r];
+                if (a.resnet) gres[(size_t)c * kFsLDT + r] = g;  // same element: in place
+                hout[(size_t)c * kFsLDT + r] = g * dzp[(size_t)c * kFsLDT + r];
+              }
             }
           } else {
             const int at = rows_s[r];
@@ -1197,7 +1211,7 @@ void mlp_fp32w_prepare(size_t smem) {
 
 size_t mlp_fp32s_smem(int nl, const int *sizes, int resnet, int *stages) {
   *stages = 0;
-  if (resnet || nl < 2 || nl - 1 > kMaxLayers) return 0;
+  if (nl < 2 || nl - 1 > kMaxLayers) return 0;
   for (int l = 0; l < nl; l++)
     if (sizes[l] % kFsKC != 0 || sizes[l] > 32767) return 0;
   int nq = 0;
@@ -1206,12 +1220,16 @@ size_t mlp_fp32s_smem(int nl, const int *sizes, int resnet, int *stages) {
     nq += ((N + kFsCB - 1) / kFsCB) * (K / kFsKC) + ((K + kFsCB - 1) / kFsCB) * (N / kFsKC);
   }
   if (nq > kFsMaxChunks) return 0;
-  const size_t limit = 227 * 1024 - 6 * 1024;  // next to ~5 KB of static data
+  // 227 KB per block, less the kernel's static shared memory (the chunk
+  // schedule and barriers)
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, k_mlp_fp32s) != cudaSuccess) return 0;
+  const size_t limit = 227 * 1024 - fa.sharedSizeBytes;
   int S = kFsMaxStages;
-  while (S >= 2 && sizeof(float) * (size_t)fs_layout(nl, sizes, S).total > limit) S--;
+  while (S >= 2 && sizeof(float) * (size_t)fs_layout(nl, sizes, S, resnet).total > limit) S--;
   if (S < 2) return 0;
   *stages = S;
-  return sizeof(float) * (size_t)fs_layout(nl, sizes, S).total;
+  return sizeof(float) * (size_t)fs_layout(nl, sizes, S, resnet).total;
 }
 
 void mlp_fp32s_pack(const float *W, int K, int N, std::vector<float> &fwd, std::vector<float> &bwd) {
