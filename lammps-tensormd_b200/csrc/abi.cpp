@@ -417,6 +417,7 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
     ta.persistent = m->tc_persistent; ta.smem_p = m->tc_smem_p;
     ta.dz_bf16_p = m->tc_dz_bf16_p ? 1 : 0;
     ta.streamed = m->tc_streamed; ta.smem_s = m->tc_smem_s; ta.stages = m->tc_stages;
+    ta.cps_s = m->tc_cps;
     ta.probe_wait = s->wait_probe;
     ta.tf32 = m->tc_tf32 ? 1 : 0;
     ta.hi2 = m->tc_hi2;
@@ -1000,7 +1001,7 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     // 3xTF32 on tcgen05 (streamed form): W as hi = tf32(W) and lo =
     // tf32(W - hi) planes, 32-column chunks, W^T (forward) and W (backward)
     int stages = 0;
-    const size_t ss = mlp_tcs_smem(h.nl, h.sizes.data(), h.resnet, 3, 1, &stages);
+    const size_t ss = mlp_tcs_smem(h.nl, h.sizes.data(), h.resnet, 3, 1, 1, &stages);
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
     if (ss == 0 || nsm <= 0) {
@@ -1054,7 +1055,7 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
     m->tc_streamed = nsm;
     m->tc_smem_s = ss;
     m->tc_stages = stages;
-    mlp_tcs_prepare(ss, 3, 1);
+    mlp_tcs_prepare(ss, 3, 1, 1);
     m->mlp_tr = 128;
   }
   if (h.precision == TMD_PREC_BF16 || h.precision == TMD_PREC_BF16X3 ||
@@ -1175,14 +1176,20 @@ int tmd_model_load(const char *coeff_args, int device, tmd_model **out) {
         m->tc_dz_bf16_p = dzb;
         mlp_tcp_prepare(sp, np, dzb);
       }
-      // weights too large to stay resident: the streamed-weight form
-      int stages = 0;
-      const size_t ss = mlp_tcs_smem(h.nl, h.sizes.data(), h.resnet, np, 0, &stages);
+      // weights too large to stay resident: the streamed-weight form, the
+      // BF16 form as two CTAs per SM where they fit
+      int stages = 0, cps = 2;
+      size_t ss = np == 1 ? mlp_tcs_smem(h.nl, h.sizes.data(), h.resnet, np, 0, 2, &stages) : 0;
+      if (ss == 0) {
+        cps = 1;
+        ss = mlp_tcs_smem(h.nl, h.sizes.data(), h.resnet, np, 0, 1, &stages);
+      }
       if (m->tc_persistent == 0 && ss > 0 && nsm > 0) {
-        m->tc_streamed = nsm;
+        m->tc_streamed = cps * nsm;
+        m->tc_cps = cps;
         m->tc_smem_s = ss;
         m->tc_stages = stages;
-        mlp_tcs_prepare(ss, np, 0);
+        mlp_tcs_prepare(ss, np, 0, cps);
       }
     }
     m->mlp_tr = 128;

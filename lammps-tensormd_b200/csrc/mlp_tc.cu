@@ -557,7 +557,7 @@ k_mlp_tcp(MlpTcArgs a) {
 // ---------------------------------------------------------------------------
 // Streamed-weight persistent form for MLPs whose weights do not fit in shared
 // memory (e.g. 512-128-128-128 per element with four elements: 393 KB of
-// BF16 W^T and W blocks per element).  One CTA of 256 threads per SM walks
+// BF16 W^T and W blocks per element).  One CTA of 512 threads per SM walks
 // the tiles with a grid stride.  The weight chunks every tile needs (64
 // reduction columns x the GEMM's rows, contiguous in the packed blocks) are a
 // fixed schedule; thread 0 streams them from global memory (L2-resident)
@@ -574,10 +574,16 @@ k_mlp_tcp(MlpTcArgs a) {
 // act' has been used.  The epilogue thread mapping, operand writes, bounded
 // waits and error path are those of k_mlp_tcp; on an error thread 0 also
 // waits (bounded) for the copies still in flight before TMEM is released.
+// CPS = 2 (BF16 form, where it fits): two CTAs of 256 threads per SM, each
+// with half of TMEM (256 columns, act' stored as packed BF16 pairs) and half
+// of shared memory, so one CTA's epilogues and block-wide waits run while the
+// other's MMAs issue (432,000-atom 4-element alloy, 512-128-128-128
+// softplus: 1.71 -> 1.44 ms per BF16 MLP; force error against FP64
+// 6.7e-4 -> 7.4e-4 eV/A from the BF16 act').
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int kTcsThreads = 512;
-constexpr int kTcsParts = kTcsThreads / 128;  // threads per tile row (column parts)
+constexpr int kTcsThreads = 512;              // CTA size with one CTA per SM
+constexpr int kTcsParts = kTcsThreads / 128;  // column parts per tile row (most)
 constexpr int kTcsMaxChunks = 192;
 constexpr int kTcsMaxBias = 512;
 constexpr int kTcsMaxStages = 8;
@@ -653,6 +659,40 @@ struct OpTf32 {
   }
 };
 
+// 32 act' values of one row as 16 packed BF16 pairs (column pair j in
+// 32-bit column j), and back
+__device__ inline void tmem_st16_pk(uint32_t taddr, const float v[32]) {
+  uint32_t r[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+    r[j] = *reinterpret_cast<const uint32_t *>(&h);
+  }
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+      "%13,%14,%15,%16};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15])
+      : "memory");
+}
+__device__ inline void tmem_ld16_pk(uint32_t taddr, float v[32]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    v[2 * j] = __uint_as_float(r[j] << 16);
+    v[2 * j + 1] = __uint_as_float(r[j] & 0xffff0000u);
+  }
+}
+
 __device__ inline void tmem_st32(uint32_t taddr, const float v[32]) {
   asm volatile(
       "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
@@ -690,9 +730,12 @@ __host__ __device__ inline TcsPlan tcs_plan(int nin, int maxh, int nb, int kc) {
 }
 }  // namespace
 
-template <int NP, class OP>
-__global__ void __launch_bounds__(kTcsThreads, 1)
+template <int NP, class OP, int CPS>
+__global__ void __launch_bounds__(kTcsThreads / CPS, CPS)
 k_mlp_tcs(MlpTcArgs a) {
+  constexpr int NT = kTcsThreads / CPS, PARTS = NT / 128, TCOLS = kTcsTmemCols / CPS;
+  constexpr bool PK = CPS == 2;  // act' as packed BF16 pairs
+  static_assert(!PK || NP == 1, "packed act' only in the BF16 form");
   extern __shared__ __align__(1024) unsigned char smraw[];
   __shared__ __align__(8) uint64_t full_b[kTcsMaxStages], empty_b[kTcsMaxStages], gbar[2],
       accb[4], drainb;
@@ -733,7 +776,7 @@ k_mlp_tcs(MlpTcArgs a) {
     for (int l = 0; l < L - 1; l++) {
       act_s[l] = o;
       bo_s[l] = ob;
-      if (l < L - 2) o += sz_s[l + 1];
+      if (l < L - 2) o += PK ? sz_s[l + 1] / 2 : sz_s[l + 1];
       ob += sz_s[l + 1];
     }
     const int *sizes = sz_s;
@@ -762,7 +805,7 @@ k_mlp_tcs(MlpTcArgs a) {
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&tmem_base_s)),
-                 "r"(kTcsTmemCols));
+                 "r"(TCOLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -893,9 +936,9 @@ k_mlp_tcs(MlpTcArgs a) {
     if (elt != cur_elt) {  // the element's biases and output weights
       cur_elt = elt;
       for (int l = 0; l < L - 1; l++)
-        for (int c = tid; c < sizes[l + 1]; c += kTcsThreads)
+        for (int c = tid; c < sizes[l + 1]; c += NT)
           bias_s[bo_s[l] + c] = __ldg(Ls[l].b + c);
-      for (int c = tid; c < sizes[L - 1]; c += kTcsThreads) wout_s[c] = __ldg(Ls[L - 1].wd + c);
+      for (int c = tid; c < sizes[L - 1]; c += NT) wout_s[c] = __ldg(Ls[L - 1].wd + c);
     }
     __syncthreads();
     const int row_atom = rows_s[row];
@@ -904,13 +947,13 @@ k_mlp_tcs(MlpTcArgs a) {
     // each thread converts kGRows core rows (8 columns of one atom row) per
     // chunk; the rows of chunk c + 1 are loaded while chunk c is published
     // and multiplied
-    constexpr int kGRows = TM * (KC / 8) / kTcsThreads;
-    static_assert(kGRows * kTcsThreads == TM * (KC / 8), "G chunk split");
+    constexpr int kGRows = TM * (KC / 8) / NT;
+    static_assert(kGRows * NT == TM * (KC / 8), "G chunk split");
     float4 gv[kGRows][2];
     auto load_g = [&](int c) {
 #pragma unroll
       for (int u = 0; u < kGRows; u++) {
-        const int idx = tid + u * kTcsThreads;
+        const int idx = tid + u * NT;
         const int r = idx / (KC / 8), k8 = idx - r * (KC / 8);
         const int at = rows_s[r];
         if (at >= 0) {
@@ -930,7 +973,7 @@ k_mlp_tcs(MlpTcArgs a) {
       if (!ok) break;
 #pragma unroll
       for (int u = 0; u < kGRows; u++) {
-        const int idx = tid + u * kTcsThreads;
+        const int idx = tid + u * NT;
         const int r = idx / (KC / 8), k8 = idx - r * (KC / 8);
         const float v[8] = {gv[u][0].x, gv[u][0].y, gv[u][0].z, gv[u][0].w,
                             gv[u][1].x, gv[u][1].y, gv[u][1].z, gv[u][1].w};
@@ -970,7 +1013,7 @@ k_mlp_tcs(MlpTcArgs a) {
         if (!ok) break;
       }
       const bool last = (l == L - 2);
-      for (int c0 = 32 * part; c0 < N; c0 += 32 * kTcsParts) {
+      for (int c0 = 32 * part; c0 < N; c0 += 32 * PARTS) {
         float v[32], d[32];
         acc_ld(c0, v, d);
 #pragma unroll
@@ -988,7 +1031,10 @@ k_mlp_tcs(MlpTcArgs a) {
             v[j] = (float)w * d[j];
           }
         }
-        if (!last) tmem_st32(trow + actl + c0, d);
+        if (!last) {
+          if (PK) tmem_st16_pk(trow + actl + c0 / 2, d);
+          else tmem_st32(trow + actl + c0, d);
+        }
 #pragma unroll
         for (int q = 0; q < 4; q++) OP::template put8<NP>(abuf, pl.a_elems, row, c0 + 8 * q, maxh, v + 8 * q);
       }
@@ -999,7 +1045,8 @@ k_mlp_tcs(MlpTcArgs a) {
     epart[part][row] = E;
     __syncthreads();
     if (part == 0 && row_atom >= 0)
-      a.E[row_atom] = ((epart[0][row] + epart[1][row]) + (epart[2][row] + epart[3][row])) +
+      a.E[row_atom] = (PARTS == 4 ? (epart[0][row] + epart[1][row]) + (epart[2][row] + epart[3][row])
+                                  : epart[0][row] + epart[1][row]) +
                       (Ls[L - 1].bd ? *Ls[L - 1].bd : 0.0);
 
     // ---------------- backward through the hidden layers ----------------
@@ -1013,10 +1060,11 @@ k_mlp_tcs(MlpTcArgs a) {
       wait_all(&accb[0], ak[0]);
       if (!ok) break;
       const int actp = act_s[l - 1];
-      for (int c0 = 32 * part; c0 < K; c0 += 32 * kTcsParts) {
+      for (int c0 = 32 * part; c0 < K; c0 += 32 * PARTS) {
         float v[32], d[32];
         acc_ld(c0, v, d);
-        tmem_ld32(trow + actp + c0, d);
+        if (PK) tmem_ld16_pk(trow + actp + c0 / 2, d);
+        else tmem_ld32(trow + actp + c0, d);
 #pragma unroll
         for (int j = 0; j < 32; j++) v[j] *= d[j];
 #pragma unroll
@@ -1028,11 +1076,12 @@ k_mlp_tcs(MlpTcArgs a) {
 
     // ---------------- dE/dG = gz . W_0^T in 128-column blocks ----------------
     {
-      // 128-column blocks over all 512 columns, each block np_ groups of 128
-      // columns (hi, then lo and hi2 when split): up to four blocks at a time
+      // 128-column blocks over all TCOLS columns, each block np_ groups of
+      // 128 columns (hi, then lo and hi2 when split): up to TCOLS / 128
+      // blocks at a time
       const int N0 = sizes[1];
       const int nblk = (nin + 127) / 128;
-      const int np_ = kSplit ? (hi2 ? 3 : 2) : 1, conc = 4 / np_;
+      const int np_ = kSplit ? (hi2 ? 3 : 2) : 1, conc = (TCOLS / 128) / np_;
       for (int b0 = 0; b0 < nblk && ok; b0 += conc) {
         const int b1 = min(nblk, b0 + conc);
         if (tid == 0) {
@@ -1048,7 +1097,7 @@ k_mlp_tcs(MlpTcArgs a) {
           wait_all(&accb[b - b0], ak[b - b0]);
           if (!ok) break;
           const int n0 = 128 * b, nout = min(128, nin - n0);
-          for (int c0 = 32 * part; c0 < nout; c0 += 32 * kTcsParts) {
+          for (int c0 = 32 * part; c0 < nout; c0 += 32 * PARTS) {
             float v[32];
             const uint32_t cb = (uint32_t)(128 * np_ * (b - b0));
             tmem_ld32(trow + cb + c0, v);
@@ -1085,12 +1134,14 @@ k_mlp_tcs(MlpTcArgs a) {
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(kTcsTmemCols));
+                 "r"(TCOLS));
 }
 
-size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int tf32, int *stages) {
+size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int tf32, int cps,
+                    int *stages) {
   *stages = 0;
   if (resnet || nl < 2 || nl - 1 > kMaxLayers) return 0;
+  if (cps != 1 && (cps != 2 || np != 1 || tf32)) return 0;
   const int kc = tf32 ? OpTf32::KC : OpBf16::KC;
   const size_t esz = tf32 ? 4 : 2;
   const int nin = sizes[0];
@@ -1104,15 +1155,22 @@ size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int tf32, int 
   const int nb = np == 3 ? 2 : 1;
   const TcsPlan pl = tcs_plan(nin, maxh, nb, kc);
   const bool split = tf32 && np == 3;  // D_hi and D_lo accumulators
-  if ((split ? 2 : 1) * pl.accw + acts > kTcsTmemCols) return 0;
+  if ((split ? 2 : 1) * pl.accw + (cps == 2 ? acts / 2 : acts) > kTcsTmemCols / cps) return 0;
   // chunk schedule length
   int nq = 0;
   for (int l = 0; l < nl - 1; l++) nq += sizes[l] / kc;
   for (int l = nl - 2; l >= 1; l--) nq += sizes[l + 1] / kc;
   nq += ((nin + 127) / 128) * (sizes[1] / kc);
   if (nq > kTcsMaxChunks) return 0;
-  // as many stages as fit next to the operand region and ~12 KB of static data
-  const size_t limit = 227 * 1024 - 12 * 1024;
+  // as many stages as fit next to the operand region and ~12 KB of static
+  // data; with two CTAs per SM each gets half of the SM's 228 KB less the
+  // 1 KB the runtime reserves per CTA and the kernel's own static data
+  size_t limit = 227 * 1024 - 12 * 1024;
+  if (cps == 2) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_mlp_tcs<1, OpBf16, 2>) != cudaSuccess) return 0;
+    limit = 228 * 1024 / 2 - 1024 - fa.sharedSizeBytes;
+  }
   const size_t abytes = (size_t)nb * pl.a_elems * esz, sbytes = (size_t)pl.stage_elems * esz;
   if (abytes + 2 * sbytes > limit) return 0;
   int S = (int)((limit - abytes) / sbytes);
@@ -1133,11 +1191,12 @@ int mlp_tcs_hi2(int nl, const int *sizes, int np, int tf32) {
   return 3 * pl.accw + acts <= kTcsTmemCols ? 1 : 0;
 }
 
-void mlp_tcs_prepare(size_t smem, int np, int tf32) {
+void mlp_tcs_prepare(size_t smem, int np, int tf32, int cps) {
   const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  if (tf32) cudaFuncSetAttribute(k_mlp_tcs<3, OpTf32>, at, (int)smem);
-  else if (np == 3) cudaFuncSetAttribute(k_mlp_tcs<3, OpBf16>, at, (int)smem);
-  else cudaFuncSetAttribute(k_mlp_tcs<1, OpBf16>, at, (int)smem);
+  if (tf32) cudaFuncSetAttribute(k_mlp_tcs<3, OpTf32, 1>, at, (int)smem);
+  else if (np == 3) cudaFuncSetAttribute(k_mlp_tcs<3, OpBf16, 1>, at, (int)smem);
+  else if (cps == 2) cudaFuncSetAttribute(k_mlp_tcs<1, OpBf16, 2>, at, (int)smem);
+  else cudaFuncSetAttribute(k_mlp_tcs<1, OpBf16, 1>, at, (int)smem);
 }
 
 size_t mlp_tcp_smem(int nl, const int *sizes, int resnet, int np, bool dz_bf16) {
@@ -1232,9 +1291,10 @@ void launch_mlp_tc(const MlpTcArgs &a, cudaStream_t st, long &launches) {
   if (a.ntiles <= 0) return;
   if (a.streamed > 0) {
     const int grid = a.ntiles < a.streamed ? a.ntiles : a.streamed;
-    if (a.tf32) k_mlp_tcs<3, OpTf32><<<grid, kTcsThreads, a.smem_s, st>>>(a);
-    else if (a.np == 3) k_mlp_tcs<3, OpBf16><<<grid, kTcsThreads, a.smem_s, st>>>(a);
-    else k_mlp_tcs<1, OpBf16><<<grid, kTcsThreads, a.smem_s, st>>>(a);
+    if (a.tf32) k_mlp_tcs<3, OpTf32, 1><<<grid, kTcsThreads, a.smem_s, st>>>(a);
+    else if (a.np == 3) k_mlp_tcs<3, OpBf16, 1><<<grid, kTcsThreads, a.smem_s, st>>>(a);
+    else if (a.cps_s == 2) k_mlp_tcs<1, OpBf16, 2><<<grid, kTcsThreads / 2, a.smem_s, st>>>(a);
+    else k_mlp_tcs<1, OpBf16, 1><<<grid, kTcsThreads, a.smem_s, st>>>(a);
     launches += 1;
     return;
   }

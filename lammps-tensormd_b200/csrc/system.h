@@ -33,6 +33,7 @@ struct tmd_model {
   int tc_streamed = 0;   // > 0: streamed-weight persistent tensor-core MLP (grid size)
   size_t tc_smem_s = 0;
   int tc_stages = 0;
+  int tc_cps = 1;        // its CTAs per SM
   int maxh = 1;
   double *d_mass = nullptr;     // per element
   int mlp_tr = 64;

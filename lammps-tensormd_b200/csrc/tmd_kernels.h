@@ -186,6 +186,7 @@ struct MlpTcArgs {
   int streamed;       // > 0: streamed-weight persistent form on this many CTAs
   size_t smem_s;      // its dynamic shared memory
   int stages;         // its weight-chunk stages
+  int cps_s;          // its CTAs per SM (2: 256 threads, act' as packed BF16 in TMEM)
   // > 0: failure-detection hook (tmd_system_set_wait_probe): every CTA first
   // waits at most this many cycles on one of its mbarriers before issuing any
   // MMA or copy; nothing arrives on it, so the kernel takes its timeout path
@@ -230,8 +231,9 @@ void mlp_tcp_prepare(size_t smem, int np, bool dz_bf16);
 // (residual layers, widths not multiples of the chunk (64 BF16 / 32 TF32
 // columns) or above 256, act' beyond 512 TMEM columns).  tf32 = 1: the
 // 3xTF32 operand format.
-size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int tf32, int *stages);
-void mlp_tcs_prepare(size_t smem, int np, int tf32);
+size_t mlp_tcs_smem(int nl, const int *sizes, int resnet, int np, int tf32, int cps,
+                    int *stages);
+void mlp_tcs_prepare(size_t smem, int np, int tf32, int cps);
 // 3xTF32: 1 when TMEM holds a second hi accumulator (MlpTcArgs::hi2).
 int mlp_tcs_hi2(int nl, const int *sizes, int np, int tf32);
 
