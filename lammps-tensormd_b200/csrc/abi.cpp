@@ -377,7 +377,7 @@ ForceArgs force_args(tmd_system *s, float scale, int variant) {
   return fa;
 }
 
-void launch_force_eval(tmd_system *s, float scale, bool want_vatom, bool kick, double kick_dtf) {
+void launch_force_eval(tmd_system *s, float scale, bool want_vatom) {
   const tmd_model *m = s->m;
   const DescArgs d = desc_args(s, s->desc_variant);
   prof_begin(s);
@@ -436,9 +436,6 @@ void launch_force_eval(tmd_system *s, float scale, bool want_vatom, bool kick, d
   ga.rev = s->rev; ga.nbr = s->nbr; ga.x = s->x; ga.box = s->box; ga.wv = s->wv;
   ga.f = s->f; ga.vatom = want_vatom ? s->vatom : nullptr;
   ga.cbox = d.cbox; ga.acell = s->acell;
-  if (kick) {
-    ga.v = s->v; ga.elem = s->elem; ga.mass_e = m->d_mass; ga.dtf = kick_dtf;
-  }
   prof_begin(s);
   launch_gather(ga, s->st, s->launches);
   prof_end(s, 4);
@@ -615,8 +612,9 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
     prof_begin(s);
     launch_neighbor_build(nb_args(s), s->st, s->launches);
     prof_end(s, 0);
-    launch_force_eval(s, 1.0f, false, true, dtf);  // with fix nve's final_integrate
+    launch_force_eval(s, 1.0f, false);
     prof_begin(s);
+    launch_nve_final(n, s->v, s->f, s->elem, s->m->d_mass, dtf, s->st, s->launches);
     if (nvt) {
       group_ke(s);
       launch_nhc_half(G, s->nhc, s->nhc_ke, n, acell, s->v, s->st, s->launches);
@@ -674,7 +672,8 @@ int run_md(tmd_system *s, int nsteps, double dt, const NvtSpec *nvt, int thermo_
     if (e == cudaSuccess)
       e = cudaStreamUpdateCaptureDependencies(s->st, &cn, 1, cudaStreamSetCaptureDependencies);
     if (e == cudaSuccess) {
-      launch_force_eval(s, 1.0f, false, true, dtf);  // with fix nve's final_integrate
+      launch_force_eval(s, 1.0f, false);
+      launch_nve_final(n, s->v, s->f, s->elem, s->m->d_mass, dtf, s->st, s->launches);
       if (nvt) {
         group_ke(s);
         launch_nhc_half(G, s->nhc, s->nhc_ke, n, acell, s->v, s->st, s->launches);

@@ -40,9 +40,7 @@ __global__ void k_gather(int n, int cap, int B, const int *__restrict__ boff,
                          const uint32_t *__restrict__ nbr, const double *__restrict__ x,
                          BoxP box, const double *__restrict__ wv,
                          double *__restrict__ f, double *__restrict__ vatom,
-                         const BoxP *__restrict__ cbox, const int *__restrict__ acell,
-                         double *__restrict__ v, const int *__restrict__ elem,
-                         const double *__restrict__ mass_e, double dtf) {
+                         const BoxP *__restrict__ cbox, const int *__restrict__ acell) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gt >> 3, sub = gt & 7;
   if (a >= n) return;
@@ -115,12 +113,6 @@ __global__ void k_gather(int n, int cap, int B, const int *__restrict__ boff,
     f[3 * a] = fx;
     f[3 * a + 1] = fy;
     f[3 * a + 2] = fz;
-    if (v) {  // FixNVE::final_integrate (fix_nve.cpp:64-141): v += dtf / m * f
-      const double dtfm = dtf / mass_e[elem[a]];
-      v[3 * a] = __dadd_rn(v[3 * a], __dmul_rn(dtfm, fx));
-      v[3 * a + 1] = __dadd_rn(v[3 * a + 1], __dmul_rn(dtfm, fy));
-      v[3 * a + 2] = __dadd_rn(v[3 * a + 2], __dmul_rn(dtfm, fz));
-    }
     if (VATOM) {
 #pragma unroll
       for (int c = 0; c < 6; c++) vatom[6 * a + c] = 0.5 * (wv[6 * a + c] + v6[c]);
@@ -135,12 +127,10 @@ void launch_gather(const GatherArgs &a, cudaStream_t st, long &launches) {
   if (grid < 1) grid = 1;
   if (a.vatom)
     k_gather<true><<<grid, T, 0, st>>>(a.n, a.cap, a.B, a.boff, a.pdf, a.rev, a.nbr, a.x,
-                                       a.box, a.wv, a.f, a.vatom, a.cbox, a.acell, a.v,
-                                       a.elem, a.mass_e, a.dtf);
+                                       a.box, a.wv, a.f, a.vatom, a.cbox, a.acell);
   else
     k_gather<false><<<grid, T, 0, st>>>(a.n, a.cap, a.B, a.boff, a.pdf, a.rev, a.nbr, a.x,
-                                        a.box, a.wv, a.f, a.vatom, a.cbox, a.acell, a.v,
-                                        a.elem, a.mass_e, a.dtf);
+                                        a.box, a.wv, a.f, a.vatom, a.cbox, a.acell);
   launches += 1;
 }
 

@@ -128,6 +128,17 @@ __global__ void k_nve_initial(int n, double *__restrict__ x, double *__restrict_
   }
 }
 
+__global__ void k_nve_final(int n, double *__restrict__ v, const double *__restrict__ f,
+                            const int *__restrict__ elem,
+                            const double *__restrict__ mass_e, double dtf) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double dtfm = dtf / mass_e[elem[i]];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    v[3 * i + c] = __dadd_rn(v[3 * i + c], __dmul_rn(dtfm, f[3 * i + c]));
+}
+
 void launch_nve_initial(int n, double *x, double *v, const double *f,
                         const int *elem, const double *mass_e, double dtf,
                         double dtv, cudaStream_t st, long &launches) {
@@ -135,8 +146,12 @@ void launch_nve_initial(int n, double *x, double *v, const double *f,
   launches += 1;
 }
 
-// final_integrate (v += dtfm * f) runs inside the force gather, k_gather,
-// as soon as an atom's force is summed.
+void launch_nve_final(int n, double *v, const double *f, const int *elem,
+                      const double *mass_e, double dtf, cudaStream_t st,
+                      long &launches) {
+  k_nve_final<<<(n + 255) / 256, 256, 0, st>>>(n, v, f, elem, mass_e, dtf);
+  launches += 1;
+}
 
 // ---------------------------------------------------------------------
 // fix nvt (FixNH, fix_nh.cpp).  One thread per group runs the chain update;

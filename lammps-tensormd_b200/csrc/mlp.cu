@@ -617,7 +617,7 @@ __device__ __forceinline__ void wt_gemm_fwd(const float *A, int lda, int K, cons
                                             int ldw, int ty, int tx, float (&acc)[kWtRI][8]) {
   const float *ap = A + ty * lda;
   const float *wp = W + 4 * tx;
-#pragma unroll 4
+#pragma unroll 2
   for (int k = 0; k < K; k += 4) {
     float4 av[kWtRI], b0[4], b1[4];
 #pragma unroll
@@ -653,7 +653,7 @@ __device__ __forceinline__ void wt_gemm_bwd(const float *A, int lda, int N, cons
     kv[j] = k < Kout;
     wr[j] = W + (kv[j] ? k : 0) * ldw;
   }
-#pragma unroll 4
+#pragma unroll 2
   for (int c = 0; c < N; c += 4) {
     float4 av[kWtRI], wv[8];
 #pragma unroll

@@ -183,10 +183,7 @@ int cap_for_density(const tmd_system *s, double dens);
 int read_status(tmd_system *s);
 int clear_status(tmd_system *s);
 int rebuild_now(tmd_system *s);
-// kick: the gather also applies the step's closing velocity half-kick
-// (fix nve final_integrate) with kick_dtf
-void launch_force_eval(tmd_system *s, float scale, bool want_vatom, bool kick = false,
-                       double kick_dtf = 0.0);
+void launch_force_eval(tmd_system *s, float scale, bool want_vatom);
 ForceArgs force_args(tmd_system *s, float scale, int variant);
 DescArgs desc_args(tmd_system *s, int variant);
 int default_desc_variant(const tmd_model *m);

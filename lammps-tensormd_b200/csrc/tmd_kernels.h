@@ -299,13 +299,6 @@ struct GatherArgs {
   double *vatom;   // nullable
   const BoxP *cbox;   // multi-cell mode (as DescArgs)
   const int *acell;
-  // v non-null: the step's closing velocity half-kick (fix nve's
-  // final_integrate, v += dtf / m * f) applied to each atom as soon as its
-  // force is summed
-  double *v;
-  const int *elem;
-  const double *mass_e;
-  double dtf;
 };
 void launch_gather(const GatherArgs &a, cudaStream_t st, long &launches);
 
@@ -420,11 +413,13 @@ void launch_nhc_setup(int ngroups, NhcState *st, const double *ke_group, cudaStr
 void launch_nhc_half(int ngroups, NhcState *st, const double *ke_group, int n,
                      const int *acell, double *v, cudaStream_t s, long &launches);
 
-// Velocity Verlet (fix_nve.cpp:64-141): the first half kick and drift; the
-// second half kick is applied by the force gather (GatherArgs::v).
+// Velocity Verlet halves (fix_nve.cpp:64-141).
 void launch_nve_initial(int n, double *x, double *v, const double *f,
                         const int *elem, const double *mass_e, double dtf,
                         double dtv, cudaStream_t st, long &launches);
+void launch_nve_final(int n, double *v, const double *f, const int *elem,
+                      const double *mass_e, double dtf, cudaStream_t st,
+                      long &launches);
 void launch_kinetic(int n, const double *v, const int *elem,
                     const double *mass_e, double *ke_atom, cudaStream_t st,
                     long &launches);
