@@ -13,6 +13,11 @@ force.yaml dump, read as text) into published.json:
   examples/tensormd/binary/medium/force.yaml       per-atom step-0 forces
   examples/tensormd/trinary/a100_log/log_release.lammps     AlMgSi energy
   examples/tensormd/W/tensormd/speedup/a100_log/log_0114.lammps  W_k32 energy
+  examples/tensormd/W/tensormd/compare/a100_log/log{2,3,4,5}.lammps
+        W_m3_k64_n128_squareplus step-0 energy and pressure of 46,080 to
+        115,200 BCC atoms (log1, 23,040 atoms, is not used: its energy is
+        1.46 eV and its pressure 876 bar away from the values the other four
+        runs give per atom)
 
 The test suite reads only the files written here.
 """
@@ -32,6 +37,7 @@ def main(ref: Path):
     files = {
         "MoNi_m3.npz": ex / "binary/medium/MoNi_m3.npz",
         "W_k32_snapshot.npz": ex / "W/tensormd/W_k32_snapshot.npz",
+        "W_m3_k64_n128_squareplus.npz": ex / "W/tensormd/W_m3_k64_n128_squareplus.npz",
         "AlMgSi.24aug13.npz": ex / "trinary/AlMgSi.24aug13.npz",
         "Mo8_Ni8_id3210.data": ex / "binary/Mo8_Ni8_id3210.data",
         "AlMgSi.data": ex / "trinary/AlMgSi.data",
@@ -57,16 +63,29 @@ def main(ref: Path):
             forces.append([int(mm.group(1)), int(mm.group(2)), float(mm.group(3)),
                            float(mm.group(4)), float(mm.group(5))])
 
-    def thermo_pe(path):
-        """PotEng of the step-0 thermo line, located by the header column."""
+    def thermo_step0(path):
+        """The step-0 thermo line as {column: value}."""
         header = None
         for line in path.read_text().splitlines():
             t = line.split()
             if t and t[0] == "Step":
                 header = t
             elif header and t and t[0] == "0" and len(t) == len(header):
-                return float(t[header.index("PotEng")])
+                return dict(zip(header, map(float, t)))
         raise RuntimeError(path)
+
+    def thermo_pe(path):
+        return thermo_step0(path)["PotEng"]
+
+    def natoms(path):
+        return int(re.search(r"Loop time of .* with (\d+) atoms", path.read_text()).group(1))
+
+    wk64 = []
+    for k in (2, 3, 4, 5):
+        lg = ex / f"W/tensormd/compare/a100_log/log{k}.lammps"
+        th = thermo_step0(lg)
+        wk64.append({"natoms": natoms(lg), "pe": th["PotEng"], "press": th["Press"],
+                     "volume": th["Volume"], "temp": th["Temp"]})
 
     almgsi = thermo_pe(ex / "trinary/a100_log/log_release.lammps")
     w = thermo_pe(ex / "W/tensormd/speedup/a100_log/log_0114.lammps")
@@ -94,6 +113,12 @@ def main(ref: Path):
                       "(bcc 3.189, 24x24x20, interp 0.001)",
             "natoms": 23040, "energy_total": w, "lattice": 3.189, "interp": 1e-3,
             "elements": ["W"],
+        },
+        "W_m3_k64": {
+            "source": "examples/tensormd/W/tensormd/compare/a100_log/log2-5.lammps "
+                      "(bcc 3.189, 24x24x40 to 24x24x100, interp 0.001, step 0 of "
+                      "velocity create 300 K)",
+            "runs": wk64, "lattice": 3.189, "interp": 1e-3, "elements": ["W"],
         },
     }
     (HERE / "published.json").write_text(json.dumps(pub, indent=1))

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from pack import Oracle
-from tmd_testutil import GOLDEN, NKTV2P, published, read_data, volume
+from tmd_testutil import GOLDEN, NKTV2P, kinetic_pressure, published, read_data, volume
 
 
 @pytest.fixture(scope="module")
@@ -56,3 +56,25 @@ def test_w_k32_energy(pub):
     o = Oracle(str(GOLDEN / "W_k32_snapshot.npz"), interp=p["interp"])
     e = o.compute(x, [0, 0], box, [1, 1, 1])["energy"]
     assert e / 2 * p["natoms"] == pytest.approx(p["energy_total"], abs=0.05)
+
+
+def test_w_m3_k64_energy_and_pressure(pub):
+    """W_m3_k64_n128_squareplus (64 filters, residual squareplus MLP) on perfect
+    BCC W of 46,080 to 115,200 atoms: every atom has the same environment, so
+    the two-atom cell gives the energy per atom and the virial pressure.  The
+    published step-0 energies (8 significant digits) within one unit of the
+    last digit; the pressures (Press minus its kinetic part) within 2e-3 bar
+    (printed to 1e-3 bar; the reference's FP32 virial moves the last digit)."""
+    p = pub["W_m3_k64"]
+    a = p["lattice"]
+    x = np.array([[0.0, 0.0, 0.0], [0.5 * a, 0.5 * a, 0.5 * a]])
+    box = np.array([0, 0, 0, a, a, a, 0, 0, 0], dtype=float)
+    o = Oracle(str(GOLDEN / "W_m3_k64_n128_squareplus.npz"), interp=p["interp"])
+    out = o.compute(x, [0, 0], box, [1, 1, 1])
+    e_atom = out["energy"] / 2
+    p_vir = out["virial"][:3].mean() / a ** 3 * NKTV2P
+    for run in p["runs"]:
+        unit = 10.0 ** (np.floor(np.log10(abs(run["pe"]))) - 7)
+        assert e_atom * run["natoms"] == pytest.approx(run["pe"], abs=unit), run
+        p_kin = kinetic_pressure(run["natoms"], run["temp"], run["volume"])
+        assert p_vir + p_kin == pytest.approx(run["press"], abs=2e-3), run

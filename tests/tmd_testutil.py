@@ -21,6 +21,22 @@ def volume(box):
     return box[3] * box[4] * box[5]
 
 
+def kinetic_pressure(natoms, temp, vol):
+    """Kinetic part of LAMMPS's pressure in bar: dof k_B T / (3 V) with
+    dof = 3 N - 3 (ComputeTemp::dof_compute, compute_temp.cpp:58-62, extra_dof
+    = dimension, compute.cpp:84) and metal k_B (update.cpp:188)."""
+    return (3 * natoms - 3) * 8.617343e-5 * temp / (3 * vol) * NKTV2P
+
+
+def bcc_lattice(a, nx, ny, nz):
+    """Perfect BCC cells (LAMMPS `lattice bcc a` + `create_atoms`): positions
+    and the orthogonal box as (xlo, ylo, zlo, xhi, yhi, zhi, xy, xz, yz)."""
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"),
+                 -1).reshape(-1, 3).astype(float)
+    x = np.concatenate([g, g + 0.5]) * a
+    return x, np.array([0, 0, 0, nx * a, ny * a, nz * a, 0, 0, 0], dtype=float)
+
+
 def canonical_pairs(off, ent):
     """Sorted (i, j, sx, sy, sz) tuples of a neighbor list."""
     n = len(off) - 1
