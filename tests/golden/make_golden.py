@@ -13,6 +13,9 @@ force.yaml dump, read as text) into published.json:
   examples/tensormd/binary/medium/force.yaml       per-atom step-0 forces
   examples/tensormd/trinary/a100_log/log_release.lammps     AlMgSi energy
   examples/tensormd/W/tensormd/speedup/a100_log/log_0114.lammps  W_k32 energy
+        and pressure (23,040 atoms)
+  examples/tensormd/scaling/weak/200/log200.lammps   W_k32 step-0 energy and
+        pressure of 200,000,000 BCC atoms
   examples/tensormd/W/tensormd/compare/a100_log/log{2,3,4,5}.lammps
         W_m3_k64_n128_squareplus step-0 energy and pressure of 46,080 to
         115,200 BCC atoms (log1, 23,040 atoms, is not used: its energy is
@@ -88,7 +91,11 @@ def main(ref: Path):
                      "volume": th["Volume"], "temp": th["Temp"]})
 
     almgsi = thermo_pe(ex / "trinary/a100_log/log_release.lammps")
-    w = thermo_pe(ex / "W/tensormd/speedup/a100_log/log_0114.lammps")
+    w_log = ex / "W/tensormd/speedup/a100_log/log_0114.lammps"
+    w = thermo_pe(w_log)
+    w_th = thermo_step0(w_log)
+    big_log = ex / "scaling/weak/200/log200.lammps"
+    big = thermo_step0(big_log)
     pub = {
         "MoNi_m3": {
             "source": "examples/tensormd/binary/medium/output (data file x 10x20x30, "
@@ -112,7 +119,14 @@ def main(ref: Path):
             "source": "examples/tensormd/W/tensormd/speedup/a100_log/log_0114.lammps "
                       "(bcc 3.189, 24x24x20, interp 0.001)",
             "natoms": 23040, "energy_total": w, "lattice": 3.189, "interp": 1e-3,
-            "elements": ["W"],
+            "elements": ["W"], "press": w_th["Press"], "volume": w_th["Volume"],
+            "temp": w_th["Temp"],
+        },
+        "W_k32_200M": {
+            "source": "examples/tensormd/scaling/weak/200/log200.lammps (bcc 3.189, "
+                      "400x500x500, interp 0.001, step 0 of velocity create 300 K)",
+            "natoms": natoms(big_log), "pe": big["PotEng"], "press": big["Press"],
+            "volume": big["Volume"], "temp": big["Temp"],
         },
         "W_m3_k64": {
             "source": "examples/tensormd/W/tensormd/compare/a100_log/log2-5.lammps "

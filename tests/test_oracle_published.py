@@ -54,8 +54,19 @@ def test_w_k32_energy(pub):
     x = np.array([[0.0, 0.0, 0.0], [0.5 * a, 0.5 * a, 0.5 * a]])
     box = np.array([0, 0, 0, a, a, a, 0, 0, 0], dtype=float)
     o = Oracle(str(GOLDEN / "W_k32_snapshot.npz"), interp=p["interp"])
-    e = o.compute(x, [0, 0], box, [1, 1, 1])["energy"]
-    assert e / 2 * p["natoms"] == pytest.approx(p["energy_total"], abs=0.05)
+    out = o.compute(x, [0, 0], box, [1, 1, 1])
+    e_atom = out["energy"] / 2
+    assert e_atom * p["natoms"] == pytest.approx(p["energy_total"], abs=0.05)
+    # step-0 pressure of the 300 K run: virial part plus the kinetic part
+    p_vir = out["virial"][:3].mean() / a ** 3 * NKTV2P
+    vol = p["natoms"] / 2 * a ** 3
+    assert p_vir + kinetic_pressure(p["natoms"], p["temp"], vol) == pytest.approx(p["press"], abs=2e-3)
+    # the 200,000,000-atom weak-scaling run of the same potential (perfect
+    # lattice: the same energy per atom; 8 significant digits printed)
+    big = pub["W_k32_200M"]
+    assert e_atom * big["natoms"] == pytest.approx(big["pe"], abs=100.0)
+    vol = big["natoms"] / 2 * a ** 3
+    assert p_vir + kinetic_pressure(big["natoms"], big["temp"], vol) == pytest.approx(big["press"], abs=2e-3)
 
 
 def test_w_m3_k64_energy_and_pressure(pub):
