@@ -16,7 +16,8 @@ import pytest
 
 from pack import Oracle, load_npz
 from tmd_b200 import PairTensorMD, TensorMDModel, TensorMDSystem, synth
-from tmd_testutil import GOLDEN, NKTV2P, canonical_pairs, frac_wrap, published, read_data, rel_rms, volume
+from tmd_testutil import (GOLDEN, NKTV2P, bcc_lattice, canonical_pairs, frac_wrap, kinetic_pressure,
+                          published, read_data, rel_rms, volume)
 
 pytestmark = pytest.mark.gpu
 
@@ -103,6 +104,30 @@ def test_moni_published_on_gpu():
     assert rel_rms(out["f"], rows) <= 2e-5
     press = out["virial"][:3].mean() / volume(box) * NKTV2P
     assert press == pytest.approx(p["press"], rel=2e-5)
+
+
+def test_w_m3_k64_published_on_gpu():
+    """GPU against the reference's published W_m3_k64_n128_squareplus numbers
+    (64 filters, residual squareplus MLP): perfect BCC W, 24 x 24 x 40 cells =
+    46,080 atoms.  Energy within 2e-7 of |E| (measured 1.2e-7: the FP32
+    rounding of the radial table, the 64-filter sums and the MLP is the same
+    in every atom of the perfect lattice, so it does not average out as it
+    does over a disordered cell); the virial pressure plus LAMMPS's kinetic
+    part at the run's 300 K within the virial bar; forces of the symmetric
+    lattice vanish up to FP32 cancellation."""
+    p = published()["W_m3_k64"]
+    run = p["runs"][0]
+    x, box = bcc_lattice(p["lattice"], 24, 24, 40)
+    assert len(x) == run["natoms"]
+    t = np.ones(len(x), dtype=np.int32)
+    _, _, out = _run(f"{GOLDEN}/W_m3_k64_n128_squareplus.npz W interp 0.001", x, t, box)
+    press = out["virial"][:3].mean() / volume(box) * NKTV2P + kinetic_pressure(
+        run["natoms"], run["temp"], volume(box))
+    fmax = np.abs(out["f"]).max()
+    diag = (out["energy"], run["pe"], press, run["press"], fmax)
+    assert out["energy"] == pytest.approx(run["pe"], rel=2e-7), diag
+    assert press == pytest.approx(run["press"], rel=VIR_REL), diag
+    assert fmax < 1e-3, diag
 
 
 def test_three_elements_against_oracle():
