@@ -4,7 +4,7 @@
 
 (default: TMD_REFERENCE_TREE, see oracle/reftree.py)
 
-Copies three shipped potentials and two data files, and extracts the
+Copies five shipped potentials and two data files, and extracts the
 published step-0 results of the reference (LAMMPS thermo lines and the
 force.yaml dump, read as text) into published.json:
 
@@ -12,6 +12,8 @@ force.yaml dump, read as text) into published.json:
         step-0 energy (15 digits), pressure components, max force component
   examples/tensormd/binary/medium/force.yaml       per-atom step-0 forces
   examples/tensormd/trinary/a100_log/log_release.lammps     AlMgSi energy
+  examples/tensormd/binary/medium/a100_log/log_release.lammps   MoNi_squareplus_500k
+        step-0 energy and pressure (data file x 10x10x10, 100 K)
   examples/tensormd/W/tensormd/speedup/a100_log/log_0114.lammps  W_k32 energy
         and pressure (23,040 atoms)
   examples/tensormd/scaling/weak/200/log200.lammps   W_k32 step-0 energy and
@@ -39,6 +41,7 @@ def main(ref: Path):
     ex = ref / "examples" / "tensormd"
     files = {
         "MoNi_m3.npz": ex / "binary/medium/MoNi_m3.npz",
+        "MoNi_squareplus_500k.npz": ex / "binary/medium/MoNi_squareplus_500k.npz",
         "W_k32_snapshot.npz": ex / "W/tensormd/W_k32_snapshot.npz",
         "W_m3_k64_n128_squareplus.npz": ex / "W/tensormd/W_m3_k64_n128_squareplus.npz",
         "AlMgSi.24aug13.npz": ex / "trinary/AlMgSi.24aug13.npz",
@@ -94,6 +97,8 @@ def main(ref: Path):
     w_log = ex / "W/tensormd/speedup/a100_log/log_0114.lammps"
     w = thermo_pe(w_log)
     w_th = thermo_step0(w_log)
+    sq_log = ex / "binary/medium/a100_log/log_release.lammps"
+    sq = thermo_step0(sq_log)
     big_log = ex / "scaling/weak/200/log200.lammps"
     big = thermo_step0(big_log)
     pub = {
@@ -121,6 +126,13 @@ def main(ref: Path):
             "natoms": 23040, "energy_total": w, "lattice": 3.189, "interp": 1e-3,
             "elements": ["W"], "press": w_th["Press"], "volume": w_th["Volume"],
             "temp": w_th["Temp"],
+        },
+        "MoNi_squareplus": {
+            "source": "examples/tensormd/binary/medium/a100_log/log_release.lammps "
+                      "(data file x 10x10x10, pair_coeff * * MoNi_squareplus_500k.npz Mo Ni "
+                      "interp 0.0001, step 0 of velocity create 100 K)",
+            "replicas": 1000, "natoms": natoms(sq_log), "pe": sq["PotEng"],
+            "press": sq["Press"], "temp": sq["Temp"], "interp": 1e-4, "elements": ["Mo", "Ni"],
         },
         "W_k32_200M": {
             "source": "examples/tensormd/scaling/weak/200/log200.lammps (bcc 3.189, "

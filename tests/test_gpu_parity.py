@@ -130,6 +130,24 @@ def test_w_m3_k64_published_on_gpu():
     assert fmax < 1e-3, diag
 
 
+def test_moni_squareplus_published_on_gpu():
+    """MoNi_squareplus_500k on the Mo8Ni8 cell: the GPU against the FP64
+    oracle at the residual-MLP bars, and the published 16,000-atom step-0
+    energy (the cell replicated 10 x 10 x 10)."""
+    p = published()["MoNi_squareplus"]
+    x, t, box = read_data(GOLDEN / "Mo8_Ni8_id3210.data")
+    x = frac_wrap(x, box)
+    _, _, out = _run(f"{GOLDEN}/MoNi_squareplus_500k.npz Mo Ni interp 0.0001", x, t, box)
+    ref = Oracle(str(GOLDEN / "MoNi_squareplus_500k.npz"), interp=1e-4).compute(
+        x, t - 1, box, [1, 1, 1])
+    assert rel_rms(out["f"], ref["f"]) <= 2e-5
+    assert abs(out["energy"] - ref["energy"]) / len(x) <= E_PER_ATOM_OTHER
+    vr = np.linalg.norm(out["virial"] - ref["virial"]) / np.linalg.norm(ref["virial"])
+    assert vr <= VIR_REL, vr
+    assert out["energy"] * p["replicas"] == pytest.approx(
+        p["pe"], abs=0.01 + p["natoms"] * E_PER_ATOM_OTHER)
+
+
 def test_three_elements_against_oracle():
     pub = published()["AlMgSi"]
     x, t, box = read_data(GOLDEN / "AlMgSi.data")

@@ -39,6 +39,20 @@ def test_moni_m3_energy_forces_pressure(pub):
     assert np.abs(out["f"]).max() == pytest.approx(p["fmax_component"], abs=1e-9)
 
 
+def test_moni_squareplus_energy_pressure(pub):
+    """MoNi_squareplus_500k on the Mo8Ni8 cell replicated 10 x 10 x 10: the
+    step-0 energy (8 significant digits) within one unit of the last digit,
+    the pressure (virial part plus the kinetic part at 100 K) within 2e-3 bar."""
+    p = pub["MoNi_squareplus"]
+    x, t, box = read_data(GOLDEN / "Mo8_Ni8_id3210.data")
+    o = Oracle(str(GOLDEN / "MoNi_squareplus_500k.npz"), interp=p["interp"])
+    out = o.compute(x, t - 1, box, [1, 1, 1])
+    assert out["energy"] * p["replicas"] == pytest.approx(p["pe"], abs=0.01)
+    p_vir = out["virial"][:3].mean() / volume(box) * NKTV2P
+    p_kin = kinetic_pressure(p["natoms"], p["temp"], volume(box) * p["replicas"])
+    assert p_vir + p_kin == pytest.approx(p["press"], abs=2e-3)
+
+
 def test_almgsi_energy(pub):
     p = pub["AlMgSi"]
     x, t, box = read_data(GOLDEN / "AlMgSi.data")
