@@ -367,7 +367,7 @@ __device__ inline void res_gemm_bwd(const float *gzT, int Nc, const float *W, in
       float4 wj[4];
 #pragma unroll
       for (int j = 0; j < 4; j++)
-        wj[j] = kv[j] ? *reinterpret_cast<const float4 *>(wr[j] + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+        wj[j] = *reinterpret_cast<const float4 *>(wr[j] + c);  // row 0 where !kv[j]: not stored
       float g[4][RT];
 #pragma unroll
       for (int q = 0; q < 4; q++) load_rows<RT>(gp + (c + q) * LDT, g[q]);
